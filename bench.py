@@ -1,0 +1,377 @@
+#!/usr/bin/env python
+"""Benchmark: spectra/s of the per-k-point Bloch integration -> BZ current
+sum -> trapezoidal FFT path on the 256x256 PiFlux-2D workload.
+
+One step = one spectrum: integrate all 65 536 k-points over the 8-cycle
+pulse (8192 measurement intervals), reduce j(t), FFT it.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--variant fp64|carry|mixed|mixed_carry]
+  python bench.py --impl reference ...   # the oracle port on the host cores
+
+Under torchrun (N > 1) every rank integrates its own pulse instance (the
+carrier phase differs per rank): weak scaling with no data-path collective;
+the only collectives are the barrier and the max-over-ranks timing.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "spectra/sec at harmonic err <=1e-4 vs FP64"
+UNIT = "spectra/s"
+
+# Algorithmic FP64 flops per attempted RKF78 step (one k-point): 13 right-hand
+# sides plus the tableau arithmetic 2*3*55 (stages) + 2*3*7 (solution) +
+# 2*3*4 (error) + ~25 (norm and control) = 421; the right-hand side of the
+# 2D pi-flux model costs 12 flops plus two cosines (counted separately).
+ALG_FLOPS_PER_KSTEP = {"piflux2d_256": 13 * 12 + 421, "dirac2d_64": 13 * 16 + 421,
+                       "honeycomb_512": 13 * 30 + 421, "dirac2d_sweep": 13 * 16 + 421}
+SPECIAL_OPS_PER_KSTEP = {"piflux2d_256": 26, "dirac2d_64": 0, "honeycomb_512": 78,
+                         "dirac2d_sweep": 0}
+
+VARIANTS = {
+    "fp64": dict(),
+    "carry": dict(proposer=1),
+    "mixed": dict(precision=1, abs_tol=1e-8, rel_tol=1e-6),
+    "mixed_carry": dict(precision=1, proposer=1, abs_tol=1e-8, rel_tol=1e-6),
+}
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid: str | None):
+        self.uuid = uuid
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+               "-lms", "200"]
+        if self.uuid:
+            cmd += ["-i", self.uuid]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=open(self.path, "w"),
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+class CpuBaseline:
+    """The oracle port timed on the host cores over a strided k-subsample of
+    the workload; spectra/s are extrapolated to the full grid."""
+
+    def __init__(self, wl, rows, target_s: float):
+        from oracle import hhg_oracle as O
+        from tests.helpers import oracle_args
+        self.O = O
+        p = wl.pulses[0]
+        self.args = oracle_args(wl.system, p, wl.opts_kw["abs_tol"], wl.opts_kw["rel_tol"])
+        self.cores = (len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity")
+                      else os.cpu_count())
+        self.n_k = rows.shape[0]
+        m, p, tc, s = self.args
+        calib = rows[:: max(1, self.n_k // max(self.cores, 8))][: max(self.cores, 8)]
+        t0 = time.perf_counter()
+        O.current_density(m, p, tc, s, calib, threads=self.cores, fast=True)
+        per_k = (time.perf_counter() - t0) / calib.shape[0]
+        n_sample = int(min(self.n_k, max(self.cores, target_s / max(per_k, 1e-9))))
+        self.stride = max(1, self.n_k // n_sample)
+        self.sample = np.ascontiguousarray(rows[:: self.stride])
+        self.n_meas = tc.n_measurements
+
+    def run(self):
+        m, p, tc, s = self.args
+        t0 = time.perf_counter()
+        _, st, rc = self.O.current_density(m, p, tc, s, self.sample, threads=self.cores,
+                                           fast=True)
+        el = time.perf_counter() - t0
+        if rc != 0:
+            raise RuntimeError(f"oracle status {rc}")
+        spectra_per_s = 1.0 / (el * self.n_k / self.sample.shape[0])
+        desc = (f"every {self.stride}th k-point ({self.sample.shape[0]} of {self.n_k}) over the "
+                f"full {self.n_meas}-interval pulse, {st.attempted} k.steps in {el:.2f} s on "
+                f"{self.cores} threads (oracle port, -O3 -ffast-math, OpenMP); spectra/s "
+                f"scaled by {self.n_k}/{self.sample.shape[0]}")
+        return spectra_per_s, desc, st.attempted / el
+
+
+def reference_arm(args, wl_name):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    from higherharmonics_b200 import workloads as W
+    from higherharmonics_b200 import api
+    wl = W.ALL[wl_name]()
+    rows = api.grid_rows(wl.system, wl.grid)
+    cb = CpuBaseline(wl, rows, target_s=args.cpu_seconds)
+    per_step = []
+    desc = ksps = None
+    for i in range(args.warmup + args.steps):
+        v, desc, ksps = cb.run()
+        if i >= args.warmup:
+            per_step.append(1.0 / v)
+    t = float(np.mean(per_step))
+    value = 1.0 / t
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": config_for(wl, "oracle port, plain FP64 RKF78"),
+        "k_steps_per_s": ksps,
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cb.cores, "kind": "port",
+                         "sample": desc},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def config_for(wl, variant_desc):
+    p = wl.pulses[0]
+    return {"workload": wl.name, "k_points": wl.n_k, "n_measurements": p.n_measurements,
+            "pulses": len(wl.pulses), "tolerances": f"{wl.opts_kw['abs_tol']:g}/{wl.opts_kw['rel_tol']:g}",
+            "variant": variant_desc,
+            "l2": "flushed (256 MiB write) before every timed step; inputs < L2"}
+
+
+def traffic_from_profile(wl_name):
+    """Per-launch DRAM bytes of the integration kernel from the committed ncu
+    summary (a line 'traffic_bytes_per_launch[<workload>]: <bytes>')."""
+    path = os.path.join(ROOT, "profiles", "bz_integrate_kernel.md")
+    if not os.path.exists(path):
+        return None
+    key = f"traffic_bytes_per_launch[{wl_name}]:"
+    for line in open(path):
+        if line.strip().startswith(key):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def our_arm(args, wl_name):
+    import torch
+    ws, rank, local = dist_env()
+    if ws > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+    from higherharmonics_b200 import api
+    from higherharmonics_b200 import workloads as W
+    from higherharmonics_b200.analysis import (default_max_order, harmonic_intensities,
+                                               harmonic_rel_err)
+
+    wl = W.ALL[wl_name]()
+    if ws > 1:  # one pulse instance per rank: weak scaling
+        for p in wl.pulses:
+            p.phase = p.phase + 0.1 * rank
+    eng = api.Engine(dev)
+    okw = VARIANTS[args.variant]
+    plan = eng.plan(wl.system, wl.pulses, wl.grid, wl.opts(**okw))
+    stream = torch.cuda.current_stream()
+    sptr = stream.cuda_stream
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def step():
+        plan.execute_async(sptr)
+        plan.spectrum_async(sptr)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    j0, st0 = plan.fetch()
+    ksteps = st0.attempted_steps
+
+    # accuracy of this variant against the plain FP64 engine (itself within
+    # 1e-9 of the oracle, see tests/test_gpu_parity.py)
+    herr = 0.0
+    if args.variant != "fp64":
+        fr, re, im = plan.fetch_spectrum(0)
+        ref = eng.plan(wl.system, wl.pulses, wl.grid, wl.opts())
+        ref.execute_async()
+        ref.spectrum_async()
+        ref.fetch(copy_j=False)
+        fr0, re0, im0 = ref.fetch_spectrum(0)
+        ref.close()
+        mo = default_max_order(fr0)
+        herr = harmonic_rel_err(harmonic_intensities(fr, re, im, mo),
+                                harmonic_intensities(fr0, re0, im0, mo), floor_rel=1e-6)
+
+    peak = eng.fp64_peak_tflops()
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    except Exception:
+        pass
+    sampler = ClockSampler(uuid)
+    sampler.start()
+    time.sleep(0.3)
+    if ws > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    e_start = torch.cuda.Event(enable_timing=True)
+    e_end = torch.cuda.Event(enable_timing=True)
+    e_start.record(stream)
+    for k in range(args.steps):
+        flush.zero_()
+        ev[k][0].record(stream)
+        plan.execute_async(sptr)
+        ev[k][1].record(stream)
+        plan.spectrum_async(sptr)
+    e_end.record(stream)
+    torch.cuda.synchronize()
+    if ws > 1:
+        torch.distributed.barrier()
+    clocks = sampler.stop()
+    elapsed_ms = e_start.elapsed_time(e_end)
+    launch_ms = [a.elapsed_time(b) for a, b in ev]
+    if ws > 1:
+        t = torch.tensor([elapsed_ms], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        elapsed_ms = float(t.item())
+    value = ws * args.steps / (elapsed_ms * 1e-3)
+
+    # end to end through the public API with host buffers
+    e2e = None
+    if not args.no_e2e:
+        n_e2e = max(1, min(args.steps, 3))
+        eng.current_density(wl.system, wl.pulses, wl.grid, wl.opts(**okw))
+        if ws > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(n_e2e):
+            j, st = eng.current_density(wl.system, wl.pulses, wl.grid, wl.opts(**okw))
+            p = wl.pulses[0]
+            eng.spectrum(j, p.n_measurements, p.window_begin, p.window_end)
+        torch.cuda.synchronize()
+        el = time.perf_counter() - t0
+        if ws > 1:
+            t = torch.tensor([el], device="cuda", dtype=torch.float64)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            el = float(t.item())
+        p = wl.pulses[0]
+        n_s = p.n_measurements + 1
+        n_fft = 4 * n_s + 1
+        h2d = wl.n_k * 64 + 256 * len(wl.pulses) + 8 * (p.n_measurements + 1) * 2 + 8 * n_s
+        d2h = 8 * n_s + 3 * 8 * n_fft
+        e2e = {"value": ws * n_e2e / el, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h),
+               "path": "Engine.current_density + Engine.spectrum (hhg_gpu_current_density + "
+                       "hhg_gpu_spectrum), host buffers, wall clock"}
+
+    if rank != 0:
+        if ws > 1:
+            torch.distributed.destroy_process_group()
+        return 0
+    avg_launch_s = float(np.mean(launch_ms)) * 1e-3
+    alg = ALG_FLOPS_PER_KSTEP.get(wl_name, 421) * ksteps
+    achieved = alg / avg_launch_s / 1e12
+    roofline = {"bound": "fp64_pipe", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": achieved / peak, "traffic": traffic_from_profile(wl_name),
+                "peak_source": "measured FP64 FMA throughput (hhg_measure_fp64_peak, burst); "
+                               "MEASURED_PEAKS.json has no FP64 figure",
+                "kernel": "bz_integrate_kernel", "kernel_ms": 1e3 * avg_launch_s,
+                "alg_flops_per_kstep": ALG_FLOPS_PER_KSTEP.get(wl_name, 421),
+                "special_ops_per_kstep": SPECIAL_OPS_PER_KSTEP.get(wl_name, 0)}
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if VARIANTS[args.variant].get("precision", 0) == 0 else "f32 rhs / f64 state",
+        "data": "synthetic", "config": config_for(wl, args.variant),
+        "k_steps_per_s": ws * ksteps / avg_launch_s if ws == 1 else None,
+        "k_steps_per_spectrum": ksteps, "harmonic_err_vs_fp64": herr,
+        "gpu_launches": 4 * args.steps, "roofline": roofline, "clocks": clocks, "e2e": e2e,
+    }
+    if ws == 1 and not args.no_cpu_baseline:
+        rows = api.grid_rows(wl.system, wl.grid)
+        cb = CpuBaseline(wl, rows, target_s=args.cpu_seconds)
+        v, desc, ksps = cb.run()
+        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": cb.cores, "kind": "port",
+                                "sample": desc, "k_steps_per_s": ksps}
+    print(json.dumps(line), flush=True)
+    plan.close()
+    eng.close()
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="piflux2d_256")
+    ap.add_argument("--variant", default="fp64", choices=sorted(VARIANTS))
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return reference_arm(args, args.workload)
+    return our_arm(args, args.workload)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,317 @@
+"""ctypes binding of the C ABI (include/hhg_gpu.h) and thin Python helpers.
+
+The compute path is ``libhhg_gpu.so`` (sm_100a kernels); this module only
+marshals descriptors.  There is no CPU fallback: if the library is missing or
+no CUDA device is visible, every call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libhhg_gpu.so")
+
+# enums (hhg_gpu.h)
+OK, BAD_CONFIG, STEP_LIMIT, NONFINITE, CUDA_ERROR, UNSUPPORTED = range(6)
+STATUS_NAMES = {0: "HHG_OK", 1: "HHG_BAD_CONFIG", 2: "HHG_STEP_LIMIT", 3: "HHG_NONFINITE",
+                4: "HHG_CUDA_ERROR", 5: "HHG_UNSUPPORTED"}
+SYS_DIRAC2D, SYS_PIFLUX2D, SYS_PIFLUX3D, SYS_HONEYCOMB, SYS_DIRAC3D = range(5)
+GRID_TENSOR_GL, GRID_RHOMBIC_GL, GRID_PIFLUX3D_REF, GRID_HONEYCOMB_HEX_REF, GRID_EXPLICIT = range(5)
+STEPPER_RKF78, STEPPER_MAGNUS4 = 0, 1
+PREC_FP64, PREC_MIXED = 0, 1
+PROPOSER_NONE, PROPOSER_CARRY, PROPOSER_LEARNED = 0, 1, 2
+PULSE_COSINE = 0
+
+EXPORTED = [
+    "hhg_abi_version", "hhg_gpu_create", "hhg_gpu_destroy", "hhg_last_error",
+    "hhg_default_solver_opts", "hhg_gauss_legendre", "hhg_grid_rows",
+    "hhg_gpu_current_density", "hhg_gpu_spectrum", "hhg_plan_create", "hhg_plan_destroy",
+    "hhg_plan_j_length", "hhg_plan_execute_async", "hhg_plan_device_j", "hhg_plan_fetch",
+    "hhg_plan_spectrum_async", "hhg_plan_fetch_spectrum", "hhg_measure_fp64_peak",
+]
+
+
+class SystemDesc(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("hopping", ctypes.c_double), ("velocity", ctypes.c_double),
+                ("mass", ctypes.c_double), ("pol_x", ctypes.c_double), ("pol_y", ctypes.c_double)]
+
+
+class PulseDesc(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int32), ("n_measurements", ctypes.c_int32),
+                ("n_subdivisions", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("amplitude", ctypes.c_double), ("n_cycles", ctypes.c_double),
+                ("t_begin", ctypes.c_double), ("phase", ctypes.c_double),
+                ("window_begin", ctypes.c_double), ("window_end", ctypes.c_double),
+                ("energy_scale", ctypes.c_double)]
+
+
+class GridDesc(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int32), ("n1", ctypes.c_int32), ("n2", ctypes.c_int32),
+                ("reserved", ctypes.c_int32), ("x_lo", ctypes.c_double),
+                ("x_hi", ctypes.c_double), ("y_lo", ctypes.c_double), ("y_hi", ctypes.c_double),
+                ("rows", ctypes.POINTER(ctypes.c_double)), ("n_rows", ctypes.c_int64)]
+
+
+class SolverOpts(ctypes.Structure):
+    _fields_ = [("stepper", ctypes.c_int32), ("precision", ctypes.c_int32),
+                ("proposer", ctypes.c_int32), ("magnus_substeps", ctypes.c_int32),
+                ("abs_tol", ctypes.c_double), ("rel_tol", ctypes.c_double),
+                ("max_failed_steps", ctypes.c_int32), ("max_attempts_per_interval", ctypes.c_int32),
+                ("tile_k", ctypes.c_int32), ("block_threads", ctypes.c_int32)]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("k_points", ctypes.c_int64), ("trajectories", ctypes.c_int64),
+                ("attempted_steps", ctypes.c_int64), ("rejected_steps", ctypes.c_int64),
+                ("failed_trajectories", ctypes.c_int64), ("poly_degree", ctypes.c_int32),
+                ("items", ctypes.c_int32), ("kernel_ms", ctypes.c_double),
+                ("total_ms", ctypes.c_double)]
+
+    def as_dict(self) -> dict:
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
+class HHGError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+_lib = None
+_D = ctypes.POINTER(ctypes.c_double)
+
+
+def load_library() -> ctypes.CDLL:
+    """Load libhhg_gpu.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with "
+                              "`python -c 'import __graft_entry__ as g; g.build()'` or "
+                              "`make -C higherharmonics_b200/csrc`")
+        L = ctypes.CDLL(LIB_PATH)
+        L.hhg_last_error.restype = ctypes.c_char_p
+        L.hhg_last_error.argtypes = [ctypes.c_void_p]
+        L.hhg_gpu_create.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int]
+        L.hhg_gpu_destroy.argtypes = [ctypes.c_void_p]
+        L.hhg_plan_create.argtypes = [ctypes.c_void_p, ctypes.POINTER(SystemDesc),
+                                      ctypes.POINTER(PulseDesc), ctypes.c_int,
+                                      ctypes.POINTER(GridDesc), ctypes.POINTER(SolverOpts),
+                                      ctypes.POINTER(ctypes.c_void_p)]
+        L.hhg_plan_destroy.argtypes = [ctypes.c_void_p]
+        L.hhg_plan_j_length.argtypes = [ctypes.c_void_p]
+        L.hhg_plan_j_length.restype = ctypes.c_int64
+        L.hhg_plan_execute_async.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.hhg_plan_device_j.argtypes = [ctypes.c_void_p]
+        L.hhg_plan_device_j.restype = ctypes.c_void_p
+        L.hhg_plan_fetch.argtypes = [ctypes.c_void_p, _D, ctypes.POINTER(Stats)]
+        L.hhg_gpu_current_density.argtypes = [ctypes.c_void_p, ctypes.POINTER(SystemDesc),
+                                              ctypes.POINTER(PulseDesc), ctypes.c_int,
+                                              ctypes.POINTER(GridDesc), ctypes.POINTER(SolverOpts),
+                                              _D, ctypes.POINTER(Stats)]
+        L.hhg_gpu_spectrum.argtypes = [ctypes.c_void_p, _D, ctypes.c_int, ctypes.c_double,
+                                       ctypes.c_double, _D, _D, _D]
+        L.hhg_grid_rows.argtypes = [ctypes.POINTER(SystemDesc), ctypes.POINTER(GridDesc), _D,
+                                    ctypes.POINTER(ctypes.c_int64)]
+        L.hhg_gauss_legendre.argtypes = [ctypes.c_int, _D, _D]
+        L.hhg_plan_spectrum_async.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.hhg_plan_fetch_spectrum.argtypes = [ctypes.c_void_p, ctypes.c_int, _D, _D, _D]
+        L.hhg_measure_fp64_peak.argtypes = [ctypes.c_void_p, _D]
+        L.hhg_default_solver_opts.argtypes = [ctypes.POINTER(SolverOpts)]
+        _lib = L
+    return _lib
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(_D)
+
+
+# ---------------------------------------------------------------------------
+# descriptor helpers
+# ---------------------------------------------------------------------------
+def system(kind: int, hopping=0.0, velocity=0.0, mass=0.0, pol=(1.0, 0.0)) -> SystemDesc:
+    return SystemDesc(kind, 0, hopping, velocity, mass, pol[0], pol[1])
+
+
+def cosine_pulse(amplitude: float, n_cycles: float, n_measurements: int, *, t_begin=0.0,
+                 phase=0.0, window=None, energy_scale=1.0, n_subdivisions=50) -> PulseDesc:
+    """CosineLaser + its TimeIntegrationConfig.  ``window`` defaults to the
+    pulse itself, [t_begin, t_begin + 2 pi n_cycles] (DiracDispatcher.cpp:37);
+    the PiFlux/Honeycomb dispatchers add one cycle (PiFluxDispatcher.cpp:53)."""
+    if window is None:
+        window = (t_begin, t_begin + 2 * math.pi * n_cycles)
+    return PulseDesc(PULSE_COSINE, n_measurements, n_subdivisions, 0, amplitude, n_cycles,
+                     t_begin, phase, window[0], window[1], energy_scale)
+
+
+def grid_tensor(n1, n2, x_lo, x_hi, y_lo, y_hi) -> GridDesc:
+    return GridDesc(GRID_TENSOR_GL, n1, n2, 0, x_lo, x_hi, y_lo, y_hi, None, 0)
+
+
+def grid_rhombic(n1, n2) -> GridDesc:
+    return GridDesc(GRID_RHOMBIC_GL, n1, n2, 0, 0, 0, 0, 0, None, 0)
+
+
+def grid_piflux3d_ref(z_range=32, n_coarse=4) -> GridDesc:
+    return GridDesc(GRID_PIFLUX3D_REF, z_range, n_coarse, 0, 0, 0, 0, 0, None, 0)
+
+
+def grid_honeycomb_hex_ref(n_k=64) -> GridDesc:
+    return GridDesc(GRID_HONEYCOMB_HEX_REF, n_k, 0, 0, 0, 0, 0, 0, None, 0)
+
+
+def grid_explicit(rows: np.ndarray) -> tuple[GridDesc, np.ndarray]:
+    rows = np.ascontiguousarray(rows, dtype=np.float64)
+    assert rows.ndim == 2 and rows.shape[1] == 8
+    return GridDesc(GRID_EXPLICIT, 0, 0, 0, 0, 0, 0, 0, _ptr(rows), rows.shape[0]), rows
+
+
+def solver(abs_tol=1e-12, rel_tol=1e-8, stepper=STEPPER_RKF78, precision=PREC_FP64,
+           proposer=PROPOSER_NONE, magnus_substeps=1, tile_k=0) -> SolverOpts:
+    o = SolverOpts()
+    load_library().hhg_default_solver_opts(ctypes.byref(o))
+    o.abs_tol, o.rel_tol = abs_tol, rel_tol
+    o.stepper, o.precision, o.proposer = stepper, precision, proposer
+    o.magnus_substeps, o.tile_k = magnus_substeps, tile_k
+    return o
+
+
+def gauss_legendre(n: int):
+    x = np.zeros(n)
+    w = np.zeros(n)
+    st = load_library().hhg_gauss_legendre(n, _ptr(x), _ptr(w))
+    if st != OK:
+        raise HHGError(st, "hhg_gauss_legendre")
+    return x, w
+
+
+def grid_rows(sys: SystemDesc, grid: GridDesc) -> np.ndarray:
+    L = load_library()
+    n = ctypes.c_int64(0)
+    st = L.hhg_grid_rows(ctypes.byref(sys), ctypes.byref(grid), None, ctypes.byref(n))
+    if st != OK:
+        raise HHGError(st, "hhg_grid_rows")
+    out = np.zeros((n.value, 8))
+    st = L.hhg_grid_rows(ctypes.byref(sys), ctypes.byref(grid), _ptr(out), ctypes.byref(n))
+    if st != OK:
+        raise HHGError(st, "hhg_grid_rows")
+    return out
+
+
+# ---------------------------------------------------------------------------
+# context / plans
+# ---------------------------------------------------------------------------
+class Engine:
+    """One hhg_ctx on one device."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load_library()
+        self.ctx = ctypes.c_void_p()
+        st = self.lib.hhg_gpu_create(ctypes.byref(self.ctx), device)
+        if st != OK:
+            raise HHGError(st, f"hhg_gpu_create(device={device}) failed")
+
+    def _check(self, st: int, what: str):
+        if st != OK:
+            raise HHGError(st, f"{what}: {self.lib.hhg_last_error(self.ctx).decode()}")
+
+    def close(self):
+        if self.ctx:
+            self.lib.hhg_gpu_destroy(self.ctx)
+            self.ctx = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def current_density(self, sys: SystemDesc, pulses, grid: GridDesc,
+                        opts: SolverOpts | None = None) -> tuple[np.ndarray, Stats]:
+        pulses = list(pulses) if not isinstance(pulses, PulseDesc) else [pulses]
+        arr = (PulseDesc * len(pulses))(*pulses)
+        n = sum(p.n_measurements + 1 for p in pulses)
+        j = np.zeros(n)
+        st = Stats()
+        o = opts if opts is not None else solver()
+        self._check(self.lib.hhg_gpu_current_density(self.ctx, ctypes.byref(sys), arr,
+                                                     len(pulses), ctypes.byref(grid),
+                                                     ctypes.byref(o), _ptr(j), ctypes.byref(st)),
+                    "hhg_gpu_current_density")
+        return j, st
+
+    def spectrum(self, j: np.ndarray, n_measurements: int, t_begin: float, t_end: float):
+        j = np.ascontiguousarray(j, dtype=np.float64)
+        n_fft = 4 * (n_measurements + 1) + 1
+        re = np.zeros(n_fft)
+        im = np.zeros(n_fft)
+        fr = np.zeros(n_fft)
+        self._check(self.lib.hhg_gpu_spectrum(self.ctx, _ptr(j), n_measurements, t_begin, t_end,
+                                              _ptr(re), _ptr(im), _ptr(fr)), "hhg_gpu_spectrum")
+        return fr, re, im
+
+    def plan(self, sys: SystemDesc, pulses, grid: GridDesc, opts: SolverOpts | None = None):
+        return Plan(self, sys, pulses, grid, opts)
+
+    def fp64_peak_tflops(self) -> float:
+        v = ctypes.c_double(0.0)
+        self._check(self.lib.hhg_measure_fp64_peak(self.ctx, ctypes.byref(v)),
+                    "hhg_measure_fp64_peak")
+        return v.value
+
+
+class Plan:
+    def __init__(self, eng: Engine, sys, pulses, grid, opts=None):
+        self.eng = eng
+        pulses = list(pulses) if not isinstance(pulses, PulseDesc) else [pulses]
+        self.pulses = pulses
+        arr = (PulseDesc * len(pulses))(*pulses)
+        o = opts if opts is not None else solver()
+        self.handle = ctypes.c_void_p()
+        eng._check(eng.lib.hhg_plan_create(eng.ctx, ctypes.byref(sys), arr, len(pulses),
+                                           ctypes.byref(grid), ctypes.byref(o),
+                                           ctypes.byref(self.handle)), "hhg_plan_create")
+        self.j_len = int(eng.lib.hhg_plan_j_length(self.handle))
+
+    def execute_async(self, stream: int | None = None):
+        self.eng._check(self.eng.lib.hhg_plan_execute_async(
+            self.handle, ctypes.c_void_p(stream) if stream else None), "hhg_plan_execute_async")
+
+    def spectrum_async(self, stream: int | None = None):
+        self.eng._check(self.eng.lib.hhg_plan_spectrum_async(
+            self.handle, ctypes.c_void_p(stream) if stream else None), "hhg_plan_spectrum_async")
+
+    def fetch_spectrum(self, pulse: int = 0):
+        n_fft = 4 * (self.pulses[pulse].n_measurements + 1) + 1
+        re, im, fr = np.zeros(n_fft), np.zeros(n_fft), np.zeros(n_fft)
+        self.eng._check(self.eng.lib.hhg_plan_fetch_spectrum(self.handle, pulse, _ptr(re),
+                                                             _ptr(im), _ptr(fr)),
+                        "hhg_plan_fetch_spectrum")
+        return fr, re, im
+
+    def device_j_ptr(self) -> int:
+        return int(self.eng.lib.hhg_plan_device_j(self.handle))
+
+    def fetch(self, copy_j: bool = True):
+        j = np.zeros(self.j_len) if copy_j else None
+        st = Stats()
+        self.eng._check(self.eng.lib.hhg_plan_fetch(self.handle, _ptr(j) if copy_j else None,
+                                                    ctypes.byref(st)), "hhg_plan_fetch")
+        return j, st
+
+    def close(self):
+        if self.handle:
+            self.eng.lib.hhg_plan_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,771 @@
+// hhg_device.cuh -- sm_100a device code for the per-k-point Bloch integration
+// (controlled RKF78 / Magnus-4) fused with the Gauss-weighted Brillouin-zone
+// current sum.
+//
+// Execution model: one lane owns one (pulse, k-point) trajectory.  A warp owns
+// a work item = one pulse x (32 * tiles) consecutive k-points and walks the
+// reference's measurement loop (PiFlux.cpp:96-110) interval by interval; the
+// lanes are lock-stepped per interval (every lane must land on t_i), and
+// inside an interval each lane runs its own adaptive step sequence under
+// predication.  The pulse is staged per interval in shared memory as Chebyshev
+// interpolants (monomial form in u in [-1,1]) of A(t) or of cos/sin(s A(t)),
+// so no transcendental is evaluated inside a right-hand side.  At every sample
+// the lanes' weighted current contributions are reduced with a butterfly
+// shuffle; lane (i mod 32) keeps sample i and every 32 samples the warp
+// stores its 32 sums with one coalesced 256-byte store into the work item's
+// row of the partial buffer.  Work items are taken from a global atomic
+// counter (persistent, work-stealing launch), and a second kernel reduces the
+// partial rows of each pulse in item order with compensated sums, so j(t) is
+// bitwise reproducible whatever the schedule.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace hhg {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr double kDblEps = 2.220446049250313080847e-16;  // std::numeric_limits<double>::epsilon()
+
+enum Model { DIRAC2D = 0, PIFLUX2D = 1, PIFLUX3D = 2, HONEYCOMB = 3, DIRAC3D = 4 };
+enum FuncKind { F_A = 0, F_COS = 1, F_SIN = 2 };
+
+// Staged functions per model: value of each outside the pulse window
+// (CosineLaser::envelope returns 0 for t <= t_begin or t >= t_end).
+template <int M> struct Traits;
+template <> struct Traits<DIRAC2D> { static constexpr int NF = 1; };
+template <> struct Traits<DIRAC3D> { static constexpr int NF = 1; };
+template <> struct Traits<PIFLUX3D> { static constexpr int NF = 2; };   // cos A, sin A
+template <> struct Traits<PIFLUX2D> { static constexpr int NF = 4; };   // cos/sin(px A), cos/sin(py A)
+template <> struct Traits<HONEYCOMB> { static constexpr int NF = 6; };  // cos/sin(s_j A), j = 0..2
+
+// Per-interval record (doubles): [0] t0, [1] t1, [2] center, [3] 1/half-width,
+// [4] A(t_s) and [5, 5 + nf) the staged functions evaluated exactly at the
+// interval's end sample t_s = (i+1) * measure_every + window_begin, then
+// nf blocks of deg + 1 monomial coefficients starting at a 16-byte boundary.
+__host__ __device__ constexpr int slot_header(int nf) { return (5 + nf + 1) & ~1; }
+__host__ __device__ constexpr int slot_doubles(int nf, int deg) {
+    return slot_header(nf) + nf * (deg + 1) + ((nf * (deg + 1)) & 1);
+}
+// Value of staged function n outside the pulse window: A -> 0, cos -> 1, sin -> 0.
+template <int NF> __host__ __device__ constexpr double outside_value(int n) {
+    return (NF > 1 && (n % 2) == 0) ? 1.0 : 0.0;
+}
+
+// Per-pulse constants, prepared on the host.
+struct PulseDev {
+    double amplitude, t_begin, t_end, inv_n_cycles, phase;
+    double window_begin, measure_every, dt0;
+    double mp[8];   // model constants already multiplied by the energy scale
+    double s[3];    // staged projections s_j (honeycomb: nn_j . pol; piflux2d: px, py)
+    double s0rec[8];  // sample-0 record: A(t_0), staged functions at A(t_0)
+    long long coef_off;   // doubles into the staging table
+    long long part_off;   // doubles into the partial buffer
+    long long j_off;      // samples into j
+    int n_meas;
+    int items;            // work items of this pulse
+};
+
+struct KParams {
+    const double *ktab;   // n_k rows of 8 doubles
+    const PulseDev *pulses;
+    const double *coef;   // staging table
+    double *part;         // partial rows
+    unsigned long long *counters;  // [0] next item [1] attempted [2] rejected [3] failed [4] nonfinite
+    int *status;
+    long long n_items;
+    int n_k;
+    int tiles_per_item;
+    int items_per_pulse;
+    int max_failed;
+    int max_attempts;
+    int magnus_substeps;
+    double abs_tol, rel_tol;
+    double grow_max;      // 0.9 * pow(pow(5, -8), -1/8), computed with the host libm
+    double err_floor;     // pow(5, -8)
+};
+
+// ---------------------------------------------------------------------------
+// Pulse (exact, for the sample-time vertices): Laser::laser_function with
+// CosineLaser::envelope (Laser.hpp:32-37, CosineLaser.cpp:22-26).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double laser_exact(const PulseDev &p, double t) {
+    double env = 0.0;
+    if (!(t <= p.t_begin || t >= p.t_end)) env = 0.5 * (1. - cos(p.inv_n_cycles * (t - p.t_begin)));
+    return p.amplitude * (env * sin(t + p.phase));
+}
+
+// Analytic continuation used for staging (no window cut).
+__device__ __forceinline__ double laser_continued(const PulseDev &p, double t) {
+    const double env = 0.5 * (1. - cos(p.inv_n_cycles * (t - p.t_begin)));
+    return p.amplitude * (env * sin(t + p.phase));
+}
+
+// ---------------------------------------------------------------------------
+// Staged evaluation: f_n(t) = sum_j c_nj u^j, u = (t - center) * inv_half.
+// ---------------------------------------------------------------------------
+template <int NF, int D, typename R>
+__device__ __forceinline__ void eval_staged(const double *__restrict__ hd, const R *__restrict__ sc,
+                                            double t, double tb, double te, R f[NF]) {
+    const R u = R((t - hd[2]) * hd[3]);
+    const bool inside = (t > tb) && (t < te);
+#pragma unroll
+    for (int n = 0; n < NF; ++n) {
+        const R *c = sc + n * (D + 1);
+        R v = c[D];
+#pragma unroll
+        for (int j = D - 1; j >= 0; --j) v = fma(v, u, c[j]);
+        f[n] = inside ? v : R(outside_value<NF>(n));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Models.  init() reads the k row and the pulse's scaled constants; rhs()
+// evaluates dS/dt from the staged values f; vertex() is the current
+// contribution (weight excluded) from the sample record r = [A(t_s), staged
+// functions evaluated exactly at t_s]; dvec() is d with dS/dt = 2 d x S.
+// ---------------------------------------------------------------------------
+template <int M, typename R> struct ModelState;
+
+// gapped 2D Dirac, d = (v (kx - px A), v (ky - py A), mass); dS/dt = 2 d x S.
+// mp: [0] 2v, [1] 2 mass, [2] px, [3] py
+template <typename R> struct ModelState<DIRAC2D, R> {
+    R ax, ay, bx, by, dz;
+    double px, py;
+    __device__ __forceinline__ void init(const PulseDev &p, const double *row) {
+        ax = R(p.mp[0] * row[0]);
+        ay = R(p.mp[0] * row[1]);
+        bx = R(p.mp[0] * p.mp[2]);
+        by = R(p.mp[0] * p.mp[3]);
+        dz = R(p.mp[1]);
+        px = p.mp[2];
+        py = p.mp[3];
+    }
+    __device__ __forceinline__ void rhs(const R *f, const R *S, R *dS) const {
+        const R d0 = ax - bx * f[0], d1 = ay - by * f[0];
+        dS[0] = d1 * S[2] - dz * S[1];
+        dS[1] = dz * S[0] - d0 * S[2];
+        dS[2] = d0 * S[1] - d1 * S[0];
+    }
+    __device__ __forceinline__ double vertex(const double *, const double *S) const {
+        return px * S[0] + py * S[1];
+    }
+    __device__ __forceinline__ void dvec(const R *f, R *d) const {
+        d[0] = R(0.5) * (ax - bx * f[0]);
+        d[1] = R(0.5) * (ay - by * f[0]);
+        d[2] = R(0.5) * dz;
+    }
+};
+
+// Reference PiFlux (PiFlux.cpp:89-94): dS/dt = 4t (cx, cy, cos(kz - A)) x S,
+// cos(kz - A) = cos kz cos A + sin kz sin A.  mp: [0] 4t
+template <typename R> struct ModelState<PIFLUX3D, R> {
+    R m0, m1, pcz, psz;
+    double cz, sz;
+    __device__ __forceinline__ void init(const PulseDev &p, const double *row) {
+        const double pf = p.mp[0];
+        m0 = R(pf * cos(row[0]));
+        m1 = R(pf * cos(row[1]));
+        sincos(row[2], &sz, &cz);
+        pcz = R(pf * cz);
+        psz = R(pf * sz);
+    }
+    __device__ __forceinline__ void rhs(const R *f, const R *S, R *dS) const {
+        const R m2 = pcz * f[0] + psz * f[1];
+        dS[0] = m1 * S[2] - m2 * S[1];
+        dS[1] = m2 * S[0] - m0 * S[2];
+        dS[2] = m0 * S[1] - m1 * S[0];
+    }
+    __device__ __forceinline__ double vertex(const double *r, const double *S) const {
+        // sin(k.z - A(t_i)) S_z (PiFlux.cpp:832-838)
+        return (sz * r[1] - cz * r[2]) * S[2];
+    }
+    __device__ __forceinline__ void dvec(const R *f, R *d) const {
+        d[0] = R(0.5) * m0;
+        d[1] = R(0.5) * m1;
+        d[2] = R(0.5) * (pcz * f[0] + psz * f[1]);
+    }
+};
+
+// 2D pi-flux, d = -2t (cos(kx - px A), cos(ky - py A), 0); dS/dt = 2 d x S.
+// mp: [0] -4t, [2] px, [3] py
+template <typename R> struct ModelState<PIFLUX2D, R> {
+    R pcx, psx, pcy, psy;
+    double cx, sx, cy, sy, px, py;
+    __device__ __forceinline__ void init(const PulseDev &p, const double *row) {
+        const double pf = p.mp[0];
+        sincos(row[0], &sx, &cx);
+        sincos(row[1], &sy, &cy);
+        pcx = R(pf * cx);
+        psx = R(pf * sx);
+        pcy = R(pf * cy);
+        psy = R(pf * sy);
+        px = p.mp[2];
+        py = p.mp[3];
+    }
+    __device__ __forceinline__ void rhs(const R *f, const R *S, R *dS) const {
+        const R m0 = pcx * f[0] + psx * f[1];
+        const R m1 = pcy * f[2] + psy * f[3];
+        dS[0] = m1 * S[2];
+        dS[1] = -(m0 * S[2]);
+        dS[2] = m0 * S[1] - m1 * S[0];
+    }
+    __device__ __forceinline__ double vertex(const double *r, const double *S) const {
+        // px sin(kx - px A) S_x + py sin(ky - py A) S_y
+        return px * (sx * r[1] - cx * r[2]) * S[0] + py * (sy * r[3] - cy * r[4]) * S[1];
+    }
+    __device__ __forceinline__ void dvec(const R *f, R *d) const {
+        d[0] = R(0.5) * (pcx * f[0] + psx * f[1]);
+        d[1] = R(0.5) * (pcy * f[2] + psy * f[3]);
+        d[2] = R(0);
+    }
+};
+
+// Reference Honeycomb (Honeycomb.cpp:131-138) with an optional staggered mass:
+// gamma' = sum_j e^{i nn_j.k} e^{-i s_j A}, s_j = nn_j . pol,
+// dS = (-pf Sz Im g - 2m Sy, -pf Sz Re g + 2m Sx, pf (Sx Im g + Sy Re g)).
+// mp: [0] 2t (pf), [1] 2 mass, [2] px, [3] py
+template <typename R> struct ModelState<HONEYCOMB, R> {
+    R c0, s0, c1, s1, c2, s2;  // cos/sin(nn_j . k)
+    R pf, dm;
+    double px, py;
+    __device__ __forceinline__ void init(const PulseDev &p, const double *row) {
+        const double nny = 0.5 * 1.732050807568877293527446341;
+        double s, c;
+        sincos(row[0], &s, &c);
+        c0 = R(c), s0 = R(s);
+        sincos(-0.5 * row[0] + nny * row[1], &s, &c);
+        c1 = R(c), s1 = R(s);
+        sincos(-0.5 * row[0] - nny * row[1], &s, &c);
+        c2 = R(c), s2 = R(s);
+        pf = R(p.mp[0]);
+        dm = R(p.mp[1]);
+        px = p.mp[2];
+        py = p.mp[3];
+    }
+    __device__ __forceinline__ void gamma(const R *f, R &gre, R &gim) const {
+        // e^{i(a - b)} = (ca cb + sa sb) + i (sa cb - ca sb)
+        gre = (c0 * f[0] + s0 * f[1]) + (c1 * f[2] + s1 * f[3]) + (c2 * f[4] + s2 * f[5]);
+        gim = (s0 * f[0] - c0 * f[1]) + (s1 * f[2] - c1 * f[3]) + (s2 * f[4] - c2 * f[5]);
+    }
+    __device__ __forceinline__ void rhs(const R *f, const R *S, R *dS) const {
+        R gre, gim;
+        gamma(f, gre, gim);
+        gre *= pf;
+        gim *= pf;
+        dS[0] = -(S[2] * gim) - dm * S[1];
+        dS[1] = -(S[2] * gre) + dm * S[0];
+        dS[2] = S[0] * gim + S[1] * gre;
+    }
+    __device__ __forceinline__ double vertex(const double *r, const double *S) const {
+        // shifted_grad_gamma and the projection (Honeycomb.cpp:49-61, 273-279, 328-330)
+        const double nny = 0.5 * 1.732050807568877293527446341;
+        const double e0r = double(c0) * r[1] + double(s0) * r[2], e0i = double(s0) * r[1] - double(c0) * r[2];
+        const double e1r = double(c1) * r[3] + double(s1) * r[4], e1i = double(s1) * r[3] - double(c1) * r[4];
+        const double e2r = double(c2) * r[5] + double(s2) * r[6], e2i = double(s2) * r[5] - double(c2) * r[6];
+        const double g0r = e0r - 0.5 * e1r - 0.5 * e2r, g0i = e0i - 0.5 * e1i - 0.5 * e2i;
+        const double g1r = nny * e1r - nny * e2r, g1i = nny * e1i - nny * e2i;
+        const double bx = g0r * S[0] + g0i * S[1];
+        const double by = g1r * S[0] + g1i * S[1];
+        return bx * px + by * py;
+    }
+    __device__ __forceinline__ void dvec(const R *f, R *d) const {
+        // d = t (Re g', -Im g', mass) = 0.5 (pf Re g', -pf Im g', 2 mass)
+        R gre, gim;
+        gamma(f, gre, gim);
+        d[0] = R(0.5) * pf * gre;
+        d[1] = R(-0.5) * pf * gim;
+        d[2] = R(0.5) * dm;
+    }
+};
+
+// Reference DiracSystem sigma RHS (DiracSystem.cpp:144-153); row = (k_z, kappa, |k|).
+template <typename R> struct ModelState<DIRAC3D, R> {
+    R ax, az, mk2;
+    __device__ __forceinline__ void init(const PulseDev &, const double *row) {
+        ax = R(2.0 * row[1] / row[2]);
+        az = R(2.0 * row[0] / row[2]);
+        mk2 = R(2.0 * row[2]);
+    }
+    __device__ __forceinline__ void rhs(const R *f, const R *S, R *dS) const {
+        const R mx = f[0] * ax;
+        const R mz = mk2 - f[0] * az;
+        dS[0] = mz * S[1];
+        dS[1] = mx * S[2] - S[0] * mz;
+        dS[2] = -mx * S[1];
+    }
+    __device__ __forceinline__ double vertex(const double *, const double *S) const { return S[2]; }
+    __device__ __forceinline__ void dvec(const R *f, R *d) const {
+        // G = [[0, mz, 0], [-mz, 0, mx], [0, -mx, 0]] = [g]_x, g = (-mx, 0, -mz) = 2 d
+        d[0] = R(-0.5) * (f[0] * ax);
+        d[1] = R(0);
+        d[2] = R(-0.5) * (mk2 - f[0] * az);
+    }
+};
+
+// ---------------------------------------------------------------------------
+// One attempted Fehlberg 7(8) step (E. Fehlberg, NASA TR R-287, 1968):
+// 13 stages, the 8th-order solution propagated, error = b8 - b7 =
+// 41/840 (k12 + k13 - k1 - k11).  Stage sums are written out with the
+// tableau's nonzero entries only.  R is the right-hand-side precision; the
+// state, the solution increment and the error estimate are FP64.
+// ---------------------------------------------------------------------------
+template <int M, int NF, int D, typename R>
+__device__ __forceinline__ void rkf78_attempt(const ModelState<M, R> &ms, const double *hd,
+                                              const R *sc, double tb, double te, double t,
+                                              double h, const double *x, double *xn, double *e,
+                                              double *k0d) {
+    R k[13][3];
+    R f[NF];
+    const R xr[3] = {R(x[0]), R(x[1]), R(x[2])};
+    const R hr = R(h);
+    eval_staged<NF, D, R>(hd, sc, t, tb, te, f);
+    ms.rhs(f, xr, k[0]);
+#define HHG_STAGE(s, cs, EXPR)                                                        \
+    {                                                                                 \
+        R xt[3];                                                                      \
+        _Pragma("unroll") for (int i = 0; i < 3; ++i) xt[i] = xr[i] + hr * (EXPR);    \
+        eval_staged<NF, D, R>(hd, sc, t + (cs) * h, tb, te, f);                       \
+        ms.rhs(f, xt, k[s]);                                                          \
+    }
+    HHG_STAGE(1, 2.0 / 27.0, R(2.0 / 27.0) * k[0][i])
+    HHG_STAGE(2, 1.0 / 9.0, R(1.0 / 36.0) * k[0][i] + R(1.0 / 12.0) * k[1][i])
+    HHG_STAGE(3, 1.0 / 6.0, R(1.0 / 24.0) * k[0][i] + R(1.0 / 8.0) * k[2][i])
+    HHG_STAGE(4, 5.0 / 12.0,
+              R(5.0 / 12.0) * k[0][i] + R(-25.0 / 16.0) * k[2][i] + R(25.0 / 16.0) * k[3][i])
+    HHG_STAGE(5, 0.5, R(1.0 / 20.0) * k[0][i] + R(1.0 / 4.0) * k[3][i] + R(1.0 / 5.0) * k[4][i])
+    HHG_STAGE(6, 5.0 / 6.0,
+              R(-25.0 / 108.0) * k[0][i] + R(125.0 / 108.0) * k[3][i] +
+                  R(-65.0 / 27.0) * k[4][i] + R(125.0 / 54.0) * k[5][i])
+    HHG_STAGE(7, 1.0 / 6.0,
+              R(31.0 / 300.0) * k[0][i] + R(61.0 / 225.0) * k[4][i] + R(-2.0 / 9.0) * k[5][i] +
+                  R(13.0 / 900.0) * k[6][i])
+    HHG_STAGE(8, 2.0 / 3.0,
+              R(2.0) * k[0][i] + R(-53.0 / 6.0) * k[3][i] + R(704.0 / 45.0) * k[4][i] +
+                  R(-107.0 / 9.0) * k[5][i] + R(67.0 / 90.0) * k[6][i] + R(3.0) * k[7][i])
+    HHG_STAGE(9, 1.0 / 3.0,
+              R(-91.0 / 108.0) * k[0][i] + R(23.0 / 108.0) * k[3][i] +
+                  R(-976.0 / 135.0) * k[4][i] + R(311.0 / 54.0) * k[5][i] +
+                  R(-19.0 / 60.0) * k[6][i] + R(17.0 / 6.0) * k[7][i] + R(-1.0 / 12.0) * k[8][i])
+    HHG_STAGE(10, 1.0,
+              R(2383.0 / 4100.0) * k[0][i] + R(-341.0 / 164.0) * k[3][i] +
+                  R(4496.0 / 1025.0) * k[4][i] + R(-301.0 / 82.0) * k[5][i] +
+                  R(2133.0 / 4100.0) * k[6][i] + R(45.0 / 82.0) * k[7][i] +
+                  R(45.0 / 164.0) * k[8][i] + R(18.0 / 41.0) * k[9][i])
+    HHG_STAGE(11, 0.0,
+              R(3.0 / 205.0) * k[0][i] + R(-6.0 / 41.0) * k[5][i] + R(-3.0 / 205.0) * k[6][i] +
+                  R(-3.0 / 41.0) * k[7][i] + R(3.0 / 41.0) * k[8][i] + R(6.0 / 41.0) * k[9][i])
+    HHG_STAGE(12, 1.0,
+              R(-1777.0 / 4100.0) * k[0][i] + R(-341.0 / 164.0) * k[3][i] +
+                  R(4496.0 / 1025.0) * k[4][i] + R(-289.0 / 82.0) * k[5][i] +
+                  R(2193.0 / 4100.0) * k[6][i] + R(51.0 / 82.0) * k[7][i] +
+                  R(33.0 / 164.0) * k[8][i] + R(12.0 / 41.0) * k[9][i] + k[11][i])
+#undef HHG_STAGE
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const R inc = R(34.0 / 105.0) * k[5][i] + R(9.0 / 35.0) * (k[6][i] + k[7][i]) +
+                      R(9.0 / 280.0) * (k[8][i] + k[9][i]) +
+                      R(41.0 / 840.0) * (k[11][i] + k[12][i]);
+        xn[i] = x[i] + h * double(inc);
+        const R de = (k[11][i] + k[12][i]) - (k[0][i] + k[10][i]);
+        e[i] = (41.0 / 840.0 * h) * double(de);
+        k0d[i] = double(k[0][i]);
+    }
+}
+
+// Warp butterfly sum (every lane receives the same, order-fixed result).
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+    return v;
+}
+
+// Rodrigues rotation S <- exp([w]_x) S (series for theta < 1e-4).
+__device__ __forceinline__ void rotate(const double *w, double *S) {
+    const double th2 = w[0] * w[0] + w[1] * w[1] + w[2] * w[2];
+    double sa, ca;
+    if (th2 < 1e-8) {
+        sa = 1.0 - th2 / 6.0 + th2 * th2 / 120.0;
+        ca = 0.5 - th2 / 24.0 + th2 * th2 / 720.0;
+    } else {
+        const double th = sqrt(th2);
+        double s, c;
+        sincos(th, &s, &c);
+        sa = s / th;
+        ca = (1.0 - c) / th2;
+    }
+    const double wx0 = w[1] * S[2] - w[2] * S[1];
+    const double wx1 = w[2] * S[0] - w[0] * S[2];
+    const double wx2 = w[0] * S[1] - w[1] * S[0];
+    const double ww0 = w[1] * wx2 - w[2] * wx1;
+    const double ww1 = w[2] * wx0 - w[0] * wx2;
+    const double ww2 = w[0] * wx1 - w[1] * wx0;
+    S[0] += sa * wx0 + ca * ww0;
+    S[1] += sa * wx1 + ca * ww1;
+    S[2] += sa * wx2 + ca * ww2;
+}
+
+// ---------------------------------------------------------------------------
+// Persistent, work-stealing integration + BZ-sum kernel.
+// STEPPER 0: controlled RKF78 with the reference's integrate_adaptive
+//   semantics (PiFlux.cpp:104-110 calling Boost.Odeint): clip the step to
+//   land on t_end; loop while t_end - t > DBL_EPSILON; err = max_i |e_i| /
+//   (abs + rel (|x_i| + dt |dxdt_i|)); err > 1: dt *= max(0.9 err^-1/6, 0.2)
+//   and retry; else accept and, if err < 0.5, dt *= 0.9 max(err, 5^-8)^-1/8.
+// STEPPER 1: Magnus-4 (two-point Gauss), magnus_substeps steps per interval:
+//   omega = h (d1 + d2) + (sqrt3/3) h^2 (d2 x d1), S <- exp([omega]_x) S.
+// PROPOSER 0: every interval restarts at dt0 = measure_every/n_subdivisions
+//   (the reference); 1: an interval starts from the controller's last
+//   proposal of the previous interval.
+// ---------------------------------------------------------------------------
+template <int M, int D, typename R, int STEPPER, int PROPOSER>
+__global__ void __launch_bounds__(128) bz_integrate_kernel(const KParams P) {
+    constexpr int NF = Traits<M>::NF;
+    constexpr int SLOT = slot_doubles(NF, D);
+    constexpr int HDR = slot_header(NF);
+    constexpr bool kNarrow = sizeof(R) != sizeof(double);
+    constexpr int RCOEF = kNarrow ? NF * (D + 1) : 1;
+    __shared__ __align__(16) double stage_raw[4][SLOT];
+    __shared__ __align__(16) R stage_r[4][RCOEF];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    double *slot = stage_raw[wib];
+    const R *sc;
+    if constexpr (kNarrow) sc = stage_r[wib];
+    else sc = (const R *)(slot + HDR);
+
+    unsigned long long my_attempts = 0, my_rejects = 0;
+    for (;;) {
+        long long item = 0;
+        if (lane == 0) item = (long long)atomicAdd(P.counters, 1ull);
+        item = __shfl_sync(kFull, item, 0);
+        if (item >= P.n_items) break;
+        const int p = (int)(item / P.items_per_pulse);
+        const int tile = (int)(item % P.items_per_pulse);
+        const PulseDev &pd = P.pulses[p];
+        const int N = pd.n_meas;
+        const double dt0 = pd.dt0;
+        const double tb = pd.t_begin, te = pd.t_end;
+        double *prow = P.part + pd.part_off + (long long)tile * (N + 1);
+        const double *coef = P.coef + pd.coef_off;
+
+        for (int sub = 0; sub < P.tiles_per_item; ++sub) {
+            const int q = (tile * P.tiles_per_item + sub) * 32 + lane;
+            const bool valid = q < P.n_k;
+            double row[8];
+#pragma unroll
+            for (int c = 0; c < 8; ++c) row[c] = valid ? __ldg(P.ktab + (size_t)q * 8 + c) : 0.0;
+            if (!valid) row[2] = 1.0;  // keeps DIRAC3D's 1/|k| finite on idle lanes
+            ModelState<M, R> ms;
+            ms.init(pd, row);
+            double S[3] = {row[4], row[5], row[6]};
+            const double w = valid ? row[3] : 0.0;
+            bool dead = !valid;
+            double carry_dt = dt0;
+            double held = 0.0;  // lane (i & 31) holds the warp sum of sample i
+
+            for (int i = 0; i <= N; ++i) {
+                const double *rec = pd.s0rec;
+                if (i > 0) {
+                    // stage interval i-1 into this warp's shared slot
+                    __syncwarp();
+                    const double *src = coef + (size_t)(i - 1) * SLOT;
+                    for (int c = lane; c < SLOT; c += 32) {
+                        const double v = __ldg(src + c);
+                        slot[c] = v;
+                        if constexpr (kNarrow) {
+                            if (c >= HDR && c - HDR < RCOEF) stage_r[wib][c - HDR] = R(v);
+                        }
+                    }
+                    __syncwarp();
+                    rec = slot + 4;
+                    const double t0 = slot[0], t1 = slot[1];
+                    if constexpr (STEPPER == 1) {
+                        if (!dead) {
+                            const int ns = P.magnus_substeps;
+                            const double hs = (t1 - t0) / ns;
+                            const double g = 0.5 - 0.28867513459481288225;
+                            const double q3 = 0.57735026918962576451 * hs * hs;
+                            for (int s = 0; s < ns; ++s) {
+                                const double ts = t0 + s * hs;
+                                R f[NF], d1[3], d2[3];
+                                eval_staged<NF, D, R>(slot, sc, ts + g * hs, tb, te, f);
+                                ms.dvec(f, d1);
+                                eval_staged<NF, D, R>(slot, sc, ts + (1.0 - g) * hs, tb, te, f);
+                                ms.dvec(f, d2);
+                                double wv[3];
+                                wv[0] = hs * double(d1[0] + d2[0]) + q3 * double(d2[1] * d1[2] - d2[2] * d1[1]);
+                                wv[1] = hs * double(d1[1] + d2[1]) + q3 * double(d2[2] * d1[0] - d2[0] * d1[2]);
+                                wv[2] = hs * double(d1[2] + d2[2]) + q3 * double(d2[0] * d1[1] - d2[1] * d1[0]);
+                                rotate(wv, S);
+                            }
+                            my_attempts += ns;
+                        }
+                    } else {
+                        double t = t0;
+                        double dt = (PROPOSER == 1) ? carry_dt : dt0;
+                        bool active = !dead;
+                        int fails = 0, attempts = 0;
+                        while (__any_sync(kFull, active)) {
+                            if (active) {
+                                if ((t + dt) - t1 > kDblEps) dt = t1 - t;
+                                double xn[3], e[3], k0[3];
+                                rkf78_attempt<M, NF, D, R>(ms, slot, sc, tb, te, t, dt, S, xn, e, k0);
+                                ++attempts;
+                                double den[3];
+                                bool tiny = true;
+#pragma unroll
+                                for (int c = 0; c < 3; ++c) {
+                                    den[c] = P.abs_tol + P.rel_tol * (fabs(S[c]) + dt * fabs(k0[c]));
+                                    tiny = tiny && (fabs(e[c]) < P.err_floor * den[c]);
+                                }
+                                double err = 0.0;
+                                if (!tiny) {
+#pragma unroll
+                                    for (int c = 0; c < 3; ++c) err = fmax(err, fabs(e[c]) / den[c]);
+                                }
+                                if (err > 1.0) {
+                                    dt *= fmax(0.9 * pow(err, -1.0 / 6.0), 0.2);
+                                    ++my_rejects;
+                                    if (++fails >= P.max_failed) {
+                                        active = false;
+                                        dead = true;
+                                        atomicAdd(P.counters + 3, 1ull);
+                                        atomicMax(P.status, 2);
+                                    }
+                                } else {
+                                    t += dt;
+                                    S[0] = xn[0];
+                                    S[1] = xn[1];
+                                    S[2] = xn[2];
+                                    fails = 0;
+                                    if (err < 0.5)
+                                        dt *= tiny ? P.grow_max : 0.9 * pow(fmax(err, P.err_floor), -1.0 / 8.0);
+                                    if (!(t1 - t > kDblEps)) active = false;
+                                    if (PROPOSER == 1) carry_dt = dt;
+                                }
+                                if (active && attempts >= P.max_attempts) {
+                                    active = false;
+                                    dead = true;
+                                    atomicAdd(P.counters + 3, 1ull);
+                                    atomicMax(P.status, 2);
+                                }
+                            }
+                        }
+                        my_attempts += attempts;
+                    }
+                    if (!dead && !(isfinite(S[0]) && isfinite(S[1]) && isfinite(S[2]))) {
+                        dead = true;
+                        atomicAdd(P.counters + 4, 1ull);
+                        atomicMax(P.status, 3);
+                    }
+                }
+                // sample i at t_i = i * measure_every + t_begin (PiFlux.cpp:834-836)
+                const double c = dead ? 0.0 : w * ms.vertex(rec, S);
+                const double sum = warp_sum(c);
+                if (lane == (i & 31)) held = sum;
+                if ((i & 31) == 31 || i == N) {
+                    const int base = i & ~31;
+                    if (base + lane <= N) {
+                        if (sub == 0)
+                            prow[base + lane] = held;
+                        else
+                            prow[base + lane] += held;
+                    }
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) {
+        my_attempts += __shfl_xor_sync(kFull, my_attempts, o);
+        my_rejects += __shfl_xor_sync(kFull, my_rejects, o);
+    }
+    if (lane == 0) {
+        atomicAdd(P.counters + 1, my_attempts);
+        atomicAdd(P.counters + 2, my_rejects);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Staging: per (pulse, interval) Chebyshev interpolants of the model's staged
+// functions at D+1 first-kind nodes, converted to monomials in u, plus the
+// exact sample record at the interval's end sample.
+// ---------------------------------------------------------------------------
+template <int M>
+__device__ __forceinline__ void staged_values(const PulseDev &pd, double A, double *v) {
+    constexpr int NF = Traits<M>::NF;
+    if constexpr (NF == 1) {
+        v[0] = A;
+    } else if constexpr (M == PIFLUX3D) {
+        sincos(A, &v[1], &v[0]);
+    } else {
+#pragma unroll
+        for (int n = 0; n < NF / 2; ++n) sincos(pd.s[n] * A, &v[2 * n + 1], &v[2 * n]);
+    }
+}
+
+template <int M, int D>
+__global__ void stage_pulses_kernel(const PulseDev *__restrict__ pulses, int n_pulses,
+                                    const double *__restrict__ tgrid,
+                                    const long long *__restrict__ interval_off,
+                                    double *__restrict__ coef, long long total_intervals) {
+    constexpr int NF = Traits<M>::NF;
+    constexpr int SLOT = slot_doubles(NF, D);
+    constexpr int HDR = slot_header(NF);
+    constexpr int NN = D + 1;
+    const long long gid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (gid >= total_intervals) return;
+    int lo = 0, hi = n_pulses;  // interval_off: exclusive prefix sums, n_pulses + 1 entries
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (interval_off[mid] <= gid) lo = mid; else hi = mid;
+    }
+    const int p = lo;
+    const int i = (int)(gid - interval_off[p]);
+    const PulseDev pd = pulses[p];
+    // tgrid holds n_meas + 1 accumulated interval ends per pulse, laid out at
+    // interval_off[p] + p
+    const double t0 = tgrid[interval_off[p] + p + i];
+    const double t1 = tgrid[interval_off[p] + p + i + 1];
+    const double ctr = 0.5 * (t0 + t1);
+    const double half = 0.5 * (t1 - t0);
+    double *out = coef + pd.coef_off + (long long)i * SLOT;
+    out[0] = t0;
+    out[1] = t1;
+    out[2] = ctr;
+    out[3] = 1.0 / half;
+    // exact sample record at t_s = (i + 1) * measure_every + window_begin
+    const double ts = (i + 1) * pd.measure_every + pd.window_begin;
+    double env = 0.0;
+    if (!(ts <= pd.t_begin || ts >= pd.t_end)) env = 0.5 * (1. - cos(pd.inv_n_cycles * (ts - pd.t_begin)));
+    const double As = pd.amplitude * (env * sin(ts + pd.phase));
+    out[4] = As;
+    double sv[NF];
+    staged_values<M>(pd, As, sv);
+    for (int n = 0; n < NF; ++n) out[5 + n] = sv[n];
+    for (int c = 5 + NF; c < HDR; ++c) out[c] = 0.0;
+    double fv[NF][NN];
+    for (int k = 0; k < NN; ++k) {
+        const double xk = cospi((k + 0.5) / NN);
+        double v[NF];
+        staged_values<M>(pd, laser_continued(pd, ctr + half * xk), v);
+        for (int n = 0; n < NF; ++n) fv[n][k] = v[n];
+    }
+    for (int n = 0; n < NF; ++n) {
+        double a[NN];
+        for (int j = 0; j < NN; ++j) {
+            double acc = 0.0;
+            for (int k = 0; k < NN; ++k) acc += fv[n][k] * cospi(j * (k + 0.5) / NN);
+            a[j] = acc * (2.0 / NN);
+        }
+        a[0] *= 0.5;
+        // monomial coefficients of sum_j a_j T_j(u) via T_{j+1} = 2u T_j - T_{j-1}
+        double m[NN], tm1[NN], tm0[NN], tn[NN];
+        for (int j = 0; j < NN; ++j) m[j] = tm1[j] = tm0[j] = 0.0;
+        tm1[0] = 1.0;
+        tm0[1] = 1.0;
+        m[0] = a[0];
+        m[1] = a[1];
+        for (int j = 2; j < NN; ++j) {
+            for (int c = 0; c < NN; ++c) tn[c] = (c > 0 ? 2.0 * tm0[c - 1] : 0.0) - tm1[c];
+            for (int c = 0; c < NN; ++c) {
+                m[c] += a[j] * tn[c];
+                tm1[c] = tm0[c];
+                tm0[c] = tn[c];
+            }
+        }
+        for (int j = 0; j < NN; ++j) out[HDR + n * NN + j] = m[j];
+    }
+    for (int c = HDR + NF * NN; c < SLOT; ++c) out[c] = 0.0;
+}
+
+// j[p][i] = sum over the pulse's items (in item order) of the partial rows,
+// with Neumaier compensation.
+static __global__ void reduce_partials_kernel(const PulseDev *__restrict__ pulses, int n_pulses,
+                                       const double *__restrict__ part, double *__restrict__ j,
+                                       long long total_samples) {
+    const long long gid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (gid >= total_samples) return;
+    int lo = 0, hi = n_pulses;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (pulses[mid].j_off <= gid) lo = mid; else hi = mid;
+    }
+    const PulseDev &pd = pulses[lo];
+    const int i = (int)(gid - pd.j_off);
+    const int len = pd.n_meas + 1;
+    const double *src = part + pd.part_off + i;
+    double s = 0.0, comp = 0.0;
+    for (int it = 0; it < pd.items; ++it) {
+        const double v = src[(size_t)it * len];
+        const double tt = s + v;
+        if (fabs(s) >= fabs(v)) comp += (s - tt) + v;
+        else comp += (v - tt) + s;
+        s = tt;
+    }
+    j[gid] = s + comp;
+}
+
+// Zero-padded copy for the r2c FFT (hhg.cpp:280-282).
+static __global__ void pad_kernel(const double *__restrict__ j, int n, double *__restrict__ x, int n_in) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n_in) x[i] = i < n ? j[i] : 0.0;
+}
+
+// TrapezoidalFFT corrections (TrapezoidalFFT.cpp:17-48) applied to the r2c
+// FFT of the zero-padded input x (n_in values): input[0] = x[0] and
+// input[n_in - 1] = x[n_in - 1] (a padding zero, hhg.cpp:280-282).
+static __global__ void trapezoid_correct_kernel(const double2 *__restrict__ F, int n_fft, int n_in,
+                                                double delta_t, double t_begin, double t_end,
+                                                const double *__restrict__ x, double *re,
+                                                double *im, double *freq) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_fft) return;
+    const double x0 = x[0], xlast = x[n_in - 1];
+    const double pi = 3.141592653589793238462643383279502884;
+    const double fr = 2 * i * pi / (n_in * delta_t);
+    const double th = fr * delta_t;
+    const unsigned long long bits = (unsigned long long)__double_as_longlong(th);
+    const bool zero = (int)((bits >> 52) & 0x7FF) < 0x3D3;  // is_zero (GlobalDefinitions.hpp:61-71)
+    double W, a0r, a0i;
+    if (zero) {
+        W = 1.0;
+        a0r = -0.5;
+        a0i = 0.0;
+    } else {
+        const double c = cos(th), s = sin(th);
+        W = 2. * (1. - c) / (th * th);
+        a0r = -(1. - c) / (th * th);
+        a0i = (th - s) / (th * th);
+    }
+    double sp, cp;
+    sincos(fr * (t_end - t_begin), &sp, &cp);
+    // alpha0 x0 + conj(alpha0) e^{i w (te - tb)} xlast
+    const double cr = a0r * x0 + (a0r * cp + a0i * sp) * xlast;
+    const double ci = a0i * x0 + (a0r * sp - a0i * cp) * xlast;
+    double sb, cb;
+    sincos(fr * t_begin, &sb, &cb);
+    const double mr = delta_t * W * cb, mi = delta_t * W * sb;
+    const double2 f = F[i];
+    re[i] = delta_t * (mr * f.x - mi * f.y + cr);
+    im[i] = delta_t * (mr * f.y + mi * f.x + ci);
+    freq[i] = fr;
+}
+
+// FP64 issue-rate probe: 8 independent FMA chains per thread.
+static __global__ void fp64_fma_probe_kernel(double *out, int iters, double a, double b) {
+    double v[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) v[c] = threadIdx.x * 1e-3 + c;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int c = 0; c < 8; ++c) v[c] = fma(v[c], a, b);
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) s += v[c];
+    if (s == 12345.678) out[0] = s;  // keeps the chains alive
+}
+
+}  // namespace hhg

@@ -1,0 +1,1037 @@
+// hhg_gpu.cu -- host side of the C ABI declared in include/hhg_gpu.h:
+// contexts, Gauss-Legendre rules, k grids with their initial Bloch vectors,
+// plans (device-resident k table, per-interval pulse staging, work list,
+// partial buffer), launches, status checking and the trapezoidal FFT.
+#include <cufft.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/hhg_gpu.h"
+#include "hhg_launch.cuh"
+
+using hhg::PulseDev;
+
+struct hhg_ctx {
+    int device = 0;
+    int sm_count = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    std::string last_error;
+    std::map<int, cufftHandle> fft_plans;
+    // spectrum scratch
+    double *d_x = nullptr, *d_out = nullptr;
+    double2 *d_F = nullptr;
+    size_t x_cap = 0, f_cap = 0;
+};
+
+struct hhg_plan {
+    hhg_ctx *ctx = nullptr;
+    int model = 0, degree = 7;
+    hhg_solver_opts opts{};
+    int n_pulses = 0;
+    int64_t n_k = 0;
+    int tiles_per_item = 1, items_per_pulse = 0;
+    long long n_items = 0;
+    long long j_len = 0, part_len = 0, coef_len = 0, n_intervals = 0;
+    std::vector<PulseDev> pulses;
+    std::vector<double> window_end;
+    int grid = 0;
+    // device buffers
+    double *d_ktab = nullptr, *d_coef = nullptr, *d_part = nullptr, *d_j = nullptr,
+           *d_tgrid = nullptr;
+    PulseDev *d_pulses = nullptr;
+    long long *d_ioff = nullptr;
+    unsigned long long *d_counters = nullptr;
+    int *d_status = nullptr;
+    bool timed = false;
+    // spectra (allocated on first hhg_plan_spectrum_async)
+    double *d_spec = nullptr, *d_x = nullptr;
+    double2 *d_F = nullptr;
+    std::vector<long long> spec_off;  // per pulse offset (in n_fft units) into d_spec
+    long long spec_len = 0;
+};
+
+namespace {
+
+constexpr double kPi = 3.141592653589793238462643383279502884;
+constexpr double kSqrt3 = 1.732050807568877293527446341;
+
+hhg_status set_err(hhg_ctx *ctx, hhg_status st, const std::string &msg) {
+    if (ctx) ctx->last_error = msg;
+    return st;
+}
+
+#define HHG_CUDA(ctx, call)                                                              \
+    do {                                                                                 \
+        cudaError_t e__ = (call);                                                        \
+        if (e__ != cudaSuccess)                                                          \
+            return set_err(ctx, HHG_CUDA_ERROR,                                          \
+                           std::string(#call) + ": " + cudaGetErrorString(e__));         \
+    } while (0)
+
+// Gauss-Legendre nodes by Newton iteration on P_n in long double.
+void gauss_legendre(int n, double *x, double *w) {
+    const long double pi = 3.141592653589793238462643383279502884L;
+    const int m = (n + 1) / 2;
+    for (int i = 0; i < m; ++i) {
+        long double z = cosl(pi * (i + 0.75L) / (n + 0.5L));
+        long double dp = 0.0L;
+        for (int it = 0; it < 100; ++it) {
+            long double p1 = 1.0L, p2 = 0.0L;
+            for (int j = 1; j <= n; ++j) {
+                const long double p3 = p2;
+                p2 = p1;
+                p1 = ((2.0L * j - 1.0L) * z * p2 - (j - 1.0L) * p3) / j;
+            }
+            dp = n * (z * p1 - p2) / (z * z - 1.0L);
+            const long double dz = p1 / dp;
+            z -= dz;
+            if (fabsl(dz) < 1e-19L * (1.0L + fabsl(z))) {
+                p1 = 1.0L;
+                p2 = 0.0L;
+                for (int j = 1; j <= n; ++j) {
+                    const long double p3 = p2;
+                    p2 = p1;
+                    p1 = ((2.0L * j - 1.0L) * z * p2 - (j - 1.0L) * p3) / j;
+                }
+                dp = n * (z * p1 - p2) / (z * z - 1.0L);
+                break;
+            }
+        }
+        const long double wi = 2.0L / ((1.0L - z * z) * dp * dp);
+        x[n - 1 - i] = (double)z;
+        x[i] = (double)(-z);
+        w[n - 1 - i] = (double)wi;
+        w[i] = (double)wi;
+    }
+    if (n & 1) x[n / 2] = 0.0;
+}
+
+// Positive half, ascending: gauss::container<n> (thread_gauss.hpp).
+void gauss_half(int n, std::vector<double> &xa, std::vector<double> &wa) {
+    std::vector<double> x(n), w(n);
+    gauss_legendre(n, x.data(), w.data());
+    xa.assign(x.begin() + n / 2, x.end());
+    wa.assign(w.begin() + n / 2, w.end());
+}
+
+bool ref_is_zero(double v) {
+    uint64_t bits;
+    std::memcpy(&bits, &v, sizeof bits);
+    return (int)((bits >> 52) & 0x7FF) < 0x3D3;
+}
+
+// Initial Bloch vector of the filled lower band at T = 0, S0 = -d_hat(k).
+void initial_state(const hhg_system_desc &s, double kx, double ky, double kz, double *s0) {
+    switch (s.kind) {
+    case HHG_SYS_PIFLUX3D: {
+        // PiFlux::ic_sigma with alpha^2 = 0, beta^2 = 1 (PiFlux.cpp:519-549)
+        const double cx = cos(kx), cy = cos(ky), cz = cos(kz);
+        const double disp = sqrt(cx * cx + cy * cy + cz * cz);
+        const double zeps = cz + disp;
+        s0[0] = (-1.0 * cx * zeps + 0.0) / (disp * zeps);
+        s0[1] = (-1.0 * cy * zeps - 0.0) / (disp * zeps);
+        s0[2] = (-1.0 * cz * zeps - 0.0) / (disp * zeps);
+        break;
+    }
+    case HHG_SYS_PIFLUX2D: {
+        const double cx = cos(kx), cy = cos(ky);
+        const double n = sqrt(cx * cx + cy * cy);
+        s0[0] = cx / n;
+        s0[1] = cy / n;
+        s0[2] = 0.0;
+        break;
+    }
+    case HHG_SYS_DIRAC2D: {
+        const double d0 = s.velocity * kx, d1 = s.velocity * ky, d2 = s.mass;
+        const double n = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+        s0[0] = -d0 / n;
+        s0[1] = -d1 / n;
+        s0[2] = -d2 / n;
+        break;
+    }
+    case HHG_SYS_HONEYCOMB: {
+        // Honeycomb::ic_sigma at T = 0 (Honeycomb.cpp:355-361)
+        double gre = 0.0, gim = 0.0;
+        const double nn[3][2] = {{1.0, 0.0}, {-0.5, 0.5 * kSqrt3}, {-0.5, -0.5 * kSqrt3}};
+        for (int j = 0; j < 3; ++j) {
+            const double ph = nn[j][0] * kx + nn[j][1] * ky;
+            gre += cos(ph);
+            gim += sin(ph);
+        }
+        if (s.mass == 0.0) {
+            const double ag = hypot(gre, gim);
+            s0[0] = -1.0 * gre / ag;
+            s0[1] = 1.0 * gim / ag;
+            s0[2] = -0.0;
+        } else {
+            const double d0 = s.hopping * gre, d1 = -s.hopping * gim, d2 = s.mass;
+            const double n = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+            s0[0] = -d0 / n;
+            s0[1] = -d1 / n;
+            s0[2] = -d2 / n;
+        }
+        break;
+    }
+    case HHG_SYS_DIRAC3D:
+        s0[0] = 0.0;
+        s0[1] = 0.0;
+        s0[2] = -1.0;  // (2 a0 b0, 0, a0^2 - b0^2), a0 = 0, b0 = 1 (DiracSystem.cpp:155-158)
+        break;
+    default:
+        s0[0] = s0[1] = s0[2] = 0.0;
+    }
+}
+
+void push_row(const hhg_system_desc &s, double kx, double ky, double kz, double w, double *o) {
+    o[0] = kx;
+    o[1] = ky;
+    o[2] = kz;
+    o[3] = w;
+    initial_state(s, kx, ky, kz, o + 4);
+    o[7] = 0.0;
+}
+
+int64_t grid_count(const hhg_grid_desc &g) {
+    switch (g.kind) {
+    case HHG_GRID_TENSOR_GL:
+    case HHG_GRID_RHOMBIC_GL:
+        return (int64_t)g.n1 * g.n2;
+    case HHG_GRID_PIFLUX3D_REF: {
+        const int64_t c = g.n2, f = 8 * c;
+        return 2 * (int64_t)g.n1 * ((2 * f) * f + (6 * c) * (2 * c) + 2 * (2 * c) * (2 * c));
+    }
+    case HHG_GRID_HONEYCOMB_HEX_REF:
+        return 4 * (int64_t)g.n1 * g.n1;
+    case HHG_GRID_EXPLICIT:
+        return g.n_rows;
+    }
+    return -1;
+}
+
+// Row builders; see the oracle for the same restatements.
+void build_rows(const hhg_system_desc &s, const hhg_grid_desc &g, double *out) {
+    size_t r = 0;
+    switch (g.kind) {
+    case HHG_GRID_TENSOR_GL: {
+        std::vector<double> gx(g.n1), wx(g.n1), gy(g.n2), wy(g.n2);
+        gauss_legendre(g.n1, gx.data(), wx.data());
+        gauss_legendre(g.n2, gy.data(), wy.data());
+        const double hx = 0.5 * (g.x_hi - g.x_lo), mx = 0.5 * (g.x_hi + g.x_lo);
+        const double hy = 0.5 * (g.y_hi - g.y_lo), my = 0.5 * (g.y_hi + g.y_lo);
+        for (int i = 0; i < g.n1; ++i)
+            for (int j = 0; j < g.n2; ++j)
+                push_row(s, hx * gx[i] + mx, hy * gy[j] + my, 0.0, hx * hy * wx[i] * wy[j],
+                         out + 8 * r++);
+        break;
+    }
+    case HHG_GRID_RHOMBIC_GL: {
+        // k = f1 b1 + f2 b2, f in [-1/2, 1/2]^2, b1 = 2pi/3 (1, -sqrt3), b2 = 2pi/3 (1, sqrt3)
+        const double b1x = 2.0 * kPi / 3.0, b1y = -2.0 * kPi / 3.0 * kSqrt3;
+        const double b2x = 2.0 * kPi / 3.0, b2y = 2.0 * kPi / 3.0 * kSqrt3;
+        const double area = fabs(b1x * b2y - b1y * b2x);
+        std::vector<double> g1(g.n1), w1(g.n1), g2(g.n2), w2(g.n2);
+        gauss_legendre(g.n1, g1.data(), w1.data());
+        gauss_legendre(g.n2, g2.data(), w2.data());
+        for (int i = 0; i < g.n1; ++i)
+            for (int j = 0; j < g.n2; ++j) {
+                const double f1 = 0.5 * g1[i], f2 = 0.5 * g2[j];
+                push_row(s, f1 * b1x + f2 * b2x, f1 * b1y + f2 * b2y, 0.0,
+                         0.25 * area * w1[i] * w2[j], out + 8 * r++);
+            }
+        break;
+    }
+    case HHG_GRID_PIFLUX3D_REF: {
+        // PiFlux::current_density_continuum_limit / improved_xy_integral
+        // (PiFlux.cpp:665-863), including the initial-state rescue of +k_z
+        // slices with cos k_z < 0 (PiFlux.cpp:812-816).
+        const int zr = g.n1, nc = g.n2, nf = 8 * nc;
+        const double pi = kPi, edge = 0.35 * pi;
+        struct Seg { double lo, hi; int nh; };
+        const Seg rx[4] = {{edge, pi - edge, nf}, {0.0, pi, 3 * nc}, {0.0, edge, nc}, {pi - edge, pi, nc}};
+        const Seg ry[4] = {{edge, 0.5 * pi, nf / 2}, {0.0, edge, nc}, {edge, 0.5 * pi, nc}, {edge, 0.5 * pi, nc}};
+        std::vector<double> za, zw;
+        gauss_half(2 * zr, za, zw);
+        std::vector<double> xa[4], xw[4], ya[4], yw[4];
+        for (int q = 0; q < 4; ++q) {
+            gauss_half(2 * rx[q].nh, xa[q], xw[q]);
+            gauss_half(2 * ry[q].nh, ya[q], yw[q]);
+        }
+        double last_cx = 0.0, last_cy = 0.0;
+        for (int z = 0; z < zr; ++z)
+            for (int sg = 0; sg < 2; ++sg) {
+                const double kz = (sg == 0 ? pi : -pi) * za[z];
+                double cz = cos(kz);
+                const double chx = sg == 0 ? 0.0 : last_cx, chy = sg == 0 ? 0.0 : last_cy;
+                if (ref_is_zero(chx) && ref_is_zero(chy) && cz < 0.0) cz *= (1. - 0.5 * 1e-4 * 1e-4);
+                for (int q = 0; q < 4; ++q) {
+                    const double xh = 0.5 * (rx[q].hi - rx[q].lo), xm = 0.5 * (rx[q].hi + rx[q].lo);
+                    const double yh = 0.5 * (ry[q].hi - ry[q].lo), ym = 0.5 * (ry[q].hi + ry[q].lo);
+                    const double tw = xh * yh;
+                    for (int i = 0; i < rx[q].nh; ++i)
+                        for (int sx = 0; sx < 2; ++sx) {
+                            const double kx = xh * (sx ? -xa[q][i] : xa[q][i]) + xm;
+                            const double mw = xw[q][i] * tw;
+                            for (int j = 0; j < ry[q].nh; ++j)
+                                for (int sy = 0; sy < 2; ++sy) {
+                                    const double ky = yh * (sy ? -ya[q][j] : ya[q][j]) + ym;
+                                    double *o = out + 8 * r++;
+                                    o[0] = kx;
+                                    o[1] = ky;
+                                    o[2] = kz;
+                                    o[3] = mw * yw[q][j] * zw[z];
+                                    const double cx = cos(kx), cy = cos(ky);
+                                    const double disp = sqrt(cx * cx + cy * cy + cz * cz);
+                                    const double zeps = cz + disp;
+                                    o[4] = (-1.0 * cx * zeps + 0.0) / (disp * zeps);
+                                    o[5] = (-1.0 * cy * zeps - 0.0) / (disp * zeps);
+                                    o[6] = (-1.0 * cz * zeps - 0.0) / (disp * zeps);
+                                    o[7] = 0.0;
+                                    last_cx = cx;
+                                    last_cy = cy;
+                                }
+                        }
+                }
+            }
+        break;
+    }
+    case HHG_GRID_HONEYCOMB_HEX_REF: {
+        // Honeycomb::compute_current_density (Honeycomb.cpp:225-323)
+        const int nk = g.n1;
+        const double min_x = -2 * kPi / 3, max_x = 2 * kPi / 3;
+        std::vector<double> a, w;
+        gauss_half(2 * nk, a, w);
+        for (int x = 0; x < nk; ++x) {
+            const double kx0 = 0.5 * (max_x - min_x) * a[x] + 0.5 * (max_x + min_x);
+            const double ymax = (4 * kPi / (3 * kSqrt3)) - (fabs(kx0) / kSqrt3);
+            for (int sx = 0; sx < 2; ++sx) {
+                const double kx = sx ? (0.5 * (max_x - min_x) * (-a[x]) + 0.5 * (max_x + min_x)) : kx0;
+                for (int y = 0; y < nk; ++y) {
+                    const double tw = 0.5 * (max_x - min_x) * (0.5 * (ymax - (-ymax))) * w[x] * w[y];
+                    for (int sy = 0; sy < 2; ++sy) {
+                        const double ay = sy ? -a[y] : a[y];
+                        const double ky = 0.5 * (ymax - (-ymax)) * ay + 0.5 * (ymax + (-ymax));
+                        push_row(s, kx, ky, 0.0, tw, out + 8 * r++);
+                    }
+                }
+            }
+        }
+        break;
+    }
+    case HHG_GRID_EXPLICIT:
+        std::memcpy(out, g.rows, sizeof(double) * 8 * (size_t)g.n_rows);
+        break;
+    }
+}
+
+hhg_status check_system(hhg_ctx *ctx, const hhg_system_desc *s) {
+    if (!s) return set_err(ctx, HHG_BAD_CONFIG, "null system descriptor");
+    if (s->kind < HHG_SYS_DIRAC2D || s->kind > HHG_SYS_DIRAC3D)
+        return set_err(ctx, HHG_BAD_CONFIG, "System type not recognized");
+    if (!std::isfinite(s->hopping) || !std::isfinite(s->velocity) || !std::isfinite(s->mass) ||
+        !std::isfinite(s->pol_x) || !std::isfinite(s->pol_y))
+        return set_err(ctx, HHG_BAD_CONFIG, "non-finite system parameter");
+    return HHG_OK;
+}
+
+hhg_status check_grid(hhg_ctx *ctx, const hhg_grid_desc *g) {
+    if (!g) return set_err(ctx, HHG_BAD_CONFIG, "null grid descriptor");
+    switch (g->kind) {
+    case HHG_GRID_TENSOR_GL:
+    case HHG_GRID_RHOMBIC_GL:
+        if (g->n1 < 1 || g->n2 < 1 || g->n1 > 65536 || g->n2 > 65536)
+            return set_err(ctx, HHG_BAD_CONFIG, "grid order out of range");
+        break;
+    case HHG_GRID_PIFLUX3D_REF:
+        if (g->n1 < 1 || g->n2 < 1 || g->n1 > 4096 || g->n2 > 256)
+            return set_err(ctx, HHG_BAD_CONFIG, "PiFlux reference grid size out of range");
+        break;
+    case HHG_GRID_HONEYCOMB_HEX_REF:
+        if (g->n1 < 1 || g->n1 > 8192) return set_err(ctx, HHG_BAD_CONFIG, "N_k out of range");
+        break;
+    case HHG_GRID_EXPLICIT:
+        if (!g->rows || g->n_rows < 1) return set_err(ctx, HHG_BAD_CONFIG, "explicit grid without rows");
+        break;
+    default:
+        return set_err(ctx, HHG_BAD_CONFIG, "grid type not recognized");
+    }
+    const int64_t n = grid_count(*g);
+    if (n < 1 || n > (int64_t)1 << 31) return set_err(ctx, HHG_BAD_CONFIG, "k grid too large");
+    return HHG_OK;
+}
+
+hhg_status check_pulse(hhg_ctx *ctx, const hhg_pulse_desc &p) {
+    if (p.kind != HHG_PULSE_COSINE) return set_err(ctx, HHG_UNSUPPORTED, "Laser type not recognized");
+    if (p.n_measurements < 1 || p.n_measurements > (1 << 24))
+        return set_err(ctx, HHG_BAD_CONFIG, "n_measurements out of range");
+    if (p.n_subdivisions < 1) return set_err(ctx, HHG_BAD_CONFIG, "n_subdivisions must be >= 1");
+    if (!(p.n_cycles > 0.0) || !std::isfinite(p.n_cycles))
+        return set_err(ctx, HHG_BAD_CONFIG, "n_cycles must be > 0");
+    if (!std::isfinite(p.amplitude) || !std::isfinite(p.t_begin) || !std::isfinite(p.phase) ||
+        !std::isfinite(p.window_begin) || !std::isfinite(p.window_end) ||
+        !std::isfinite(p.energy_scale))
+        return set_err(ctx, HHG_BAD_CONFIG, "non-finite pulse parameter");
+    if (!(p.window_end > p.window_begin)) return set_err(ctx, HHG_BAD_CONFIG, "empty time window");
+    if (!(p.energy_scale > 0.0)) return set_err(ctx, HHG_BAD_CONFIG, "energy_scale must be > 0");
+    return HHG_OK;
+}
+
+int model_nf(int m) {
+    switch (m) {
+    case HHG_SYS_DIRAC2D: return 1;
+    case HHG_SYS_DIRAC3D: return 1;
+    case HHG_SYS_PIFLUX3D: return 2;
+    case HHG_SYS_PIFLUX2D: return 4;
+    case HHG_SYS_HONEYCOMB: return 6;
+    }
+    return 0;
+}
+
+// Chebyshev-tail test of the staged interpolants, in long double so the
+// fit's own rounding (~1e-19) sits below the threshold: the smallest degree in
+// {5, 7, 11} whose Chebyshev tail beyond it is below 2^-56 of the function scale
+// on sampled intervals, or -1 if even degree 11 is not enough.
+long double pulse_value_ld(const hhg_pulse_desc &p, long double t) {
+    const long double inv = 1.0L / p.n_cycles;
+    return (long double)p.amplitude * ((0.5L * (1.0L - cosl(inv * (t - p.t_begin)))) * sinl(t + p.phase));
+}
+
+int choose_degree(const hhg_pulse_desc &p, const double *proj, int nf) {
+    const int NN = 16;
+    const long double pi = 3.141592653589793238462643383279502884L;
+    const long double me = ((long double)p.window_end - p.window_begin) / p.n_measurements;
+    const int samples = std::min(p.n_measurements, 257);
+    long double tail5 = 0.0L, tail7 = 0.0L, tail11 = 0.0L, scale = 1.0L;
+    for (int q = 0; q < samples; ++q) {
+        const int i = (int)((long long)q * p.n_measurements / samples);
+        const long double ctr = p.window_begin + (i + 0.5L) * me, half = 0.5L * me;
+        const int groups = nf == 1 ? 1 : nf / 2;
+        for (int n = 0; n < groups; ++n) {
+            for (int part = 0; part < (nf == 1 ? 1 : 2); ++part) {
+                long double fv[NN];
+                for (int k = 0; k < NN; ++k) {
+                    const long double A = pulse_value_ld(p, ctr + half * cosl(pi * (k + 0.5L) / NN));
+                    if (nf == 1) fv[k] = A;
+                    else fv[k] = part == 0 ? cosl(proj[n] * A) : sinl(proj[n] * A);
+                }
+                for (int j = 0; j < NN; ++j) {
+                    long double acc = 0.0L;
+                    for (int k = 0; k < NN; ++k) acc += fv[k] * cosl(pi * j * (k + 0.5L) / NN);
+                    acc = fabsl(acc * 2.0L / NN);
+                    if (j == 0) scale = std::max(scale, acc);
+                    if (j > 5) tail5 = std::max(tail5, acc);
+                    if (j > 7) tail7 = std::max(tail7, acc);
+                    if (j > 11) tail11 = std::max(tail11, acc);
+                }
+            }
+        }
+    }
+    const long double thr = ldexpl(1.0L, -56) * scale;
+    if (tail5 <= thr) return 5;
+    if (tail7 <= thr) return 7;
+    if (tail11 <= thr) return 11;
+    return -1;
+}
+
+hhg_status launch_variant(const hhg_plan *pl, hhg::LaunchReq &r) {
+    cudaError_t e = cudaErrorInvalidValue;
+    switch (pl->model) {
+    case HHG_SYS_DIRAC2D: e = hhg::launch_dirac2d(r); break;
+    case HHG_SYS_PIFLUX2D: e = hhg::launch_piflux2d(r); break;
+    case HHG_SYS_PIFLUX3D: e = hhg::launch_piflux3d(r); break;
+    case HHG_SYS_HONEYCOMB: e = hhg::launch_honeycomb(r); break;
+    case HHG_SYS_DIRAC3D: e = hhg::launch_dirac3d(r); break;
+    }
+    if (e != cudaSuccess)
+        return set_err(pl->ctx, HHG_CUDA_ERROR, std::string("integration launch: ") + cudaGetErrorString(e));
+    return HHG_OK;
+}
+
+hhg_status stage_variant(const hhg_plan *pl, hhg::StageReq &s) {
+    cudaError_t e = cudaErrorInvalidValue;
+    switch (pl->model) {
+    case HHG_SYS_DIRAC2D: e = hhg::stage_dirac2d(s); break;
+    case HHG_SYS_PIFLUX2D: e = hhg::stage_piflux2d(s); break;
+    case HHG_SYS_PIFLUX3D: e = hhg::stage_piflux3d(s); break;
+    case HHG_SYS_HONEYCOMB: e = hhg::stage_honeycomb(s); break;
+    case HHG_SYS_DIRAC3D: e = hhg::stage_dirac3d(s); break;
+    }
+    if (e != cudaSuccess)
+        return set_err(pl->ctx, HHG_CUDA_ERROR, std::string("staging launch: ") + cudaGetErrorString(e));
+    return HHG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int hhg_abi_version(void) { return HHG_ABI_VERSION; }
+
+void hhg_default_solver_opts(hhg_solver_opts *o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof *o);
+    o->stepper = HHG_STEPPER_RKF78;
+    o->precision = HHG_PREC_FP64;
+    o->proposer = HHG_PROPOSER_NONE;
+    o->magnus_substeps = 1;
+    o->abs_tol = 1.0e-12;  // PiFlux.cpp:20-21
+    o->rel_tol = 1.0e-8;
+    o->max_failed_steps = 500;
+    o->max_attempts_per_interval = 100000;
+    o->tile_k = 0;
+    o->block_threads = 128;
+}
+
+hhg_status hhg_gpu_create(hhg_ctx **out, int device) {
+    if (!out) return HHG_BAD_CONFIG;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return HHG_CUDA_ERROR;
+    if (device < 0 || device >= n) return HHG_BAD_CONFIG;
+    hhg_ctx *c = new hhg_ctx();
+    c->device = device;
+    if (cudaSetDevice(device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return HHG_CUDA_ERROR;
+    }
+    for (auto &e : c->ev) cudaEventCreate(&e);
+    *out = c;
+    return HHG_OK;
+}
+
+void hhg_gpu_destroy(hhg_ctx *c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    for (auto &kv : c->fft_plans) cufftDestroy(kv.second);
+    cudaFree(c->d_x);
+    cudaFree(c->d_F);
+    cudaFree(c->d_out);
+    for (auto &e : c->ev) cudaEventDestroy(e);
+    cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+const char *hhg_last_error(const hhg_ctx *c) { return c ? c->last_error.c_str() : "null context"; }
+
+hhg_status hhg_gauss_legendre(int n, double *x, double *w) {
+    if (n < 1 || n > 1 << 20 || !x || !w) return HHG_BAD_CONFIG;
+    gauss_legendre(n, x, w);
+    return HHG_OK;
+}
+
+hhg_status hhg_grid_rows(const hhg_system_desc *sys, const hhg_grid_desc *grid, double *rows,
+                         int64_t *n_rows) {
+    hhg_status st = check_system(nullptr, sys);
+    if (st != HHG_OK) return st;
+    st = check_grid(nullptr, grid);
+    if (st != HHG_OK) return st;
+    const int64_t n = grid_count(*grid);
+    if (n_rows) *n_rows = n;
+    if (rows) build_rows(*sys, *grid, rows);
+    return HHG_OK;
+}
+
+hhg_status hhg_plan_create(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_pulse_desc *pulses,
+                           int n_pulses, const hhg_grid_desc *grid, const hhg_solver_opts *opts,
+                           hhg_plan **out) {
+    if (!ctx || !out) return HHG_BAD_CONFIG;
+    *out = nullptr;
+    hhg_status st = check_system(ctx, sys);
+    if (st != HHG_OK) return st;
+    st = check_grid(ctx, grid);
+    if (st != HHG_OK) return st;
+    if (!pulses || n_pulses < 1 || n_pulses > (1 << 20))
+        return set_err(ctx, HHG_BAD_CONFIG, "need at least one pulse");
+    for (int p = 0; p < n_pulses; ++p)
+        if ((st = check_pulse(ctx, pulses[p])) != HHG_OK) return st;
+    hhg_solver_opts o;
+    hhg_default_solver_opts(&o);
+    if (opts) o = *opts;
+    if (o.stepper != HHG_STEPPER_RKF78 && o.stepper != HHG_STEPPER_MAGNUS4)
+        return set_err(ctx, HHG_BAD_CONFIG, "unknown stepper");
+    if (o.stepper == HHG_STEPPER_MAGNUS4 && (o.magnus_substeps < 1 || o.magnus_substeps > 4096))
+        return set_err(ctx, HHG_BAD_CONFIG, "magnus_substeps out of range");
+    if (o.stepper == HHG_STEPPER_MAGNUS4 && o.precision != HHG_PREC_FP64)
+        return set_err(ctx, HHG_UNSUPPORTED, "Magnus-4 runs in FP64 only");
+    if (o.precision != HHG_PREC_FP64 && o.precision != HHG_PREC_MIXED)
+        return set_err(ctx, HHG_BAD_CONFIG, "unknown precision");
+    if (o.proposer == HHG_PROPOSER_LEARNED)
+        return set_err(ctx, HHG_UNSUPPORTED, "learned proposer requires a trained network (hhg_learned_*)");
+    if (o.proposer != HHG_PROPOSER_NONE && o.proposer != HHG_PROPOSER_CARRY)
+        return set_err(ctx, HHG_BAD_CONFIG, "unknown proposer");
+    if (!(o.abs_tol >= 0.0) || !(o.rel_tol >= 0.0) || !(o.abs_tol + o.rel_tol > 0.0))
+        return set_err(ctx, HHG_BAD_CONFIG, "tolerances must be >= 0 and not both 0");
+    if (o.max_failed_steps < 1) o.max_failed_steps = 500;
+    if (o.max_attempts_per_interval < 1) o.max_attempts_per_interval = 100000;
+
+    HHG_CUDA(ctx, cudaSetDevice(ctx->device));
+    hhg_plan *pl = new hhg_plan();
+    pl->ctx = ctx;
+    pl->model = sys->kind;
+    pl->opts = o;
+    pl->n_pulses = n_pulses;
+    const int nf = model_nf(sys->kind);
+
+    // k table
+    pl->n_k = grid_count(*grid);
+    std::vector<double> ktab((size_t)pl->n_k * 8);
+    build_rows(*sys, *grid, ktab.data());
+
+    // per-pulse records, staged projections and degree
+    const double nny = 0.5 * kSqrt3;
+    double proj[3] = {0, 0, 0};
+    if (sys->kind == HHG_SYS_PIFLUX2D) {
+        proj[0] = sys->pol_x;
+        proj[1] = sys->pol_y;
+    } else if (sys->kind == HHG_SYS_HONEYCOMB) {
+        proj[0] = 1.0 * sys->pol_x + 0.0 * sys->pol_y;
+        proj[1] = -0.5 * sys->pol_x + nny * sys->pol_y;
+        proj[2] = -0.5 * sys->pol_x - nny * sys->pol_y;
+    } else if (sys->kind == HHG_SYS_PIFLUX3D) {
+        proj[0] = 1.0;
+    }
+    int degree = 5;
+    for (int p = 0; p < n_pulses; ++p) {
+        const int d = choose_degree(pulses[p], proj, nf);
+        if (d < 0) {
+            delete pl;
+            return set_err(ctx, HHG_UNSUPPORTED,
+                           "measurement interval too coarse for the staged pulse interpolants");
+        }
+        degree = std::max(degree, d);
+    }
+    pl->degree = degree;
+    const int slot = hhg::slot_doubles(nf, degree);
+
+    // work decomposition
+    const int64_t tiles = (pl->n_k + 31) / 32;
+    int tpi = o.tile_k > 0 ? o.tile_k : 1;
+    if (o.tile_k <= 0) {
+        // auto: keep at least ~8 items per resident warp when there is work
+        // for that, and the partial buffer below 8 GB
+        const long long resident = (long long)ctx->sm_count * 16;
+        long long total_samples = 0;
+        for (int p = 0; p < n_pulses; ++p) total_samples += pulses[p].n_measurements + 1;
+        while (true) {
+            const long long items = (long long)n_pulses * ((tiles + tpi - 1) / tpi);
+            const double part_bytes = 8.0 * (double)((tiles + tpi - 1) / tpi) * (double)total_samples;
+            if (part_bytes > 8e9 || items > 64 * resident) {
+                if (tpi >= tiles) break;
+                tpi *= 2;
+                continue;
+            }
+            break;
+        }
+    }
+    pl->tiles_per_item = tpi;
+    pl->items_per_pulse = (int)((tiles + tpi - 1) / tpi);
+    pl->n_items = (long long)pl->items_per_pulse * n_pulses;
+
+    pl->pulses.resize(n_pulses);
+    pl->window_end.resize(n_pulses);
+    for (int p = 0; p < n_pulses; ++p) pl->window_end[p] = pulses[p].window_end;
+    std::vector<long long> ioff(n_pulses + 1, 0);
+    long long coef_len = 0, part_len = 0, j_len = 0;
+    for (int p = 0; p < n_pulses; ++p) {
+        const hhg_pulse_desc &q = pulses[p];
+        PulseDev &d = pl->pulses[p];
+        std::memset(&d, 0, sizeof d);
+        d.amplitude = q.amplitude;
+        d.t_begin = q.t_begin;
+        d.t_end = q.t_begin + 2 * kPi * q.n_cycles;  // CosineLaser::base_duration (CosineLaser.hpp:13-15)
+        d.inv_n_cycles = 1. / q.n_cycles;
+        d.phase = q.phase;
+        d.window_begin = q.window_begin;
+        d.measure_every = (q.window_end - q.window_begin) / q.n_measurements;
+        d.dt0 = d.measure_every / q.n_subdivisions;
+        const double es = q.energy_scale;
+        switch (sys->kind) {
+        case HHG_SYS_DIRAC2D:
+            d.mp[0] = 2.0 * sys->velocity * es;
+            d.mp[1] = 2.0 * sys->mass * es;
+            break;
+        case HHG_SYS_PIFLUX3D:
+            d.mp[0] = 4.0 * sys->hopping * es;
+            break;
+        case HHG_SYS_PIFLUX2D:
+            d.mp[0] = -4.0 * sys->hopping * es;
+            break;
+        case HHG_SYS_HONEYCOMB:
+            d.mp[0] = 2.0 * sys->hopping * es;
+            d.mp[1] = 2.0 * sys->mass * es;
+            break;
+        default:
+            break;
+        }
+        d.mp[2] = sys->pol_x;
+        d.mp[3] = sys->pol_y;
+        for (int n = 0; n < 3; ++n) d.s[n] = proj[n];
+        // sample-0 record, exact: A(t_0) and the staged functions at it
+        const double t0s = 0 * d.measure_every + d.window_begin;
+        double env = 0.0;
+        if (!(t0s <= d.t_begin || t0s >= d.t_end)) env = 0.5 * (1. - cos(d.inv_n_cycles * (t0s - d.t_begin)));
+        const double A0 = d.amplitude * (env * sin(t0s + d.phase));
+        d.s0rec[0] = A0;
+        if (nf == 1) d.s0rec[1] = A0;
+        else if (sys->kind == HHG_SYS_PIFLUX3D) {
+            d.s0rec[1] = cos(A0);
+            d.s0rec[2] = sin(A0);
+        } else
+            for (int n = 0; n < nf / 2; ++n) {
+                d.s0rec[1 + 2 * n] = cos(proj[n] * A0);
+                d.s0rec[2 + 2 * n] = sin(proj[n] * A0);
+            }
+        d.n_meas = q.n_measurements;
+        d.items = pl->items_per_pulse;
+        d.coef_off = coef_len;
+        d.part_off = part_len;
+        d.j_off = j_len;
+        coef_len += (long long)q.n_measurements * slot;
+        part_len += (long long)pl->items_per_pulse * (q.n_measurements + 1);
+        j_len += q.n_measurements + 1;
+        ioff[p + 1] = ioff[p] + q.n_measurements;
+    }
+    pl->coef_len = coef_len;
+    pl->part_len = part_len;
+    pl->j_len = j_len;
+    pl->n_intervals = ioff[n_pulses];
+    // accumulated interval ends (t_begin = t_end; t_end += measure_every, PiFlux.cpp:108-109)
+    std::vector<double> tgrid((size_t)(pl->n_intervals + n_pulses));
+    for (int p = 0; p < n_pulses; ++p) {
+        double *tg = tgrid.data() + ioff[p] + p;
+        double t_begin = pl->pulses[p].window_begin;
+        double t_end = t_begin + pl->pulses[p].measure_every;
+        tg[0] = t_begin;
+        for (int i = 1; i <= pulses[p].n_measurements; ++i) {
+            tg[i] = t_end;
+            t_begin = t_end;
+            t_end += pl->pulses[p].measure_every;
+        }
+    }
+
+    auto fail = [&](const char *what, cudaError_t e) {
+        hhg_plan_destroy(pl);
+        return set_err(ctx, HHG_CUDA_ERROR, std::string(what) + ": " + cudaGetErrorString(e));
+    };
+    cudaError_t e;
+    cudaStream_t s = ctx->stream;
+    if ((e = cudaMalloc(&pl->d_ktab, ktab.size() * sizeof(double))) != cudaSuccess) return fail("alloc k table", e);
+    if ((e = cudaMalloc(&pl->d_pulses, n_pulses * sizeof(PulseDev))) != cudaSuccess) return fail("alloc pulses", e);
+    if ((e = cudaMalloc(&pl->d_coef, coef_len * sizeof(double))) != cudaSuccess) return fail("alloc staging", e);
+    if ((e = cudaMalloc(&pl->d_part, part_len * sizeof(double))) != cudaSuccess) return fail("alloc partials", e);
+    if ((e = cudaMalloc(&pl->d_j, j_len * sizeof(double))) != cudaSuccess) return fail("alloc j", e);
+    if ((e = cudaMalloc(&pl->d_tgrid, tgrid.size() * sizeof(double))) != cudaSuccess) return fail("alloc tgrid", e);
+    if ((e = cudaMalloc(&pl->d_ioff, ioff.size() * sizeof(long long))) != cudaSuccess) return fail("alloc offsets", e);
+    if ((e = cudaMalloc(&pl->d_counters, 8 * sizeof(unsigned long long))) != cudaSuccess) return fail("alloc counters", e);
+    if ((e = cudaMalloc(&pl->d_status, sizeof(int))) != cudaSuccess) return fail("alloc status", e);
+    if ((e = cudaMemcpyAsync(pl->d_ktab, ktab.data(), ktab.size() * sizeof(double), cudaMemcpyHostToDevice, s)) != cudaSuccess) return fail("upload k table", e);
+    if ((e = cudaMemcpyAsync(pl->d_pulses, pl->pulses.data(), n_pulses * sizeof(PulseDev), cudaMemcpyHostToDevice, s)) != cudaSuccess) return fail("upload pulses", e);
+    if ((e = cudaMemcpyAsync(pl->d_tgrid, tgrid.data(), tgrid.size() * sizeof(double), cudaMemcpyHostToDevice, s)) != cudaSuccess) return fail("upload tgrid", e);
+    if ((e = cudaMemcpyAsync(pl->d_ioff, ioff.data(), ioff.size() * sizeof(long long), cudaMemcpyHostToDevice, s)) != cudaSuccess) return fail("upload offsets", e);
+    hhg::StageReq sr{pl->d_pulses, n_pulses, pl->d_tgrid, pl->d_ioff, pl->d_coef, pl->n_intervals, degree, s};
+    if ((st = stage_variant(pl, sr)) != HHG_OK) {
+        hhg_plan_destroy(pl);
+        return st;
+    }
+    // persistent grid: resident CTAs, but no more than the items need
+    int occ = 0;
+    hhg::LaunchReq lr{};
+    lr.degree = degree;
+    lr.precision = o.precision;
+    lr.stepper = o.stepper;
+    lr.proposer = o.proposer;
+    lr.grid = 0;
+    lr.occupancy_out = &occ;
+    if ((st = launch_variant(pl, lr)) != HHG_OK) {
+        hhg_plan_destroy(pl);
+        return st;
+    }
+    const long long max_ctas = (long long)std::max(occ, 1) * ctx->sm_count;
+    const long long need = (pl->n_items + 3) / 4;
+    pl->grid = (int)std::max(1LL, std::min(max_ctas, need));
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return fail("plan setup", e);
+    *out = pl;
+    return HHG_OK;
+}
+
+void hhg_plan_destroy(hhg_plan *pl) {
+    if (!pl) return;
+    cudaSetDevice(pl->ctx->device);
+    cudaFree(pl->d_ktab);
+    cudaFree(pl->d_pulses);
+    cudaFree(pl->d_coef);
+    cudaFree(pl->d_part);
+    cudaFree(pl->d_j);
+    cudaFree(pl->d_tgrid);
+    cudaFree(pl->d_ioff);
+    cudaFree(pl->d_counters);
+    cudaFree(pl->d_status);
+    cudaFree(pl->d_spec);
+    cudaFree(pl->d_x);
+    cudaFree(pl->d_F);
+    delete pl;
+}
+
+int64_t hhg_plan_j_length(const hhg_plan *pl) { return pl ? pl->j_len : 0; }
+
+const double *hhg_plan_device_j(const hhg_plan *pl) { return pl ? pl->d_j : nullptr; }
+
+hhg_status hhg_plan_execute_async(hhg_plan *pl, void *stream) {
+    if (!pl) return HHG_BAD_CONFIG;
+    hhg_ctx *ctx = pl->ctx;
+    cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+    HHG_CUDA(ctx, cudaSetDevice(ctx->device));
+    HHG_CUDA(ctx, cudaMemsetAsync(pl->d_counters, 0, 8 * sizeof(unsigned long long), s));
+    HHG_CUDA(ctx, cudaMemsetAsync(pl->d_status, 0, sizeof(int), s));
+    hhg::LaunchReq lr{};
+    lr.kp.ktab = pl->d_ktab;
+    lr.kp.pulses = pl->d_pulses;
+    lr.kp.coef = pl->d_coef;
+    lr.kp.part = pl->d_part;
+    lr.kp.counters = pl->d_counters;
+    lr.kp.status = pl->d_status;
+    lr.kp.n_items = pl->n_items;
+    lr.kp.n_k = (int)pl->n_k;
+    lr.kp.tiles_per_item = pl->tiles_per_item;
+    lr.kp.items_per_pulse = pl->items_per_pulse;
+    lr.kp.max_failed = pl->opts.max_failed_steps;
+    lr.kp.max_attempts = pl->opts.max_attempts_per_interval;
+    lr.kp.magnus_substeps = pl->opts.magnus_substeps;
+    lr.kp.abs_tol = pl->opts.abs_tol;
+    lr.kp.rel_tol = pl->opts.rel_tol;
+    lr.kp.err_floor = pow(5.0, -8.0);
+    lr.kp.grow_max = 9.0 / 10.0 * pow(pow(5.0, -8.0), -1.0 / 8);
+    lr.degree = pl->degree;
+    lr.precision = pl->opts.precision;
+    lr.stepper = pl->opts.stepper;
+    lr.proposer = pl->opts.proposer;
+    lr.grid = pl->grid;
+    lr.stream = s;
+    lr.occupancy_out = nullptr;
+    const bool timed = true;
+    HHG_CUDA(ctx, cudaEventRecord(ctx->ev[0], s));
+    hhg_status st = launch_variant(pl, lr);
+    if (st != HHG_OK) return st;
+    HHG_CUDA(ctx, cudaEventRecord(ctx->ev[1], s));
+    const int threads = 256;
+    const long long blocks = (pl->j_len + threads - 1) / threads;
+    hhg::reduce_partials_kernel<<<(unsigned)blocks, threads, 0, s>>>(pl->d_pulses, pl->n_pulses,
+                                                                     pl->d_part, pl->d_j, pl->j_len);
+    HHG_CUDA(ctx, cudaGetLastError());
+    HHG_CUDA(ctx, cudaEventRecord(ctx->ev[2], s));
+    pl->timed = timed;
+    return HHG_OK;
+}
+
+hhg_status hhg_plan_fetch(hhg_plan *pl, double *j_out, hhg_stats *stats) {
+    if (!pl) return HHG_BAD_CONFIG;
+    hhg_ctx *ctx = pl->ctx;
+    HHG_CUDA(ctx, cudaSetDevice(ctx->device));
+    HHG_CUDA(ctx, cudaDeviceSynchronize());
+    unsigned long long cnt[8];
+    int status = 0;
+    HHG_CUDA(ctx, cudaMemcpy(cnt, pl->d_counters, sizeof cnt, cudaMemcpyDeviceToHost));
+    HHG_CUDA(ctx, cudaMemcpy(&status, pl->d_status, sizeof status, cudaMemcpyDeviceToHost));
+    if (j_out) HHG_CUDA(ctx, cudaMemcpy(j_out, pl->d_j, pl->j_len * sizeof(double), cudaMemcpyDeviceToHost));
+    if (stats) {
+        std::memset(stats, 0, sizeof *stats);
+        stats->k_points = pl->n_k;
+        stats->trajectories = pl->n_k * pl->n_pulses;
+        stats->attempted_steps = (int64_t)cnt[1];
+        stats->rejected_steps = (int64_t)cnt[2];
+        stats->failed_trajectories = (int64_t)(cnt[3] + cnt[4]);
+        stats->poly_degree = pl->degree;
+        stats->items = (int32_t)pl->n_items;
+        if (pl->timed) {
+            float a = 0.f, b = 0.f;
+            cudaEventElapsedTime(&a, ctx->ev[0], ctx->ev[1]);
+            cudaEventElapsedTime(&b, ctx->ev[0], ctx->ev[2]);
+            stats->kernel_ms = a;
+            stats->total_ms = b;
+        }
+    }
+    if (status == 2)
+        return set_err(ctx, HHG_STEP_LIMIT,
+                       "Max number of iterations exceeded (" + std::to_string(pl->opts.max_failed_steps) +
+                           "). A new step size was not found.");
+    if (status == 3) return set_err(ctx, HHG_NONFINITE, "non-finite Bloch vector");
+    return HHG_OK;
+}
+
+hhg_status hhg_gpu_current_density(hhg_ctx *ctx, const hhg_system_desc *sys,
+                                   const hhg_pulse_desc *pulses, int n_pulses,
+                                   const hhg_grid_desc *grid, const hhg_solver_opts *opts,
+                                   double *j_out, hhg_stats *stats) {
+    if (!ctx || !j_out) return set_err(ctx, HHG_BAD_CONFIG, "null context or output");
+    hhg_plan *pl = nullptr;
+    hhg_status st = hhg_plan_create(ctx, sys, pulses, n_pulses, grid, opts, &pl);
+    if (st != HHG_OK) return st;
+    st = hhg_plan_execute_async(pl, nullptr);
+    if (st == HHG_OK) st = hhg_plan_fetch(pl, j_out, stats);
+    hhg_plan_destroy(pl);
+    return st;
+}
+
+hhg_status hhg_gpu_spectrum(hhg_ctx *ctx, const double *j, int n_measurements, double t_begin,
+                            double t_end, double *re_out, double *im_out, double *freq_out) {
+    if (!ctx || !j || !re_out || !im_out || !freq_out || n_measurements < 1)
+        return set_err(ctx, HHG_BAD_CONFIG, "bad spectrum arguments");
+    if (!(t_end > t_begin)) return set_err(ctx, HHG_BAD_CONFIG, "empty time window");
+    HHG_CUDA(ctx, cudaSetDevice(ctx->device));
+    const int n = n_measurements + 1;
+    const long long n_in_ll = 8LL * n;  // zero_padding (hhg.cpp:36)
+    if (n_in_ll > (1LL << 30)) return set_err(ctx, HHG_BAD_CONFIG, "spectrum too long");
+    const int n_in = (int)n_in_ll;
+    const int n_fft = n_in / 2 + 1;
+    cudaStream_t s = ctx->stream;
+    if (ctx->x_cap < (size_t)n_in) {
+        cudaFree(ctx->d_x);
+        ctx->d_x = nullptr;
+        HHG_CUDA(ctx, cudaMalloc(&ctx->d_x, sizeof(double) * n_in));
+        ctx->x_cap = n_in;
+    }
+    if (ctx->f_cap < (size_t)n_fft) {
+        cudaFree(ctx->d_F);
+        cudaFree(ctx->d_out);
+        ctx->d_F = nullptr;
+        ctx->d_out = nullptr;
+        HHG_CUDA(ctx, cudaMalloc(&ctx->d_F, sizeof(double2) * n_fft));
+        HHG_CUDA(ctx, cudaMalloc(&ctx->d_out, sizeof(double) * 3 * n_fft));
+        ctx->f_cap = n_fft;
+    }
+    cufftHandle plan;
+    auto it = ctx->fft_plans.find(n_in);
+    if (it == ctx->fft_plans.end()) {
+        if (cufftPlan1d(&plan, n_in, CUFFT_D2Z, 1) != CUFFT_SUCCESS)
+            return set_err(ctx, HHG_CUDA_ERROR, "cufftPlan1d failed");
+        ctx->fft_plans[n_in] = plan;
+    } else {
+        plan = it->second;
+    }
+    if (cufftSetStream(plan, s) != CUFFT_SUCCESS) return set_err(ctx, HHG_CUDA_ERROR, "cufftSetStream failed");
+    // the host j goes into the tail of the padded buffer's scratch, then pad
+    double *d_j = ctx->d_out;  // 3 n_fft >= n doubles of scratch
+    HHG_CUDA(ctx, cudaMemcpyAsync(d_j, j, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    hhg::pad_kernel<<<(n_in + 255) / 256, 256, 0, s>>>(d_j, n, ctx->d_x, n_in);
+    HHG_CUDA(ctx, cudaGetLastError());
+    if (cufftExecD2Z(plan, ctx->d_x, (cufftDoubleComplex *)ctx->d_F) != CUFFT_SUCCESS)
+        return set_err(ctx, HHG_CUDA_ERROR, "cufftExecD2Z failed");
+    const double delta_t = (t_end - t_begin) / n_measurements;
+    hhg::trapezoid_correct_kernel<<<(n_fft + 255) / 256, 256, 0, s>>>(
+        ctx->d_F, n_fft, n_in, delta_t, t_begin, t_end, ctx->d_x, ctx->d_out,
+        ctx->d_out + n_fft, ctx->d_out + 2 * n_fft);
+    HHG_CUDA(ctx, cudaGetLastError());
+    HHG_CUDA(ctx, cudaMemcpyAsync(re_out, ctx->d_out, sizeof(double) * n_fft, cudaMemcpyDeviceToHost, s));
+    HHG_CUDA(ctx, cudaMemcpyAsync(im_out, ctx->d_out + n_fft, sizeof(double) * n_fft, cudaMemcpyDeviceToHost, s));
+    HHG_CUDA(ctx, cudaMemcpyAsync(freq_out, ctx->d_out + 2 * n_fft, sizeof(double) * n_fft, cudaMemcpyDeviceToHost, s));
+    HHG_CUDA(ctx, cudaStreamSynchronize(s));
+    return HHG_OK;
+}
+
+namespace {
+hhg_status get_fft_plan(hhg_ctx *ctx, int n_in, cufftHandle *out) {
+    auto it = ctx->fft_plans.find(n_in);
+    if (it != ctx->fft_plans.end()) {
+        *out = it->second;
+        return HHG_OK;
+    }
+    cufftHandle plan;
+    if (cufftPlan1d(&plan, n_in, CUFFT_D2Z, 1) != CUFFT_SUCCESS)
+        return set_err(ctx, HHG_CUDA_ERROR, "cufftPlan1d failed");
+    ctx->fft_plans[n_in] = plan;
+    *out = plan;
+    return HHG_OK;
+}
+}  // namespace
+
+hhg_status hhg_plan_spectrum_async(hhg_plan *pl, void *stream) {
+    if (!pl) return HHG_BAD_CONFIG;
+    hhg_ctx *ctx = pl->ctx;
+    cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+    HHG_CUDA(ctx, cudaSetDevice(ctx->device));
+    if (!pl->d_spec) {
+        long long max_in = 0, off = 0;
+        pl->spec_off.assign(pl->n_pulses + 1, 0);
+        for (int p = 0; p < pl->n_pulses; ++p) {
+            const long long n_in = 8LL * (pl->pulses[p].n_meas + 1);
+            max_in = std::max(max_in, n_in);
+            pl->spec_off[p] = off;
+            off += n_in / 2 + 1;
+        }
+        pl->spec_off[pl->n_pulses] = off;
+        pl->spec_len = off;
+        HHG_CUDA(ctx, cudaMalloc(&pl->d_spec, sizeof(double) * 3 * off));
+        HHG_CUDA(ctx, cudaMalloc(&pl->d_x, sizeof(double) * max_in));
+        HHG_CUDA(ctx, cudaMalloc(&pl->d_F, sizeof(double2) * (max_in / 2 + 1)));
+    }
+    for (int p = 0; p < pl->n_pulses; ++p) {
+        const PulseDev &d = pl->pulses[p];
+        const int n = d.n_meas + 1;
+        const int n_in = 8 * n, n_fft = n_in / 2 + 1;
+        cufftHandle fp;
+        hhg_status st = get_fft_plan(ctx, n_in, &fp);
+        if (st != HHG_OK) return st;
+        if (cufftSetStream(fp, s) != CUFFT_SUCCESS) return set_err(ctx, HHG_CUDA_ERROR, "cufftSetStream failed");
+        hhg::pad_kernel<<<(n_in + 255) / 256, 256, 0, s>>>(pl->d_j + d.j_off, n, pl->d_x, n_in);
+        HHG_CUDA(ctx, cudaGetLastError());
+        if (cufftExecD2Z(fp, pl->d_x, (cufftDoubleComplex *)pl->d_F) != CUFFT_SUCCESS)
+            return set_err(ctx, HHG_CUDA_ERROR, "cufftExecD2Z failed");
+        double *base = pl->d_spec + 3 * pl->spec_off[p];
+        hhg::trapezoid_correct_kernel<<<(n_fft + 255) / 256, 256, 0, s>>>(
+            pl->d_F, n_fft, n_in, d.measure_every, d.window_begin, pl->window_end[p], pl->d_x,
+            base, base + n_fft, base + 2 * n_fft);
+        HHG_CUDA(ctx, cudaGetLastError());
+    }
+    return HHG_OK;
+}
+
+hhg_status hhg_plan_fetch_spectrum(hhg_plan *pl, int pulse, double *re_out, double *im_out,
+                                   double *freq_out) {
+    if (!pl || pulse < 0 || pulse >= pl->n_pulses || !pl->d_spec) return HHG_BAD_CONFIG;
+    hhg_ctx *ctx = pl->ctx;
+    HHG_CUDA(ctx, cudaSetDevice(ctx->device));
+    HHG_CUDA(ctx, cudaDeviceSynchronize());
+    const long long n_fft = pl->spec_off[pulse + 1] - pl->spec_off[pulse];
+    const double *base = pl->d_spec + 3 * pl->spec_off[pulse];
+    if (re_out) HHG_CUDA(ctx, cudaMemcpy(re_out, base, sizeof(double) * n_fft, cudaMemcpyDeviceToHost));
+    if (im_out) HHG_CUDA(ctx, cudaMemcpy(im_out, base + n_fft, sizeof(double) * n_fft, cudaMemcpyDeviceToHost));
+    if (freq_out) HHG_CUDA(ctx, cudaMemcpy(freq_out, base + 2 * n_fft, sizeof(double) * n_fft, cudaMemcpyDeviceToHost));
+    return HHG_OK;
+}
+
+hhg_status hhg_measure_fp64_peak(hhg_ctx *ctx, double *tflops) {
+    if (!ctx || !tflops) return HHG_BAD_CONFIG;
+    HHG_CUDA(ctx, cudaSetDevice(ctx->device));
+    double *d_out = nullptr;
+    HHG_CUDA(ctx, cudaMalloc(&d_out, sizeof(double)));
+    const int threads = 256, blocks = ctx->sm_count * 8, iters = 4096;
+    cudaStream_t s = ctx->stream;
+    for (int w = 0; w < 2; ++w)
+        hhg::fp64_fma_probe_kernel<<<blocks, threads, 0, s>>>(d_out, iters, 0.999999, 1e-7);
+    float best = 1e30f;
+    for (int r = 0; r < 5; ++r) {
+        cudaEventRecord(ctx->ev[0], s);
+        hhg::fp64_fma_probe_kernel<<<blocks, threads, 0, s>>>(d_out, iters, 0.999999, 1e-7);
+        cudaEventRecord(ctx->ev[1], s);
+        cudaEventSynchronize(ctx->ev[1]);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]);
+        best = std::min(best, ms);
+    }
+    cudaError_t e = cudaGetLastError();
+    cudaFree(d_out);
+    if (e != cudaSuccess) return set_err(ctx, HHG_CUDA_ERROR, cudaGetErrorString(e));
+    const double flops = 2.0 * 8.0 * iters * (double)threads * blocks;
+    *tflops = flops / (best * 1e-3) / 1e12;
+    return HHG_OK;
+}
+
+}  // extern "C"

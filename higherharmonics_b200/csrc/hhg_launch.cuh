@@ -1,0 +1,101 @@
+// hhg_launch.cuh -- per-model kernel instantiation and launch dispatch.  Each
+// kernels_<model>.cu includes this header once with HHG_MODEL set, so the
+// model families compile in parallel translation units.
+#pragma once
+
+#include "hhg_device.cuh"
+
+namespace hhg {
+
+struct LaunchReq {
+    KParams kp;
+    int degree;     // 5, 7 or 11
+    int precision;  // 0 FP64, 1 mixed (FP32 right-hand side)
+    int stepper;    // 0 RKF78, 1 Magnus-4
+    int proposer;   // 0 restart at dt0, 1 carry
+    int grid;       // CTAs; 0 = query occupancy only
+    cudaStream_t stream;
+    int *occupancy_out;  // blocks per SM for the selected variant (if non-null)
+};
+
+struct StageReq {
+    const PulseDev *pulses;
+    int n_pulses;
+    const double *tgrid;
+    const long long *interval_off;
+    double *coef;
+    long long total_intervals;
+    int degree;
+    cudaStream_t stream;
+};
+
+template <int M, int D, typename R, int ST, int PR>
+cudaError_t launch_one(const LaunchReq &r) {
+    auto kern = bz_integrate_kernel<M, D, R, ST, PR>;
+    if (r.occupancy_out) {
+        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(r.occupancy_out, kern, 128, 0);
+        if (e != cudaSuccess) return e;
+    }
+    if (r.grid <= 0) return cudaSuccess;
+    kern<<<r.grid, 128, 0, r.stream>>>(r.kp);
+    return cudaGetLastError();
+}
+
+template <int M, int D>
+cudaError_t launch_deg(const LaunchReq &r) {
+    if (r.stepper == 1) return launch_one<M, D, double, 1, 0>(r);
+    if (r.precision == 0) {
+        if (r.proposer == 0) return launch_one<M, D, double, 0, 0>(r);
+        return launch_one<M, D, double, 0, 1>(r);
+    }
+    if (r.proposer == 0) return launch_one<M, D, float, 0, 0>(r);
+    return launch_one<M, D, float, 0, 1>(r);
+}
+
+template <int M>
+cudaError_t launch_model(const LaunchReq &r) {
+    if (r.degree == 5) return launch_deg<M, 5>(r);
+    if (r.degree == 7) return launch_deg<M, 7>(r);
+    if (r.degree == 11) return launch_deg<M, 11>(r);
+    return cudaErrorInvalidValue;
+}
+
+template <int M>
+cudaError_t stage_model(const StageReq &s) {
+    const int threads = 128;
+    const long long blocks = (s.total_intervals + threads - 1) / threads;
+    if (s.degree == 5)
+        stage_pulses_kernel<M, 5><<<(unsigned)blocks, threads, 0, s.stream>>>(
+            s.pulses, s.n_pulses, s.tgrid, s.interval_off, s.coef, s.total_intervals);
+    else if (s.degree == 7)
+        stage_pulses_kernel<M, 7><<<(unsigned)blocks, threads, 0, s.stream>>>(
+            s.pulses, s.n_pulses, s.tgrid, s.interval_off, s.coef, s.total_intervals);
+    else if (s.degree == 11)
+        stage_pulses_kernel<M, 11><<<(unsigned)blocks, threads, 0, s.stream>>>(
+            s.pulses, s.n_pulses, s.tgrid, s.interval_off, s.coef, s.total_intervals);
+    else
+        return cudaErrorInvalidValue;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_dirac2d(const LaunchReq &r);
+cudaError_t launch_piflux2d(const LaunchReq &r);
+cudaError_t launch_piflux3d(const LaunchReq &r);
+cudaError_t launch_honeycomb(const LaunchReq &r);
+cudaError_t launch_dirac3d(const LaunchReq &r);
+cudaError_t stage_dirac2d(const StageReq &s);
+cudaError_t stage_piflux2d(const StageReq &s);
+cudaError_t stage_piflux3d(const StageReq &s);
+cudaError_t stage_honeycomb(const StageReq &s);
+cudaError_t stage_dirac3d(const StageReq &s);
+
+}  // namespace hhg
+
+#ifdef HHG_MODEL
+#define HHG_CAT2(a, b) a##b
+#define HHG_CAT(a, b) HHG_CAT2(a, b)
+namespace hhg {
+cudaError_t HHG_CAT(launch_, HHG_MODEL_NAME)(const LaunchReq &r) { return launch_model<HHG_MODEL>(r); }
+cudaError_t HHG_CAT(stage_, HHG_MODEL_NAME)(const StageReq &s) { return stage_model<HHG_MODEL>(s); }
+}  // namespace hhg
+#endif

@@ -1,0 +1,220 @@
+/*
+ * hhg_gpu.h -- C ABI of the B200 engine for HigherHarmonics' per-k-point
+ * Bloch integration -> Brillouin-zone current sum -> trapezoidal FFT path.
+ *
+ * The reference has no FFI: its boundary is the C++ class
+ * HHG::Dispatch::Dispatcher (sources/HHG/Dispatch/Dispatcher.hpp:14-50),
+ * whose compute(rank, n_ranks, n_z) fills current_density_time through
+ *   System::compute_current_density(Laser const*, TimeIntegrationConfig const&,
+ *                                   int rank, int n_ranks[, int n_z])
+ * (sources/HHG/Systems/PiFlux.hpp:92-93, Honeycomb.hpp:70-71,
+ *  DiracSystem.hpp:58-59), after which main() runs the TrapezoidalFFT
+ * (sources/hhg.cpp:264-292).  The entry points below replace those calls with
+ * plain-C types: POD descriptors in, caller-owned host buffers out, status
+ * codes instead of C++ exceptions.  No CUDA or torch type appears here; a
+ * stream is passed as an opaque pointer where one is accepted.
+ *
+ * Units are the reference's (Laser.hpp:13-16): time in 1/omega_L, energies
+ * in hbar*omega_L, momenta in inverse lattice units, hbar = e = 1.  Each
+ * pulse carries an energy_scale that multiplies every model energy, so a
+ * model given in other reduced units (e.g. the 2D Dirac model with omega =
+ * 0.1) is integrated in the reference's units with energy_scale = 1/omega.
+ *
+ * Threading: one host thread per context.  Calls are synchronous unless
+ * named *_async.  Several contexts may share a device.
+ */
+#ifndef HHG_GPU_H
+#define HHG_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HHG_ABI_VERSION 1
+
+/* Errors: the reference throws std::invalid_argument / std::runtime_error
+ * (sources/hhg.cpp:232, Dispatch/PiFluxDispatcher.cpp:104) and Boost.Odeint
+ * throws when 500 consecutive steps fail; these map to status codes. */
+typedef enum hhg_status {
+    HHG_OK = 0,
+    HHG_BAD_CONFIG = 1,   /* invalid descriptor / unknown system or laser type */
+    HHG_STEP_LIMIT = 2,   /* a trajectory exceeded the failed-step / step limit */
+    HHG_NONFINITE = 3,    /* a trajectory produced a non-finite Bloch vector */
+    HHG_CUDA_ERROR = 4,   /* CUDA runtime / cuFFT failure */
+    HHG_UNSUPPORTED = 5   /* valid request this build does not implement */
+} hhg_status;
+
+/* Model families (the reference's system_type, sources/hhg.cpp:224-233). */
+typedef enum hhg_system_kind {
+    HHG_SYS_DIRAC2D = 0,   /* gapped 2D Dirac: d = (v(kx-Ax), v(ky-Ay), mass) */
+    HHG_SYS_PIFLUX2D = 1,  /* square-lattice pi-flux: d = -2t(cos(kx-Ax), cos(ky-Ay), 0) */
+    HHG_SYS_PIFLUX3D = 2,  /* reference PiFlux: d = 2t(cos kx, cos ky, cos(kz-A)), field || z */
+    HHG_SYS_HONEYCOMB = 3, /* reference Honeycomb, optional staggered mass */
+    HHG_SYS_DIRAC3D = 4    /* reference DiracSystem sigma form, k = (k_z, kappa) */
+} hhg_system_kind;
+
+/* System: replaces the System ctor arguments (e.g. PiFlux.cpp:56-71).
+ * hopping = t (PiFlux: band_width/sqrt(12), Honeycomb: band_width/6),
+ * velocity = v (Dirac2D), mass = gap term, (pol_x, pol_y) = field
+ * polarisation unit vector (Honeycomb's laser_theta, Honeycomb.hpp:93-95). */
+typedef struct hhg_system_desc {
+    int32_t kind;
+    int32_t reserved;
+    double hopping;
+    double velocity;
+    double mass;
+    double pol_x, pol_y;
+} hhg_system_desc;
+
+typedef enum hhg_pulse_kind {
+    HHG_PULSE_COSINE = 0 /* CosineLaser, sources/HHG/Laser/CosineLaser.cpp:22-26 */
+} hhg_pulse_kind;
+
+/* One pulse instance plus its TimeIntegrationConfig
+ * (sources/HHG/TimeIntegrationConfig.hpp:5-12).  A(t) =
+ * amplitude * envelope(t) * sin(t + phase) with envelope = 0.5(1 - cos((t -
+ * t_begin)/n_cycles)) on (t_begin, t_begin + 2 pi n_cycles), 0 elsewhere;
+ * phase = 0 is the reference.  The sampled window is [window_begin,
+ * window_end] in n_measurements intervals of n_subdivisions initial RKF78
+ * steps each (the reference uses 50, e.g. PiFluxDispatcher.cpp:53). */
+typedef struct hhg_pulse_desc {
+    int32_t kind;
+    int32_t n_measurements;
+    int32_t n_subdivisions;
+    int32_t reserved;
+    double amplitude;     /* Laser::momentum_amplitude */
+    double n_cycles;
+    double t_begin;       /* Laser::t_begin */
+    double phase;
+    double window_begin;  /* TimeIntegrationConfig::t_begin */
+    double window_end;    /* TimeIntegrationConfig::t_end */
+    double energy_scale;  /* multiplies hopping, velocity and mass */
+} hhg_pulse_desc;
+
+/* k-point quadrature. */
+typedef enum hhg_grid_kind {
+    HHG_GRID_TENSOR_GL = 0,        /* n1 x n2 Gauss-Legendre on [x_lo,x_hi]x[y_lo,y_hi] */
+    HHG_GRID_RHOMBIC_GL = 1,       /* n1 x n2 GL in fractional coords of the honeycomb BZ */
+    HHG_GRID_PIFLUX3D_REF = 2,     /* PiFlux::current_density_continuum_limit grid, n1 = z_range, n2 = N_coarse */
+    HHG_GRID_HONEYCOMB_HEX_REF = 3,/* Honeycomb::compute_current_density grid, n1 = N_k */
+    HHG_GRID_EXPLICIT = 4          /* caller rows: kx, ky, kz, weight, S0x, S0y, S0z, 0 */
+} hhg_grid_kind;
+
+typedef struct hhg_grid_desc {
+    int32_t kind;
+    int32_t n1, n2;
+    int32_t reserved;
+    double x_lo, x_hi, y_lo, y_hi;
+    const double *rows; /* HHG_GRID_EXPLICIT: n_rows x 8 doubles, host memory */
+    int64_t n_rows;
+} hhg_grid_desc;
+
+typedef enum hhg_stepper { HHG_STEPPER_RKF78 = 0, HHG_STEPPER_MAGNUS4 = 1 } hhg_stepper;
+typedef enum hhg_precision { HHG_PREC_FP64 = 0, HHG_PREC_MIXED = 1 } hhg_precision;
+typedef enum hhg_proposer {
+    HHG_PROPOSER_NONE = 0,    /* reference: every interval restarts at dt = measure_every / n_subdivisions */
+    HHG_PROPOSER_CARRY = 1,   /* first step of an interval = last controller proposal */
+    HHG_PROPOSER_LEARNED = 2  /* first step of an interval = trained MLP proposal */
+} hhg_proposer;
+
+/* Solver options.  abs_tol / rel_tol: the reference uses 1e-12 / 1e-8
+ * (PiFlux.cpp:20-21).  max_failed_steps: Boost.Odeint's failed_step_checker
+ * limit (500).  max_attempts_per_interval bounds every device loop.
+ * tile_k: k-points per work item in units of 32 (0 = auto).
+ * block_threads: threads per CTA (0 = auto). */
+typedef struct hhg_solver_opts {
+    int32_t stepper;
+    int32_t precision;
+    int32_t proposer;
+    int32_t magnus_substeps;
+    double abs_tol, rel_tol;
+    int32_t max_failed_steps;
+    int32_t max_attempts_per_interval;
+    int32_t tile_k;
+    int32_t block_threads;
+} hhg_solver_opts;
+
+typedef struct hhg_stats {
+    int64_t k_points;
+    int64_t trajectories;
+    int64_t attempted_steps;  /* k.steps: attempted RKF78 steps (or Magnus sub-steps) */
+    int64_t rejected_steps;
+    int64_t failed_trajectories;
+    int32_t poly_degree;      /* degree of the staged A(t) interpolants */
+    int32_t items;            /* work items of the persistent launch */
+    double kernel_ms;         /* device time of the integration kernel(s), CUDA events */
+    double total_ms;          /* device time of the whole call */
+} hhg_stats;
+
+typedef struct hhg_ctx hhg_ctx;
+typedef struct hhg_plan hhg_plan;
+
+/* Library / context management. */
+int hhg_abi_version(void);
+hhg_status hhg_gpu_create(hhg_ctx **ctx, int device);
+void hhg_gpu_destroy(hhg_ctx *ctx);
+const char *hhg_last_error(const hhg_ctx *ctx);
+void hhg_default_solver_opts(hhg_solver_opts *opts);
+
+/* Gauss-Legendre nodes / weights on [-1,1], ascending (the reference's
+ * gauss::container<n> tables, sources/HHG/thread_gauss.hpp, hold the positive
+ * half of the same rule). */
+hhg_status hhg_gauss_legendre(int n, double *x, double *w);
+
+/* Number of k rows a grid descriptor expands to, and the rows themselves
+ * (kx, ky, kz, weight, S0x, S0y, S0z, 0) for the given system.  rows may be
+ * NULL to query the count only. */
+hhg_status hhg_grid_rows(const hhg_system_desc *sys, const hhg_grid_desc *grid, double *rows,
+                         int64_t *n_rows);
+
+/* One-shot drop-in for System::compute_current_density over n_pulses pulse
+ * instances: j_out (host, caller-owned) receives for pulse p the
+ * n_measurements_p + 1 samples of j(t) at offset sum_{q<p}(n_measurements_q
+ * + 1).  Synchronous. */
+hhg_status hhg_gpu_current_density(hhg_ctx *ctx, const hhg_system_desc *sys,
+                                   const hhg_pulse_desc *pulses, int n_pulses,
+                                   const hhg_grid_desc *grid, const hhg_solver_opts *opts,
+                                   double *j_out, hhg_stats *stats);
+
+/* TrapezoidalFFT::compute (sources/HHG/Fourier/TrapezoidalFFT.cpp:11-49) on
+ * the x8 zero-padded j(t) (sources/hhg.cpp:36,277-285), on the device.
+ * j has n_measurements + 1 samples on [t_begin, t_end]; re/im/freq receive
+ * 4 (n_measurements + 1) + 1 values each (host, caller-owned). */
+hhg_status hhg_gpu_spectrum(hhg_ctx *ctx, const double *j, int n_measurements, double t_begin,
+                            double t_end, double *re_out, double *im_out, double *freq_out);
+
+/* Plans: build the k table, pulse staging and work list once, then execute
+ * on device-resident buffers. */
+hhg_status hhg_plan_create(hhg_ctx *ctx, const hhg_system_desc *sys,
+                           const hhg_pulse_desc *pulses, int n_pulses,
+                           const hhg_grid_desc *grid, const hhg_solver_opts *opts,
+                           hhg_plan **plan);
+void hhg_plan_destroy(hhg_plan *plan);
+/* Total j samples over all pulses (length of a j buffer for this plan). */
+int64_t hhg_plan_j_length(const hhg_plan *plan);
+/* Launch the integration + reduction into the plan's device j buffer on
+ * `stream` (a cudaStream_t, or NULL for the context stream).  Asynchronous. */
+hhg_status hhg_plan_execute_async(hhg_plan *plan, void *stream);
+/* Device pointer of the plan's j buffer (valid until hhg_plan_destroy). */
+const double *hhg_plan_device_j(const hhg_plan *plan);
+/* Synchronise, check the device status word and copy j to host. */
+hhg_status hhg_plan_fetch(hhg_plan *plan, double *j_out, hhg_stats *stats);
+/* TrapezoidalFFT of every pulse's device-resident j into plan-owned device
+ * buffers (the device-side counterpart of hhg_gpu_spectrum).  Asynchronous. */
+hhg_status hhg_plan_spectrum_async(hhg_plan *plan, void *stream);
+/* Copy pulse `pulse`'s spectrum (4 (n_measurements + 1) + 1 values each) to
+ * host.  Synchronous. */
+hhg_status hhg_plan_fetch_spectrum(hhg_plan *plan, int pulse, double *re_out, double *im_out,
+                                   double *freq_out);
+
+/* Diagnostic without a reference counterpart: measured FP64 FMA throughput
+ * of the device (TFLOP/s, FMA = 2 flops), the denominator of the
+ * integration kernel's roofline. */
+hhg_status hhg_measure_fp64_peak(hhg_ctx *ctx, double *tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

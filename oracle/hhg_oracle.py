@@ -1,0 +1,288 @@
+"""CPU oracle bindings and the reference's Fourier tail, restated.
+
+TEST INFRASTRUCTURE ONLY.  The pytest suite, ``__graft_entry__.smoke()`` and
+the CPU-baseline leg of ``bench.py`` import this module as the checker; the
+product package never does.
+
+* ``libhhg_oracle.so`` (built from ``hhg_oracle.c`` by ``oracle/Makefile``)
+  holds the FP64 restatement of the per-k Bloch integration and BZ sums.
+* ``trapezoidal_fft`` restates ``TrapezoidalFFT::compute``
+  (sources/HHG/Fourier/TrapezoidalFFT.cpp:11-49) with the x8 zero padding of
+  sources/hhg.cpp:36,280-282, using numpy's r2c FFT in place of FFTW.
+
+Parity status: unpinned at the Boost.Odeint boundary (see hhg_oracle.h).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+DIRAC2D, PIFLUX2D, PIFLUX3D, HONEYCOMB, DIRAC3D = 0, 1, 2, 3, 4
+KROW = 8
+
+
+class OrcModel(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int), ("hopping", ctypes.c_double),
+                ("velocity", ctypes.c_double), ("mass", ctypes.c_double),
+                ("pol_x", ctypes.c_double), ("pol_y", ctypes.c_double)]
+
+
+class OrcPulse(ctypes.Structure):
+    _fields_ = [("amplitude", ctypes.c_double), ("t_begin", ctypes.c_double),
+                ("t_end", ctypes.c_double), ("inv_n_cycles", ctypes.c_double),
+                ("phase", ctypes.c_double)]
+
+
+class OrcTimeConfig(ctypes.Structure):
+    _fields_ = [("t_begin", ctypes.c_double), ("t_end", ctypes.c_double),
+                ("n_measurements", ctypes.c_int), ("n_subdivisions", ctypes.c_int)]
+
+
+class OrcSolver(ctypes.Structure):
+    _fields_ = [("abs_tol", ctypes.c_double), ("rel_tol", ctypes.c_double),
+                ("max_failed", ctypes.c_int), ("stepper", ctypes.c_int),
+                ("magnus_substeps", ctypes.c_int)]
+
+
+class OrcStats(ctypes.Structure):
+    _fields_ = [("attempted", ctypes.c_uint64), ("accepted", ctypes.c_uint64),
+                ("rejected", ctypes.c_uint64), ("failed_k", ctypes.c_uint64)]
+
+
+_LIBS: dict[str, ctypes.CDLL] = {}
+_D = ctypes.POINTER(ctypes.c_double)
+
+
+def build() -> None:
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib(fast: bool = False) -> ctypes.CDLL:
+    name = "libhhg_oracle_fast.so" if fast else "libhhg_oracle.so"
+    if name not in _LIBS:
+        path = os.path.join(HERE, name)
+        if not os.path.exists(path):
+            build()
+        L = ctypes.CDLL(path)
+        L.orc_laser.restype = ctypes.c_double
+        L.orc_raw_laser.restype = ctypes.c_double
+        L.orc_vertex.restype = ctypes.c_double
+        for fn in ("orc_grid_tensor", "orc_grid_rhombic", "orc_grid_piflux3d_ref",
+                   "orc_grid_honeycomb_hex_ref", "orc_evolve_k", "orc_current_density",
+                   "orc_step_history", "orc_dirac3d_sigma_k"):
+            getattr(L, fn).restype = ctypes.c_int
+        L.orc_grid_tensor.argtypes = [ctypes.POINTER(OrcModel), ctypes.c_int, ctypes.c_int,
+                                      ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                      ctypes.c_double, _D]
+        _LIBS[name] = L
+    return _LIBS[name]
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(_D)
+
+
+@dataclass
+class Pulse:
+    """CosineLaser (sources/HHG/Laser/CosineLaser.cpp) plus a carrier phase."""
+    amplitude: float
+    n_cycles: float
+    t_begin: float = 0.0
+    phase: float = 0.0
+
+    @property
+    def t_end(self) -> float:
+        return self.t_begin + 2 * np.pi * self.n_cycles
+
+    def c(self) -> OrcPulse:
+        return OrcPulse(self.amplitude, self.t_begin, self.t_end, 1.0 / self.n_cycles, self.phase)
+
+
+def model(kind: int, hopping=0.0, velocity=0.0, mass=0.0, pol=(1.0, 0.0)) -> OrcModel:
+    return OrcModel(kind, hopping, velocity, mass, pol[0], pol[1])
+
+
+def solver(abs_tol=1e-12, rel_tol=1e-8, stepper=0, magnus_substeps=1) -> OrcSolver:
+    return OrcSolver(abs_tol, rel_tol, 500, stepper, magnus_substeps)
+
+
+def time_config(t_begin, t_end, n, n_sub=50) -> OrcTimeConfig:
+    return OrcTimeConfig(t_begin, t_end, n, n_sub)
+
+
+def gauss_legendre(n: int):
+    x = np.zeros(n)
+    w = np.zeros(n)
+    lib().orc_gauss_legendre(ctypes.c_int(n), _p(x), _p(w))
+    return x, w
+
+
+def laser(p: Pulse, t) -> np.ndarray:
+    pc = p.c()
+    return np.array([lib().orc_laser(ctypes.byref(pc), ctypes.c_double(float(v)))
+                     for v in np.atleast_1d(t)])
+
+
+def grid_tensor(m: OrcModel, nx, ny, x_lo, x_hi, y_lo, y_hi) -> np.ndarray:
+    out = np.zeros((nx * ny, KROW))
+    lib().orc_grid_tensor(ctypes.byref(m), nx, ny, x_lo, x_hi, y_lo, y_hi, _p(out))
+    return out
+
+
+def grid_rhombic(m: OrcModel, n1, n2) -> np.ndarray:
+    out = np.zeros((n1 * n2, KROW))
+    lib().orc_grid_rhombic(ctypes.byref(m), ctypes.c_int(n1), ctypes.c_int(n2), _p(out))
+    return out
+
+
+def grid_piflux3d_ref(m: OrcModel, z_range=32, n_coarse=4) -> np.ndarray:
+    n = lib().orc_grid_piflux3d_ref(ctypes.byref(m), z_range, n_coarse, None)
+    out = np.zeros((n, KROW))
+    lib().orc_grid_piflux3d_ref(ctypes.byref(m), z_range, n_coarse, _p(out))
+    return out
+
+
+def grid_honeycomb_hex_ref(m: OrcModel, n_k=64) -> np.ndarray:
+    n = lib().orc_grid_honeycomb_hex_ref(ctypes.byref(m), n_k, None)
+    out = np.zeros((n, KROW))
+    lib().orc_grid_honeycomb_hex_ref(ctypes.byref(m), n_k, _p(out))
+    return out
+
+
+def evolve_k(m, p: Pulse, tc, s, krow) -> tuple[np.ndarray, OrcStats]:
+    st = OrcStats()
+    out = np.zeros((tc.n_measurements + 1, 3))
+    krow = np.ascontiguousarray(krow, dtype=np.float64)
+    pc = p.c()
+    rc = lib().orc_evolve_k(ctypes.byref(m), ctypes.byref(pc), ctypes.byref(tc),
+                            ctypes.byref(s), _p(krow), _p(out), ctypes.byref(st))
+    if rc != 0:
+        raise RuntimeError(f"orc_evolve_k failed with status {rc}")
+    return out, st
+
+
+def step_history(m, p: Pulse, tc, s, krow, cap=1 << 20) -> np.ndarray:
+    hist = np.zeros((cap, 4))
+    krow = np.ascontiguousarray(krow, dtype=np.float64)
+    pc = p.c()
+    n = lib().orc_step_history(ctypes.byref(m), ctypes.byref(pc), ctypes.byref(tc),
+                               ctypes.byref(s), _p(krow), ctypes.c_int(cap), _p(hist))
+    if n < 0:
+        raise RuntimeError(f"orc_step_history failed with status {-n}")
+    return hist[:n]
+
+
+def current_density(m, p: Pulse, tc, s, ktab: np.ndarray, threads=0, fast=False):
+    ktab = np.ascontiguousarray(ktab, dtype=np.float64)
+    j = np.zeros(tc.n_measurements + 1)
+    st = OrcStats()
+    pc = p.c()
+    rc = lib(fast).orc_current_density(ctypes.byref(m), ctypes.byref(pc), ctypes.byref(tc),
+                                       ctypes.byref(s), ctypes.c_int(ktab.shape[0]), _p(ktab),
+                                       _p(j), ctypes.byref(st), ctypes.c_int(threads))
+    return j, st, rc
+
+
+def magnus_coefficients(p: Pulse, delta_t, t0) -> np.ndarray:
+    out = np.zeros(4)
+    pc = p.c()
+    lib().orc_magnus_coefficients(ctypes.byref(pc), ctypes.c_double(delta_t),
+                                  ctypes.c_double(t0), _p(out))
+    return out
+
+
+def dirac_magnus_U(k, kappa, k_z, delta_t, coeffs) -> np.ndarray:
+    U = np.zeros(9)
+    cf = np.ascontiguousarray(coeffs, dtype=np.float64)
+    lib().orc_dirac_magnus_U(ctypes.c_double(k), ctypes.c_double(kappa), ctypes.c_double(k_z),
+                             ctypes.c_double(delta_t), _p(cf), _p(U))
+    return U.reshape(3, 3)
+
+
+def dirac3d_magnus_k(p: Pulse, tc, k_z, kappa) -> np.ndarray:
+    out = np.zeros(tc.n_measurements + 1)
+    pc = p.c()
+    lib().orc_dirac3d_magnus_k(ctypes.byref(pc), ctypes.byref(tc), ctypes.c_double(k_z),
+                               ctypes.c_double(kappa), _p(out))
+    return out
+
+
+def dirac3d_sigma_k(p: Pulse, tc, s, k_z, kappa) -> np.ndarray:
+    out = np.zeros(tc.n_measurements + 1)
+    st = OrcStats()
+    pc = p.c()
+    rc = lib().orc_dirac3d_sigma_k(ctypes.byref(pc), ctypes.byref(tc), ctypes.byref(s),
+                                   ctypes.c_double(k_z), ctypes.c_double(kappa), _p(out),
+                                   ctypes.byref(st))
+    if rc != 0:
+        raise RuntimeError(f"orc_dirac3d_sigma_k failed with status {rc}")
+    return out
+
+
+def rkf78_tableau():
+    c = np.zeros(13)
+    a = np.zeros(169)
+    b = np.zeros(13)
+    db = np.zeros(13)
+    lib().orc_rkf78_tableau(_p(c), _p(a), _p(b), _p(db))
+    return c, a.reshape(13, 13), b, db
+
+
+# --------------------------------------------------------------------------
+# Fourier tail
+# --------------------------------------------------------------------------
+ZERO_PADDING = 8  # sources/hhg.cpp:36
+
+
+def _is_zero(x: float) -> bool:
+    """GlobalDefinitions.hpp:61-71: |x| < 2^-44 by the biased exponent."""
+    bits = np.array([x], dtype=np.float64).view(np.uint64)[0]
+    return int((int(bits) >> 52) & 0x7FF) < 0x3D3
+
+
+def trapezoidal_fft(j: np.ndarray, t_begin: float, t_end: float, n_measurements: int):
+    """TrapezoidalFFT::compute on the x8 zero-padded j(t) (hhg.cpp:277-285).
+
+    Returns (frequencies, real, imag), each of length n_in/2 + 1 with
+    n_in = 8 (N + 1).  The end-point correction reads input[n_in - 1], which
+    the zero padding makes 0, exactly as the reference does.
+    """
+    delta_t = (t_end - t_begin) / n_measurements
+    n_in = ZERO_PADDING * (n_measurements + 1)
+    x = np.zeros(n_in)
+    x[: len(j)] = j
+    F = np.fft.rfft(x)
+    n_fft = n_in // 2 + 1
+    freq = 2 * np.arange(n_fft) * np.pi / (n_in * delta_t)
+    theta = freq * delta_t
+    W = np.empty(n_fft)
+    a0 = np.empty(n_fft, dtype=np.complex128)
+    for i, th in enumerate(theta):
+        if _is_zero(th):
+            W[i] = 1.0
+            a0[i] = -0.5
+        else:
+            W[i] = 2.0 * (1.0 - np.cos(th)) / (th * th)
+            a0[i] = (-(1.0 - np.cos(th)) + 1j * (th - np.sin(th))) / (th * th)
+    corr = a0 * x[0] + np.conj(a0) * np.exp(1j * freq * (t_end - t_begin)) * x[n_in - 1]
+    out = (delta_t * W) * np.exp(1j * freq * t_begin) * F + corr
+    return freq, delta_t * out.real, delta_t * out.imag
+
+
+def harmonic_intensities(freq, re, im, max_order: int):
+    """I(n) = |j_hat(n omega_L)|^2 at integer harmonics n = 1..max_order.
+
+    Frequencies are in units of omega_L (time in 1/omega_L), so harmonic n
+    sits at freq = n; the nearest bin is used.
+    """
+    p = re * re + im * im
+    out = np.zeros(max_order)
+    for n in range(1, max_order + 1):
+        out[n - 1] = p[int(np.argmin(np.abs(freq - n)))]
+    return out
