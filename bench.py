@@ -222,8 +222,12 @@ def our_arm(args, wl_name):
     eng = api.Engine(dev)
     okw = VARIANTS[args.variant]
     plan = eng.plan(wl.system, wl.pulses, wl.grid, wl.opts(**okw))
-    stream = torch.cuda.current_stream()
+    # a dedicated stream: the legacy default stream has handle 0, which the
+    # C ABI reads as "the context's own stream"
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     sptr = stream.cuda_stream
+    assert sptr != 0
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
     def step():

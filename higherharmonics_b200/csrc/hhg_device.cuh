@@ -7,13 +7,28 @@
 // reference's measurement loop (PiFlux.cpp:96-110) interval by interval; the
 // lanes are lock-stepped per interval (every lane must land on t_i), and
 // inside an interval each lane runs its own adaptive step sequence under
-// predication.  The pulse is staged per interval in shared memory as Chebyshev
-// interpolants (monomial form in u in [-1,1]) of A(t) or of cos/sin(s A(t)),
-// so no transcendental is evaluated inside a right-hand side.  At every sample
-// the lanes' weighted current contributions are reduced with a butterfly
-// shuffle; lane (i mod 32) keeps sample i and every 32 samples the warp
-// stores its 32 sums with one coalesced 256-byte store into the work item's
-// row of the partial buffer.  Work items are taken from a global atomic
+// predication.
+//
+// The pulse is staged per interval in shared memory, in two forms:
+//  * Chebyshev interpolants (monomial form in u in [-1,1]) of A(t) or of
+//    cos/sin(s A(t)), so no transcendental is evaluated inside a right-hand
+//    side for an arbitrary step;
+//  * the exact values at the 13 stage times of the interval's "standard
+//    schedule": the reference restarts every interval at dt0 = measure_every /
+//    n_subdivisions (PiFlux.cpp:98,105), and a trajectory whose error stays
+//    below 5^-8 grows dt by exactly 0.9 * 5 each step, so every such lane takes
+//    the same (t, dt) sequence.  When all active lanes of a warp are on that
+//    schedule (a warp vote per attempt) the right-hand sides read the
+//    tabulated values with broadcast shared-memory loads.
+// The right-hand side combines the FP64 pulse values with the k-dependent
+// constants in FP64 and only then narrows to the stage precision R, so in the
+// mixed-precision variant every FP32 rounding depends on k and averages out in
+// the Brillouin-zone sum instead of acting like a common field error.
+//
+// At every sample the lanes' weighted current contributions are reduced with a
+// butterfly shuffle; lane (i mod 32) keeps sample i and every 32 samples the
+// warp stores its 32 sums with one coalesced 256-byte store into the work
+// item's row of the partial buffer.  Work items are taken from a global atomic
 // counter (persistent, work-stealing launch), and a second kernel reduces the
 // partial rows of each pulse in item order with compensated sums, so j(t) is
 // bitwise reproducible whatever the schedule.
@@ -26,38 +41,63 @@ namespace hhg {
 
 constexpr unsigned kFull = 0xffffffffu;
 constexpr double kDblEps = 2.220446049250313080847e-16;  // std::numeric_limits<double>::epsilon()
+constexpr int kMaxStd = 5;  // tabulated steps of the standard schedule per interval
 
-enum Model { DIRAC2D = 0, PIFLUX2D = 1, PIFLUX3D = 2, HONEYCOMB = 3, DIRAC3D = 4 };
-enum FuncKind { F_A = 0, F_COS = 1, F_SIN = 2 };
+// Model variants.  *_SYM / *_X are the same physics with fewer distinct
+// pulse projections (PiFlux-2D with px == py; honeycomb with the field along
+// x, where the bonds 2 and 3 share one projection).
+enum Model {
+    DIRAC2D = 0, PIFLUX2D = 1, PIFLUX3D = 2, HONEYCOMB = 3, DIRAC3D = 4,
+    PIFLUX2D_SYM = 5, HONEYCOMB_X = 6
+};
 
-// Staged functions per model: value of each outside the pulse window
-// (CosineLaser::envelope returns 0 for t <= t_begin or t >= t_end).
+// Number of staged pulse functions per model: A for the Dirac models, (cos,
+// sin) pairs of s A(t) for the lattice models.
 template <int M> struct Traits;
 template <> struct Traits<DIRAC2D> { static constexpr int NF = 1; };
 template <> struct Traits<DIRAC3D> { static constexpr int NF = 1; };
-template <> struct Traits<PIFLUX3D> { static constexpr int NF = 2; };   // cos A, sin A
-template <> struct Traits<PIFLUX2D> { static constexpr int NF = 4; };   // cos/sin(px A), cos/sin(py A)
-template <> struct Traits<HONEYCOMB> { static constexpr int NF = 6; };  // cos/sin(s_j A), j = 0..2
+template <> struct Traits<PIFLUX3D> { static constexpr int NF = 2; };
+template <> struct Traits<PIFLUX2D> { static constexpr int NF = 4; };
+template <> struct Traits<PIFLUX2D_SYM> { static constexpr int NF = 2; };
+template <> struct Traits<HONEYCOMB> { static constexpr int NF = 6; };
+template <> struct Traits<HONEYCOMB_X> { static constexpr int NF = 4; };
 
-// Per-interval record (doubles): [0] t0, [1] t1, [2] center, [3] 1/half-width,
-// [4] A(t_s) and [5, 5 + nf) the staged functions evaluated exactly at the
-// interval's end sample t_s = (i+1) * measure_every + window_begin, then
-// nf blocks of deg + 1 monomial coefficients starting at a 16-byte boundary.
+// Per-interval record (doubles):
+//   [0] t0, [1] t1, [2] center, [3] 1/half-width, [4] A(t_s) and
+//   [5, 5+nf) the staged functions evaluated exactly at the interval's end
+//   sample t_s = (i+1) * measure_every + window_begin        (header, even)
+//   nf * (deg + 1) monomial coefficients                        (poly)
+//   [n_std, pad, ts[kMaxStd], hs[kMaxStd]]                      (schedule)
+//   kMaxStd x 13 x nf exact stage values                        (table)
 __host__ __device__ constexpr int slot_header(int nf) { return (5 + nf + 1) & ~1; }
+__host__ __device__ constexpr int slot_poly(int nf) { return slot_header(nf); }
+__host__ __device__ constexpr int slot_sched(int nf, int deg) {
+    return slot_header(nf) + ((nf * (deg + 1) + 1) & ~1);
+}
+__host__ __device__ constexpr int slot_table(int nf, int deg) {
+    return slot_sched(nf, deg) + 2 + 2 * kMaxStd;
+}
 __host__ __device__ constexpr int slot_doubles(int nf, int deg) {
-    return slot_header(nf) + nf * (deg + 1) + ((nf * (deg + 1)) & 1);
+    return slot_table(nf, deg) + ((kMaxStd * 13 * nf + 1) & ~1);
 }
 // Value of staged function n outside the pulse window: A -> 0, cos -> 1, sin -> 0.
 template <int NF> __host__ __device__ constexpr double outside_value(int n) {
     return (NF > 1 && (n % 2) == 0) ? 1.0 : 0.0;
 }
 
+// Fehlberg 7(8) nodes c_s (E. Fehlberg, NASA TR R-287, 1968).
+__host__ __device__ constexpr double rk_c(int s) {
+    return s == 0 ? 0.0 : s == 1 ? 2.0 / 27.0 : s == 2 ? 1.0 / 9.0 : s == 3 ? 1.0 / 6.0
+         : s == 4 ? 5.0 / 12.0 : s == 5 ? 0.5 : s == 6 ? 5.0 / 6.0 : s == 7 ? 1.0 / 6.0
+         : s == 8 ? 2.0 / 3.0 : s == 9 ? 1.0 / 3.0 : s == 10 ? 1.0 : s == 11 ? 0.0 : 1.0;
+}
+
 // Per-pulse constants, prepared on the host.
 struct PulseDev {
     double amplitude, t_begin, t_end, inv_n_cycles, phase;
     double window_begin, measure_every, dt0;
-    double mp[8];   // model constants already multiplied by the energy scale
-    double s[3];    // staged projections s_j (honeycomb: nn_j . pol; piflux2d: px, py)
+    double mp[8];     // model constants already multiplied by the energy scale
+    double s[3];      // staged projections (lattice models)
     double s0rec[8];  // sample-0 record: A(t_0), staged functions at A(t_0)
     long long coef_off;   // doubles into the staging table
     long long part_off;   // doubles into the partial buffer
@@ -86,8 +126,8 @@ struct KParams {
 };
 
 // ---------------------------------------------------------------------------
-// Pulse (exact, for the sample-time vertices): Laser::laser_function with
-// CosineLaser::envelope (Laser.hpp:32-37, CosineLaser.cpp:22-26).
+// Pulse: Laser::laser_function with CosineLaser::envelope (Laser.hpp:32-37,
+// CosineLaser.cpp:22-26); the continued form drops the window cut.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ double laser_exact(const PulseDev &p, double t) {
     double env = 0.0;
@@ -95,54 +135,83 @@ __device__ __forceinline__ double laser_exact(const PulseDev &p, double t) {
     return p.amplitude * (env * sin(t + p.phase));
 }
 
-// Analytic continuation used for staging (no window cut).
 __device__ __forceinline__ double laser_continued(const PulseDev &p, double t) {
     const double env = 0.5 * (1. - cos(p.inv_n_cycles * (t - p.t_begin)));
     return p.amplitude * (env * sin(t + p.phase));
 }
 
-// ---------------------------------------------------------------------------
-// Staged evaluation: f_n(t) = sum_j c_nj u^j, u = (t - center) * inv_half.
-// ---------------------------------------------------------------------------
-template <int NF, int D, typename R>
-__device__ __forceinline__ void eval_staged(const double *__restrict__ hd, const R *__restrict__ sc,
-                                            double t, double tb, double te, R f[NF]) {
-    const R u = R((t - hd[2]) * hd[3]);
-    const bool inside = (t > tb) && (t < te);
+// Staged functions of a pulse value A.
+template <int M>
+__device__ __forceinline__ void staged_values(const PulseDev &pd, double A, double *v) {
+    constexpr int NF = Traits<M>::NF;
+    if constexpr (NF == 1) {
+        v[0] = A;
+    } else if constexpr (M == PIFLUX3D) {
+        sincos(A, &v[1], &v[0]);
+    } else {
 #pragma unroll
-    for (int n = 0; n < NF; ++n) {
-        const R *c = sc + n * (D + 1);
-        R v = c[D];
-#pragma unroll
-        for (int j = D - 1; j >= 0; --j) v = fma(v, u, c[j]);
-        f[n] = inside ? v : R(outside_value<NF>(n));
+        for (int n = 0; n < NF / 2; ++n) sincos(pd.s[n] * A, &v[2 * n + 1], &v[2 * n]);
     }
 }
 
 // ---------------------------------------------------------------------------
+// Pulse evaluators used inside a step: polynomial (any t) or table (stage s of
+// a standard step).  Both return FP64 values.
+// ---------------------------------------------------------------------------
+template <int NF, int D>
+struct PolyEval {
+    const double *hd;  // interval record
+    double tb, te;
+    __device__ __forceinline__ void operator()(int, double t, double *f) const {
+        const double u = (t - hd[2]) * hd[3];
+        const bool inside = (t > tb) && (t < te);
+        const double *c0 = hd + slot_poly(NF);
+#pragma unroll
+        for (int n = 0; n < NF; ++n) {
+            const double *c = c0 + n * (D + 1);
+            double v = c[D];
+#pragma unroll
+            for (int j = D - 1; j >= 0; --j) v = fma(v, u, c[j]);
+            f[n] = inside ? v : outside_value<NF>(n);
+        }
+    }
+};
+
+template <int NF>
+struct TableEval {
+    const double *tab;  // 13 x NF values of one standard step
+    __device__ __forceinline__ void operator()(int s, double, double *f) const {
+#pragma unroll
+        for (int n = 0; n < NF; ++n) f[n] = tab[s * NF + n];
+    }
+};
+
+// ---------------------------------------------------------------------------
 // Models.  init() reads the k row and the pulse's scaled constants; rhs()
-// evaluates dS/dt from the staged values f; vertex() is the current
-// contribution (weight excluded) from the sample record r = [A(t_s), staged
-// functions evaluated exactly at t_s]; dvec() is d with dS/dt = 2 d x S.
+// evaluates dS/dt from the FP64 pulse values f (k-dependent field terms in
+// FP64, narrowed once to R); vertex() is the current contribution (weight
+// excluded) from the sample record r = [A(t_s), staged functions at t_s];
+// dvec() gives d with dS/dt = 2 d x S (Magnus-4).
 // ---------------------------------------------------------------------------
 template <int M, typename R> struct ModelState;
 
 // gapped 2D Dirac, d = (v (kx - px A), v (ky - py A), mass); dS/dt = 2 d x S.
 // mp: [0] 2v, [1] 2 mass, [2] px, [3] py
 template <typename R> struct ModelState<DIRAC2D, R> {
-    R ax, ay, bx, by, dz;
+    double ax, ay, bx, by;
+    R dz;
     double px, py;
     __device__ __forceinline__ void init(const PulseDev &p, const double *row) {
-        ax = R(p.mp[0] * row[0]);
-        ay = R(p.mp[0] * row[1]);
-        bx = R(p.mp[0] * p.mp[2]);
-        by = R(p.mp[0] * p.mp[3]);
+        ax = p.mp[0] * row[0];
+        ay = p.mp[0] * row[1];
+        bx = p.mp[0] * p.mp[2];
+        by = p.mp[0] * p.mp[3];
         dz = R(p.mp[1]);
         px = p.mp[2];
         py = p.mp[3];
     }
-    __device__ __forceinline__ void rhs(const R *f, const R *S, R *dS) const {
-        const R d0 = ax - bx * f[0], d1 = ay - by * f[0];
+    __device__ __forceinline__ void rhs(const double *f, const R *S, R *dS) const {
+        const R d0 = R(ax - bx * f[0]), d1 = R(ay - by * f[0]);
         dS[0] = d1 * S[2] - dz * S[1];
         dS[1] = dz * S[0] - d0 * S[2];
         dS[2] = d0 * S[1] - d1 * S[0];
@@ -150,28 +219,28 @@ template <typename R> struct ModelState<DIRAC2D, R> {
     __device__ __forceinline__ double vertex(const double *, const double *S) const {
         return px * S[0] + py * S[1];
     }
-    __device__ __forceinline__ void dvec(const R *f, R *d) const {
-        d[0] = R(0.5) * (ax - bx * f[0]);
-        d[1] = R(0.5) * (ay - by * f[0]);
-        d[2] = R(0.5) * dz;
+    __device__ __forceinline__ void dvec(const double *f, double *d) const {
+        d[0] = 0.5 * (ax - bx * f[0]);
+        d[1] = 0.5 * (ay - by * f[0]);
+        d[2] = 0.5 * double(dz);
     }
 };
 
 // Reference PiFlux (PiFlux.cpp:89-94): dS/dt = 4t (cx, cy, cos(kz - A)) x S,
 // cos(kz - A) = cos kz cos A + sin kz sin A.  mp: [0] 4t
 template <typename R> struct ModelState<PIFLUX3D, R> {
-    R m0, m1, pcz, psz;
-    double cz, sz;
+    R m0, m1;
+    double pcz, psz, cz, sz;
     __device__ __forceinline__ void init(const PulseDev &p, const double *row) {
         const double pf = p.mp[0];
         m0 = R(pf * cos(row[0]));
         m1 = R(pf * cos(row[1]));
         sincos(row[2], &sz, &cz);
-        pcz = R(pf * cz);
-        psz = R(pf * sz);
+        pcz = pf * cz;
+        psz = pf * sz;
     }
-    __device__ __forceinline__ void rhs(const R *f, const R *S, R *dS) const {
-        const R m2 = pcz * f[0] + psz * f[1];
+    __device__ __forceinline__ void rhs(const double *f, const R *S, R *dS) const {
+        const R m2 = R(pcz * f[0] + psz * f[1]);
         dS[0] = m1 * S[2] - m2 * S[1];
         dS[1] = m2 * S[0] - m0 * S[2];
         dS[2] = m0 * S[1] - m1 * S[0];
@@ -180,126 +249,127 @@ template <typename R> struct ModelState<PIFLUX3D, R> {
         // sin(k.z - A(t_i)) S_z (PiFlux.cpp:832-838)
         return (sz * r[1] - cz * r[2]) * S[2];
     }
-    __device__ __forceinline__ void dvec(const R *f, R *d) const {
-        d[0] = R(0.5) * m0;
-        d[1] = R(0.5) * m1;
-        d[2] = R(0.5) * (pcz * f[0] + psz * f[1]);
+    __device__ __forceinline__ void dvec(const double *f, double *d) const {
+        d[0] = 0.5 * double(m0);
+        d[1] = 0.5 * double(m1);
+        d[2] = 0.5 * (pcz * f[0] + psz * f[1]);
     }
 };
 
 // 2D pi-flux, d = -2t (cos(kx - px A), cos(ky - py A), 0); dS/dt = 2 d x S.
-// mp: [0] -4t, [2] px, [3] py
-template <typename R> struct ModelState<PIFLUX2D, R> {
-    R pcx, psx, pcy, psy;
-    double cx, sx, cy, sy, px, py;
+// mp: [0] -4t, [2] px, [3] py.  SYM: px == py, one (cos, sin) pair.
+template <typename R, bool SYM> struct PiFlux2DState {
+    static constexpr int Y = SYM ? 0 : 2;
+    double pcx, psx, pcy, psy, cx, sx, cy, sy, px, py;
     __device__ __forceinline__ void init(const PulseDev &p, const double *row) {
         const double pf = p.mp[0];
         sincos(row[0], &sx, &cx);
         sincos(row[1], &sy, &cy);
-        pcx = R(pf * cx);
-        psx = R(pf * sx);
-        pcy = R(pf * cy);
-        psy = R(pf * sy);
+        pcx = pf * cx;
+        psx = pf * sx;
+        pcy = pf * cy;
+        psy = pf * sy;
         px = p.mp[2];
         py = p.mp[3];
     }
-    __device__ __forceinline__ void rhs(const R *f, const R *S, R *dS) const {
-        const R m0 = pcx * f[0] + psx * f[1];
-        const R m1 = pcy * f[2] + psy * f[3];
+    __device__ __forceinline__ void rhs(const double *f, const R *S, R *dS) const {
+        const R m0 = R(pcx * f[0] + psx * f[1]);
+        const R m1 = R(pcy * f[Y] + psy * f[Y + 1]);
         dS[0] = m1 * S[2];
         dS[1] = -(m0 * S[2]);
         dS[2] = m0 * S[1] - m1 * S[0];
     }
     __device__ __forceinline__ double vertex(const double *r, const double *S) const {
         // px sin(kx - px A) S_x + py sin(ky - py A) S_y
-        return px * (sx * r[1] - cx * r[2]) * S[0] + py * (sy * r[3] - cy * r[4]) * S[1];
+        return px * (sx * r[1] - cx * r[2]) * S[0] + py * (sy * r[1 + Y] - cy * r[2 + Y]) * S[1];
     }
-    __device__ __forceinline__ void dvec(const R *f, R *d) const {
-        d[0] = R(0.5) * (pcx * f[0] + psx * f[1]);
-        d[1] = R(0.5) * (pcy * f[2] + psy * f[3]);
-        d[2] = R(0);
+    __device__ __forceinline__ void dvec(const double *f, double *d) const {
+        d[0] = 0.5 * (pcx * f[0] + psx * f[1]);
+        d[1] = 0.5 * (pcy * f[Y] + psy * f[Y + 1]);
+        d[2] = 0.0;
     }
 };
+template <typename R> struct ModelState<PIFLUX2D, R> : PiFlux2DState<R, false> {};
+template <typename R> struct ModelState<PIFLUX2D_SYM, R> : PiFlux2DState<R, true> {};
 
 // Reference Honeycomb (Honeycomb.cpp:131-138) with an optional staggered mass:
 // gamma' = sum_j e^{i nn_j.k} e^{-i s_j A}, s_j = nn_j . pol,
 // dS = (-pf Sz Im g - 2m Sy, -pf Sz Re g + 2m Sx, pf (Sx Im g + Sy Re g)).
-// mp: [0] 2t (pf), [1] 2 mass, [2] px, [3] py
-template <typename R> struct ModelState<HONEYCOMB, R> {
-    R c0, s0, c1, s1, c2, s2;  // cos/sin(nn_j . k)
-    R pf, dm;
-    double px, py;
+// mp: [0] 2t (pf), [1] 2 mass, [2] px, [3] py.  X: bonds 2 and 3 share one
+// projection (field along x), so the staged pairs are those of (s_0, s_1).
+template <typename R, bool X> struct HoneycombState {
+    static constexpr int Q2 = X ? 2 : 4;
+    double c0, s0, c1, s1, c2, s2;  // cos/sin(nn_j . k)
+    R dm;
+    double pf, px, py;
     __device__ __forceinline__ void init(const PulseDev &p, const double *row) {
         const double nny = 0.5 * 1.732050807568877293527446341;
-        double s, c;
-        sincos(row[0], &s, &c);
-        c0 = R(c), s0 = R(s);
-        sincos(-0.5 * row[0] + nny * row[1], &s, &c);
-        c1 = R(c), s1 = R(s);
-        sincos(-0.5 * row[0] - nny * row[1], &s, &c);
-        c2 = R(c), s2 = R(s);
-        pf = R(p.mp[0]);
+        pf = p.mp[0];
+        sincos(row[0], &s0, &c0);
+        sincos(-0.5 * row[0] + nny * row[1], &s1, &c1);
+        sincos(-0.5 * row[0] - nny * row[1], &s2, &c2);
         dm = R(p.mp[1]);
         px = p.mp[2];
         py = p.mp[3];
     }
-    __device__ __forceinline__ void gamma(const R *f, R &gre, R &gim) const {
+    __device__ __forceinline__ void gamma(const double *f, double &gre, double &gim) const {
         // e^{i(a - b)} = (ca cb + sa sb) + i (sa cb - ca sb)
-        gre = (c0 * f[0] + s0 * f[1]) + (c1 * f[2] + s1 * f[3]) + (c2 * f[4] + s2 * f[5]);
-        gim = (s0 * f[0] - c0 * f[1]) + (s1 * f[2] - c1 * f[3]) + (s2 * f[4] - c2 * f[5]);
+        gre = (c0 * f[0] + s0 * f[1]) + (c1 * f[2] + s1 * f[3]) + (c2 * f[Q2] + s2 * f[Q2 + 1]);
+        gim = (s0 * f[0] - c0 * f[1]) + (s1 * f[2] - c1 * f[3]) + (s2 * f[Q2] - c2 * f[Q2 + 1]);
     }
-    __device__ __forceinline__ void rhs(const R *f, const R *S, R *dS) const {
-        R gre, gim;
+    __device__ __forceinline__ void rhs(const double *f, const R *S, R *dS) const {
+        double gre, gim;
         gamma(f, gre, gim);
-        gre *= pf;
-        gim *= pf;
-        dS[0] = -(S[2] * gim) - dm * S[1];
-        dS[1] = -(S[2] * gre) + dm * S[0];
-        dS[2] = S[0] * gim + S[1] * gre;
+        const R gr = R(pf * gre), gi = R(pf * gim);
+        dS[0] = -(S[2] * gi) - dm * S[1];
+        dS[1] = -(S[2] * gr) + dm * S[0];
+        dS[2] = S[0] * gi + S[1] * gr;
     }
     __device__ __forceinline__ double vertex(const double *r, const double *S) const {
         // shifted_grad_gamma and the projection (Honeycomb.cpp:49-61, 273-279, 328-330)
         const double nny = 0.5 * 1.732050807568877293527446341;
-        const double e0r = double(c0) * r[1] + double(s0) * r[2], e0i = double(s0) * r[1] - double(c0) * r[2];
-        const double e1r = double(c1) * r[3] + double(s1) * r[4], e1i = double(s1) * r[3] - double(c1) * r[4];
-        const double e2r = double(c2) * r[5] + double(s2) * r[6], e2i = double(s2) * r[5] - double(c2) * r[6];
+        const double e0r = c0 * r[1] + s0 * r[2], e0i = s0 * r[1] - c0 * r[2];
+        const double e1r = c1 * r[3] + s1 * r[4], e1i = s1 * r[3] - c1 * r[4];
+        const double e2r = c2 * r[1 + Q2] + s2 * r[2 + Q2], e2i = s2 * r[1 + Q2] - c2 * r[2 + Q2];
         const double g0r = e0r - 0.5 * e1r - 0.5 * e2r, g0i = e0i - 0.5 * e1i - 0.5 * e2i;
         const double g1r = nny * e1r - nny * e2r, g1i = nny * e1i - nny * e2i;
         const double bx = g0r * S[0] + g0i * S[1];
         const double by = g1r * S[0] + g1i * S[1];
         return bx * px + by * py;
     }
-    __device__ __forceinline__ void dvec(const R *f, R *d) const {
+    __device__ __forceinline__ void dvec(const double *f, double *d) const {
         // d = t (Re g', -Im g', mass) = 0.5 (pf Re g', -pf Im g', 2 mass)
-        R gre, gim;
+        double gre, gim;
         gamma(f, gre, gim);
-        d[0] = R(0.5) * pf * gre;
-        d[1] = R(-0.5) * pf * gim;
-        d[2] = R(0.5) * dm;
+        d[0] = 0.5 * pf * gre;
+        d[1] = -0.5 * pf * gim;
+        d[2] = 0.5 * double(dm);
     }
 };
+template <typename R> struct ModelState<HONEYCOMB, R> : HoneycombState<R, false> {};
+template <typename R> struct ModelState<HONEYCOMB_X, R> : HoneycombState<R, true> {};
 
 // Reference DiracSystem sigma RHS (DiracSystem.cpp:144-153); row = (k_z, kappa, |k|).
 template <typename R> struct ModelState<DIRAC3D, R> {
-    R ax, az, mk2;
+    double ax, az, mk2;
     __device__ __forceinline__ void init(const PulseDev &, const double *row) {
-        ax = R(2.0 * row[1] / row[2]);
-        az = R(2.0 * row[0] / row[2]);
-        mk2 = R(2.0 * row[2]);
+        ax = 2.0 * row[1] / row[2];
+        az = 2.0 * row[0] / row[2];
+        mk2 = 2.0 * row[2];
     }
-    __device__ __forceinline__ void rhs(const R *f, const R *S, R *dS) const {
-        const R mx = f[0] * ax;
-        const R mz = mk2 - f[0] * az;
+    __device__ __forceinline__ void rhs(const double *f, const R *S, R *dS) const {
+        const R mx = R(f[0] * ax);
+        const R mz = R(mk2 - f[0] * az);
         dS[0] = mz * S[1];
         dS[1] = mx * S[2] - S[0] * mz;
         dS[2] = -mx * S[1];
     }
     __device__ __forceinline__ double vertex(const double *, const double *S) const { return S[2]; }
-    __device__ __forceinline__ void dvec(const R *f, R *d) const {
+    __device__ __forceinline__ void dvec(const double *f, double *d) const {
         // G = [[0, mz, 0], [-mz, 0, mx], [0, -mx, 0]] = [g]_x, g = (-mx, 0, -mz) = 2 d
-        d[0] = R(-0.5) * (f[0] * ax);
-        d[1] = R(0);
-        d[2] = R(-0.5) * (mk2 - f[0] * az);
+        d[0] = -0.5 * (f[0] * ax);
+        d[1] = 0.0;
+        d[2] = -0.5 * (mk2 - f[0] * az);
     }
 };
 
@@ -307,59 +377,50 @@ template <typename R> struct ModelState<DIRAC3D, R> {
 // One attempted Fehlberg 7(8) step (E. Fehlberg, NASA TR R-287, 1968):
 // 13 stages, the 8th-order solution propagated, error = b8 - b7 =
 // 41/840 (k12 + k13 - k1 - k11).  Stage sums are written out with the
-// tableau's nonzero entries only.  R is the right-hand-side precision; the
-// state, the solution increment and the error estimate are FP64.
+// tableau's nonzero entries only.  R is the stage precision; the state, the
+// solution increment and the error estimate are FP64.
 // ---------------------------------------------------------------------------
-template <int M, int NF, int D, typename R>
-__device__ __forceinline__ void rkf78_attempt(const ModelState<M, R> &ms, const double *hd,
-                                              const R *sc, double tb, double te, double t,
-                                              double h, const double *x, double *xn, double *e,
-                                              double *k0d) {
+template <int M, int NF, typename R, class Eval>
+__device__ __forceinline__ void rkf78_attempt(const ModelState<M, R> &ms, const Eval &ev,
+                                              double t, double h, const double *x, double *xn,
+                                              double *e, double *k0d) {
     R k[13][3];
-    R f[NF];
+    double f[NF];
     const R xr[3] = {R(x[0]), R(x[1]), R(x[2])};
     const R hr = R(h);
-    eval_staged<NF, D, R>(hd, sc, t, tb, te, f);
+    ev(0, t, f);
     ms.rhs(f, xr, k[0]);
-#define HHG_STAGE(s, cs, EXPR)                                                        \
-    {                                                                                 \
-        R xt[3];                                                                      \
-        _Pragma("unroll") for (int i = 0; i < 3; ++i) xt[i] = xr[i] + hr * (EXPR);    \
-        eval_staged<NF, D, R>(hd, sc, t + (cs) * h, tb, te, f);                       \
-        ms.rhs(f, xt, k[s]);                                                          \
+#define HHG_STAGE(s, EXPR)                                                          \
+    {                                                                               \
+        R xt[3];                                                                    \
+        _Pragma("unroll") for (int i = 0; i < 3; ++i) xt[i] = xr[i] + hr * (EXPR);  \
+        ev(s, t + rk_c(s) * h, f);                                                  \
+        ms.rhs(f, xt, k[s]);                                                        \
     }
-    HHG_STAGE(1, 2.0 / 27.0, R(2.0 / 27.0) * k[0][i])
-    HHG_STAGE(2, 1.0 / 9.0, R(1.0 / 36.0) * k[0][i] + R(1.0 / 12.0) * k[1][i])
-    HHG_STAGE(3, 1.0 / 6.0, R(1.0 / 24.0) * k[0][i] + R(1.0 / 8.0) * k[2][i])
-    HHG_STAGE(4, 5.0 / 12.0,
-              R(5.0 / 12.0) * k[0][i] + R(-25.0 / 16.0) * k[2][i] + R(25.0 / 16.0) * k[3][i])
-    HHG_STAGE(5, 0.5, R(1.0 / 20.0) * k[0][i] + R(1.0 / 4.0) * k[3][i] + R(1.0 / 5.0) * k[4][i])
-    HHG_STAGE(6, 5.0 / 6.0,
-              R(-25.0 / 108.0) * k[0][i] + R(125.0 / 108.0) * k[3][i] +
-                  R(-65.0 / 27.0) * k[4][i] + R(125.0 / 54.0) * k[5][i])
-    HHG_STAGE(7, 1.0 / 6.0,
-              R(31.0 / 300.0) * k[0][i] + R(61.0 / 225.0) * k[4][i] + R(-2.0 / 9.0) * k[5][i] +
-                  R(13.0 / 900.0) * k[6][i])
-    HHG_STAGE(8, 2.0 / 3.0,
-              R(2.0) * k[0][i] + R(-53.0 / 6.0) * k[3][i] + R(704.0 / 45.0) * k[4][i] +
-                  R(-107.0 / 9.0) * k[5][i] + R(67.0 / 90.0) * k[6][i] + R(3.0) * k[7][i])
-    HHG_STAGE(9, 1.0 / 3.0,
-              R(-91.0 / 108.0) * k[0][i] + R(23.0 / 108.0) * k[3][i] +
-                  R(-976.0 / 135.0) * k[4][i] + R(311.0 / 54.0) * k[5][i] +
-                  R(-19.0 / 60.0) * k[6][i] + R(17.0 / 6.0) * k[7][i] + R(-1.0 / 12.0) * k[8][i])
-    HHG_STAGE(10, 1.0,
-              R(2383.0 / 4100.0) * k[0][i] + R(-341.0 / 164.0) * k[3][i] +
-                  R(4496.0 / 1025.0) * k[4][i] + R(-301.0 / 82.0) * k[5][i] +
-                  R(2133.0 / 4100.0) * k[6][i] + R(45.0 / 82.0) * k[7][i] +
-                  R(45.0 / 164.0) * k[8][i] + R(18.0 / 41.0) * k[9][i])
-    HHG_STAGE(11, 0.0,
-              R(3.0 / 205.0) * k[0][i] + R(-6.0 / 41.0) * k[5][i] + R(-3.0 / 205.0) * k[6][i] +
-                  R(-3.0 / 41.0) * k[7][i] + R(3.0 / 41.0) * k[8][i] + R(6.0 / 41.0) * k[9][i])
-    HHG_STAGE(12, 1.0,
-              R(-1777.0 / 4100.0) * k[0][i] + R(-341.0 / 164.0) * k[3][i] +
-                  R(4496.0 / 1025.0) * k[4][i] + R(-289.0 / 82.0) * k[5][i] +
-                  R(2193.0 / 4100.0) * k[6][i] + R(51.0 / 82.0) * k[7][i] +
-                  R(33.0 / 164.0) * k[8][i] + R(12.0 / 41.0) * k[9][i] + k[11][i])
+    HHG_STAGE(1, R(2.0 / 27.0) * k[0][i])
+    HHG_STAGE(2, R(1.0 / 36.0) * k[0][i] + R(1.0 / 12.0) * k[1][i])
+    HHG_STAGE(3, R(1.0 / 24.0) * k[0][i] + R(1.0 / 8.0) * k[2][i])
+    HHG_STAGE(4, R(5.0 / 12.0) * k[0][i] + R(-25.0 / 16.0) * k[2][i] + R(25.0 / 16.0) * k[3][i])
+    HHG_STAGE(5, R(1.0 / 20.0) * k[0][i] + R(1.0 / 4.0) * k[3][i] + R(1.0 / 5.0) * k[4][i])
+    HHG_STAGE(6, R(-25.0 / 108.0) * k[0][i] + R(125.0 / 108.0) * k[3][i] +
+                     R(-65.0 / 27.0) * k[4][i] + R(125.0 / 54.0) * k[5][i])
+    HHG_STAGE(7, R(31.0 / 300.0) * k[0][i] + R(61.0 / 225.0) * k[4][i] + R(-2.0 / 9.0) * k[5][i] +
+                     R(13.0 / 900.0) * k[6][i])
+    HHG_STAGE(8, R(2.0) * k[0][i] + R(-53.0 / 6.0) * k[3][i] + R(704.0 / 45.0) * k[4][i] +
+                     R(-107.0 / 9.0) * k[5][i] + R(67.0 / 90.0) * k[6][i] + R(3.0) * k[7][i])
+    HHG_STAGE(9, R(-91.0 / 108.0) * k[0][i] + R(23.0 / 108.0) * k[3][i] +
+                     R(-976.0 / 135.0) * k[4][i] + R(311.0 / 54.0) * k[5][i] +
+                     R(-19.0 / 60.0) * k[6][i] + R(17.0 / 6.0) * k[7][i] + R(-1.0 / 12.0) * k[8][i])
+    HHG_STAGE(10, R(2383.0 / 4100.0) * k[0][i] + R(-341.0 / 164.0) * k[3][i] +
+                      R(4496.0 / 1025.0) * k[4][i] + R(-301.0 / 82.0) * k[5][i] +
+                      R(2133.0 / 4100.0) * k[6][i] + R(45.0 / 82.0) * k[7][i] +
+                      R(45.0 / 164.0) * k[8][i] + R(18.0 / 41.0) * k[9][i])
+    HHG_STAGE(11, R(3.0 / 205.0) * k[0][i] + R(-6.0 / 41.0) * k[5][i] + R(-3.0 / 205.0) * k[6][i] +
+                      R(-3.0 / 41.0) * k[7][i] + R(3.0 / 41.0) * k[8][i] + R(6.0 / 41.0) * k[9][i])
+    HHG_STAGE(12, R(-1777.0 / 4100.0) * k[0][i] + R(-341.0 / 164.0) * k[3][i] +
+                      R(4496.0 / 1025.0) * k[4][i] + R(-289.0 / 82.0) * k[5][i] +
+                      R(2193.0 / 4100.0) * k[6][i] + R(51.0 / 82.0) * k[7][i] +
+                      R(33.0 / 164.0) * k[8][i] + R(12.0 / 41.0) * k[9][i] + k[11][i])
 #undef HHG_STAGE
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
@@ -405,6 +466,40 @@ __device__ __forceinline__ void rotate(const double *w, double *S) {
     S[2] += sa * wx2 + ca * ww2;
 }
 
+// Step-size control after an attempt (controlled_runge_kutta with the
+// default error checker and step adjuster).  Returns true if accepted and
+// updates dt.  err < 5^-8 takes the host-computed growth constant;
+// FAST_POW evaluates the power of the growth/shrink factor in FP32.
+template <bool FAST_POW>
+__device__ __forceinline__ bool control(const KParams &P, const double *S, const double *e,
+                                        const double *k0, double &dt) {
+    double den[3];
+    bool tiny = true;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        den[c] = P.abs_tol + P.rel_tol * (fabs(S[c]) + dt * fabs(k0[c]));
+        tiny = tiny && (fabs(e[c]) < P.err_floor * den[c]);
+    }
+    if (tiny) {
+        dt *= P.grow_max;
+        return true;
+    }
+    double err = 0.0;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) err = fmax(err, fabs(e[c]) / den[c]);
+    if (err > 1.0) {
+        const double f = FAST_POW ? 0.9 * double(__powf(float(err), -1.0f / 6.0f))
+                                  : 0.9 * pow(err, -1.0 / 6.0);
+        dt *= fmax(f, 0.2);
+        return false;
+    }
+    if (err < 0.5) {
+        const double ee = fmax(err, P.err_floor);
+        dt *= FAST_POW ? 0.9 * double(__powf(float(ee), -0.125f)) : 0.9 * pow(ee, -1.0 / 8.0);
+    }
+    return true;
+}
+
 // ---------------------------------------------------------------------------
 // Persistent, work-stealing integration + BZ-sum kernel.
 // STEPPER 0: controlled RKF78 with the reference's integrate_adaptive
@@ -417,22 +512,20 @@ __device__ __forceinline__ void rotate(const double *w, double *S) {
 // PROPOSER 0: every interval restarts at dt0 = measure_every/n_subdivisions
 //   (the reference); 1: an interval starts from the controller's last
 //   proposal of the previous interval.
+// The mixed-precision variant (R = float) evaluates the growth/shrink factor's
+// power in FP32 (the error norm, the comparison and dt stay FP64).
 // ---------------------------------------------------------------------------
 template <int M, int D, typename R, int STEPPER, int PROPOSER>
-__global__ void __launch_bounds__(128) bz_integrate_kernel(const KParams P) {
+__global__ void __launch_bounds__(128, 3) bz_integrate_kernel(const KParams P) {
     constexpr int NF = Traits<M>::NF;
     constexpr int SLOT = slot_doubles(NF, D);
-    constexpr int HDR = slot_header(NF);
+    constexpr int SCHED = slot_sched(NF, D);
+    constexpr int TAB = slot_table(NF, D);
     constexpr bool kNarrow = sizeof(R) != sizeof(double);
-    constexpr int RCOEF = kNarrow ? NF * (D + 1) : 1;
     __shared__ __align__(16) double stage_raw[4][SLOT];
-    __shared__ __align__(16) R stage_r[4][RCOEF];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
     double *slot = stage_raw[wib];
-    const R *sc;
-    if constexpr (kNarrow) sc = stage_r[wib];
-    else sc = (const R *)(slot + HDR);
 
     unsigned long long my_attempts = 0, my_rejects = 0;
     for (;;) {
@@ -469,17 +562,14 @@ __global__ void __launch_bounds__(128) bz_integrate_kernel(const KParams P) {
                 if (i > 0) {
                     // stage interval i-1 into this warp's shared slot
                     __syncwarp();
-                    const double *src = coef + (size_t)(i - 1) * SLOT;
-                    for (int c = lane; c < SLOT; c += 32) {
-                        const double v = __ldg(src + c);
-                        slot[c] = v;
-                        if constexpr (kNarrow) {
-                            if (c >= HDR && c - HDR < RCOEF) stage_r[wib][c - HDR] = R(v);
-                        }
-                    }
+                    const double2 *src =
+                        reinterpret_cast<const double2 *>(coef + (size_t)(i - 1) * SLOT);
+                    double2 *dst = reinterpret_cast<double2 *>(slot);
+                    for (int c = lane; c < SLOT / 2; c += 32) dst[c] = __ldg(src + c);
                     __syncwarp();
                     rec = slot + 4;
                     const double t0 = slot[0], t1 = slot[1];
+                    const PolyEval<NF, D> poly{slot, tb, te};
                     if constexpr (STEPPER == 1) {
                         if (!dead) {
                             const int ns = P.magnus_substeps;
@@ -488,44 +578,50 @@ __global__ void __launch_bounds__(128) bz_integrate_kernel(const KParams P) {
                             const double q3 = 0.57735026918962576451 * hs * hs;
                             for (int s = 0; s < ns; ++s) {
                                 const double ts = t0 + s * hs;
-                                R f[NF], d1[3], d2[3];
-                                eval_staged<NF, D, R>(slot, sc, ts + g * hs, tb, te, f);
+                                double f[NF], d1[3], d2[3];
+                                poly(0, ts + g * hs, f);
                                 ms.dvec(f, d1);
-                                eval_staged<NF, D, R>(slot, sc, ts + (1.0 - g) * hs, tb, te, f);
+                                poly(0, ts + (1.0 - g) * hs, f);
                                 ms.dvec(f, d2);
                                 double wv[3];
-                                wv[0] = hs * double(d1[0] + d2[0]) + q3 * double(d2[1] * d1[2] - d2[2] * d1[1]);
-                                wv[1] = hs * double(d1[1] + d2[1]) + q3 * double(d2[2] * d1[0] - d2[0] * d1[2]);
-                                wv[2] = hs * double(d1[2] + d2[2]) + q3 * double(d2[0] * d1[1] - d2[1] * d1[0]);
+                                wv[0] = hs * (d1[0] + d2[0]) + q3 * (d2[1] * d1[2] - d2[2] * d1[1]);
+                                wv[1] = hs * (d1[1] + d2[1]) + q3 * (d2[2] * d1[0] - d2[0] * d1[2]);
+                                wv[2] = hs * (d1[2] + d2[2]) + q3 * (d2[0] * d1[1] - d2[1] * d1[0]);
                                 rotate(wv, S);
                             }
                             my_attempts += ns;
                         }
                     } else {
+                        const int n_std = (PROPOSER == 0) ? (int)slot[SCHED] : 0;
                         double t = t0;
                         double dt = (PROPOSER == 1) ? carry_dt : dt0;
                         bool active = !dead;
-                        int fails = 0, attempts = 0;
+                        int fails = 0, attempts = 0, wa = 0;
                         while (__any_sync(kFull, active)) {
+                            if (active && (t + dt) - t1 > kDblEps) dt = t1 - t;
+                            // every active lane on the standard schedule -> table path
+                            const bool on = !active || (wa < n_std && t == slot[SCHED + 2 + wa] &&
+                                                        dt == slot[SCHED + 2 + kMaxStd + wa]);
+                            const bool table = (PROPOSER == 0) && __all_sync(kFull, on);
                             if (active) {
-                                if ((t + dt) - t1 > kDblEps) dt = t1 - t;
                                 double xn[3], e[3], k0[3];
-                                rkf78_attempt<M, NF, D, R>(ms, slot, sc, tb, te, t, dt, S, xn, e, k0);
+                                if (table) {
+                                    const TableEval<NF> tev{slot + TAB + wa * 13 * NF};
+                                    rkf78_attempt<M, NF, R>(ms, tev, t, dt, S, xn, e, k0);
+                                } else {
+                                    rkf78_attempt<M, NF, R>(ms, poly, t, dt, S, xn, e, k0);
+                                }
                                 ++attempts;
-                                double den[3];
-                                bool tiny = true;
-#pragma unroll
-                                for (int c = 0; c < 3; ++c) {
-                                    den[c] = P.abs_tol + P.rel_tol * (fabs(S[c]) + dt * fabs(k0[c]));
-                                    tiny = tiny && (fabs(e[c]) < P.err_floor * den[c]);
-                                }
-                                double err = 0.0;
-                                if (!tiny) {
-#pragma unroll
-                                    for (int c = 0; c < 3; ++c) err = fmax(err, fabs(e[c]) / den[c]);
-                                }
-                                if (err > 1.0) {
-                                    dt *= fmax(0.9 * pow(err, -1.0 / 6.0), 0.2);
+                                const double dt_used = dt;
+                                if (control<kNarrow>(P, S, e, k0, dt)) {
+                                    t += dt_used;
+                                    S[0] = xn[0];
+                                    S[1] = xn[1];
+                                    S[2] = xn[2];
+                                    fails = 0;
+                                    if (!(t1 - t > kDblEps)) active = false;
+                                    if (PROPOSER == 1) carry_dt = dt;
+                                } else {
                                     ++my_rejects;
                                     if (++fails >= P.max_failed) {
                                         active = false;
@@ -533,16 +629,6 @@ __global__ void __launch_bounds__(128) bz_integrate_kernel(const KParams P) {
                                         atomicAdd(P.counters + 3, 1ull);
                                         atomicMax(P.status, 2);
                                     }
-                                } else {
-                                    t += dt;
-                                    S[0] = xn[0];
-                                    S[1] = xn[1];
-                                    S[2] = xn[2];
-                                    fails = 0;
-                                    if (err < 0.5)
-                                        dt *= tiny ? P.grow_max : 0.9 * pow(fmax(err, P.err_floor), -1.0 / 8.0);
-                                    if (!(t1 - t > kDblEps)) active = false;
-                                    if (PROPOSER == 1) carry_dt = dt;
                                 }
                                 if (active && attempts >= P.max_attempts) {
                                     active = false;
@@ -551,6 +637,7 @@ __global__ void __launch_bounds__(128) bz_integrate_kernel(const KParams P) {
                                     atomicMax(P.status, 2);
                                 }
                             }
+                            ++wa;
                         }
                         my_attempts += attempts;
                     }
@@ -588,31 +675,21 @@ __global__ void __launch_bounds__(128) bz_integrate_kernel(const KParams P) {
 }
 
 // ---------------------------------------------------------------------------
-// Staging: per (pulse, interval) Chebyshev interpolants of the model's staged
-// functions at D+1 first-kind nodes, converted to monomials in u, plus the
-// exact sample record at the interval's end sample.
+// Staging: per (pulse, interval) the exact end-sample record, Chebyshev
+// interpolants of the staged functions at D+1 first-kind nodes (monomials in
+// u), and the standard schedule with its exact stage values.
 // ---------------------------------------------------------------------------
-template <int M>
-__device__ __forceinline__ void staged_values(const PulseDev &pd, double A, double *v) {
-    constexpr int NF = Traits<M>::NF;
-    if constexpr (NF == 1) {
-        v[0] = A;
-    } else if constexpr (M == PIFLUX3D) {
-        sincos(A, &v[1], &v[0]);
-    } else {
-#pragma unroll
-        for (int n = 0; n < NF / 2; ++n) sincos(pd.s[n] * A, &v[2 * n + 1], &v[2 * n]);
-    }
-}
-
 template <int M, int D>
 __global__ void stage_pulses_kernel(const PulseDev *__restrict__ pulses, int n_pulses,
                                     const double *__restrict__ tgrid,
                                     const long long *__restrict__ interval_off,
-                                    double *__restrict__ coef, long long total_intervals) {
+                                    double *__restrict__ coef, long long total_intervals,
+                                    double grow_max) {
     constexpr int NF = Traits<M>::NF;
     constexpr int SLOT = slot_doubles(NF, D);
     constexpr int HDR = slot_header(NF);
+    constexpr int SCHED = slot_sched(NF, D);
+    constexpr int TAB = slot_table(NF, D);
     constexpr int NN = D + 1;
     const long long gid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (gid >= total_intervals) return;
@@ -624,27 +701,24 @@ __global__ void stage_pulses_kernel(const PulseDev *__restrict__ pulses, int n_p
     const int p = lo;
     const int i = (int)(gid - interval_off[p]);
     const PulseDev pd = pulses[p];
-    // tgrid holds n_meas + 1 accumulated interval ends per pulse, laid out at
-    // interval_off[p] + p
+    // tgrid holds n_meas + 1 accumulated interval ends per pulse, at interval_off[p] + p
     const double t0 = tgrid[interval_off[p] + p + i];
     const double t1 = tgrid[interval_off[p] + p + i + 1];
     const double ctr = 0.5 * (t0 + t1);
     const double half = 0.5 * (t1 - t0);
     double *out = coef + pd.coef_off + (long long)i * SLOT;
+    for (int c = 0; c < SLOT; ++c) out[c] = 0.0;
     out[0] = t0;
     out[1] = t1;
     out[2] = ctr;
     out[3] = 1.0 / half;
     // exact sample record at t_s = (i + 1) * measure_every + window_begin
-    const double ts = (i + 1) * pd.measure_every + pd.window_begin;
-    double env = 0.0;
-    if (!(ts <= pd.t_begin || ts >= pd.t_end)) env = 0.5 * (1. - cos(pd.inv_n_cycles * (ts - pd.t_begin)));
-    const double As = pd.amplitude * (env * sin(ts + pd.phase));
+    const double As = laser_exact(pd, (i + 1) * pd.measure_every + pd.window_begin);
     out[4] = As;
     double sv[NF];
     staged_values<M>(pd, As, sv);
     for (int n = 0; n < NF; ++n) out[5 + n] = sv[n];
-    for (int c = 5 + NF; c < HDR; ++c) out[c] = 0.0;
+    // Chebyshev interpolants of the continued functions
     double fv[NF][NN];
     for (int k = 0; k < NN; ++k) {
         const double xk = cospi((k + 0.5) / NN);
@@ -677,14 +751,31 @@ __global__ void stage_pulses_kernel(const PulseDev *__restrict__ pulses, int n_p
         }
         for (int j = 0; j < NN; ++j) out[HDR + n * NN + j] = m[j];
     }
-    for (int c = HDR + NF * NN; c < SLOT; ++c) out[c] = 0.0;
+    // standard schedule: dt0, dt0 g, dt0 g^2, ... clipped to land on t1,
+    // with exactly the lanes' arithmetic
+    double t = t0, h = pd.dt0;
+    int n_std = 0;
+    while (n_std < kMaxStd && t1 - t > kDblEps) {
+        if ((t + h) - t1 > kDblEps) h = t1 - t;
+        out[SCHED + 2 + n_std] = t;
+        out[SCHED + 2 + kMaxStd + n_std] = h;
+        for (int s = 0; s < 13; ++s) {
+            double v[NF];
+            staged_values<M>(pd, laser_exact(pd, t + rk_c(s) * h), v);
+            for (int n = 0; n < NF; ++n) out[TAB + (n_std * 13 + s) * NF + n] = v[n];
+        }
+        ++n_std;
+        t += h;
+        h *= grow_max;
+    }
+    out[SCHED] = (double)n_std;
 }
 
 // j[p][i] = sum over the pulse's items (in item order) of the partial rows,
 // with Neumaier compensation.
 static __global__ void reduce_partials_kernel(const PulseDev *__restrict__ pulses, int n_pulses,
-                                       const double *__restrict__ part, double *__restrict__ j,
-                                       long long total_samples) {
+                                              const double *__restrict__ part,
+                                              double *__restrict__ j, long long total_samples) {
     const long long gid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (gid >= total_samples) return;
     int lo = 0, hi = n_pulses;
@@ -708,7 +799,8 @@ static __global__ void reduce_partials_kernel(const PulseDev *__restrict__ pulse
 }
 
 // Zero-padded copy for the r2c FFT (hhg.cpp:280-282).
-static __global__ void pad_kernel(const double *__restrict__ j, int n, double *__restrict__ x, int n_in) {
+static __global__ void pad_kernel(const double *__restrict__ j, int n, double *__restrict__ x,
+                                  int n_in) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n_in) x[i] = i < n ? j[i] : 0.0;
 }

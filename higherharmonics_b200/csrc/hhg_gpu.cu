@@ -382,13 +382,23 @@ hhg_status check_pulse(hhg_ctx *ctx, const hhg_pulse_desc &p) {
     return HHG_OK;
 }
 
+// Internal kernel model (hhg::Model): the ABI kind, or a variant with fewer
+// distinct pulse projections when the polarisation allows it.
+int kernel_model(const hhg_system_desc &s) {
+    if (s.kind == HHG_SYS_PIFLUX2D && s.pol_x == s.pol_y) return hhg::PIFLUX2D_SYM;
+    if (s.kind == HHG_SYS_HONEYCOMB && s.pol_y == 0.0) return hhg::HONEYCOMB_X;
+    return s.kind;
+}
+
 int model_nf(int m) {
     switch (m) {
-    case HHG_SYS_DIRAC2D: return 1;
-    case HHG_SYS_DIRAC3D: return 1;
-    case HHG_SYS_PIFLUX3D: return 2;
-    case HHG_SYS_PIFLUX2D: return 4;
-    case HHG_SYS_HONEYCOMB: return 6;
+    case hhg::DIRAC2D: return 1;
+    case hhg::DIRAC3D: return 1;
+    case hhg::PIFLUX3D: return 2;
+    case hhg::PIFLUX2D: return 4;
+    case hhg::HONEYCOMB: return 6;
+    case hhg::PIFLUX2D_SYM: return 2;
+    case hhg::HONEYCOMB_X: return 4;
     }
     return 0;
 }
@@ -447,6 +457,8 @@ hhg_status launch_variant(const hhg_plan *pl, hhg::LaunchReq &r) {
     case HHG_SYS_PIFLUX3D: e = hhg::launch_piflux3d(r); break;
     case HHG_SYS_HONEYCOMB: e = hhg::launch_honeycomb(r); break;
     case HHG_SYS_DIRAC3D: e = hhg::launch_dirac3d(r); break;
+    case hhg::PIFLUX2D_SYM: e = hhg::launch_piflux2d_sym(r); break;
+    case hhg::HONEYCOMB_X: e = hhg::launch_honeycomb_x(r); break;
     }
     if (e != cudaSuccess)
         return set_err(pl->ctx, HHG_CUDA_ERROR, std::string("integration launch: ") + cudaGetErrorString(e));
@@ -461,6 +473,8 @@ hhg_status stage_variant(const hhg_plan *pl, hhg::StageReq &s) {
     case HHG_SYS_PIFLUX3D: e = hhg::stage_piflux3d(s); break;
     case HHG_SYS_HONEYCOMB: e = hhg::stage_honeycomb(s); break;
     case HHG_SYS_DIRAC3D: e = hhg::stage_dirac3d(s); break;
+    case hhg::PIFLUX2D_SYM: e = hhg::stage_piflux2d_sym(s); break;
+    case hhg::HONEYCOMB_X: e = hhg::stage_honeycomb_x(s); break;
     }
     if (e != cudaSuccess)
         return set_err(pl->ctx, HHG_CUDA_ERROR, std::string("staging launch: ") + cudaGetErrorString(e));
@@ -575,10 +589,10 @@ hhg_status hhg_plan_create(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_p
     HHG_CUDA(ctx, cudaSetDevice(ctx->device));
     hhg_plan *pl = new hhg_plan();
     pl->ctx = ctx;
-    pl->model = sys->kind;
+    pl->model = kernel_model(*sys);
     pl->opts = o;
     pl->n_pulses = n_pulses;
-    const int nf = model_nf(sys->kind);
+    const int nf = model_nf(pl->model);
 
     // k table
     pl->n_k = grid_count(*grid);
@@ -588,15 +602,26 @@ hhg_status hhg_plan_create(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_p
     // per-pulse records, staged projections and degree
     const double nny = 0.5 * kSqrt3;
     double proj[3] = {0, 0, 0};
-    if (sys->kind == HHG_SYS_PIFLUX2D) {
+    switch (pl->model) {
+    case hhg::PIFLUX2D:
         proj[0] = sys->pol_x;
         proj[1] = sys->pol_y;
-    } else if (sys->kind == HHG_SYS_HONEYCOMB) {
+        break;
+    case hhg::PIFLUX2D_SYM:
+        proj[0] = sys->pol_x;
+        break;
+    case hhg::HONEYCOMB:
         proj[0] = 1.0 * sys->pol_x + 0.0 * sys->pol_y;
         proj[1] = -0.5 * sys->pol_x + nny * sys->pol_y;
         proj[2] = -0.5 * sys->pol_x - nny * sys->pol_y;
-    } else if (sys->kind == HHG_SYS_PIFLUX3D) {
+        break;
+    case hhg::HONEYCOMB_X:
+        proj[0] = sys->pol_x;
+        proj[1] = -0.5 * sys->pol_x;
+        break;
+    case hhg::PIFLUX3D:
         proj[0] = 1.0;
+        break;
     }
     int degree = 5;
     for (int p = 0; p < n_pulses; ++p) {
@@ -681,7 +706,7 @@ hhg_status hhg_plan_create(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_p
         const double A0 = d.amplitude * (env * sin(t0s + d.phase));
         d.s0rec[0] = A0;
         if (nf == 1) d.s0rec[1] = A0;
-        else if (sys->kind == HHG_SYS_PIFLUX3D) {
+        else if (pl->model == hhg::PIFLUX3D) {
             d.s0rec[1] = cos(A0);
             d.s0rec[2] = sin(A0);
         } else
@@ -736,7 +761,8 @@ hhg_status hhg_plan_create(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_p
     if ((e = cudaMemcpyAsync(pl->d_pulses, pl->pulses.data(), n_pulses * sizeof(PulseDev), cudaMemcpyHostToDevice, s)) != cudaSuccess) return fail("upload pulses", e);
     if ((e = cudaMemcpyAsync(pl->d_tgrid, tgrid.data(), tgrid.size() * sizeof(double), cudaMemcpyHostToDevice, s)) != cudaSuccess) return fail("upload tgrid", e);
     if ((e = cudaMemcpyAsync(pl->d_ioff, ioff.data(), ioff.size() * sizeof(long long), cudaMemcpyHostToDevice, s)) != cudaSuccess) return fail("upload offsets", e);
-    hhg::StageReq sr{pl->d_pulses, n_pulses, pl->d_tgrid, pl->d_ioff, pl->d_coef, pl->n_intervals, degree, s};
+    hhg::StageReq sr{pl->d_pulses, n_pulses, pl->d_tgrid, pl->d_ioff, pl->d_coef,
+                     pl->n_intervals, degree, 9.0 / 10.0 * pow(pow(5.0, -8.0), -1.0 / 8), s};
     if ((st = stage_variant(pl, sr)) != HHG_OK) {
         hhg_plan_destroy(pl);
         return st;

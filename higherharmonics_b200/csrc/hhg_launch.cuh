@@ -26,6 +26,7 @@ struct StageReq {
     double *coef;
     long long total_intervals;
     int degree;
+    double grow_max;
     cudaStream_t stream;
 };
 
@@ -66,13 +67,13 @@ cudaError_t stage_model(const StageReq &s) {
     const long long blocks = (s.total_intervals + threads - 1) / threads;
     if (s.degree == 5)
         stage_pulses_kernel<M, 5><<<(unsigned)blocks, threads, 0, s.stream>>>(
-            s.pulses, s.n_pulses, s.tgrid, s.interval_off, s.coef, s.total_intervals);
+            s.pulses, s.n_pulses, s.tgrid, s.interval_off, s.coef, s.total_intervals, s.grow_max);
     else if (s.degree == 7)
         stage_pulses_kernel<M, 7><<<(unsigned)blocks, threads, 0, s.stream>>>(
-            s.pulses, s.n_pulses, s.tgrid, s.interval_off, s.coef, s.total_intervals);
+            s.pulses, s.n_pulses, s.tgrid, s.interval_off, s.coef, s.total_intervals, s.grow_max);
     else if (s.degree == 11)
         stage_pulses_kernel<M, 11><<<(unsigned)blocks, threads, 0, s.stream>>>(
-            s.pulses, s.n_pulses, s.tgrid, s.interval_off, s.coef, s.total_intervals);
+            s.pulses, s.n_pulses, s.tgrid, s.interval_off, s.coef, s.total_intervals, s.grow_max);
     else
         return cudaErrorInvalidValue;
     return cudaGetLastError();
@@ -83,11 +84,15 @@ cudaError_t launch_piflux2d(const LaunchReq &r);
 cudaError_t launch_piflux3d(const LaunchReq &r);
 cudaError_t launch_honeycomb(const LaunchReq &r);
 cudaError_t launch_dirac3d(const LaunchReq &r);
+cudaError_t launch_piflux2d_sym(const LaunchReq &r);
+cudaError_t launch_honeycomb_x(const LaunchReq &r);
 cudaError_t stage_dirac2d(const StageReq &s);
 cudaError_t stage_piflux2d(const StageReq &s);
 cudaError_t stage_piflux3d(const StageReq &s);
 cudaError_t stage_honeycomb(const StageReq &s);
 cudaError_t stage_dirac3d(const StageReq &s);
+cudaError_t stage_piflux2d_sym(const StageReq &s);
+cudaError_t stage_honeycomb_x(const StageReq &s);
 
 }  // namespace hhg
 

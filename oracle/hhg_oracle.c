@@ -753,7 +753,11 @@ int orc_current_density(const orc_model *m, const orc_pulse *p, const orc_time_c
                         const orc_solver *s, int n_k, const double *ktab, double *j_out,
                         orc_stats *st, int n_threads) {
     const int ns = tc->n_measurements + 1;
-    const int chunk = 64;
+    /* chunk size depends on n_k only (so the sum is the same for any thread
+     * count) and keeps >= 1024 chunks for load balance on many cores */
+    int chunk = n_k / 1024;
+    if (chunk < 1) chunk = 1;
+    if (chunk > 64) chunk = 64;
     const int n_chunks = (n_k + chunk - 1) / chunk;
     const double measure_every = (tc->t_end - tc->t_begin) / tc->n_measurements;
     double *t_samples = malloc(sizeof(double) * ns);

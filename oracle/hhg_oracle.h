@@ -98,8 +98,8 @@ double orc_vertex(const orc_model *m, const orc_pulse *p, const double *krow, do
                   const double *S);
 
 /* BZ sum j(t_i) = sum_k w_k vertex(k, A(t_i)) S(k, t_i), i = 0..n.  Fixed
- * reduction order (chunks of 64 k-points, summed in order), any thread
- * count. */
+ * reduction order (chunks of n_k/1024 in [1, 64] k-points, summed in
+ * order), the same for any thread count. */
 int orc_current_density(const orc_model *m, const orc_pulse *p, const orc_time_config *tc,
                         const orc_solver *s, int n_k, const double *ktab, double *j_out,
                         orc_stats *st, int n_threads);

@@ -52,6 +52,26 @@ def test_piflux2d_parity(engine):
     assert abs(st.attempted_steps - ost.attempted) <= 1e-3 * ost.attempted
 
 
+def test_piflux2d_general_polarisation_parity(engine):
+    sys = api.system(api.SYS_PIFLUX2D, hopping=1.0, pol=(0.6, 0.8))
+    pulse = api.cosine_pulse(0.9, 2, 2048, phase=0.3, window=(0.0, 6 * math.pi), energy_scale=10.0)
+    grid = api.grid_tensor(12, 12, -math.pi, math.pi, -math.pi, math.pi)
+    j, jr, st, ost, err, herr = _parity(engine, sys, pulse, grid, 1e-12, 1e-8)
+    assert err <= J_TOL, err
+    assert herr <= H_TOL, herr
+
+
+def test_long_standard_schedule_parity(engine):
+    # n_subdivisions = 2000 gives 6 steps per interval: the tabulated schedule
+    # covers 5, the last one runs on the interpolants
+    sys = api.system(api.SYS_DIRAC2D, velocity=1.0, mass=0.05)
+    pulse = api.cosine_pulse(1.0, 1, 512, energy_scale=10.0, n_subdivisions=2000)
+    grid = api.grid_tensor(8, 8, -2, 2, -2, 2)
+    j, jr, st, ost, err, herr = _parity(engine, sys, pulse, grid, 1e-10, 1e-10)
+    assert err <= J_TOL, err
+    assert st.attempted_steps == ost.attempted
+
+
 def test_piflux3d_reference_grid_parity(engine):
     # reference PiFlux with its continuum-limit grid (z_range = 2, N_coarse = 2)
     sys = api.system(api.SYS_PIFLUX3D, hopping=1.0)
