@@ -231,6 +231,7 @@ def our_arm(args, wl_name):
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
     def step():
+        flush.zero_()
         plan.execute_async(sptr)
         plan.spectrum_async(sptr)
 
@@ -285,6 +286,7 @@ def our_arm(args, wl_name):
     clocks = sampler.stop()
     elapsed_ms = e_start.elapsed_time(e_end)
     launch_ms = [a.elapsed_time(b) for a, b in ev]
+    step_sum_ms = sum(ev[k][0].elapsed_time(ev[k + 1][0]) for k in range(args.steps - 1))
     if ws > 1:
         t = torch.tensor([elapsed_ms], device="cuda", dtype=torch.float64)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
@@ -343,6 +345,9 @@ def our_arm(args, wl_name):
         "k_steps_per_s": ws * ksteps / avg_launch_s if ws == 1 else None,
         "k_steps_per_spectrum": ksteps, "harmonic_err_vs_fp64": herr,
         "gpu_launches": 4 * args.steps, "roofline": roofline, "clocks": clocks, "e2e": e2e,
+        "timing": {"device_ms_total": elapsed_ms, "launch_ms": launch_ms,
+                   "mean_step_ms_between_launch_starts": (step_sum_ms / (args.steps - 1)
+                                                          if args.steps > 1 else None)},
     }
     if ws == 1 and not args.no_cpu_baseline:
         rows = api.grid_rows(wl.system, wl.grid)

@@ -20,10 +20,10 @@
 //    the same (t, dt) sequence.  When all active lanes of a warp are on that
 //    schedule (a warp vote per attempt) the right-hand sides read the
 //    tabulated values with broadcast shared-memory loads.
-// The right-hand side combines the FP64 pulse values with the k-dependent
-// constants in FP64 and only then narrows to the stage precision R, so in the
-// mixed-precision variant every FP32 rounding depends on k and averages out in
-// the Brillouin-zone sum instead of acting like a common field error.
+// In the mixed-precision variant the pulse values and the k-dependent
+// constants are float pairs and every field term gets one final FP32 rounding
+// that depends on k, so FP32 errors average out in the Brillouin-zone sum
+// instead of acting like a common field error.
 //
 // At every sample the lanes' weighted current contributions are reduced with a
 // butterfly shuffle; lane (i mod 32) keeps sample i and every 32 samples the
@@ -42,6 +42,11 @@ namespace hhg {
 constexpr unsigned kFull = 0xffffffffu;
 constexpr double kDblEps = 2.220446049250313080847e-16;  // std::numeric_limits<double>::epsilon()
 constexpr int kMaxStd = 5;  // tabulated steps of the standard schedule per interval
+// Integration CTAs are 2 warps; at <= 144 registers 7 CTAs (14 warps) fit an
+// SM, so a 256x256 grid (2048 warps) is resident in a single wave on 148 SMs.
+constexpr int kWarpsPerBlock = 2;
+constexpr int kBlockThreads = 32 * kWarpsPerBlock;
+constexpr int kMinBlocksPerSM = 7;
 
 // Model variants.  *_SYM / *_X are the same physics with fewer distinct
 // pulse projections (PiFlux-2D with px == py; honeycomb with the field along
@@ -155,14 +160,49 @@ __device__ __forceinline__ void staged_values(const PulseDev &pd, double A, doub
 }
 
 // ---------------------------------------------------------------------------
-// Pulse evaluators used inside a step: polynomial (any t) or table (stage s of
-// a standard step).  Both return FP64 values.
+// Number types.  The FP64 path works in double throughout.  The mixed path
+// (R = float) carries pulse values and k-dependent constants as unevaluated
+// float pairs (hi, lo) and forms each field term with one final FP32
+// rounding, so no rounding is common to all k-points (a common one would act
+// like a field error that the Brillouin-zone sum cannot average out) and no
+// FP64 <-> FP32 conversion sits inside a right-hand side.
 // ---------------------------------------------------------------------------
-template <int NF, int D>
+template <typename R> struct Num;
+template <> struct Num<double> {
+    using V = double;  // pulse value / k constant
+    static __device__ __forceinline__ V mk(double x) { return x; }
+    static __device__ __forceinline__ double lin(V a, V b, V f) { return a - b * f; }       // a - b f
+    static __device__ __forceinline__ double dot2(V a, V b, V c, V d) { return a * b + c * d; }
+    static __device__ __forceinline__ double mul(V a, V f) { return a * f; }
+};
+template <> struct Num<float> {
+    using V = float2;
+    static __device__ __forceinline__ V mk(double x) {
+        const float h = (float)x;
+        return make_float2(h, (float)(x - (double)h));
+    }
+    static __device__ __forceinline__ float lin(V a, V b, V f) {
+        const float lo = a.y - b.x * f.y - b.y * f.x;
+        return fmaf(-b.x, f.x, a.x) + lo;
+    }
+    static __device__ __forceinline__ float dot2(V a, V b, V c, V d) {
+        const float lo = a.x * b.y + a.y * b.x + c.x * d.y + c.y * d.x;
+        return fmaf(a.x, b.x, fmaf(c.x, d.x, lo));
+    }
+    static __device__ __forceinline__ float mul(V a, V f) {
+        return fmaf(a.x, f.x, a.x * f.y + a.y * f.x);
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Pulse evaluators used inside a step: polynomial (any t) or table (stage s of
+// a standard step).  Values come back as Num<R>::V.
+// ---------------------------------------------------------------------------
+template <int NF, int D, typename R>
 struct PolyEval {
     const double *hd;  // interval record
     double tb, te;
-    __device__ __forceinline__ void operator()(int, double t, double *f) const {
+    __device__ __forceinline__ void operator()(int, double t, typename Num<R>::V *f) const {
         const double u = (t - hd[2]) * hd[3];
         const bool inside = (t > tb) && (t < te);
         const double *c0 = hd + slot_poly(NF);
@@ -172,15 +212,15 @@ struct PolyEval {
             double v = c[D];
 #pragma unroll
             for (int j = D - 1; j >= 0; --j) v = fma(v, u, c[j]);
-            f[n] = inside ? v : outside_value<NF>(n);
+            f[n] = Num<R>::mk(inside ? v : outside_value<NF>(n));
         }
     }
 };
 
-template <int NF>
+template <int NF, typename R>
 struct TableEval {
-    const double *tab;  // 13 x NF values of one standard step
-    __device__ __forceinline__ void operator()(int s, double, double *f) const {
+    const typename Num<R>::V *tab;  // 13 x NF values of one standard step
+    __device__ __forceinline__ void operator()(int s, double, typename Num<R>::V *f) const {
 #pragma unroll
         for (int n = 0; n < NF; ++n) f[n] = tab[s * NF + n];
     }
@@ -188,30 +228,31 @@ struct TableEval {
 
 // ---------------------------------------------------------------------------
 // Models.  init() reads the k row and the pulse's scaled constants; rhs()
-// evaluates dS/dt from the FP64 pulse values f (k-dependent field terms in
-// FP64, narrowed once to R); vertex() is the current contribution (weight
-// excluded) from the sample record r = [A(t_s), staged functions at t_s];
-// dvec() gives d with dS/dt = 2 d x S (Magnus-4).
+// evaluates dS/dt in precision R from the pulse values f; vertex() is the
+// current contribution (weight excluded, FP64) from the sample record r =
+// [A(t_s), staged functions at t_s]; dvec() gives d with dS/dt = 2 d x S
+// (Magnus-4, FP64 only).
 // ---------------------------------------------------------------------------
 template <int M, typename R> struct ModelState;
 
 // gapped 2D Dirac, d = (v (kx - px A), v (ky - py A), mass); dS/dt = 2 d x S.
 // mp: [0] 2v, [1] 2 mass, [2] px, [3] py
 template <typename R> struct ModelState<DIRAC2D, R> {
-    double ax, ay, bx, by;
+    using N = Num<R>;
+    typename N::V ax, ay, bx, by;
     R dz;
     double px, py;
     __device__ __forceinline__ void init(const PulseDev &p, const double *row) {
-        ax = p.mp[0] * row[0];
-        ay = p.mp[0] * row[1];
-        bx = p.mp[0] * p.mp[2];
-        by = p.mp[0] * p.mp[3];
+        ax = N::mk(p.mp[0] * row[0]);
+        ay = N::mk(p.mp[0] * row[1]);
+        bx = N::mk(p.mp[0] * p.mp[2]);
+        by = N::mk(p.mp[0] * p.mp[3]);
         dz = R(p.mp[1]);
         px = p.mp[2];
         py = p.mp[3];
     }
-    __device__ __forceinline__ void rhs(const double *f, const R *S, R *dS) const {
-        const R d0 = R(ax - bx * f[0]), d1 = R(ay - by * f[0]);
+    __device__ __forceinline__ void rhs(const typename N::V *f, const R *S, R *dS) const {
+        const R d0 = R(N::lin(ax, bx, f[0])), d1 = R(N::lin(ay, by, f[0]));
         dS[0] = d1 * S[2] - dz * S[1];
         dS[1] = dz * S[0] - d0 * S[2];
         dS[2] = d0 * S[1] - d1 * S[0];
@@ -220,8 +261,8 @@ template <typename R> struct ModelState<DIRAC2D, R> {
         return px * S[0] + py * S[1];
     }
     __device__ __forceinline__ void dvec(const double *f, double *d) const {
-        d[0] = 0.5 * (ax - bx * f[0]);
-        d[1] = 0.5 * (ay - by * f[0]);
+        d[0] = 0.5 * N::lin(ax, bx, f[0]);
+        d[1] = 0.5 * N::lin(ay, by, f[0]);
         d[2] = 0.5 * double(dz);
     }
 };
@@ -229,18 +270,20 @@ template <typename R> struct ModelState<DIRAC2D, R> {
 // Reference PiFlux (PiFlux.cpp:89-94): dS/dt = 4t (cx, cy, cos(kz - A)) x S,
 // cos(kz - A) = cos kz cos A + sin kz sin A.  mp: [0] 4t
 template <typename R> struct ModelState<PIFLUX3D, R> {
+    using N = Num<R>;
     R m0, m1;
-    double pcz, psz, cz, sz;
+    typename N::V pcz, psz;
+    double cz, sz;
     __device__ __forceinline__ void init(const PulseDev &p, const double *row) {
         const double pf = p.mp[0];
         m0 = R(pf * cos(row[0]));
         m1 = R(pf * cos(row[1]));
         sincos(row[2], &sz, &cz);
-        pcz = pf * cz;
-        psz = pf * sz;
+        pcz = N::mk(pf * cz);
+        psz = N::mk(pf * sz);
     }
-    __device__ __forceinline__ void rhs(const double *f, const R *S, R *dS) const {
-        const R m2 = R(pcz * f[0] + psz * f[1]);
+    __device__ __forceinline__ void rhs(const typename N::V *f, const R *S, R *dS) const {
+        const R m2 = R(N::dot2(pcz, f[0], psz, f[1]));
         dS[0] = m1 * S[2] - m2 * S[1];
         dS[1] = m2 * S[0] - m0 * S[2];
         dS[2] = m0 * S[1] - m1 * S[0];
@@ -252,29 +295,31 @@ template <typename R> struct ModelState<PIFLUX3D, R> {
     __device__ __forceinline__ void dvec(const double *f, double *d) const {
         d[0] = 0.5 * double(m0);
         d[1] = 0.5 * double(m1);
-        d[2] = 0.5 * (pcz * f[0] + psz * f[1]);
+        d[2] = 0.5 * N::dot2(pcz, f[0], psz, f[1]);
     }
 };
 
 // 2D pi-flux, d = -2t (cos(kx - px A), cos(ky - py A), 0); dS/dt = 2 d x S.
 // mp: [0] -4t, [2] px, [3] py.  SYM: px == py, one (cos, sin) pair.
 template <typename R, bool SYM> struct PiFlux2DState {
+    using N = Num<R>;
     static constexpr int Y = SYM ? 0 : 2;
-    double pcx, psx, pcy, psy, cx, sx, cy, sy, px, py;
+    typename N::V pcx, psx, pcy, psy;
+    double cx, sx, cy, sy, px, py;
     __device__ __forceinline__ void init(const PulseDev &p, const double *row) {
         const double pf = p.mp[0];
         sincos(row[0], &sx, &cx);
         sincos(row[1], &sy, &cy);
-        pcx = pf * cx;
-        psx = pf * sx;
-        pcy = pf * cy;
-        psy = pf * sy;
+        pcx = N::mk(pf * cx);
+        psx = N::mk(pf * sx);
+        pcy = N::mk(pf * cy);
+        psy = N::mk(pf * sy);
         px = p.mp[2];
         py = p.mp[3];
     }
-    __device__ __forceinline__ void rhs(const double *f, const R *S, R *dS) const {
-        const R m0 = R(pcx * f[0] + psx * f[1]);
-        const R m1 = R(pcy * f[Y] + psy * f[Y + 1]);
+    __device__ __forceinline__ void rhs(const typename N::V *f, const R *S, R *dS) const {
+        const R m0 = R(N::dot2(pcx, f[0], psx, f[1]));
+        const R m1 = R(N::dot2(pcy, f[Y], psy, f[Y + 1]));
         dS[0] = m1 * S[2];
         dS[1] = -(m0 * S[2]);
         dS[2] = m0 * S[1] - m1 * S[0];
@@ -284,8 +329,8 @@ template <typename R, bool SYM> struct PiFlux2DState {
         return px * (sx * r[1] - cx * r[2]) * S[0] + py * (sy * r[1 + Y] - cy * r[2 + Y]) * S[1];
     }
     __device__ __forceinline__ void dvec(const double *f, double *d) const {
-        d[0] = 0.5 * (pcx * f[0] + psx * f[1]);
-        d[1] = 0.5 * (pcy * f[Y] + psy * f[Y + 1]);
+        d[0] = 0.5 * N::dot2(pcx, f[0], psx, f[1]);
+        d[1] = 0.5 * N::dot2(pcy, f[Y], psy, f[Y + 1]);
         d[2] = 0.0;
     }
 };
@@ -298,8 +343,10 @@ template <typename R> struct ModelState<PIFLUX2D_SYM, R> : PiFlux2DState<R, true
 // mp: [0] 2t (pf), [1] 2 mass, [2] px, [3] py.  X: bonds 2 and 3 share one
 // projection (field along x), so the staged pairs are those of (s_0, s_1).
 template <typename R, bool X> struct HoneycombState {
+    using N = Num<R>;
     static constexpr int Q2 = X ? 2 : 4;
-    double c0, s0, c1, s1, c2, s2;  // cos/sin(nn_j . k)
+    typename N::V pc0, ps0, pc1, ps1, pc2, ps2, mc0, mc1, mc2;  // pf cos/sin(nn_j . k), -pf cos
+    double c0, s0, c1, s1, c2, s2;                              // cos/sin(nn_j . k)
     R dm;
     double pf, px, py;
     __device__ __forceinline__ void init(const PulseDev &p, const double *row) {
@@ -308,19 +355,23 @@ template <typename R, bool X> struct HoneycombState {
         sincos(row[0], &s0, &c0);
         sincos(-0.5 * row[0] + nny * row[1], &s1, &c1);
         sincos(-0.5 * row[0] - nny * row[1], &s2, &c2);
+        pc0 = N::mk(pf * c0), ps0 = N::mk(pf * s0), mc0 = N::mk(-pf * c0);
+        pc1 = N::mk(pf * c1), ps1 = N::mk(pf * s1), mc1 = N::mk(-pf * c1);
+        pc2 = N::mk(pf * c2), ps2 = N::mk(pf * s2), mc2 = N::mk(-pf * c2);
         dm = R(p.mp[1]);
         px = p.mp[2];
         py = p.mp[3];
     }
-    __device__ __forceinline__ void gamma(const double *f, double &gre, double &gim) const {
-        // e^{i(a - b)} = (ca cb + sa sb) + i (sa cb - ca sb)
-        gre = (c0 * f[0] + s0 * f[1]) + (c1 * f[2] + s1 * f[3]) + (c2 * f[Q2] + s2 * f[Q2 + 1]);
-        gim = (s0 * f[0] - c0 * f[1]) + (s1 * f[2] - c1 * f[3]) + (s2 * f[Q2] - c2 * f[Q2 + 1]);
+    // pf Re gamma', pf Im gamma' with e^{i(a - b)} = (ca cb + sa sb) + i (sa cb - ca sb)
+    __device__ __forceinline__ void gamma(const typename N::V *f, R &gr, R &gi) const {
+        gr = R(N::dot2(pc0, f[0], ps0, f[1])) + R(N::dot2(pc1, f[2], ps1, f[3])) +
+             R(N::dot2(pc2, f[Q2], ps2, f[Q2 + 1]));
+        gi = R(N::dot2(ps0, f[0], mc0, f[1])) + R(N::dot2(ps1, f[2], mc1, f[3])) +
+             R(N::dot2(ps2, f[Q2], mc2, f[Q2 + 1]));
     }
-    __device__ __forceinline__ void rhs(const double *f, const R *S, R *dS) const {
-        double gre, gim;
-        gamma(f, gre, gim);
-        const R gr = R(pf * gre), gi = R(pf * gim);
+    __device__ __forceinline__ void rhs(const typename N::V *f, const R *S, R *dS) const {
+        R gr, gi;
+        gamma(f, gr, gi);
         dS[0] = -(S[2] * gi) - dm * S[1];
         dS[1] = -(S[2] * gr) + dm * S[0];
         dS[2] = S[0] * gi + S[1] * gr;
@@ -339,8 +390,8 @@ template <typename R, bool X> struct HoneycombState {
     }
     __device__ __forceinline__ void dvec(const double *f, double *d) const {
         // d = t (Re g', -Im g', mass) = 0.5 (pf Re g', -pf Im g', 2 mass)
-        double gre, gim;
-        gamma(f, gre, gim);
+        const double gre = (c0 * f[0] + s0 * f[1]) + (c1 * f[2] + s1 * f[3]) + (c2 * f[Q2] + s2 * f[Q2 + 1]);
+        const double gim = (s0 * f[0] - c0 * f[1]) + (s1 * f[2] - c1 * f[3]) + (s2 * f[Q2] - c2 * f[Q2 + 1]);
         d[0] = 0.5 * pf * gre;
         d[1] = -0.5 * pf * gim;
         d[2] = 0.5 * double(dm);
@@ -351,15 +402,16 @@ template <typename R> struct ModelState<HONEYCOMB_X, R> : HoneycombState<R, true
 
 // Reference DiracSystem sigma RHS (DiracSystem.cpp:144-153); row = (k_z, kappa, |k|).
 template <typename R> struct ModelState<DIRAC3D, R> {
-    double ax, az, mk2;
+    using N = Num<R>;
+    typename N::V ax, az, mk2;
     __device__ __forceinline__ void init(const PulseDev &, const double *row) {
-        ax = 2.0 * row[1] / row[2];
-        az = 2.0 * row[0] / row[2];
-        mk2 = 2.0 * row[2];
+        ax = N::mk(2.0 * row[1] / row[2]);
+        az = N::mk(2.0 * row[0] / row[2]);
+        mk2 = N::mk(2.0 * row[2]);
     }
-    __device__ __forceinline__ void rhs(const double *f, const R *S, R *dS) const {
-        const R mx = R(f[0] * ax);
-        const R mz = R(mk2 - f[0] * az);
+    __device__ __forceinline__ void rhs(const typename N::V *f, const R *S, R *dS) const {
+        const R mx = R(N::mul(ax, f[0]));
+        const R mz = R(N::lin(mk2, az, f[0]));
         dS[0] = mz * S[1];
         dS[1] = mx * S[2] - S[0] * mz;
         dS[2] = -mx * S[1];
@@ -367,9 +419,9 @@ template <typename R> struct ModelState<DIRAC3D, R> {
     __device__ __forceinline__ double vertex(const double *, const double *S) const { return S[2]; }
     __device__ __forceinline__ void dvec(const double *f, double *d) const {
         // G = [[0, mz, 0], [-mz, 0, mx], [0, -mx, 0]] = [g]_x, g = (-mx, 0, -mz) = 2 d
-        d[0] = -0.5 * (f[0] * ax);
+        d[0] = -0.5 * N::mul(ax, f[0]);
         d[1] = 0.0;
-        d[2] = -0.5 * (mk2 - f[0] * az);
+        d[2] = -0.5 * N::lin(mk2, az, f[0]);
     }
 };
 
@@ -385,7 +437,7 @@ __device__ __forceinline__ void rkf78_attempt(const ModelState<M, R> &ms, const 
                                               double t, double h, const double *x, double *xn,
                                               double *e, double *k0d) {
     R k[13][3];
-    double f[NF];
+    typename Num<R>::V f[NF];
     const R xr[3] = {R(x[0]), R(x[1]), R(x[2])};
     const R hr = R(h);
     ev(0, t, f);
@@ -397,30 +449,31 @@ __device__ __forceinline__ void rkf78_attempt(const ModelState<M, R> &ms, const 
         ev(s, t + rk_c(s) * h, f);                                                  \
         ms.rhs(f, xt, k[s]);                                                        \
     }
+    // sums grouped as independent pairs (shorter dependency chains)
     HHG_STAGE(1, R(2.0 / 27.0) * k[0][i])
     HHG_STAGE(2, R(1.0 / 36.0) * k[0][i] + R(1.0 / 12.0) * k[1][i])
     HHG_STAGE(3, R(1.0 / 24.0) * k[0][i] + R(1.0 / 8.0) * k[2][i])
-    HHG_STAGE(4, R(5.0 / 12.0) * k[0][i] + R(-25.0 / 16.0) * k[2][i] + R(25.0 / 16.0) * k[3][i])
-    HHG_STAGE(5, R(1.0 / 20.0) * k[0][i] + R(1.0 / 4.0) * k[3][i] + R(1.0 / 5.0) * k[4][i])
-    HHG_STAGE(6, R(-25.0 / 108.0) * k[0][i] + R(125.0 / 108.0) * k[3][i] +
-                     R(-65.0 / 27.0) * k[4][i] + R(125.0 / 54.0) * k[5][i])
-    HHG_STAGE(7, R(31.0 / 300.0) * k[0][i] + R(61.0 / 225.0) * k[4][i] + R(-2.0 / 9.0) * k[5][i] +
-                     R(13.0 / 900.0) * k[6][i])
-    HHG_STAGE(8, R(2.0) * k[0][i] + R(-53.0 / 6.0) * k[3][i] + R(704.0 / 45.0) * k[4][i] +
-                     R(-107.0 / 9.0) * k[5][i] + R(67.0 / 90.0) * k[6][i] + R(3.0) * k[7][i])
-    HHG_STAGE(9, R(-91.0 / 108.0) * k[0][i] + R(23.0 / 108.0) * k[3][i] +
-                     R(-976.0 / 135.0) * k[4][i] + R(311.0 / 54.0) * k[5][i] +
-                     R(-19.0 / 60.0) * k[6][i] + R(17.0 / 6.0) * k[7][i] + R(-1.0 / 12.0) * k[8][i])
-    HHG_STAGE(10, R(2383.0 / 4100.0) * k[0][i] + R(-341.0 / 164.0) * k[3][i] +
-                      R(4496.0 / 1025.0) * k[4][i] + R(-301.0 / 82.0) * k[5][i] +
-                      R(2133.0 / 4100.0) * k[6][i] + R(45.0 / 82.0) * k[7][i] +
-                      R(45.0 / 164.0) * k[8][i] + R(18.0 / 41.0) * k[9][i])
-    HHG_STAGE(11, R(3.0 / 205.0) * k[0][i] + R(-6.0 / 41.0) * k[5][i] + R(-3.0 / 205.0) * k[6][i] +
-                      R(-3.0 / 41.0) * k[7][i] + R(3.0 / 41.0) * k[8][i] + R(6.0 / 41.0) * k[9][i])
-    HHG_STAGE(12, R(-1777.0 / 4100.0) * k[0][i] + R(-341.0 / 164.0) * k[3][i] +
-                      R(4496.0 / 1025.0) * k[4][i] + R(-289.0 / 82.0) * k[5][i] +
-                      R(2193.0 / 4100.0) * k[6][i] + R(51.0 / 82.0) * k[7][i] +
-                      R(33.0 / 164.0) * k[8][i] + R(12.0 / 41.0) * k[9][i] + k[11][i])
+    HHG_STAGE(4, R(5.0 / 12.0) * k[0][i] + (R(-25.0 / 16.0) * k[2][i] + R(25.0 / 16.0) * k[3][i]))
+    HHG_STAGE(5, R(1.0 / 20.0) * k[0][i] + (R(1.0 / 4.0) * k[3][i] + R(1.0 / 5.0) * k[4][i]))
+    HHG_STAGE(6, (R(-25.0 / 108.0) * k[0][i] + R(125.0 / 108.0) * k[3][i]) +
+                     (R(-65.0 / 27.0) * k[4][i] + R(125.0 / 54.0) * k[5][i]))
+    HHG_STAGE(7, (R(31.0 / 300.0) * k[0][i] + R(61.0 / 225.0) * k[4][i]) +
+                     (R(-2.0 / 9.0) * k[5][i] + R(13.0 / 900.0) * k[6][i]))
+    HHG_STAGE(8, (R(2.0) * k[0][i] + R(-53.0 / 6.0) * k[3][i] + R(704.0 / 45.0) * k[4][i]) +
+                     (R(-107.0 / 9.0) * k[5][i] + R(67.0 / 90.0) * k[6][i] + R(3.0) * k[7][i]))
+    HHG_STAGE(9, (R(-91.0 / 108.0) * k[0][i] + R(23.0 / 108.0) * k[3][i] +
+                  R(-976.0 / 135.0) * k[4][i] + R(311.0 / 54.0) * k[5][i]) +
+                     (R(-19.0 / 60.0) * k[6][i] + R(17.0 / 6.0) * k[7][i] + R(-1.0 / 12.0) * k[8][i]))
+    HHG_STAGE(10, (R(2383.0 / 4100.0) * k[0][i] + R(-341.0 / 164.0) * k[3][i] +
+                   R(4496.0 / 1025.0) * k[4][i] + R(-301.0 / 82.0) * k[5][i]) +
+                      (R(2133.0 / 4100.0) * k[6][i] + R(45.0 / 82.0) * k[7][i] +
+                       R(45.0 / 164.0) * k[8][i] + R(18.0 / 41.0) * k[9][i]))
+    HHG_STAGE(11, (R(3.0 / 205.0) * k[0][i] + R(-6.0 / 41.0) * k[5][i] + R(-3.0 / 205.0) * k[6][i]) +
+                      (R(-3.0 / 41.0) * k[7][i] + R(3.0 / 41.0) * k[8][i] + R(6.0 / 41.0) * k[9][i]))
+    HHG_STAGE(12, (R(-1777.0 / 4100.0) * k[0][i] + R(-341.0 / 164.0) * k[3][i] +
+                   R(4496.0 / 1025.0) * k[4][i] + R(-289.0 / 82.0) * k[5][i]) +
+                      (R(2193.0 / 4100.0) * k[6][i] + R(51.0 / 82.0) * k[7][i] +
+                       R(33.0 / 164.0) * k[8][i] + R(12.0 / 41.0) * k[9][i] + k[11][i]))
 #undef HHG_STAGE
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
@@ -516,16 +569,24 @@ __device__ __forceinline__ bool control(const KParams &P, const double *S, const
 // power in FP32 (the error norm, the comparison and dt stay FP64).
 // ---------------------------------------------------------------------------
 template <int M, int D, typename R, int STEPPER, int PROPOSER>
-__global__ void __launch_bounds__(128, 3) bz_integrate_kernel(const KParams P) {
+__global__ void __launch_bounds__(kBlockThreads, kMinBlocksPerSM) bz_integrate_kernel(const KParams P) {
     constexpr int NF = Traits<M>::NF;
     constexpr int SLOT = slot_doubles(NF, D);
     constexpr int SCHED = slot_sched(NF, D);
     constexpr int TAB = slot_table(NF, D);
     constexpr bool kNarrow = sizeof(R) != sizeof(double);
-    __shared__ __align__(16) double stage_raw[4][SLOT];
+    // the carry proposer never reads the standard-schedule table
+    constexpr int COPY = (PROPOSER == 0) ? SLOT : SCHED;
+    constexpr int NTAB = kMaxStd * 13 * NF;
+    using V = typename Num<R>::V;
+    __shared__ __align__(16) double stage_raw[kWarpsPerBlock][SLOT];
+    __shared__ __align__(16) V stage_tab[kWarpsPerBlock][kNarrow && PROPOSER == 0 ? NTAB : 1];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
     double *slot = stage_raw[wib];
+    const V *tabv;
+    if constexpr (kNarrow && PROPOSER == 0) tabv = stage_tab[wib];
+    else tabv = reinterpret_cast<const V *>(slot + TAB);
 
     unsigned long long my_attempts = 0, my_rejects = 0;
     for (;;) {
@@ -565,11 +626,15 @@ __global__ void __launch_bounds__(128, 3) bz_integrate_kernel(const KParams P) {
                     const double2 *src =
                         reinterpret_cast<const double2 *>(coef + (size_t)(i - 1) * SLOT);
                     double2 *dst = reinterpret_cast<double2 *>(slot);
-                    for (int c = lane; c < SLOT / 2; c += 32) dst[c] = __ldg(src + c);
+                    for (int c = lane; c < COPY / 2; c += 32) dst[c] = __ldg(src + c);
+                    if constexpr (kNarrow && PROPOSER == 0) {
+                        __syncwarp();
+                        for (int c = lane; c < NTAB; c += 32) stage_tab[wib][c] = Num<R>::mk(slot[TAB + c]);
+                    }
                     __syncwarp();
                     rec = slot + 4;
                     const double t0 = slot[0], t1 = slot[1];
-                    const PolyEval<NF, D> poly{slot, tb, te};
+                    const PolyEval<NF, D, R> poly{slot, tb, te};
                     if constexpr (STEPPER == 1) {
                         if (!dead) {
                             const int ns = P.magnus_substeps;
@@ -579,9 +644,10 @@ __global__ void __launch_bounds__(128, 3) bz_integrate_kernel(const KParams P) {
                             for (int s = 0; s < ns; ++s) {
                                 const double ts = t0 + s * hs;
                                 double f[NF], d1[3], d2[3];
-                                poly(0, ts + g * hs, f);
+                                const PolyEval<NF, D, double> pd64{slot, tb, te};
+                                pd64(0, ts + g * hs, f);
                                 ms.dvec(f, d1);
-                                poly(0, ts + (1.0 - g) * hs, f);
+                                pd64(0, ts + (1.0 - g) * hs, f);
                                 ms.dvec(f, d2);
                                 double wv[3];
                                 wv[0] = hs * (d1[0] + d2[0]) + q3 * (d2[1] * d1[2] - d2[2] * d1[1]);
@@ -606,7 +672,7 @@ __global__ void __launch_bounds__(128, 3) bz_integrate_kernel(const KParams P) {
                             if (active) {
                                 double xn[3], e[3], k0[3];
                                 if (table) {
-                                    const TableEval<NF> tev{slot + TAB + wa * 13 * NF};
+                                    const TableEval<NF, R> tev{tabv + wa * 13 * NF};
                                     rkf78_attempt<M, NF, R>(ms, tev, t, dt, S, xn, e, k0);
                                 } else {
                                     rkf78_attempt<M, NF, R>(ms, poly, t, dt, S, xn, e, k0);

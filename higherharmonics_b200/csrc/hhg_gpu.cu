@@ -642,7 +642,7 @@ hhg_status hhg_plan_create(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_p
     if (o.tile_k <= 0) {
         // auto: keep at least ~8 items per resident warp when there is work
         // for that, and the partial buffer below 8 GB
-        const long long resident = (long long)ctx->sm_count * 16;
+        const long long resident = (long long)ctx->sm_count * hhg::kWarpsPerBlock * hhg::kMinBlocksPerSM;
         long long total_samples = 0;
         for (int p = 0; p < n_pulses; ++p) total_samples += pulses[p].n_measurements + 1;
         while (true) {
@@ -781,7 +781,7 @@ hhg_status hhg_plan_create(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_p
         return st;
     }
     const long long max_ctas = (long long)std::max(occ, 1) * ctx->sm_count;
-    const long long need = (pl->n_items + 3) / 4;
+    const long long need = (pl->n_items + hhg::kWarpsPerBlock - 1) / hhg::kWarpsPerBlock;
     pl->grid = (int)std::max(1LL, std::min(max_ctas, need));
     if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return fail("plan setup", e);
     *out = pl;

@@ -34,11 +34,11 @@ template <int M, int D, typename R, int ST, int PR>
 cudaError_t launch_one(const LaunchReq &r) {
     auto kern = bz_integrate_kernel<M, D, R, ST, PR>;
     if (r.occupancy_out) {
-        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(r.occupancy_out, kern, 128, 0);
+        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(r.occupancy_out, kern, kBlockThreads, 0);
         if (e != cudaSuccess) return e;
     }
     if (r.grid <= 0) return cudaSuccess;
-    kern<<<r.grid, 128, 0, r.stream>>>(r.kp);
+    kern<<<r.grid, kBlockThreads, 0, r.stream>>>(r.kp);
     return cudaGetLastError();
 }
 

@@ -177,3 +177,43 @@ def test_batched_pulses_match_single(engine):
         seg = jb[off:off + p.n_measurements + 1]
         assert np.array_equal(seg, js)
         off += p.n_measurements + 1
+
+
+def _spectrum_err(engine, sys, pulse, grid, opts, opts_ref):
+    from higherharmonics_b200.analysis import (default_max_order, harmonic_intensities,
+                                               harmonic_rel_err)
+    j, st = engine.current_density(sys, pulse, grid, opts)
+    jr, str_ = engine.current_density(sys, pulse, grid, opts_ref)
+    a = engine.spectrum(j, pulse.n_measurements, pulse.window_begin, pulse.window_end)
+    b = engine.spectrum(jr, pulse.n_measurements, pulse.window_begin, pulse.window_end)
+    mo = default_max_order(b[0])
+    return (harmonic_rel_err(harmonic_intensities(*a, mo), harmonic_intensities(*b, mo)),
+            rel_l2(j, jr), st, str_)
+
+
+@pytest.mark.parametrize("model", ["piflux2d", "honeycomb", "dirac2d"])
+def test_fast_variants_meet_harmonic_bar(engine, model):
+    """Mixed precision and the carried step proposal stay within the 1e-4
+    harmonic-intensity bar of the plain FP64 path."""
+    if model == "piflux2d":
+        s = 1 / math.sqrt(2)
+        sys = api.system(api.SYS_PIFLUX2D, hopping=1.0, pol=(s, s))
+        pulse = api.cosine_pulse(1.0, 2, 2048, window=(0.0, 6 * math.pi), energy_scale=20.0)
+        grid = api.grid_tensor(64, 64, -math.pi, math.pi, -math.pi, math.pi)
+        ref = api.solver(1e-12, 1e-8)
+    elif model == "honeycomb":
+        sys = api.system(api.SYS_HONEYCOMB, hopping=1.0, mass=0.1)
+        pulse = api.cosine_pulse(1.0, 2, 2048, window=(0.0, 6 * math.pi), energy_scale=12.5)
+        grid = api.grid_rhombic(64, 64)
+        ref = api.solver(1e-12, 1e-8)
+    else:
+        sys = api.system(api.SYS_DIRAC2D, velocity=1.0, mass=0.05)
+        pulse = api.cosine_pulse(1.0, 4, 4096, energy_scale=10.0)
+        grid = api.grid_tensor(32, 32, -2, 2, -2, 2)
+        ref = api.solver(1e-10, 1e-10)
+    for opts in (api.solver(ref.abs_tol, ref.rel_tol, proposer=api.PROPOSER_CARRY),
+                 api.solver(1e-8, 1e-6, precision=api.PREC_MIXED),
+                 api.solver(1e-8, 1e-6, precision=api.PREC_MIXED, proposer=api.PROPOSER_CARRY)):
+        herr, jerr, st, st_ref = _spectrum_err(engine, sys, pulse, grid, opts, ref)
+        assert herr <= 1e-4, (opts.precision, opts.proposer, herr)
+        assert jerr <= 1e-4, (opts.precision, opts.proposer, jerr)
