@@ -200,6 +200,7 @@ template <> struct Num<float> {
 // ---------------------------------------------------------------------------
 template <int NF, int D, typename R>
 struct PolyEval {
+    static constexpr bool kReuse = true;  // stages sharing a node reuse the values
     const double *hd;  // interval record
     double tb, te;
     __device__ __forceinline__ void operator()(int, double t, typename Num<R>::V *f) const {
@@ -219,6 +220,7 @@ struct PolyEval {
 
 template <int NF, typename R>
 struct TableEval {
+    static constexpr bool kReuse = false;  // a shared-memory reload is cheaper than registers
     const typename Num<R>::V *tab;  // 13 x NF values of one standard step
     __device__ __forceinline__ void operator()(int s, double, typename Num<R>::V *f) const {
 #pragma unroll
@@ -442,11 +444,28 @@ __device__ __forceinline__ void rkf78_attempt(const ModelState<M, R> &ms, const 
     const R hr = R(h);
     ev(0, t, f);
     ms.rhs(f, xr, k[0]);
+    // stages 7, 11 and 12 share their nodes with 3, 0 and 10 (c = 1/6, 0, 1)
+    typename Num<R>::V f0[Eval::kReuse ? NF : 1], f3[Eval::kReuse ? NF : 1],
+        f10[Eval::kReuse ? NF : 1];
+    if constexpr (Eval::kReuse) {
+#pragma unroll
+        for (int n = 0; n < NF; ++n) f0[n] = f[n];
+    }
 #define HHG_STAGE(s, EXPR)                                                          \
     {                                                                               \
         R xt[3];                                                                    \
         _Pragma("unroll") for (int i = 0; i < 3; ++i) xt[i] = xr[i] + hr * (EXPR);  \
-        ev(s, t + rk_c(s) * h, f);                                                  \
+        if constexpr (Eval::kReuse && (s == 7 || s == 11 || s == 12)) {             \
+            _Pragma("unroll") for (int n = 0; n < NF; ++n)                          \
+                f[n] = (s == 7) ? f3[n] : (s == 11) ? f0[n] : f10[n];               \
+        } else {                                                                    \
+            ev(s, t + rk_c(s) * h, f);                                              \
+        }                                                                           \
+        if constexpr (Eval::kReuse && (s == 3 || s == 10)) {                        \
+            _Pragma("unroll") for (int n = 0; n < NF; ++n) {                        \
+                if (s == 3) f3[n] = f[n]; else f10[n] = f[n];                       \
+            }                                                                       \
+        }                                                                           \
         ms.rhs(f, xt, k[s]);                                                        \
     }
     // sums grouped as independent pairs (shorter dependency chains)
