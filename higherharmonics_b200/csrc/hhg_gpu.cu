@@ -1061,3 +1061,4 @@ hhg_status hhg_measure_fp64_peak(hhg_ctx *ctx, double *tflops) {
 }
 
 }  // extern "C"
+
