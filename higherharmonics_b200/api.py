@@ -33,6 +33,7 @@ EXPORTED = [
     "hhg_gpu_current_density", "hhg_gpu_spectrum", "hhg_plan_create", "hhg_plan_destroy",
     "hhg_plan_j_length", "hhg_plan_execute_async", "hhg_plan_device_j", "hhg_plan_fetch",
     "hhg_plan_spectrum_async", "hhg_plan_fetch_spectrum", "hhg_measure_fp64_peak",
+    "hhg_gpu_current_density_noalloc",
 ]
 
 
@@ -123,6 +124,10 @@ def load_library() -> ctypes.CDLL:
         L.hhg_plan_spectrum_async.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         L.hhg_plan_fetch_spectrum.argtypes = [ctypes.c_void_p, ctypes.c_int, _D, _D, _D]
         L.hhg_measure_fp64_peak.argtypes = [ctypes.c_void_p, _D]
+        L.hhg_gpu_current_density_noalloc.argtypes = [
+            ctypes.POINTER(SystemDesc), ctypes.POINTER(PulseDesc), ctypes.c_void_p, ctypes.c_int64,
+            ctypes.POINTER(SolverOpts), ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(Stats),
+            ctypes.c_char_p, ctypes.c_size_t]
         L.hhg_default_solver_opts.argtypes = [ctypes.POINTER(SolverOpts)]
         _lib = L
     return _lib

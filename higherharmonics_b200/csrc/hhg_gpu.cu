@@ -1062,3 +1062,83 @@ hhg_status hhg_measure_fp64_peak(hhg_ctx *ctx, double *tflops) {
 
 }  // extern "C"
 
+// ---------------------------------------------------------------------------
+// Per-pulse preparation for the allocation-free entry point (hhg_noalloc.cu).
+// Same arithmetic as hhg_plan_create for one pulse; kept separate so the plan
+// path is untouched.
+// ---------------------------------------------------------------------------
+#include "hhg_pulse_prep.hpp"
+
+namespace hhg_prep {
+
+hhg_status prepare_pulse(const hhg_system_desc *sys, const hhg_pulse_desc *pulse, PulsePrep &out) {
+    hhg_status st = check_system(nullptr, sys);
+    if (st != HHG_OK) return st;
+    if (!pulse) return HHG_BAD_CONFIG;
+    if ((st = check_pulse(nullptr, *pulse)) != HHG_OK) return st;
+    out.model = kernel_model(*sys);
+    out.nf = model_nf(out.model);
+    const double nny = 0.5 * kSqrt3;
+    double proj[3] = {0, 0, 0};
+    switch (out.model) {
+    case hhg::PIFLUX2D: proj[0] = sys->pol_x; proj[1] = sys->pol_y; break;
+    case hhg::PIFLUX2D_SYM: proj[0] = sys->pol_x; break;
+    case hhg::HONEYCOMB:
+        proj[0] = 1.0 * sys->pol_x + 0.0 * sys->pol_y;
+        proj[1] = -0.5 * sys->pol_x + nny * sys->pol_y;
+        proj[2] = -0.5 * sys->pol_x - nny * sys->pol_y;
+        break;
+    case hhg::HONEYCOMB_X: proj[0] = sys->pol_x; proj[1] = -0.5 * sys->pol_x; break;
+    case hhg::PIFLUX3D: proj[0] = 1.0; break;
+    }
+    const int d = choose_degree(*pulse, proj, out.nf);
+    out.degree = d < 0 ? -1 : std::max(5, d);
+    const hhg_pulse_desc &q = *pulse;
+    PulseDev &p = out.pulse;
+    std::memset(&p, 0, sizeof p);
+    p.amplitude = q.amplitude;
+    p.t_begin = q.t_begin;
+    p.t_end = q.t_begin + 2 * kPi * q.n_cycles;
+    p.inv_n_cycles = 1. / q.n_cycles;
+    p.phase = q.phase;
+    p.window_begin = q.window_begin;
+    p.measure_every = (q.window_end - q.window_begin) / q.n_measurements;
+    p.dt0 = p.measure_every / q.n_subdivisions;
+    const double es = q.energy_scale;
+    switch (sys->kind) {
+    case HHG_SYS_DIRAC2D: p.mp[0] = 2.0 * sys->velocity * es; p.mp[1] = 2.0 * sys->mass * es; break;
+    case HHG_SYS_PIFLUX3D: p.mp[0] = 4.0 * sys->hopping * es; break;
+    case HHG_SYS_PIFLUX2D: p.mp[0] = -4.0 * sys->hopping * es; break;
+    case HHG_SYS_HONEYCOMB: p.mp[0] = 2.0 * sys->hopping * es; p.mp[1] = 2.0 * sys->mass * es; break;
+    default: break;
+    }
+    p.mp[2] = sys->pol_x;
+    p.mp[3] = sys->pol_y;
+    for (int n = 0; n < 3; ++n) p.s[n] = proj[n];
+    const double t0s = 0 * p.measure_every + p.window_begin;
+    double env = 0.0;
+    if (!(t0s <= p.t_begin || t0s >= p.t_end)) env = 0.5 * (1. - cos(p.inv_n_cycles * (t0s - p.t_begin)));
+    const double A0 = p.amplitude * (env * sin(t0s + p.phase));
+    p.s0rec[0] = A0;
+    if (out.nf == 1) p.s0rec[1] = A0;
+    else if (out.model == hhg::PIFLUX3D) {
+        p.s0rec[1] = cos(A0);
+        p.s0rec[2] = sin(A0);
+    } else
+        for (int n = 0; n < out.nf / 2; ++n) {
+            p.s0rec[1 + 2 * n] = cos(proj[n] * A0);
+            p.s0rec[2 + 2 * n] = sin(proj[n] * A0);
+        }
+    p.n_meas = q.n_measurements;
+    out.tgrid.assign((size_t)q.n_measurements + 1, 0.0);
+    double t_begin = p.window_begin, t_end = t_begin + p.measure_every;
+    out.tgrid[0] = t_begin;
+    for (int i = 1; i <= q.n_measurements; ++i) {
+        out.tgrid[i] = t_end;
+        t_begin = t_end;
+        t_end += p.measure_every;
+    }
+    return HHG_OK;
+}
+
+}  // namespace hhg_prep

@@ -26,6 +26,7 @@
 #ifndef HHG_GPU_H
 #define HHG_GPU_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -213,6 +214,36 @@ hhg_status hhg_plan_fetch_spectrum(hhg_plan *plan, int pulse, double *re_out, do
  * of the device (TFLOP/s, FMA = 2 flops), the denominator of the
  * integration kernel's roofline. */
 hhg_status hhg_measure_fp64_peak(hhg_ctx *ctx, double *tflops);
+
+/* Allocation-free variant of hhg_gpu_current_density for one pulse.  It has
+ * no counterpart in the reference (which runs on the CPU).
+ *
+ * For callers that cannot allocate device memory during the call: code
+ * running under another framework's memory pool or allocator hooks,
+ * real-time loops where cudaMalloc's implicit synchronisation is not
+ * acceptable, and jobs that budget every byte of a shared GPU.  The caller
+ * passes the k table (n_rows x 8 doubles, the layout of hhg_grid_rows) and
+ * receives j (n_measurements + 1 doubles), both in device memory.  The
+ * integration scratch (pulse staging, partial current rows, counters) lives
+ * in a fixed 64 MiB device array inside the library, so this call performs
+ * no cudaMalloc/cudaFree and calls no allocating library routine; problems
+ * whose scratch exceeds 64 MiB are rejected with HHG_BAD_CONFIG and a
+ * message in err (e.g. 128x128 k rows over 8192 intervals fit).  Every GPU
+ * on which the entry point is used holds the 64 MiB until the process exits.
+ *
+ * Runs asynchronously on `stream` (a cudaStream_t; NULL = the legacy default
+ * stream) on the current device.  With stats != NULL it synchronises the
+ * stream and reports HHG_STEP_LIMIT / HHG_NONFINITE like the other entry
+ * points; with stats == NULL those conditions are not checked.  The first
+ * call on a device looks up the scratch array's device address (once per
+ * device); make that first call before any stream capture.  All calls share
+ * the one array: calls that overlap on the GPU race and must be serialised by
+ * the caller.  err (optional, err_cap bytes) receives a message on failure. */
+hhg_status hhg_gpu_current_density_noalloc(const hhg_system_desc *sys,
+                                           const hhg_pulse_desc *pulse, const double *d_rows,
+                                           int64_t n_rows, const hhg_solver_opts *opts,
+                                           double *d_j_out, void *stream, hhg_stats *stats,
+                                           char *err, size_t err_cap);
 
 #ifdef __cplusplus
 }
