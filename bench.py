@@ -45,6 +45,8 @@ VARIANTS = {
     "carry": dict(proposer=1),
     "mixed": dict(precision=1, abs_tol=1e-8, rel_tol=1e-6),
     "mixed_carry": dict(precision=1, proposer=1, abs_tol=1e-8, rel_tol=1e-6),
+    "lockstep": dict(proposer=3),
+    "mixed_lockstep": dict(precision=1, proposer=3, abs_tol=1e-8, rel_tol=1e-6),
 }
 
 

@@ -85,6 +85,16 @@ __host__ __device__ constexpr int slot_table(int nf, int deg) {
 __host__ __device__ constexpr int slot_doubles(int nf, int deg) {
     return slot_table(nf, deg) + ((kMaxStd * 13 * nf + 1) & ~1);
 }
+// Dyadic layout (warp-synchronous stepping): after the header and the
+// interpolants, the exact stage values of every step of size
+// (t1 - t0) / 2^L, L < kDyaLevels, level-major: for L, position q, stage s,
+// function n at index ((2^L - 1 + q) * 13 + s) * nf + n.  Mixed precision
+// stores float pairs in the same 8-byte slots.
+constexpr int kDyaLevels = 3;
+__host__ __device__ constexpr int slot_dyadic(int nf, int deg) { return slot_sched(nf, deg); }
+__host__ __device__ constexpr int slot_doubles_dyadic(int nf, int deg) {
+    return slot_dyadic(nf, deg) + (((1 << kDyaLevels) - 1) * 13 * nf + 1) / 2 * 2;
+}
 // Value of staged function n outside the pulse window: A -> 0, cos -> 1, sin -> 0.
 template <int NF> __host__ __device__ constexpr double outside_value(int n) {
     return (NF > 1 && (n % 2) == 0) ? 1.0 : 0.0;
@@ -573,39 +583,121 @@ __device__ __forceinline__ bool control(const KParams &P, const double *S, const
 }
 
 // ---------------------------------------------------------------------------
+// The reference's per-lane controller for one interval, from (t, dt) to t1:
+// integrate_adaptive semantics (PiFlux.cpp:104-110 calling Boost.Odeint):
+// clip the step to land on t1; loop while t1 - t > DBL_EPSILON; err =
+// max_i |e_i| / (abs + rel (|x_i| + dt |dxdt_i|)); err > 1: dt *= max(0.9
+// err^-1/6, 0.2) and retry; else accept and, if err < 0.5, dt *= 0.9 max(err,
+// 5^-8)^-1/8.  With USE_STD the warp reads the tabulated pulse values while all
+// active lanes are on the standard schedule.  Called by the whole warp.
+// ---------------------------------------------------------------------------
+template <int M, int NF, int D, typename R, bool USE_STD, bool CARRY>
+__device__ __forceinline__ void lane_controller(const KParams &P, const ModelState<M, R> &ms,
+                                                const PolyEval<NF, D, R> &poly,
+                                                const double *slot, const typename Num<R>::V *tabv,
+                                                int n_std, double t, double dt, double t1,
+                                                double *S, bool &dead, double &carry_dt,
+                                                unsigned long long &attempts_out,
+                                                unsigned long long &rejects) {
+    constexpr bool kNarrow = sizeof(R) != sizeof(double);
+    constexpr int SCHED = slot_sched(NF, D);
+    bool active = !dead;
+    int fails = 0, attempts = 0, wa = 0;
+    while (__any_sync(kFull, active)) {
+        if (active && (t + dt) - t1 > kDblEps) dt = t1 - t;
+        bool table = false;
+        if constexpr (USE_STD) {
+            // every active lane on the standard schedule -> table path
+            const bool on = !active || (wa < n_std && t == slot[SCHED + 2 + wa] &&
+                                        dt == slot[SCHED + 2 + kMaxStd + wa]);
+            table = __all_sync(kFull, on);
+        }
+        if (active) {
+            double xn[3], e[3], k0[3];
+            if (table) {
+                const TableEval<NF, R> tev{tabv + wa * 13 * NF};
+                rkf78_attempt<M, NF, R>(ms, tev, t, dt, S, xn, e, k0);
+            } else {
+                rkf78_attempt<M, NF, R>(ms, poly, t, dt, S, xn, e, k0);
+            }
+            ++attempts;
+            const double dt_used = dt;
+            if (control<kNarrow>(P, S, e, k0, dt)) {
+                t += dt_used;
+                S[0] = xn[0];
+                S[1] = xn[1];
+                S[2] = xn[2];
+                fails = 0;
+                if (!(t1 - t > kDblEps)) active = false;
+                if (CARRY) carry_dt = dt;
+            } else {
+                ++rejects;
+                if (++fails >= P.max_failed) {
+                    active = false;
+                    dead = true;
+                    atomicAdd(P.counters + 3, 1ull);
+                    atomicMax(P.status, 2);
+                }
+            }
+            if (active && attempts >= P.max_attempts) {
+                active = false;
+                dead = true;
+                atomicAdd(P.counters + 3, 1ull);
+                atomicMax(P.status, 2);
+            }
+        }
+        ++wa;
+    }
+    attempts_out += attempts;
+}
+
+// ---------------------------------------------------------------------------
 // Persistent, work-stealing integration + BZ-sum kernel.
-// STEPPER 0: controlled RKF78 with the reference's integrate_adaptive
-//   semantics (PiFlux.cpp:104-110 calling Boost.Odeint): clip the step to
-//   land on t_end; loop while t_end - t > DBL_EPSILON; err = max_i |e_i| /
-//   (abs + rel (|x_i| + dt |dxdt_i|)); err > 1: dt *= max(0.9 err^-1/6, 0.2)
-//   and retry; else accept and, if err < 0.5, dt *= 0.9 max(err, 5^-8)^-1/8.
-// STEPPER 1: Magnus-4 (two-point Gauss), magnus_substeps steps per interval:
-//   omega = h (d1 + d2) + (sqrt3/3) h^2 (d2 x d1), S <- exp([omega]_x) S.
-// PROPOSER 0: every interval restarts at dt0 = measure_every/n_subdivisions
-//   (the reference); 1: an interval starts from the controller's last
-//   proposal of the previous interval.
+// STEPPER 0: controlled RKF78; STEPPER 1: Magnus-4 (two-point Gauss),
+//   magnus_substeps steps per interval: omega = h (d1 + d2) + (sqrt3/3) h^2
+//   (d2 x d1), S <- exp([omega]_x) S.
+// PROPOSER 0: the reference's per-lane controller, every interval restarting
+//   at dt0 = measure_every / n_subdivisions;
+// PROPOSER 1: per-lane controller, an interval starts from the controller's
+//   last proposal of the previous interval;
+// PROPOSER 2: warp-synchronous dyadic stepping: all lanes of a warp take the
+//   step (t1 - t0) / 2^L at positions q of the dyadic grid; the step is
+//   accepted only if every lane's embedded error passes (|e_i| <= abs + rel
+//   (|x_i| + h |dxdt_i|), the reference's norm), otherwise the warp retries at
+//   L + 1; after an accepted step the warp coarsens when every lane's error
+//   would still pass at twice the step (err < 1/600 ~ 0.9^8 / 2^8) and q is
+//   even.  Levels below kDyaLevels read the tabulated pulse values from the
+//   staging slot (global memory, broadcast within the warp); beyond
+//   kLevelMax the warp falls back to the per-lane controller.  The level is
+//   carried to the next interval.
 // The mixed-precision variant (R = float) evaluates the growth/shrink factor's
 // power in FP32 (the error norm, the comparison and dt stay FP64).
 // ---------------------------------------------------------------------------
+constexpr int kLevelMax = 10;
+constexpr double kCoarsen = 1.0 / 600.0;
+
 template <int M, int D, typename R, int STEPPER, int PROPOSER>
 __global__ void __launch_bounds__(kBlockThreads, kMinBlocksPerSM) bz_integrate_kernel(const KParams P) {
     constexpr int NF = Traits<M>::NF;
-    constexpr int SLOT = slot_doubles(NF, D);
+    constexpr bool kDyadic = PROPOSER >= 2;
+    constexpr int SLOT = kDyadic ? slot_doubles_dyadic(NF, D) : slot_doubles(NF, D);
     constexpr int SCHED = slot_sched(NF, D);
     constexpr int TAB = slot_table(NF, D);
+    constexpr int DYA = slot_dyadic(NF, D);
     constexpr bool kNarrow = sizeof(R) != sizeof(double);
-    // the carry proposer never reads the standard-schedule table
+    // only the reference schedule reads the standard table; the dyadic table
+    // is read from global memory
     constexpr int COPY = (PROPOSER == 0) ? SLOT : SCHED;
     constexpr int NTAB = kMaxStd * 13 * NF;
     using V = typename Num<R>::V;
-    __shared__ __align__(16) double stage_raw[kWarpsPerBlock][SLOT];
+    __shared__ __align__(16) double stage_raw[kWarpsPerBlock][COPY];
     __shared__ __align__(16) V stage_tab[kWarpsPerBlock][kNarrow && PROPOSER == 0 ? NTAB : 1];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
     double *slot = stage_raw[wib];
     const V *tabv;
     if constexpr (kNarrow && PROPOSER == 0) tabv = stage_tab[wib];
-    else tabv = reinterpret_cast<const V *>(slot + TAB);
+    else tabv = reinterpret_cast<const V *>(slot + (PROPOSER == 0 ? TAB : 0));
 
     unsigned long long my_attempts = 0, my_rejects = 0;
     for (;;) {
@@ -635,6 +727,7 @@ __global__ void __launch_bounds__(kBlockThreads, kMinBlocksPerSM) bz_integrate_k
             const double w = valid ? row[3] : 0.0;
             bool dead = !valid;
             double carry_dt = dt0;
+            int level = 0;      // warp-uniform dyadic level carried across intervals
             double held = 0.0;  // lane (i & 31) holds the warp sum of sample i
 
             for (int i = 0; i <= N; ++i) {
@@ -642,8 +735,8 @@ __global__ void __launch_bounds__(kBlockThreads, kMinBlocksPerSM) bz_integrate_k
                 if (i > 0) {
                     // stage interval i-1 into this warp's shared slot
                     __syncwarp();
-                    const double2 *src =
-                        reinterpret_cast<const double2 *>(coef + (size_t)(i - 1) * SLOT);
+                    const double *gslot = coef + (size_t)(i - 1) * SLOT;
+                    const double2 *src = reinterpret_cast<const double2 *>(gslot);
                     double2 *dst = reinterpret_cast<double2 *>(slot);
                     for (int c = lane; c < COPY / 2; c += 32) dst[c] = __ldg(src + c);
                     if constexpr (kNarrow && PROPOSER == 0) {
@@ -676,55 +769,71 @@ __global__ void __launch_bounds__(kBlockThreads, kMinBlocksPerSM) bz_integrate_k
                             }
                             my_attempts += ns;
                         }
-                    } else {
+                    } else if constexpr (!kDyadic) {
                         const int n_std = (PROPOSER == 0) ? (int)slot[SCHED] : 0;
-                        double t = t0;
-                        double dt = (PROPOSER == 1) ? carry_dt : dt0;
-                        bool active = !dead;
-                        int fails = 0, attempts = 0, wa = 0;
-                        while (__any_sync(kFull, active)) {
-                            if (active && (t + dt) - t1 > kDblEps) dt = t1 - t;
-                            // every active lane on the standard schedule -> table path
-                            const bool on = !active || (wa < n_std && t == slot[SCHED + 2 + wa] &&
-                                                        dt == slot[SCHED + 2 + kMaxStd + wa]);
-                            const bool table = (PROPOSER == 0) && __all_sync(kFull, on);
-                            if (active) {
-                                double xn[3], e[3], k0[3];
-                                if (table) {
-                                    const TableEval<NF, R> tev{tabv + wa * 13 * NF};
-                                    rkf78_attempt<M, NF, R>(ms, tev, t, dt, S, xn, e, k0);
+                        lane_controller<M, NF, D, R, PROPOSER == 0, PROPOSER == 1>(
+                            P, ms, poly, slot, tabv, n_std, t0, (PROPOSER == 1) ? carry_dt : dt0,
+                            t1, S, dead, carry_dt, my_attempts, my_rejects);
+                    } else {
+                        const V *dtab = reinterpret_cast<const V *>(gslot + DYA);
+                        const double span = t1 - t0;
+                        int L = level, qpos = 0;
+                        bool fallback = false, coarse_end = false;
+                        for (;;) {
+                            const double h = ldexp(span, -L);
+                            const double tq = t0 + qpos * h;
+                            bool ok = true, small = true;
+                            double xn[3];
+                            if (!dead) {
+                                double e[3], k0[3];
+                                if (L < kDyaLevels) {
+                                    const TableEval<NF, R> tev{dtab + ((1 << L) - 1 + qpos) * 13 * NF};
+                                    rkf78_attempt<M, NF, R>(ms, tev, tq, h, S, xn, e, k0);
                                 } else {
-                                    rkf78_attempt<M, NF, R>(ms, poly, t, dt, S, xn, e, k0);
+                                    rkf78_attempt<M, NF, R>(ms, poly, tq, h, S, xn, e, k0);
                                 }
-                                ++attempts;
-                                const double dt_used = dt;
-                                if (control<kNarrow>(P, S, e, k0, dt)) {
-                                    t += dt_used;
+                                ++my_attempts;
+#pragma unroll
+                                for (int c = 0; c < 3; ++c) {
+                                    const double den = P.abs_tol + P.rel_tol * (fabs(S[c]) + h * fabs(k0[c]));
+                                    ok = ok && !(fabs(e[c]) > den);
+                                    small = small && (fabs(e[c]) < kCoarsen * den);
+                                }
+                            }
+                            if (__all_sync(kFull, ok)) {
+                                if (!dead) {
                                     S[0] = xn[0];
                                     S[1] = xn[1];
                                     S[2] = xn[2];
-                                    fails = 0;
-                                    if (!(t1 - t > kDblEps)) active = false;
-                                    if (PROPOSER == 1) carry_dt = dt;
-                                } else {
-                                    ++my_rejects;
-                                    if (++fails >= P.max_failed) {
-                                        active = false;
-                                        dead = true;
-                                        atomicAdd(P.counters + 3, 1ull);
-                                        atomicMax(P.status, 2);
-                                    }
                                 }
-                                if (active && attempts >= P.max_attempts) {
-                                    active = false;
-                                    dead = true;
-                                    atomicAdd(P.counters + 3, 1ull);
-                                    atomicMax(P.status, 2);
+                                ++qpos;
+                                const bool coarse = __all_sync(kFull, small);
+                                if (qpos == (1 << L)) {
+                                    coarse_end = coarse;
+                                    break;
                                 }
+                                if (coarse && L > 0 && !(qpos & 1)) {
+                                    --L;
+                                    qpos >>= 1;
+                                }
+                            } else {
+                                if (!dead && !ok) ++my_rejects;
+                                if (L >= kLevelMax) {
+                                    fallback = true;
+                                    break;
+                                }
+                                ++L;
+                                qpos <<= 1;
                             }
-                            ++wa;
                         }
-                        my_attempts += attempts;
+                        if (fallback) {
+                            // the plain controller takes over for the rest of the interval
+                            const double h = ldexp(span, -L);
+                            lane_controller<M, NF, D, R, false, false>(
+                                P, ms, poly, slot, tabv, 0, t0 + qpos * h, 0.5 * h, t1, S, dead,
+                                carry_dt, my_attempts, my_rejects);
+                        }
+                        level = (coarse_end && L > 0) ? L - 1 : (L > kLevelMax ? kLevelMax : L);
                     }
                     if (!dead && !(isfinite(S[0]) && isfinite(S[1]) && isfinite(S[2]))) {
                         dead = true;
@@ -762,16 +871,18 @@ __global__ void __launch_bounds__(kBlockThreads, kMinBlocksPerSM) bz_integrate_k
 // ---------------------------------------------------------------------------
 // Staging: per (pulse, interval) the exact end-sample record, Chebyshev
 // interpolants of the staged functions at D+1 first-kind nodes (monomials in
-// u), and the standard schedule with its exact stage values.
+// u), and either (LAYOUT 0) the standard schedule with its exact stage values
+// or (LAYOUT 1 / 2) the exact stage values of the dyadic steps, as doubles or
+// as float pairs.
 // ---------------------------------------------------------------------------
-template <int M, int D>
+template <int M, int D, int LAYOUT>
 __global__ void stage_pulses_kernel(const PulseDev *__restrict__ pulses, int n_pulses,
                                     const double *__restrict__ tgrid,
                                     const long long *__restrict__ interval_off,
                                     double *__restrict__ coef, long long total_intervals,
                                     double grow_max) {
     constexpr int NF = Traits<M>::NF;
-    constexpr int SLOT = slot_doubles(NF, D);
+    constexpr int SLOT = LAYOUT == 0 ? slot_doubles(NF, D) : slot_doubles_dyadic(NF, D);
     constexpr int HDR = slot_header(NF);
     constexpr int SCHED = slot_sched(NF, D);
     constexpr int TAB = slot_table(NF, D);
@@ -835,6 +946,31 @@ __global__ void stage_pulses_kernel(const PulseDev *__restrict__ pulses, int n_p
             }
         }
         for (int j = 0; j < NN; ++j) out[HDR + n * NN + j] = m[j];
+    }
+    if constexpr (LAYOUT != 0) {
+        // dyadic steps: position q of level L starts at t0 + q (t1 - t0) 2^-L
+        constexpr int DYA = slot_dyadic(NF, D);
+        const double span = t1 - t0;
+        for (int L = 0; L < kDyaLevels; ++L) {
+            const double h = ldexp(span, -L);
+            for (int q = 0; q < (1 << L); ++q) {
+                const double tq = t0 + q * h;
+                for (int s = 0; s < 13; ++s) {
+                    double v[NF];
+                    staged_values<M>(pd, laser_exact(pd, tq + rk_c(s) * h), v);
+                    for (int n = 0; n < NF; ++n) {
+                        double *dst = out + DYA + ((((1 << L) - 1 + q) * 13 + s) * NF + n);
+                        if constexpr (LAYOUT == 1) {
+                            *dst = v[n];
+                        } else {
+                            const float hi = (float)v[n];
+                            *reinterpret_cast<float2 *>(dst) = make_float2(hi, (float)(v[n] - (double)hi));
+                        }
+                    }
+                }
+            }
+        }
+        return;
     }
     // standard schedule: dt0, dt0 g, dt0 g^2, ... clipped to land on t1,
     // with exactly the lanes' arithmetic

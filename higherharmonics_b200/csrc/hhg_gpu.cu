@@ -390,6 +390,11 @@ int kernel_model(const hhg_system_desc &s) {
     return s.kind;
 }
 
+// Kernel step-control mode for an ABI proposer: 0 restart, 1 carry, 2 dyadic.
+int kernel_proposer(int abi) {
+    return abi == HHG_PROPOSER_CARRY ? 1 : (abi == HHG_PROPOSER_NONE ? 0 : 2);
+}
+
 int model_nf(int m) {
     switch (m) {
     case hhg::DIRAC2D: return 1;
@@ -579,7 +584,8 @@ hhg_status hhg_plan_create(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_p
         return set_err(ctx, HHG_BAD_CONFIG, "unknown precision");
     if (o.proposer == HHG_PROPOSER_LEARNED)
         return set_err(ctx, HHG_UNSUPPORTED, "learned proposer requires a trained network (hhg_learned_*)");
-    if (o.proposer != HHG_PROPOSER_NONE && o.proposer != HHG_PROPOSER_CARRY)
+    if (o.proposer != HHG_PROPOSER_NONE && o.proposer != HHG_PROPOSER_CARRY &&
+        o.proposer != HHG_PROPOSER_LOCKSTEP)
         return set_err(ctx, HHG_BAD_CONFIG, "unknown proposer");
     if (!(o.abs_tol >= 0.0) || !(o.rel_tol >= 0.0) || !(o.abs_tol + o.rel_tol > 0.0))
         return set_err(ctx, HHG_BAD_CONFIG, "tolerances must be >= 0 and not both 0");
@@ -634,7 +640,8 @@ hhg_status hhg_plan_create(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_p
         degree = std::max(degree, d);
     }
     pl->degree = degree;
-    const int slot = hhg::slot_doubles(nf, degree);
+    const bool dyadic = o.proposer == HHG_PROPOSER_LOCKSTEP;
+    const int slot = dyadic ? hhg::slot_doubles_dyadic(nf, degree) : hhg::slot_doubles(nf, degree);
 
     // work decomposition
     const int64_t tiles = (pl->n_k + 31) / 32;
@@ -763,6 +770,7 @@ hhg_status hhg_plan_create(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_p
     if ((e = cudaMemcpyAsync(pl->d_ioff, ioff.data(), ioff.size() * sizeof(long long), cudaMemcpyHostToDevice, s)) != cudaSuccess) return fail("upload offsets", e);
     hhg::StageReq sr{pl->d_pulses, n_pulses, pl->d_tgrid, pl->d_ioff, pl->d_coef,
                      pl->n_intervals, degree, 9.0 / 10.0 * pow(pow(5.0, -8.0), -1.0 / 8), s};
+    sr.layout = dyadic ? (o.precision == HHG_PREC_MIXED ? 2 : 1) : 0;
     if ((st = stage_variant(pl, sr)) != HHG_OK) {
         hhg_plan_destroy(pl);
         return st;
@@ -773,7 +781,7 @@ hhg_status hhg_plan_create(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_p
     lr.degree = degree;
     lr.precision = o.precision;
     lr.stepper = o.stepper;
-    lr.proposer = o.proposer;
+    lr.proposer = kernel_proposer(o.proposer);
     lr.grid = 0;
     lr.occupancy_out = &occ;
     if ((st = launch_variant(pl, lr)) != HHG_OK) {
@@ -838,7 +846,7 @@ hhg_status hhg_plan_execute_async(hhg_plan *pl, void *stream) {
     lr.degree = pl->degree;
     lr.precision = pl->opts.precision;
     lr.stepper = pl->opts.stepper;
-    lr.proposer = pl->opts.proposer;
+    lr.proposer = kernel_proposer(pl->opts.proposer);
     lr.grid = pl->grid;
     lr.stream = s;
     lr.occupancy_out = nullptr;

@@ -12,7 +12,7 @@ struct LaunchReq {
     int degree;     // 5, 7 or 11
     int precision;  // 0 FP64, 1 mixed (FP32 right-hand side)
     int stepper;    // 0 RKF78, 1 Magnus-4
-    int proposer;   // 0 restart at dt0, 1 carry
+    int proposer;   // 0 restart at dt0, 1 carry, 2 warp-synchronous dyadic
     int grid;       // CTAs; 0 = query occupancy only
     cudaStream_t stream;
     int *occupancy_out;  // blocks per SM for the selected variant (if non-null)
@@ -28,6 +28,7 @@ struct StageReq {
     int degree;
     double grow_max;
     cudaStream_t stream;
+    int layout = 0;  // 0 standard schedule, 1 dyadic FP64, 2 dyadic float pairs
 };
 
 template <int M, int D, typename R, int ST, int PR>
@@ -47,10 +48,12 @@ cudaError_t launch_deg(const LaunchReq &r) {
     if (r.stepper == 1) return launch_one<M, D, double, 1, 0>(r);
     if (r.precision == 0) {
         if (r.proposer == 0) return launch_one<M, D, double, 0, 0>(r);
-        return launch_one<M, D, double, 0, 1>(r);
+        if (r.proposer == 1) return launch_one<M, D, double, 0, 1>(r);
+        return launch_one<M, D, double, 0, 2>(r);
     }
     if (r.proposer == 0) return launch_one<M, D, float, 0, 0>(r);
-    return launch_one<M, D, float, 0, 1>(r);
+    if (r.proposer == 1) return launch_one<M, D, float, 0, 1>(r);
+    return launch_one<M, D, float, 0, 2>(r);
 }
 
 template <int M>
@@ -61,21 +64,28 @@ cudaError_t launch_model(const LaunchReq &r) {
     return cudaErrorInvalidValue;
 }
 
+template <int M, int D, int LAYOUT>
+void stage_one(const StageReq &s, unsigned blocks, int threads) {
+    stage_pulses_kernel<M, D, LAYOUT><<<blocks, threads, 0, s.stream>>>(
+        s.pulses, s.n_pulses, s.tgrid, s.interval_off, s.coef, s.total_intervals, s.grow_max);
+}
+
+template <int M, int D>
+void stage_deg(const StageReq &s, unsigned blocks, int threads) {
+    if (s.layout == 0) stage_one<M, D, 0>(s, blocks, threads);
+    else if (s.layout == 1) stage_one<M, D, 1>(s, blocks, threads);
+    else stage_one<M, D, 2>(s, blocks, threads);
+}
+
 template <int M>
 cudaError_t stage_model(const StageReq &s) {
     const int threads = 128;
     const long long blocks = (s.total_intervals + threads - 1) / threads;
-    if (s.degree == 5)
-        stage_pulses_kernel<M, 5><<<(unsigned)blocks, threads, 0, s.stream>>>(
-            s.pulses, s.n_pulses, s.tgrid, s.interval_off, s.coef, s.total_intervals, s.grow_max);
-    else if (s.degree == 7)
-        stage_pulses_kernel<M, 7><<<(unsigned)blocks, threads, 0, s.stream>>>(
-            s.pulses, s.n_pulses, s.tgrid, s.interval_off, s.coef, s.total_intervals, s.grow_max);
-    else if (s.degree == 11)
-        stage_pulses_kernel<M, 11><<<(unsigned)blocks, threads, 0, s.stream>>>(
-            s.pulses, s.n_pulses, s.tgrid, s.interval_off, s.coef, s.total_intervals, s.grow_max);
-    else
-        return cudaErrorInvalidValue;
+    if (s.layout < 0 || s.layout > 2) return cudaErrorInvalidValue;
+    if (s.degree == 5) stage_deg<M, 5>(s, (unsigned)blocks, threads);
+    else if (s.degree == 7) stage_deg<M, 7>(s, (unsigned)blocks, threads);
+    else if (s.degree == 11) stage_deg<M, 11>(s, (unsigned)blocks, threads);
+    else return cudaErrorInvalidValue;
     return cudaGetLastError();
 }
 

@@ -117,7 +117,8 @@ typedef enum hhg_precision { HHG_PREC_FP64 = 0, HHG_PREC_MIXED = 1 } hhg_precisi
 typedef enum hhg_proposer {
     HHG_PROPOSER_NONE = 0,    /* reference: every interval restarts at dt = measure_every / n_subdivisions */
     HHG_PROPOSER_CARRY = 1,   /* first step of an interval = last controller proposal */
-    HHG_PROPOSER_LEARNED = 2  /* first step of an interval = trained MLP proposal */
+    HHG_PROPOSER_LEARNED = 2, /* warp-synchronous dyadic steps, level proposed by a trained MLP */
+    HHG_PROPOSER_LOCKSTEP = 3 /* warp-synchronous dyadic steps, level carried between intervals */
 } hhg_proposer;
 
 /* Solver options.  abs_tol / rel_tol: the reference uses 1e-12 / 1e-8

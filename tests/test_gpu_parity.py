@@ -212,8 +212,10 @@ def test_fast_variants_meet_harmonic_bar(engine, model):
         grid = api.grid_tensor(32, 32, -2, 2, -2, 2)
         ref = api.solver(1e-10, 1e-10)
     for opts in (api.solver(ref.abs_tol, ref.rel_tol, proposer=api.PROPOSER_CARRY),
+                 api.solver(ref.abs_tol, ref.rel_tol, proposer=api.PROPOSER_LOCKSTEP),
                  api.solver(1e-8, 1e-6, precision=api.PREC_MIXED),
-                 api.solver(1e-8, 1e-6, precision=api.PREC_MIXED, proposer=api.PROPOSER_CARRY)):
+                 api.solver(1e-8, 1e-6, precision=api.PREC_MIXED, proposer=api.PROPOSER_CARRY),
+                 api.solver(1e-8, 1e-6, precision=api.PREC_MIXED, proposer=api.PROPOSER_LOCKSTEP)):
         herr, jerr, st, st_ref = _spectrum_err(engine, sys, pulse, grid, opts, ref)
         assert herr <= 1e-4, (opts.precision, opts.proposer, herr)
         assert jerr <= 1e-4, (opts.precision, opts.proposer, jerr)
