@@ -5,7 +5,7 @@ sum -> trapezoidal FFT path on the 256x256 PiFlux-2D workload.
 One step = one spectrum: integrate all 65 536 k-points over the 8-cycle
 pulse (8192 measurement intervals), reduce j(t), FFT it.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--variant fp64|carry|mixed|mixed_carry]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--variant NAME]
   python bench.py --impl reference ...   # the oracle port on the host cores
 
 Under torchrun (N > 1) every rank integrates its own pulse instance (the
@@ -47,7 +47,30 @@ VARIANTS = {
     "mixed_carry": dict(precision=1, proposer=1, abs_tol=1e-8, rel_tol=1e-6),
     "lockstep": dict(proposer=3),
     "mixed_lockstep": dict(precision=1, proposer=3, abs_tol=1e-8, rel_tol=1e-6),
+    "learned": dict(proposer=2),
+    "mixed_learned": dict(precision=1, proposer=2, abs_tol=1e-8, rel_tol=1e-6),
 }
+LEARNED_RECORDS = 1 << 21
+LEARNED_EPOCHS = 20
+
+
+def train_proposer(eng, wl, api):
+    """Step-size history of a carry run of the same workload at the plain
+    tolerances -> the learned proposer, trained on the GPU (outside the timed
+    region; reported under "training")."""
+    p = wl.pulses[0]
+    every = max(1, math.ceil(wl.n_k * p.n_measurements / LEARNED_RECORDS))
+    t0 = time.perf_counter()
+    recs, cst = eng.learned_collect(wl.system, wl.pulses, wl.grid, wl.opts(), hist_every=every,
+                                    cap=LEARNED_RECORDS)
+    t1 = time.perf_counter()
+    net = api.mlp_init(1, recs)
+    loss, train_ms = eng.mlp_train(recs, net, api.train_opts(epochs=LEARNED_EPOCHS))
+    t2 = time.perf_counter()
+    return net, {"records": int(recs.shape[0]), "hist_every": every,
+                 "collect_s": t1 - t0, "train_s": t2 - t1, "train_device_ms": train_ms,
+                 "epochs": LEARNED_EPOCHS, "loss_first_last": [float(loss[0]), float(loss[-1])],
+                 "network": "8-64-64-64-1 SiLU, BF16/FP32, tcgen05 training"}
 
 
 def dist_env():
@@ -222,7 +245,11 @@ def our_arm(args, wl_name):
         for p in wl.pulses:
             p.phase = p.phase + 0.1 * rank
     eng = api.Engine(dev)
-    okw = VARIANTS[args.variant]
+    okw = dict(VARIANTS[args.variant])
+    training = None
+    if okw.get("proposer") == api.PROPOSER_LEARNED:
+        net, training = train_proposer(eng, wl, api)
+        okw["mlp"] = net
     plan = eng.plan(wl.system, wl.pulses, wl.grid, wl.opts(**okw))
     # a dedicated stream: the legacy default stream has handle 0, which the
     # C ABI reads as "the context's own stream"
@@ -347,6 +374,7 @@ def our_arm(args, wl_name):
         "k_steps_per_s": ws * ksteps / avg_launch_s if ws == 1 else None,
         "k_steps_per_spectrum": ksteps, "harmonic_err_vs_fp64": herr,
         "gpu_launches": 4 * args.steps, "roofline": roofline, "clocks": clocks, "e2e": e2e,
+        "training": training,
         "timing": {"device_ms_total": elapsed_ms, "launch_ms": launch_ms,
                    "mean_step_ms_between_launch_starts": (step_sum_ms / (args.steps - 1)
                                                           if args.steps > 1 else None)},

@@ -34,7 +34,16 @@ EXPORTED = [
     "hhg_plan_j_length", "hhg_plan_execute_async", "hhg_plan_device_j", "hhg_plan_fetch",
     "hhg_plan_spectrum_async", "hhg_plan_fetch_spectrum", "hhg_measure_fp64_peak",
     "hhg_gpu_current_density_noalloc",
+    "hhg_learned_collect", "hhg_default_train_opts", "hhg_mlp_init", "hhg_mlp_train",
+    "hhg_mlp_gradients", "hhg_mlp_predict",
 ]
+ABI_VERSION = 2
+MLP_INPUTS, MLP_HIDDEN = 8, 64
+MLP_N_PARAMS = 64 * 8 + 64 + 64 * 64 + 64 + 64 * 64 + 64 + 64 + 1
+HIST_FIELDS = 12
+# slices of hhg_mlp.params: w1[64][8], b1, w2[64][64], b2, w3[64][64], b3, w4[64], b4
+MLP_LAYOUT = [("w1", (64, 8)), ("b1", (64,)), ("w2", (64, 64)), ("b2", (64,)),
+              ("w3", (64, 64)), ("b3", (64,)), ("w4", (64,)), ("b4", (1,))]
 
 
 class SystemDesc(ctypes.Structure):
@@ -59,12 +68,43 @@ class GridDesc(ctypes.Structure):
                 ("rows", ctypes.POINTER(ctypes.c_double)), ("n_rows", ctypes.c_int64)]
 
 
+class Mlp(ctypes.Structure):
+    """hhg_mlp: the learned step-size proposer's weights and standardisation."""
+    _fields_ = [("params", ctypes.c_float * MLP_N_PARAMS),
+                ("in_mu", ctypes.c_float * MLP_INPUTS), ("in_isig", ctypes.c_float * MLP_INPUTS),
+                ("out_mu", ctypes.c_float), ("out_sigma", ctypes.c_float),
+                ("level_margin", ctypes.c_float), ("reserved", ctypes.c_float)]
+
+    def param_array(self) -> np.ndarray:
+        """Writable float32 view of params."""
+        return np.ctypeslib.as_array(self.params)
+
+    def tensors(self) -> dict:
+        """params split into the named layer arrays (copies, float64)."""
+        flat = self.param_array().astype(np.float64)
+        out, o = {}, 0
+        for name, shape in MLP_LAYOUT:
+            n = int(np.prod(shape))
+            out[name] = flat[o:o + n].reshape(shape)
+            o += n
+        return out
+
+
 class SolverOpts(ctypes.Structure):
     _fields_ = [("stepper", ctypes.c_int32), ("precision", ctypes.c_int32),
                 ("proposer", ctypes.c_int32), ("magnus_substeps", ctypes.c_int32),
                 ("abs_tol", ctypes.c_double), ("rel_tol", ctypes.c_double),
                 ("max_failed_steps", ctypes.c_int32), ("max_attempts_per_interval", ctypes.c_int32),
-                ("tile_k", ctypes.c_int32), ("block_threads", ctypes.c_int32)]
+                ("tile_k", ctypes.c_int32), ("block_threads", ctypes.c_int32),
+                ("mlp", ctypes.POINTER(Mlp)), ("mlp_every", ctypes.c_int32),
+                ("reserved", ctypes.c_int32)]
+
+
+class TrainOpts(ctypes.Structure):
+    _fields_ = [("epochs", ctypes.c_int32), ("batch", ctypes.c_int32), ("lr", ctypes.c_float),
+                ("beta1", ctypes.c_float), ("beta2", ctypes.c_float), ("eps", ctypes.c_float),
+                ("lr_final", ctypes.c_float), ("reserved", ctypes.c_int32),
+                ("seed", ctypes.c_uint64)]
 
 
 class Stats(ctypes.Structure):
@@ -129,12 +169,37 @@ def load_library() -> ctypes.CDLL:
             ctypes.POINTER(SolverOpts), ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(Stats),
             ctypes.c_char_p, ctypes.c_size_t]
         L.hhg_default_solver_opts.argtypes = [ctypes.POINTER(SolverOpts)]
+        _F = ctypes.POINTER(ctypes.c_float)
+        L.hhg_learned_collect.argtypes = [ctypes.c_void_p, ctypes.POINTER(SystemDesc),
+                                          ctypes.POINTER(PulseDesc), ctypes.c_int,
+                                          ctypes.POINTER(GridDesc), ctypes.POINTER(SolverOpts),
+                                          ctypes.c_int, _F, ctypes.c_int64,
+                                          ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(Stats)]
+        L.hhg_default_train_opts.argtypes = [ctypes.POINTER(TrainOpts)]
+        L.hhg_mlp_init.argtypes = [ctypes.c_uint64, _F, ctypes.c_int64, ctypes.POINTER(Mlp)]
+        L.hhg_mlp_train.argtypes = [ctypes.c_void_p, _F, ctypes.c_int64, ctypes.POINTER(TrainOpts),
+                                    ctypes.POINTER(Mlp), _F, _D]
+        L.hhg_mlp_gradients.argtypes = [ctypes.c_void_p, _F, ctypes.c_int64, ctypes.POINTER(Mlp),
+                                        _F, _F]
+        L.hhg_mlp_predict.argtypes = [ctypes.c_void_p, _F, ctypes.c_int64, ctypes.POINTER(Mlp),
+                                      ctypes.c_int, _F]
         _lib = L
     return _lib
 
 
 def _ptr(a: np.ndarray):
     return a.ctypes.data_as(_D)
+
+
+def _fptr(a: np.ndarray):
+    assert a.dtype == np.float32 and a.flags.c_contiguous
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+def _records(rec) -> np.ndarray:
+    rec = np.ascontiguousarray(rec, dtype=np.float32)
+    assert rec.ndim == 2 and rec.shape[1] == HIST_FIELDS, rec.shape
+    return rec
 
 
 # ---------------------------------------------------------------------------
@@ -178,13 +243,41 @@ def grid_explicit(rows: np.ndarray) -> tuple[GridDesc, np.ndarray]:
 
 
 def solver(abs_tol=1e-12, rel_tol=1e-8, stepper=STEPPER_RKF78, precision=PREC_FP64,
-           proposer=PROPOSER_NONE, magnus_substeps=1, tile_k=0) -> SolverOpts:
+           proposer=PROPOSER_NONE, magnus_substeps=1, tile_k=0, mlp: "Mlp | None" = None,
+           mlp_every=16) -> SolverOpts:
     o = SolverOpts()
     load_library().hhg_default_solver_opts(ctypes.byref(o))
     o.abs_tol, o.rel_tol = abs_tol, rel_tol
     o.stepper, o.precision, o.proposer = stepper, precision, proposer
     o.magnus_substeps, o.tile_k = magnus_substeps, tile_k
+    if mlp is not None:
+        o.mlp = ctypes.pointer(mlp)
+        o._mlp_ref = mlp  # keep the network alive as long as the options
+    o.mlp_every = mlp_every
     return o
+
+
+def train_opts(**kw) -> TrainOpts:
+    o = TrainOpts()
+    load_library().hhg_default_train_opts(ctypes.byref(o))
+    for k, v in kw.items():
+        if not hasattr(o, k):
+            raise AttributeError(k)
+        setattr(o, k, v)
+    return o
+
+
+def mlp_init(seed: int = 1, records: np.ndarray | None = None) -> Mlp:
+    """Initial weights from `seed` and, with records, the fitted standardisation."""
+    net = Mlp()
+    if records is None:
+        st = load_library().hhg_mlp_init(seed, None, 0, ctypes.byref(net))
+    else:
+        rec = _records(records)
+        st = load_library().hhg_mlp_init(seed, _fptr(rec), rec.shape[0], ctypes.byref(net))
+    if st != OK:
+        raise HHGError(st, "hhg_mlp_init")
+    return net
 
 
 def gauss_legendre(n: int):
@@ -263,6 +356,50 @@ class Engine:
 
     def plan(self, sys: SystemDesc, pulses, grid: GridDesc, opts: SolverOpts | None = None):
         return Plan(self, sys, pulses, grid, opts)
+
+    def learned_collect(self, sys: SystemDesc, pulses, grid: GridDesc,
+                        opts: SolverOpts | None = None, hist_every: int = 4,
+                        cap: int = 1 << 20) -> tuple[np.ndarray, Stats]:
+        """Step-size history records (n x HIST_FIELDS float32) of a carry run."""
+        pulses = list(pulses) if not isinstance(pulses, PulseDesc) else [pulses]
+        arr = (PulseDesc * len(pulses))(*pulses)
+        rec = np.zeros((cap, HIST_FIELDS), np.float32)
+        n = ctypes.c_int64(0)
+        st = Stats()
+        o = opts if opts is not None else solver()
+        self._check(self.lib.hhg_learned_collect(self.ctx, ctypes.byref(sys), arr, len(pulses),
+                                                 ctypes.byref(grid), ctypes.byref(o), hist_every,
+                                                 _fptr(rec), cap, ctypes.byref(n),
+                                                 ctypes.byref(st)), "hhg_learned_collect")
+        return rec[:n.value].copy(), st
+
+    def mlp_train(self, records: np.ndarray, net: Mlp, opts: TrainOpts | None = None):
+        """Train `net` in place on the GPU; returns (per-epoch loss, device ms)."""
+        rec = _records(records)
+        o = opts if opts is not None else train_opts()
+        loss = np.zeros(o.epochs, np.float32)
+        ms = ctypes.c_double(0.0)
+        self._check(self.lib.hhg_mlp_train(self.ctx, _fptr(rec), rec.shape[0], ctypes.byref(o),
+                                           ctypes.byref(net), _fptr(loss), ctypes.byref(ms)),
+                    "hhg_mlp_train")
+        return loss, ms.value
+
+    def mlp_gradients(self, records: np.ndarray, net: Mlp) -> tuple[np.ndarray, float]:
+        rec = _records(records)
+        g = np.zeros(MLP_N_PARAMS, np.float32)
+        loss = np.zeros(1, np.float32)
+        self._check(self.lib.hhg_mlp_gradients(self.ctx, _fptr(rec), rec.shape[0],
+                                               ctypes.byref(net), _fptr(g), _fptr(loss)),
+                    "hhg_mlp_gradients")
+        return g, float(loss[0])
+
+    def mlp_predict(self, records: np.ndarray, net: Mlp, path: int = 0) -> np.ndarray:
+        rec = _records(records)
+        out = np.zeros(rec.shape[0], np.float32)
+        self._check(self.lib.hhg_mlp_predict(self.ctx, _fptr(rec), rec.shape[0],
+                                             ctypes.byref(net), path, _fptr(out)),
+                    "hhg_mlp_predict")
+        return out
 
     def fp64_peak_tflops(self) -> float:
         v = ctypes.c_double(0.0)

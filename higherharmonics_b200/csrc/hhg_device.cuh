@@ -38,6 +38,10 @@
 #include <stdint.h>
 
 namespace hhg {
+struct MlpPacked;
+}
+
+namespace hhg {
 
 constexpr unsigned kFull = 0xffffffffu;
 constexpr double kDblEps = 2.220446049250313080847e-16;  // std::numeric_limits<double>::epsilon()
@@ -86,12 +90,14 @@ __host__ __device__ constexpr int slot_doubles(int nf, int deg) {
     return slot_table(nf, deg) + ((kMaxStd * 13 * nf + 1) & ~1);
 }
 // Dyadic layout (warp-synchronous stepping): after the header and the
-// interpolants, the exact stage values of every step of size
+// interpolants, A(t0) and E(t0) = -dA/dt(t0), then the exact stage values of
+// every step of size
 // (t1 - t0) / 2^L, L < kDyaLevels, level-major: for L, position q, stage s,
 // function n at index ((2^L - 1 + q) * 13 + s) * nf + n.  Mixed precision
 // stores float pairs in the same 8-byte slots.
 constexpr int kDyaLevels = 3;
-__host__ __device__ constexpr int slot_dyadic(int nf, int deg) { return slot_sched(nf, deg); }
+// [A(t0), E(t0)] then the table
+__host__ __device__ constexpr int slot_dyadic(int nf, int deg) { return slot_sched(nf, deg) + 2; }
 __host__ __device__ constexpr int slot_doubles_dyadic(int nf, int deg) {
     return slot_dyadic(nf, deg) + (((1 << kDyaLevels) - 1) * 13 * nf + 1) / 2 * 2;
 }
@@ -138,7 +144,16 @@ struct KParams {
     double abs_tol, rel_tol;
     double grow_max;      // 0.9 * pow(pow(5, -8), -1/8), computed with the host libm
     double err_floor;     // pow(5, -8)
+    // learned proposer (PROPOSER 3): network and inference period in intervals
+    const MlpPacked *mlp;
+    int mlp_every;
+    // history recording (PROPOSER 4): records of kHistFields floats
+    int hist_every;
+    float *hist;
+    unsigned long long *hist_count;
+    long long hist_cap;
 };
+constexpr int kHistFields = 12;
 
 // ---------------------------------------------------------------------------
 // Pulse: Laser::laser_function with CosineLaser::envelope (Laser.hpp:32-37,
@@ -168,6 +183,10 @@ __device__ __forceinline__ void staged_values(const PulseDev &pd, double A, doub
         for (int n = 0; n < NF / 2; ++n) sincos(pd.s[n] * A, &v[2 * n + 1], &v[2 * n]);
     }
 }
+
+}  // namespace hhg
+#include "hhg_mlp.cuh"
+namespace hhg {
 
 // ---------------------------------------------------------------------------
 // Number types.  The FP64 path works in double throughout.  The mixed path
@@ -591,14 +610,17 @@ __device__ __forceinline__ bool control(const KParams &P, const double *S, const
 // 5^-8)^-1/8.  With USE_STD the warp reads the tabulated pulse values while all
 // active lanes are on the standard schedule.  Called by the whole warp.
 // ---------------------------------------------------------------------------
-template <int M, int NF, int D, typename R, bool USE_STD, bool CARRY>
+template <int M, int NF, int D, typename R, bool USE_STD, bool CARRY, bool REC = false>
 __device__ __forceinline__ void lane_controller(const KParams &P, const ModelState<M, R> &ms,
                                                 const PolyEval<NF, D, R> &poly,
                                                 const double *slot, const typename Num<R>::V *tabv,
                                                 int n_std, double t, double dt, double t1,
                                                 double *S, bool &dead, double &carry_dt,
                                                 unsigned long long &attempts_out,
-                                                unsigned long long &rejects) {
+                                                unsigned long long &rejects,
+                                                const double *row = nullptr,
+                                                const PulseDev *pd = nullptr,
+                                                bool rec_lane = false) {
     constexpr bool kNarrow = sizeof(R) != sizeof(double);
     constexpr int SCHED = slot_sched(NF, D);
     bool active = !dead;
@@ -622,6 +644,30 @@ __device__ __forceinline__ void lane_controller(const KParams &P, const ModelSta
             }
             ++attempts;
             const double dt_used = dt;
+            if (REC && rec_lane && attempts == 1) {
+                // accept/reject history of the interval's first attempt:
+                // features, and the level T = log2(span / h*) of the largest
+                // step with err <= 0.9, h* = h (0.9 / err)^(1/8)
+                double err = 0.0;
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+                    err = fmax(err, fabs(e[c]) / (P.abs_tol + P.rel_tol * (fabs(S[c]) + dt * fabs(k0[c]))));
+                const double span = slot[1] - slot[0];
+                double T = log2(span / dt_used) - (err > 0.0 ? 0.125 * log2(0.9 / err) : 64.0);
+                T = fmin(fmax(T, -1.0), 12.0);
+                const unsigned long long at = atomicAdd(P.hist_count, 1ull);
+                if ((long long)at < P.hist_cap) {
+                    float f[kMlpIn];
+                    mlp_features(row, laser_exact(*pd, t), laser_field(*pd, t), S, log2(dt_used / span), f);
+                    float *o = P.hist + (size_t)at * kHistFields;
+#pragma unroll
+                    for (int c = 0; c < kMlpIn; ++c) o[c] = f[c];
+                    o[8] = float(T);
+                    o[9] = float(dt_used / span);
+                    o[10] = float(err);
+                    o[11] = 0.0f;
+                }
+            }
             if (control<kNarrow>(P, S, e, k0, dt)) {
                 t += dt_used;
                 S[0] = xn[0];
@@ -674,12 +720,19 @@ __device__ __forceinline__ void lane_controller(const KParams &P, const ModelSta
 // power in FP32 (the error norm, the comparison and dt stay FP64).
 // ---------------------------------------------------------------------------
 constexpr int kLevelMax = 10;
+// dynamic shared memory of the learned-proposer kernels
+__host__ __device__ constexpr int mlp_smem_bytes() {
+    return (int)sizeof(MlpSmem) + kWarpsPerBlock * 32 * kLdIn * 2;
+}
 constexpr double kCoarsen = 1.0 / 600.0;
 
 template <int M, int D, typename R, int STEPPER, int PROPOSER>
 __global__ void __launch_bounds__(kBlockThreads, kMinBlocksPerSM) bz_integrate_kernel(const KParams P) {
     constexpr int NF = Traits<M>::NF;
-    constexpr bool kDyadic = PROPOSER >= 2;
+    constexpr bool kDyadic = PROPOSER == 2 || PROPOSER == 3;
+    constexpr bool kLearned = PROPOSER == 3;
+    constexpr bool kCarry = PROPOSER == 1 || PROPOSER == 4;
+    constexpr bool kRecord = PROPOSER == 4;
     constexpr int SLOT = kDyadic ? slot_doubles_dyadic(NF, D) : slot_doubles(NF, D);
     constexpr int SCHED = slot_sched(NF, D);
     constexpr int TAB = slot_table(NF, D);
@@ -692,9 +745,18 @@ __global__ void __launch_bounds__(kBlockThreads, kMinBlocksPerSM) bz_integrate_k
     using V = typename Num<R>::V;
     __shared__ __align__(16) double stage_raw[kWarpsPerBlock][COPY];
     __shared__ __align__(16) V stage_tab[kWarpsPerBlock][kNarrow && PROPOSER == 0 ? NTAB : 1];
+    // learned proposer: the network and per-warp input tiles in dynamic shared
+    // memory (mlp_smem_bytes(); none for the other modes)
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    MlpSmem *mlp_s = reinterpret_cast<MlpSmem *>(dyn_smem);
+    __nv_bfloat16 *mlp_stage = reinterpret_cast<__nv_bfloat16 *>(dyn_smem + sizeof(MlpSmem));
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
     double *slot = stage_raw[wib];
+    if constexpr (kLearned) {
+        mlp_load_smem(P.mlp, mlp_s);
+        __syncthreads();
+    }
     const V *tabv;
     if constexpr (kNarrow && PROPOSER == 0) tabv = stage_tab[wib];
     else tabv = reinterpret_cast<const V *>(slot + (PROPOSER == 0 ? TAB : 0));
@@ -771,12 +833,27 @@ __global__ void __launch_bounds__(kBlockThreads, kMinBlocksPerSM) bz_integrate_k
                         }
                     } else if constexpr (!kDyadic) {
                         const int n_std = (PROPOSER == 0) ? (int)slot[SCHED] : 0;
-                        lane_controller<M, NF, D, R, PROPOSER == 0, PROPOSER == 1>(
-                            P, ms, poly, slot, tabv, n_std, t0, (PROPOSER == 1) ? carry_dt : dt0,
-                            t1, S, dead, carry_dt, my_attempts, my_rejects);
+                        // every lane records every hist_every-th interval, staggered
+                        const bool rec_lane =
+                            kRecord && ((i - 1 + lane + (int)(item & 1023)) % P.hist_every) == 0;
+                        lane_controller<M, NF, D, R, PROPOSER == 0, kCarry, kRecord>(
+                            P, ms, poly, slot, tabv, n_std, t0, kCarry ? carry_dt : dt0,
+                            t1, S, dead, carry_dt, my_attempts, my_rejects, row, &pd, rec_lane);
                     } else {
                         const V *dtab = reinterpret_cast<const V *>(gslot + DYA);
                         const double span = t1 - t0;
+                        if constexpr (kLearned) {
+                            if (((i - 1) % P.mlp_every) == 0) {
+                                // the network proposes each lane's level; the warp takes the
+                                // finest one (dead lanes propose level 0)
+                                float f[kMlpIn];
+                                mlp_features(row, gslot[DYA - 2], gslot[DYA - 1], S, -double(level), f);
+                                const float T = mlp_warp_infer(*mlp_s, f, mlp_stage + wib * 32 * kLdIn);
+                                int want = dead ? 0 : (int)ceilf(T + mlp_s->level_margin);
+                                want = want < 0 ? 0 : (want > kLevelMax ? kLevelMax : want);
+                                level = __reduce_max_sync(kFull, (unsigned)want);
+                            }
+                        }
                         int L = level, qpos = 0;
                         bool fallback = false, coarse_end = false;
                         for (;;) {
@@ -951,6 +1028,8 @@ __global__ void stage_pulses_kernel(const PulseDev *__restrict__ pulses, int n_p
         // dyadic steps: position q of level L starts at t0 + q (t1 - t0) 2^-L
         constexpr int DYA = slot_dyadic(NF, D);
         const double span = t1 - t0;
+        out[DYA - 2] = laser_exact(pd, t0);
+        out[DYA - 1] = laser_field(pd, t0);
         for (int L = 0; L < kDyaLevels; ++L) {
             const double h = ldexp(span, -L);
             for (int q = 0; q < (1 << L); ++q) {

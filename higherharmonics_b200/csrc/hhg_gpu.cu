@@ -55,7 +55,25 @@ struct hhg_plan {
     double2 *d_F = nullptr;
     std::vector<long long> spec_off;  // per pulse offset (in n_fft units) into d_spec
     long long spec_len = 0;
+    // learned proposer: packed network
+    hhg::MlpPacked *d_mlp = nullptr;
+    // step-history recording (hhg_learned_collect)
+    bool record = false;
+    int hist_every = 1;
+    long long hist_cap = 0;
+    float *d_hist = nullptr;
+    unsigned long long *d_hist_count = nullptr;
 };
+
+namespace hhg {
+void pack_mlp(const hhg_mlp &net, MlpPacked *out);
+hhg_status mlp_train_impl(cudaStream_t s, const float *records, int64_t n, const hhg_train_opts &o,
+                          hhg_mlp *net, float *epoch_loss, double *train_ms, std::string *msg);
+hhg_status mlp_gradients_impl(cudaStream_t s, const float *records, int64_t n, const hhg_mlp *net,
+                              float *grad_out, float *loss_out, std::string *msg);
+hhg_status mlp_predict_impl(cudaStream_t s, const float *records, int64_t n, const hhg_mlp *net,
+                            int path, float *out, std::string *msg);
+}  // namespace hhg
 
 namespace {
 
@@ -390,9 +408,15 @@ int kernel_model(const hhg_system_desc &s) {
     return s.kind;
 }
 
-// Kernel step-control mode for an ABI proposer: 0 restart, 1 carry, 2 dyadic.
+// Kernel step-control mode for an ABI proposer: 0 restart, 1 carry, 2 dyadic,
+// 3 learned dyadic.
 int kernel_proposer(int abi) {
-    return abi == HHG_PROPOSER_CARRY ? 1 : (abi == HHG_PROPOSER_NONE ? 0 : 2);
+    switch (abi) {
+    case HHG_PROPOSER_CARRY: return 1;
+    case HHG_PROPOSER_LOCKSTEP: return 2;
+    case HHG_PROPOSER_LEARNED: return 3;
+    default: return 0;
+    }
 }
 
 int model_nf(int m) {
@@ -505,6 +529,8 @@ void hhg_default_solver_opts(hhg_solver_opts *o) {
     o->max_attempts_per_interval = 100000;
     o->tile_k = 0;
     o->block_threads = 128;
+    o->mlp = nullptr;
+    o->mlp_every = 16;
 }
 
 hhg_status hhg_gpu_create(hhg_ctx **out, int device) {
@@ -582,11 +608,17 @@ hhg_status hhg_plan_create(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_p
         return set_err(ctx, HHG_UNSUPPORTED, "Magnus-4 runs in FP64 only");
     if (o.precision != HHG_PREC_FP64 && o.precision != HHG_PREC_MIXED)
         return set_err(ctx, HHG_BAD_CONFIG, "unknown precision");
-    if (o.proposer == HHG_PROPOSER_LEARNED)
-        return set_err(ctx, HHG_UNSUPPORTED, "learned proposer requires a trained network (hhg_learned_*)");
     if (o.proposer != HHG_PROPOSER_NONE && o.proposer != HHG_PROPOSER_CARRY &&
-        o.proposer != HHG_PROPOSER_LOCKSTEP)
+        o.proposer != HHG_PROPOSER_LOCKSTEP && o.proposer != HHG_PROPOSER_LEARNED)
         return set_err(ctx, HHG_BAD_CONFIG, "unknown proposer");
+    if (o.proposer == HHG_PROPOSER_LEARNED) {
+        if (!o.mlp || !(o.mlp->out_sigma > 0.0f))
+            return set_err(ctx, HHG_BAD_CONFIG,
+                           "the learned proposer needs opts.mlp: a network from hhg_mlp_init + hhg_mlp_train");
+        if (o.mlp_every < 1) return set_err(ctx, HHG_BAD_CONFIG, "mlp_every must be >= 1");
+        if (o.stepper != HHG_STEPPER_RKF78)
+            return set_err(ctx, HHG_UNSUPPORTED, "the learned proposer drives the RKF78 stepper");
+    }
     if (!(o.abs_tol >= 0.0) || !(o.rel_tol >= 0.0) || !(o.abs_tol + o.rel_tol > 0.0))
         return set_err(ctx, HHG_BAD_CONFIG, "tolerances must be >= 0 and not both 0");
     if (o.max_failed_steps < 1) o.max_failed_steps = 500;
@@ -640,7 +672,7 @@ hhg_status hhg_plan_create(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_p
         degree = std::max(degree, d);
     }
     pl->degree = degree;
-    const bool dyadic = o.proposer == HHG_PROPOSER_LOCKSTEP;
+    const bool dyadic = o.proposer == HHG_PROPOSER_LOCKSTEP || o.proposer == HHG_PROPOSER_LEARNED;
     const int slot = dyadic ? hhg::slot_doubles_dyadic(nf, degree) : hhg::slot_doubles(nf, degree);
 
     // work decomposition
@@ -764,6 +796,15 @@ hhg_status hhg_plan_create(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_p
     if ((e = cudaMalloc(&pl->d_ioff, ioff.size() * sizeof(long long))) != cudaSuccess) return fail("alloc offsets", e);
     if ((e = cudaMalloc(&pl->d_counters, 8 * sizeof(unsigned long long))) != cudaSuccess) return fail("alloc counters", e);
     if ((e = cudaMalloc(&pl->d_status, sizeof(int))) != cudaSuccess) return fail("alloc status", e);
+    if (o.proposer == HHG_PROPOSER_LEARNED) {
+        hhg::MlpPacked packed;
+        hhg::pack_mlp(*o.mlp, &packed);
+        if ((e = cudaMalloc(&pl->d_mlp, sizeof packed)) != cudaSuccess) return fail("alloc network", e);
+        // synchronous: `packed` lives on this stack frame
+        if ((e = cudaMemcpy(pl->d_mlp, &packed, sizeof packed, cudaMemcpyHostToDevice)) != cudaSuccess)
+            return fail("upload network", e);
+        pl->opts.mlp = nullptr;  // the plan keeps its device copy only
+    }
     if ((e = cudaMemcpyAsync(pl->d_ktab, ktab.data(), ktab.size() * sizeof(double), cudaMemcpyHostToDevice, s)) != cudaSuccess) return fail("upload k table", e);
     if ((e = cudaMemcpyAsync(pl->d_pulses, pl->pulses.data(), n_pulses * sizeof(PulseDev), cudaMemcpyHostToDevice, s)) != cudaSuccess) return fail("upload pulses", e);
     if ((e = cudaMemcpyAsync(pl->d_tgrid, tgrid.data(), tgrid.size() * sizeof(double), cudaMemcpyHostToDevice, s)) != cudaSuccess) return fail("upload tgrid", e);
@@ -811,6 +852,9 @@ void hhg_plan_destroy(hhg_plan *pl) {
     cudaFree(pl->d_spec);
     cudaFree(pl->d_x);
     cudaFree(pl->d_F);
+    cudaFree(pl->d_mlp);
+    cudaFree(pl->d_hist);
+    cudaFree(pl->d_hist_count);
     delete pl;
 }
 
@@ -843,10 +887,16 @@ hhg_status hhg_plan_execute_async(hhg_plan *pl, void *stream) {
     lr.kp.rel_tol = pl->opts.rel_tol;
     lr.kp.err_floor = pow(5.0, -8.0);
     lr.kp.grow_max = 9.0 / 10.0 * pow(pow(5.0, -8.0), -1.0 / 8);
+    lr.kp.mlp = pl->d_mlp;
+    lr.kp.mlp_every = std::max(pl->opts.mlp_every, 1);
+    lr.kp.hist_every = pl->hist_every;
+    lr.kp.hist = pl->d_hist;
+    lr.kp.hist_count = pl->d_hist_count;
+    lr.kp.hist_cap = pl->hist_cap;
     lr.degree = pl->degree;
     lr.precision = pl->opts.precision;
     lr.stepper = pl->opts.stepper;
-    lr.proposer = kernel_proposer(pl->opts.proposer);
+    lr.proposer = pl->record ? 4 : kernel_proposer(pl->opts.proposer);
     lr.grid = pl->grid;
     lr.stream = s;
     lr.occupancy_out = nullptr;
@@ -1150,3 +1200,91 @@ hhg_status prepare_pulse(const hhg_system_desc *sys, const hhg_pulse_desc *pulse
 }
 
 }  // namespace hhg_prep
+
+// ---------------------------------------------------------------------------
+// Learned step-size proposer: collection and the training entry points
+// ---------------------------------------------------------------------------
+extern "C" {
+
+hhg_status hhg_learned_collect(hhg_ctx *ctx, const hhg_system_desc *sys,
+                               const hhg_pulse_desc *pulses, int n_pulses,
+                               const hhg_grid_desc *grid, const hhg_solver_opts *opts,
+                               int hist_every, float *records, int64_t cap, int64_t *n_records,
+                               hhg_stats *stats) {
+    if (!ctx) return HHG_BAD_CONFIG;
+    if (hist_every < 1 || cap < 0 || (cap > 0 && !records) || cap > ((int64_t)1 << 31))
+        return set_err(ctx, HHG_BAD_CONFIG, "hist_every >= 1, 0 <= cap <= 2^31, records for cap > 0");
+    hhg_solver_opts o;
+    hhg_default_solver_opts(&o);
+    if (opts) o = *opts;
+    o.stepper = HHG_STEPPER_RKF78;
+    o.precision = HHG_PREC_FP64;
+    o.proposer = HHG_PROPOSER_CARRY;
+    o.mlp = nullptr;
+    hhg_plan *pl = nullptr;
+    hhg_status st = hhg_plan_create(ctx, sys, pulses, n_pulses, grid, &o, &pl);
+    if (st != HHG_OK) return st;
+    pl->record = true;
+    pl->hist_every = hist_every;
+    pl->hist_cap = cap;
+    cudaError_t e;
+    if ((e = cudaMalloc(&pl->d_hist, sizeof(float) * HHG_HIST_FIELDS * std::max<int64_t>(cap, 1))) != cudaSuccess ||
+        (e = cudaMalloc(&pl->d_hist_count, sizeof(unsigned long long))) != cudaSuccess) {
+        hhg_plan_destroy(pl);
+        return set_err(ctx, HHG_CUDA_ERROR, std::string("alloc history: ") + cudaGetErrorString(e));
+    }
+    cudaMemsetAsync(pl->d_hist_count, 0, sizeof(unsigned long long), ctx->stream);
+    st = hhg_plan_execute_async(pl, nullptr);
+    if (st == HHG_OK) st = hhg_plan_fetch(pl, nullptr, stats);
+    if (st == HHG_OK) {
+        unsigned long long cnt = 0;
+        if ((e = cudaMemcpy(&cnt, pl->d_hist_count, sizeof cnt, cudaMemcpyDeviceToHost)) != cudaSuccess) {
+            hhg_plan_destroy(pl);
+            return set_err(ctx, HHG_CUDA_ERROR, std::string("read history count: ") + cudaGetErrorString(e));
+        }
+        const int64_t n = std::min<int64_t>((int64_t)cnt, cap);
+        if (n > 0 &&
+            (e = cudaMemcpy(records, pl->d_hist, sizeof(float) * HHG_HIST_FIELDS * n, cudaMemcpyDeviceToHost)) !=
+                cudaSuccess) {
+            hhg_plan_destroy(pl);
+            return set_err(ctx, HHG_CUDA_ERROR, std::string("read history: ") + cudaGetErrorString(e));
+        }
+        if (n_records) *n_records = n;
+    }
+    hhg_plan_destroy(pl);
+    return st;
+}
+
+hhg_status hhg_mlp_train(hhg_ctx *ctx, const float *records, int64_t n_records,
+                         const hhg_train_opts *opts, hhg_mlp *net, float *epoch_loss,
+                         double *train_ms) {
+    if (!ctx) return HHG_BAD_CONFIG;
+    HHG_CUDA(ctx, cudaSetDevice(ctx->device));
+    hhg_train_opts o;
+    hhg_default_train_opts(&o);
+    if (opts) o = *opts;
+    std::string msg;
+    const hhg_status st =
+        hhg::mlp_train_impl(ctx->stream, records, n_records, o, net, epoch_loss, train_ms, &msg);
+    return st == HHG_OK ? st : set_err(ctx, st, msg);
+}
+
+hhg_status hhg_mlp_gradients(hhg_ctx *ctx, const float *records, int64_t n_records,
+                             const hhg_mlp *net, float *grad_out, float *loss_out) {
+    if (!ctx) return HHG_BAD_CONFIG;
+    HHG_CUDA(ctx, cudaSetDevice(ctx->device));
+    std::string msg;
+    const hhg_status st = hhg::mlp_gradients_impl(ctx->stream, records, n_records, net, grad_out, loss_out, &msg);
+    return st == HHG_OK ? st : set_err(ctx, st, msg);
+}
+
+hhg_status hhg_mlp_predict(hhg_ctx *ctx, const float *records, int64_t n_records,
+                           const hhg_mlp *net, int path, float *level_out) {
+    if (!ctx) return HHG_BAD_CONFIG;
+    HHG_CUDA(ctx, cudaSetDevice(ctx->device));
+    std::string msg;
+    const hhg_status st = hhg::mlp_predict_impl(ctx->stream, records, n_records, net, path, level_out, &msg);
+    return st == HHG_OK ? st : set_err(ctx, st, msg);
+}
+
+}  // extern "C"

@@ -12,7 +12,8 @@ struct LaunchReq {
     int degree;     // 5, 7 or 11
     int precision;  // 0 FP64, 1 mixed (FP32 right-hand side)
     int stepper;    // 0 RKF78, 1 Magnus-4
-    int proposer;   // 0 restart at dt0, 1 carry, 2 warp-synchronous dyadic
+    int proposer;   // 0 restart at dt0, 1 carry, 2 warp-synchronous dyadic, 3 learned dyadic,
+                    // 4 carry + history recording
     int grid;       // CTAs; 0 = query occupancy only
     cudaStream_t stream;
     int *occupancy_out;  // blocks per SM for the selected variant (if non-null)
@@ -34,12 +35,13 @@ struct StageReq {
 template <int M, int D, typename R, int ST, int PR>
 cudaError_t launch_one(const LaunchReq &r) {
     auto kern = bz_integrate_kernel<M, D, R, ST, PR>;
+    const int dyn = PR == 3 ? mlp_smem_bytes() : 0;
     if (r.occupancy_out) {
-        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(r.occupancy_out, kern, kBlockThreads, 0);
+        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(r.occupancy_out, kern, kBlockThreads, dyn);
         if (e != cudaSuccess) return e;
     }
     if (r.grid <= 0) return cudaSuccess;
-    kern<<<r.grid, kBlockThreads, 0, r.stream>>>(r.kp);
+    kern<<<r.grid, kBlockThreads, dyn, r.stream>>>(r.kp);
     return cudaGetLastError();
 }
 
@@ -47,13 +49,22 @@ template <int M, int D>
 cudaError_t launch_deg(const LaunchReq &r) {
     if (r.stepper == 1) return launch_one<M, D, double, 1, 0>(r);
     if (r.precision == 0) {
-        if (r.proposer == 0) return launch_one<M, D, double, 0, 0>(r);
-        if (r.proposer == 1) return launch_one<M, D, double, 0, 1>(r);
-        return launch_one<M, D, double, 0, 2>(r);
+        switch (r.proposer) {
+        case 0: return launch_one<M, D, double, 0, 0>(r);
+        case 1: return launch_one<M, D, double, 0, 1>(r);
+        case 2: return launch_one<M, D, double, 0, 2>(r);
+        case 3: return launch_one<M, D, double, 0, 3>(r);
+        case 4: return launch_one<M, D, double, 0, 4>(r);
+        }
+        return cudaErrorInvalidValue;
     }
-    if (r.proposer == 0) return launch_one<M, D, float, 0, 0>(r);
-    if (r.proposer == 1) return launch_one<M, D, float, 0, 1>(r);
-    return launch_one<M, D, float, 0, 2>(r);
+    switch (r.proposer) {
+    case 0: return launch_one<M, D, float, 0, 0>(r);
+    case 1: return launch_one<M, D, float, 0, 1>(r);
+    case 2: return launch_one<M, D, float, 0, 2>(r);
+    case 3: return launch_one<M, D, float, 0, 3>(r);
+    }
+    return cudaErrorInvalidValue;
 }
 
 template <int M>

@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define HHG_ABI_VERSION 1
+#define HHG_ABI_VERSION 2
 
 /* Errors: the reference throws std::invalid_argument / std::runtime_error
  * (sources/hhg.cpp:232, Dispatch/PiFluxDispatcher.cpp:104) and Boost.Odeint
@@ -136,7 +136,48 @@ typedef struct hhg_solver_opts {
     int32_t max_attempts_per_interval;
     int32_t tile_k;
     int32_t block_threads;
+    const struct hhg_mlp *mlp; /* HHG_PROPOSER_LEARNED: the trained network (host memory) */
+    int32_t mlp_every;         /* intervals between network proposals (>= 1, default 16) */
+    int32_t reserved;
 } hhg_solver_opts;
+
+/* The learned step-size proposer (no counterpart in the reference, whose
+ * controller restarts every interval at measure_every / n_subdivisions):
+ * an MLP 8 -> 64 -> 64 -> 64 -> 1 with SiLU after the first three layers,
+ * BF16 weights and activations, FP32 accumulation.  Inputs per k-point at the
+ * start of a measurement interval: kx/pi, ky/pi, A(t0), E(t0) = -dA/dt, the
+ * Bloch vector S(t0), log2(h / interval); output: the level
+ * T = log2(interval / h*) of the largest step h* the RKF78 error norm accepts
+ * (with a 0.9 safety factor).  A warp of 32 k-points steps at level
+ * max ceil(T + level_margin).  params: w1[64][8], b1[64], w2[64][64], b2[64],
+ * w3[64][64], b3[64], w4[64], b4 (row-major [out][in]); inputs are
+ * standardised by (x - in_mu) * in_isig, the output de-standardised by
+ * T = y * out_sigma + out_mu. */
+#define HHG_MLP_INPUTS 8
+#define HHG_MLP_HIDDEN 64
+#define HHG_MLP_N_PARAMS (64 * 8 + 64 + 64 * 64 + 64 + 64 * 64 + 64 + 64 + 1)
+typedef struct hhg_mlp {
+    float params[HHG_MLP_N_PARAMS];
+    float in_mu[HHG_MLP_INPUTS];
+    float in_isig[HHG_MLP_INPUTS];
+    float out_mu, out_sigma;
+    float level_margin;
+    float reserved;
+} hhg_mlp;
+
+/* One training record (floats): the 8 raw inputs, the target level T,
+ * h / interval of the recorded attempt, its error norm, 0. */
+#define HHG_HIST_FIELDS 12
+
+typedef struct hhg_train_opts {
+    int32_t epochs;
+    int32_t batch;      /* rows per Adam step (multiple of 128) */
+    float lr;           /* Adam step size */
+    float beta1, beta2, eps;
+    float lr_final;     /* cosine decay from lr to lr_final over all steps */
+    int32_t reserved;
+    uint64_t seed;      /* batch order */
+} hhg_train_opts;
 
 typedef struct hhg_stats {
     int64_t k_points;
@@ -245,6 +286,46 @@ hhg_status hhg_gpu_current_density_noalloc(const hhg_system_desc *sys,
                                            int64_t n_rows, const hhg_solver_opts *opts,
                                            double *d_j_out, void *stream, hhg_stats *stats,
                                            char *err, size_t err_cap);
+
+/* Learned step-size proposer: collection, training and inference.  None has
+ * a counterpart in the reference.
+ *
+ * hhg_learned_collect runs the integration with the carry controller in FP64
+ * (opts' tolerances and limits; its proposer and precision are ignored) and
+ * records, for every hist_every-th interval of each lane (staggered across
+ * lanes), the interval's first attempt as one HHG_HIST_FIELDS record:
+ * inputs, and T = log2(interval / h) - log2(0.9 / err) / 8 clamped to
+ * [-1, 12].  Up to cap records go to `records` (host); n_records receives
+ * the number written. */
+hhg_status hhg_learned_collect(hhg_ctx *ctx, const hhg_system_desc *sys,
+                               const hhg_pulse_desc *pulses, int n_pulses,
+                               const hhg_grid_desc *grid, const hhg_solver_opts *opts,
+                               int hist_every, float *records, int64_t cap, int64_t *n_records,
+                               hhg_stats *stats);
+void hhg_default_train_opts(hhg_train_opts *opts);
+/* Deterministic initial weights (uniform +-1/sqrt(fan_in), from `seed`) and,
+ * when records != NULL, the input / output standardisation fitted to them
+ * (mean and 1 / standard deviation per input; mean and standard deviation of
+ * T).  level_margin is set to 0.25. */
+hhg_status hhg_mlp_init(uint64_t seed, const float *records, int64_t n_records, hhg_mlp *net);
+/* Adam on the mean squared error of the standardised level, on the GPU: the
+ * forward and backward GEMMs run on the tensor cores (tcgen05, BF16 inputs,
+ * FP32 accumulation in tensor memory), Adam on FP32 master weights.  net
+ * holds the initial weights and the standardisation on entry and the trained
+ * weights on return.  epoch_loss (optional, epochs entries) receives the mean
+ * batch loss of each epoch; train_ms (optional) the device time. */
+hhg_status hhg_mlp_train(hhg_ctx *ctx, const float *records, int64_t n_records,
+                         const hhg_train_opts *opts, hhg_mlp *net, float *epoch_loss,
+                         double *train_ms);
+/* Loss and its gradient with respect to params (HHG_MLP_N_PARAMS floats) over
+ * n_records records (<= 1 << 20) as one batch, by the training kernels. */
+hhg_status hhg_mlp_gradients(hhg_ctx *ctx, const float *records, int64_t n_records,
+                             const hhg_mlp *net, float *grad_out, float *loss_out);
+/* Predicted level T for n_records records: path 0 = the warp-level inference
+ * used inside the integration kernel (mma.sync), path 1 = the training
+ * forward pass (tcgen05). */
+hhg_status hhg_mlp_predict(hhg_ctx *ctx, const float *records, int64_t n_records,
+                           const hhg_mlp *net, int path, float *level_out);
 
 #ifdef __cplusplus
 }

@@ -31,7 +31,7 @@ def test_library_exports_every_declared_symbol():
     missing = [n for n in names if not hasattr(lib, n)]
     assert not missing, missing
     assert set(names) == set(api.EXPORTED)
-    assert lib.hhg_abi_version() == 1
+    assert lib.hhg_abi_version() == api.ABI_VERSION
 
 
 def _c_layout():
@@ -43,7 +43,12 @@ def _c_layout():
                                  "n_rows"],
                "hhg_solver_opts": ["stepper", "precision", "proposer", "magnus_substeps",
                                    "abs_tol", "rel_tol", "max_failed_steps",
-                                   "max_attempts_per_interval", "tile_k", "block_threads"],
+                                   "max_attempts_per_interval", "tile_k", "block_threads",
+                                   "mlp", "mlp_every", "reserved"],
+               "hhg_mlp": ["params", "in_mu", "in_isig", "out_mu", "out_sigma", "level_margin",
+                           "reserved"],
+               "hhg_train_opts": ["epochs", "batch", "lr", "beta1", "beta2", "eps", "lr_final",
+                                  "reserved", "seed"],
                "hhg_stats": ["k_points", "trajectories", "attempted_steps", "rejected_steps",
                              "failed_trajectories", "poly_degree", "items", "kernel_ms",
                              "total_ms"]}
@@ -70,7 +75,8 @@ def test_ctypes_layout_matches_c():
     lay = _c_layout()
     for cname, py in [("hhg_system_desc", api.SystemDesc), ("hhg_pulse_desc", api.PulseDesc),
                       ("hhg_grid_desc", api.GridDesc), ("hhg_solver_opts", api.SolverOpts),
-                      ("hhg_stats", api.Stats)]:
+                      ("hhg_stats", api.Stats), ("hhg_mlp", api.Mlp),
+                      ("hhg_train_opts", api.TrainOpts)]:
         assert lay[(cname, "size")] == ctypes.sizeof(py), cname
         for fname, _ in py._fields_:
             if (cname, fname) in lay:

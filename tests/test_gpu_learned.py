@@ -1,0 +1,145 @@
+"""GPU checks of the learned step-size proposer through the C ABI.
+
+- the tensor-core (tcgen05) training kernels' loss and gradients against the
+  CPU oracle's BF16-emulating backward pass (ragged batch: not a multiple of
+  the 128-row tile);
+- both inference paths (the training forward on tcgen05, and the warp-level
+  mma.sync inference inside the integration kernel) against the oracle;
+- training lowers the loss on a smooth synthetic target;
+- collection -> training -> the learned proposer on a pi-flux workload: its
+  spectrum stays within the 1e-4 harmonic bar of the plain FP64 path, and it
+  needs at least 3x fewer RKF78 attempts than the reference's controller
+  (the method without a proposer, which restarts every interval at
+  measure_every / n_subdivisions).
+"""
+import math
+
+import numpy as np
+import pytest
+
+from higherharmonics_b200 import api
+from higherharmonics_b200.analysis import default_max_order, harmonic_intensities, harmonic_rel_err
+from oracle import mlp_oracle as MO
+from tests.helpers import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+GRAD_TOL = 1e-3      # relative L2 per parameter block, GPU vs BF16-emulating oracle
+PRED_TOL_TC = 2e-3   # levels, tcgen05 forward vs oracle (same FP32 SiLU, BF16 roundings)
+PRED_TOL_WARP = 0.1  # levels, BF16 tanh-form SiLU of the in-kernel inference vs its emulation
+
+
+def _synthetic(n, seed=3):
+    rng = np.random.default_rng(seed)
+    rec = np.zeros((n, api.HIST_FIELDS), np.float32)
+    rec[:, :8] = rng.normal(size=(n, 8)) * np.array([0.5, 0.5, 1.0, 0.05, 0.6, 0.6, 0.5, 2.0]) + \
+        np.array([0.0, 0.0, 0.0, 0.0, 0.0, 0.0, -0.5, -3.0])
+    x = rec[:, :8].astype(np.float64)
+    rec[:, 8] = 2.0 + np.sin(3 * x[:, 0]) + 0.5 * x[:, 2] ** 2 + 4 * np.abs(x[:, 3]) + 0.3 * x[:, 7]
+    return rec
+
+
+def _args(net):
+    return (np.array(net.in_mu), np.array(net.in_isig), net.out_mu, net.out_sigma)
+
+
+@pytest.mark.parametrize("n", [3000, 128, 1])
+def test_gradients_match_oracle(engine, n):
+    rec = _synthetic(n)
+    net = api.mlp_init(7, _synthetic(4096))
+    g, loss = engine.mlp_gradients(rec, net)
+    loss_ref, g_ref = MO.loss_and_grad(net.param_array(), rec, *_args(net), emulate=True)
+    assert abs(loss - loss_ref) <= 1e-4 * max(loss_ref, 1e-6)
+    o = 0
+    for name, shape in MO.LAYOUT:
+        k = int(np.prod(shape))
+        a, b = g[o:o + k].astype(np.float64), g_ref[o:o + k]
+        err = np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30)
+        assert err <= GRAD_TOL, (name, err)
+        o += k
+
+
+def test_predictions_match_oracle(engine):
+    rec = _synthetic(1000)  # 1000 = 31 full warps + a ragged one; 7 full tiles + a ragged one
+    net = api.mlp_init(5, rec)
+    engine.mlp_train(rec, net, api.train_opts(epochs=3, batch=256))  # non-trivial weights
+    tc = engine.mlp_predict(rec, net, path=1)
+    ref = MO.predict(net.param_array(), rec, *_args(net), emulate=True)
+    assert np.max(np.abs(tc - ref)) <= PRED_TOL_TC
+    warp = engine.mlp_predict(rec, net, path=0)
+    ref_w = MO.predict(net.param_array(), rec, *_args(net), emulate=True, act="bf16_tanh")
+    assert np.max(np.abs(warp - ref_w)) <= PRED_TOL_WARP
+    assert np.median(np.abs(warp - ref)) <= 0.05
+
+
+def test_training_reduces_loss(engine):
+    rec = _synthetic(1 << 16)
+    net = api.mlp_init(1, rec)
+    loss, ms = engine.mlp_train(rec, net, api.train_opts(epochs=8))
+    assert np.all(np.isfinite(loss)) and ms > 0
+    assert loss[-1] < 0.3 * loss[0], loss
+    assert np.all(np.diff(loss[2:]) < 0.02), loss
+    pred = engine.mlp_predict(rec, net, path=1)
+    resid = pred - rec[:, 8]
+    assert np.sqrt(np.mean(resid ** 2)) < 0.5 * rec[:, 8].std()
+
+
+def test_bad_training_inputs_are_rejected(engine):
+    rec = _synthetic(64)
+    net = api.mlp_init(1, rec)
+    with pytest.raises(api.HHGError):
+        engine.mlp_train(rec, net)  # fewer than 128 records
+    with pytest.raises(api.HHGError):
+        engine.mlp_train(_synthetic(1024), net, api.train_opts(batch=100))
+    bad = api.Mlp()  # out_sigma = 0: no standardisation
+    with pytest.raises(api.HHGError):
+        engine.mlp_predict(rec, bad)
+    s = 1 / math.sqrt(2)
+    sys = api.system(api.SYS_PIFLUX2D, hopping=1.0, pol=(s, s))
+    pulse = api.cosine_pulse(1.0, 2, 256, window=(0.0, 6 * math.pi), energy_scale=20.0)
+    grid = api.grid_tensor(8, 8, -math.pi, math.pi, -math.pi, math.pi)
+    with pytest.raises(api.HHGError):
+        engine.current_density(sys, pulse, grid, api.solver(proposer=api.PROPOSER_LEARNED))
+
+
+def _spectrum(engine, j, p):
+    return engine.spectrum(j, p.n_measurements, p.window_begin, p.window_end)
+
+
+def test_learned_proposer_end_to_end(engine):
+    s = 1 / math.sqrt(2)
+    sys = api.system(api.SYS_PIFLUX2D, hopping=1.0, pol=(s, s))
+    pulse = api.cosine_pulse(1.0, 2, 2048, window=(0.0, 6 * math.pi), energy_scale=20.0)
+    grid = api.grid_tensor(64, 64, -math.pi, math.pi, -math.pi, math.pi)
+    ref_opts = api.solver(1e-12, 1e-8)
+    recs, cst = engine.learned_collect(sys, pulse, grid, ref_opts, hist_every=4, cap=1 << 21)
+    assert recs.shape[0] == 64 * 64 * 2048 // 4
+    assert np.all(np.isfinite(recs[:, :11]))
+    assert np.all((recs[:, 8] >= -1.0) & (recs[:, 8] <= 12.0))
+    net = api.mlp_init(1, recs)
+    loss, _ = engine.mlp_train(recs, net, api.train_opts(epochs=4))
+    assert loss[-1] < loss[0]
+
+    j_ref, st_ref = engine.current_density(sys, pulse, grid, ref_opts)
+    fr = _spectrum(engine, j_ref, pulse)
+    mo = default_max_order(fr[0])
+    I_ref = harmonic_intensities(*fr, mo)
+    runs = {}
+    for name, opts in {
+        "learned": api.solver(1e-12, 1e-8, proposer=api.PROPOSER_LEARNED, mlp=net),
+        "learned_every1": api.solver(1e-12, 1e-8, proposer=api.PROPOSER_LEARNED, mlp=net,
+                                     mlp_every=1),
+        "mixed_learned": api.solver(1e-8, 1e-6, precision=api.PREC_MIXED,
+                                    proposer=api.PROPOSER_LEARNED, mlp=net),
+    }.items():
+        j, st = engine.current_density(sys, pulse, grid, opts)
+        herr = harmonic_rel_err(harmonic_intensities(*_spectrum(engine, j, pulse), mo), I_ref)
+        runs[name] = (herr, rel_l2(j, j_ref), st)
+        assert herr <= 1e-4, (name, herr)
+        assert rel_l2(j, j_ref) <= 1e-4, (name, rel_l2(j, j_ref))
+        assert st.failed_trajectories == 0
+        # gain over the reference's restart controller at the same tolerances
+        assert 3 * st.attempted_steps <= st_ref.attempted_steps, (name, st.attempted_steps,
+                                                                  st_ref.attempted_steps)
+    # the FP64 learned run is as accurate as the plain path's own tolerance allows
+    assert runs["learned"][1] <= 1e-7
