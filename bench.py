@@ -201,10 +201,12 @@ def reference_arm(args, wl_name):
     return 0
 
 
-def config_for(wl, variant_desc):
+def config_for(wl, variant_desc, okw=None):
     p = wl.pulses[0]
+    tol = dict(wl.opts_kw)
+    tol.update({k: v for k, v in (okw or {}).items() if k in ("abs_tol", "rel_tol")})
     return {"workload": wl.name, "k_points": wl.n_k, "n_measurements": p.n_measurements,
-            "pulses": len(wl.pulses), "tolerances": f"{wl.opts_kw['abs_tol']:g}/{wl.opts_kw['rel_tol']:g}",
+            "pulses": len(wl.pulses), "tolerances": f"{tol['abs_tol']:g}/{tol['rel_tol']:g}",
             "variant": variant_desc,
             "l2": "flushed (256 MiB write) before every timed step; inputs < L2"}
 
@@ -223,6 +225,40 @@ def traffic_from_profile(wl_name):
             except ValueError:
                 return None
     return None
+
+
+def compare_variants(args, eng, wl, api, stream, flush, main_variant):
+    """spectra/s of the plain FP64 path and of the learned mixed-precision
+    path on the same workload, same timing method (CUDA events over K graph
+    launches, L2 flushed before each): the learned+FP32 vs plain FP64 ratio."""
+    import torch
+    out = {}
+    for v in ("fp64", "mixed_learned", "mixed_lockstep"):
+        if v == main_variant:
+            continue
+        okw = dict(VARIANTS[v])
+        if okw.get("proposer") == api.PROPOSER_LEARNED:
+            okw["mlp"], _ = train_proposer(eng, wl, api)
+        plan = eng.plan(wl.system, wl.pulses, wl.grid, wl.opts(**okw))
+        plan.autotune(reps=1)
+        sptr = stream.cuda_stream
+        for _ in range(3):
+            flush.zero_()
+            plan.execute_graph(sptr, with_spectrum=True)
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(args.steps):
+            flush.zero_()
+            plan.execute_graph(sptr, with_spectrum=True)
+        b.record(stream)
+        torch.cuda.synchronize()
+        _, st = plan.fetch(copy_j=False)
+        out[v] = {"value": args.steps / (a.elapsed_time(b) * 1e-3), "unit": UNIT,
+                  "k_steps_per_spectrum": st.attempted_steps}
+        plan.close()
+    return out
 
 
 def our_arm(args, wl_name):
@@ -251,6 +287,7 @@ def our_arm(args, wl_name):
         net, training = train_proposer(eng, wl, api)
         okw["mlp"] = net
     plan = eng.plan(wl.system, wl.pulses, wl.grid, wl.opts(**okw))
+    tune = plan.autotune(reps=2)
     # a dedicated stream: the legacy default stream has handle 0, which the
     # C ABI reads as "the context's own stream"
     stream = torch.cuda.Stream()
@@ -261,8 +298,7 @@ def our_arm(args, wl_name):
 
     def step():
         flush.zero_()
-        plan.execute_async(sptr)
-        plan.spectrum_async(sptr)
+        plan.execute_graph(sptr, with_spectrum=True)
 
     for _ in range(args.warmup):
         step()
@@ -305,9 +341,8 @@ def our_arm(args, wl_name):
     for k in range(args.steps):
         flush.zero_()
         ev[k][0].record(stream)
-        plan.execute_async(sptr)
+        plan.execute_graph(sptr, with_spectrum=True)
         ev[k][1].record(stream)
-        plan.spectrum_async(sptr)
     e_end.record(stream)
     torch.cuda.synchronize()
     if ws > 1:
@@ -321,6 +356,10 @@ def our_arm(args, wl_name):
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         elapsed_ms = float(t.item())
     value = ws * args.steps / (elapsed_ms * 1e-3)
+    # the integration kernel's own duration in the last timed launch (event
+    # nodes inside the graph, on the launching stream)
+    _, st_last = plan.fetch(copy_j=False)
+    kernel_ms_last = st_last.kernel_ms
 
     # end to end through the public API with host buffers
     e2e = None
@@ -356,13 +395,16 @@ def our_arm(args, wl_name):
             torch.distributed.destroy_process_group()
         return 0
     avg_launch_s = float(np.mean(launch_ms)) * 1e-3
+    kernel_s = kernel_ms_last * 1e-3 if kernel_ms_last > 0 else avg_launch_s
     alg = ALG_FLOPS_PER_KSTEP.get(wl_name, 421) * ksteps
-    achieved = alg / avg_launch_s / 1e12
+    achieved = alg / kernel_s / 1e12
     roofline = {"bound": "fp64_pipe", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": achieved / peak, "traffic": traffic_from_profile(wl_name),
                 "peak_source": "measured FP64 FMA throughput (hhg_measure_fp64_peak, burst); "
                                "MEASURED_PEAKS.json has no FP64 figure",
-                "kernel": "bz_integrate_kernel", "kernel_ms": 1e3 * avg_launch_s,
+                "kernel": "bz_integrate_kernel", "kernel_ms": 1e3 * kernel_s,
+                "kernel_ms_source": "CUDA events around the integration kernel inside the graph, "
+                                    "last timed step",
                 "alg_flops_per_kstep": ALG_FLOPS_PER_KSTEP.get(wl_name, 421),
                 "special_ops_per_kstep": SPECIAL_OPS_PER_KSTEP.get(wl_name, 0)}
     line = {
@@ -370,11 +412,14 @@ def our_arm(args, wl_name):
         "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None,
         "dtype": "f64" if VARIANTS[args.variant].get("precision", 0) == 0 else "f32 rhs / f64 state",
-        "data": "synthetic", "config": config_for(wl, args.variant),
-        "k_steps_per_s": ws * ksteps / avg_launch_s if ws == 1 else None,
+        "data": "synthetic", "config": config_for(wl, args.variant, VARIANTS[args.variant]),
+        "k_steps_per_s": ws * ksteps / kernel_s if ws == 1 else None,
         "k_steps_per_spectrum": ksteps, "harmonic_err_vs_fp64": herr,
         "gpu_launches": 4 * args.steps, "roofline": roofline, "clocks": clocks, "e2e": e2e,
         "training": training,
+        "autotune": {"chosen": tune.as_list()[tune.best], "candidates": tune.as_list()},
+        "path": "plan with autotuned work decomposition, one CUDA graph launch per spectrum "
+                "(integration + BZ reduction + trapezoidal FFT)",
         "timing": {"device_ms_total": elapsed_ms, "launch_ms": launch_ms,
                    "mean_step_ms_between_launch_starts": (step_sum_ms / (args.steps - 1)
                                                           if args.steps > 1 else None)},
@@ -385,6 +430,8 @@ def our_arm(args, wl_name):
         v, desc, ksps = cb.run()
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": cb.cores, "kind": "port",
                                 "sample": desc, "k_steps_per_s": ksps}
+    if ws == 1 and not args.no_compare:
+        line["compare"] = compare_variants(args, eng, wl, api, stream, flush, args.variant)
     print(json.dumps(line), flush=True)
     plan.close()
     eng.close()
@@ -400,10 +447,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="piflux2d_256")
-    ap.add_argument("--variant", default="fp64", choices=sorted(VARIANTS))
+    ap.add_argument("--variant", default="mixed_lockstep", choices=sorted(VARIANTS))
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-compare", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

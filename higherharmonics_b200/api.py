@@ -35,8 +35,9 @@ EXPORTED = [
     "hhg_plan_spectrum_async", "hhg_plan_fetch_spectrum", "hhg_measure_fp64_peak",
     "hhg_gpu_current_density_noalloc",
     "hhg_learned_collect", "hhg_default_train_opts", "hhg_mlp_init", "hhg_mlp_train",
-    "hhg_mlp_gradients", "hhg_mlp_predict",
+    "hhg_mlp_gradients", "hhg_mlp_predict", "hhg_plan_execute_graph", "hhg_plan_autotune",
 ]
+TUNE_MAX = 16
 ABI_VERSION = 2
 MLP_INPUTS, MLP_HIDDEN = 8, 64
 MLP_N_PARAMS = 64 * 8 + 64 + 64 * 64 + 64 + 64 * 64 + 64 + 64 + 1
@@ -105,6 +106,16 @@ class TrainOpts(ctypes.Structure):
                 ("beta1", ctypes.c_float), ("beta2", ctypes.c_float), ("eps", ctypes.c_float),
                 ("lr_final", ctypes.c_float), ("reserved", ctypes.c_int32),
                 ("seed", ctypes.c_uint64)]
+
+
+class TuneReport(ctypes.Structure):
+    _fields_ = [("n_candidates", ctypes.c_int32), ("best", ctypes.c_int32),
+                ("tile_k", ctypes.c_int32 * TUNE_MAX), ("grid", ctypes.c_int32 * TUNE_MAX),
+                ("kernel_ms", ctypes.c_double * TUNE_MAX)]
+
+    def as_list(self) -> list:
+        return [{"tile_k": self.tile_k[i], "grid": self.grid[i], "kernel_ms": self.kernel_ms[i]}
+                for i in range(self.n_candidates)]
 
 
 class Stats(ctypes.Structure):
@@ -176,6 +187,8 @@ def load_library() -> ctypes.CDLL:
                                           ctypes.c_int, _F, ctypes.c_int64,
                                           ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(Stats)]
         L.hhg_default_train_opts.argtypes = [ctypes.POINTER(TrainOpts)]
+        L.hhg_plan_execute_graph.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+        L.hhg_plan_autotune.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(TuneReport)]
         L.hhg_mlp_init.argtypes = [ctypes.c_uint64, _F, ctypes.c_int64, ctypes.POINTER(Mlp)]
         L.hhg_mlp_train.argtypes = [ctypes.c_void_p, _F, ctypes.c_int64, ctypes.POINTER(TrainOpts),
                                     ctypes.POINTER(Mlp), _F, _D]
@@ -424,6 +437,18 @@ class Plan:
     def execute_async(self, stream: int | None = None):
         self.eng._check(self.eng.lib.hhg_plan_execute_async(
             self.handle, ctypes.c_void_p(stream) if stream else None), "hhg_plan_execute_async")
+
+    def execute_graph(self, stream: int | None = None, with_spectrum: bool = True):
+        """One CUDA-graph launch of the execution (+ spectra)."""
+        self.eng._check(self.eng.lib.hhg_plan_execute_graph(
+            self.handle, ctypes.c_void_p(stream) if stream else None, int(with_spectrum)),
+            "hhg_plan_execute_graph")
+
+    def autotune(self, reps: int = 2) -> TuneReport:
+        rep = TuneReport()
+        self.eng._check(self.eng.lib.hhg_plan_autotune(self.handle, reps, ctypes.byref(rep)),
+                        "hhg_plan_autotune")
+        return rep
 
     def spectrum_async(self, stream: int | None = None):
         self.eng._check(self.eng.lib.hhg_plan_spectrum_async(

@@ -63,6 +63,11 @@ struct hhg_plan {
     long long hist_cap = 0;
     float *d_hist = nullptr;
     unsigned long long *d_hist_count = nullptr;
+    long long part_cap = 0;  // doubles allocated for d_part
+    int occupancy = 1;       // resident CTAs per SM of the selected kernel variant
+    // CUDA graph of one execution (integration + reduction [+ spectra])
+    cudaGraphExec_t gexec = nullptr;
+    int graph_spec = -1;
 };
 
 namespace hhg {
@@ -829,6 +834,8 @@ hhg_status hhg_plan_create(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_p
         hhg_plan_destroy(pl);
         return st;
     }
+    pl->occupancy = std::max(occ, 1);
+    pl->part_cap = part_len;
     const long long max_ctas = (long long)std::max(occ, 1) * ctx->sm_count;
     const long long need = (pl->n_items + hhg::kWarpsPerBlock - 1) / hhg::kWarpsPerBlock;
     pl->grid = (int)std::max(1LL, std::min(max_ctas, need));
@@ -855,6 +862,7 @@ void hhg_plan_destroy(hhg_plan *pl) {
     cudaFree(pl->d_mlp);
     cudaFree(pl->d_hist);
     cudaFree(pl->d_hist_count);
+    if (pl->gexec) cudaGraphExecDestroy(pl->gexec);
     delete pl;
 }
 
@@ -862,11 +870,13 @@ int64_t hhg_plan_j_length(const hhg_plan *pl) { return pl ? pl->j_len : 0; }
 
 const double *hhg_plan_device_j(const hhg_plan *pl) { return pl ? pl->d_j : nullptr; }
 
-hhg_status hhg_plan_execute_async(hhg_plan *pl, void *stream) {
-    if (!pl) return HHG_BAD_CONFIG;
+}  // extern "C"
+
+namespace {
+// Integration + reduction of one execution on stream s; with `events` the
+// context's timing events bracket the launches (not inside a graph capture).
+hhg_status enqueue_integration(hhg_plan *pl, cudaStream_t s, bool events) {
     hhg_ctx *ctx = pl->ctx;
-    cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
-    HHG_CUDA(ctx, cudaSetDevice(ctx->device));
     HHG_CUDA(ctx, cudaMemsetAsync(pl->d_counters, 0, 8 * sizeof(unsigned long long), s));
     HHG_CUDA(ctx, cudaMemsetAsync(pl->d_status, 0, sizeof(int), s));
     hhg::LaunchReq lr{};
@@ -900,20 +910,33 @@ hhg_status hhg_plan_execute_async(hhg_plan *pl, void *stream) {
     lr.grid = pl->grid;
     lr.stream = s;
     lr.occupancy_out = nullptr;
-    const bool timed = true;
-    HHG_CUDA(ctx, cudaEventRecord(ctx->ev[0], s));
+    if (events) HHG_CUDA(ctx, cudaEventRecord(ctx->ev[0], s));
     hhg_status st = launch_variant(pl, lr);
     if (st != HHG_OK) return st;
-    HHG_CUDA(ctx, cudaEventRecord(ctx->ev[1], s));
+    if (events) HHG_CUDA(ctx, cudaEventRecord(ctx->ev[1], s));
     const int threads = 256;
     const long long blocks = (pl->j_len + threads - 1) / threads;
     hhg::reduce_partials_kernel<<<(unsigned)blocks, threads, 0, s>>>(pl->d_pulses, pl->n_pulses,
                                                                      pl->d_part, pl->d_j, pl->j_len);
     HHG_CUDA(ctx, cudaGetLastError());
-    HHG_CUDA(ctx, cudaEventRecord(ctx->ev[2], s));
-    pl->timed = timed;
+    if (events) {
+        HHG_CUDA(ctx, cudaEventRecord(ctx->ev[2], s));
+        pl->timed = true;
+    }
     return HHG_OK;
 }
+}  // namespace
+
+extern "C" {
+
+hhg_status hhg_plan_execute_async(hhg_plan *pl, void *stream) {
+    if (!pl) return HHG_BAD_CONFIG;
+    hhg_ctx *ctx = pl->ctx;
+    cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+    HHG_CUDA(ctx, cudaSetDevice(ctx->device));
+    return enqueue_integration(pl, s, true);
+}
+
 
 hhg_status hhg_plan_fetch(hhg_plan *pl, double *j_out, hhg_stats *stats) {
     if (!pl) return HHG_BAD_CONFIG;
@@ -1034,13 +1057,10 @@ hhg_status get_fft_plan(hhg_ctx *ctx, int n_in, cufftHandle *out) {
     *out = plan;
     return HHG_OK;
 }
-}  // namespace
 
-hhg_status hhg_plan_spectrum_async(hhg_plan *pl, void *stream) {
-    if (!pl) return HHG_BAD_CONFIG;
+// Spectrum buffers and FFT plans (allocating: never inside a capture).
+hhg_status prepare_spectrum(hhg_plan *pl) {
     hhg_ctx *ctx = pl->ctx;
-    cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
-    HHG_CUDA(ctx, cudaSetDevice(ctx->device));
     if (!pl->d_spec) {
         long long max_in = 0, off = 0;
         pl->spec_off.assign(pl->n_pulses + 1, 0);
@@ -1056,6 +1076,17 @@ hhg_status hhg_plan_spectrum_async(hhg_plan *pl, void *stream) {
         HHG_CUDA(ctx, cudaMalloc(&pl->d_x, sizeof(double) * max_in));
         HHG_CUDA(ctx, cudaMalloc(&pl->d_F, sizeof(double2) * (max_in / 2 + 1)));
     }
+    for (int p = 0; p < pl->n_pulses; ++p) {
+        cufftHandle fp;
+        const hhg_status st = get_fft_plan(ctx, 8 * (pl->pulses[p].n_meas + 1), &fp);
+        if (st != HHG_OK) return st;
+    }
+    return HHG_OK;
+}
+
+// Zero-padding, FFT and trapezoid correction of every pulse's j on stream s.
+hhg_status enqueue_spectrum(hhg_plan *pl, cudaStream_t s) {
+    hhg_ctx *ctx = pl->ctx;
     for (int p = 0; p < pl->n_pulses; ++p) {
         const PulseDev &d = pl->pulses[p];
         const int n = d.n_meas + 1;
@@ -1076,6 +1107,18 @@ hhg_status hhg_plan_spectrum_async(hhg_plan *pl, void *stream) {
     }
     return HHG_OK;
 }
+}  // namespace
+
+hhg_status hhg_plan_spectrum_async(hhg_plan *pl, void *stream) {
+    if (!pl) return HHG_BAD_CONFIG;
+    hhg_ctx *ctx = pl->ctx;
+    cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+    HHG_CUDA(ctx, cudaSetDevice(ctx->device));
+    const hhg_status st = prepare_spectrum(pl);
+    if (st != HHG_OK) return st;
+    return enqueue_spectrum(pl, s);
+}
+
 
 hhg_status hhg_plan_fetch_spectrum(hhg_plan *pl, int pulse, double *re_out, double *im_out,
                                    double *freq_out) {
@@ -1285,6 +1328,148 @@ hhg_status hhg_mlp_predict(hhg_ctx *ctx, const float *records, int64_t n_records
     std::string msg;
     const hhg_status st = hhg::mlp_predict_impl(ctx->stream, records, n_records, net, path, level_out, &msg);
     return st == HHG_OK ? st : set_err(ctx, st, msg);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// CUDA graph execution and the work-decomposition autotuner
+// ---------------------------------------------------------------------------
+namespace {
+void drop_graph(hhg_plan *pl) {
+    if (pl->gexec) cudaGraphExecDestroy(pl->gexec);
+    pl->gexec = nullptr;
+    pl->graph_spec = -1;
+}
+
+// k tiles of 32 per work item (tpi) and the persistent grid (ctas, 0 = all
+// resident CTAs): re-derive the item list, the partial-row offsets and the
+// device pulse table.
+hhg_status retile(hhg_plan *pl, int tpi, long long ctas) {
+    hhg_ctx *ctx = pl->ctx;
+    const long long tiles = (pl->n_k + 31) / 32;
+    tpi = (int)std::max(1LL, std::min<long long>(tpi, tiles));
+    const int ipp = (int)((tiles + tpi - 1) / tpi);
+    long long part_len = 0;
+    for (int p = 0; p < pl->n_pulses; ++p) {
+        PulseDev &d = pl->pulses[p];
+        d.items = ipp;
+        d.part_off = part_len;
+        part_len += (long long)ipp * (d.n_meas + 1);
+    }
+    if (part_len > pl->part_cap) {
+        cudaFree(pl->d_part);
+        pl->d_part = nullptr;
+        pl->part_cap = 0;
+        HHG_CUDA(ctx, cudaMalloc(&pl->d_part, sizeof(double) * part_len));
+        pl->part_cap = part_len;
+    }
+    pl->part_len = part_len;
+    pl->tiles_per_item = tpi;
+    pl->items_per_pulse = ipp;
+    pl->n_items = (long long)ipp * pl->n_pulses;
+    HHG_CUDA(ctx, cudaMemcpy(pl->d_pulses, pl->pulses.data(), sizeof(PulseDev) * pl->n_pulses,
+                             cudaMemcpyHostToDevice));
+    const long long max_ctas = (long long)pl->occupancy * ctx->sm_count;
+    const long long need = (pl->n_items + hhg::kWarpsPerBlock - 1) / hhg::kWarpsPerBlock;
+    const long long want = ctas > 0 ? std::min(ctas, max_ctas) : max_ctas;
+    pl->grid = (int)std::max(1LL, std::min(want, need));
+    drop_graph(pl);
+    return HHG_OK;
+}
+}  // namespace
+
+extern "C" {
+
+hhg_status hhg_plan_execute_graph(hhg_plan *pl, void *stream, int with_spectrum) {
+    if (!pl) return HHG_BAD_CONFIG;
+    hhg_ctx *ctx = pl->ctx;
+    cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+    HHG_CUDA(ctx, cudaSetDevice(ctx->device));
+    with_spectrum = with_spectrum ? 1 : 0;
+    if (!pl->gexec || pl->graph_spec != with_spectrum) {
+        drop_graph(pl);
+        if (with_spectrum) {
+            const hhg_status st = prepare_spectrum(pl);
+            if (st != HHG_OK) return st;
+        }
+        // capture on the context's own (non-blocking) stream; the graph is
+        // launched on the caller's stream
+        HHG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        HHG_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        // the timing events become event-record nodes of the graph: kernel_ms
+        // of the stats is the integration kernel's time in the last launch
+        hhg_status st = enqueue_integration(pl, ctx->stream, true);
+        if (st == HHG_OK && with_spectrum) st = enqueue_spectrum(pl, ctx->stream);
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+        if (st != HHG_OK) {
+            if (g) cudaGraphDestroy(g);
+            return st;
+        }
+        if (e != cudaSuccess)
+            return set_err(ctx, HHG_CUDA_ERROR, std::string("graph capture: ") + cudaGetErrorString(e));
+        const cudaError_t e2 = cudaGraphInstantiate(&pl->gexec, g, 0);
+        cudaGraphDestroy(g);
+        if (e2 != cudaSuccess) {
+            pl->gexec = nullptr;
+            return set_err(ctx, HHG_CUDA_ERROR, std::string("graph instantiate: ") + cudaGetErrorString(e2));
+        }
+        pl->graph_spec = with_spectrum;
+    }
+    HHG_CUDA(ctx, cudaGraphLaunch(pl->gexec, s));
+    pl->timed = true;
+    return HHG_OK;
+}
+
+hhg_status hhg_plan_autotune(hhg_plan *pl, int reps, hhg_tune_report *report) {
+    if (!pl) return HHG_BAD_CONFIG;
+    hhg_ctx *ctx = pl->ctx;
+    HHG_CUDA(ctx, cudaSetDevice(ctx->device));
+    reps = std::max(1, std::min(reps, 16));
+    const long long tiles = (pl->n_k + 31) / 32;
+    const long long resident = (long long)pl->occupancy * ctx->sm_count;
+    std::vector<std::pair<int, long long>> cand;
+    for (int tpi : {1, 2, 4, 8, 16}) {
+        if (tpi > 1 && tpi > tiles) break;
+        // the partial rows stay below 8 GB
+        const double part_bytes = 8.0 * (double)((tiles + tpi - 1) / tpi) * (double)pl->j_len;
+        if (part_bytes > 8e9) continue;
+        for (long long ctas : {resident, resident / 2})
+            if ((int)cand.size() < HHG_TUNE_MAX) cand.emplace_back(tpi, std::max(1LL, ctas));
+    }
+    if (cand.empty()) return set_err(ctx, HHG_UNSUPPORTED, "no tiling fits the partial-row budget");
+    std::vector<double> ms(cand.size(), 1e300);
+    std::vector<int> grids(cand.size(), 0);
+    for (size_t c = 0; c < cand.size(); ++c) {
+        hhg_status st = retile(pl, cand[c].first, cand[c].second);
+        if (st != HHG_OK) return st;
+        grids[c] = pl->grid;
+        for (int r = 0; r <= reps; ++r) {  // first run untimed (warm-up)
+            st = enqueue_integration(pl, ctx->stream, true);
+            if (st != HHG_OK) return st;
+            HHG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+            float a = 0.f;
+            HHG_CUDA(ctx, cudaEventElapsedTime(&a, ctx->ev[0], ctx->ev[1]));
+            if (r > 0) ms[c] = std::min(ms[c], (double)a);
+        }
+    }
+    size_t best = 0;
+    for (size_t c = 1; c < cand.size(); ++c)
+        if (ms[c] < ms[best]) best = c;
+    hhg_status st = retile(pl, cand[best].first, cand[best].second);
+    if (st != HHG_OK) return st;
+    if (report) {
+        std::memset(report, 0, sizeof *report);
+        report->n_candidates = (int32_t)cand.size();
+        report->best = (int32_t)best;
+        for (size_t c = 0; c < cand.size(); ++c) {
+            report->tile_k[c] = cand[c].first;
+            report->grid[c] = grids[c];
+            report->kernel_ms[c] = ms[c];
+        }
+    }
+    return HHG_OK;
 }
 
 }  // extern "C"

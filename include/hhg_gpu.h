@@ -252,6 +252,32 @@ hhg_status hhg_plan_spectrum_async(hhg_plan *plan, void *stream);
 hhg_status hhg_plan_fetch_spectrum(hhg_plan *plan, int pulse, double *re_out, double *im_out,
                                    double *freq_out);
 
+/* The plan's execution (integration + reduction, and with with_spectrum != 0
+ * the spectra) as one CUDA graph launch on `stream`.  The graph is captured
+ * on the first call (and again after hhg_plan_autotune or when with_spectrum
+ * changes) on the context's stream; it replaces hhg_plan_execute_async [+
+ * hhg_plan_spectrum_async] and is read back with hhg_plan_fetch /
+ * hhg_plan_fetch_spectrum (kernel_ms: the integration kernel in the last
+ * launch; total_ms: integration + reduction).  No counterpart in the
+ * reference. */
+hhg_status hhg_plan_execute_graph(hhg_plan *plan, void *stream, int with_spectrum);
+
+/* Work-decomposition autotuner (no counterpart in the reference): times the
+ * integration kernel over candidate k tiles per work item (32 k-points per
+ * tile: 1, 2, 4, 8, 16) and persistent grid sizes (all resident CTAs, half),
+ * `reps` timed runs each after one warm-up run, and keeps the fastest.  The
+ * plan's results are unchanged by the choice (every candidate computes the
+ * same trajectories; only the partial-row summation order changes). */
+#define HHG_TUNE_MAX 16
+typedef struct hhg_tune_report {
+    int32_t n_candidates;
+    int32_t best;
+    int32_t tile_k[HHG_TUNE_MAX];
+    int32_t grid[HHG_TUNE_MAX];
+    double kernel_ms[HHG_TUNE_MAX];
+} hhg_tune_report;
+hhg_status hhg_plan_autotune(hhg_plan *plan, int reps, hhg_tune_report *report);
+
 /* Diagnostic without a reference counterpart: measured FP64 FMA throughput
  * of the device (TFLOP/s, FMA = 2 flops), the denominator of the
  * integration kernel's roofline. */

@@ -49,6 +49,7 @@ def _c_layout():
                            "reserved"],
                "hhg_train_opts": ["epochs", "batch", "lr", "beta1", "beta2", "eps", "lr_final",
                                   "reserved", "seed"],
+               "hhg_tune_report": ["n_candidates", "best", "tile_k", "grid", "kernel_ms"],
                "hhg_stats": ["k_points", "trajectories", "attempted_steps", "rejected_steps",
                              "failed_trajectories", "poly_degree", "items", "kernel_ms",
                              "total_ms"]}
@@ -76,7 +77,7 @@ def test_ctypes_layout_matches_c():
     for cname, py in [("hhg_system_desc", api.SystemDesc), ("hhg_pulse_desc", api.PulseDesc),
                       ("hhg_grid_desc", api.GridDesc), ("hhg_solver_opts", api.SolverOpts),
                       ("hhg_stats", api.Stats), ("hhg_mlp", api.Mlp),
-                      ("hhg_train_opts", api.TrainOpts)]:
+                      ("hhg_train_opts", api.TrainOpts), ("hhg_tune_report", api.TuneReport)]:
         assert lay[(cname, "size")] == ctypes.sizeof(py), cname
         for fname, _ in py._fields_:
             if (cname, fname) in lay:

@@ -1,0 +1,82 @@
+"""GPU checks of the batching layer: CUDA-graph execution of a plan and the
+work-decomposition autotuner.  Neither changes any trajectory: the graph
+replays the same launches, and the autotuner only regroups k tiles into work
+items (which changes the order of the partial-row sums, so j may move by a
+few units in the last place)."""
+import math
+
+import numpy as np
+import pytest
+
+from higherharmonics_b200 import api
+from tests.helpers import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def _dirac_batch():
+    sys = api.system(api.SYS_DIRAC2D, velocity=1.0, mass=0.05)
+    pulses = [api.cosine_pulse(0.3 + 0.2 * i, 1.5 + 0.5 * i, 1024 + 512 * i, phase=0.4 * i,
+                               energy_scale=1 / (0.06 + 0.02 * i)) for i in range(4)]
+    grid = api.grid_tensor(48, 48, -2, 2, -2, 2)
+    return sys, pulses, grid
+
+
+def test_graph_matches_stream_execution(engine):
+    sys, pulses, grid = _dirac_batch()
+    opts = api.solver(1e-10, 1e-10)
+    plan = engine.plan(sys, pulses, grid, opts)
+    plan.execute_async()
+    plan.spectrum_async()
+    j0, st0 = plan.fetch()
+    spec0 = [plan.fetch_spectrum(p) for p in range(len(pulses))]
+    for rep in range(2):  # capture, then replay
+        plan.execute_graph(with_spectrum=True)
+        j1, st1 = plan.fetch()
+        assert np.array_equal(j0, j1)
+        assert st1.attempted_steps == st0.attempted_steps
+        assert st1.kernel_ms > 0 and st1.total_ms >= st1.kernel_ms
+        for p in range(len(pulses)):
+            for a, b in zip(spec0[p], plan.fetch_spectrum(p)):
+                assert np.array_equal(a, b)
+    # integration-only graph, then back to the spectrum graph
+    plan.execute_graph(with_spectrum=False)
+    j2, _ = plan.fetch()
+    assert np.array_equal(j0, j2)
+    plan.close()
+
+
+def test_graph_on_caller_stream(engine):
+    import torch
+    sys, pulses, grid = _dirac_batch()
+    plan = engine.plan(sys, pulses[:1], grid, api.solver(1e-10, 1e-10))
+    plan.execute_async()
+    j0, _ = plan.fetch()
+    s = torch.cuda.Stream()
+    plan.execute_graph(s.cuda_stream, with_spectrum=False)
+    s.synchronize()
+    j1, _ = plan.fetch()
+    assert np.array_equal(j0, j1)
+    plan.close()
+
+
+@pytest.mark.parametrize("proposer", [api.PROPOSER_NONE, api.PROPOSER_LOCKSTEP])
+def test_autotune_keeps_results(engine, proposer):
+    s = 1 / math.sqrt(2)
+    sys = api.system(api.SYS_PIFLUX2D, hopping=1.0, pol=(s, s))
+    pulse = api.cosine_pulse(1.0, 2, 2048, window=(0.0, 6 * math.pi), energy_scale=20.0)
+    grid = api.grid_tensor(96, 96, -math.pi, math.pi, -math.pi, math.pi)
+    plan = engine.plan(sys, pulse, grid, api.solver(1e-12, 1e-8, proposer=proposer))
+    plan.execute_async()
+    j0, st0 = plan.fetch()
+    rep = plan.autotune(reps=1)
+    cands = rep.as_list()
+    assert rep.n_candidates >= 4
+    assert {c["tile_k"] for c in cands} >= {1, 2, 4}
+    assert all(c["kernel_ms"] > 0 for c in cands)
+    assert cands[rep.best]["kernel_ms"] == min(c["kernel_ms"] for c in cands)
+    plan.execute_graph(with_spectrum=True)
+    j1, st1 = plan.fetch()
+    assert st1.attempted_steps == st0.attempted_steps
+    assert rel_l2(j1, j0) <= 1e-13
+    plan.close()
