@@ -19,6 +19,9 @@ using hhg::PulseDev;
 
 struct hhg_ctx {
     int device = 0;
+    // plans of the one-shot entry point, most recently used first (key: the
+    // serialised descriptors)
+    std::vector<std::pair<std::string, hhg_plan *>> plan_cache;
     int sm_count = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -413,6 +416,41 @@ int kernel_model(const hhg_system_desc &s) {
     return s.kind;
 }
 
+constexpr size_t kPlanCacheSize = 4;
+
+// Byte key of the descriptors of one one-shot call: every field that changes
+// the computation (explicit k rows and the learned network by value).
+std::string plan_key(const hhg_system_desc *sys, const hhg_pulse_desc *pulses, int n_pulses,
+                     const hhg_grid_desc *grid, const hhg_solver_opts *opts) {
+    std::string k;
+    auto put = [&k](const void *p, size_t n) { k.append(static_cast<const char *>(p), n); };
+    put(&sys->kind, 4);
+    put(&sys->hopping, 8 * 5);
+    put(&n_pulses, 4);
+    for (int i = 0; i < n_pulses; ++i) {
+        const hhg_pulse_desc &q = pulses[i];
+        put(&q.kind, 4 * 3);
+        put(&q.amplitude, 8 * 7);
+    }
+    put(&grid->kind, 4 * 3);
+    put(&grid->x_lo, 8 * 4);
+    put(&grid->n_rows, 8);
+    if (grid->kind == HHG_GRID_EXPLICIT && grid->rows && grid->n_rows > 0)
+        put(grid->rows, sizeof(double) * 8 * (size_t)grid->n_rows);
+    if (opts) {
+        put(&opts->stepper, 4 * 4);
+        put(&opts->abs_tol, 8 * 2);
+        put(&opts->max_failed_steps, 4 * 4);
+        put(&opts->mlp_every, 4);
+        const bool learned = opts->proposer == HHG_PROPOSER_LEARNED && opts->mlp;
+        put(&learned, 1);
+        if (learned) put(opts->mlp, sizeof(hhg_mlp));
+    } else {
+        put("default", 7);
+    }
+    return k;
+}
+
 // Kernel step-control mode for an ABI proposer: 0 restart, 1 carry, 2 dyadic,
 // 3 learned dyadic.
 int kernel_proposer(int abi) {
@@ -560,6 +598,8 @@ hhg_status hhg_gpu_create(hhg_ctx **out, int device) {
 void hhg_gpu_destroy(hhg_ctx *c) {
     if (!c) return;
     cudaSetDevice(c->device);
+    for (auto &kv : c->plan_cache) hhg_plan_destroy(kv.second);
+    c->plan_cache.clear();
     for (auto &kv : c->fft_plans) cufftDestroy(kv.second);
     cudaFree(c->d_x);
     cudaFree(c->d_F);
@@ -978,12 +1018,30 @@ hhg_status hhg_gpu_current_density(hhg_ctx *ctx, const hhg_system_desc *sys,
                                    const hhg_grid_desc *grid, const hhg_solver_opts *opts,
                                    double *j_out, hhg_stats *stats) {
     if (!ctx || !j_out) return set_err(ctx, HHG_BAD_CONFIG, "null context or output");
+    if (!sys || !pulses || !grid || n_pulses < 1 || n_pulses > (1 << 20))
+        return set_err(ctx, HHG_BAD_CONFIG, "null descriptor or bad pulse count");
+    // repeated calls with the same descriptors reuse the plan (k table, pulse
+    // staging, device buffers); the integration itself runs every call
+    const std::string key = plan_key(sys, pulses, n_pulses, grid, opts);
     hhg_plan *pl = nullptr;
-    hhg_status st = hhg_plan_create(ctx, sys, pulses, n_pulses, grid, opts, &pl);
-    if (st != HHG_OK) return st;
-    st = hhg_plan_execute_async(pl, nullptr);
+    auto &cache = ctx->plan_cache;
+    for (size_t i = 0; i < cache.size(); ++i)
+        if (cache[i].first == key) {
+            pl = cache[i].second;
+            std::rotate(cache.begin(), cache.begin() + i, cache.begin() + i + 1);
+            break;
+        }
+    if (!pl) {
+        hhg_status st = hhg_plan_create(ctx, sys, pulses, n_pulses, grid, opts, &pl);
+        if (st != HHG_OK) return st;
+        cache.insert(cache.begin(), {key, pl});
+        while (cache.size() > kPlanCacheSize) {
+            hhg_plan_destroy(cache.back().second);
+            cache.pop_back();
+        }
+    }
+    hhg_status st = hhg_plan_execute_async(pl, nullptr);
     if (st == HHG_OK) st = hhg_plan_fetch(pl, j_out, stats);
-    hhg_plan_destroy(pl);
     return st;
 }
 
@@ -1397,9 +1455,7 @@ hhg_status hhg_plan_execute_graph(hhg_plan *pl, void *stream, int with_spectrum)
         // launched on the caller's stream
         HHG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
         HHG_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-        // the timing events become event-record nodes of the graph: kernel_ms
-        // of the stats is the integration kernel's time in the last launch
-        hhg_status st = enqueue_integration(pl, ctx->stream, true);
+        hhg_status st = enqueue_integration(pl, ctx->stream, false);
         if (st == HHG_OK && with_spectrum) st = enqueue_spectrum(pl, ctx->stream);
         cudaGraph_t g = nullptr;
         const cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
@@ -1417,7 +1473,11 @@ hhg_status hhg_plan_execute_graph(hhg_plan *pl, void *stream, int with_spectrum)
         }
         pl->graph_spec = with_spectrum;
     }
+    // events recorded inside a captured graph do not time; bracket the launch
+    HHG_CUDA(ctx, cudaEventRecord(ctx->ev[0], s));
     HHG_CUDA(ctx, cudaGraphLaunch(pl->gexec, s));
+    HHG_CUDA(ctx, cudaEventRecord(ctx->ev[1], s));
+    HHG_CUDA(ctx, cudaEventRecord(ctx->ev[2], s));
     pl->timed = true;
     return HHG_OK;
 }

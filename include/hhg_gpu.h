@@ -215,7 +215,10 @@ hhg_status hhg_grid_rows(const hhg_system_desc *sys, const hhg_grid_desc *grid, 
 /* One-shot drop-in for System::compute_current_density over n_pulses pulse
  * instances: j_out (host, caller-owned) receives for pulse p the
  * n_measurements_p + 1 samples of j(t) at offset sum_{q<p}(n_measurements_q
- * + 1).  Synchronous. */
+ * + 1).  Synchronous.  The context keeps the plans (k table, pulse staging,
+ * device buffers) of its last 4 distinct descriptor sets and reuses one when
+ * a call repeats its descriptors byte for byte (explicit k rows and the
+ * learned network compared by value); the integration runs every call. */
 hhg_status hhg_gpu_current_density(hhg_ctx *ctx, const hhg_system_desc *sys,
                                    const hhg_pulse_desc *pulses, int n_pulses,
                                    const hhg_grid_desc *grid, const hhg_solver_opts *opts,
@@ -257,9 +260,8 @@ hhg_status hhg_plan_fetch_spectrum(hhg_plan *plan, int pulse, double *re_out, do
  * on the first call (and again after hhg_plan_autotune or when with_spectrum
  * changes) on the context's stream; it replaces hhg_plan_execute_async [+
  * hhg_plan_spectrum_async] and is read back with hhg_plan_fetch /
- * hhg_plan_fetch_spectrum (kernel_ms: the integration kernel in the last
- * launch; total_ms: integration + reduction).  No counterpart in the
- * reference. */
+ * hhg_plan_fetch_spectrum (kernel_ms and total_ms: the whole graph launch).
+ * No counterpart in the reference. */
 hhg_status hhg_plan_execute_graph(hhg_plan *plan, void *stream, int with_spectrum);
 
 /* Work-decomposition autotuner (no counterpart in the reference): times the

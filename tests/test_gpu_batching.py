@@ -80,3 +80,38 @@ def test_autotune_keeps_results(engine, proposer):
     assert st1.attempted_steps == st0.attempted_steps
     assert rel_l2(j1, j0) <= 1e-13
     plan.close()
+
+
+def test_one_shot_plan_cache_has_no_stale_hits(engine):
+    """The one-shot entry point reuses plans for repeated descriptors; any
+    change of a descriptor (a pulse field, explicit k rows by value, the
+    tolerances) must give the freshly computed result."""
+    sys = api.system(api.SYS_DIRAC2D, velocity=1.0, mass=0.05)
+    pulse = api.cosine_pulse(1.0, 1, 512, energy_scale=10.0)
+    grid = api.grid_tensor(16, 16, -2, 2, -2, 2)
+    opts = api.solver(1e-10, 1e-10)
+    a, _ = engine.current_density(sys, pulse, grid, opts)
+    b, _ = engine.current_density(sys, pulse, grid, opts)
+    assert np.array_equal(a, b)
+    pulse2 = api.cosine_pulse(1.1, 1, 512, energy_scale=10.0)
+    c, _ = engine.current_density(sys, pulse2, grid, opts)
+    assert not np.array_equal(a, c)
+    # fresh engine: no cache, same answer for pulse2
+    e2 = api.Engine(0)
+    c2, _ = e2.current_density(sys, pulse2, grid, opts)
+    assert np.array_equal(c, c2)
+    rows = api.grid_rows(sys, grid)
+    g1, keep1 = api.grid_explicit(rows.copy())
+    r1, _ = engine.current_density(sys, pulse, g1, opts)
+    assert np.array_equal(r1, a)
+    rows2 = rows.copy()
+    rows2[:, 3] *= 2.0  # weights doubled -> j doubled, same buffer address pattern
+    g2, keep2 = api.grid_explicit(rows2)
+    r2, _ = engine.current_density(sys, pulse, g2, opts)
+    assert np.allclose(r2, 2 * a, rtol=1e-14, atol=0)
+    # the restart schedule makes the step sequence tolerance-independent here;
+    # the carried proposal changes it
+    d, std = engine.current_density(sys, pulse, grid, api.solver(1e-10, 1e-10,
+                                                                 proposer=api.PROPOSER_CARRY))
+    assert not np.array_equal(a, d)
+    e2.close()
