@@ -442,14 +442,16 @@ def our_arm(args, wl_name):
 def ncu_case(args):
     """A small case of the bench workload for ncu captures (committed so the
     profile summaries name a command that runs committed files only): the
-    same grid and pulse shape over 1 cycle (1024 intervals), two executions
+    same grid and pulse shape over --ncu-cycles cycles (default 1: 1024
+    intervals), two executions
     of the selected variant; with --variant mlp_train, history collection on
     that case and 2 epochs of proposer training.  Prints one line, no timing."""
     from higherharmonics_b200 import api
     from higherharmonics_b200 import workloads as W
     import inspect
     make = W.ALL[args.workload]
-    wl = make(n_cycles=1) if "n_cycles" in inspect.signature(make).parameters else make()
+    wl = (make(n_cycles=args.ncu_cycles) if "n_cycles" in inspect.signature(make).parameters
+          else make())
     eng = api.Engine(0)
     if args.variant == "mlp_train":
         recs, _ = eng.learned_collect(wl.system, wl.pulses, wl.grid, wl.opts(), hist_every=32,
@@ -482,6 +484,8 @@ def main():
     ap.add_argument("--variant", default="mixed_lockstep", choices=sorted(VARIANTS) + ["mlp_train"])
     ap.add_argument("--ncu-case", action="store_true",
                     help="run the small profiling case of the workload (no timing)")
+    ap.add_argument("--ncu-cycles", type=int, default=1,
+                    help="pulse cycles of the --ncu-case workload (the bench uses the full length)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")

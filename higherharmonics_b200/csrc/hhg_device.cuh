@@ -1071,31 +1071,59 @@ __global__ void stage_pulses_kernel(const PulseDev *__restrict__ pulses, int n_p
     out[SCHED] = (double)n_std;
 }
 
-// j[p][i] = sum over the pulse's items (in item order) of the partial rows,
-// with Neumaier compensation.
-static __global__ void reduce_partials_kernel(const PulseDev *__restrict__ pulses, int n_pulses,
-                                              const double *__restrict__ part,
-                                              double *__restrict__ j, long long total_samples) {
-    const long long gid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (gid >= total_samples) return;
-    int lo = 0, hi = n_pulses;
-    while (hi - lo > 1) {
-        const int mid = (lo + hi) >> 1;
-        if (pulses[mid].j_off <= gid) lo = mid; else hi = mid;
-    }
-    const PulseDev &pd = pulses[lo];
-    const int i = (int)(gid - pd.j_off);
-    const int len = pd.n_meas + 1;
-    const double *src = part + pd.part_off + i;
+// j[p][i] = sum over the pulse's items of the partial rows, with Neumaier
+// compensation, in a fixed order (deterministic): a CTA covers 32 consecutive
+// samples; warp w sums items w, w + kRedWarps, ... (coalesced 256-byte row
+// segments, several loads in flight per warp), then warp 0 adds the kRedWarps
+// partial sums in warp order.  Launch: ceil(total_samples / 32) CTAs of
+// kReduceThreads threads.
+constexpr int kRedWarps = 8;
+constexpr int kReduceThreads = 32 * kRedWarps;
+__host__ __device__ inline long long reduce_blocks(long long total_samples) {
+    return (total_samples + 31) / 32;
+}
+
+__device__ __forceinline__ void neumaier_add(double &s, double &comp, double v) {
+    const double t = s + v;
+    if (fabs(s) >= fabs(v)) comp += (s - t) + v;
+    else comp += (v - t) + s;
+    s = t;
+}
+
+static __global__ void __launch_bounds__(kReduceThreads)
+reduce_partials_kernel(const PulseDev *__restrict__ pulses, int n_pulses,
+                       const double *__restrict__ part, double *__restrict__ j,
+                       long long total_samples) {
+    __shared__ double s_sum[kRedWarps][32], s_comp[kRedWarps][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const long long gid = blockIdx.x * 32LL + lane;
     double s = 0.0, comp = 0.0;
-    for (int it = 0; it < pd.items; ++it) {
-        const double v = src[(size_t)it * len];
-        const double tt = s + v;
-        if (fabs(s) >= fabs(v)) comp += (s - tt) + v;
-        else comp += (v - tt) + s;
-        s = tt;
+    if (gid < total_samples) {
+        int lo = 0, hi = n_pulses;
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (pulses[mid].j_off <= gid) lo = mid; else hi = mid;
+        }
+        const PulseDev &pd = pulses[lo];
+        const int i = (int)(gid - pd.j_off);
+        const size_t len = (size_t)pd.n_meas + 1;
+        const double *src = part + pd.part_off + i;
+        const int items = pd.items;
+#pragma unroll 4
+        for (int it = w; it < items; it += kRedWarps) neumaier_add(s, comp, __ldcs(src + (size_t)it * len));
     }
-    j[gid] = s + comp;
+    s_sum[w][lane] = s;
+    s_comp[w][lane] = comp;
+    __syncthreads();
+    if (w == 0 && gid < total_samples) {
+        double t = s_sum[0][lane], c = s_comp[0][lane];
+#pragma unroll
+        for (int q = 1; q < kRedWarps; ++q) {
+            neumaier_add(t, c, s_sum[q][lane]);
+            c += s_comp[q][lane];
+        }
+        j[gid] = t + c;
+    }
 }
 
 // Zero-padded copy for the r2c FFT (hhg.cpp:280-282).

@@ -954,10 +954,8 @@ hhg_status enqueue_integration(hhg_plan *pl, cudaStream_t s, bool events) {
     hhg_status st = launch_variant(pl, lr);
     if (st != HHG_OK) return st;
     if (events) HHG_CUDA(ctx, cudaEventRecord(ctx->ev[1], s));
-    const int threads = 256;
-    const long long blocks = (pl->j_len + threads - 1) / threads;
-    hhg::reduce_partials_kernel<<<(unsigned)blocks, threads, 0, s>>>(pl->d_pulses, pl->n_pulses,
-                                                                     pl->d_part, pl->d_j, pl->j_len);
+    hhg::reduce_partials_kernel<<<(unsigned)hhg::reduce_blocks(pl->j_len), hhg::kReduceThreads, 0, s>>>(
+        pl->d_pulses, pl->n_pulses, pl->d_part, pl->d_j, pl->j_len);
     HHG_CUDA(ctx, cudaGetLastError());
     if (events) {
         HHG_CUDA(ctx, cudaEventRecord(ctx->ev[2], s));

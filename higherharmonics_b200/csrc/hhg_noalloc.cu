@@ -230,8 +230,8 @@ extern "C" hhg_status hhg_gpu_current_density_noalloc(const hhg_system_desc *sys
     lr.occupancy_out = nullptr;
     lr.stream = s;
     if ((e = launch_model(prep.model, lr)) != cudaSuccess) return fail(e);
-    hhg::reduce_partials_kernel<<<(N + 1 + 255) / 256, 256, 0, s>>>(d_pulse, 1, d_part, d_j_out,
-                                                                      (long long)N + 1);
+    hhg::reduce_partials_kernel<<<(unsigned)hhg::reduce_blocks((long long)N + 1), hhg::kReduceThreads, 0, s>>>(
+        d_pulse, 1, d_part, d_j_out, (long long)N + 1);
     if ((e = cudaGetLastError()) != cudaSuccess) return fail(e);
 
     if (!stats) return HHG_OK;
