@@ -35,7 +35,7 @@ EXPORTED = [
     "hhg_plan_spectrum_async", "hhg_plan_fetch_spectrum", "hhg_measure_fp64_peak",
     "hhg_gpu_current_density_noalloc",
     "hhg_learned_collect", "hhg_default_train_opts", "hhg_mlp_init", "hhg_mlp_train",
-    "hhg_mlp_gradients", "hhg_mlp_predict", "hhg_plan_execute_graph", "hhg_plan_autotune",
+    "hhg_mlp_gradients", "hhg_mlp_predict", "hhg_plan_execute_graph", "hhg_plan_autotune", "hhg_measure_fp32_peak",
 ]
 TUNE_MAX = 16
 ABI_VERSION = 2
@@ -175,6 +175,7 @@ def load_library() -> ctypes.CDLL:
         L.hhg_plan_spectrum_async.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         L.hhg_plan_fetch_spectrum.argtypes = [ctypes.c_void_p, ctypes.c_int, _D, _D, _D]
         L.hhg_measure_fp64_peak.argtypes = [ctypes.c_void_p, _D]
+        L.hhg_measure_fp32_peak.argtypes = [ctypes.c_void_p, _D]
         L.hhg_gpu_current_density_noalloc.argtypes = [
             ctypes.POINTER(SystemDesc), ctypes.POINTER(PulseDesc), ctypes.c_void_p, ctypes.c_int64,
             ctypes.POINTER(SolverOpts), ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(Stats),
@@ -418,6 +419,12 @@ class Engine:
         v = ctypes.c_double(0.0)
         self._check(self.lib.hhg_measure_fp64_peak(self.ctx, ctypes.byref(v)),
                     "hhg_measure_fp64_peak")
+        return v.value
+
+    def fp32_peak_tflops(self) -> float:
+        v = ctypes.c_double(0.0)
+        self._check(self.lib.hhg_measure_fp32_peak(self.ctx, ctypes.byref(v)),
+                    "hhg_measure_fp32_peak")
         return v.value
 
 

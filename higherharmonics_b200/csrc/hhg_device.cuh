@@ -1188,4 +1188,20 @@ static __global__ void fp64_fma_probe_kernel(double *out, int iters, double a, d
     if (s == 12345.678) out[0] = s;  // keeps the chains alive
 }
 
+// The same probe on the FP32 pipe (the mixed-precision variant's stage
+// arithmetic): 8 independent FMA chains per thread.
+static __global__ void fp32_fma_probe_kernel(float *out, int iters, float a, float b) {
+    float v[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) v[c] = threadIdx.x * 1e-3f + c;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int c = 0; c < 8; ++c) v[c] = fmaf(v[c], a, b);
+    }
+    float s = 0.0f;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) s += v[c];
+    if (s == 12345.678f) out[0] = s;  // keeps the chains alive
+}
+
 }  // namespace hhg

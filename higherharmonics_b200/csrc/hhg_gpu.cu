@@ -1190,19 +1190,22 @@ hhg_status hhg_plan_fetch_spectrum(hhg_plan *pl, int pulse, double *re_out, doub
     return HHG_OK;
 }
 
-hhg_status hhg_measure_fp64_peak(hhg_ctx *ctx, double *tflops) {
+extern "C++" {
+namespace {
+// Best of 5 timed launches of an FMA-chain probe (after 2 warm-up launches).
+template <typename T, typename K>
+hhg_status measure_fma_peak(hhg_ctx *ctx, K kern, T a, T b, double *tflops) {
     if (!ctx || !tflops) return HHG_BAD_CONFIG;
     HHG_CUDA(ctx, cudaSetDevice(ctx->device));
-    double *d_out = nullptr;
-    HHG_CUDA(ctx, cudaMalloc(&d_out, sizeof(double)));
+    T *d_out = nullptr;
+    HHG_CUDA(ctx, cudaMalloc(&d_out, sizeof(T)));
     const int threads = 256, blocks = ctx->sm_count * 8, iters = 4096;
     cudaStream_t s = ctx->stream;
-    for (int w = 0; w < 2; ++w)
-        hhg::fp64_fma_probe_kernel<<<blocks, threads, 0, s>>>(d_out, iters, 0.999999, 1e-7);
+    for (int w = 0; w < 2; ++w) kern<<<blocks, threads, 0, s>>>(d_out, iters, a, b);
     float best = 1e30f;
     for (int r = 0; r < 5; ++r) {
         cudaEventRecord(ctx->ev[0], s);
-        hhg::fp64_fma_probe_kernel<<<blocks, threads, 0, s>>>(d_out, iters, 0.999999, 1e-7);
+        kern<<<blocks, threads, 0, s>>>(d_out, iters, a, b);
         cudaEventRecord(ctx->ev[1], s);
         cudaEventSynchronize(ctx->ev[1]);
         float ms = 0.f;
@@ -1215,6 +1218,16 @@ hhg_status hhg_measure_fp64_peak(hhg_ctx *ctx, double *tflops) {
     const double flops = 2.0 * 8.0 * iters * (double)threads * blocks;
     *tflops = flops / (best * 1e-3) / 1e12;
     return HHG_OK;
+}
+}  // namespace
+}  // extern "C++"
+
+hhg_status hhg_measure_fp64_peak(hhg_ctx *ctx, double *tflops) {
+    return measure_fma_peak<double>(ctx, hhg::fp64_fma_probe_kernel, 0.999999, 1e-7, tflops);
+}
+
+hhg_status hhg_measure_fp32_peak(hhg_ctx *ctx, double *tflops) {
+    return measure_fma_peak<float>(ctx, hhg::fp32_fma_probe_kernel, 0.999999f, 1e-7f, tflops);
 }
 
 }  // extern "C"

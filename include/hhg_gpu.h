@@ -284,6 +284,8 @@ hhg_status hhg_plan_autotune(hhg_plan *plan, int reps, hhg_tune_report *report);
  * of the device (TFLOP/s, FMA = 2 flops), the denominator of the
  * integration kernel's roofline. */
 hhg_status hhg_measure_fp64_peak(hhg_ctx *ctx, double *tflops);
+/* The same for the FP32 pipe (the mixed-precision variant's denominator). */
+hhg_status hhg_measure_fp32_peak(hhg_ctx *ctx, double *tflops);
 
 /* Allocation-free variant of hhg_gpu_current_density for one pulse.  It has
  * no counterpart in the reference (which runs on the CPU).

@@ -200,7 +200,8 @@ static void model_rhs(const orc_model *m, const kctx *k, const orc_pulse *p, dou
     case ORC_HONEYCOMB: {
         /* Honeycomb::time_evolution_sigma right_side (Honeycomb.cpp:131-138)
          * with shifted_gamma (Honeycomb.cpp:41-47); the staggered-mass term
-         * 2*mass*(-S_y, S_x, 0) is the BASELINE variant (0 = reference). */
+         * 2*mass*(-S_y, S_x, 0) is the gapped variant of the 512x512 rhombic
+         * workload (mass 0 = the reference model). */
         const double pf = 2 * m->hopping;
         const double xs = m->pol_x * A, ys = m->pol_y * A;
         double gre = 0.0, gim = 0.0;
@@ -592,7 +593,8 @@ static int integrate_interval(const rhs_ctx *c, double *x, double t0, double t1,
 /* ------------------------------------------------------------------------ */
 /* Magnus-4 (two-point Gauss, one step per sub-interval) for dS/dt = 2 d x S:
  * omega = h (d1 + d2) + (sqrt3/3) h^2 (d2 x d1), S <- exp([omega]_x) S.
- * Not a reference path: the BASELINE "4th-order Magnus variant"; the
+ * Not a reference path: the 4th-order Magnus variant of the honeycomb
+ * workload; the
  * reference's general so(3) Magnus (GeneralMagnus.cpp) is its design source. */
 /* ------------------------------------------------------------------------ */
 static void dvec(const orc_model *m, const kctx *k, const orc_pulse *p, double t, double *d) {
