@@ -35,10 +35,20 @@ UNIT = "spectra/s"
 # sides plus the tableau arithmetic 2*3*55 (stages) + 2*3*7 (solution) +
 # 2*3*4 (error) + ~25 (norm and control) = 421; the right-hand side of the
 # 2D pi-flux model costs 12 flops plus two cosines (counted separately).
+# The PiFlux relaxation right-hand side (PiFlux.cpp:113-186 as the kernel
+# writes it) costs 103 flops: cos(kz - A) 3, |u| 5, the two occupation
+# energies and Fermi denominators 8, (a2 - b2)/|u| 1, coherent part with the
+# -g_s S + g_d r_d terms 27, 2 sqrt(a2 b2) 2, z_eps and the normalisation 2,
+# the squared cosines 5, the diagonal_sigma numerators 18, their norm 3, the
+# is_zero test 3, prod/imag 3, the off-diagonal terms 23; plus 8 special
+# operations (2 exp, 3 divisions, 2 sqrt, 1 rsqrt).
 ALG_FLOPS_PER_KSTEP = {"piflux2d_256": 13 * 12 + 421, "dirac2d_64": 13 * 16 + 421,
-                       "honeycomb_512": 13 * 30 + 421, "dirac2d_sweep": 13 * 16 + 421}
+                       "honeycomb_512": 13 * 30 + 421, "dirac2d_sweep": 13 * 16 + 421,
+                       "piflux3d_relax": 13 * 103 + 421}
 SPECIAL_OPS_PER_KSTEP = {"piflux2d_256": 26, "dirac2d_64": 0, "honeycomb_512": 78,
-                         "dirac2d_sweep": 0}
+                         "dirac2d_sweep": 0, "piflux3d_relax": 13 * 8}
+# the relaxation workload runs the reference step schedule in FP64 only
+DEFAULT_VARIANT = {"piflux3d_relax": "fp64"}
 # The mixed-precision variant splits that work: solution, error estimate, error
 # norm and control stay FP64 (2*3*7 + 2*3*4 + ~25 = 91 flops); the right-hand
 # sides and the stage sums (13 F_rhs + 2*3*55) run on the FP32 pipe.
@@ -238,7 +248,7 @@ def compare_variants(args, eng, wl, api, stream, flush, main_variant):
     import torch
     out = {}
     for v in ("fp64", "mixed_learned", "mixed_lockstep"):
-        if v == main_variant:
+        if v == main_variant or (v != "fp64" and args.workload in DEFAULT_VARIANT):
             continue
         okw = dict(VARIANTS[v])
         if okw.get("proposer") == api.PROPOSER_LEARNED:
@@ -499,7 +509,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="piflux2d_256")
-    ap.add_argument("--variant", default="mixed_lockstep", choices=sorted(VARIANTS) + ["mlp_train"])
+    ap.add_argument("--variant", default=None, choices=sorted(VARIANTS) + ["mlp_train"],
+                    help="default: mixed_lockstep (fp64 for piflux3d_relax)")
     ap.add_argument("--ncu-case", action="store_true",
                     help="run the small profiling case of the workload (no timing)")
     ap.add_argument("--ncu-cycles", type=int, default=1,
@@ -509,6 +520,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-compare", action="store_true")
     args = ap.parse_args()
+    if args.variant is None:
+        args.variant = DEFAULT_VARIANT.get(args.workload, "mixed_lockstep")
     if args.warmup < 3:
         args.warmup = 3
     if args.ncu_case:

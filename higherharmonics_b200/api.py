@@ -38,7 +38,7 @@ EXPORTED = [
     "hhg_mlp_gradients", "hhg_mlp_predict", "hhg_plan_execute_graph", "hhg_plan_autotune", "hhg_measure_fp32_peak",
 ]
 TUNE_MAX = 16
-ABI_VERSION = 2
+ABI_VERSION = 3
 MLP_INPUTS, MLP_HIDDEN = 8, 64
 MLP_N_PARAMS = 64 * 8 + 64 + 64 * 64 + 64 + 64 * 64 + 64 + 64 + 1
 HIST_FIELDS = 12
@@ -50,7 +50,9 @@ MLP_LAYOUT = [("w1", (64, 8)), ("b1", (64,)), ("w2", (64, 64)), ("b2", (64,)),
 class SystemDesc(ctypes.Structure):
     _fields_ = [("kind", ctypes.c_int32), ("reserved", ctypes.c_int32),
                 ("hopping", ctypes.c_double), ("velocity", ctypes.c_double),
-                ("mass", ctypes.c_double), ("pol_x", ctypes.c_double), ("pol_y", ctypes.c_double)]
+                ("mass", ctypes.c_double), ("pol_x", ctypes.c_double), ("pol_y", ctypes.c_double),
+                ("beta", ctypes.c_double), ("fermi_energy", ctypes.c_double),
+                ("inv_diag_relax", ctypes.c_double), ("inv_offdiag_relax", ctypes.c_double)]
 
 
 class PulseDesc(ctypes.Structure):
@@ -219,8 +221,14 @@ def _records(rec) -> np.ndarray:
 # ---------------------------------------------------------------------------
 # descriptor helpers
 # ---------------------------------------------------------------------------
-def system(kind: int, hopping=0.0, velocity=0.0, mass=0.0, pol=(1.0, 0.0)) -> SystemDesc:
-    return SystemDesc(kind, 0, hopping, velocity, mass, pol[0], pol[1])
+def system(kind: int, hopping=0.0, velocity=0.0, mass=0.0, pol=(1.0, 0.0), *, beta=0.0,
+           fermi_energy=0.0, inv_diag_relax=0.0, inv_offdiag_relax=0.0) -> SystemDesc:
+    """System descriptor.  beta = photon_energy / (k_B T) (0: T = 0),
+    fermi_energy = E_F / photon_energy, inv_*_relax = 1e15 hbar / (tau
+    photon_energy) (PiFlux.cpp:56-71); inv_diag_relax > 0 selects the
+    relaxation right-hand side."""
+    return SystemDesc(kind, 0, hopping, velocity, mass, pol[0], pol[1], beta, fermi_energy,
+                      inv_diag_relax, inv_offdiag_relax)
 
 
 def cosine_pulse(amplitude: float, n_cycles: float, n_measurements: int, *, t_begin=0.0,

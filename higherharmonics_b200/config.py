@@ -1,0 +1,140 @@
+"""The reference's parameter files as engine descriptors.
+
+A parameter file (params/*.config in the reference) holds `key value` lines;
+`#` starts a comment; this reader ignores words after the value (wang.config
+lists units there).  `from_config` maps
+one onto (system, pulse, grid, solver) descriptors with the unit conversions
+of the reference's dispatchers and system constructors:
+
+  beta          = photon_energy / (k_B T), T = 0 -> 0       (PiFlux.cpp:63)
+  E_F           -> E_F / photon_energy                      (PiFlux.cpp:64)
+  hopping       = band_width / sqrt(12) (PiFlux, PiFlux.cpp:65),
+                  band_width / 6 (Honeycomb, Honeycomb.cpp:91)
+  lattice const = sqrt(3) hbar v_F / (photon_energy band_width) (PiFlux.cpp:66),
+                  4 hbar v_F / (photon_energy band_width) (Honeycomb.cpp:92)
+  1/tau         = 1e15 hbar / (tau photon_energy)           (PiFlux.cpp:67-68)
+  A0            = lattice const * 1e11 E0 / photon_energy   (Laser.cpp:24-25)
+  off-diagonal tau <= 0 -> the diagonal one (PiFluxDispatcher.cpp:22-35)
+  N             = n_laser_cycles * 1024 intervals           (hhg.cpp:86-87)
+  window        = [pi t0_offset, laser end + 2 pi] for the cosine laser
+                  (PiFluxDispatcher.cpp:50-53, HoneycombDispatcher.cpp:32-35)
+  grids         = the reference's compiled-in quadratures: PiFlux z_range 32,
+                  N_coarse 4 (PiFlux.hpp:11-22); Honeycomb N_k 64
+                  (Honeycomb.hpp:12-21)
+
+Only the cosine laser exists on the device; the experimental, power-law,
+quench, double and continuous lasers and the Dirac system's adaptive kappa
+quadrature raise UnsupportedConfig.  Keys the path does not read (data_dir,
+debug_data, occupations, split_current, n_z) are accepted and ignored; the
+run modes occupations/split_current != "no" and debug_data != "no" raise
+UnsupportedConfig because they produce other outputs than j(t).
+"""
+from __future__ import annotations
+
+import math
+import os
+from dataclasses import dataclass
+
+from . import api
+
+HBAR = 6.582119569509065698e-13  # meV s (GlobalDefinitions.hpp:28)
+K_B = 0.08617333262145177434     # meV / K (GlobalDefinitions.hpp:29)
+SQRT3 = 1.732050807568877293527446341
+SQRT12 = 3.464101615137754587054892683
+MEASUREMENTS_PER_CYCLE = 1 << 10
+PIFLUX_Z_RANGE, PIFLUX_N_COARSE = 32, 4
+HONEYCOMB_N_K = 64
+
+
+class UnsupportedConfig(ValueError):
+    """A valid reference configuration that this engine does not run."""
+
+
+def read_config(source: str) -> dict[str, str]:
+    """Parse a parameter file (a path or the text itself) into {key: value}."""
+    text = open(source).read() if os.path.exists(source) else source
+    out: dict[str, str] = {}
+    for line in text.splitlines():
+        line = line.split("#", 1)[0].strip()
+        if not line:
+            continue
+        parts = line.split()
+        if len(parts) < 2:
+            raise ValueError(f"config line without a value: {line!r}")
+        out[parts[0]] = parts[1]
+    return out
+
+
+def _is_zero(x: float) -> bool:
+    # GlobalDefinitions.hpp:61-71: |x| < 2^-44 by the biased exponent
+    return abs(x) < 2.0 ** -44
+
+
+@dataclass
+class Run:
+    system_type: str
+    system: api.SystemDesc
+    pulse: api.PulseDesc
+    grid: api.GridDesc
+    opts: api.SolverOpts
+    lattice_constant: float
+
+
+def from_config(cfg: dict | str, *, grid: api.GridDesc | None = None,
+                n_measurements: int | None = None) -> Run:
+    """Descriptors for one reference run.  ``grid`` / ``n_measurements``
+    override the reference's compiled-in quadrature and its 1024 samples per
+    cycle (for smaller test runs)."""
+    if isinstance(cfg, str):
+        cfg = read_config(cfg)
+
+    def num(key: str) -> float:
+        if key not in cfg:
+            raise ValueError(f"missing config key {key!r}")
+        return float(cfg[key])
+
+    system_type = cfg.get("system_type", "")
+    if system_type not in ("PiFlux", "Honeycomb", "Dirac", "ModifiedPiFlux"):
+        raise ValueError(f"System type '{system_type}' not recognized!")
+    if system_type in ("Dirac", "ModifiedPiFlux"):
+        raise UnsupportedConfig(f"system_type {system_type}: the Dirac current density needs the "
+                                "reference's adaptive kappa quadrature; ModifiedPiFlux is not built")
+    for mode in ("occupations", "split_current", "debug_data"):
+        if cfg.get(mode, "no") != "no":
+            raise UnsupportedConfig(f"{mode} = {cfg[mode]}: only the current density j(t) is built")
+    laser_type = cfg.get("laser_type", "")
+    if laser_type != "cosine":
+        raise UnsupportedConfig(f"laser_type {laser_type!r}: only the cosine laser runs on the device")
+
+    T, E_F, v_F = num("T"), num("E_F"), num("v_F")
+    band_width, E0, pe = num("band_width"), num("field_amplitude"), num("photon_energy")
+    tau_d = num("diagonal_relaxation_time")
+    tau_o = float(cfg.get("offdiagonal_relaxation_time", "-1"))
+    n_cycles = int(num("n_laser_cycles"))
+    t0_offset = float(cfg.get("t0_offset", "0"))
+
+    beta = 0.0 if _is_zero(T) else pe / (K_B * T)
+    inv_d = (1e15 * HBAR) / (tau_d * pe)
+    if system_type == "PiFlux":
+        hopping = band_width / SQRT12
+        lattice = SQRT3 * HBAR * v_F / (pe * band_width)
+        inv_o = (1e15 * HBAR) / ((tau_o if tau_o > 0 else tau_d) * pe)
+        kind, pol = api.SYS_PIFLUX3D, (1.0, 0.0)
+        g = grid or api.grid_piflux3d_ref(PIFLUX_Z_RANGE, PIFLUX_N_COARSE)
+    else:
+        hopping = band_width / 6
+        lattice = 4 * HBAR * v_F / (pe * band_width)
+        inv_o = 0.0
+        kind, pol = api.SYS_HONEYCOMB, (1.0, 0.0)  # laser_theta = 0 (Honeycomb.hpp:87)
+        g = grid or api.grid_honeycomb_hex_ref(HONEYCOMB_N_K)
+    relax = inv_d > 0.0  # __time_evolution__ (PiFlux.cpp:509-516, Honeycomb.cpp:214-223)
+    sys_ = api.system(kind, hopping=hopping, pol=pol, beta=beta, fermi_energy=E_F / pe,
+                      inv_diag_relax=inv_d if relax else 0.0,
+                      inv_offdiag_relax=inv_o if relax else 0.0)
+    amplitude = lattice * 1e11 * E0 / pe
+    t_begin = math.pi * t0_offset
+    t_end = t_begin + 2 * math.pi * n_cycles  # CosineLaser::base_duration
+    n = n_measurements or n_cycles * MEASUREMENTS_PER_CYCLE
+    pulse = api.cosine_pulse(amplitude, n_cycles, n, t_begin=t_begin,
+                             window=(t_begin, t_end + 2 * math.pi))
+    return Run(system_type, sys_, pulse, g, api.solver(1e-12, 1e-8), lattice)

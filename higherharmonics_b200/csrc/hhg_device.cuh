@@ -55,21 +55,53 @@ constexpr int kMinBlocksPerSM = 7;
 // Model variants.  *_SYM / *_X are the same physics with fewer distinct
 // pulse projections (PiFlux-2D with px == py; honeycomb with the field along
 // x, where the bonds 2 and 3 share one projection).
+// *_RELAX are the reference models with their relaxation-time right-hand
+// sides (PiFlux.cpp:113-186, Honeycomb.cpp:160-212, DiracSystem.cpp:213-251);
+// they stage the same pulse functions as their base model.
 enum Model {
     DIRAC2D = 0, PIFLUX2D = 1, PIFLUX3D = 2, HONEYCOMB = 3, DIRAC3D = 4,
-    PIFLUX2D_SYM = 5, HONEYCOMB_X = 6
+    PIFLUX2D_SYM = 5, HONEYCOMB_X = 6,
+    PIFLUX3D_RELAX = 7, HONEYCOMB_RELAX = 8, DIRAC3D_RELAX = 9
 };
+__host__ __device__ constexpr int base_model(int m) {
+    return m == PIFLUX3D_RELAX ? PIFLUX3D : m == HONEYCOMB_RELAX ? HONEYCOMB
+         : m == DIRAC3D_RELAX ? DIRAC3D : m;
+}
 
 // Number of staged pulse functions per model: A for the Dirac models, (cos,
-// sin) pairs of s A(t) for the lattice models.
-template <int M> struct Traits;
-template <> struct Traits<DIRAC2D> { static constexpr int NF = 1; };
-template <> struct Traits<DIRAC3D> { static constexpr int NF = 1; };
-template <> struct Traits<PIFLUX3D> { static constexpr int NF = 2; };
-template <> struct Traits<PIFLUX2D> { static constexpr int NF = 4; };
-template <> struct Traits<PIFLUX2D_SYM> { static constexpr int NF = 2; };
-template <> struct Traits<HONEYCOMB> { static constexpr int NF = 6; };
-template <> struct Traits<HONEYCOMB_X> { static constexpr int NF = 4; };
+// sin) pairs of s A(t) for the lattice models.  kRelax: FP64 RKF78 only.
+// kStart: the right-hand side also reads the step's start state.
+// kMinBlocks: integration CTAs per SM the register budget is sized for.
+template <int M> struct Traits {
+    static constexpr bool kRelax = false;
+    static constexpr bool kStart = false;
+    static constexpr int kMinBlocks = kMinBlocksPerSM;
+};
+template <> struct Traits<DIRAC2D> : Traits<-1> { static constexpr int NF = 1; };
+template <> struct Traits<DIRAC3D> : Traits<-1> { static constexpr int NF = 1; };
+template <> struct Traits<PIFLUX3D> : Traits<-1> { static constexpr int NF = 2; };
+template <> struct Traits<PIFLUX2D> : Traits<-1> { static constexpr int NF = 4; };
+template <> struct Traits<PIFLUX2D_SYM> : Traits<-1> { static constexpr int NF = 2; };
+template <> struct Traits<HONEYCOMB> : Traits<-1> { static constexpr int NF = 6; };
+template <> struct Traits<HONEYCOMB_X> : Traits<-1> { static constexpr int NF = 4; };
+template <> struct Traits<PIFLUX3D_RELAX> {
+    static constexpr int NF = 2;
+    static constexpr bool kRelax = true;
+    static constexpr bool kStart = true;
+    static constexpr int kMinBlocks = 4;  // the equilibrium terms need ~200 registers
+};
+template <> struct Traits<HONEYCOMB_RELAX> {
+    static constexpr int NF = 6;
+    static constexpr bool kRelax = true;
+    static constexpr bool kStart = false;
+    static constexpr int kMinBlocks = 4;  // the equilibrium terms need ~200 registers
+};
+template <> struct Traits<DIRAC3D_RELAX> {
+    static constexpr int NF = 1;
+    static constexpr bool kRelax = true;
+    static constexpr bool kStart = false;
+    static constexpr int kMinBlocks = 4;  // the equilibrium terms need ~200 registers
+};
 
 // Per-interval record (doubles):
 //   [0] t0, [1] t1, [2] center, [3] 1/half-width, [4] A(t_s) and
@@ -176,7 +208,7 @@ __device__ __forceinline__ void staged_values(const PulseDev &pd, double A, doub
     constexpr int NF = Traits<M>::NF;
     if constexpr (NF == 1) {
         v[0] = A;
-    } else if constexpr (M == PIFLUX3D) {
+    } else if constexpr (base_model(M) == PIFLUX3D) {
         sincos(A, &v[1], &v[0]);
     } else {
 #pragma unroll
@@ -457,6 +489,149 @@ template <typename R> struct ModelState<DIRAC3D, R> {
 };
 
 // ---------------------------------------------------------------------------
+// Relaxation-time models (FP64).  The equilibrium state follows k - A(t)
+// and the Fermi occupations of the reference (fermi_function,
+// GlobalDefinitions.hpp:36-41; beta = 0 stands for T = 0, a step function).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double fermi_occ(double e, double beta) {
+    if (beta == 0.0) return e != 0.0 ? (e < 0.0 ? 1.0 : 0.0) : 0.5;
+    return 1.0 / (1.0 + exp(beta * e));
+}
+// is_zero (GlobalDefinitions.hpp:61-71): |x| < 2^-44 by the biased exponent.
+__device__ __forceinline__ bool ref_is_zero_dev(double v) {
+    return (int)(((unsigned long long)__double_as_longlong(v) >> 52) & 0x7FF) < 0x3D3;
+}
+
+// PiFlux with relaxation (PiFlux.cpp:113-186):
+//   dS/dt = 4t (cx, cy, cos(kz - A)) x S - [g_d (S/3 - r_d) + g_o (2S/3 - r_o)]
+// with u = k - A (cos components, RESCUE_TRAFO when cos kx, cos ky vanish and
+// cos(kz - A) < 0), |u|, occupations a2 = f(-E_F + 2t|u|), b2 = f(-E_F - 2t|u|),
+// r_d = (a2 - b2) u / |u| and r_o = 2 sqrt(a2 b2) times the unit in-plane
+// direction of diagonal_sigma(X, u) (PiFlux.cpp:1037-1048) mapped back,
+// where X is the step's start state (the lambda's captured current_state,
+// which Boost.Odeint's try_step updates only on acceptance).
+// mp: [0] 4t, [1] 2t, [4] E_F, [5] beta, [6] g_d, [7] g_o.
+template <typename R> struct ModelState<PIFLUX3D_RELAX, R> {
+    static_assert(sizeof(R) == sizeof(double), "relaxation models run in FP64");
+    double pf, cx, cy, cz, sz, e2t, ef, beta, gd, go, gs;
+    bool rescue;
+    __device__ __forceinline__ void init(const PulseDev &p, const double *row) {
+        pf = p.mp[0];
+        cx = cos(row[0]);
+        cy = cos(row[1]);
+        sincos(row[2], &sz, &cz);
+        e2t = p.mp[1];
+        ef = p.mp[4];
+        beta = p.mp[5];
+        gd = p.mp[6];
+        go = p.mp[7];
+        gs = gd * (1.0 / 3.0) + go * (2.0 / 3.0);
+        rescue = ref_is_zero_dev(cx) && ref_is_zero_dev(cy);
+    }
+    __device__ __forceinline__ void rhs(const double *f, const double *S, const double *X,
+                                        double *dS) const {
+        const double czA = cz * f[0] + sz * f[1];  // cos(kz - A)
+        double ux = cx, uz = czA;
+        if (rescue && uz < 0.0) {
+            ux = fabs(uz) * 1e-4;
+            uz *= (1. - 0.5 * 1e-4 * 1e-4);
+        }
+        const double disp = sqrt(ux * ux + cy * cy + uz * uz);
+        const double a2 = fermi_occ(-ef + e2t * disp, beta);
+        const double b2 = fermi_occ(-ef - e2t * disp, beta);
+        const double fd = (a2 - b2) / disp;
+        // coherent part and the -g_s S + g_d r_d terms
+        dS[0] = pf * (cy * S[2] - czA * S[1]) - gs * S[0] + gd * (ux * fd);
+        dS[1] = pf * (czA * S[0] - cx * S[2]) - gs * S[1] + gd * (cy * fd);
+        dS[2] = pf * (cx * S[1] - cy * S[0]) - gs * S[2] + gd * (uz * fd);
+        const double sq = 2.0 * sqrt(a2 * b2);
+        if (sq != 0.0) {
+            const double zeps = uz + disp;
+            const double inv_norm = 1.0 / (disp * zeps);
+            // diagonal_sigma numerators (x, y) of the start state
+            const double z2 = zeps * zeps, xx = ux * ux, yy = cy * cy, xy = 2.0 * ux * cy;
+            const double n0 = X[0] * (z2 - xx + yy) - xy * X[1] - (2.0 * ux * zeps) * X[2];
+            const double n1 = X[1] * (z2 + xx - yy) - xy * X[0] - (2.0 * cy * zeps) * X[2];
+            const double n2 = n0 * n0 + n1 * n1;
+            double prod, imag;
+            // is_zero(|diagonal_sigma_xy|), |.| = sqrt(n2) / (2 disp zeps)
+            if (n2 * (0.25 * inv_norm * inv_norm) < 0x1p-88) {
+                prod = sq;
+                imag = 0.0;
+            } else {
+                const double r = sq * rsqrt(n2);
+                prod = n0 * r;
+                imag = n1 * r;
+            }
+            const double go_n = go * inv_norm;
+            dS[0] += go_n * (prod * (yy + uz * zeps) - imag * (ux * cy));
+            dS[1] += go_n * (imag * (xx + uz * zeps) - prod * (ux * cy));
+            dS[2] -= go_n * ((prod * ux + imag * cy) * zeps);
+        }
+    }
+    __device__ __forceinline__ double vertex(const double *r, const double *S) const {
+        return (sz * r[1] - cz * r[2]) * S[2];
+    }
+};
+
+// Honeycomb with relaxation (Honeycomb.cpp:160-212): the coherent form minus
+// g (S - S_eq(k - A)), S_eq = ic_sigma = (-(a2 - b2) Re g/|g|, (a2 - b2) Im g/|g|,
+// -2 sqrt(a2 b2)), a2 = f(E_F - t|g|), b2 = f(E_F + t|g|) (Honeycomb.cpp:347-361).
+// mp: [0] 2t, [4] E_F, [5] beta, [6] g (mass 0).
+template <typename R> struct ModelState<HONEYCOMB_RELAX, R> : HoneycombState<double, false> {
+    static_assert(sizeof(R) == sizeof(double), "relaxation models run in FP64");
+    double ef, beta, g;
+    __device__ __forceinline__ void init(const PulseDev &p, const double *row) {
+        HoneycombState<double, false>::init(p, row);
+        ef = p.mp[4];
+        beta = p.mp[5];
+        g = p.mp[6];
+    }
+    __device__ __forceinline__ void rhs(const double *f, const double *S, double *dS) const {
+        double gr, gi;  // 2t Re gamma', 2t Im gamma'
+        gamma(f, gr, gi);
+        const double G = sqrt(gr * gr + gi * gi);
+        const double tg = 0.5 * G;  // t |gamma'|
+        const double a2 = fermi_occ(ef - tg, beta);
+        const double b2 = fermi_occ(ef + tg, beta);
+        const double dg = (a2 - b2) / G;
+        const double eq2 = -2.0 * sqrt(a2 * b2);
+        dS[0] = -(S[2] * gi) - g * (S[0] + dg * gr);
+        dS[1] = -(S[2] * gr) - g * (S[1] - dg * gi);
+        dS[2] = (S[0] * gi + S[1] * gr) - g * (S[2] - eq2);
+    }
+};
+
+// DiracSystem with relaxation towards the initial state (DiracSystem.cpp:213-251).
+// mp: [6] g; the initial state comes from the k row.
+template <typename R> struct ModelState<DIRAC3D_RELAX, R> : ModelState<DIRAC3D, double> {
+    static_assert(sizeof(R) == sizeof(double), "relaxation models run in FP64");
+    double g, e0, e1, e2;
+    __device__ __forceinline__ void init(const PulseDev &p, const double *row) {
+        ModelState<DIRAC3D, double>::init(p, row);
+        g = p.mp[6];
+        e0 = row[4];
+        e1 = row[5];
+        e2 = row[6];
+    }
+    __device__ __forceinline__ void rhs(const double *f, const double *S, double *dS) const {
+        const double mx = ax * f[0];
+        const double mz = mk2 - az * f[0];
+        dS[0] = mz * S[1] - (S[0] - e0) * g;
+        dS[1] = mx * S[2] - S[0] * mz - (S[1] - e1) * g;
+        dS[2] = -mx * S[1] - (S[2] - e2) * g;
+    }
+};
+
+// Right-hand side call: models with kStart also read the step's start state x.
+template <int M, typename R, class V>
+__device__ __forceinline__ void model_rhs(const ModelState<M, R> &ms, const V *f, const R *S,
+                                          const double *x, R *dS) {
+    if constexpr (Traits<M>::kStart) ms.rhs(f, S, x, dS);
+    else ms.rhs(f, S, dS);
+}
+
+// ---------------------------------------------------------------------------
 // One attempted Fehlberg 7(8) step (E. Fehlberg, NASA TR R-287, 1968):
 // 13 stages, the 8th-order solution propagated, error = b8 - b7 =
 // 41/840 (k12 + k13 - k1 - k11).  Stage sums are written out with the
@@ -472,7 +647,7 @@ __device__ __forceinline__ void rkf78_attempt(const ModelState<M, R> &ms, const 
     const R xr[3] = {R(x[0]), R(x[1]), R(x[2])};
     const R hr = R(h);
     ev(0, t, f);
-    ms.rhs(f, xr, k[0]);
+    model_rhs(ms, f, xr, x, k[0]);
     // stages 7, 11 and 12 share their nodes with 3, 0 and 10 (c = 1/6, 0, 1)
     typename Num<R>::V f0[Eval::kReuse ? NF : 1], f3[Eval::kReuse ? NF : 1],
         f10[Eval::kReuse ? NF : 1];
@@ -495,7 +670,7 @@ __device__ __forceinline__ void rkf78_attempt(const ModelState<M, R> &ms, const 
                 if (s == 3) f3[n] = f[n]; else f10[n] = f[n];                       \
             }                                                                       \
         }                                                                           \
-        ms.rhs(f, xt, k[s]);                                                        \
+        model_rhs(ms, f, xt, x, k[s]);                                              \
     }
     // sums grouped as independent pairs (shorter dependency chains)
     HHG_STAGE(1, R(2.0 / 27.0) * k[0][i])
@@ -727,7 +902,7 @@ __host__ __device__ constexpr int mlp_smem_bytes() {
 constexpr double kCoarsen = 1.0 / 600.0;
 
 template <int M, int D, typename R, int STEPPER, int PROPOSER>
-__global__ void __launch_bounds__(kBlockThreads, kMinBlocksPerSM) bz_integrate_kernel(const KParams P) {
+__global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integrate_kernel(const KParams P) {
     constexpr int NF = Traits<M>::NF;
     constexpr bool kDyadic = PROPOSER == 2 || PROPOSER == 3;
     constexpr bool kLearned = PROPOSER == 3;

@@ -153,19 +153,35 @@ bool ref_is_zero(double v) {
     return (int)((bits >> 52) & 0x7FF) < 0x3D3;
 }
 
-// Initial Bloch vector of the filled lower band at T = 0, S0 = -d_hat(k).
+// fermi_function (GlobalDefinitions.hpp:36-41); beta == 0 stands for the
+// reference's T = 0 sentinel (a step with 1/2 at zero energy).
+double fermi_occ(double e, double beta) {
+    if (beta == 0.0) return e != 0 ? (e < 0 ? 1.0 : 0.0) : 0.5;
+    return 1. / (1. + exp(beta * e));
+}
+
+// PiFlux::ic_sigma (PiFlux.cpp:519-549) with alpha^2 = occupation_a, beta^2 =
+// occupation_b (PiFlux.cpp:420-426) at the momentum cosines (cx, cy, cz).
+void piflux_ic(const hhg_system_desc &s, double cx, double cy, double cz, double *s0) {
+    const double disp = sqrt(cx * cx + cy * cy + cz * cz);
+    const double a2 = fermi_occ(-s.fermi_energy + 2 * s.hopping * disp, s.beta);
+    const double b2 = fermi_occ(-s.fermi_energy - 2 * s.hopping * disp, s.beta);
+    const double diff = a2 - b2;
+    const double prod = 2 * sqrt(a2 * b2);
+    const double zeps = cz + disp;
+    s0[0] = (diff * cx * zeps + prod * (cy * cy + cz * zeps)) / (disp * zeps);
+    s0[1] = (diff * cy * zeps - prod * cx * cy) / (disp * zeps);
+    s0[2] = (diff * cz * zeps - prod * cx * zeps) / (disp * zeps);
+}
+
+// Initial Bloch vector: the reference models' ic_sigma / Fermi-occupied state
+// (T = 0, E_F = 0: the filled lower band), the variants' filled lower band
+// S0 = -d_hat(k).
 void initial_state(const hhg_system_desc &s, double kx, double ky, double kz, double *s0) {
     switch (s.kind) {
-    case HHG_SYS_PIFLUX3D: {
-        // PiFlux::ic_sigma with alpha^2 = 0, beta^2 = 1 (PiFlux.cpp:519-549)
-        const double cx = cos(kx), cy = cos(ky), cz = cos(kz);
-        const double disp = sqrt(cx * cx + cy * cy + cz * cz);
-        const double zeps = cz + disp;
-        s0[0] = (-1.0 * cx * zeps + 0.0) / (disp * zeps);
-        s0[1] = (-1.0 * cy * zeps - 0.0) / (disp * zeps);
-        s0[2] = (-1.0 * cz * zeps - 0.0) / (disp * zeps);
+    case HHG_SYS_PIFLUX3D:
+        piflux_ic(s, cos(kx), cos(ky), cos(kz), s0);
         break;
-    }
     case HHG_SYS_PIFLUX2D: {
         const double cx = cos(kx), cy = cos(ky);
         const double n = sqrt(cx * cx + cy * cy);
@@ -192,10 +208,14 @@ void initial_state(const hhg_system_desc &s, double kx, double ky, double kz, do
             gim += sin(ph);
         }
         if (s.mass == 0.0) {
+            // Honeycomb::ic_sigma with occupation_a/b (Honeycomb.cpp:347-361)
             const double ag = hypot(gre, gim);
-            s0[0] = -1.0 * gre / ag;
-            s0[1] = 1.0 * gim / ag;
-            s0[2] = -0.0;
+            const double a2 = fermi_occ(s.fermi_energy - s.hopping * ag, s.beta);
+            const double b2 = fermi_occ(s.fermi_energy + s.hopping * ag, s.beta);
+            const double diff = a2 - b2;
+            s0[0] = -diff * gre / ag;
+            s0[1] = diff * gim / ag;
+            s0[2] = -(2 * sqrt(a2 * b2));
         } else {
             const double d0 = s.hopping * gre, d1 = -s.hopping * gim, d2 = s.mass;
             const double n = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
@@ -205,11 +225,17 @@ void initial_state(const hhg_system_desc &s, double kx, double ky, double kz, do
         }
         break;
     }
-    case HHG_SYS_DIRAC3D:
-        s0[0] = 0.0;
+    case HHG_SYS_DIRAC3D: {
+        // (2 a0 b0, 0, a0^2 - b0^2), a0 = f(E_F + |k|), b0 = f(E_F - |k|)
+        // (DiracSystem.cpp:155-158, 253-255); kx = k_z, ky = kappa
+        const double disp = sqrt(ky * ky + kx * kx);
+        const double a0 = fermi_occ(s.fermi_energy + disp, s.beta);
+        const double b0 = fermi_occ(s.fermi_energy - disp, s.beta);
+        s0[0] = 2. * a0 * b0;
         s0[1] = 0.0;
-        s0[2] = -1.0;  // (2 a0 b0, 0, a0^2 - b0^2), a0 = 0, b0 = 1 (DiracSystem.cpp:155-158)
+        s0[2] = a0 * a0 - b0 * b0;
         break;
+    }
     default:
         s0[0] = s0[1] = s0[2] = 0.0;
     }
@@ -313,11 +339,7 @@ void build_rows(const hhg_system_desc &s, const hhg_grid_desc &g, double *out) {
                                     o[2] = kz;
                                     o[3] = mw * yw[q][j] * zw[z];
                                     const double cx = cos(kx), cy = cos(ky);
-                                    const double disp = sqrt(cx * cx + cy * cy + cz * cz);
-                                    const double zeps = cz + disp;
-                                    o[4] = (-1.0 * cx * zeps + 0.0) / (disp * zeps);
-                                    o[5] = (-1.0 * cy * zeps - 0.0) / (disp * zeps);
-                                    o[6] = (-1.0 * cz * zeps - 0.0) / (disp * zeps);
+                                    piflux_ic(s, cx, cy, cz, o + 4);
                                     o[7] = 0.0;
                                     last_cx = cx;
                                     last_cy = cy;
@@ -361,8 +383,19 @@ hhg_status check_system(hhg_ctx *ctx, const hhg_system_desc *s) {
     if (s->kind < HHG_SYS_DIRAC2D || s->kind > HHG_SYS_DIRAC3D)
         return set_err(ctx, HHG_BAD_CONFIG, "System type not recognized");
     if (!std::isfinite(s->hopping) || !std::isfinite(s->velocity) || !std::isfinite(s->mass) ||
-        !std::isfinite(s->pol_x) || !std::isfinite(s->pol_y))
+        !std::isfinite(s->pol_x) || !std::isfinite(s->pol_y) || !std::isfinite(s->beta) ||
+        !std::isfinite(s->fermi_energy) || !std::isfinite(s->inv_diag_relax) ||
+        !std::isfinite(s->inv_offdiag_relax))
         return set_err(ctx, HHG_BAD_CONFIG, "non-finite system parameter");
+    if (s->beta < 0.0 || s->inv_diag_relax < 0.0 || s->inv_offdiag_relax < 0.0)
+        return set_err(ctx, HHG_BAD_CONFIG, "beta and the relaxation rates must be >= 0");
+    const bool thermal = s->beta != 0.0 || s->fermi_energy != 0.0 || s->inv_diag_relax > 0.0;
+    const bool reference_model = s->kind == HHG_SYS_PIFLUX3D || s->kind == HHG_SYS_DIRAC3D ||
+                                 (s->kind == HHG_SYS_HONEYCOMB && s->mass == 0.0);
+    if (thermal && !reference_model)
+        return set_err(ctx, HHG_UNSUPPORTED,
+                       "temperature, Fermi energy and relaxation are defined for the reference "
+                       "models (PiFlux-3D, Honeycomb without mass, Dirac-3D) only");
     return HHG_OK;
 }
 
@@ -411,6 +444,12 @@ hhg_status check_pulse(hhg_ctx *ctx, const hhg_pulse_desc &p) {
 // Internal kernel model (hhg::Model): the ABI kind, or a variant with fewer
 // distinct pulse projections when the polarisation allows it.
 int kernel_model(const hhg_system_desc &s) {
+    if (s.inv_diag_relax > 0.0) {
+        // relaxation right-hand sides (PiFlux.cpp:509-516, Honeycomb.cpp:214-223)
+        if (s.kind == HHG_SYS_PIFLUX3D) return hhg::PIFLUX3D_RELAX;
+        if (s.kind == HHG_SYS_HONEYCOMB) return hhg::HONEYCOMB_RELAX;
+        if (s.kind == HHG_SYS_DIRAC3D) return hhg::DIRAC3D_RELAX;
+    }
     if (s.kind == HHG_SYS_PIFLUX2D && s.pol_x == s.pol_y) return hhg::PIFLUX2D_SYM;
     if (s.kind == HHG_SYS_HONEYCOMB && s.pol_y == 0.0) return hhg::HONEYCOMB_X;
     return s.kind;
@@ -425,7 +464,7 @@ std::string plan_key(const hhg_system_desc *sys, const hhg_pulse_desc *pulses, i
     std::string k;
     auto put = [&k](const void *p, size_t n) { k.append(static_cast<const char *>(p), n); };
     put(&sys->kind, 4);
-    put(&sys->hopping, 8 * 5);
+    put(&sys->hopping, 8 * 9);
     put(&n_pulses, 4);
     for (int i = 0; i < n_pulses; ++i) {
         const hhg_pulse_desc &q = pulses[i];
@@ -463,7 +502,7 @@ int kernel_proposer(int abi) {
 }
 
 int model_nf(int m) {
-    switch (m) {
+    switch (hhg::base_model(m)) {
     case hhg::DIRAC2D: return 1;
     case hhg::DIRAC3D: return 1;
     case hhg::PIFLUX3D: return 2;
@@ -521,6 +560,52 @@ int choose_degree(const hhg_pulse_desc &p, const double *proj, int nf) {
     return -1;
 }
 
+// Thermal and relaxation constants of the *_RELAX kernel models, in the
+// pulse's energy units (energy_scale es multiplies energies and rates,
+// divides beta): [1] 2t (PiFlux occupation energies), [4] E_F, [5] beta,
+// [6] diagonal rate, [7] off-diagonal rate.
+void set_relax_params(const hhg_system_desc &s, double es, double *mp) {
+    if (s.inv_diag_relax <= 0.0) return;
+    if (s.kind == HHG_SYS_PIFLUX3D) mp[1] = 2.0 * s.hopping * es;
+    mp[4] = s.fermi_energy * es;
+    mp[5] = s.beta / es;
+    mp[6] = s.inv_diag_relax * es;
+    mp[7] = s.inv_offdiag_relax * es;
+}
+
+// A(t) of one pulse on the host, as the device's laser_exact.
+double host_laser(const hhg_pulse_desc &q, double t) {
+    const double te = q.t_begin + 2 * kPi * q.n_cycles;
+    double env = 0.0;
+    if (!(t <= q.t_begin || t >= te)) env = 0.5 * (1. - cos((1. / q.n_cycles) * (t - q.t_begin)));
+    return q.amplitude * (env * sin(t + q.phase));
+}
+
+// Requests the relaxation kernels do not cover.
+hhg_status check_relax(hhg_ctx *ctx, const hhg_system_desc &s, const hhg_pulse_desc *pulses,
+                       int n_pulses, const hhg_solver_opts &o) {
+    if (s.inv_diag_relax <= 0.0) return HHG_OK;
+    if (o.stepper != HHG_STEPPER_RKF78 || o.precision != HHG_PREC_FP64)
+        return set_err(ctx, HHG_UNSUPPORTED, "relaxation right-hand sides run with FP64 RKF78 only");
+    if (s.kind == HHG_SYS_PIFLUX3D && s.beta != 0.0 && s.inv_offdiag_relax > 0.0 &&
+        o.proposer != HHG_PROPOSER_NONE)
+        // the off-diagonal equilibrium reads the step's start state
+        // (PiFlux.cpp:145), so j(t) is a first-order function of the step
+        // sequence: only the reference schedule reproduces the reference
+        return set_err(ctx, HHG_UNSUPPORTED,
+                       "PiFlux relaxation at T > 0 depends on the step sequence; use the reference "
+                       "step schedule (HHG_PROPOSER_NONE)");
+    if (s.kind == HHG_SYS_HONEYCOMB)
+        for (int p = 0; p < n_pulses; ++p)
+            if (host_laser(pulses[p], pulses[p].window_begin) != 0.0)
+                // the reference starts from the equilibrium at k - A(t_begin)
+                // (Honeycomb.cpp:193-194); the k table holds the one at A = 0
+                return set_err(ctx, HHG_UNSUPPORTED,
+                               "honeycomb relaxation needs A(window_begin) = 0 (window starting "
+                               "at or before the pulse)");
+    return HHG_OK;
+}
+
 hhg_status launch_variant(const hhg_plan *pl, hhg::LaunchReq &r) {
     cudaError_t e = cudaErrorInvalidValue;
     switch (pl->model) {
@@ -531,6 +616,9 @@ hhg_status launch_variant(const hhg_plan *pl, hhg::LaunchReq &r) {
     case HHG_SYS_DIRAC3D: e = hhg::launch_dirac3d(r); break;
     case hhg::PIFLUX2D_SYM: e = hhg::launch_piflux2d_sym(r); break;
     case hhg::HONEYCOMB_X: e = hhg::launch_honeycomb_x(r); break;
+    case hhg::PIFLUX3D_RELAX: e = hhg::launch_piflux3d_relax(r); break;
+    case hhg::HONEYCOMB_RELAX: e = hhg::launch_honeycomb_relax(r); break;
+    case hhg::DIRAC3D_RELAX: e = hhg::launch_dirac3d_relax(r); break;
     }
     if (e != cudaSuccess)
         return set_err(pl->ctx, HHG_CUDA_ERROR, std::string("integration launch: ") + cudaGetErrorString(e));
@@ -547,6 +635,9 @@ hhg_status stage_variant(const hhg_plan *pl, hhg::StageReq &s) {
     case HHG_SYS_DIRAC3D: e = hhg::stage_dirac3d(s); break;
     case hhg::PIFLUX2D_SYM: e = hhg::stage_piflux2d_sym(s); break;
     case hhg::HONEYCOMB_X: e = hhg::stage_honeycomb_x(s); break;
+    case hhg::PIFLUX3D_RELAX: e = hhg::stage_piflux3d_relax(s); break;
+    case hhg::HONEYCOMB_RELAX: e = hhg::stage_honeycomb_relax(s); break;
+    case hhg::DIRAC3D_RELAX: e = hhg::stage_dirac3d_relax(s); break;
     }
     if (e != cudaSuccess)
         return set_err(pl->ctx, HHG_CUDA_ERROR, std::string("staging launch: ") + cudaGetErrorString(e));
@@ -668,6 +759,7 @@ hhg_status hhg_plan_create(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_p
         return set_err(ctx, HHG_BAD_CONFIG, "tolerances must be >= 0 and not both 0");
     if (o.max_failed_steps < 1) o.max_failed_steps = 500;
     if (o.max_attempts_per_interval < 1) o.max_attempts_per_interval = 100000;
+    if ((st = check_relax(ctx, *sys, pulses, n_pulses, o)) != HHG_OK) return st;
 
     HHG_CUDA(ctx, cudaSetDevice(ctx->device));
     hhg_plan *pl = new hhg_plan();
@@ -685,7 +777,7 @@ hhg_status hhg_plan_create(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_p
     // per-pulse records, staged projections and degree
     const double nny = 0.5 * kSqrt3;
     double proj[3] = {0, 0, 0};
-    switch (pl->model) {
+    switch (hhg::base_model(pl->model)) {
     case hhg::PIFLUX2D:
         proj[0] = sys->pol_x;
         proj[1] = sys->pol_y;
@@ -782,6 +874,7 @@ hhg_status hhg_plan_create(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_p
         }
         d.mp[2] = sys->pol_x;
         d.mp[3] = sys->pol_y;
+        set_relax_params(*sys, es, d.mp);
         for (int n = 0; n < 3; ++n) d.s[n] = proj[n];
         // sample-0 record, exact: A(t_0) and the staged functions at it
         const double t0s = 0 * d.measure_every + d.window_begin;
@@ -790,7 +883,7 @@ hhg_status hhg_plan_create(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_p
         const double A0 = d.amplitude * (env * sin(t0s + d.phase));
         d.s0rec[0] = A0;
         if (nf == 1) d.s0rec[1] = A0;
-        else if (pl->model == hhg::PIFLUX3D) {
+        else if (hhg::base_model(pl->model) == hhg::PIFLUX3D) {
             d.s0rec[1] = cos(A0);
             d.s0rec[2] = sin(A0);
         } else
@@ -1250,7 +1343,7 @@ hhg_status prepare_pulse(const hhg_system_desc *sys, const hhg_pulse_desc *pulse
     out.nf = model_nf(out.model);
     const double nny = 0.5 * kSqrt3;
     double proj[3] = {0, 0, 0};
-    switch (out.model) {
+    switch (hhg::base_model(out.model)) {
     case hhg::PIFLUX2D: proj[0] = sys->pol_x; proj[1] = sys->pol_y; break;
     case hhg::PIFLUX2D_SYM: proj[0] = sys->pol_x; break;
     case hhg::HONEYCOMB:
@@ -1284,6 +1377,7 @@ hhg_status prepare_pulse(const hhg_system_desc *sys, const hhg_pulse_desc *pulse
     }
     p.mp[2] = sys->pol_x;
     p.mp[3] = sys->pol_y;
+    set_relax_params(*sys, es, p.mp);
     for (int n = 0; n < 3; ++n) p.s[n] = proj[n];
     const double t0s = 0 * p.measure_every + p.window_begin;
     double env = 0.0;
@@ -1291,7 +1385,7 @@ hhg_status prepare_pulse(const hhg_system_desc *sys, const hhg_pulse_desc *pulse
     const double A0 = p.amplitude * (env * sin(t0s + p.phase));
     p.s0rec[0] = A0;
     if (out.nf == 1) p.s0rec[1] = A0;
-    else if (out.model == hhg::PIFLUX3D) {
+    else if (hhg::base_model(out.model) == hhg::PIFLUX3D) {
         p.s0rec[1] = cos(A0);
         p.s0rec[2] = sin(A0);
     } else

@@ -47,8 +47,9 @@ cudaError_t launch_one(const LaunchReq &r) {
 
 template <int M, int D>
 cudaError_t launch_deg(const LaunchReq &r) {
-    if (r.stepper == 1) return launch_one<M, D, double, 1, 0>(r);
-    if (r.precision == 0) {
+    if constexpr (Traits<M>::kRelax) {
+        // relaxation right-hand sides: FP64 controlled RKF78 only
+        if (r.stepper != 0 || r.precision != 0) return cudaErrorNotSupported;
         switch (r.proposer) {
         case 0: return launch_one<M, D, double, 0, 0>(r);
         case 1: return launch_one<M, D, double, 0, 1>(r);
@@ -57,14 +58,26 @@ cudaError_t launch_deg(const LaunchReq &r) {
         case 4: return launch_one<M, D, double, 0, 4>(r);
         }
         return cudaErrorInvalidValue;
+    } else {
+        if (r.stepper == 1) return launch_one<M, D, double, 1, 0>(r);
+        if (r.precision == 0) {
+            switch (r.proposer) {
+            case 0: return launch_one<M, D, double, 0, 0>(r);
+            case 1: return launch_one<M, D, double, 0, 1>(r);
+            case 2: return launch_one<M, D, double, 0, 2>(r);
+            case 3: return launch_one<M, D, double, 0, 3>(r);
+            case 4: return launch_one<M, D, double, 0, 4>(r);
+            }
+            return cudaErrorInvalidValue;
+        }
+        switch (r.proposer) {
+        case 0: return launch_one<M, D, float, 0, 0>(r);
+        case 1: return launch_one<M, D, float, 0, 1>(r);
+        case 2: return launch_one<M, D, float, 0, 2>(r);
+        case 3: return launch_one<M, D, float, 0, 3>(r);
+        }
+        return cudaErrorInvalidValue;
     }
-    switch (r.proposer) {
-    case 0: return launch_one<M, D, float, 0, 0>(r);
-    case 1: return launch_one<M, D, float, 0, 1>(r);
-    case 2: return launch_one<M, D, float, 0, 2>(r);
-    case 3: return launch_one<M, D, float, 0, 3>(r);
-    }
-    return cudaErrorInvalidValue;
 }
 
 template <int M>
@@ -107,6 +120,9 @@ cudaError_t launch_honeycomb(const LaunchReq &r);
 cudaError_t launch_dirac3d(const LaunchReq &r);
 cudaError_t launch_piflux2d_sym(const LaunchReq &r);
 cudaError_t launch_honeycomb_x(const LaunchReq &r);
+cudaError_t launch_piflux3d_relax(const LaunchReq &r);
+cudaError_t launch_honeycomb_relax(const LaunchReq &r);
+cudaError_t launch_dirac3d_relax(const LaunchReq &r);
 cudaError_t stage_dirac2d(const StageReq &s);
 cudaError_t stage_piflux2d(const StageReq &s);
 cudaError_t stage_piflux3d(const StageReq &s);
@@ -114,6 +130,9 @@ cudaError_t stage_honeycomb(const StageReq &s);
 cudaError_t stage_dirac3d(const StageReq &s);
 cudaError_t stage_piflux2d_sym(const StageReq &s);
 cudaError_t stage_honeycomb_x(const StageReq &s);
+cudaError_t stage_piflux3d_relax(const StageReq &s);
+cudaError_t stage_honeycomb_relax(const StageReq &s);
+cudaError_t stage_dirac3d_relax(const StageReq &s);
 
 }  // namespace hhg
 

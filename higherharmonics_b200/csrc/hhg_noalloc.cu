@@ -138,6 +138,10 @@ extern "C" hhg_status hhg_gpu_current_density_noalloc(const hhg_system_desc *sys
         set_msg(err, err_cap, "measurement interval too coarse for the staged pulse interpolants");
         return HHG_UNSUPPORTED;
     }
+    if (sys->inv_diag_relax > 0.0) {
+        set_msg(err, err_cap, "the allocation-free entry point integrates the coherent equations only");
+        return HHG_UNSUPPORTED;
+    }
     const int N = pulse->n_measurements;
     const int slot = hhg::slot_doubles(prep.nf, prep.degree);
     const long long items = (n_rows + 31) / 32;

@@ -1,4 +1,6 @@
-"""The five synthetic workloads the engine is measured and checked on.
+"""The synthetic workloads the engine is measured and checked on: the five
+configurations of the hot path plus the reference's production PiFlux run
+with relaxation.
 
 Units: the reference's (time in 1/omega_L, energies in hbar omega_L).  A
 model given in "reduced units" with a laser frequency omega is integrated
@@ -53,7 +55,9 @@ class Workload:
     @property
     def n_k(self) -> int:
         g = self.grid
-        return g.n1 * g.n2
+        if g.kind in (api.GRID_TENSOR_GL, api.GRID_RHOMBIC_GL):
+            return g.n1 * g.n2
+        return int(api.grid_rows(self.system, g).shape[0])
 
 
 def dirac2d_64(n_grid=64, n_cycles=4, omega=0.1) -> Workload:
@@ -129,10 +133,44 @@ def honeycomb_1024x64(n_pulses=64, n_grid=1024, n_cycles=6, omega=0.08) -> Workl
                     honeycomb_1024x64.__doc__)
 
 
+# params.config's material with the cosine laser (the reference ships that
+# file with laser_type powerlaw1, which has no device form yet)
+PIFLUX_PRODUCTION_CONFIG = """\
+T 300
+E_F 118
+v_F 1.5e6
+band_width 300
+field_amplitude 1.6
+photon_energy 5.25
+diagonal_relaxation_time 15
+offdiagonal_relaxation_time -1
+laser_type cosine
+n_laser_cycles {n_cycles}
+t0_offset 0
+system_type PiFlux
+"""
+
+
+def piflux3d_relax(n_cycles=16) -> Workload:
+    """The reference's production PiFlux run: T = 300 K, E_F = 118 meV,
+    v_F = 1.5e6 m/s, band width 300 meV, photon energy 5.25 meV, field
+    1.6 MV/cm, diagonal relaxation time 15 fs (off-diagonal -> diagonal),
+    cosine laser, 16 cycles, 1024 intervals per cycle over the pulse plus one
+    relaxation cycle, on the reference's continuum-limit grid (z_range 32,
+    N_coarse 4: 151 552 k-points); FP64 RKF78 1e-12 / 1e-8 with the reference
+    step schedule (the relaxation right-hand side reads the step's start
+    state, so the schedule is part of the result)."""
+    from . import config
+    run = config.from_config(PIFLUX_PRODUCTION_CONFIG.format(n_cycles=n_cycles))
+    return Workload(f"piflux3d_relax_ref_{n_cycles}cyc", run.system, [run.pulse], run.grid,
+                    dict(abs_tol=1e-12, rel_tol=1e-8), piflux3d_relax.__doc__)
+
+
 ALL = {
     "dirac2d_64": dirac2d_64,
     "piflux2d_256": piflux2d_256,
     "honeycomb_512": honeycomb_512,
     "dirac2d_sweep": dirac2d_sweep,
     "honeycomb_1024x64": honeycomb_1024x64,
+    "piflux3d_relax": piflux3d_relax,
 }

@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define HHG_ABI_VERSION 2
+#define HHG_ABI_VERSION 3
 
 /* Errors: the reference throws std::invalid_argument / std::runtime_error
  * (sources/hhg.cpp:232, Dispatch/PiFluxDispatcher.cpp:104) and Boost.Odeint
@@ -59,7 +59,25 @@ typedef enum hhg_system_kind {
 /* System: replaces the System ctor arguments (e.g. PiFlux.cpp:56-71).
  * hopping = t (PiFlux: band_width/sqrt(12), Honeycomb: band_width/6),
  * velocity = v (Dirac2D), mass = gap term, (pol_x, pol_y) = field
- * polarisation unit vector (Honeycomb's laser_theta, Honeycomb.hpp:93-95). */
+ * polarisation unit vector (Honeycomb's laser_theta, Honeycomb.hpp:93-95).
+ *
+ * Thermal initial state and relaxation (the reference models PiFlux-3D,
+ * Honeycomb without mass and Dirac-3D only; the variant models take the
+ * filled lower band and no relaxation):
+ *   beta         = photon_energy / (k_B T) (PiFlux.cpp:63); 0 stands for
+ *                  T = 0, the reference's is_zero(T) branch, whose Fermi
+ *                  function is a step (GlobalDefinitions.hpp:36-41);
+ *   fermi_energy = E_F / photon_energy (PiFlux.cpp:64);
+ *   inv_diag_relax, inv_offdiag_relax = 1e15 hbar / (tau photon_energy)
+ *                  (PiFlux.cpp:67-68); inv_diag_relax > 0 selects the
+ *                  relaxation right-hand side as the reference's
+ *                  __time_evolution__ does (PiFlux.cpp:509-516,
+ *                  Honeycomb.cpp:214-223); the off-diagonal rate is read by
+ *                  PiFlux-3D only (the dispatcher substitutes the diagonal
+ *                  time when offdiagonal_relaxation_time <= 0,
+ *                  PiFluxDispatcher.cpp:22-35).
+ * All four are in the model's energy units: a pulse's energy_scale
+ * multiplies fermi_energy and the rates and divides beta. */
 typedef struct hhg_system_desc {
     int32_t kind;
     int32_t reserved;
@@ -67,6 +85,10 @@ typedef struct hhg_system_desc {
     double velocity;
     double mass;
     double pol_x, pol_y;
+    double beta;
+    double fermi_energy;
+    double inv_diag_relax;
+    double inv_offdiag_relax;
 } hhg_system_desc;
 
 typedef enum hhg_pulse_kind {

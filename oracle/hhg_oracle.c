@@ -159,6 +159,7 @@ static const double NN[3][2] = {{1.0, 0.0}, {-0.5, 0.5 * 1.732050807568877293527
 
 typedef struct {
     double kx, ky, kz, cx, cy; /* cx/cy cache cos(kx), cos(ky) for the PiFlux-3D form */
+    double s0[3];              /* initial Bloch vector (Dirac-3D relaxation target) */
 } kctx;
 
 static inline void cross(const double *m, const double *s, double *o) {
@@ -168,11 +169,100 @@ static inline void cross(const double *m, const double *s, double *o) {
     o[2] = m[0] * s[1] - m[1] * s[0];
 }
 
+/* fermi_function (sources/HHG/GlobalDefinitions.hpp:36-41); beta == 0
+ * stands for the reference's T = 0 sentinel beta = numeric_limits::max(),
+ * for which the function is a step with 1/2 at zero energy. */
+static double fermi(double energy, double beta) {
+    if (beta == 0.0) return energy != 0 ? (energy < 0 ? 1.0 : 0.0) : 0.5;
+    return 1. / (1. + exp(beta * energy));
+}
+
+/* PiFlux::ic_sigma (PiFlux.cpp:519-549) with alpha^2 = occupation_a and
+ * beta^2 = occupation_b (PiFlux.cpp:420-426) of the momentum (cx, cy, cz). */
+static void piflux_ic(const orc_model *m, double cx, double cy, double cz, double *s0) {
+    const double disp = sqrt(cx * cx + cy * cy + cz * cz);
+    const double a2 = fermi(-m->fermi_energy + 2 * m->hopping * disp, m->beta);
+    const double b2 = fermi(-m->fermi_energy - 2 * m->hopping * disp, m->beta);
+    const double diff = a2 - b2;
+    const double prod = 2 * sqrt(a2 * b2);
+    const double zeps = cz + disp;
+    s0[0] = (diff * cx * zeps + prod * (cy * cy + cz * zeps)) / (disp * zeps);
+    s0[1] = (diff * cy * zeps - prod * cx * cy) / (disp * zeps);
+    s0[2] = (diff * cz * zeps - prod * cx * zeps) / (disp * zeps);
+}
+
+/* Honeycomb::ic_sigma (Honeycomb.cpp:355-361) with occupation_a/b
+ * (Honeycomb.cpp:347-353) at gamma = gre + i gim. */
+static void honeycomb_ic(const orc_model *m, double gre, double gim, double *s0) {
+    const double ag = hypot(gre, gim);
+    const double a2 = fermi(m->fermi_energy - m->hopping * ag, m->beta);
+    const double b2 = fermi(m->fermi_energy + m->hopping * ag, m->beta);
+    const double diff = a2 - b2;
+    const double prod = 2 * sqrt(a2 * b2);
+    s0[0] = -diff * gre / ag;
+    s0[1] = diff * gim / ag;
+    s0[2] = -prod;
+}
+
+/* PiFlux::time_evolution_diagonal_relaxation right_side with its
+ * update_equilibrium_state (PiFlux.cpp:113-186).  The equilibrium's
+ * off-diagonal direction is taken from diagonal_sigma (PiFlux.cpp:1037-1048)
+ * of the lambda's captured current_state, which Boost.Odeint's
+ * controlled_runge_kutta::try_step holds at the step's start state while it
+ * evaluates the stages (the new state is copied in only on acceptance): X. */
+static void piflux_relax_rhs(const orc_model *m, const kctx *k, double A, const double *S,
+                             const double *X, double *dS) {
+    const double pf = 4 * m->hopping;
+    double cx = k->cx, cy = k->cy, cz = cos(k->kz - A); /* shifted_k.update_z(k.z - A) */
+    const double mv[3] = {k->cx, k->cy, cos(k->kz - A)};
+    if (ref_is_zero(cx) && ref_is_zero(cy) && cz < 0.0) {
+        cx = fabs(cz) * 1e-4; /* RESCUE_TRAFO (PiFlux.cpp:51, 136-139) */
+        cz *= (1. - 0.5 * 1e-4 * 1e-4);
+    }
+    const double disp = sqrt(cx * cx + cy * cy + cz * cz);
+    const double a2 = fermi(-m->fermi_energy + 2 * m->hopping * disp, m->beta);
+    const double b2 = fermi(-m->fermi_energy - 2 * m->hopping * disp, m->beta);
+    const double diff = a2 - b2;
+    /* diagonal_sigma(current_state, shifted_k), components x and y */
+    const double z = cz + disp;
+    const double nrm = 2 * disp * z;
+    const double xz = 2 * cx * z, yz = 2 * cy * z, xy = 2 * cx * cy;
+    const double sg0 = (X[0] * (z * z - cx * cx + cy * cy) - xy * X[1] - xz * X[2]) / nrm;
+    const double sg1 = (X[1] * (z * z + cx * cx - cy * cy) - xy * X[0] - yz * X[2]) / nrm;
+    const double xyl = sqrt(sg0 * sg0 + sg1 * sg1);
+    const double prod = 2 * sqrt(a2 * b2) * (ref_is_zero(xyl) ? 1.0 : sg0 / xyl);
+    const double imag = 2 * sqrt(a2 * b2) * (ref_is_zero(xyl) ? 0.0 : sg1 / xyl);
+    const double zeps = cz + disp;
+    const double norm = disp * zeps;
+    const double fd = diff * zeps / norm;
+    const double rd[3] = {cx * fd, cy * fd, cz * fd};
+    double ro[3];
+    ro[0] = prod * (cy * cy + cz * zeps);
+    ro[1] = prod * (-cx * cy);
+    ro[2] = prod * (-cx * zeps);
+    ro[0] += imag * (-cx * cy);
+    ro[1] += imag * (cx * cx + cz * zeps);
+    ro[2] += imag * (-cy * zeps);
+    for (int i = 0; i < 3; ++i) ro[i] /= norm;
+    cross(mv, S, dS);
+    for (int i = 0; i < 3; ++i) {
+        dS[i] *= pf;
+        dS[i] -= m->inv_diag_relax * (S[i] / 3.0 - rd[i]) +
+                 m->inv_offdiag_relax * (S[i] * (2. / 3.) - ro[i]);
+    }
+}
+
+/* X: the step's start state (read by the PiFlux-3D relaxation form only). */
 static void model_rhs(const orc_model *m, const kctx *k, const orc_pulse *p, double t,
-                      const double *S, double *dS) {
+                      const double *S, const double *X, double *dS) {
     const double A = orc_laser(p, t);
+    const int relax = m->inv_diag_relax > 0.0;
     switch (m->kind) {
     case ORC_PIFLUX3D: {
+        if (relax) {
+            piflux_relax_rhs(m, k, A, S, X, dS);
+            break;
+        }
         /* PiFlux::time_evolution_sigma right_side (PiFlux.cpp:89-94) */
         const double pf = 4 * m->hopping;
         const double mv[3] = {k->cx, k->cy, cos(k->kz - A)};
@@ -217,6 +307,13 @@ static void model_rhs(const orc_model *m, const kctx *k, const orc_pulse *p, dou
             dS[0] -= 2.0 * m->mass * S[1];
             dS[1] += 2.0 * m->mass * S[0];
         }
+        if (relax) {
+            /* Honeycomb::time_evolution_diagonal_relaxation (Honeycomb.cpp:160-212):
+             * dxdt -= 1/tau (state - ic_sigma(k - A)) */
+            double eq[3];
+            honeycomb_ic(m, gre, gim, eq);
+            for (int i = 0; i < 3; ++i) dS[i] -= m->inv_diag_relax * (S[i] - eq[i]);
+        }
         break;
     }
     case ORC_DIRAC3D: {
@@ -224,6 +321,15 @@ static void model_rhs(const orc_model *m, const kctx *k, const orc_pulse *p, dou
          * kx = k_z, ky = kappa, kz = |k| */
         const double mx = A * 2.0 * k->ky / k->kz;
         const double mz = 2.0 * (k->kz - A * k->kx / k->kz);
+        if (relax) {
+            /* DiracSystem::time_evolution_diagonal_relaxation (DiracSystem.cpp:213-251):
+             * relaxation towards the initial state */
+            const double g = m->inv_diag_relax;
+            dS[0] = mz * S[1] - (S[0] - k->s0[0]) * g;
+            dS[1] = mx * S[2] - S[0] * mz - (S[1] - k->s0[1]) * g;
+            dS[2] = -mx * S[1] - (S[2] - k->s0[2]) * g;
+            break;
+        }
         dS[0] = mz * S[1];
         dS[1] = mx * S[2] - S[0] * mz;
         dS[2] = -mx * S[1];
@@ -271,16 +377,10 @@ double orc_vertex(const orc_model *m, const orc_pulse *p, const double *krow, do
 
 void orc_initial_state(const orc_model *m, double kx, double ky, double kz, double *s0) {
     switch (m->kind) {
-    case ORC_PIFLUX3D: {
-        /* ic_sigma at T = 0, E_F = 0 (PiFlux.cpp:519-549): -(cx, cy, cz)/|d| */
-        const double cx = cos(kx), cy = cos(ky), cz = cos(kz);
-        const double disp = sqrt(cx * cx + cy * cy + cz * cz);
-        const double zeps = cz + disp;
-        s0[0] = (-1.0 * cx * zeps + 0.0) / (disp * zeps);
-        s0[1] = (-1.0 * cy * zeps - 0.0) / (disp * zeps);
-        s0[2] = (-1.0 * cz * zeps - 0.0) / (disp * zeps);
+    case ORC_PIFLUX3D:
+        /* ic_sigma (PiFlux.cpp:519-549); T = 0, E_F = 0: -(cx, cy, cz)/|d| */
+        piflux_ic(m, cos(kx), cos(ky), cos(kz), s0);
         break;
-    }
     case ORC_PIFLUX2D: {
         const double cx = cos(kx), cy = cos(ky);
         const double n = sqrt(cx * cx + cy * cy);
@@ -306,10 +406,7 @@ void orc_initial_state(const orc_model *m, double kx, double ky, double kz, doub
             gim += sin(ph);
         }
         if (m->mass == 0.0) {
-            const double ag = hypot(gre, gim);
-            s0[0] = -1.0 * gre / ag;
-            s0[1] = 1.0 * gim / ag;
-            s0[2] = -0.0;
+            honeycomb_ic(m, gre, gim, s0);
         } else {
             const double d0 = m->hopping * gre, d1 = -m->hopping * gim, d2 = m->mass;
             const double n = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
@@ -319,12 +416,17 @@ void orc_initial_state(const orc_model *m, double kx, double ky, double kz, doub
         }
         break;
     }
-    case ORC_DIRAC3D:
-        /* (2 a0 b0, 0, a0^2 - b0^2) with a0 = 0, b0 = 1 (DiracSystem.cpp:155-158) */
-        s0[0] = 0.0;
+    case ORC_DIRAC3D: {
+        /* (2 a0 b0, 0, a0^2 - b0^2), a0 = f(E_F + |k|), b0 = f(E_F - |k|)
+         * (DiracSystem.cpp:155-158, dispersion :253-255); kx = k_z, ky = kappa */
+        const double disp = sqrt(ky * ky + kx * kx);
+        const double a0 = fermi(m->fermi_energy + disp, m->beta);
+        const double b0 = fermi(m->fermi_energy - disp, m->beta);
+        s0[0] = 2. * a0 * b0;
         s0[1] = 0.0;
-        s0[2] = -1.0;
+        s0[2] = a0 * a0 - b0 * b0;
         break;
+    }
     default:
         s0[0] = s0[1] = s0[2] = 0.0;
     }
@@ -440,11 +542,7 @@ int orc_grid_piflux3d_ref(const orc_model *m, int z_range, int n_coarse, double 
                                 o[3] = mw * yw[j] * zw[z];
                                 /* ic_sigma with the (possibly rescued) cos_z */
                                 const double cx = cos(kx), cy = cos(ky);
-                                const double disp = sqrt(cx * cx + cy * cy + cz * cz);
-                                const double zeps = cz + disp;
-                                o[4] = (-1.0 * cx * zeps + 0.0) / (disp * zeps);
-                                o[5] = (-1.0 * cy * zeps - 0.0) / (disp * zeps);
-                                o[6] = (-1.0 * cz * zeps - 0.0) / (disp * zeps);
+                                piflux_ic(m, cx, cy, cz, o + 4);
                                 o[7] = 0.0;
                                 last_cx = cx;
                                 last_cy = cy;
@@ -455,7 +553,6 @@ int orc_grid_piflux3d_ref(const orc_model *m, int z_range, int n_coarse, double 
         }
     }
     free(za), free(zw);
-    (void)m;
     return (int)row;
 }
 
@@ -510,7 +607,7 @@ static int rkf78_try(const rhs_ctx *c, double *x, double *t, double *dt, double 
                      double rel_tol, double *err_out) {
     double K[13][3];
     double xt[3];
-    model_rhs(c->m, c->k, c->p, *t, x, K[0]);
+    model_rhs(c->m, c->k, c->p, *t, x, x, K[0]);
     const double h = *dt;
     for (int s = 1; s < 13; ++s) {
         for (int i = 0; i < 3; ++i) {
@@ -519,7 +616,7 @@ static int rkf78_try(const rhs_ctx *c, double *x, double *t, double *dt, double 
                 if (RK_A[s][j] != 0.0) acc += (RK_A[s][j] * h) * K[j][i];
             xt[i] = acc;
         }
-        model_rhs(c->m, c->k, c->p, *t + RK_C[s] * h, xt, K[s]);
+        model_rhs(c->m, c->k, c->p, *t + RK_C[s] * h, xt, x, K[s]);
     }
     double xn[3], err = 0.0;
     for (int i = 0; i < 3; ++i) {
@@ -677,6 +774,9 @@ static void make_kctx(const double *krow, kctx *k) {
     k->kz = krow[2];
     k->cx = cos(krow[0]);
     k->cy = cos(krow[1]);
+    k->s0[0] = krow[4];
+    k->s0[1] = krow[5];
+    k->s0[2] = krow[6];
 }
 
 typedef void (*sample_fn)(void *user, int i, const double *S);

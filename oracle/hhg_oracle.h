@@ -43,6 +43,16 @@ typedef struct {
     double velocity;     /* v in hbar*omega_L per unit k (Dirac2D) */
     double mass;         /* staggered mass / gap term (Dirac2D, Honeycomb) */
     double pol_x, pol_y; /* field polarisation unit vector (cos theta, sin theta) */
+    /* Thermal state and relaxation (PiFlux-3D, Honeycomb, Dirac-3D):
+     * beta = photon_energy / (k_B T) with 0 standing for T = 0 (the
+     * reference's beta = DBL_MAX sentinel, PiFlux.cpp:63), fermi_energy =
+     * E_F / photon_energy, inv_*_relax = 1e15 hbar / (tau photon_energy)
+     * (PiFlux.cpp:67-68); inv_diag_relax > 0 selects the relaxation
+     * right-hand side (PiFlux.cpp:509-516, Honeycomb.cpp:214-223). */
+    double beta;
+    double fermi_energy;
+    double inv_diag_relax;
+    double inv_offdiag_relax;
 } orc_model;
 
 typedef struct {
@@ -86,7 +96,9 @@ int orc_grid_rhombic(const orc_model *m, int n1, int n2, double *out);
 int orc_grid_piflux3d_ref(const orc_model *m, int z_range, int n_coarse, double *out);
 int orc_grid_honeycomb_hex_ref(const orc_model *m, int n_k, double *out);
 
-/* Initial Bloch vector of the filled lower band at T = 0 (S0 = -d_hat). */
+/* Initial Bloch vector: the reference's ic_sigma / Fermi-occupied state of
+ * the reference models (T = 0, E_F = 0: the filled lower band, S0 = -d_hat);
+ * the variant models take the filled lower band. */
 void orc_initial_state(const orc_model *m, double kx, double ky, double kz, double *s0);
 
 /* One k-point: Bloch vector at every sample (n_measurements+1 rows of 3). */

@@ -30,7 +30,9 @@ KROW = 8
 class OrcModel(ctypes.Structure):
     _fields_ = [("kind", ctypes.c_int), ("hopping", ctypes.c_double),
                 ("velocity", ctypes.c_double), ("mass", ctypes.c_double),
-                ("pol_x", ctypes.c_double), ("pol_y", ctypes.c_double)]
+                ("pol_x", ctypes.c_double), ("pol_y", ctypes.c_double),
+                ("beta", ctypes.c_double), ("fermi_energy", ctypes.c_double),
+                ("inv_diag_relax", ctypes.c_double), ("inv_offdiag_relax", ctypes.c_double)]
 
 
 class OrcPulse(ctypes.Structure):
@@ -104,8 +106,10 @@ class Pulse:
         return OrcPulse(self.amplitude, self.t_begin, self.t_end, 1.0 / self.n_cycles, self.phase)
 
 
-def model(kind: int, hopping=0.0, velocity=0.0, mass=0.0, pol=(1.0, 0.0)) -> OrcModel:
-    return OrcModel(kind, hopping, velocity, mass, pol[0], pol[1])
+def model(kind: int, hopping=0.0, velocity=0.0, mass=0.0, pol=(1.0, 0.0), *, beta=0.0,
+          fermi_energy=0.0, inv_diag_relax=0.0, inv_offdiag_relax=0.0) -> OrcModel:
+    return OrcModel(kind, hopping, velocity, mass, pol[0], pol[1], beta, fermi_energy,
+                    inv_diag_relax, inv_offdiag_relax)
 
 
 def solver(abs_tol=1e-12, rel_tol=1e-8, stepper=0, magnus_substeps=1) -> OrcSolver:
@@ -127,6 +131,15 @@ def laser(p: Pulse, t) -> np.ndarray:
     pc = p.c()
     return np.array([lib().orc_laser(ctypes.byref(pc), ctypes.c_double(float(v)))
                      for v in np.atleast_1d(t)])
+
+
+def initial_state(m: OrcModel, kx: float, ky: float, kz: float) -> np.ndarray:
+    """orc_initial_state: the model's initial Bloch vector at (kx, ky, kz)."""
+    L = lib()
+    out = np.zeros(3)
+    L.orc_initial_state(ctypes.byref(m), ctypes.c_double(kx), ctypes.c_double(ky),
+                        ctypes.c_double(kz), _p(out))
+    return out
 
 
 def grid_tensor(m: OrcModel, nx, ny, x_lo, x_hi, y_lo, y_hi) -> np.ndarray:

@@ -14,7 +14,9 @@ SYS_TO_ORC = {0: O.DIRAC2D, 1: O.PIFLUX2D, 2: O.PIFLUX3D, 3: O.HONEYCOMB, 4: O.D
 def oracle_args(sys, pulse, abs_tol, rel_tol, stepper=0, magnus_substeps=1):
     es = pulse.energy_scale
     m = O.model(SYS_TO_ORC[sys.kind], hopping=sys.hopping * es, velocity=sys.velocity * es,
-                mass=sys.mass * es, pol=(sys.pol_x, sys.pol_y))
+                mass=sys.mass * es, pol=(sys.pol_x, sys.pol_y), beta=sys.beta / es,
+                fermi_energy=sys.fermi_energy * es, inv_diag_relax=sys.inv_diag_relax * es,
+                inv_offdiag_relax=sys.inv_offdiag_relax * es)
     p = O.Pulse(pulse.amplitude, pulse.n_cycles, pulse.t_begin, pulse.phase)
     tc = O.time_config(pulse.window_begin, pulse.window_end, pulse.n_measurements,
                        pulse.n_subdivisions)
