@@ -35,18 +35,18 @@ UNIT = "spectra/s"
 # sides plus the tableau arithmetic 2*3*55 (stages) + 2*3*7 (solution) +
 # 2*3*4 (error) + ~25 (norm and control) = 421; the right-hand side of the
 # 2D pi-flux model costs 12 flops plus two cosines (counted separately).
-# The PiFlux relaxation right-hand side (PiFlux.cpp:113-186 as the kernel
-# writes it) costs 103 flops: cos(kz - A) 3, |u| 5, the two occupation
-# energies and Fermi denominators 8, (a2 - b2)/|u| 1, coherent part with the
-# -g_s S + g_d r_d terms 27, 2 sqrt(a2 b2) 2, z_eps and the normalisation 2,
-# the squared cosines 5, the diagonal_sigma numerators 18, their norm 3, the
-# is_zero test 3, prod/imag 3, the off-diagonal terms 23; plus 8 special
-# operations (2 exp, 3 divisions, 2 sqrt, 1 rsqrt).
+# The PiFlux relaxation right-hand side (PiFlux.cpp:113-186 in the kernel's
+# form: off-diagonal equilibrium as the normalised perpendicular part of the
+# start state, Fermi pair through one reciprocal square root) costs 76 flops:
+# cos(kz - A) 3, |u|^2 5, |u| 1, occupation energies 4, Fermi pair 11,
+# g_d (a2 - b2)/|u| 2, coherent part with -g_s S + g_d r_d 24, perpendicular
+# projection, its norm and the g_o term 26; plus 5 special operations (2 exp,
+# 3 rsqrt).
 ALG_FLOPS_PER_KSTEP = {"piflux2d_256": 13 * 12 + 421, "dirac2d_64": 13 * 16 + 421,
                        "honeycomb_512": 13 * 30 + 421, "dirac2d_sweep": 13 * 16 + 421,
-                       "piflux3d_relax": 13 * 103 + 421}
+                       "piflux3d_relax": 13 * 76 + 421}
 SPECIAL_OPS_PER_KSTEP = {"piflux2d_256": 26, "dirac2d_64": 0, "honeycomb_512": 78,
-                         "dirac2d_sweep": 0, "piflux3d_relax": 13 * 8}
+                         "dirac2d_sweep": 0, "piflux3d_relax": 13 * 5}
 # the relaxation workload runs the reference step schedule in FP64 only
 DEFAULT_VARIANT = {"piflux3d_relax": "fp64"}
 # The mixed-precision variant splits that work: solution, error estimate, error
@@ -227,17 +227,17 @@ def config_for(wl, variant_desc, okw=None):
 
 def traffic_from_profile(wl_name):
     """Per-launch DRAM bytes of the integration kernel from the committed ncu
-    summary (a line 'traffic_bytes_per_launch[<workload>]: <bytes>')."""
-    path = os.path.join(ROOT, "profiles", "bz_integrate_kernel.md")
-    if not os.path.exists(path):
-        return None
+    summaries (a line 'traffic_bytes_per_launch[<workload>]: <bytes>' in one
+    of profiles/bz_integrate_kernel*.md)."""
+    import glob
     key = f"traffic_bytes_per_launch[{wl_name}]:"
-    for line in open(path):
-        if line.strip().startswith(key):
-            try:
-                return float(line.split(":", 1)[1].split()[0])
-            except ValueError:
-                return None
+    for path in sorted(glob.glob(os.path.join(ROOT, "profiles", "bz_integrate_kernel*.md"))):
+        for line in open(path):
+            if line.strip().startswith(key):
+                try:
+                    return float(line.split(":", 1)[1].split()[0])
+                except ValueError:
+                    return None
     return None
 
 

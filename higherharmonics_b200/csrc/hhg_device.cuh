@@ -88,19 +88,21 @@ template <> struct Traits<PIFLUX3D_RELAX> {
     static constexpr int NF = 2;
     static constexpr bool kRelax = true;
     static constexpr bool kStart = true;
-    static constexpr int kMinBlocks = 4;  // the equilibrium terms need ~200 registers
+    // 255 registers, 8 warps per SM: at 168 registers (12 warps) the stage
+    // values spill and the kernel runs 1.7x slower (measured)
+    static constexpr int kMinBlocks = 4;
 };
 template <> struct Traits<HONEYCOMB_RELAX> {
     static constexpr int NF = 6;
     static constexpr bool kRelax = true;
     static constexpr bool kStart = false;
-    static constexpr int kMinBlocks = 4;  // the equilibrium terms need ~200 registers
+    static constexpr int kMinBlocks = 4;  // 255 registers: the six staged functions spill at 168
 };
 template <> struct Traits<DIRAC3D_RELAX> {
     static constexpr int NF = 1;
     static constexpr bool kRelax = true;
     static constexpr bool kStart = false;
-    static constexpr int kMinBlocks = 4;  // the equilibrium terms need ~200 registers
+    static constexpr int kMinBlocks = kMinBlocksPerSM;
 };
 
 // Per-interval record (doubles):
@@ -501,15 +503,39 @@ __device__ __forceinline__ double fermi_occ(double e, double beta) {
 __device__ __forceinline__ bool ref_is_zero_dev(double v) {
     return (int)(((unsigned long long)__double_as_longlong(v) >> 52) & 0x7FF) < 0x3D3;
 }
+// The two occupations a = f(e_a), b = f(e_b) enter the relaxation terms only
+// as a - b and 2 sqrt(a b): with x = exp(beta e), a - b = (x_b - x_a) / den and
+// sqrt(a b) = den^-1/2, den = (1 + x_a)(1 + x_b), so one reciprocal square
+// root serves both.  Exponents are clamped at 300 (f < 1e-130 there) so den
+// stays finite.  Not inlined: the two exp bodies would otherwise be copied
+// into each of the 13 stages of both step paths, and the kernel outgrows the
+// instruction cache (measured: fetch stalls dominate).
+struct FermiPair {
+    double diff, sq;
+};
+static __device__ __noinline__ FermiPair fermi_pair(double ea, double eb, double beta) {
+    if (beta == 0.0) {
+        const double a = fermi_occ(ea, 0.0), b = fermi_occ(eb, 0.0);
+        return {a - b, 2.0 * sqrt(a * b)};
+    }
+    const double xa = exp(fmin(beta * ea, 300.0));
+    const double xb = exp(fmin(beta * eb, 300.0));
+    const double r = rsqrt((1.0 + xa) * (1.0 + xb));
+    return {(xb - xa) * (r * r), 2.0 * r};
+}
 
 // PiFlux with relaxation (PiFlux.cpp:113-186):
 //   dS/dt = 4t (cx, cy, cos(kz - A)) x S - [g_d (S/3 - r_d) + g_o (2S/3 - r_o)]
 // with u = k - A (cos components, RESCUE_TRAFO when cos kx, cos ky vanish and
-// cos(kz - A) < 0), |u|, occupations a2 = f(-E_F + 2t|u|), b2 = f(-E_F - 2t|u|),
-// r_d = (a2 - b2) u / |u| and r_o = 2 sqrt(a2 b2) times the unit in-plane
-// direction of diagonal_sigma(X, u) (PiFlux.cpp:1037-1048) mapped back,
-// where X is the step's start state (the lambda's captured current_state,
-// which Boost.Odeint's try_step updates only on acceptance).
+// cos(kz - A) < 0), occupations a2 = f(-E_F + 2t|u|), b2 = f(-E_F - 2t|u|),
+// r_d = (a2 - b2) u / |u|.  r_o is the reference's off-diagonal equilibrium:
+// diagonal_sigma (PiFlux.cpp:1037-1048) rotates the start state X into the
+// band frame (e1, e2, u/|u|), the in-plane part is normalised, scaled by
+// 2 sqrt(a2 b2) and rotated back (PiFlux.cpp:145-170).  The rotation is
+// orthogonal, so r_o = 2 sqrt(a2 b2) X_perp / |X_perp| with X_perp = X -
+// (X.u) u / |u|^2; only when |X_perp| is zero (is_zero) does the reference's
+// e1 appear.  X is the step's start state (the lambda's captured
+// current_state, which Boost.Odeint's try_step updates only on acceptance).
 // mp: [0] 4t, [1] 2t, [4] E_F, [5] beta, [6] g_d, [7] g_o.
 template <typename R> struct ModelState<PIFLUX3D_RELAX, R> {
     static_assert(sizeof(R) == sizeof(double), "relaxation models run in FP64");
@@ -536,37 +562,33 @@ template <typename R> struct ModelState<PIFLUX3D_RELAX, R> {
             ux = fabs(uz) * 1e-4;
             uz *= (1. - 0.5 * 1e-4 * 1e-4);
         }
-        const double disp = sqrt(ux * ux + cy * cy + uz * uz);
-        const double a2 = fermi_occ(-ef + e2t * disp, beta);
-        const double b2 = fermi_occ(-ef - e2t * disp, beta);
-        const double fd = (a2 - b2) / disp;
-        // coherent part and the -g_s S + g_d r_d terms
-        dS[0] = pf * (cy * S[2] - czA * S[1]) - gs * S[0] + gd * (ux * fd);
-        dS[1] = pf * (czA * S[0] - cx * S[2]) - gs * S[1] + gd * (cy * fd);
-        dS[2] = pf * (cx * S[1] - cy * S[0]) - gs * S[2] + gd * (uz * fd);
-        const double sq = 2.0 * sqrt(a2 * b2);
+        const double d2 = ux * ux + cy * cy + uz * uz;
+        const double rd = rsqrt(d2);  // 1 / |u|
+        const double disp = d2 * rd;
+        const FermiPair fp = fermi_pair(e2t * disp - ef, -e2t * disp - ef, beta);
+        const double sq = fp.sq;
+        const double fd = gd * (fp.diff * rd);
+        // coherent part, -g_s S and g_d r_d
+        dS[0] = pf * (cy * S[2] - czA * S[1]) - gs * S[0] + ux * fd;
+        dS[1] = pf * (czA * S[0] - cx * S[2]) - gs * S[1] + cy * fd;
+        dS[2] = pf * (cx * S[1] - cy * S[0]) - gs * S[2] + uz * fd;
         if (sq != 0.0) {
-            const double zeps = uz + disp;
-            const double inv_norm = 1.0 / (disp * zeps);
-            // diagonal_sigma numerators (x, y) of the start state
-            const double z2 = zeps * zeps, xx = ux * ux, yy = cy * cy, xy = 2.0 * ux * cy;
-            const double n0 = X[0] * (z2 - xx + yy) - xy * X[1] - (2.0 * ux * zeps) * X[2];
-            const double n1 = X[1] * (z2 + xx - yy) - xy * X[0] - (2.0 * cy * zeps) * X[2];
-            const double n2 = n0 * n0 + n1 * n1;
-            double prod, imag;
-            // is_zero(|diagonal_sigma_xy|), |.| = sqrt(n2) / (2 disp zeps)
-            if (n2 * (0.25 * inv_norm * inv_norm) < 0x1p-88) {
-                prod = sq;
-                imag = 0.0;
+            const double c = (X[0] * ux + X[1] * cy + X[2] * uz) * (rd * rd);
+            const double p0 = X[0] - c * ux, p1 = X[1] - c * cy, p2 = X[2] - c * uz;
+            const double n2 = p0 * p0 + p1 * p1 + p2 * p2;
+            if (n2 >= 0x1p-88) {
+                const double w = go * sq * rsqrt(n2);
+                dS[0] += w * p0;
+                dS[1] += w * p1;
+                dS[2] += w * p2;
             } else {
-                const double r = sq * rsqrt(n2);
-                prod = n0 * r;
-                imag = n1 * r;
+                // is_zero(|X_perp|): prod = 2 sqrt(a2 b2), imag = 0, r_o = sq e1
+                const double zeps = uz + disp;
+                const double w = go * sq / (disp * zeps);
+                dS[0] += w * (cy * cy + uz * zeps);
+                dS[1] -= w * (ux * cy);
+                dS[2] -= w * (ux * zeps);
             }
-            const double go_n = go * inv_norm;
-            dS[0] += go_n * (prod * (yy + uz * zeps) - imag * (ux * cy));
-            dS[1] += go_n * (imag * (xx + uz * zeps) - prod * (ux * cy));
-            dS[2] -= go_n * ((prod * ux + imag * cy) * zeps);
         }
     }
     __device__ __forceinline__ double vertex(const double *r, const double *S) const {
@@ -590,15 +612,15 @@ template <typename R> struct ModelState<HONEYCOMB_RELAX, R> : HoneycombState<dou
     __device__ __forceinline__ void rhs(const double *f, const double *S, double *dS) const {
         double gr, gi;  // 2t Re gamma', 2t Im gamma'
         gamma(f, gr, gi);
-        const double G = sqrt(gr * gr + gi * gi);
-        const double tg = 0.5 * G;  // t |gamma'|
-        const double a2 = fermi_occ(ef - tg, beta);
-        const double b2 = fermi_occ(ef + tg, beta);
-        const double dg = (a2 - b2) / G;
-        const double eq2 = -2.0 * sqrt(a2 * b2);
+        const double G2 = gr * gr + gi * gi;
+        const double rG = rsqrt(G2);
+        const double tg = 0.5 * (G2 * rG);  // t |gamma'|
+        const FermiPair fp = fermi_pair(ef - tg, ef + tg, beta);
+        const double sq = fp.sq;
+        const double dg = fp.diff * rG;
         dS[0] = -(S[2] * gi) - g * (S[0] + dg * gr);
         dS[1] = -(S[2] * gr) - g * (S[1] - dg * gi);
-        dS[2] = (S[0] * gi + S[1] * gr) - g * (S[2] - eq2);
+        dS[2] = (S[0] * gi + S[1] * gr) - g * (S[2] + sq);
     }
 };
 
@@ -1011,7 +1033,11 @@ __global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integ
                         // every lane records every hist_every-th interval, staggered
                         const bool rec_lane =
                             kRecord && ((i - 1 + lane + (int)(item & 1023)) % P.hist_every) == 0;
-                        lane_controller<M, NF, D, R, PROPOSER == 0, kCarry, kRecord>(
+                        // the relaxation models' steps follow their dynamics, not the
+                        // standard schedule; without the table path their attempt code is
+                        // half the size (5 % faster, measured)
+                        lane_controller<M, NF, D, R, PROPOSER == 0 && !Traits<M>::kRelax, kCarry,
+                                        kRecord>(
                             P, ms, poly, slot, tabv, n_std, t0, kCarry ? carry_dt : dt0,
                             t1, S, dead, carry_dt, my_attempts, my_rejects, row, &pd, rec_lane);
                     } else {
