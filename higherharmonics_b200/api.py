@@ -22,7 +22,7 @@ STATUS_NAMES = {0: "HHG_OK", 1: "HHG_BAD_CONFIG", 2: "HHG_STEP_LIMIT", 3: "HHG_N
                 4: "HHG_CUDA_ERROR", 5: "HHG_UNSUPPORTED"}
 SYS_DIRAC2D, SYS_PIFLUX2D, SYS_PIFLUX3D, SYS_HONEYCOMB, SYS_DIRAC3D = range(5)
 GRID_TENSOR_GL, GRID_RHOMBIC_GL, GRID_PIFLUX3D_REF, GRID_HONEYCOMB_HEX_REF, GRID_EXPLICIT = range(5)
-STEPPER_RKF78, STEPPER_MAGNUS4 = 0, 1
+STEPPER_RKF78, STEPPER_MAGNUS4, STEPPER_DIRAC_MAGNUS = 0, 1, 2
 PREC_FP64, PREC_MIXED = 0, 1
 PROPOSER_NONE, PROPOSER_CARRY, PROPOSER_LEARNED, PROPOSER_LOCKSTEP = 0, 1, 2, 3
 PULSE_COSINE = 0

@@ -764,6 +764,93 @@ __device__ __forceinline__ void rotate(const double *w, double *S) {
     S[2] += sa * wx2 + ca * ww2;
 }
 
+// The reference's Dirac-3D Magnus step (DiracSystem.cpp:190-210): with the
+// interval's Legendre moments m_q of A (Laser.cpp:40-55, staged per interval)
+// divided by |k|, Omega is the fourth-order Magnus series of
+// MagnusMatrix.cpp:25-57 for M(t) = H + A(t) A_k with H <-> h = (0, 0, 2|k| dt)
+// and A_k <-> (2 kappa dt, 0, -2 k_z dt).  For 3x3 skew matrices the
+// commutator is the cross product of the axial vectors, so each nested
+// commutator is a nested cross product; (a, b, c) of the reference's Omega
+// are (-w_2, w_1, -w_0), and U = exp(Omega) in the reference's closed form
+// (MagnusMatrix.cpp:59-75).
+__device__ __forceinline__ void cross3(const double *a, const double *b, double *o) {
+    o[0] = a[1] * b[2] - a[2] * b[1];
+    o[1] = a[2] * b[0] - a[0] * b[2];
+    o[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+__device__ __forceinline__ void dirac_magnus_step(double k_z, double kappa, double mk, double dt,
+                                                  const double *mom, double *S) {
+    const double inv = 1.0 / mk;
+    const double cf0 = mom[0] * inv, cf1 = mom[1] * inv, cf2 = mom[2] * inv, cf3 = mom[3] * inv;
+    const double ks = 2.0 * mk * dt, kap = 2.0 * kappa * dt, kzs = 2.0 * k_z * dt;
+    const double av[3] = {kap, 0.0, -kzs};
+    double m1[3], m2[3], m3[3], m4[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        m1[i] = (i == 2 ? ks : 0.0) + cf0 * av[i];
+        m2[i] = cf1 * av[i];
+        m3[i] = cf2 * av[i];
+        m4[i] = cf3 * av[i];
+    }
+    double c12[3], c13[3], c14[3], c112[3], c113[3], t1[3], t2[3], t3[3], w[3];
+    cross3(m1, m2, c12);
+    cross3(m1, m3, c13);
+    cross3(m1, m4, c14);
+    cross3(m1, c12, c112);
+    cross3(m1, c13, c113);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) w[i] = m1[i] - c12[i] / 6.0;
+#define HHG_W(coef, v)                                  \
+    _Pragma("unroll") for (int i = 0; i < 3; ++i) w[i] += (coef) * (v)[i];
+    cross3(m2, c12, t1);
+    HHG_W(-1.0 / 60.0, t1)
+    cross3(m1, c112, t1);
+    HHG_W(1.0 / 360.0, t1)
+    cross3(m2, c14, t1);
+    HHG_W(1.0 / 140.0, t1)
+    cross3(m3, c13, t1);
+    HHG_W(-1.0 / 420.0, t1)
+    cross3(m4, c12, t1);
+    HHG_W(-1.0 / 210.0, t1)
+    cross3(m1, c14, t2);
+    cross3(m1, t2, t1);
+    HHG_W(-1.0 / 840.0, t1)
+    cross3(m2, c113, t1);
+    HHG_W(1.0 / 504.0, t1)
+    cross3(m2, c12, t2);
+    cross3(m2, t2, t1);
+    HHG_W(-1.0 / 840.0, t1)
+    cross3(m3, c112, t1);
+    HHG_W(1.0 / 2520.0, t1)
+    cross3(m1, c113, t2);
+    cross3(m1, t2, t1);
+    HHG_W(-1.0 / 2520.0, t1)
+    cross3(c12, c112, t1);
+    HHG_W(-1.0 / 7560.0, t1)
+    cross3(m1, c112, t2);
+    cross3(m2, t2, t1);
+    HHG_W(1.0 / 2520.0, t1)
+    cross3(m1, c112, t3);
+    cross3(m1, t3, t2);
+    cross3(m1, t2, t1);
+    HHG_W(-1.0 / 15120.0, t1)
+#undef HHG_W
+    const double a = -w[2], b = w[1], c = -w[0];
+    const double n2 = a * a + b * b + c * c;
+    const double ev = sqrt(n2);
+    double y, x;
+    sincos(ev, &y, &x);
+    const double in2 = 1.0 / n2;
+    const double s0 = S[0], s1 = S[1], s2 = S[2];
+    S[0] = (((a * a + b * b) * x + c * c) * s0 + (b * c * (x - 1) + a * ev * y) * s1 +
+            (-a * c * (x - 1) + b * ev * y) * s2) * in2;
+    S[1] = ((b * c * (x - 1) - a * ev * y) * s0 + ((a * a + c * c) * x + b * b) * s1 +
+            (a * b * (x - 1) + c * ev * y) * s2) * in2;
+    S[2] = ((-a * c * (x - 1) - b * ev * y) * s0 + (a * b * (x - 1) - c * ev * y) * s1 +
+            ((b * b + c * c) * x + a * a) * s2) * in2;
+}
+
 // Step-size control after an attempt (controlled_runge_kutta with the
 // default error checker and step adjuster).  Returns true if accepted and
 // updates dt.  err < 5^-8 takes the host-computed growth constant;
@@ -1028,6 +1115,13 @@ __global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integ
                             }
                             my_attempts += ns;
                         }
+                    } else if constexpr (STEPPER == 2) {
+                        // the interval's Legendre moments sit where the standard
+                        // schedule's table would (staging layout 3)
+                        if (!dead) {
+                            dirac_magnus_step(row[0], row[1], row[2], pd.measure_every, slot + TAB, S);
+                            ++my_attempts;
+                        }
                     } else if constexpr (!kDyadic) {
                         const int n_std = (PROPOSER == 0) ? (int)slot[SCHED] : 0;
                         // every lane records every hist_every-th interval, staggered
@@ -1153,14 +1247,18 @@ __global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integ
 // or (LAYOUT 1 / 2) the exact stage values of the dyadic steps, as doubles or
 // as float pairs.
 // ---------------------------------------------------------------------------
+// LAYOUT 3: layout 0's header and interpolants plus, at the table offset,
+// the interval's first four Legendre moments of A for the Dirac Magnus step
+// (Laser::magnus_coefficients, Laser.cpp:40-55), from gl30 = the reference's
+// 30-point rule on [0, 1] (nodes, then weights, gauss.hpp:14-80).
 template <int M, int D, int LAYOUT>
 __global__ void stage_pulses_kernel(const PulseDev *__restrict__ pulses, int n_pulses,
                                     const double *__restrict__ tgrid,
                                     const long long *__restrict__ interval_off,
                                     double *__restrict__ coef, long long total_intervals,
-                                    double grow_max) {
+                                    double grow_max, const double *__restrict__ gl30) {
     constexpr int NF = Traits<M>::NF;
-    constexpr int SLOT = LAYOUT == 0 ? slot_doubles(NF, D) : slot_doubles_dyadic(NF, D);
+    constexpr int SLOT = (LAYOUT == 0 || LAYOUT == 3) ? slot_doubles(NF, D) : slot_doubles_dyadic(NF, D);
     constexpr int HDR = slot_header(NF);
     constexpr int SCHED = slot_sched(NF, D);
     constexpr int TAB = slot_table(NF, D);
@@ -1224,6 +1322,30 @@ __global__ void stage_pulses_kernel(const PulseDev *__restrict__ pulses, int n_p
             }
         }
         for (int j = 0; j < NN; ++j) out[HDR + n * NN + j] = m[j];
+    }
+    if constexpr (LAYOUT == 3) {
+        // moments over [t0, t0 + measure_every] of the raw pulse (the envelope
+        // times the carrier), scaled by (2q + 1) A0 as Laser.cpp:50-54
+        double c0 = 0.0, c1 = 0.0, c2 = 0.0, c3 = 0.0;
+        for (int q = 0; q < 30; ++q) {
+            const double a = gl30[q], wq = gl30[30 + q];
+            const double l2 = 2. * a - 1.;
+            const double l3 = 6. * a * (a - 1.) + 1.;
+            const double l4 = 20. * a * a * a - 30. * a * a + 12. * a + 1.;  // as gauss.hpp:96-99
+            const double t = t0 + pd.measure_every * a;
+            double env = 0.0;
+            if (!(t <= pd.t_begin || t >= pd.t_end)) env = 0.5 * (1. - cos(pd.inv_n_cycles * (t - pd.t_begin)));
+            const double lv = env * sin(t + pd.phase);
+            c0 += wq * lv;
+            c1 += wq * l2 * lv;
+            c2 += wq * l3 * lv;
+            c3 += wq * l4 * lv;
+        }
+        out[TAB + 0] = c0 * pd.amplitude;
+        out[TAB + 1] = c1 * (3. * pd.amplitude);
+        out[TAB + 2] = c2 * (5. * pd.amplitude);
+        out[TAB + 3] = c3 * (7. * pd.amplitude);
+        return;
     }
     if constexpr (LAYOUT != 0) {
         // dyadic steps: position q of level L starts at t0 + q (t1 - t0) 2^-L

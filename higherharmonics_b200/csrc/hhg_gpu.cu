@@ -736,8 +736,15 @@ hhg_status hhg_plan_create(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_p
     hhg_solver_opts o;
     hhg_default_solver_opts(&o);
     if (opts) o = *opts;
-    if (o.stepper != HHG_STEPPER_RKF78 && o.stepper != HHG_STEPPER_MAGNUS4)
+    if (o.stepper != HHG_STEPPER_RKF78 && o.stepper != HHG_STEPPER_MAGNUS4 &&
+        o.stepper != HHG_STEPPER_DIRAC_MAGNUS)
         return set_err(ctx, HHG_BAD_CONFIG, "unknown stepper");
+    if (o.stepper == HHG_STEPPER_DIRAC_MAGNUS &&
+        (sys->kind != HHG_SYS_DIRAC3D || o.precision != HHG_PREC_FP64 ||
+         o.proposer != HHG_PROPOSER_NONE))
+        return set_err(ctx, HHG_UNSUPPORTED,
+                       "the closed-form Magnus step is the Dirac-3D model's, in FP64, one step per "
+                       "interval (no step proposer)");
     if (o.stepper == HHG_STEPPER_MAGNUS4 && (o.magnus_substeps < 1 || o.magnus_substeps > 4096))
         return set_err(ctx, HHG_BAD_CONFIG, "magnus_substeps out of range");
     if (o.stepper == HHG_STEPPER_MAGNUS4 && o.precision != HHG_PREC_FP64)
@@ -901,6 +908,24 @@ hhg_status hhg_plan_create(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_p
         j_len += q.n_measurements + 1;
         ioff[p + 1] = ioff[p] + q.n_measurements;
     }
+    // the Dirac Magnus staging reads the reference's 30-point rule on [0, 1]
+    // (gauss.hpp:14-80: negative nodes by increasing |x|, then positive ones),
+    // stored after the staging slots
+    const bool magnus_moments = o.stepper == HHG_STEPPER_DIRAC_MAGNUS;
+    std::vector<double> gl30;
+    if (magnus_moments) {
+        double x[30], w[30];
+        gauss_legendre(30, x, w);
+        gl30.assign(60, 0.0);
+        for (int i = 0; i < 15; ++i) {
+            gl30[i] = 0.5 * (-x[15 + i] + 1.);
+            gl30[15 + i] = 0.5 * (x[15 + i] + 1.);
+            gl30[30 + i] = 0.5 * w[15 + i];
+            gl30[45 + i] = 0.5 * w[15 + i];
+        }
+    }
+    const long long gl_off = coef_len;
+    if (magnus_moments) coef_len += 60;
     pl->coef_len = coef_len;
     pl->part_len = part_len;
     pl->j_len = j_len;
@@ -947,9 +972,13 @@ hhg_status hhg_plan_create(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_p
     if ((e = cudaMemcpyAsync(pl->d_pulses, pl->pulses.data(), n_pulses * sizeof(PulseDev), cudaMemcpyHostToDevice, s)) != cudaSuccess) return fail("upload pulses", e);
     if ((e = cudaMemcpyAsync(pl->d_tgrid, tgrid.data(), tgrid.size() * sizeof(double), cudaMemcpyHostToDevice, s)) != cudaSuccess) return fail("upload tgrid", e);
     if ((e = cudaMemcpyAsync(pl->d_ioff, ioff.data(), ioff.size() * sizeof(long long), cudaMemcpyHostToDevice, s)) != cudaSuccess) return fail("upload offsets", e);
+    if (magnus_moments &&
+        (e = cudaMemcpyAsync(pl->d_coef + gl_off, gl30.data(), 60 * sizeof(double), cudaMemcpyHostToDevice, s)) != cudaSuccess)
+        return fail("upload quadrature", e);
     hhg::StageReq sr{pl->d_pulses, n_pulses, pl->d_tgrid, pl->d_ioff, pl->d_coef,
                      pl->n_intervals, degree, 9.0 / 10.0 * pow(pow(5.0, -8.0), -1.0 / 8), s};
-    sr.layout = dyadic ? (o.precision == HHG_PREC_MIXED ? 2 : 1) : 0;
+    sr.layout = dyadic ? (o.precision == HHG_PREC_MIXED ? 2 : 1) : (magnus_moments ? 3 : 0);
+    if (magnus_moments) sr.gl30 = pl->d_coef + gl_off;
     if ((st = stage_variant(pl, sr)) != HHG_OK) {
         hhg_plan_destroy(pl);
         return st;

@@ -29,7 +29,8 @@ struct StageReq {
     int degree;
     double grow_max;
     cudaStream_t stream;
-    int layout = 0;  // 0 standard schedule, 1 dyadic FP64, 2 dyadic float pairs
+    int layout = 0;  // 0 standard schedule, 1 dyadic FP64, 2 dyadic float pairs, 3 Dirac Magnus moments
+    const double *gl30 = nullptr;  // layout 3: 30 nodes on [0, 1], then 30 weights (device)
 };
 
 template <int M, int D, typename R, int ST, int PR>
@@ -59,6 +60,11 @@ cudaError_t launch_deg(const LaunchReq &r) {
         }
         return cudaErrorInvalidValue;
     } else {
+        if (r.stepper == 2) {
+            // the reference's closed-form Dirac Magnus step
+            if constexpr (M == DIRAC3D) return launch_one<M, D, double, 2, 0>(r);
+            else return cudaErrorNotSupported;
+        }
         if (r.stepper == 1) return launch_one<M, D, double, 1, 0>(r);
         if (r.precision == 0) {
             switch (r.proposer) {
@@ -91,21 +97,24 @@ cudaError_t launch_model(const LaunchReq &r) {
 template <int M, int D, int LAYOUT>
 void stage_one(const StageReq &s, unsigned blocks, int threads) {
     stage_pulses_kernel<M, D, LAYOUT><<<blocks, threads, 0, s.stream>>>(
-        s.pulses, s.n_pulses, s.tgrid, s.interval_off, s.coef, s.total_intervals, s.grow_max);
+        s.pulses, s.n_pulses, s.tgrid, s.interval_off, s.coef, s.total_intervals, s.grow_max,
+        s.gl30);
 }
 
 template <int M, int D>
 void stage_deg(const StageReq &s, unsigned blocks, int threads) {
     if (s.layout == 0) stage_one<M, D, 0>(s, blocks, threads);
     else if (s.layout == 1) stage_one<M, D, 1>(s, blocks, threads);
-    else stage_one<M, D, 2>(s, blocks, threads);
+    else if (s.layout == 2) stage_one<M, D, 2>(s, blocks, threads);
+    else if constexpr (M == DIRAC3D) stage_one<M, D, 3>(s, blocks, threads);
 }
 
 template <int M>
 cudaError_t stage_model(const StageReq &s) {
     const int threads = 128;
     const long long blocks = (s.total_intervals + threads - 1) / threads;
-    if (s.layout < 0 || s.layout > 2) return cudaErrorInvalidValue;
+    if (s.layout < 0 || s.layout > 3 || (s.layout == 3 && (M != DIRAC3D || !s.gl30)))
+        return cudaErrorInvalidValue;
     if (s.degree == 5) stage_deg<M, 5>(s, (unsigned)blocks, threads);
     else if (s.degree == 7) stage_deg<M, 7>(s, (unsigned)blocks, threads);
     else if (s.degree == 11) stage_deg<M, 11>(s, (unsigned)blocks, threads);

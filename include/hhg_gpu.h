@@ -134,7 +134,19 @@ typedef struct hhg_grid_desc {
     int64_t n_rows;
 } hhg_grid_desc;
 
-typedef enum hhg_stepper { HHG_STEPPER_RKF78 = 0, HHG_STEPPER_MAGNUS4 = 1 } hhg_stepper;
+/* Steppers.  RKF78: the reference's controlled Fehlberg 7(8) (PiFlux.cpp:104-110).
+ * MAGNUS4: two-point Gauss 4th-order Magnus, magnus_substeps per interval
+ * (no reference counterpart).  DIRAC_MAGNUS: the reference's Dirac path,
+ * DiracSystem::time_evolution_magnus (DiracSystem.cpp:176-211) -- one
+ * closed-form step per interval, S <- exp(Omega) S, Omega from the first
+ * four Legendre moments of A over the interval (30-point Gauss,
+ * Laser.cpp:40-55) and the Magnus series of MagnusMatrix.cpp:25-76;
+ * HHG_SYS_DIRAC3D only. */
+typedef enum hhg_stepper {
+    HHG_STEPPER_RKF78 = 0,
+    HHG_STEPPER_MAGNUS4 = 1,
+    HHG_STEPPER_DIRAC_MAGNUS = 2
+} hhg_stepper;
 typedef enum hhg_precision { HHG_PREC_FP64 = 0, HHG_PREC_MIXED = 1 } hhg_precision;
 typedef enum hhg_proposer {
     HHG_PROPOSER_NONE = 0,    /* reference: every interval restarts at dt = measure_every / n_subdivisions */

@@ -793,11 +793,25 @@ static int evolve_generic(const orc_model *m, const orc_pulse *p, const orc_time
     double t_begin = tc->t_begin;
     double t_end = t_begin + measure_every;
     fn(user, 0, S);
+    if (s->stepper == 2 && m->kind != ORC_DIRAC3D) return ORC_BAD_CONFIG;
     for (int i = 1; i <= tc->n_measurements; ++i) {
         if (s->stepper == 1) {
             magnus4_interval(m, &k, p, t_begin, t_end, s->magnus_substeps, S);
             st->attempted += s->magnus_substeps;
             st->accepted += s->magnus_substeps;
+        } else if (s->stepper == 2) {
+            /* DiracSystem::time_evolution_magnus (DiracSystem.cpp:190-210) on the
+             * row's (k_z, kappa, |k|) and initial state */
+            double cf[4], U[9];
+            orc_magnus_coefficients(p, measure_every, t_begin, cf);
+            for (int q = 0; q < 4; ++q) cf[q] /= k.kz;
+            orc_dirac_magnus_U(2 * k.kz, 2 * k.ky, 2 * k.kx, measure_every, cf, U);
+            const double s0 = U[0] * S[0] + U[1] * S[1] + U[2] * S[2];
+            const double s1 = U[3] * S[0] + U[4] * S[1] + U[5] * S[2];
+            const double s2 = U[6] * S[0] + U[7] * S[1] + U[8] * S[2];
+            S[0] = s0, S[1] = s1, S[2] = s2;
+            st->attempted++;
+            st->accepted++;
         } else {
             const int rc = integrate_interval(&c, S, t_begin, t_end, dt, s, st, hist, nh, cap);
             if (rc != ORC_OK) return rc;

@@ -71,7 +71,8 @@ typedef struct {
 typedef struct {
     double abs_tol, rel_tol;
     int max_failed; /* Boost.Odeint failed_step_checker limit (500) */
-    int stepper;    /* 0 = controlled RKF78, 1 = Magnus-4 (one step per sub-interval) */
+    int stepper;    /* 0 = controlled RKF78, 1 = Magnus-4 (one step per sub-interval),
+                     * 2 = the reference's Dirac-3D closed-form Magnus step per interval */
     int magnus_substeps;
 } orc_solver;
 

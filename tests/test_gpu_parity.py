@@ -219,3 +219,33 @@ def test_fast_variants_meet_harmonic_bar(engine, model):
         herr, jerr, st, st_ref = _spectrum_err(engine, sys, pulse, grid, opts, ref)
         assert herr <= 1e-4, (opts.precision, opts.proposer, herr)
         assert jerr <= 1e-4, (opts.precision, opts.proposer, jerr)
+
+
+@pytest.mark.parametrize("beta,ef", [(0.0, 0.0), (1.5, 0.3)])
+def test_dirac3d_reference_magnus_parity(engine, beta, ef):
+    # DiracSystem::time_evolution_magnus (DiracSystem.cpp:176-211): one closed-form
+    # step per interval from the 30-point Legendre moments of A
+    rng = np.random.default_rng(11)
+    m = O.model(O.DIRAC3D, beta=beta, fermi_energy=ef)
+    rows = []
+    for _ in range(96):
+        kz, kap = rng.uniform(-1.5, 1.5), rng.uniform(0.05, 1.5)
+        mk = math.hypot(kz, kap)
+        rows.append([kz, kap, mk, kz * kap / mk, *O.initial_state(m, kz, kap, mk), 0.0])
+    rows = np.array(rows)
+    sys = api.system(api.SYS_DIRAC3D, beta=beta, fermi_energy=ef)
+    pulse = api.cosine_pulse(0.6, 2, 2048)
+    grid, keep = api.grid_explicit(rows)
+    j, st = engine.current_density(sys, pulse, grid, api.solver(stepper=api.STEPPER_DIRAC_MAGNUS))
+    jr, ost = oracle_j(sys, pulse, rows, 1e-12, 1e-8, stepper=2)
+    assert rel_l2(j, jr) <= 1e-12, rel_l2(j, jr)
+    assert st.attempted_steps == ost.attempted == 96 * 2048
+
+
+def test_dirac_magnus_refused_elsewhere(engine):
+    pulse = api.cosine_pulse(0.6, 1, 64)
+    grid = api.grid_tensor(4, 4, -1, 1, -1, 1)
+    with pytest.raises(api.HHGError) as ei:
+        engine.current_density(api.system(api.SYS_DIRAC2D, velocity=1.0), pulse, grid,
+                               api.solver(stepper=api.STEPPER_DIRAC_MAGNUS))
+    assert ei.value.status == api.UNSUPPORTED

@@ -73,3 +73,17 @@ def test_general_magnus4_converges_to_rkf78():
     # fourth order: halving the step cuts the error ~16x
     assert errs[0] / errs[1] > 10 and errs[1] / errs[2] > 10
     assert errs[2] < 1e-7
+
+
+def test_generic_dirac_magnus_stepper_is_the_reference_loop():
+    # the oracle's per-k loop with stepper 2 reproduces its restatement of
+    # DiracSystem::time_evolution_magnus bit for bit
+    import math
+    p = O.Pulse(0.7, 2)
+    tc = O.time_config(0.0, 4 * math.pi, 256)
+    for kz, kap in ((0.4, 0.9), (-1.1, 0.2), (0.05, 1.3)):
+        mk = math.hypot(kz, kap)
+        row = np.array([kz, kap, mk, 1.0, 0.0, 0.0, -1.0, 0.0])
+        states, st = O.evolve_k(O.model(O.DIRAC3D), p, tc, O.solver(stepper=2), row)
+        assert np.array_equal(states[:, 2], O.dirac3d_magnus_k(p, tc, kz, kap))
+        assert st.attempted == 256
