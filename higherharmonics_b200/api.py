@@ -25,7 +25,7 @@ GRID_TENSOR_GL, GRID_RHOMBIC_GL, GRID_PIFLUX3D_REF, GRID_HONEYCOMB_HEX_REF, GRID
 STEPPER_RKF78, STEPPER_MAGNUS4, STEPPER_DIRAC_MAGNUS = 0, 1, 2
 PREC_FP64, PREC_MIXED = 0, 1
 PROPOSER_NONE, PROPOSER_CARRY, PROPOSER_LEARNED, PROPOSER_LOCKSTEP = 0, 1, 2, 3
-PULSE_COSINE = 0
+PULSE_COSINE, PULSE_CONTINUOUS, PULSE_GAUSS, PULSE_SPLINE = 0, 1, 2, 3
 
 EXPORTED = [
     "hhg_abi_version", "hhg_gpu_create", "hhg_gpu_destroy", "hhg_last_error",
@@ -61,7 +61,10 @@ class PulseDesc(ctypes.Structure):
                 ("amplitude", ctypes.c_double), ("n_cycles", ctypes.c_double),
                 ("t_begin", ctypes.c_double), ("phase", ctypes.c_double),
                 ("window_begin", ctypes.c_double), ("window_end", ctypes.c_double),
-                ("energy_scale", ctypes.c_double)]
+                ("energy_scale", ctypes.c_double), ("samples", ctypes.POINTER(ctypes.c_double)),
+                ("n_samples", ctypes.c_int64), ("sample_dt", ctypes.c_double),
+                ("deriv_begin", ctypes.c_double), ("deriv_end", ctypes.c_double),
+                ("spline_cut", ctypes.c_double)]
 
 
 class GridDesc(ctypes.Structure):
@@ -240,6 +243,43 @@ def cosine_pulse(amplitude: float, n_cycles: float, n_measurements: int, *, t_be
         window = (t_begin, t_begin + 2 * math.pi * n_cycles)
     return PulseDesc(PULSE_COSINE, n_measurements, n_subdivisions, 0, amplitude, n_cycles,
                      t_begin, phase, window[0], window[1], energy_scale)
+
+
+def continuous_pulse(amplitude: float, n_measurements: int, window, *, phase=0.0,
+                     energy_scale=1.0, n_subdivisions=50) -> PulseDesc:
+    """ContinuousLaser: A(t) = A0 sin(t + phase) (ContinuousLaser.cpp); the
+    reference samples it on [-n_cycles pi, n_cycles pi] (PiFluxDispatcher.cpp:46-48)."""
+    return PulseDesc(PULSE_CONTINUOUS, n_measurements, n_subdivisions, 0, amplitude, 0.0, 0.0,
+                     phase, window[0], window[1], energy_scale)
+
+
+def gauss_pulse(amplitude: float, n_cycles: float, n_measurements: int, *, t_begin=0.0,
+                phase=0.0, window=None, energy_scale=1.0, n_subdivisions=50) -> PulseDesc:
+    """GaussLaser: A0 exp(-(t - c)^2 / 2 s^2) sin(t + phase), c = t_begin +
+    3 pi n_cycles, s = pi n_cycles / sqrt(2 ln 20) (GaussLaser.cpp); the
+    default window is the laser's [t_begin, t_begin + 6 pi n_cycles]."""
+    if window is None:
+        window = (t_begin, t_begin + 6 * math.pi * n_cycles)
+    return PulseDesc(PULSE_GAUSS, n_measurements, n_subdivisions, 0, amplitude, n_cycles,
+                     t_begin, phase, window[0], window[1], energy_scale)
+
+
+def spline_pulse(samples, t_begin: float, sample_dt: float, n_measurements: int, window, *,
+                 cut=None, deriv=(math.nan, math.nan), amplitude=1.0, energy_scale=1.0,
+                 n_subdivisions=50) -> PulseDesc:
+    """A(t) = amplitude * s(t) for t <= cut (default: the last sample), 0
+    after: s is the clamped cubic spline through the samples at t_begin +
+    k sample_dt with end slopes ``deriv`` (NaN: estimated), as the
+    reference's spline lasers (Laser.hpp:32-37).  The descriptor keeps a
+    reference to the sample array."""
+    y = np.ascontiguousarray(samples, dtype=np.float64)
+    if cut is None:
+        cut = t_begin + (y.size - 1) * sample_dt
+    d = PulseDesc(PULSE_SPLINE, n_measurements, n_subdivisions, 0, amplitude, 0.0, t_begin, 0.0,
+                  window[0], window[1], energy_scale, y.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                  y.size, sample_dt, deriv[0], deriv[1], cut)
+    d._samples = y
+    return d
 
 
 def grid_tensor(n1, n2, x_lo, x_hi, y_lo, y_hi) -> GridDesc:

@@ -22,11 +22,19 @@ of the reference's dispatchers and system constructors:
                   N_coarse 4 (PiFlux.hpp:11-22); Honeycomb N_k 64
                   (Honeycomb.hpp:12-21)
 
-Only the cosine laser exists on the device; the experimental, power-law,
-quench, double and continuous lasers and the Dirac system's adaptive kappa
-quadrature raise UnsupportedConfig.  Keys the path does not read (data_dir,
-debug_data, occupations, split_current, n_z) are accepted and ignored; the
-run modes occupations/split_current != "no" and debug_data != "no" raise
+Lasers (the dispatchers' laser_type branches, PiFluxDispatcher.cpp:44-106,
+HoneycombDispatcher.cpp:28-56): cosine, continuous and gauss run as analytic
+pulses; powerlaw<e>, quench and the double lasers dcos/dcosA/dcosB and
+dgauss/dgaussA/dgaussB are splines in the reference and are handed to the
+device as the same spline samples (PowerLawField.cpp:19-31,
+QuenchedField.cpp:15-29, DoubleLaser.hpp:42-68).  The photon energy of the
+system is multiplied by the experimental one for the exp and double lasers
+(Dispatcher.cpp:10-19).  The experimental lasers exp/expA/expB need the
+measured field of the reference's source, which this package does not carry:
+they raise UnsupportedConfig (api.spline_pulse takes such samples).  The
+Dirac system's adaptive kappa quadrature is not built either.  Keys the path
+does not read (data_dir, n_z) are accepted and ignored; the run modes
+occupations/split_current != "no" and debug_data != "no" raise
 UnsupportedConfig because they produce other outputs than j(t).
 """
 from __future__ import annotations
@@ -42,6 +50,9 @@ K_B = 0.08617333262145177434     # meV / K (GlobalDefinitions.hpp:29)
 SQRT3 = 1.732050807568877293527446341
 SQRT12 = 3.464101615137754587054892683
 MEASUREMENTS_PER_CYCLE = 1 << 10
+EXP_PHOTON_ENERGY = 6.091420442472572  # meV (ExperimentParams.hpp:11)
+DOUBLE_LASERS = {"dcos": ("cosine", "both"), "dcosA": ("cosine", "A"), "dcosB": ("cosine", "B"),
+                 "dgauss": ("gauss", "both"), "dgaussA": ("gauss", "A"), "dgaussB": ("gauss", "B")}
 PIFLUX_Z_RANGE, PIFLUX_N_COARSE = 32, 4
 HONEYCOMB_N_K = 64
 
@@ -103,11 +114,18 @@ def from_config(cfg: dict | str, *, grid: api.GridDesc | None = None,
         if cfg.get(mode, "no") != "no":
             raise UnsupportedConfig(f"{mode} = {cfg[mode]}: only the current density j(t) is built")
     laser_type = cfg.get("laser_type", "")
-    if laser_type != "cosine":
-        raise UnsupportedConfig(f"laser_type {laser_type!r}: only the cosine laser runs on the device")
+    known = {"cosine", "continuous", "gauss", "quench", "exp", "expA", "expB"} | set(DOUBLE_LASERS)
+    if not (laser_type in known or laser_type.startswith("powerlaw")) or \
+            (system_type == "Honeycomb" and (laser_type in DOUBLE_LASERS or laser_type == "gauss")):
+        raise ValueError(f"Laser type '{laser_type}' is not recognized!")
+    if laser_type in ("exp", "expA", "expB"):
+        raise UnsupportedConfig(f"laser_type {laser_type}: the measured pulse of the reference's "
+                                "ExperimentalLaser is not part of this package; pass its samples "
+                                "with api.spline_pulse")
 
     T, E_F, v_F = num("T"), num("E_F"), num("v_F")
-    band_width, E0, pe = num("band_width"), num("field_amplitude"), num("photon_energy")
+    band_width, E0, pe_in = num("band_width"), num("field_amplitude"), num("photon_energy")
+    pe = pe_in * EXP_PHOTON_ENERGY if laser_type in DOUBLE_LASERS else pe_in  # get_photon_energy
     tau_d = num("diagonal_relaxation_time")
     tau_o = float(cfg.get("offdiagonal_relaxation_time", "-1"))
     n_cycles = int(num("n_laser_cycles"))
@@ -131,10 +149,74 @@ def from_config(cfg: dict | str, *, grid: api.GridDesc | None = None,
     sys_ = api.system(kind, hopping=hopping, pol=pol, beta=beta, fermi_energy=E_F / pe,
                       inv_diag_relax=inv_d if relax else 0.0,
                       inv_offdiag_relax=inv_o if relax else 0.0)
-    amplitude = lattice * 1e11 * E0 / pe
-    t_begin = math.pi * t0_offset
-    t_end = t_begin + 2 * math.pi * n_cycles  # CosineLaser::base_duration
     n = n_measurements or n_cycles * MEASUREMENTS_PER_CYCLE
-    pulse = api.cosine_pulse(amplitude, n_cycles, n, t_begin=t_begin,
-                             window=(t_begin, t_end + 2 * math.pi))
+    pulse = make_pulse(laser_type, lattice, E0, pe_in, n_cycles, t0_offset, n)
     return Run(system_type, sys_, pulse, g, api.solver(1e-12, 1e-8), lattice)
+
+
+def _amplitude(ratio: float, E0: float, pe: float) -> float:
+    return ratio * 1e11 * E0 / pe  # Laser.cpp:24-25
+
+
+def _cosine(A0: float, n: float, t_begin: float, t: float) -> float:
+    # CosineLaser::laser_function (CosineLaser.cpp:22-26, Laser.hpp:32-37)
+    if t <= t_begin or t >= t_begin + 2 * math.pi * n:
+        return 0.0
+    return A0 * (0.5 * (1. - math.cos((1. / n) * (t - t_begin))) * math.sin(t))
+
+
+def _gauss(A0: float, n: float, t_begin: float, t: float) -> float:
+    # GaussLaser (GaussLaser.cpp:9-38)
+    centre = t_begin + 0.5 * (2.0 * math.pi * 3.0 * n)
+    sigma = math.pi * n / math.sqrt(2.0 * math.log(1.0 / 0.05))
+    return A0 * (math.exp(-((t - centre) * (t - centre)) / (2.0 * sigma * sigma)) * math.sin(t))
+
+
+def make_pulse(laser_type: str, ratio: float, E0: float, pe_in: float, n_cycles: int,
+               t0_offset: float, n: int) -> api.PulseDesc:
+    """The pulse and TimeIntegrationConfig of one laser_type, as the PiFlux /
+    Honeycomb dispatchers build them from the config's photon_energy pe_in."""
+    pe = pe_in * EXP_PHOTON_ENERGY if laser_type in DOUBLE_LASERS else pe_in
+    if laser_type == "cosine":
+        t_begin = math.pi * t0_offset
+        t_end = t_begin + 2 * math.pi * n_cycles  # CosineLaser::base_duration
+        return api.cosine_pulse(_amplitude(ratio, E0, pe), n_cycles, n, t_begin=t_begin,
+                                window=(t_begin, t_end + 2 * math.pi))
+    if laser_type == "continuous":
+        return api.continuous_pulse(_amplitude(ratio, E0, pe), n,
+                                    (-n_cycles * math.pi, n_cycles * math.pi))
+    if laser_type == "gauss":
+        t_begin = t0_offset  # GaussLaser(.., n_laser_cycles, t0_offset)
+        return api.gauss_pulse(_amplitude(ratio, E0, pe), n_cycles, n, t_begin=t_begin,
+                               window=(t_begin, t_begin + 2 * math.pi * 3.0 * n_cycles))
+    if laser_type == "quench" or laser_type.startswith("powerlaw"):
+        # a 256-sample spline template over [0, duration], duration = t0_offset
+        A0, t_end, N = _amplitude(ratio, E0, pe), t0_offset, 256
+        if laser_type == "quench":
+            y = [0.0 if (i < N // 4 or i > 3 * N // 4) else
+                 (0.5 * A0 if i in (N // 4, 3 * N // 4) else A0) for i in range(N)]
+            deriv = (0.0, 0.0)
+        else:
+            e = float(laser_type[len("powerlaw"):])
+            dt = t_end / N
+            norm = 1. / t_end ** e if e > 0 else 1. / dt ** e
+            y = [0.0] + [A0 * (i * dt) ** e * norm for i in range(1, N)]
+            deriv = (math.nan, math.nan)  # boost estimates them; exact for the linear ramp
+        return api.spline_pulse(y, 0.0, t_end / (N - 1), n, (0.0, t_end), cut=t_end, deriv=deriv)
+    base, active = DOUBLE_LASERS[laser_type]
+    # DoubleLaser<Base>(photon_energy, E0, ratio, n_cycles, t0_offset): laser A
+    # with 1.6 E0 at t = 0, laser B with 0.7 E0 delayed by t0_offset ps, sampled
+    # at 1000 points over 1.5 base durations, spline with zero end slopes
+    duration = 2 * math.pi * n_cycles * (3.0 if base == "gauss" else 1.0)
+    t_max = 1.5 * duration
+    shift = pe_in * (t0_offset * EXP_PHOTON_ENERGY / (1e12 * HBAR))  # ps_to_uniteless
+    one = _gauss if base == "gauss" else _cosine
+    aA, aB = _amplitude(ratio, 1.6 * E0, pe), _amplitude(ratio, 0.7 * E0, pe)
+    N = 1000
+    dt = t_max / (N - 1)
+    y = []
+    for i in range(N):
+        t = i * dt
+        a, b = one(aA, n_cycles, 0.0, t), one(aB, n_cycles, 0.0, t - shift + 0.0)
+        y.append(a + b if active == "both" else (a if active == "A" else b))
+    return api.spline_pulse(y, 0.0, dt, n, (0.0, t_max), cut=t_max, deriv=(0.0, 0.0))

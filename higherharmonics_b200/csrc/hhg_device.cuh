@@ -147,7 +147,13 @@ __host__ __device__ constexpr double rk_c(int s) {
          : s == 8 ? 2.0 / 3.0 : s == 9 ? 1.0 / 3.0 : s == 10 ? 1.0 : s == 11 ? 0.0 : 1.0;
 }
 
-// Per-pulse constants, prepared on the host.
+// Pulse shapes (hhg_pulse_kind): the reference's CosineLaser, ContinuousLaser,
+// GaussLaser and the spline lasers (Laser.hpp:32-37 with use_spline).
+enum PulseKind { PULSE_COSINE = 0, PULSE_CONTINUOUS = 1, PULSE_GAUSS = 2, PULSE_SPLINE = 3 };
+
+// Per-pulse constants, prepared on the host.  A(t) is zero outside the open
+// window (t_begin, t_end): the CosineLaser window, (-inf, inf) for the
+// continuous and Gaussian pulses, (-inf, spline_cut] for a spline.
 struct PulseDev {
     double amplitude, t_begin, t_end, inv_n_cycles, phase;
     double window_begin, measure_every, dt0;
@@ -159,6 +165,11 @@ struct PulseDev {
     long long j_off;      // samples into j
     int n_meas;
     int items;            // work items of this pulse
+    int kind;             // PulseKind
+    int spline_n;         // SPLINE: samples (the coefficient array holds spline_n + 2)
+    double gauss_c, gauss_2s2;         // GAUSS: centre and 2 sigma^2
+    double spline_t0, spline_inv_h;    // SPLINE: first sample time, 1 / sample spacing
+    const double *spline;              // SPLINE: cubic B-spline coefficients c_{-1..n} (device)
 };
 
 struct KParams {
@@ -190,18 +201,69 @@ struct KParams {
 constexpr int kHistFields = 12;
 
 // ---------------------------------------------------------------------------
-// Pulse: Laser::laser_function with CosineLaser::envelope (Laser.hpp:32-37,
-// CosineLaser.cpp:22-26); the continued form drops the window cut.
+// Pulse: Laser::laser_function (Laser.hpp:32-37) with the envelope of
+// CosineLaser (CosineLaser.cpp:22-26), ContinuousLaser (1), GaussLaser
+// (GaussLaser.cpp) or the spline; the continued form drops the window cut.
 // ---------------------------------------------------------------------------
+// Cubic B-spline of a SPLINE pulse on uniform knots t0 + k h: on the piece
+// t_k <= t < t_(k+1) (the first / last piece continued outside), s = sum of
+// c_(k-1..k+2) times the uniform cubic B-spline weights; d receives ds/dt.
+__device__ __forceinline__ double spline_value(const PulseDev &p, double t, double *d = nullptr) {
+    const double u = (t - p.spline_t0) * p.spline_inv_h;
+    int k = (int)floor(u);
+    k = k < 0 ? 0 : (k > p.spline_n - 2 ? p.spline_n - 2 : k);
+    const double x = u - k, y = 1.0 - x, x2 = x * x, x3 = x2 * x;
+    const double *c = p.spline + k;  // c[0] = c_(k-1)
+    const double w0 = y * y * y / 6.0;
+    const double w1 = (3.0 * x3 - 6.0 * x2 + 4.0) / 6.0;
+    const double w2 = (-3.0 * x3 + 3.0 * x2 + 3.0 * x + 1.0) / 6.0;
+    const double w3 = x3 / 6.0;
+    if (d) {
+        const double d0 = -0.5 * y * y, d1 = 1.5 * x2 - 2.0 * x;
+        const double d2 = -1.5 * x2 + x + 0.5, d3 = 0.5 * x2;
+        *d = (d0 * c[0] + d1 * c[1] + d2 * c[2] + d3 * c[3]) * p.spline_inv_h;
+    }
+    return w0 * c[0] + w1 * c[1] + w2 * c[2] + w3 * c[3];
+}
+
+// envelope(t) sin(t + phase) without the window cut (A / amplitude)
+__device__ __forceinline__ double laser_shape(const PulseDev &p, double t) {
+    if (p.kind == PULSE_CONTINUOUS) return sin(t + p.phase);
+    if (p.kind == PULSE_GAUSS) {
+        const double x = t - p.gauss_c;
+        return exp(-(x * x) / p.gauss_2s2) * sin(t + p.phase);
+    }
+    if (p.kind == PULSE_SPLINE) return spline_value(p, t);
+    return 0.5 * (1. - cos(p.inv_n_cycles * (t - p.t_begin))) * sin(t + p.phase);
+}
+
+// A(t) / amplitude with the window cut (Laser::raw_laser_function)
+__device__ __forceinline__ double laser_raw(const PulseDev &p, double t) {
+    if (p.kind == PULSE_COSINE) {
+        double env = 0.0;
+        if (!(t <= p.t_begin || t >= p.t_end)) env = 0.5 * (1. - cos(p.inv_n_cycles * (t - p.t_begin)));
+        return env * sin(t + p.phase);
+    }
+    if (t <= p.t_begin || t >= p.t_end) return 0.0;
+    return laser_shape(p, t);
+}
+
 __device__ __forceinline__ double laser_exact(const PulseDev &p, double t) {
-    double env = 0.0;
-    if (!(t <= p.t_begin || t >= p.t_end)) env = 0.5 * (1. - cos(p.inv_n_cycles * (t - p.t_begin)));
-    return p.amplitude * (env * sin(t + p.phase));
+    if (p.kind == PULSE_COSINE) {
+        double env = 0.0;
+        if (!(t <= p.t_begin || t >= p.t_end)) env = 0.5 * (1. - cos(p.inv_n_cycles * (t - p.t_begin)));
+        return p.amplitude * (env * sin(t + p.phase));
+    }
+    if (t <= p.t_begin || t >= p.t_end) return 0.0;
+    return p.amplitude * laser_shape(p, t);
 }
 
 __device__ __forceinline__ double laser_continued(const PulseDev &p, double t) {
-    const double env = 0.5 * (1. - cos(p.inv_n_cycles * (t - p.t_begin)));
-    return p.amplitude * (env * sin(t + p.phase));
+    if (p.kind == PULSE_COSINE) {
+        const double env = 0.5 * (1. - cos(p.inv_n_cycles * (t - p.t_begin)));
+        return p.amplitude * (env * sin(t + p.phase));
+    }
+    return p.amplitude * laser_shape(p, t);
 }
 
 // Staged functions of a pulse value A.
@@ -1324,18 +1386,15 @@ __global__ void stage_pulses_kernel(const PulseDev *__restrict__ pulses, int n_p
         for (int j = 0; j < NN; ++j) out[HDR + n * NN + j] = m[j];
     }
     if constexpr (LAYOUT == 3) {
-        // moments over [t0, t0 + measure_every] of the raw pulse (the envelope
-        // times the carrier), scaled by (2q + 1) A0 as Laser.cpp:50-54
+        // moments over [t0, t0 + measure_every] of the raw pulse (A / A0),
+        // scaled by (2q + 1) A0 as Laser.cpp:50-54
         double c0 = 0.0, c1 = 0.0, c2 = 0.0, c3 = 0.0;
         for (int q = 0; q < 30; ++q) {
             const double a = gl30[q], wq = gl30[30 + q];
             const double l2 = 2. * a - 1.;
             const double l3 = 6. * a * (a - 1.) + 1.;
             const double l4 = 20. * a * a * a - 30. * a * a + 12. * a + 1.;  // as gauss.hpp:96-99
-            const double t = t0 + pd.measure_every * a;
-            double env = 0.0;
-            if (!(t <= pd.t_begin || t >= pd.t_end)) env = 0.5 * (1. - cos(pd.inv_n_cycles * (t - pd.t_begin)));
-            const double lv = env * sin(t + pd.phase);
+            const double lv = laser_raw(pd, t0 + pd.measure_every * a);
             c0 += wq * lv;
             c1 += wq * l2 * lv;
             c2 += wq * l3 * lv;

@@ -426,12 +426,23 @@ hhg_status check_grid(hhg_ctx *ctx, const hhg_grid_desc *g) {
 }
 
 hhg_status check_pulse(hhg_ctx *ctx, const hhg_pulse_desc &p) {
-    if (p.kind != HHG_PULSE_COSINE) return set_err(ctx, HHG_UNSUPPORTED, "Laser type not recognized");
+    if (p.kind < HHG_PULSE_COSINE || p.kind > HHG_PULSE_SPLINE)
+        return set_err(ctx, HHG_BAD_CONFIG, "Laser type not recognized");
     if (p.n_measurements < 1 || p.n_measurements > (1 << 24))
         return set_err(ctx, HHG_BAD_CONFIG, "n_measurements out of range");
     if (p.n_subdivisions < 1) return set_err(ctx, HHG_BAD_CONFIG, "n_subdivisions must be >= 1");
-    if (!(p.n_cycles > 0.0) || !std::isfinite(p.n_cycles))
+    if ((p.kind == HHG_PULSE_COSINE || p.kind == HHG_PULSE_GAUSS) &&
+        (!(p.n_cycles > 0.0) || !std::isfinite(p.n_cycles)))
         return set_err(ctx, HHG_BAD_CONFIG, "n_cycles must be > 0");
+    if (p.kind == HHG_PULSE_SPLINE) {
+        if (!p.samples || p.n_samples < 5 || p.n_samples > (1 << 24))
+            return set_err(ctx, HHG_BAD_CONFIG, "a spline pulse needs 5 <= n_samples <= 2^24 samples");
+        if (!(p.sample_dt > 0.0) || !std::isfinite(p.sample_dt) || !std::isfinite(p.spline_cut) ||
+            std::isinf(p.deriv_begin) || std::isinf(p.deriv_end))
+            return set_err(ctx, HHG_BAD_CONFIG, "spline pulse: sample_dt > 0, finite cut and derivatives");
+        for (int64_t k = 0; k < p.n_samples; ++k)
+            if (!std::isfinite(p.samples[k])) return set_err(ctx, HHG_BAD_CONFIG, "non-finite pulse sample");
+    }
     if (!std::isfinite(p.amplitude) || !std::isfinite(p.t_begin) || !std::isfinite(p.phase) ||
         !std::isfinite(p.window_begin) || !std::isfinite(p.window_end) ||
         !std::isfinite(p.energy_scale))
@@ -470,6 +481,10 @@ std::string plan_key(const hhg_system_desc *sys, const hhg_pulse_desc *pulses, i
         const hhg_pulse_desc &q = pulses[i];
         put(&q.kind, 4 * 3);
         put(&q.amplitude, 8 * 7);
+        if (q.kind == HHG_PULSE_SPLINE && q.samples && q.n_samples > 0) {
+            put(&q.n_samples, 8 * 5);
+            put(q.samples, sizeof(double) * (size_t)q.n_samples);
+        }
     }
     put(&grid->kind, 4 * 3);
     put(&grid->x_lo, 8 * 4);
@@ -518,16 +533,147 @@ int model_nf(int m) {
 // fit's own rounding (~1e-19) sits below the threshold: the smallest degree in
 // {5, 7, 11} whose Chebyshev tail beyond it is below 2^-56 of the function scale
 // on sampled intervals, or -1 if even degree 11 is not enough.
-long double pulse_value_ld(const hhg_pulse_desc &p, long double t) {
-    const long double inv = 1.0L / p.n_cycles;
-    return (long double)p.amplitude * ((0.5L * (1.0L - cosl(inv * (t - p.t_begin)))) * sinl(t + p.phase));
+// ---------------------------------------------------------------------------
+// Pulses on the host: the spline coefficients, A(t) for the sample-0 record
+// and the window checks, the continued A(t) in long double for the degree test.
+// ---------------------------------------------------------------------------
+// Clamped cubic spline through y[0..n) at spacing h as cardinal cubic
+// B-spline coefficients c_(-1..n) (n + 2 values): interpolation (c_(k-1) +
+// 4 c_k + c_(k+1)) / 6 = y_k, end slopes (c_1 - c_(-1)) / 2h = d0 and (c_n -
+// c_(n-2)) / 2h = dn, eliminated into a tridiagonal system solved in long
+// double.  A NaN slope takes the one-sided five-point difference.
+std::vector<double> spline_coefficients(const double *y, int64_t n, double h, double d0, double dn) {
+    if (std::isnan(d0)) d0 = (-25.0 * y[0] + 48.0 * y[1] - 36.0 * y[2] + 16.0 * y[3] - 3.0 * y[4]) / (12.0 * h);
+    if (std::isnan(dn))
+        dn = (25.0 * y[n - 1] - 48.0 * y[n - 2] + 36.0 * y[n - 3] - 16.0 * y[n - 4] + 3.0 * y[n - 5]) / (12.0 * h);
+    std::vector<long double> sub(n), diag(n), sup(n), rhs(n), c(n);
+    for (int64_t k = 0; k < n; ++k) {
+        sub[k] = 1.0L;
+        diag[k] = 4.0L;
+        sup[k] = 1.0L;
+        rhs[k] = 6.0L * y[k];
+    }
+    sup[0] = 2.0L;
+    rhs[0] += 2.0L * h * d0;
+    sub[n - 1] = 2.0L;
+    rhs[n - 1] -= 2.0L * h * dn;
+    for (int64_t k = 1; k < n; ++k) {  // Thomas elimination (diagonally dominant)
+        const long double m = sub[k] / diag[k - 1];
+        diag[k] -= m * sup[k - 1];
+        rhs[k] -= m * rhs[k - 1];
+    }
+    c[n - 1] = rhs[n - 1] / diag[n - 1];
+    for (int64_t k = n - 2; k >= 0; --k) c[k] = (rhs[k] - sup[k] * c[k + 1]) / diag[k];
+    std::vector<double> out(n + 2);
+    out[0] = (double)(c[1] - 2.0L * h * d0);
+    for (int64_t k = 0; k < n; ++k) out[k + 1] = (double)c[k];
+    out[n + 1] = (double)(c[n - 2] + 2.0L * h * dn);
+    return out;
 }
 
+struct HostPulse {
+    const hhg_pulse_desc &q;
+    std::vector<double> coef;  // SPLINE
+    explicit HostPulse(const hhg_pulse_desc &p) : q(p) {
+        if (q.kind == HHG_PULSE_SPLINE)
+            coef = spline_coefficients(q.samples, q.n_samples, q.sample_dt, q.deriv_begin, q.deriv_end);
+    }
+    // GaussLaser (GaussLaser.cpp): centre and 2 sigma^2
+    long double gauss_c() const { return q.t_begin + 3.0L * kPi * q.n_cycles; }
+    double gauss_2s2() const {
+        const double sigma = kPi * q.n_cycles / std::sqrt(2.0 * std::log(1.0 / 0.05));
+        return 2.0 * sigma * sigma;
+    }
+    long double spline_ld(long double t) const {
+        const int64_t n = q.n_samples;
+        const long double u = (t - q.t_begin) / q.sample_dt;
+        int64_t k = (int64_t)floorl(u);
+        k = k < 0 ? 0 : (k > n - 2 ? n - 2 : k);
+        const long double x = u - k, y = 1.0L - x;
+        const double *c = coef.data() + k;
+        return (y * y * y * c[0] + (3 * x * x * x - 6 * x * x + 4) * c[1] +
+                (-3 * x * x * x + 3 * x * x + 3 * x + 1) * c[2] + x * x * x * c[3]) / 6.0L;
+    }
+    // A(t) without the window cut
+    long double continued_ld(long double t) const {
+        switch (q.kind) {
+        case HHG_PULSE_CONTINUOUS: return (long double)q.amplitude * sinl(t + q.phase);
+        case HHG_PULSE_GAUSS: {
+            const long double x = t - gauss_c();
+            return (long double)q.amplitude * expl(-(x * x) / gauss_2s2()) * sinl(t + q.phase);
+        }
+        case HHG_PULSE_SPLINE: return (long double)q.amplitude * spline_ld(t);
+        default: {
+            const long double inv = 1.0L / q.n_cycles;
+            return (long double)q.amplitude * ((0.5L * (1.0L - cosl(inv * (t - q.t_begin)))) * sinl(t + q.phase));
+        }
+        }
+    }
+    // the open window outside which A = 0
+    void window(double &tb, double &te) const {
+        tb = -INFINITY;
+        te = INFINITY;
+        if (q.kind == HHG_PULSE_COSINE) {
+            tb = q.t_begin;
+            te = q.t_begin + 2 * kPi * q.n_cycles;  // CosineLaser::base_duration (CosineLaser.hpp:13-15)
+        } else if (q.kind == HHG_PULSE_SPLINE) {
+            te = std::nextafter(q.spline_cut, INFINITY);  // A(t) = 0 for t > t_end (Laser.hpp:35)
+        }
+    }
+    // A(t) as the device's laser_exact
+    double value(double t) const {
+        if (q.kind == HHG_PULSE_COSINE) {
+            const double te = q.t_begin + 2 * kPi * q.n_cycles;
+            double env = 0.0;
+            if (!(t <= q.t_begin || t >= te)) env = 0.5 * (1. - cos((1. / q.n_cycles) * (t - q.t_begin)));
+            return q.amplitude * (env * sin(t + q.phase));
+        }
+        double tb, te;
+        window(tb, te);
+        if (t <= tb || t >= te) return 0.0;
+        return (double)continued_ld(t);
+    }
+};
+
+// Everything of a device pulse record that depends on the pulse alone; the
+// spline coefficient pointer is set by the caller once the device copy exists.
+void fill_pulse_dev(const hhg_pulse_desc &q, const HostPulse &hp, PulseDev &d) {
+    d.amplitude = q.amplitude;
+    hp.window(d.t_begin, d.t_end);
+    d.inv_n_cycles = q.kind == HHG_PULSE_COSINE ? 1. / q.n_cycles : 0.0;
+    d.phase = q.phase;
+    d.window_begin = q.window_begin;
+    d.measure_every = (q.window_end - q.window_begin) / q.n_measurements;
+    d.dt0 = d.measure_every / q.n_subdivisions;
+    d.kind = q.kind;
+    if (q.kind == HHG_PULSE_GAUSS) {
+        d.gauss_c = (double)hp.gauss_c();
+        d.gauss_2s2 = hp.gauss_2s2();
+    }
+    if (q.kind == HHG_PULSE_SPLINE) {
+        d.spline_n = (int)q.n_samples;
+        d.spline_t0 = q.t_begin;
+        d.spline_inv_h = 1.0 / q.sample_dt;
+    }
+    d.n_meas = q.n_measurements;
+}
+
+// Chebyshev-tail threshold of the staged interpolants: 2^-56 of the function
+// scale, tested on up to 257 evenly spread intervals (the analytic pulses
+// are uniformly smooth).  A spline pulse is only C2 at its knots: at the
+// reference's sampling (1024 intervals per cycle, DoubleLaser's 1000 knots
+// over 1.5 pulse durations) the tail of an interval holding a knot is ~4e-16
+// of the scale in the median and up to 3e-12 where the sampled sub-pulse has a
+// kink (the CosineLaser's window edge) or its steepest curvature, so the
+// spline threshold is 2^-36 and every interval is tested; knots denser than
+// the intervals, or a spline that turns within a knot or two (QuenchedField's
+// step, 4e-9), are refused.
 int choose_degree(const hhg_pulse_desc &p, const double *proj, int nf) {
+    const HostPulse hp(p);
     const int NN = 16;
     const long double pi = 3.141592653589793238462643383279502884L;
     const long double me = ((long double)p.window_end - p.window_begin) / p.n_measurements;
-    const int samples = std::min(p.n_measurements, 257);
+    const int samples = p.kind == HHG_PULSE_SPLINE ? p.n_measurements : std::min(p.n_measurements, 257);
     long double tail5 = 0.0L, tail7 = 0.0L, tail11 = 0.0L, scale = 1.0L;
     for (int q = 0; q < samples; ++q) {
         const int i = (int)((long long)q * p.n_measurements / samples);
@@ -537,7 +683,7 @@ int choose_degree(const hhg_pulse_desc &p, const double *proj, int nf) {
             for (int part = 0; part < (nf == 1 ? 1 : 2); ++part) {
                 long double fv[NN];
                 for (int k = 0; k < NN; ++k) {
-                    const long double A = pulse_value_ld(p, ctr + half * cosl(pi * (k + 0.5L) / NN));
+                    const long double A = hp.continued_ld(ctr + half * cosl(pi * (k + 0.5L) / NN));
                     if (nf == 1) fv[k] = A;
                     else fv[k] = part == 0 ? cosl(proj[n] * A) : sinl(proj[n] * A);
                 }
@@ -553,7 +699,7 @@ int choose_degree(const hhg_pulse_desc &p, const double *proj, int nf) {
             }
         }
     }
-    const long double thr = ldexpl(1.0L, -56) * scale;
+    const long double thr = ldexpl(1.0L, p.kind == HHG_PULSE_SPLINE ? -36 : -56) * scale;
     if (tail5 <= thr) return 5;
     if (tail7 <= thr) return 7;
     if (tail11 <= thr) return 11;
@@ -574,12 +720,7 @@ void set_relax_params(const hhg_system_desc &s, double es, double *mp) {
 }
 
 // A(t) of one pulse on the host, as the device's laser_exact.
-double host_laser(const hhg_pulse_desc &q, double t) {
-    const double te = q.t_begin + 2 * kPi * q.n_cycles;
-    double env = 0.0;
-    if (!(t <= q.t_begin || t >= te)) env = 0.5 * (1. - cos((1. / q.n_cycles) * (t - q.t_begin)));
-    return q.amplitude * (env * sin(t + q.phase));
-}
+double host_laser(const hhg_pulse_desc &q, double t) { return HostPulse(q).value(t); }
 
 // Requests the relaxation kernels do not cover.
 hhg_status check_relax(hhg_ctx *ctx, const hhg_system_desc &s, const hhg_pulse_desc *pulses,
@@ -811,7 +952,10 @@ hhg_status hhg_plan_create(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_p
         if (d < 0) {
             delete pl;
             return set_err(ctx, HHG_UNSUPPORTED,
-                           "measurement interval too coarse for the staged pulse interpolants");
+                           pulses[p].kind == HHG_PULSE_SPLINE
+                               ? "spline pulse: knots too dense or too steep for the measurement "
+                                 "intervals (more n_measurements, or smoother samples)"
+                               : "measurement interval too coarse for the staged pulse interpolants");
         }
         degree = std::max(degree, d);
     }
@@ -848,18 +992,18 @@ hhg_status hhg_plan_create(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_p
     for (int p = 0; p < n_pulses; ++p) pl->window_end[p] = pulses[p].window_end;
     std::vector<long long> ioff(n_pulses + 1, 0);
     long long coef_len = 0, part_len = 0, j_len = 0;
+    std::vector<double> spline_coef;  // spline pulses' coefficients, stored after the slots
+    std::vector<long long> spline_off(n_pulses, -1);
     for (int p = 0; p < n_pulses; ++p) {
         const hhg_pulse_desc &q = pulses[p];
         PulseDev &d = pl->pulses[p];
         std::memset(&d, 0, sizeof d);
-        d.amplitude = q.amplitude;
-        d.t_begin = q.t_begin;
-        d.t_end = q.t_begin + 2 * kPi * q.n_cycles;  // CosineLaser::base_duration (CosineLaser.hpp:13-15)
-        d.inv_n_cycles = 1. / q.n_cycles;
-        d.phase = q.phase;
-        d.window_begin = q.window_begin;
-        d.measure_every = (q.window_end - q.window_begin) / q.n_measurements;
-        d.dt0 = d.measure_every / q.n_subdivisions;
+        const HostPulse hp(q);
+        fill_pulse_dev(q, hp, d);
+        if (q.kind == HHG_PULSE_SPLINE) {
+            spline_off[p] = (long long)spline_coef.size();
+            spline_coef.insert(spline_coef.end(), hp.coef.begin(), hp.coef.end());
+        }
         const double es = q.energy_scale;
         switch (sys->kind) {
         case HHG_SYS_DIRAC2D:
@@ -884,10 +1028,7 @@ hhg_status hhg_plan_create(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_p
         set_relax_params(*sys, es, d.mp);
         for (int n = 0; n < 3; ++n) d.s[n] = proj[n];
         // sample-0 record, exact: A(t_0) and the staged functions at it
-        const double t0s = 0 * d.measure_every + d.window_begin;
-        double env = 0.0;
-        if (!(t0s <= d.t_begin || t0s >= d.t_end)) env = 0.5 * (1. - cos(d.inv_n_cycles * (t0s - d.t_begin)));
-        const double A0 = d.amplitude * (env * sin(t0s + d.phase));
+        const double A0 = hp.value(0 * d.measure_every + d.window_begin);
         d.s0rec[0] = A0;
         if (nf == 1) d.s0rec[1] = A0;
         else if (hhg::base_model(pl->model) == hhg::PIFLUX3D) {
@@ -926,6 +1067,8 @@ hhg_status hhg_plan_create(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_p
     }
     const long long gl_off = coef_len;
     if (magnus_moments) coef_len += 60;
+    const long long spline_base = coef_len;
+    coef_len += (long long)spline_coef.size();
     pl->coef_len = coef_len;
     pl->part_len = part_len;
     pl->j_len = j_len;
@@ -959,6 +1102,8 @@ hhg_status hhg_plan_create(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_p
     if ((e = cudaMalloc(&pl->d_ioff, ioff.size() * sizeof(long long))) != cudaSuccess) return fail("alloc offsets", e);
     if ((e = cudaMalloc(&pl->d_counters, 8 * sizeof(unsigned long long))) != cudaSuccess) return fail("alloc counters", e);
     if ((e = cudaMalloc(&pl->d_status, sizeof(int))) != cudaSuccess) return fail("alloc status", e);
+    for (int p = 0; p < n_pulses; ++p)
+        if (spline_off[p] >= 0) pl->pulses[p].spline = pl->d_coef + spline_base + spline_off[p];
     if (o.proposer == HHG_PROPOSER_LEARNED) {
         hhg::MlpPacked packed;
         hhg::pack_mlp(*o.mlp, &packed);
@@ -975,6 +1120,10 @@ hhg_status hhg_plan_create(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_p
     if (magnus_moments &&
         (e = cudaMemcpyAsync(pl->d_coef + gl_off, gl30.data(), 60 * sizeof(double), cudaMemcpyHostToDevice, s)) != cudaSuccess)
         return fail("upload quadrature", e);
+    if (!spline_coef.empty() &&
+        (e = cudaMemcpyAsync(pl->d_coef + spline_base, spline_coef.data(), spline_coef.size() * sizeof(double),
+                             cudaMemcpyHostToDevice, s)) != cudaSuccess)
+        return fail("upload pulse splines", e);
     hhg::StageReq sr{pl->d_pulses, n_pulses, pl->d_tgrid, pl->d_ioff, pl->d_coef,
                      pl->n_intervals, degree, 9.0 / 10.0 * pow(pow(5.0, -8.0), -1.0 / 8), s};
     sr.layout = dyadic ? (o.precision == HHG_PREC_MIXED ? 2 : 1) : (magnus_moments ? 3 : 0);
@@ -1386,16 +1535,11 @@ hhg_status prepare_pulse(const hhg_system_desc *sys, const hhg_pulse_desc *pulse
     const int d = choose_degree(*pulse, proj, out.nf);
     out.degree = d < 0 ? -1 : std::max(5, d);
     const hhg_pulse_desc &q = *pulse;
+    if (q.kind == HHG_PULSE_SPLINE) return HHG_UNSUPPORTED;  // its coefficients would need device memory
     PulseDev &p = out.pulse;
     std::memset(&p, 0, sizeof p);
-    p.amplitude = q.amplitude;
-    p.t_begin = q.t_begin;
-    p.t_end = q.t_begin + 2 * kPi * q.n_cycles;
-    p.inv_n_cycles = 1. / q.n_cycles;
-    p.phase = q.phase;
-    p.window_begin = q.window_begin;
-    p.measure_every = (q.window_end - q.window_begin) / q.n_measurements;
-    p.dt0 = p.measure_every / q.n_subdivisions;
+    const HostPulse hp(q);
+    fill_pulse_dev(q, hp, p);
     const double es = q.energy_scale;
     switch (sys->kind) {
     case HHG_SYS_DIRAC2D: p.mp[0] = 2.0 * sys->velocity * es; p.mp[1] = 2.0 * sys->mass * es; break;
@@ -1408,10 +1552,7 @@ hhg_status prepare_pulse(const hhg_system_desc *sys, const hhg_pulse_desc *pulse
     p.mp[3] = sys->pol_y;
     set_relax_params(*sys, es, p.mp);
     for (int n = 0; n < 3; ++n) p.s[n] = proj[n];
-    const double t0s = 0 * p.measure_every + p.window_begin;
-    double env = 0.0;
-    if (!(t0s <= p.t_begin || t0s >= p.t_end)) env = 0.5 * (1. - cos(p.inv_n_cycles * (t0s - p.t_begin)));
-    const double A0 = p.amplitude * (env * sin(t0s + p.phase));
+    const double A0 = hp.value(0 * p.measure_every + p.window_begin);
     p.s0rec[0] = A0;
     if (out.nf == 1) p.s0rec[1] = A0;
     else if (hhg::base_model(out.model) == hhg::PIFLUX3D) {

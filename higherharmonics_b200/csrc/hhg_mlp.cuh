@@ -35,12 +35,24 @@ struct MlpPacked {
     float in_mu[kMlpIn], in_isig[kMlpIn];
 };
 
-// E(t) = -dA/dt of the CosineLaser pulse (zero outside the window).
+// E(t) = -dA/dt of the pulse (zero outside the window).
 __device__ __forceinline__ double laser_field(const PulseDev &p, double t) {
     if (t <= p.t_begin || t >= p.t_end) return 0.0;
-    double se, ce, sc, cc;
-    sincos(p.inv_n_cycles * (t - p.t_begin), &se, &ce);
+    double sc, cc;
     sincos(t + p.phase, &sc, &cc);
+    if (p.kind == PULSE_CONTINUOUS) return -p.amplitude * cc;
+    if (p.kind == PULSE_GAUSS) {
+        const double x = t - p.gauss_c;
+        const double env = exp(-(x * x) / p.gauss_2s2), denv = -2.0 * x / p.gauss_2s2 * env;
+        return -p.amplitude * (denv * sc + env * cc);
+    }
+    if (p.kind == PULSE_SPLINE) {
+        double d;
+        spline_value(p, t, &d);
+        return -p.amplitude * d;
+    }
+    double se, ce;
+    sincos(p.inv_n_cycles * (t - p.t_begin), &se, &ce);
     const double env = 0.5 * (1. - ce), denv = 0.5 * p.inv_n_cycles * se;
     return -p.amplitude * (denv * sc + env * cc);
 }

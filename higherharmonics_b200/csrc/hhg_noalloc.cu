@@ -128,6 +128,10 @@ extern "C" hhg_status hhg_gpu_current_density_noalloc(const hhg_system_desc *sys
     if (o.max_failed_steps < 1) o.max_failed_steps = 500;
     if (o.max_attempts_per_interval < 1) o.max_attempts_per_interval = 100000;
 
+    if (pulse && pulse->kind == HHG_PULSE_SPLINE) {
+        set_msg(err, err_cap, "the allocation-free entry point takes the analytic pulse shapes, not splines");
+        return HHG_UNSUPPORTED;
+    }
     hhg_prep::PulsePrep prep;
     hhg_status st = hhg_prep::prepare_pulse(sys, pulse, prep);
     if (st != HHG_OK) {

@@ -92,16 +92,31 @@ typedef struct hhg_system_desc {
 } hhg_system_desc;
 
 typedef enum hhg_pulse_kind {
-    HHG_PULSE_COSINE = 0 /* CosineLaser, sources/HHG/Laser/CosineLaser.cpp:22-26 */
+    HHG_PULSE_COSINE = 0,     /* CosineLaser, sources/HHG/Laser/CosineLaser.cpp:22-26 */
+    HHG_PULSE_CONTINUOUS = 1, /* ContinuousLaser: envelope 1 (ContinuousLaser.cpp) */
+    HHG_PULSE_GAUSS = 2,      /* GaussLaser (GaussLaser.cpp): envelope
+                                 exp(-(t - c)^2 / (2 s^2)), c = t_begin + 3 pi n_cycles,
+                                 s = pi n_cycles / sqrt(2 ln 20); no window cut */
+    HHG_PULSE_SPLINE = 3      /* Laser::laser_function with use_spline (Laser.hpp:32-37):
+                                 a cubic spline through caller samples, 0 after
+                                 spline_cut -- the reference's PowerLawField,
+                                 QuenchedField, DoubleLaser and ExperimentalLaser */
 } hhg_pulse_kind;
 
 /* One pulse instance plus its TimeIntegrationConfig
  * (sources/HHG/TimeIntegrationConfig.hpp:5-12).  A(t) =
- * amplitude * envelope(t) * sin(t + phase) with envelope = 0.5(1 - cos((t -
- * t_begin)/n_cycles)) on (t_begin, t_begin + 2 pi n_cycles), 0 elsewhere;
- * phase = 0 is the reference.  The sampled window is [window_begin,
- * window_end] in n_measurements intervals of n_subdivisions initial RKF78
- * steps each (the reference uses 50, e.g. PiFluxDispatcher.cpp:53). */
+ * amplitude * envelope(t) * sin(t + phase): for COSINE envelope = 0.5(1 -
+ * cos((t - t_begin)/n_cycles)) on (t_begin, t_begin + 2 pi n_cycles), 0
+ * elsewhere; CONTINUOUS and GAUSS as above; phase = 0 is the reference.  For
+ * SPLINE, A(t) = amplitude * s(t) for t <= spline_cut and 0 after, where s is
+ * the cubic spline through samples[k] at t_begin + k sample_dt (k <
+ * n_samples) with s' = deriv_begin at the first and deriv_end at the last
+ * sample (clamped ends, as boost::math cardinal_cubic_b_spline with given
+ * endpoint derivatives; a NaN derivative is estimated by the one-sided
+ * five-point difference), beyond the last sample the last piece continued.
+ * The sampled window is [window_begin, window_end] in n_measurements
+ * intervals of n_subdivisions initial RKF78 steps each (the reference uses
+ * 50, e.g. PiFluxDispatcher.cpp:53). */
 typedef struct hhg_pulse_desc {
     int32_t kind;
     int32_t n_measurements;
@@ -114,6 +129,11 @@ typedef struct hhg_pulse_desc {
     double window_begin;  /* TimeIntegrationConfig::t_begin */
     double window_end;    /* TimeIntegrationConfig::t_end */
     double energy_scale;  /* multiplies hopping, velocity and mass */
+    const double *samples;  /* HHG_PULSE_SPLINE: n_samples values, host memory (read during the call) */
+    int64_t n_samples;      /* >= 4 */
+    double sample_dt;
+    double deriv_begin, deriv_end;
+    double spline_cut;      /* Laser::t_end of a spline laser */
 } hhg_pulse_desc;
 
 /* k-point quadrature. */

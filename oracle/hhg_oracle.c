@@ -79,8 +79,63 @@ static inline double cosine_envelope(const orc_pulse *p, double t) {
     return 0.5 * (1. - cos(p->inv_n_cycles * (t - p->t_begin)));
 }
 
+void orc_spline_moments(const double *y, int n, double h, double d0, double dn, double *m) {
+    if (isnan(d0)) d0 = (-25.0 * y[0] + 48.0 * y[1] - 36.0 * y[2] + 16.0 * y[3] - 3.0 * y[4]) / (12.0 * h);
+    if (isnan(dn))
+        dn = (25.0 * y[n - 1] - 48.0 * y[n - 2] + 36.0 * y[n - 3] - 16.0 * y[n - 4] + 3.0 * y[n - 5]) / (12.0 * h);
+    /* 2 M_0 + M_1 = 6 ((y_1 - y_0)/h - d0)/h; M_(k-1) + 4 M_k + M_(k+1) =
+     * 6 (y_(k+1) - 2 y_k + y_(k-1))/h^2; M_(n-2) + 2 M_(n-1) = 6 (dn - (y_(n-1)
+     * - y_(n-2))/h)/h; solved by Gaussian elimination of the tridiagonal */
+    double *cp = malloc(sizeof(double) * n), *dp = malloc(sizeof(double) * n);
+    for (int k = 0; k < n; ++k) {
+        double a = 1.0, b = 4.0, c = 1.0, r;
+        if (k == 0) {
+            a = 0.0, b = 2.0;
+            r = 6.0 * ((y[1] - y[0]) / h - d0) / h;
+        } else if (k == n - 1) {
+            b = 2.0, c = 0.0;
+            r = 6.0 * (dn - (y[n - 1] - y[n - 2]) / h) / h;
+        } else {
+            r = 6.0 * (y[k + 1] - 2.0 * y[k] + y[k - 1]) / (h * h);
+        }
+        const double den = k == 0 ? b : b - a * cp[k - 1];
+        cp[k] = c / den;
+        dp[k] = (k == 0 ? r : r - a * dp[k - 1]) / den;
+    }
+    m[n - 1] = dp[n - 1];
+    for (int k = n - 2; k >= 0; --k) m[k] = dp[k] - cp[k] * m[k + 1];
+    free(cp), free(dp);
+}
+
+/* s(t) on the piece of t (the first / last piece continued outside) */
+static double spline_eval(const orc_pulse *p, double t) {
+    const double h = p->spline_h;
+    int k = (int)floor((t - p->t_begin) / h);
+    if (k < 0) k = 0;
+    if (k > p->spline_n - 2) k = p->spline_n - 2;
+    const double a = (p->t_begin + (k + 1) * h) - t, b = t - (p->t_begin + k * h);
+    const double *y = p->spline_y, *m = p->spline_m;
+    return m[k] * a * a * a / (6.0 * h) + m[k + 1] * b * b * b / (6.0 * h) +
+           (y[k] - m[k] * h * h / 6.0) * a / h + (y[k + 1] - m[k + 1] * h * h / 6.0) * b / h;
+}
+
+/* Laser::raw_laser_function (Laser.hpp:38-42): the CosineLaser, the
+ * ContinuousLaser (envelope 1), the GaussLaser envelope
+ * exp(-((t - c)(t - c)) / (2 s s)) (GaussLaser.cpp:36-38) or the spline,
+ * which is 0 after t_end (Laser.hpp:35). */
 double orc_raw_laser(const orc_pulse *p, double t) {
-    return cosine_envelope(p, t) * sin(t + p->phase);
+    switch (p->kind) {
+    case ORC_PULSE_CONTINUOUS:
+        return sin(t + p->phase);
+    case ORC_PULSE_GAUSS: {
+        const double x = t - p->gauss_center;
+        return exp(-(x * x) / (2.0 * p->gauss_sigma * p->gauss_sigma)) * sin(t + p->phase);
+    }
+    case ORC_PULSE_SPLINE:
+        return t > p->t_end ? 0.0 : spline_eval(p, t);
+    default:
+        return cosine_envelope(p, t) * sin(t + p->phase);
+    }
 }
 
 double orc_laser(const orc_pulse *p, double t) { return p->amplitude * orc_raw_laser(p, t); }

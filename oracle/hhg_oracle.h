@@ -55,12 +55,22 @@ typedef struct {
     double inv_offdiag_relax;
 } orc_model;
 
+enum { ORC_PULSE_COSINE = 0, ORC_PULSE_CONTINUOUS = 1, ORC_PULSE_GAUSS = 2, ORC_PULSE_SPLINE = 3 };
+
 typedef struct {
     double amplitude;    /* A0 = Laser::momentum_amplitude */
     double t_begin;      /* Laser::t_begin */
     double t_end;        /* Laser::t_end */
     double inv_n_cycles; /* CosineLaser::envelope_omega = 1/n_cycles */
     double phase;        /* carrier phase phi (0 in the reference) */
+    int kind;            /* ORC_PULSE_*; 0 = the CosineLaser above */
+    double gauss_center, gauss_sigma; /* GaussLaser (GaussLaser.cpp) */
+    /* spline pulse: A = amplitude * s(t) for t <= t_end, 0 after; s through
+     * spline_y[k] at t_begin + k spline_h with second derivatives spline_m
+     * (orc_spline_moments) */
+    const double *spline_y, *spline_m;
+    int spline_n;
+    double spline_h;
 } orc_pulse;
 
 typedef struct {
@@ -82,6 +92,11 @@ typedef struct {
 
 /* k table row: kx, ky, kz, weight, S0x, S0y, S0z, pad (8 doubles) */
 #define ORC_KROW 8
+
+/* Second derivatives M_k of the clamped cubic spline through y[0..n) at
+ * spacing h with end slopes d0, dn (NaN: the one-sided five-point
+ * difference): the moment equations of the interpolating cubic spline. */
+void orc_spline_moments(const double *y, int n, double h, double d0, double dn, double *m);
 
 double orc_laser(const orc_pulse *p, double t);
 double orc_raw_laser(const orc_pulse *p, double t);

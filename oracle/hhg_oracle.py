@@ -38,7 +38,11 @@ class OrcModel(ctypes.Structure):
 class OrcPulse(ctypes.Structure):
     _fields_ = [("amplitude", ctypes.c_double), ("t_begin", ctypes.c_double),
                 ("t_end", ctypes.c_double), ("inv_n_cycles", ctypes.c_double),
-                ("phase", ctypes.c_double)]
+                ("phase", ctypes.c_double), ("kind", ctypes.c_int),
+                ("gauss_center", ctypes.c_double), ("gauss_sigma", ctypes.c_double),
+                ("spline_y", ctypes.POINTER(ctypes.c_double)),
+                ("spline_m", ctypes.POINTER(ctypes.c_double)), ("spline_n", ctypes.c_int),
+                ("spline_h", ctypes.c_double)]
 
 
 class OrcTimeConfig(ctypes.Structure):
@@ -104,6 +108,60 @@ class Pulse:
 
     def c(self) -> OrcPulse:
         return OrcPulse(self.amplitude, self.t_begin, self.t_end, 1.0 / self.n_cycles, self.phase)
+
+
+PULSE_CONTINUOUS, PULSE_GAUSS, PULSE_SPLINE = 1, 2, 3
+
+
+@dataclass
+class ContinuousPulse:
+    """ContinuousLaser (ContinuousLaser.cpp): envelope 1."""
+    amplitude: float
+    phase: float = 0.0
+    t_begin: float = 0.0
+
+    def c(self) -> OrcPulse:
+        p = OrcPulse(self.amplitude, -np.inf, np.inf, 0.0, self.phase)
+        p.kind = PULSE_CONTINUOUS
+        return p
+
+
+@dataclass
+class GaussPulse:
+    """GaussLaser (GaussLaser.cpp): centre t_begin + 3 pi n_cycles, sigma =
+    pi n_cycles / sqrt(2 ln 20)."""
+    amplitude: float
+    n_cycles: float
+    t_begin: float = 0.0
+    phase: float = 0.0
+
+    def c(self) -> OrcPulse:
+        p = OrcPulse(self.amplitude, self.t_begin, self.t_begin + 6 * np.pi * self.n_cycles, 0.0,
+                     self.phase)
+        p.kind = PULSE_GAUSS
+        p.gauss_center = self.t_begin + 0.5 * (2.0 * np.pi * 3.0 * self.n_cycles)
+        p.gauss_sigma = np.pi * self.n_cycles / np.sqrt(2.0 * np.log(1.0 / 0.05))
+        return p
+
+
+class SplinePulse:
+    """A = amplitude * s(t) for t <= cut, 0 after: the clamped cubic spline
+    through samples at t_begin + k dt (orc_spline_moments)."""
+
+    def __init__(self, samples, t_begin, dt, cut=None, deriv=(np.nan, np.nan), amplitude=1.0):
+        self.y = np.ascontiguousarray(samples, dtype=np.float64)
+        self.m = np.zeros_like(self.y)
+        lib().orc_spline_moments(_p(self.y), ctypes.c_int(self.y.size), ctypes.c_double(dt),
+                                 ctypes.c_double(deriv[0]), ctypes.c_double(deriv[1]), _p(self.m))
+        self.t_begin, self.dt, self.amplitude = t_begin, dt, amplitude
+        self.cut = t_begin + (self.y.size - 1) * dt if cut is None else cut
+
+    def c(self) -> OrcPulse:
+        p = OrcPulse(self.amplitude, self.t_begin, self.cut, 0.0, 0.0)
+        p.kind = PULSE_SPLINE
+        p.spline_y, p.spline_m = _p(self.y), _p(self.m)
+        p.spline_n, p.spline_h = self.y.size, self.dt
+        return p
 
 
 def model(kind: int, hopping=0.0, velocity=0.0, mass=0.0, pol=(1.0, 0.0), *, beta=0.0,

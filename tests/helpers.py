@@ -11,13 +11,25 @@ from oracle import hhg_oracle as O
 SYS_TO_ORC = {0: O.DIRAC2D, 1: O.PIFLUX2D, 2: O.PIFLUX3D, 3: O.HONEYCOMB, 4: O.DIRAC3D}
 
 
+def oracle_pulse(pulse):
+    """The oracle's pulse for a C-ABI pulse descriptor."""
+    if pulse.kind == 1:
+        return O.ContinuousPulse(pulse.amplitude, pulse.phase)
+    if pulse.kind == 2:
+        return O.GaussPulse(pulse.amplitude, pulse.n_cycles, pulse.t_begin, pulse.phase)
+    if pulse.kind == 3:
+        return O.SplinePulse(pulse._samples, pulse.t_begin, pulse.sample_dt, cut=pulse.spline_cut,
+                             deriv=(pulse.deriv_begin, pulse.deriv_end), amplitude=pulse.amplitude)
+    return O.Pulse(pulse.amplitude, pulse.n_cycles, pulse.t_begin, pulse.phase)
+
+
 def oracle_args(sys, pulse, abs_tol, rel_tol, stepper=0, magnus_substeps=1):
     es = pulse.energy_scale
     m = O.model(SYS_TO_ORC[sys.kind], hopping=sys.hopping * es, velocity=sys.velocity * es,
                 mass=sys.mass * es, pol=(sys.pol_x, sys.pol_y), beta=sys.beta / es,
                 fermi_energy=sys.fermi_energy * es, inv_diag_relax=sys.inv_diag_relax * es,
                 inv_offdiag_relax=sys.inv_offdiag_relax * es)
-    p = O.Pulse(pulse.amplitude, pulse.n_cycles, pulse.t_begin, pulse.phase)
+    p = oracle_pulse(pulse)
     tc = O.time_config(pulse.window_begin, pulse.window_end, pulse.n_measurements,
                        pulse.n_subdivisions)
     s = O.solver(abs_tol, rel_tol, stepper=stepper, magnus_substeps=magnus_substeps)

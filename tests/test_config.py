@@ -90,7 +90,6 @@ def test_descriptors_pass_the_abi_checks():
 
 
 @pytest.mark.parametrize("edit,exc", [
-    (("laser_type cosine", "laser_type powerlaw1"), config.UnsupportedConfig),
     (("laser_type cosine", "laser_type expA"), config.UnsupportedConfig),
     (("system_type PiFlux", "system_type Dirac"), config.UnsupportedConfig),
     (("occupations no", "occupations only"), config.UnsupportedConfig),
@@ -101,3 +100,58 @@ def test_descriptors_pass_the_abi_checks():
 def test_refused_configurations(edit, exc):
     with pytest.raises(exc):
         config.from_config(PIFLUX.replace(*edit))
+
+
+def _laser(lt, t0="8", cycles="2"):
+    return config.from_config(PIFLUX.replace("laser_type cosine", f"laser_type {lt}")
+                              .replace("t0_offset 2", f"t0_offset {t0}")
+                              .replace("n_laser_cycles 4", f"n_laser_cycles {cycles}"))
+
+
+def test_laser_types_map_to_pulses():
+    pe, E0 = 5.25, 1.6
+    lattice = math.sqrt(3) * HBAR * 1.5e6 / (pe * 300)
+    A0 = lattice * 1e11 * E0 / pe
+    r = _laser("continuous")
+    assert r.pulse.kind == api.PULSE_CONTINUOUS and r.pulse.amplitude == pytest.approx(A0)
+    assert (r.pulse.window_begin, r.pulse.window_end) == pytest.approx((-2 * math.pi, 2 * math.pi))
+    r = _laser("gauss")
+    assert r.pulse.kind == api.PULSE_GAUSS and r.pulse.t_begin == 8.0
+    assert r.pulse.window_end == pytest.approx(8.0 + 12 * math.pi)
+    r = _laser("quench")
+    p = r.pulse
+    assert p.kind == api.PULSE_SPLINE and p.n_samples == 256 and p.spline_cut == 8.0
+    y = p._samples
+    assert y[63] == 0 and y[64] == pytest.approx(0.5 * A0) and y[100] == pytest.approx(A0) and y[193] == 0
+    assert p.sample_dt == pytest.approx(8.0 / 255) and (p.deriv_begin, p.deriv_end) == (0.0, 0.0)
+    r = _laser("powerlaw1")
+    y = r.pulse._samples
+    assert y[0] == 0 and y[128] == pytest.approx(A0 * 0.5) and math.isnan(r.pulse.deriv_begin)
+
+
+def test_double_lasers_use_the_experimental_photon_energy():
+    r = _laser("dcos", t0="0.5")
+    pe = 5.25 * config.EXP_PHOTON_ENERGY
+    lattice = math.sqrt(3) * HBAR * 1.5e6 / (pe * 300)
+    assert r.lattice_constant == pytest.approx(lattice, rel=1e-15)
+    assert r.system.fermi_energy == pytest.approx(118 / pe)
+    p = r.pulse
+    assert p.n_samples == 1000 and p.spline_cut == pytest.approx(1.5 * 4 * math.pi)
+    # laser A (1.6 E0) plus laser B (0.7 E0) delayed by 0.5 ps
+    shift = 5.25 * (0.5 * config.EXP_PHOTON_ENERGY / (1e12 * HBAR))
+    t = 500 * p.sample_dt
+    a = lattice * 1e11 * 1.6 * 1.6 / pe
+    b = lattice * 1e11 * 0.7 * 1.6 / pe
+
+    def cosl(A, t):
+        return 0.0 if (t <= 0 or t >= 4 * math.pi) else A * 0.5 * (1 - math.cos(t / 2)) * math.sin(t)
+    assert p._samples[500] == pytest.approx(cosl(a, t) + cosl(b, t - shift), rel=1e-12, abs=1e-12)
+    assert _laser("dcosA", t0="0.5").pulse._samples[500] == pytest.approx(cosl(a, t), abs=1e-12)
+
+
+def test_experimental_and_unknown_lasers():
+    with pytest.raises(config.UnsupportedConfig):
+        _laser("expB")
+    with pytest.raises(ValueError):
+        config.from_config(PIFLUX.replace("laser_type cosine", "laser_type dgauss")
+                           .replace("system_type PiFlux", "system_type Honeycomb"))

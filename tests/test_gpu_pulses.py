@@ -1,0 +1,168 @@
+"""Pulse shapes beyond the CosineLaser on the GPU (through the C ABI) against
+the CPU oracle: ContinuousLaser, GaussLaser and the spline lasers
+(Laser.hpp:32-37 with use_spline: PowerLawField, QuenchedField, DoubleLaser),
+same nodes, weights and pulses.  Bar: j(t) relative L2 <= 1e-9 and harmonic
+intensities within 1e-6 above the noise floor for the reference step
+schedule; the step proposers within the 1e-4 harmonic bar.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from higherharmonics_b200 import api, config
+from tests.helpers import harmonic_rel_err, harmonics, oracle_j, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+J_TOL = 1e-9
+H_TOL = 1e-6
+
+
+def _parity(engine, sys, pulse, grid, abs_tol=1e-12, rel_tol=1e-8, rows=None, **okw):
+    if rows is None:
+        rows = api.grid_rows(sys, grid)
+    j, st = engine.current_density(sys, pulse, grid, api.solver(abs_tol, rel_tol, **okw))
+    jr, _ = oracle_j(sys, pulse, rows, abs_tol, rel_tol,
+                     stepper=okw.get("stepper", 0), magnus_substeps=okw.get("magnus_substeps", 1))
+    return rel_l2(j, jr), harmonic_rel_err(harmonics(j, pulse), harmonics(jr, pulse))
+
+
+def _double_cosine(a, b, n_cycles, shift, n=1000):
+    # the reference's DoubleLaser<CosineLaser> samples (DoubleLaser.hpp:42-68)
+    t_max = 1.5 * 2 * math.pi * n_cycles
+    dt = t_max / (n - 1)
+
+    def one(A, t):
+        if t <= 0 or t >= 2 * math.pi * n_cycles:
+            return 0.0
+        return A * (0.5 * (1. - math.cos(t / n_cycles)) * math.sin(t))
+    return [one(a, i * dt) + one(b, i * dt - shift) for i in range(n)], dt, t_max
+
+
+def test_continuous_pulse_parity(engine):
+    sys = api.system(api.SYS_DIRAC2D, velocity=1.0, mass=0.05)
+    pulse = api.continuous_pulse(0.4, 2048, (-2 * math.pi, 2 * math.pi), phase=0.3, energy_scale=10.0)
+    err, herr = _parity(engine, sys, pulse, api.grid_tensor(12, 12, -2, 2, -2, 2), 1e-10, 1e-10)
+    assert err <= J_TOL, err
+    assert herr <= H_TOL, herr
+
+
+def test_gauss_pulse_parity(engine):
+    s = 1 / math.sqrt(2)
+    sys = api.system(api.SYS_PIFLUX2D, hopping=1.0, pol=(s, s))
+    pulse = api.gauss_pulse(0.9, 1, 2048, t_begin=0.5, energy_scale=8.0)
+    err, herr = _parity(engine, sys, pulse, api.grid_tensor(12, 12, -math.pi, math.pi, -math.pi, math.pi))
+    assert err <= J_TOL, err
+    assert herr <= H_TOL, herr
+
+
+@pytest.mark.parametrize("deriv", [(0.0, 0.0), (math.nan, math.nan)])
+def test_double_cosine_spline_parity(engine, deriv):
+    y, dt, t_max = _double_cosine(0.9, 0.4, 2, 3.0)
+    sys = api.system(api.SYS_PIFLUX3D, hopping=1.0)
+    pulse = api.spline_pulse(y, 0.0, dt, 2048, (0.0, t_max), cut=t_max, deriv=deriv)
+    err, herr = _parity(engine, sys, pulse, api.grid_piflux3d_ref(2, 1))
+    assert err <= J_TOL, err
+    assert herr <= H_TOL, herr
+
+
+def test_spline_cut_inside_the_window(engine):
+    # A = 0 after the cut (Laser.hpp:35) although the spline is nonzero there
+    # and the window continues
+    y, dt, t_max = _double_cosine(0.8, 0.0, 2, 0.0)
+    sys = api.system(api.SYS_DIRAC2D, velocity=1.0, mass=0.05)
+    cut = 2.6 * math.pi
+    pulse = api.spline_pulse(y, 0.0, dt, 2048, (0.0, t_max), cut=cut, deriv=(0.0, 0.0),
+                             energy_scale=10.0)
+    err, herr = _parity(engine, sys, pulse, api.grid_tensor(12, 12, -2, 2, -2, 2), 1e-10, 1e-10)
+    assert err <= J_TOL, err
+
+
+def test_steep_spline_refused(engine):
+    # QuenchedField's template (QuenchedField.cpp:15-29): the field turns on
+    # within two knots, which one interpolant per measurement interval cannot
+    # follow to 2^-36; the call says so instead of losing accuracy
+    n = 256
+    y = [0.0 if (i < 64 or i > 192) else (0.35 if i in (64, 192) else 0.7) for i in range(n)]
+    pulse = api.spline_pulse(y, 0.0, 6 * math.pi / (n - 1), 2048, (0.0, 6 * math.pi),
+                             deriv=(0.0, 0.0), energy_scale=10.0)
+    with pytest.raises(api.HHGError) as ei:
+        engine.current_density(api.system(api.SYS_DIRAC2D, velocity=1.0, mass=0.05), pulse,
+                               api.grid_tensor(4, 4, -2, 2, -2, 2), api.solver())
+    assert ei.value.status == api.UNSUPPORTED and "spline" in str(ei.value)
+
+
+def test_spline_pulse_lockstep_meets_harmonic_bar(engine):
+    from higherharmonics_b200.analysis import (default_max_order, harmonic_intensities,
+                                               harmonic_rel_err as herr_fn)
+    y, dt, t_max = _double_cosine(1.0, 0.5, 2, 2.0)
+    s = 1 / math.sqrt(2)
+    sys = api.system(api.SYS_PIFLUX2D, hopping=1.0, pol=(s, s))
+    pulse = api.spline_pulse(y, 0.0, dt, 2048, (0.0, t_max), cut=t_max, deriv=(0.0, 0.0),
+                             energy_scale=10.0)
+    grid = api.grid_tensor(32, 32, -math.pi, math.pi, -math.pi, math.pi)
+    jr, st_ref = engine.current_density(sys, pulse, grid, api.solver())
+    b = engine.spectrum(jr, pulse.n_measurements, pulse.window_begin, pulse.window_end)
+    mo = default_max_order(b[0])
+    for opts in (api.solver(proposer=api.PROPOSER_LOCKSTEP),
+                 api.solver(1e-8, 1e-6, precision=api.PREC_MIXED, proposer=api.PROPOSER_LOCKSTEP)):
+        j, st = engine.current_density(sys, pulse, grid, opts)
+        a = engine.spectrum(j, pulse.n_measurements, pulse.window_begin, pulse.window_end)
+        assert herr_fn(harmonic_intensities(*a, mo), harmonic_intensities(*b, mo)) <= 1e-4
+        assert rel_l2(j, jr) <= 1e-4
+
+
+def test_dirac_magnus_with_gauss_pulse(engine):
+    rng = np.random.default_rng(2)
+    rows = []
+    for _ in range(48):
+        kz, kap = rng.uniform(-1.2, 1.2), rng.uniform(0.1, 1.2)
+        mk = math.hypot(kz, kap)
+        rows.append([kz, kap, mk, kz * kap / mk, 0.0, 0.0, -1.0, 0.0])
+    rows = np.array(rows)
+    grid, keep = api.grid_explicit(rows)
+    pulse = api.gauss_pulse(0.5, 1, 2048)
+    err, _ = _parity(engine, api.system(api.SYS_DIRAC3D), pulse, grid, rows=rows,
+                     stepper=api.STEPPER_DIRAC_MAGNUS)
+    assert err <= 1e-12, err
+
+
+@pytest.mark.parametrize("laser", ["dcos", "dgaussA", "powerlaw1", "gauss", "continuous"])
+def test_reference_laser_types_from_config(engine, laser):
+    # a small PiFlux run of each laser_type the config reader hands to the device
+    txt = f"""
+    T 0
+    E_F 0
+    v_F 2e4
+    band_width 10
+    field_amplitude 0.05
+    photon_energy 1
+    diagonal_relaxation_time -1
+    laser_type {laser}
+    n_laser_cycles 1
+    t0_offset {0.02 if laser == 'dcos' else 6}
+    system_type PiFlux
+    """
+    run = config.from_config(txt, grid=api.grid_piflux3d_ref(1, 1))  # 1024 intervals per cycle
+    err, herr = _parity(engine, run.system, run.pulse, run.grid)
+    assert err <= J_TOL, (laser, err)
+
+
+def test_spline_refused_by_the_allocation_free_entry_point():
+    import ctypes
+
+    import torch
+    lib = api.load_library()
+    y = np.linspace(0, 1, 16)
+    pulse = api.spline_pulse(y, 0.0, 0.1, 64, (0.0, 1.5))
+    sys = api.system(api.SYS_DIRAC2D, velocity=1.0)
+    opts = api.solver()
+    rows = torch.zeros(8, dtype=torch.float64, device="cuda")
+    j = torch.zeros(65, dtype=torch.float64, device="cuda")
+    err = ctypes.create_string_buffer(256)
+    st = lib.hhg_gpu_current_density_noalloc(ctypes.byref(sys), ctypes.byref(pulse),
+                                             ctypes.c_void_p(rows.data_ptr()), 1,
+                                             ctypes.byref(opts), ctypes.c_void_p(j.data_ptr()),
+                                             None, None, err, 256)
+    assert st == api.UNSUPPORTED and b"spline" in err.value
