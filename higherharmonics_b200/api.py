@@ -21,7 +21,9 @@ OK, BAD_CONFIG, STEP_LIMIT, NONFINITE, CUDA_ERROR, UNSUPPORTED = range(6)
 STATUS_NAMES = {0: "HHG_OK", 1: "HHG_BAD_CONFIG", 2: "HHG_STEP_LIMIT", 3: "HHG_NONFINITE",
                 4: "HHG_CUDA_ERROR", 5: "HHG_UNSUPPORTED"}
 SYS_DIRAC2D, SYS_PIFLUX2D, SYS_PIFLUX3D, SYS_HONEYCOMB, SYS_DIRAC3D = range(5)
-GRID_TENSOR_GL, GRID_RHOMBIC_GL, GRID_PIFLUX3D_REF, GRID_HONEYCOMB_HEX_REF, GRID_EXPLICIT = range(5)
+(GRID_TENSOR_GL, GRID_RHOMBIC_GL, GRID_PIFLUX3D_REF, GRID_HONEYCOMB_HEX_REF, GRID_EXPLICIT,
+ GRID_PIFLUX3D_OCCUPATION, GRID_PIFLUX3D_CUBE) = range(7)
+KOUT_BLOCH, KOUT_OCCUPATIONS = 0, 1
 STEPPER_RKF78, STEPPER_MAGNUS4, STEPPER_DIRAC_MAGNUS = 0, 1, 2
 PREC_FP64, PREC_MIXED = 0, 1
 PROPOSER_NONE, PROPOSER_CARRY, PROPOSER_LEARNED, PROPOSER_LOCKSTEP = 0, 1, 2, 3
@@ -36,6 +38,7 @@ EXPORTED = [
     "hhg_gpu_current_density_noalloc",
     "hhg_learned_collect", "hhg_default_train_opts", "hhg_mlp_init", "hhg_mlp_train",
     "hhg_mlp_gradients", "hhg_mlp_predict", "hhg_plan_execute_graph", "hhg_plan_autotune", "hhg_measure_fp32_peak",
+    "hhg_gpu_k_resolved", "hhg_gpu_split_current", "hhg_gpu_spectrum_welch", "hhg_pulse_values",
 ]
 TUNE_MAX = 16
 ABI_VERSION = 3
@@ -186,6 +189,17 @@ def load_library() -> ctypes.CDLL:
             ctypes.POINTER(SolverOpts), ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(Stats),
             ctypes.c_char_p, ctypes.c_size_t]
         L.hhg_default_solver_opts.argtypes = [ctypes.POINTER(SolverOpts)]
+        L.hhg_gpu_k_resolved.argtypes = [ctypes.c_void_p, ctypes.POINTER(SystemDesc),
+                                         ctypes.POINTER(PulseDesc), ctypes.POINTER(GridDesc),
+                                         ctypes.POINTER(SolverOpts), ctypes.c_int, _D,
+                                         ctypes.POINTER(Stats)]
+        L.hhg_gpu_split_current.argtypes = [ctypes.c_void_p, ctypes.POINTER(SystemDesc),
+                                            ctypes.POINTER(PulseDesc), ctypes.POINTER(GridDesc),
+                                            ctypes.POINTER(SolverOpts), ctypes.c_double, _D, _D,
+                                            ctypes.POINTER(Stats)]
+        L.hhg_gpu_spectrum_welch.argtypes = [ctypes.c_void_p, _D, ctypes.c_int, ctypes.c_double,
+                                             ctypes.c_double, _D, _D, _D]
+        L.hhg_pulse_values.argtypes = [ctypes.POINTER(PulseDesc), _D, ctypes.c_int64, _D]
         _F = ctypes.POINTER(ctypes.c_float)
         L.hhg_learned_collect.argtypes = [ctypes.c_void_p, ctypes.POINTER(SystemDesc),
                                           ctypes.POINTER(PulseDesc), ctypes.c_int,
@@ -296,6 +310,26 @@ def grid_piflux3d_ref(z_range=32, n_coarse=4) -> GridDesc:
 
 def grid_honeycomb_hex_ref(n_k=64) -> GridDesc:
     return GridDesc(GRID_HONEYCOMB_HEX_REF, n_k, 0, 0, 0, 0, 0, 0, None, 0)
+
+
+def grid_piflux3d_occupation(n: int) -> GridDesc:
+    """PiFlux::compute_occupation_numbers' N x N grid (PiFlux.cpp:909-953)."""
+    return GridDesc(GRID_PIFLUX3D_OCCUPATION, n, 0, 0, 0, 0, 0, 0, None, 0)
+
+
+def grid_piflux3d_cube(n: int) -> GridDesc:
+    """PiFlux::current_per_energy's N^3 grid and its -z mirror (PiFlux.cpp:955-1035)."""
+    return GridDesc(GRID_PIFLUX3D_CUBE, n, 0, 0, 0, 0, 0, 0, None, 0)
+
+
+def pulse_values(pulse: PulseDesc, t) -> np.ndarray:
+    """A(t) of a pulse as the engine stages it (host)."""
+    t = np.ascontiguousarray(np.atleast_1d(t), dtype=np.float64)
+    out = np.zeros_like(t)
+    st = load_library().hhg_pulse_values(ctypes.byref(pulse), _ptr(t), t.size, _ptr(out))
+    if st != OK:
+        raise HHGError(st, "hhg_pulse_values")
+    return out
 
 
 def grid_explicit(rows: np.ndarray) -> tuple[GridDesc, np.ndarray]:
@@ -414,6 +448,43 @@ class Engine:
         fr = np.zeros(n_fft)
         self._check(self.lib.hhg_gpu_spectrum(self.ctx, _ptr(j), n_measurements, t_begin, t_end,
                                               _ptr(re), _ptr(im), _ptr(fr)), "hhg_gpu_spectrum")
+        return fr, re, im
+
+    def k_resolved(self, sys: SystemDesc, pulse: PulseDesc, grid: GridDesc,
+                   opts: SolverOpts | None = None, kind: int = KOUT_BLOCH):
+        """Every trajectory at every sample: (n_measurements + 1, n_k, 3) Bloch
+        vectors or (.., 2) band occupations (hhg_gpu_k_resolved)."""
+        n_k = int(grid_rows(sys, grid).shape[0])
+        w = 3 if kind == KOUT_BLOCH else 2
+        out = np.zeros((pulse.n_measurements + 1, n_k, w))
+        st = Stats()
+        self._check(self.lib.hhg_gpu_k_resolved(self.ctx, ctypes.byref(sys), ctypes.byref(pulse),
+                                                ctypes.byref(grid),
+                                                ctypes.byref(opts) if opts else None, kind,
+                                                _ptr(out), ctypes.byref(st)), "hhg_gpu_k_resolved")
+        return out, st
+
+    def split_current(self, sys: SystemDesc, pulse: PulseDesc, grid: GridDesc,
+                      opts: SolverOpts | None = None, energy_cut: float = 0.5 * math.sqrt(3.0)):
+        """j(t) split at the instantaneous energy cut (hhg_gpu_split_current)."""
+        lo = np.zeros(pulse.n_measurements + 1)
+        hi = np.zeros(pulse.n_measurements + 1)
+        st = Stats()
+        self._check(self.lib.hhg_gpu_split_current(self.ctx, ctypes.byref(sys), ctypes.byref(pulse),
+                                                   ctypes.byref(grid),
+                                                   ctypes.byref(opts) if opts else None,
+                                                   energy_cut, _ptr(lo), _ptr(hi), ctypes.byref(st)),
+                    "hhg_gpu_split_current")
+        return lo, hi, st
+
+    def spectrum_welch(self, j: np.ndarray, n_measurements: int, t_begin: float, t_end: float):
+        """Welch-windowed N-point FFT of a continuous-laser current (hhg_gpu_spectrum_welch)."""
+        j = np.ascontiguousarray(j, dtype=np.float64)
+        n_fft = n_measurements // 2 + 1
+        re, im, fr = np.zeros(n_fft), np.zeros(n_fft), np.zeros(n_fft)
+        self._check(self.lib.hhg_gpu_spectrum_welch(self.ctx, _ptr(j), n_measurements, t_begin, t_end,
+                                                    _ptr(re), _ptr(im), _ptr(fr)),
+                    "hhg_gpu_spectrum_welch")
         return fr, re, im
 
     def plan(self, sys: SystemDesc, pulses, grid: GridDesc, opts: SolverOpts | None = None):

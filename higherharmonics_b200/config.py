@@ -32,10 +32,12 @@ system is multiplied by the experimental one for the exp and double lasers
 (Dispatcher.cpp:10-19).  The experimental lasers exp/expA/expB need the
 measured field of the reference's source, which this package does not carry:
 they raise UnsupportedConfig (api.spline_pulse takes such samples).  The
-Dirac system's adaptive kappa quadrature is not built either.  Keys the path
-does not read (data_dir, n_z) are accepted and ignored; the run modes
-occupations/split_current != "no" and debug_data != "no" raise
-UnsupportedConfig because they produce other outputs than j(t).
+Dirac system's adaptive kappa quadrature is not built either.  The
+occupation and split-current run modes are in higherharmonics_b200.runmodes;
+requesting either shortens the double / Gaussian / experimental laser windows to
+0.75 t_end for every mode, as the dispatcher's reduced_duration does
+(PiFluxDispatcher.cpp:45).  debug_data != "no" raises UnsupportedConfig (the
+debug traces are not built); data_dir and n_z are read by the run modes only.
 """
 from __future__ import annotations
 
@@ -110,9 +112,9 @@ def from_config(cfg: dict | str, *, grid: api.GridDesc | None = None,
     if system_type in ("Dirac", "ModifiedPiFlux"):
         raise UnsupportedConfig(f"system_type {system_type}: the Dirac current density needs the "
                                 "reference's adaptive kappa quadrature; ModifiedPiFlux is not built")
-    for mode in ("occupations", "split_current", "debug_data"):
-        if cfg.get(mode, "no") != "no":
-            raise UnsupportedConfig(f"{mode} = {cfg[mode]}: only the current density j(t) is built")
+    if cfg.get("debug_data", "no") != "no":
+        raise UnsupportedConfig(f"debug_data = {cfg['debug_data']}: the debug traces are not built")
+    reduced = cfg.get("occupations", "no") != "no" or cfg.get("split_current", "no") != "no"
     laser_type = cfg.get("laser_type", "")
     known = {"cosine", "continuous", "gauss", "quench", "exp", "expA", "expB"} | set(DOUBLE_LASERS)
     if not (laser_type in known or laser_type.startswith("powerlaw")) or \
@@ -150,7 +152,7 @@ def from_config(cfg: dict | str, *, grid: api.GridDesc | None = None,
                       inv_diag_relax=inv_d if relax else 0.0,
                       inv_offdiag_relax=inv_o if relax else 0.0)
     n = n_measurements or n_cycles * MEASUREMENTS_PER_CYCLE
-    pulse = make_pulse(laser_type, lattice, E0, pe_in, n_cycles, t0_offset, n)
+    pulse = make_pulse(laser_type, lattice, E0, pe_in, n_cycles, t0_offset, n, reduced)
     return Run(system_type, sys_, pulse, g, api.solver(1e-12, 1e-8), lattice)
 
 
@@ -173,9 +175,11 @@ def _gauss(A0: float, n: float, t_begin: float, t: float) -> float:
 
 
 def make_pulse(laser_type: str, ratio: float, E0: float, pe_in: float, n_cycles: int,
-               t0_offset: float, n: int) -> api.PulseDesc:
+               t0_offset: float, n: int, reduced: bool = False) -> api.PulseDesc:
     """The pulse and TimeIntegrationConfig of one laser_type, as the PiFlux /
-    Honeycomb dispatchers build them from the config's photon_energy pe_in."""
+    Honeycomb dispatchers build them from the config's photon_energy pe_in
+    (reduced: the occupation / split-current runs' 0.75 t_end windows)."""
+    cut = 0.75 if reduced else 1.0
     pe = pe_in * EXP_PHOTON_ENERGY if laser_type in DOUBLE_LASERS else pe_in
     if laser_type == "cosine":
         t_begin = math.pi * t0_offset
@@ -188,7 +192,7 @@ def make_pulse(laser_type: str, ratio: float, E0: float, pe_in: float, n_cycles:
     if laser_type == "gauss":
         t_begin = t0_offset  # GaussLaser(.., n_laser_cycles, t0_offset)
         return api.gauss_pulse(_amplitude(ratio, E0, pe), n_cycles, n, t_begin=t_begin,
-                               window=(t_begin, t_begin + 2 * math.pi * 3.0 * n_cycles))
+                               window=(t_begin, cut * (t_begin + 2 * math.pi * 3.0 * n_cycles)))
     if laser_type == "quench" or laser_type.startswith("powerlaw"):
         # a 256-sample spline template over [0, duration], duration = t0_offset
         A0, t_end, N = _amplitude(ratio, E0, pe), t0_offset, 256
@@ -219,4 +223,4 @@ def make_pulse(laser_type: str, ratio: float, E0: float, pe_in: float, n_cycles:
         t = i * dt
         a, b = one(aA, n_cycles, 0.0, t), one(aB, n_cycles, 0.0, t - shift + 0.0)
         y.append(a + b if active == "both" else (a if active == "A" else b))
-    return api.spline_pulse(y, 0.0, dt, n, (0.0, t_max), cut=t_max, deriv=(0.0, 0.0))
+    return api.spline_pulse(y, 0.0, dt, n, (0.0, cut * t_max), cut=t_max, deriv=(0.0, 0.0))

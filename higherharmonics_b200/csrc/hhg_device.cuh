@@ -197,6 +197,11 @@ struct KParams {
     float *hist;
     unsigned long long *hist_count;
     long long hist_cap;
+    // output modes (OUT 1: current split at energy_cut, channel 1 rows at
+    // part + chan_stride; OUT 2/3: k-resolved samples into kout)
+    double energy_cut;
+    long long chan_stride;
+    double *kout;
 };
 constexpr int kHistFields = 12;
 
@@ -707,6 +712,43 @@ template <typename R> struct ModelState<DIRAC3D_RELAX, R> : ModelState<DIRAC3D, 
     }
 };
 
+// ---------------------------------------------------------------------------
+// k-resolved observables of the PiFlux models at a sample, from the sample
+// record r = [A(t_i), cos A, sin A] and the momentum cosines:
+// piflux_energy = |d(k - A)| / 2t = dispersion(k.shift_z(A))
+// (PiFlux::current_per_energy, PiFlux.cpp:998-999);
+// piflux_occupations = the reference's compute_occupations (PiFlux.cpp:227-235)
+// at the shifted momentum u (RESCUE_TRAFO as update_equilibrium_state,
+// PiFlux.cpp:252-258): diagonal_sigma's third component is S.u/|u| and its
+// norm is |S|, so lower = sqrt((|S| - S.u/|u|)/2), upper = sqrt((|S| + S.u/|u|)/2).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double piflux_energy(const double *r, double cx, double cy, double cz,
+                                                double sz) {
+    const double uz = cz * r[1] + sz * r[2];
+    return sqrt(cx * cx + cy * cy + uz * uz);
+}
+
+__device__ __forceinline__ void piflux_occupations(const double *r, double cx, double cy, double cz,
+                                                   double sz, const double *S, double *o) {
+    double ux = cx, uz = cz * r[1] + sz * r[2];
+    if (ref_is_zero_dev(cx) && ref_is_zero_dev(cy) && uz < 0.0) {
+        ux = fabs(uz) * 1e-4;
+        uz *= (1. - 0.5 * 1e-4 * 1e-4);
+    }
+    const double d = sqrt(ux * ux + cy * cy + uz * uz);
+    const double a = (S[0] * ux + S[1] * cy + S[2] * uz) / d;
+    const double n = sqrt(S[0] * S[0] + S[1] * S[1] + S[2] * S[2]);
+    o[0] = sqrt(0.5 * fmax(n - a, 0.0));
+    o[1] = sqrt(0.5 * fmax(n + a, 0.0));
+}
+
+// Momentum cosines of a PiFlux k row (cos kx, cos ky, cos kz, sin kz).
+__device__ __forceinline__ void piflux_cosines(const double *row, double *c) {
+    c[0] = cos(row[0]);
+    c[1] = cos(row[1]);
+    sincos(row[2], &c[3], &c[2]);
+}
+
 // Right-hand side call: models with kStart also read the step's start state x.
 template <int M, typename R, class V>
 __device__ __forceinline__ void model_rhs(const ModelState<M, R> &ms, const V *f, const R *S,
@@ -1072,7 +1114,14 @@ __host__ __device__ constexpr int mlp_smem_bytes() {
 }
 constexpr double kCoarsen = 1.0 / 600.0;
 
-template <int M, int D, typename R, int STEPPER, int PROPOSER>
+// OUT 0: the Brillouin-zone sum of the current (one partial row per item);
+// OUT 1: the same split by the instantaneous energy |d(k - A(t_i))| < energy_cut
+//   into two channels (PiFlux::current_per_energy, PiFlux.cpp:955-1035);
+// OUT 2: every trajectory's Bloch vector at every sample, kout[i][k][3];
+// OUT 3: every trajectory's band occupations at every sample, kout[i][k][2]
+//   (PiFlux::evolve_occupation_numbers, PiFlux.cpp:222-318).
+// OUT 1-3 are built for the PiFlux models only.
+template <int M, int D, typename R, int STEPPER, int PROPOSER, int OUT = 0>
 __global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integrate_kernel(const KParams P) {
     constexpr int NF = Traits<M>::NF;
     constexpr bool kDyadic = PROPOSER == 2 || PROPOSER == 3;
@@ -1137,6 +1186,9 @@ __global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integ
             double carry_dt = dt0;
             int level = 0;      // warp-uniform dyadic level carried across intervals
             double held = 0.0;  // lane (i & 31) holds the warp sum of sample i
+            double held2 = 0.0; // ... and of its second channel (OUT 1)
+            double kc[4];       // momentum cosines (OUT 1-3)
+            if constexpr (OUT != 0) piflux_cosines(row, kc);
 
             for (int i = 0; i <= N; ++i) {
                 const double *rec = pd.s0rec;
@@ -1276,16 +1328,55 @@ __global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integ
                     }
                 }
                 // sample i at t_i = i * measure_every + t_begin (PiFlux.cpp:834-836)
-                const double c = dead ? 0.0 : w * ms.vertex(rec, S);
-                const double sum = warp_sum(c);
-                if (lane == (i & 31)) held = sum;
-                if ((i & 31) == 31 || i == N) {
-                    const int base = i & ~31;
-                    if (base + lane <= N) {
-                        if (sub == 0)
-                            prow[base + lane] = held;
-                        else
-                            prow[base + lane] += held;
+                if constexpr (OUT == 0) {
+                    const double c = dead ? 0.0 : w * ms.vertex(rec, S);
+                    const double sum = warp_sum(c);
+                    if (lane == (i & 31)) held = sum;
+                    if ((i & 31) == 31 || i == N) {
+                        const int base = i & ~31;
+                        if (base + lane <= N) {
+                            if (sub == 0)
+                                prow[base + lane] = held;
+                            else
+                                prow[base + lane] += held;
+                        }
+                    }
+                } else if constexpr (OUT == 1) {
+                    double c_lo = 0.0, c_hi = 0.0;
+                    if (!dead) {
+                        const double c = w * ms.vertex(rec, S);
+                        if (piflux_energy(rec, kc[0], kc[1], kc[2], kc[3]) < P.energy_cut) c_lo = c;
+                        else c_hi = c;
+                    }
+                    const double s_lo = warp_sum(c_lo), s_hi = warp_sum(c_hi);
+                    if (lane == (i & 31)) {
+                        held = s_lo;
+                        held2 = s_hi;
+                    }
+                    if ((i & 31) == 31 || i == N) {
+                        const int base = i & ~31;
+                        if (base + lane <= N) {
+                            double *p2 = prow + P.chan_stride;
+                            if (sub == 0) {
+                                prow[base + lane] = held;
+                                p2[base + lane] = held2;
+                            } else {
+                                prow[base + lane] += held;
+                                p2[base + lane] += held2;
+                            }
+                        }
+                    }
+                } else if (valid) {
+                    constexpr int W = OUT == 2 ? 3 : 2;
+                    double *o = P.kout + ((size_t)i * P.n_k + q) * W;
+                    if (dead) {
+                        for (int c = 0; c < W; ++c) o[c] = __longlong_as_double(0x7ff8000000000000LL);
+                    } else if constexpr (OUT == 2) {
+                        o[0] = S[0];
+                        o[1] = S[1];
+                        o[2] = S[2];
+                    } else {
+                        piflux_occupations(rec, kc[0], kc[1], kc[2], kc[3], S, o);
                     }
                 }
             }
@@ -1553,6 +1644,24 @@ static __global__ void trapezoid_correct_kernel(const double2 *__restrict__ F, i
     re[i] = delta_t * (mr * f.x - mi * f.y + cr);
     im[i] = delta_t * (mr * f.y + mi * f.x + ci);
     freq[i] = fr;
+}
+
+// Welch window of the continuous-laser spectrum (WelchWindow.hpp:11-13,
+// applied at hhg.cpp:264-267): x_i = (1 - (i - N/2)^2 / (N^2/4)) j_i, i < N.
+static __global__ void welch_kernel(const double *__restrict__ j, int n, double *__restrict__ x) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) x[i] = (1. - (i - 0.5 * n) * (i - 0.5 * n) / (0.25 * n * n)) * j[i];
+}
+
+// r2c output -> real part, imaginary part, frequencies i / delta_t
+// (hhg.cpp:268-273).
+static __global__ void split_spectrum_kernel(const double2 *__restrict__ F, int n_fft, double delta_t,
+                                             double *re, double *im, double *freq) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_fft) return;
+    re[i] = F[i].x;
+    im[i] = F[i].y;
+    freq[i] = i / delta_t;
 }
 
 // FP64 issue-rate probe: 8 independent FMA chains per thread.

@@ -71,6 +71,12 @@ struct hhg_plan {
     // CUDA graph of one execution (integration + reduction [+ spectra])
     cudaGraphExec_t gexec = nullptr;
     int graph_spec = -1;
+    // output mode (bz_integrate_kernel's OUT): 1 split current (two partial
+    // channels, j of 2 j_len), 2/3 k-resolved samples into d_kout
+    int out_mode = 0;
+    double energy_cut = 0.0;
+    double *d_kout = nullptr;
+    long long kout_len = 0;
 };
 
 namespace hhg {
@@ -263,8 +269,34 @@ int64_t grid_count(const hhg_grid_desc &g) {
         return 4 * (int64_t)g.n1 * g.n1;
     case HHG_GRID_EXPLICIT:
         return g.n_rows;
+    case HHG_GRID_PIFLUX3D_OCCUPATION:
+        return (int64_t)g.n1 * g.n1;
+    case HHG_GRID_PIFLUX3D_CUBE:
+        return 2 * (int64_t)g.n1 * g.n1 * g.n1;
     }
     return -1;
+}
+
+// A PiFlux row of a momentum_type built from (x, y, z) with the reference's
+// construction-time rescue (PiFlux.cpp:934-938, 983-988): when cos x and cos y
+// vanish (is_zero) and cos z < 0, cos x becomes |cos z| 1e-4 and cos z is
+// scaled by 1 - 0.5e-8.  Unlike the continuum-limit grid the rescued cos x
+// stays in the momentum that is evolved, so the row carries it as kx =
+// acos(|cos z| 1e-4); the initial state uses the rescued cosines.
+void piflux_rescued_row(const hhg_system_desc &s, double x, double y, double z, double w, double *o) {
+    double cx = cos(x), cy = cos(y), cz = cos(z);
+    double kx = x;
+    if (ref_is_zero(cx) && ref_is_zero(cy) && cz < 0.0) {
+        cx = std::fabs(cz) * 1e-4;
+        cz *= (1. - 0.5 * 1e-4 * 1e-4);
+        kx = std::acos(cx);
+    }
+    o[0] = kx;
+    o[1] = y;
+    o[2] = z;
+    o[3] = w;
+    piflux_ic(s, cx, cy, cz, o + 4);
+    o[7] = 0.0;
 }
 
 // Row builders; see the oracle for the same restatements.
@@ -375,6 +407,33 @@ void build_rows(const hhg_system_desc &s, const hhg_grid_desc &g, double *out) {
     case HHG_GRID_EXPLICIT:
         std::memcpy(out, g.rows, sizeof(double) * 8 * (size_t)g.n_rows);
         break;
+    case HHG_GRID_PIFLUX3D_OCCUPATION: {
+        // PiFlux::compute_occupation_numbers (PiFlux.cpp:909-953): i = x N + z,
+        // k = (x dx, pi/2, dz z)
+        const int N = g.n1;
+        const double dx = kPi / N, dz = kPi / N;
+        for (int i = 0; i < N * N; ++i) {
+            const int x = i / N, z = i % N;
+            piflux_rescued_row(s, x * dx, 0.5 * kPi, dz * z, 1.0, out + 8 * r++);
+        }
+        break;
+    }
+    case HHG_GRID_PIFLUX3D_CUBE: {
+        // PiFlux::current_per_energy (PiFlux.cpp:955-1035): i = z N^2 + y N + x,
+        // k = (x, y, z) dxy and its -z mirror (k.invert()), both weighted 1/N^3
+        const int N = g.n1;
+        const double d = kPi / N;
+        const double w = 1.0 / ((double)N * N * N);
+        for (int64_t i = 0; i < (int64_t)N * N * N; ++i) {
+            const int z = (int)(i / ((int64_t)N * N)), y = (int)((i / N) % N), x = (int)(i % N);
+            piflux_rescued_row(s, x * d, y * d, d * z, w, out + 8 * r);
+            double *m = out + 8 * (r + 1);
+            std::memcpy(m, out + 8 * r, 8 * sizeof(double));
+            m[2] = -m[2];
+            r += 2;
+        }
+        break;
+    }
     }
 }
 
@@ -416,6 +475,12 @@ hhg_status check_grid(hhg_ctx *ctx, const hhg_grid_desc *g) {
         break;
     case HHG_GRID_EXPLICIT:
         if (!g->rows || g->n_rows < 1) return set_err(ctx, HHG_BAD_CONFIG, "explicit grid without rows");
+        break;
+    case HHG_GRID_PIFLUX3D_OCCUPATION:
+        if (g->n1 < 1 || g->n1 > 16384) return set_err(ctx, HHG_BAD_CONFIG, "occupation grid N out of range");
+        break;
+    case HHG_GRID_PIFLUX3D_CUBE:
+        if (g->n1 < 1 || g->n1 > 1024) return set_err(ctx, HHG_BAD_CONFIG, "cube grid N out of range");
         break;
     default:
         return set_err(ctx, HHG_BAD_CONFIG, "grid type not recognized");
@@ -1173,6 +1238,7 @@ void hhg_plan_destroy(hhg_plan *pl) {
     cudaFree(pl->d_mlp);
     cudaFree(pl->d_hist);
     cudaFree(pl->d_hist_count);
+    cudaFree(pl->d_kout);
     if (pl->gexec) cudaGraphExecDestroy(pl->gexec);
     delete pl;
 }
@@ -1214,6 +1280,10 @@ hhg_status enqueue_integration(hhg_plan *pl, cudaStream_t s, bool events) {
     lr.kp.hist = pl->d_hist;
     lr.kp.hist_count = pl->d_hist_count;
     lr.kp.hist_cap = pl->hist_cap;
+    lr.kp.energy_cut = pl->energy_cut;
+    lr.kp.chan_stride = pl->part_len;
+    lr.kp.kout = pl->d_kout;
+    lr.out_mode = pl->out_mode;
     lr.degree = pl->degree;
     lr.precision = pl->opts.precision;
     lr.stepper = pl->opts.stepper;
@@ -1225,9 +1295,13 @@ hhg_status enqueue_integration(hhg_plan *pl, cudaStream_t s, bool events) {
     hhg_status st = launch_variant(pl, lr);
     if (st != HHG_OK) return st;
     if (events) HHG_CUDA(ctx, cudaEventRecord(ctx->ev[1], s));
-    hhg::reduce_partials_kernel<<<(unsigned)hhg::reduce_blocks(pl->j_len), hhg::kReduceThreads, 0, s>>>(
-        pl->d_pulses, pl->n_pulses, pl->d_part, pl->d_j, pl->j_len);
-    HHG_CUDA(ctx, cudaGetLastError());
+    // one reduction per output channel; k-resolved samples need none
+    const int channels = pl->out_mode == 0 ? 1 : (pl->out_mode == 1 ? 2 : 0);
+    for (int c = 0; c < channels; ++c) {
+        hhg::reduce_partials_kernel<<<(unsigned)hhg::reduce_blocks(pl->j_len), hhg::kReduceThreads, 0, s>>>(
+            pl->d_pulses, pl->n_pulses, pl->d_part + c * pl->part_len, pl->d_j + c * pl->j_len, pl->j_len);
+        HHG_CUDA(ctx, cudaGetLastError());
+    }
     if (events) {
         HHG_CUDA(ctx, cudaEventRecord(ctx->ev[2], s));
         pl->timed = true;
@@ -1804,6 +1878,172 @@ hhg_status hhg_plan_autotune(hhg_plan *pl, int reps, hhg_tune_report *report) {
             report->kernel_ms[c] = ms[c];
         }
     }
+    return HHG_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// k-resolved samples and the energy-split current (the reference's occupation
+// tracking and split-current run modes)
+// ---------------------------------------------------------------------------
+namespace {
+// A plan of one pulse switched to output mode `mode` (bz_integrate_kernel's
+// OUT): buffers for the mode and the persistent grid of that kernel variant.
+hhg_status output_plan(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_pulse_desc *pulse,
+                       const hhg_grid_desc *grid, const hhg_solver_opts *opts, int mode,
+                       hhg_plan **out) {
+    *out = nullptr;
+    if (!sys || !pulse || !grid) return set_err(ctx, HHG_BAD_CONFIG, "null descriptor");
+    if (sys->kind != HHG_SYS_PIFLUX3D)
+        return set_err(ctx, HHG_UNSUPPORTED, "k-resolved and split-current outputs are PiFlux-3D's");
+    hhg_solver_opts o;
+    hhg_default_solver_opts(&o);
+    if (opts) o = *opts;
+    if (o.stepper != HHG_STEPPER_RKF78 || o.precision != HHG_PREC_FP64 ||
+        (o.proposer != HHG_PROPOSER_NONE && o.proposer != HHG_PROPOSER_CARRY))
+        return set_err(ctx, HHG_UNSUPPORTED,
+                       "k-resolved and split-current outputs run FP64 RKF78 with the NONE or CARRY proposer");
+    hhg_plan *pl = nullptr;
+    hhg_status st = hhg_plan_create(ctx, sys, pulse, 1, grid, &o, &pl);
+    if (st != HHG_OK) return st;
+    auto fail = [&](const char *what, cudaError_t e) {
+        hhg_plan_destroy(pl);
+        return set_err(ctx, HHG_CUDA_ERROR, std::string(what) + ": " + cudaGetErrorString(e));
+    };
+    cudaError_t e;
+    pl->out_mode = mode;
+    if (mode == 1) {  // a second channel of partial rows and of j
+        cudaFree(pl->d_part);
+        cudaFree(pl->d_j);
+        pl->d_part = nullptr;
+        pl->d_j = nullptr;
+        if ((e = cudaMalloc(&pl->d_part, 2 * pl->part_len * sizeof(double))) != cudaSuccess) return fail("alloc partials", e);
+        if ((e = cudaMalloc(&pl->d_j, 2 * pl->j_len * sizeof(double))) != cudaSuccess) return fail("alloc j", e);
+    } else {
+        const int width = mode == 2 ? 3 : 2;
+        pl->kout_len = (long long)(pulse->n_measurements + 1) * pl->n_k * width;
+        if ((e = cudaMalloc(&pl->d_kout, pl->kout_len * sizeof(double))) != cudaSuccess)
+            return fail("alloc k-resolved output", e);
+    }
+    int occ = 0;
+    hhg::LaunchReq lr{};
+    lr.degree = pl->degree;
+    lr.precision = o.precision;
+    lr.stepper = o.stepper;
+    lr.proposer = kernel_proposer(o.proposer);
+    lr.out_mode = mode;
+    lr.grid = 0;
+    lr.occupancy_out = &occ;
+    if ((st = launch_variant(pl, lr)) != HHG_OK) {
+        hhg_plan_destroy(pl);
+        return st;
+    }
+    const long long need = (pl->n_items + hhg::kWarpsPerBlock - 1) / hhg::kWarpsPerBlock;
+    pl->grid = (int)std::max(1LL, std::min((long long)std::max(occ, 1) * ctx->sm_count, need));
+    *out = pl;
+    return HHG_OK;
+}
+}  // namespace
+
+extern "C" {
+
+hhg_status hhg_gpu_k_resolved(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_pulse_desc *pulse,
+                              const hhg_grid_desc *grid, const hhg_solver_opts *opts, int kind,
+                              double *out, hhg_stats *stats) {
+    if (!ctx || !out) return set_err(ctx, HHG_BAD_CONFIG, "null context or output");
+    if (kind != HHG_KOUT_BLOCH && kind != HHG_KOUT_OCCUPATIONS)
+        return set_err(ctx, HHG_BAD_CONFIG, "unknown k-resolved observable");
+    hhg_plan *pl = nullptr;
+    hhg_status st = output_plan(ctx, sys, pulse, grid, opts, kind == HHG_KOUT_BLOCH ? 2 : 3, &pl);
+    if (st != HHG_OK) return st;
+    st = hhg_plan_execute_async(pl, nullptr);
+    if (st == HHG_OK) st = hhg_plan_fetch(pl, nullptr, stats);
+    if (st == HHG_OK || st == HHG_STEP_LIMIT || st == HHG_NONFINITE) {
+        const cudaError_t e = cudaMemcpy(out, pl->d_kout, pl->kout_len * sizeof(double), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) st = set_err(ctx, HHG_CUDA_ERROR, std::string("fetch k-resolved output: ") + cudaGetErrorString(e));
+    }
+    hhg_plan_destroy(pl);
+    return st;
+}
+
+hhg_status hhg_gpu_split_current(hhg_ctx *ctx, const hhg_system_desc *sys,
+                                 const hhg_pulse_desc *pulse, const hhg_grid_desc *grid,
+                                 const hhg_solver_opts *opts, double energy_cut, double *j_low,
+                                 double *j_high, hhg_stats *stats) {
+    if (!ctx || !j_low || !j_high) return set_err(ctx, HHG_BAD_CONFIG, "null context or output");
+    if (!std::isfinite(energy_cut)) return set_err(ctx, HHG_BAD_CONFIG, "non-finite energy cut");
+    hhg_plan *pl = nullptr;
+    hhg_status st = output_plan(ctx, sys, pulse, grid, opts, 1, &pl);
+    if (st != HHG_OK) return st;
+    pl->energy_cut = energy_cut;
+    st = hhg_plan_execute_async(pl, nullptr);
+    if (st == HHG_OK) st = hhg_plan_fetch(pl, j_low, stats);
+    if (st == HHG_OK || st == HHG_STEP_LIMIT || st == HHG_NONFINITE) {
+        const cudaError_t e =
+            cudaMemcpy(j_high, pl->d_j + pl->j_len, pl->j_len * sizeof(double), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) st = set_err(ctx, HHG_CUDA_ERROR, std::string("fetch j: ") + cudaGetErrorString(e));
+    }
+    hhg_plan_destroy(pl);
+    return st;
+}
+
+}  // extern "C"
+
+extern "C" {
+
+hhg_status hhg_gpu_spectrum_welch(hhg_ctx *ctx, const double *j, int n_measurements, double t_begin,
+                                  double t_end, double *re_out, double *im_out, double *freq_out) {
+    if (!ctx || !j || !re_out || !im_out || !freq_out || n_measurements < 2)
+        return set_err(ctx, HHG_BAD_CONFIG, "bad spectrum arguments");
+    if (!(t_end > t_begin)) return set_err(ctx, HHG_BAD_CONFIG, "empty time window");
+    if (n_measurements > (1 << 28)) return set_err(ctx, HHG_BAD_CONFIG, "spectrum too long");
+    HHG_CUDA(ctx, cudaSetDevice(ctx->device));
+    const int n = n_measurements, n_fft = n / 2 + 1;
+    cudaStream_t s = ctx->stream;
+    if (ctx->x_cap < (size_t)(2 * n)) {
+        cudaFree(ctx->d_x);
+        ctx->d_x = nullptr;
+        HHG_CUDA(ctx, cudaMalloc(&ctx->d_x, sizeof(double) * 2 * n));
+        ctx->x_cap = 2 * n;
+    }
+    if (ctx->f_cap < (size_t)n_fft) {
+        cudaFree(ctx->d_F);
+        cudaFree(ctx->d_out);
+        ctx->d_F = nullptr;
+        ctx->d_out = nullptr;
+        HHG_CUDA(ctx, cudaMalloc(&ctx->d_F, sizeof(double2) * n_fft));
+        HHG_CUDA(ctx, cudaMalloc(&ctx->d_out, sizeof(double) * 3 * n_fft));
+        ctx->f_cap = n_fft;
+    }
+    cufftHandle plan;
+    hhg_status st = get_fft_plan(ctx, n, &plan);
+    if (st != HHG_OK) return st;
+    if (cufftSetStream(plan, s) != CUFFT_SUCCESS) return set_err(ctx, HHG_CUDA_ERROR, "cufftSetStream failed");
+    // the first n samples (the reference's N-point FFT reads N of its N + 1)
+    double *d_j = ctx->d_x + n;
+    HHG_CUDA(ctx, cudaMemcpyAsync(d_j, j, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    hhg::welch_kernel<<<(n + 255) / 256, 256, 0, s>>>(d_j, n, ctx->d_x);
+    HHG_CUDA(ctx, cudaGetLastError());
+    if (cufftExecD2Z(plan, ctx->d_x, (cufftDoubleComplex *)ctx->d_F) != CUFFT_SUCCESS)
+        return set_err(ctx, HHG_CUDA_ERROR, "cufftExecD2Z failed");
+    hhg::split_spectrum_kernel<<<(n_fft + 255) / 256, 256, 0, s>>>(
+        ctx->d_F, n_fft, (t_end - t_begin) / n_measurements, ctx->d_out, ctx->d_out + n_fft,
+        ctx->d_out + 2 * n_fft);
+    HHG_CUDA(ctx, cudaGetLastError());
+    HHG_CUDA(ctx, cudaMemcpyAsync(re_out, ctx->d_out, sizeof(double) * n_fft, cudaMemcpyDeviceToHost, s));
+    HHG_CUDA(ctx, cudaMemcpyAsync(im_out, ctx->d_out + n_fft, sizeof(double) * n_fft, cudaMemcpyDeviceToHost, s));
+    HHG_CUDA(ctx, cudaMemcpyAsync(freq_out, ctx->d_out + 2 * n_fft, sizeof(double) * n_fft, cudaMemcpyDeviceToHost, s));
+    HHG_CUDA(ctx, cudaStreamSynchronize(s));
+    return HHG_OK;
+}
+
+hhg_status hhg_pulse_values(const hhg_pulse_desc *pulse, const double *t, int64_t n, double *A) {
+    if (!pulse || (n > 0 && (!t || !A)) || n < 0) return HHG_BAD_CONFIG;
+    const hhg_status st = check_pulse(nullptr, *pulse);
+    if (st != HHG_OK) return st;
+    const HostPulse hp(*pulse);
+    for (int64_t i = 0; i < n; ++i) A[i] = hp.value(t[i]);
     return HHG_OK;
 }
 

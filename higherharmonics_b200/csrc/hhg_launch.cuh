@@ -17,6 +17,7 @@ struct LaunchReq {
     int grid;       // CTAs; 0 = query occupancy only
     cudaStream_t stream;
     int *occupancy_out;  // blocks per SM for the selected variant (if non-null)
+    int out_mode = 0;    // bz_integrate_kernel's OUT (1-3: PiFlux models, FP64, proposer 0/1)
 };
 
 struct StageReq {
@@ -33,9 +34,9 @@ struct StageReq {
     const double *gl30 = nullptr;  // layout 3: 30 nodes on [0, 1], then 30 weights (device)
 };
 
-template <int M, int D, typename R, int ST, int PR>
+template <int M, int D, typename R, int ST, int PR, int OUT = 0>
 cudaError_t launch_one(const LaunchReq &r) {
-    auto kern = bz_integrate_kernel<M, D, R, ST, PR>;
+    auto kern = bz_integrate_kernel<M, D, R, ST, PR, OUT>;
     const int dyn = PR == 3 ? mlp_smem_bytes() : 0;
     if (r.occupancy_out) {
         cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(r.occupancy_out, kern, kBlockThreads, dyn);
@@ -46,8 +47,28 @@ cudaError_t launch_one(const LaunchReq &r) {
     return cudaGetLastError();
 }
 
+// k-resolved and split-current outputs (OUT 1-3): PiFlux models, FP64 RKF78,
+// the reference schedule or the carried step
+template <int M, int D>
+cudaError_t launch_out(const LaunchReq &r) {
+    if constexpr (base_model(M) == PIFLUX3D) {
+        if (r.stepper != 0 || r.precision != 0 || (r.proposer != 0 && r.proposer != 1))
+            return cudaErrorNotSupported;
+        const bool carry = r.proposer == 1;
+        switch (r.out_mode) {
+        case 1: return carry ? launch_one<M, D, double, 0, 1, 1>(r) : launch_one<M, D, double, 0, 0, 1>(r);
+        case 2: return carry ? launch_one<M, D, double, 0, 1, 2>(r) : launch_one<M, D, double, 0, 0, 2>(r);
+        case 3: return carry ? launch_one<M, D, double, 0, 1, 3>(r) : launch_one<M, D, double, 0, 0, 3>(r);
+        }
+        return cudaErrorInvalidValue;
+    } else {
+        return cudaErrorNotSupported;
+    }
+}
+
 template <int M, int D>
 cudaError_t launch_deg(const LaunchReq &r) {
+    if (r.out_mode != 0) return launch_out<M, D>(r);
     if constexpr (Traits<M>::kRelax) {
         // relaxation right-hand sides: FP64 controlled RKF78 only
         if (r.stepper != 0 || r.precision != 0) return cudaErrorNotSupported;

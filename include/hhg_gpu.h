@@ -142,7 +142,12 @@ typedef enum hhg_grid_kind {
     HHG_GRID_RHOMBIC_GL = 1,       /* n1 x n2 GL in fractional coords of the honeycomb BZ */
     HHG_GRID_PIFLUX3D_REF = 2,     /* PiFlux::current_density_continuum_limit grid, n1 = z_range, n2 = N_coarse */
     HHG_GRID_HONEYCOMB_HEX_REF = 3,/* Honeycomb::compute_current_density grid, n1 = N_k */
-    HHG_GRID_EXPLICIT = 4          /* caller rows: kx, ky, kz, weight, S0x, S0y, S0z, 0 */
+    HHG_GRID_EXPLICIT = 4,         /* caller rows: kx, ky, kz, weight, S0x, S0y, S0z, 0 */
+    HHG_GRID_PIFLUX3D_OCCUPATION = 5, /* PiFlux::compute_occupation_numbers grid (PiFlux.cpp:909-953):
+                                         k = (x pi/N, pi/2, z pi/N), x, z < N = n1, row x N + z */
+    HHG_GRID_PIFLUX3D_CUBE = 6     /* PiFlux::current_per_energy grid (PiFlux.cpp:955-1035): k =
+                                      (x, y, +-z) pi/N, x, y, z < N = n1, weight 1/N^3, rows
+                                      2 (z N^2 + y N + x) + (0: +z, 1: -z) */
 } hhg_grid_kind;
 
 typedef struct hhg_grid_desc {
@@ -247,6 +252,13 @@ typedef struct hhg_stats {
 
 typedef struct hhg_ctx hhg_ctx;
 typedef struct hhg_plan hhg_plan;
+
+/* k-resolved observables (hhg_gpu_k_resolved). */
+typedef enum hhg_kresolved {
+    HHG_KOUT_BLOCH = 0,       /* the Bloch vector S: 3 doubles */
+    HHG_KOUT_OCCUPATIONS = 1  /* lower and upper band amplitudes of S at k - A(t_i):
+                                 sqrt((|S| -+ S.d_hat)/2), 2 doubles (PiFlux.cpp:227-235) */
+} hhg_kresolved;
 
 /* Library / context management. */
 int hhg_abi_version(void);
@@ -410,6 +422,42 @@ hhg_status hhg_mlp_gradients(hhg_ctx *ctx, const float *records, int64_t n_recor
  * forward pass (tcgen05). */
 hhg_status hhg_mlp_predict(hhg_ctx *ctx, const float *records, int64_t n_records,
                            const hhg_mlp *net, int path, float *level_out);
+
+/* k-resolved samples of one pulse: out[(i n_k + k) width + c] for every sample i
+ * <= n_measurements and k-point k (host memory, (n_measurements + 1) n_k width
+ * doubles), width 3 (HHG_KOUT_BLOCH) or 2 (HHG_KOUT_OCCUPATIONS).  The
+ * reference's occupation tracking (PiFlux::evolve_occupation_numbers and
+ * compute_occupation_numbers, PiFlux.cpp:222-318 and 909-953; the occupations
+ * mode of hhg.cpp:120-168) is HHG_KOUT_OCCUPATIONS on
+ * HHG_GRID_PIFLUX3D_OCCUPATION, with the z index of sample i shifted by
+ * round(A(t_i) / dz) on the host.  PiFlux-3D only, FP64 RKF78, proposer NONE
+ * or CARRY; a trajectory that failed reads NaN. */
+hhg_status hhg_gpu_k_resolved(hhg_ctx *ctx, const hhg_system_desc *sys,
+                              const hhg_pulse_desc *pulse, const hhg_grid_desc *grid,
+                              const hhg_solver_opts *opts, int kind, double *out,
+                              hhg_stats *stats);
+
+/* The current split by the instantaneous band energy |d(k - A(t_i))| / 2t <
+ * energy_cut (PiFlux::current_per_energy, PiFlux.cpp:955-1035; the
+ * split_current mode of hhg.cpp:170-219, cut sqrt(3)/2): j_low and j_high,
+ * n_measurements + 1 doubles each (host).  PiFlux-3D only, FP64 RKF78,
+ * proposer NONE or CARRY. */
+hhg_status hhg_gpu_split_current(hhg_ctx *ctx, const hhg_system_desc *sys,
+                                 const hhg_pulse_desc *pulse, const hhg_grid_desc *grid,
+                                 const hhg_solver_opts *opts, double energy_cut, double *j_low,
+                                 double *j_high, hhg_stats *stats);
+
+/* The continuous laser's spectrum (hhg.cpp:264-275): the first n_measurements
+ * samples of j times the Welch window 1 - (i - N/2)^2 / (N^2/4)
+ * (WelchWindow.hpp:11-13), an N-point r2c FFT (Fourier/FFT.cpp:8-42), and the
+ * frequencies i / measure_every; N/2 + 1 values each (host). */
+hhg_status hhg_gpu_spectrum_welch(hhg_ctx *ctx, const double *j, int n_measurements,
+                                  double t_begin, double t_end, double *re_out, double *im_out,
+                                  double *freq_out);
+
+/* A(t) of a pulse at n times (host only; Laser::laser_function as the engine
+ * stages it, e.g. for the reference's laser_function output, hhg.cpp:301-305). */
+hhg_status hhg_pulse_values(const hhg_pulse_desc *pulse, const double *t, int64_t n, double *A);
 
 #ifdef __cplusplus
 }

@@ -137,6 +137,21 @@ int orc_current_density(const orc_model *m, const orc_pulse *p, const orc_time_c
 int orc_step_history(const orc_model *m, const orc_pulse *p, const orc_time_config *tc,
                      const orc_solver *s, const double *krow, int cap, double *hist);
 
+/* k-resolved samples: kind 0 the Bloch vector (3 doubles), kind 1 the
+ * reference's compute_occupations (PiFlux.cpp:227-235) at the shifted momentum
+ * of update_equilibrium_state (PiFlux.cpp:252-258): (lower, upper).  out[(i n_k
+ * + k) width + c].  PiFlux-3D rows. */
+int orc_k_resolved(const orc_model *m, const orc_pulse *p, const orc_time_config *tc,
+                   const orc_solver *s, int n_k, const double *ktab, int kind, double *out,
+                   int n_threads);
+
+/* PiFlux::current_per_energy (PiFlux.cpp:955-1035): j split by the
+ * instantaneous energy dispersion(k.shift_z(A(t_i))) < cut; weights from the
+ * rows.  Fixed reduction order as orc_current_density. */
+int orc_split_current(const orc_model *m, const orc_pulse *p, const orc_time_config *tc,
+                      const orc_solver *s, int n_k, const double *ktab, double cut,
+                      double *j_low, double *j_high, int n_threads);
+
 /* Reference Laser::magnus_coefficients (sources/HHG/Laser/Laser.cpp:40-55). */
 void orc_magnus_coefficients(const orc_pulse *p, double delta_t, double t0, double *coeffs4);
 

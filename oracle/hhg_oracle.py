@@ -260,6 +260,30 @@ def current_density(m, p: Pulse, tc, s, ktab: np.ndarray, threads=0, fast=False)
     return j, st, rc
 
 
+def k_resolved(m, p, tc, s, ktab: np.ndarray, kind: int, threads=0):
+    """orc_k_resolved: (n_measurements + 1, n_k, 3 | 2) samples and status."""
+    ktab = np.ascontiguousarray(ktab, dtype=np.float64)
+    w = 3 if kind == 0 else 2
+    out = np.zeros((tc.n_measurements + 1, ktab.shape[0], w))
+    pc = p.c()
+    rc = lib().orc_k_resolved(ctypes.byref(m), ctypes.byref(pc), ctypes.byref(tc), ctypes.byref(s),
+                              ctypes.c_int(ktab.shape[0]), _p(ktab), ctypes.c_int(kind), _p(out),
+                              ctypes.c_int(threads))
+    return out, rc
+
+
+def split_current(m, p, tc, s, ktab: np.ndarray, cut: float, threads=0):
+    """orc_split_current: (j_low, j_high, status)."""
+    ktab = np.ascontiguousarray(ktab, dtype=np.float64)
+    lo = np.zeros(tc.n_measurements + 1)
+    hi = np.zeros(tc.n_measurements + 1)
+    pc = p.c()
+    rc = lib().orc_split_current(ctypes.byref(m), ctypes.byref(pc), ctypes.byref(tc), ctypes.byref(s),
+                                 ctypes.c_int(ktab.shape[0]), _p(ktab), ctypes.c_double(cut), _p(lo),
+                                 _p(hi), ctypes.c_int(threads))
+    return lo, hi, rc
+
+
 def magnus_coefficients(p: Pulse, delta_t, t0) -> np.ndarray:
     out = np.zeros(4)
     pc = p.c()

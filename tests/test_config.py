@@ -92,8 +92,7 @@ def test_descriptors_pass_the_abi_checks():
 @pytest.mark.parametrize("edit,exc", [
     (("laser_type cosine", "laser_type expA"), config.UnsupportedConfig),
     (("system_type PiFlux", "system_type Dirac"), config.UnsupportedConfig),
-    (("occupations no", "occupations only"), config.UnsupportedConfig),
-    (("split_current no", "split_current yes"), config.UnsupportedConfig),
+    (("debug_data no", "debug_data yes"), config.UnsupportedConfig),
     (("system_type PiFlux", "system_type Graphene"), ValueError),
     (("E_F 118\n", ""), ValueError),
 ])
@@ -155,3 +154,17 @@ def test_experimental_and_unknown_lasers():
     with pytest.raises(ValueError):
         config.from_config(PIFLUX.replace("laser_type cosine", "laser_type dgauss")
                            .replace("system_type PiFlux", "system_type Honeycomb"))
+
+
+def test_run_modes_shorten_the_double_laser_window():
+    # reduced_duration (PiFluxDispatcher.cpp:45): 0.75 t_end for every mode
+    full = _laser("dcos", t0="0.5").pulse
+    cfg = PIFLUX.replace("laser_type cosine", "laser_type dcos").replace("t0_offset 2", "t0_offset 0.5") \
+        .replace("n_laser_cycles 4", "n_laser_cycles 2").replace("occupations no", "occupations yes")
+    red = config.from_config(cfg).pulse
+    assert red.window_end == pytest.approx(0.75 * full.window_end)
+    assert red.spline_cut == full.spline_cut
+    # the cosine laser's window is not shortened
+    cos_full = config.from_config(PIFLUX).pulse
+    cos_red = config.from_config(PIFLUX.replace("split_current no", "split_current yes")).pulse
+    assert cos_red.window_end == cos_full.window_end

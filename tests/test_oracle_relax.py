@@ -155,3 +155,19 @@ def test_abi_rejects_thermal_variant_models():
                              grid) == api.BAD_CONFIG
     assert _grid_rows_status(api.system(api.SYS_PIFLUX3D, hopping=1.0, beta=1.0, inv_diag_relax=2.0),
                              grid) == api.OK
+
+
+def test_host_pulse_values_match_the_oracle():
+    # hhg_pulse_values (host) and the oracle's A(t) for every pulse kind
+    t = np.linspace(-1.0, 30.0, 211)
+    cases = [(api.cosine_pulse(0.7, 2, 64, t_begin=1.0, phase=0.2), O.Pulse(0.7, 2, 1.0, 0.2)),
+             (api.continuous_pulse(0.4, 64, (-3, 3), phase=0.1), O.ContinuousPulse(0.4, 0.1)),
+             (api.gauss_pulse(0.9, 1, 64, t_begin=0.5, phase=0.3), O.GaussPulse(0.9, 1, 0.5, 0.3))]
+    y = np.sin(np.linspace(0, 3, 40)) ** 2
+    cases.append((api.spline_pulse(y, 0.5, 0.6, 64, (0.5, 20.0), cut=20.0, deriv=(0.0, math.nan),
+                                   amplitude=1.5),
+                  O.SplinePulse(y, 0.5, 0.6, cut=20.0, deriv=(0.0, math.nan), amplitude=1.5)))
+    for desc, op in cases:
+        a = api.pulse_values(desc, t)
+        b = O.laser(op, t)
+        assert np.max(np.abs(a - b)) <= 1e-13 * max(1.0, np.abs(b).max()), desc.kind
