@@ -76,12 +76,19 @@ template <int M> struct Traits {
     static constexpr bool kRelax = false;
     static constexpr bool kStart = false;
     static constexpr int kMinBlocks = kMinBlocksPerSM;
+    static constexpr bool kPacked = false;  // FP32 right-hand side on packed (x, y) pairs
 };
 template <> struct Traits<DIRAC2D> : Traits<-1> { static constexpr int NF = 1; };
 template <> struct Traits<DIRAC3D> : Traits<-1> { static constexpr int NF = 1; };
 template <> struct Traits<PIFLUX3D> : Traits<-1> { static constexpr int NF = 2; };
-template <> struct Traits<PIFLUX2D> : Traits<-1> { static constexpr int NF = 4; };
-template <> struct Traits<PIFLUX2D_SYM> : Traits<-1> { static constexpr int NF = 2; };
+template <> struct Traits<PIFLUX2D> : Traits<-1> {
+    static constexpr int NF = 4;
+    static constexpr bool kPacked = true;
+};
+template <> struct Traits<PIFLUX2D_SYM> : Traits<-1> {
+    static constexpr int NF = 2;
+    static constexpr bool kPacked = true;
+};
 template <> struct Traits<HONEYCOMB> : Traits<-1> { static constexpr int NF = 6; };
 template <> struct Traits<HONEYCOMB_X> : Traits<-1> { static constexpr int NF = 4; };
 template <> struct Traits<PIFLUX3D_RELAX> {
@@ -438,6 +445,7 @@ template <typename R, bool SYM> struct PiFlux2DState {
     static constexpr int Y = SYM ? 0 : 2;
     typename N::V pcx, psx, pcy, psy;
     double cx, sx, cy, sy, px, py;
+    float2 pc_hi, pc_lo, ps_hi, ps_lo;  // FP32: (x, y) pairs of the float-pair constants
     __device__ __forceinline__ void init(const PulseDev &p, const double *row) {
         const double pf = p.mp[0];
         sincos(row[0], &sx, &cx);
@@ -446,6 +454,12 @@ template <typename R, bool SYM> struct PiFlux2DState {
         psx = N::mk(pf * sx);
         pcy = N::mk(pf * cy);
         psy = N::mk(pf * sy);
+        if constexpr (sizeof(R) == sizeof(float)) {
+            pc_hi = make_float2(pcx.x, pcy.x);
+            pc_lo = make_float2(pcx.y, pcy.y);
+            ps_hi = make_float2(psx.x, psy.x);
+            ps_lo = make_float2(psx.y, psy.y);
+        }
         px = p.mp[2];
         py = p.mp[3];
     }
@@ -455,6 +469,20 @@ template <typename R, bool SYM> struct PiFlux2DState {
         dS[0] = m1 * S[2];
         dS[1] = -(m0 * S[2]);
         dS[2] = m0 * S[1] - m1 * S[0];
+    }
+    // FP32 on packed pairs: (m0, m1) = Num<float>::dot2 of both projections in
+    // one set of paired FMAs, then dS = (m1 Sz, -m0 Sz, m0 Sy - m1 Sx)
+    __device__ __forceinline__ void rhs2(const float2 *f, float2 s_xy, float s_z, float2 &d_xy,
+                                         float &d_z) const {
+        const float2 bhi = make_float2(f[0].x, f[Y].x), blo = make_float2(f[0].y, f[Y].y);
+        const float2 dhi = make_float2(f[1].x, f[Y + 1].x), dlo = make_float2(f[1].y, f[Y + 1].y);
+        float2 lo = __fmul2_rn(pc_hi, blo);
+        lo = __ffma2_rn(pc_lo, bhi, lo);
+        lo = __ffma2_rn(ps_hi, dlo, lo);
+        lo = __ffma2_rn(ps_lo, dhi, lo);
+        const float2 m = __ffma2_rn(pc_hi, bhi, __ffma2_rn(ps_hi, dhi, lo));
+        d_xy = __fmul2_rn(make_float2(m.y, -m.x), make_float2(s_z, s_z));
+        d_z = fmaf(m.x, s_xy.y, -(m.y * s_xy.x));
     }
     __device__ __forceinline__ double vertex(const double *r, const double *S) const {
         // px sin(kx - px A) S_x + py sin(ky - py A) S_y
@@ -758,6 +786,132 @@ __device__ __forceinline__ void model_rhs(const ModelState<M, R> &ms, const V *f
 }
 
 // ---------------------------------------------------------------------------
+// The mixed-precision (FP32) attempt on packed pairs: the x and y components
+// of every stage, stage sum, solution and error increment share one paired
+// FP32 instruction (fma.rn.f32x2 and friends, sm_100), the z component runs
+// scalar.  The kernel is issue-bound in FP32, so halving the instructions of
+// the stage arithmetic counts directly.  Same tableau, same grouping of the
+// sums as rkf78_attempt.
+// ---------------------------------------------------------------------------
+template <int M, class V>
+__device__ __forceinline__ void rhs_packed(const ModelState<M, float> &ms, const V *f, float2 s_xy,
+                                           float s_z, const double *x, float2 &d_xy, float &d_z) {
+    if constexpr (Traits<M>::kPacked) {
+        ms.rhs2(f, s_xy, s_z, d_xy, d_z);
+    } else {
+        const float S[3] = {s_xy.x, s_xy.y, s_z};
+        float d[3];
+        model_rhs(ms, f, S, x, d);
+        d_xy = make_float2(d[0], d[1]);
+        d_z = d[2];
+    }
+}
+
+__device__ __forceinline__ float2 pk(double c) { return make_float2(float(c), float(c)); }
+__device__ __forceinline__ float2 pmul(double c, float2 v) { return __fmul2_rn(pk(c), v); }
+__device__ __forceinline__ float2 pfma(double c, float2 v, float2 acc) { return __ffma2_rn(pk(c), v, acc); }
+__device__ __forceinline__ float2 padd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+
+template <int M, int NF, class Eval>
+__device__ __forceinline__ void rkf78_attempt_packed(const ModelState<M, float> &ms, const Eval &ev,
+                                                     double t, double h, const double *x,
+                                                     double *xn, double *e, double *k0d) {
+    float2 k2[13];
+    float kz[13];
+    typename Num<float>::V f[NF];
+    const float2 x2 = make_float2(float(x[0]), float(x[1]));
+    const float xz = float(x[2]);
+    const float hr = float(h);
+    const float2 h2 = make_float2(hr, hr);
+    ev(0, t, f);
+    rhs_packed(ms, f, x2, xz, x, k2[0], kz[0]);
+    typename Num<float>::V f0[Eval::kReuse ? NF : 1], f3[Eval::kReuse ? NF : 1],
+        f10[Eval::kReuse ? NF : 1];
+    if constexpr (Eval::kReuse) {
+#pragma unroll
+        for (int n = 0; n < NF; ++n) f0[n] = f[n];
+    }
+#define HHG_PSTAGE(s, SUM2, SUMZ)                                                   \
+    {                                                                               \
+        const float2 xt2 = __ffma2_rn(h2, (SUM2), x2);                              \
+        const float xtz = xz + hr * (SUMZ);                                         \
+        if constexpr (Eval::kReuse && (s == 7 || s == 11 || s == 12)) {             \
+            _Pragma("unroll") for (int n = 0; n < NF; ++n)                          \
+                f[n] = (s == 7) ? f3[n] : (s == 11) ? f0[n] : f10[n];               \
+        } else {                                                                    \
+            ev(s, t + rk_c(s) * h, f);                                              \
+        }                                                                           \
+        if constexpr (Eval::kReuse && (s == 3 || s == 10)) {                        \
+            _Pragma("unroll") for (int n = 0; n < NF; ++n) {                        \
+                if (s == 3) f3[n] = f[n]; else f10[n] = f[n];                       \
+            }                                                                       \
+        }                                                                           \
+        rhs_packed(ms, f, xt2, xtz, x, k2[s], kz[s]);                               \
+    }
+#define Z(c, j) (float(c) * kz[j])
+    HHG_PSTAGE(1, pmul(2.0 / 27.0, k2[0]), Z(2.0 / 27.0, 0))
+    HHG_PSTAGE(2, pfma(1.0 / 12.0, k2[1], pmul(1.0 / 36.0, k2[0])),
+               Z(1.0 / 36.0, 0) + Z(1.0 / 12.0, 1))
+    HHG_PSTAGE(3, pfma(1.0 / 8.0, k2[2], pmul(1.0 / 24.0, k2[0])),
+               Z(1.0 / 24.0, 0) + Z(1.0 / 8.0, 2))
+    HHG_PSTAGE(4, padd(pmul(5.0 / 12.0, k2[0]), pfma(25.0 / 16.0, k2[3], pmul(-25.0 / 16.0, k2[2]))),
+               Z(5.0 / 12.0, 0) + (Z(-25.0 / 16.0, 2) + Z(25.0 / 16.0, 3)))
+    HHG_PSTAGE(5, padd(pmul(1.0 / 20.0, k2[0]), pfma(1.0 / 5.0, k2[4], pmul(1.0 / 4.0, k2[3]))),
+               Z(1.0 / 20.0, 0) + (Z(1.0 / 4.0, 3) + Z(1.0 / 5.0, 4)))
+    HHG_PSTAGE(6, padd(pfma(125.0 / 108.0, k2[3], pmul(-25.0 / 108.0, k2[0])),
+                       pfma(125.0 / 54.0, k2[5], pmul(-65.0 / 27.0, k2[4]))),
+               (Z(-25.0 / 108.0, 0) + Z(125.0 / 108.0, 3)) + (Z(-65.0 / 27.0, 4) + Z(125.0 / 54.0, 5)))
+    HHG_PSTAGE(7, padd(pfma(61.0 / 225.0, k2[4], pmul(31.0 / 300.0, k2[0])),
+                       pfma(13.0 / 900.0, k2[6], pmul(-2.0 / 9.0, k2[5]))),
+               (Z(31.0 / 300.0, 0) + Z(61.0 / 225.0, 4)) + (Z(-2.0 / 9.0, 5) + Z(13.0 / 900.0, 6)))
+    HHG_PSTAGE(8, padd(pfma(704.0 / 45.0, k2[4], pfma(-53.0 / 6.0, k2[3], pmul(2.0, k2[0]))),
+                       pfma(3.0, k2[7], pfma(67.0 / 90.0, k2[6], pmul(-107.0 / 9.0, k2[5])))),
+               (Z(2.0, 0) + Z(-53.0 / 6.0, 3) + Z(704.0 / 45.0, 4)) +
+                   (Z(-107.0 / 9.0, 5) + Z(67.0 / 90.0, 6) + Z(3.0, 7)))
+    HHG_PSTAGE(9, padd(pfma(311.0 / 54.0, k2[5], pfma(-976.0 / 135.0, k2[4],
+                                                      pfma(23.0 / 108.0, k2[3], pmul(-91.0 / 108.0, k2[0])))),
+                       pfma(-1.0 / 12.0, k2[8], pfma(17.0 / 6.0, k2[7], pmul(-19.0 / 60.0, k2[6])))),
+               (Z(-91.0 / 108.0, 0) + Z(23.0 / 108.0, 3) + Z(-976.0 / 135.0, 4) + Z(311.0 / 54.0, 5)) +
+                   (Z(-19.0 / 60.0, 6) + Z(17.0 / 6.0, 7) + Z(-1.0 / 12.0, 8)))
+    HHG_PSTAGE(10, padd(pfma(-301.0 / 82.0, k2[5], pfma(4496.0 / 1025.0, k2[4],
+                                                        pfma(-341.0 / 164.0, k2[3], pmul(2383.0 / 4100.0, k2[0])))),
+                        pfma(18.0 / 41.0, k2[9], pfma(45.0 / 164.0, k2[8],
+                                                      pfma(45.0 / 82.0, k2[7], pmul(2133.0 / 4100.0, k2[6]))))),
+               (Z(2383.0 / 4100.0, 0) + Z(-341.0 / 164.0, 3) + Z(4496.0 / 1025.0, 4) + Z(-301.0 / 82.0, 5)) +
+                   (Z(2133.0 / 4100.0, 6) + Z(45.0 / 82.0, 7) + Z(45.0 / 164.0, 8) + Z(18.0 / 41.0, 9)))
+    HHG_PSTAGE(11, padd(pfma(-3.0 / 205.0, k2[6], pfma(-6.0 / 41.0, k2[5], pmul(3.0 / 205.0, k2[0]))),
+                        pfma(6.0 / 41.0, k2[9], pfma(3.0 / 41.0, k2[8], pmul(-3.0 / 41.0, k2[7])))),
+               (Z(3.0 / 205.0, 0) + Z(-6.0 / 41.0, 5) + Z(-3.0 / 205.0, 6)) +
+                   (Z(-3.0 / 41.0, 7) + Z(3.0 / 41.0, 8) + Z(6.0 / 41.0, 9)))
+    HHG_PSTAGE(12, padd(pfma(-289.0 / 82.0, k2[5], pfma(4496.0 / 1025.0, k2[4],
+                                                        pfma(-341.0 / 164.0, k2[3], pmul(-1777.0 / 4100.0, k2[0])))),
+                        padd(pfma(12.0 / 41.0, k2[9], pfma(33.0 / 164.0, k2[8],
+                                                           pfma(51.0 / 82.0, k2[7], pmul(2193.0 / 4100.0, k2[6])))),
+                             k2[11])),
+               (Z(-1777.0 / 4100.0, 0) + Z(-341.0 / 164.0, 3) + Z(4496.0 / 1025.0, 4) + Z(-289.0 / 82.0, 5)) +
+                   (Z(2193.0 / 4100.0, 6) + Z(51.0 / 82.0, 7) + Z(33.0 / 164.0, 8) + Z(12.0 / 41.0, 9) + kz[11]))
+#undef HHG_PSTAGE
+    const float2 inc2 = pfma(41.0 / 840.0, padd(k2[11], k2[12]),
+                             pfma(9.0 / 280.0, padd(k2[8], k2[9]),
+                                  pfma(9.0 / 35.0, padd(k2[6], k2[7]), pmul(34.0 / 105.0, k2[5]))));
+    const float incz = Z(34.0 / 105.0, 5) + float(9.0 / 35.0) * (kz[6] + kz[7]) +
+                       float(9.0 / 280.0) * (kz[8] + kz[9]) + float(41.0 / 840.0) * (kz[11] + kz[12]);
+#undef Z
+    const float2 de2 = pfma(-1.0, padd(k2[0], k2[10]), padd(k2[11], k2[12]));
+    const float dez = (kz[11] + kz[12]) - (kz[0] + kz[10]);
+    xn[0] = x[0] + h * double(inc2.x);
+    xn[1] = x[1] + h * double(inc2.y);
+    xn[2] = x[2] + h * double(incz);
+    const double eh = 41.0 / 840.0 * h;
+    e[0] = eh * double(de2.x);
+    e[1] = eh * double(de2.y);
+    e[2] = eh * double(dez);
+    k0d[0] = double(k2[0].x);
+    k0d[1] = double(k2[0].y);
+    k0d[2] = double(kz[0]);
+}
+
+// ---------------------------------------------------------------------------
 // One attempted Fehlberg 7(8) step (E. Fehlberg, NASA TR R-287, 1968):
 // 13 stages, the 8th-order solution propagated, error = b8 - b7 =
 // 41/840 (k12 + k13 - k1 - k11).  Stage sums are written out with the
@@ -768,6 +922,9 @@ template <int M, int NF, typename R, class Eval>
 __device__ __forceinline__ void rkf78_attempt(const ModelState<M, R> &ms, const Eval &ev,
                                               double t, double h, const double *x, double *xn,
                                               double *e, double *k0d) {
+  if constexpr (sizeof(R) == sizeof(float)) {
+    rkf78_attempt_packed<M, NF>(ms, ev, t, h, x, xn, e, k0d);
+  } else {
     R k[13][3];
     typename Num<R>::V f[NF];
     const R xr[3] = {R(x[0]), R(x[1]), R(x[2])};
@@ -834,6 +991,7 @@ __device__ __forceinline__ void rkf78_attempt(const ModelState<M, R> &ms, const 
         e[i] = (41.0 / 840.0 * h) * double(de);
         k0d[i] = double(k[0][i]);
     }
+  }
 }
 
 // Warp butterfly sum (every lane receives the same, order-fixed result).
