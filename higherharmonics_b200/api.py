@@ -39,9 +39,10 @@ EXPORTED = [
     "hhg_learned_collect", "hhg_default_train_opts", "hhg_mlp_init", "hhg_mlp_train",
     "hhg_mlp_gradients", "hhg_mlp_predict", "hhg_plan_execute_graph", "hhg_plan_autotune", "hhg_measure_fp32_peak",
     "hhg_gpu_k_resolved", "hhg_gpu_split_current", "hhg_gpu_spectrum_welch", "hhg_pulse_values",
+    "hhg_gpu_dirac_current_density",
 ]
 TUNE_MAX = 16
-ABI_VERSION = 3
+ABI_VERSION = 4
 MLP_INPUTS, MLP_HIDDEN = 8, 64
 MLP_N_PARAMS = 64 * 8 + 64 + 64 * 64 + 64 + 64 * 64 + 64 + 64 + 1
 HIST_FIELDS = 12
@@ -137,6 +138,30 @@ class Stats(ctypes.Structure):
         return {n: getattr(self, n) for n, _ in self._fields_}
 
 
+class KappaQuad(ctypes.Structure):
+    """hhg_kappa_quad: the Dirac-3D momentum quadrature (k_z slices x the
+    adaptive kappa rule of DiracSystem::compute_current_density)."""
+    _fields_ = [("max_k", ctypes.c_double), ("threshold", ctypes.c_double),
+                ("n_z", ctypes.c_int32), ("n_kappa", ctypes.c_int32),
+                ("n_splits", ctypes.c_int32), ("max_halvings", ctypes.c_int32)]
+
+
+class KappaStats(ctypes.Structure):
+    _fields_ = [("trajectories", ctypes.c_int64), ("rounds", ctypes.c_int32),
+                ("splits", ctypes.c_int32), ("unconverged", ctypes.c_int32),
+                ("max_level", ctypes.c_int32)]
+
+    def as_dict(self) -> dict:
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
+def kappa_quad(max_k: float, n_z: int, n_kappa: int = 10, threshold: float = 1e-3,
+               n_splits: int = 100, max_halvings: int = 0) -> KappaQuad:
+    """Defaults: the reference's DiracDispatcher (n_kappa 10, threshold 1e-3,
+    DiracDispatcher.cpp:13-14) and split_integrate<100>."""
+    return KappaQuad(max_k, threshold, n_z, n_kappa, n_splits, max_halvings)
+
+
 class HHGError(RuntimeError):
     def __init__(self, status: int, msg: str):
         super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}")
@@ -200,6 +225,10 @@ def load_library() -> ctypes.CDLL:
         L.hhg_gpu_spectrum_welch.argtypes = [ctypes.c_void_p, _D, ctypes.c_int, ctypes.c_double,
                                              ctypes.c_double, _D, _D, _D]
         L.hhg_pulse_values.argtypes = [ctypes.POINTER(PulseDesc), _D, ctypes.c_int64, _D]
+        L.hhg_gpu_dirac_current_density.argtypes = [
+            ctypes.c_void_p, ctypes.POINTER(SystemDesc), ctypes.POINTER(PulseDesc),
+            ctypes.POINTER(KappaQuad), ctypes.POINTER(SolverOpts), _D, ctypes.POINTER(KappaStats),
+            ctypes.POINTER(Stats)]
         _F = ctypes.POINTER(ctypes.c_float)
         L.hhg_learned_collect.argtypes = [ctypes.c_void_p, ctypes.POINTER(SystemDesc),
                                           ctypes.POINTER(PulseDesc), ctypes.c_int,
@@ -476,6 +505,20 @@ class Engine:
                                                    energy_cut, _ptr(lo), _ptr(hi), ctypes.byref(st)),
                     "hhg_gpu_split_current")
         return lo, hi, st
+
+    def dirac_current_density(self, sys: SystemDesc, pulse: PulseDesc, quad: KappaQuad,
+                              opts: SolverOpts | None = None):
+        """The Dirac-3D current density over k_z slices and the adaptive kappa
+        rule (hhg_gpu_dirac_current_density): j, KappaStats, Stats.  The
+        default stepper is the reference's closed-form Magnus step; with
+        relaxation pass an RKF78 solver."""
+        j = np.zeros(pulse.n_measurements + 1)
+        qs, st = KappaStats(), Stats()
+        o = opts if opts is not None else solver(stepper=STEPPER_DIRAC_MAGNUS)
+        self._check(self.lib.hhg_gpu_dirac_current_density(
+            self.ctx, ctypes.byref(sys), ctypes.byref(pulse), ctypes.byref(quad), ctypes.byref(o),
+            _ptr(j), ctypes.byref(qs), ctypes.byref(st)), "hhg_gpu_dirac_current_density")
+        return j, qs, st
 
     def spectrum_welch(self, j: np.ndarray, n_measurements: int, t_begin: float, t_end: float):
         """Welch-windowed N-point FFT of a continuous-laser current (hhg_gpu_spectrum_welch)."""

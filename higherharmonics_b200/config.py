@@ -31,8 +31,17 @@ QuenchedField.cpp:15-29, DoubleLaser.hpp:42-68).  The photon energy of the
 system is multiplied by the experimental one for the exp and double lasers
 (Dispatcher.cpp:10-19).  The experimental lasers exp/expA/expB need the
 measured field of the reference's source, which this package does not carry:
-they raise UnsupportedConfig (api.spline_pulse takes such samples).  The
-Dirac system's adaptive kappa quadrature is not built either.  The
+they raise UnsupportedConfig (api.spline_pulse takes such samples).
+
+system_type Dirac follows DiracDispatcher (DiracDispatcher.cpp:16-63) and the
+DiracSystem constructor (DiracSystem.cpp:52-63): the same beta, E_F and 1/tau,
+max_k = band_width, A0 = (hbar v_F / photon_energy) 1e11 E0 / photon_energy
+(laser_model_ratio, DiracSystem.hpp:30-32), the cosine window [pi t0_offset,
+laser end] without the extra 2 pi, the lasers continuous / cosine / quench /
+powerlaw<e>, and the momentum quadrature n_z slices x the adaptive kappa rule
+with n_kappa = 10 and threshold 1e-3 (DiracDispatcher.cpp:13-14); its
+coherent path is the closed-form Magnus step, the relaxation path FP64 RKF78
+(DiracDispatcher.cpp:66-79).  The
 occupation and split-current run modes are in higherharmonics_b200.runmodes;
 requesting either shortens the double / Gaussian / experimental laser windows to
 0.75 t_end for every mode, as the dispatcher's reduced_duration does
@@ -56,6 +65,7 @@ EXP_PHOTON_ENERGY = 6.091420442472572  # meV (ExperimentParams.hpp:11)
 DOUBLE_LASERS = {"dcos": ("cosine", "both"), "dcosA": ("cosine", "A"), "dcosB": ("cosine", "B"),
                  "dgauss": ("gauss", "both"), "dgaussA": ("gauss", "A"), "dgaussB": ("gauss", "B")}
 PIFLUX_Z_RANGE, PIFLUX_N_COARSE = 32, 4
+DIRAC_N_KAPPA, DIRAC_KAPPA_THRESHOLD, DIRAC_SPLITS = 10, 1e-3, 100
 HONEYCOMB_N_K = 64
 
 
@@ -85,12 +95,16 @@ def _is_zero(x: float) -> bool:
 
 @dataclass
 class Run:
+    """Descriptors of one run.  `lattice_constant` is the laser model ratio of
+    the system (Dirac: hbar v_F / photon_energy); the Dirac system integrates
+    over `quad` instead of a grid."""
     system_type: str
     system: api.SystemDesc
     pulse: api.PulseDesc
-    grid: api.GridDesc
+    grid: api.GridDesc | None
     opts: api.SolverOpts
     lattice_constant: float
+    quad: api.KappaQuad | None = None
 
 
 def from_config(cfg: dict | str, *, grid: api.GridDesc | None = None,
@@ -109,16 +123,15 @@ def from_config(cfg: dict | str, *, grid: api.GridDesc | None = None,
     system_type = cfg.get("system_type", "")
     if system_type not in ("PiFlux", "Honeycomb", "Dirac", "ModifiedPiFlux"):
         raise ValueError(f"System type '{system_type}' not recognized!")
-    if system_type in ("Dirac", "ModifiedPiFlux"):
-        raise UnsupportedConfig(f"system_type {system_type}: the Dirac current density needs the "
-                                "reference's adaptive kappa quadrature; ModifiedPiFlux is not built")
+    if system_type == "ModifiedPiFlux":
+        raise UnsupportedConfig("system_type ModifiedPiFlux is not built")
     if cfg.get("debug_data", "no") != "no":
         raise UnsupportedConfig(f"debug_data = {cfg['debug_data']}: the debug traces are not built")
     reduced = cfg.get("occupations", "no") != "no" or cfg.get("split_current", "no") != "no"
     laser_type = cfg.get("laser_type", "")
     known = {"cosine", "continuous", "gauss", "quench", "exp", "expA", "expB"} | set(DOUBLE_LASERS)
     if not (laser_type in known or laser_type.startswith("powerlaw")) or \
-            (system_type == "Honeycomb" and (laser_type in DOUBLE_LASERS or laser_type == "gauss")):
+            (system_type in ("Honeycomb", "Dirac") and (laser_type in DOUBLE_LASERS or laser_type == "gauss")):
         raise ValueError(f"Laser type '{laser_type}' is not recognized!")
     if laser_type in ("exp", "expA", "expB"):
         raise UnsupportedConfig(f"laser_type {laser_type}: the measured pulse of the reference's "
@@ -135,6 +148,25 @@ def from_config(cfg: dict | str, *, grid: api.GridDesc | None = None,
 
     beta = 0.0 if _is_zero(T) else pe / (K_B * T)
     inv_d = (1e15 * HBAR) / (tau_d * pe)
+    n = n_measurements or n_cycles * MEASUREMENTS_PER_CYCLE
+    if system_type == "Dirac":
+        relax = tau_d > 0  # DiracDispatcher::compute (DiracDispatcher.cpp:66-79)
+        sys_ = api.system(api.SYS_DIRAC3D, beta=beta, fermi_energy=E_F / pe,
+                          inv_diag_relax=inv_d if relax else 0.0)
+        ratio = HBAR * v_F / pe  # DiracSystem::laser_model_ratio
+        if laser_type == "cosine":
+            # CosineLaser(.., n_laser_cycles, pi t0_offset) with time_config =
+            # {t_begin, t_end} (DiracDispatcher.cpp:34-37)
+            t_begin = math.pi * t0_offset
+            pulse = api.cosine_pulse(_amplitude(ratio, E0, pe), n_cycles, n, t_begin=t_begin,
+                                     window=(t_begin, t_begin + 2 * math.pi * n_cycles))
+        else:
+            pulse = make_pulse(laser_type, ratio, E0, pe_in, n_cycles, t0_offset, n)
+        quad = api.kappa_quad(band_width, int(num("n_z")), DIRAC_N_KAPPA,
+                              DIRAC_KAPPA_THRESHOLD, DIRAC_SPLITS)
+        opts = (api.solver(1e-12, 1e-8) if relax else
+                api.solver(stepper=api.STEPPER_DIRAC_MAGNUS))
+        return Run(system_type, sys_, pulse, None, opts, ratio, quad)
     if system_type == "PiFlux":
         hopping = band_width / SQRT12
         lattice = SQRT3 * HBAR * v_F / (pe * band_width)
@@ -151,7 +183,6 @@ def from_config(cfg: dict | str, *, grid: api.GridDesc | None = None,
     sys_ = api.system(kind, hopping=hopping, pol=pol, beta=beta, fermi_energy=E_F / pe,
                       inv_diag_relax=inv_d if relax else 0.0,
                       inv_offdiag_relax=inv_o if relax else 0.0)
-    n = n_measurements or n_cycles * MEASUREMENTS_PER_CYCLE
     pulse = make_pulse(laser_type, lattice, E0, pe_in, n_cycles, t0_offset, n, reduced)
     return Run(system_type, sys_, pulse, g, api.solver(1e-12, 1e-8), lattice)
 

@@ -1277,8 +1277,11 @@ constexpr double kCoarsen = 1.0 / 600.0;
 //   into two channels (PiFlux::current_per_energy, PiFlux.cpp:955-1035);
 // OUT 2: every trajectory's Bloch vector at every sample, kout[i][k][3];
 // OUT 3: every trajectory's band occupations at every sample, kout[i][k][2]
-//   (PiFlux::evolve_occupation_numbers, PiFlux.cpp:222-318).
-// OUT 1-3 are built for the PiFlux models only.
+//   (PiFlux::evolve_occupation_numbers, PiFlux.cpp:222-318);
+// OUT 4: every trajectory's weighted current w_k vertex(S) at every sample,
+//   kout[i][k] (the kappa integrand of DiracSystem::compute_current_density,
+//   DiracSystem.cpp:300-311; dead trajectories give 0 and are counted).
+// OUT 1-3 are built for the PiFlux models only, OUT 4 for the Dirac-3D ones.
 template <int M, int D, typename R, int STEPPER, int PROPOSER, int OUT = 0>
 __global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integrate_kernel(const KParams P) {
     constexpr int NF = Traits<M>::NF;
@@ -1346,7 +1349,7 @@ __global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integ
             double held = 0.0;  // lane (i & 31) holds the warp sum of sample i
             double held2 = 0.0; // ... and of its second channel (OUT 1)
             double kc[4];       // momentum cosines (OUT 1-3)
-            if constexpr (OUT != 0) piflux_cosines(row, kc);
+            if constexpr (OUT >= 1 && OUT <= 3) piflux_cosines(row, kc);
 
             for (int i = 0; i <= N; ++i) {
                 const double *rec = pd.s0rec;
@@ -1524,6 +1527,8 @@ __global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integ
                             }
                         }
                     }
+                } else if constexpr (OUT == 4) {
+                    if (valid) P.kout[(size_t)i * P.n_k + q] = dead ? 0.0 : w * ms.vertex(rec, S);
                 } else if (valid) {
                     constexpr int W = OUT == 2 ? 3 : 2;
                     double *o = P.kout + ((size_t)i * P.n_k + q) * W;
@@ -1755,6 +1760,70 @@ reduce_partials_kernel(const PulseDev *__restrict__ pulses, int n_pulses,
         }
         j[gid] = t + c;
     }
+}
+
+// ---------------------------------------------------------------------------
+// The adaptive kappa rule of the Dirac-3D current density.  One refinement
+// round over a batch of splits: split b of the batch owns the contribution
+// rows [row_begin[b], row_end[b]) of contrib[i][row] (w_k S_z(k, t_i) of its
+// new nodes) and updates its trapezoid estimate
+//   T[split[b]][i] <- scale[b] T + h[b] sum_rows contrib[i][row]
+// (scale 0 on the first round, 1/2 after a halving), writing change[b] =
+// max_i |T_new - T_old| (NaN if any sample is NaN).  Rows are summed
+// lane-strided, then by the warp butterfly: a fixed order.
+// ---------------------------------------------------------------------------
+constexpr int kKappaThreads = 256;
+static __global__ void __launch_bounds__(kKappaThreads)
+kappa_round_kernel(const double *__restrict__ contrib, long long n_rows, int n_samples,
+                   const int *__restrict__ split, const long long *__restrict__ row_begin,
+                   const long long *__restrict__ row_end, const double *__restrict__ scale,
+                   const double *__restrict__ h, double *__restrict__ T,
+                   double *__restrict__ change) {
+    constexpr int kWarps = kKappaThreads / 32;
+    __shared__ double wmax[kWarps];
+    const int b = blockIdx.x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double *Ts = T + (size_t)split[b] * n_samples;
+    const long long r0 = row_begin[b], r1 = row_end[b];
+    const double sc = scale[b], hb = h[b];
+    double dmax = 0.0;
+    for (int i = warp; i < n_samples; i += kWarps) {
+        const double *c = contrib + (size_t)i * n_rows;
+        double acc = 0.0;
+        for (long long r = r0 + lane; r < r1; r += 32) acc += c[r];
+        acc = warp_sum(acc);
+        if (lane == 0) {
+            const double old = Ts[i];
+            // two rounded products and a rounded sum (no contraction)
+            const double v = __dadd_rn(__dmul_rn(sc, old), __dmul_rn(hb, acc));
+            Ts[i] = v;
+            const double d = fabs(v - old);
+            if (d > dmax || d != d) dmax = d;
+        }
+    }
+    if (lane == 0) wmax[warp] = dmax;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double m = 0.0;
+        for (int w = 0; w < kWarps; ++w)
+            if (wmax[w] > m || wmax[w] != wmax[w]) m = wmax[w];
+        change[b] = m;
+    }
+}
+
+// j[i] = dz * sum over slices (in order) of the slice's sum over its splits
+// (in order) of T[slice][split][i] (DiracSystem.cpp:313-321).
+static __global__ void kappa_sum_kernel(const double *__restrict__ T, int n_slices, int n_splits,
+                                        int n_samples, double dz, double *__restrict__ j) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_samples) return;
+    double acc = 0.0;
+    for (int z = 0; z < n_slices; ++z) {
+        double sl = 0.0;
+        for (int s = 0; s < n_splits; ++s) sl = __dadd_rn(sl, T[((size_t)z * n_splits + s) * n_samples + i]);
+        acc = __dadd_rn(acc, sl);
+    }
+    j[i] = acc * dz;
 }
 
 // Zero-padded copy for the r2c FFT (hhg.cpp:280-282).

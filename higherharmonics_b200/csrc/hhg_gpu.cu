@@ -1990,6 +1990,290 @@ hhg_status hhg_gpu_split_current(hhg_ctx *ctx, const hhg_system_desc *sys,
 
 }  // extern "C"
 
+// ---------------------------------------------------------------------------
+// The Dirac-3D momentum quadrature: k_z slices x the adaptive kappa rule
+// (DiracSystem::compute_current_density, DiracSystem.cpp:271-331)
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int kDefaultHalvings = 12;
+constexpr double kKappaChunkBytes = 4.0 * (1 << 30);  // per-trajectory samples of one launch
+
+struct KappaSplit {
+    int slice;     // index of the k_z slice
+    double a, H;   // start and length of the split
+    int level;     // halvings of the estimate held on the device
+    bool done;
+};
+
+// Nodes a split integrates at its current level: level 0 the n_kappa + 1
+// trapezoid nodes a + m H/n_kappa (the two ends weighted 1/2; kappa = 0 is
+// left out, the reference's integrand is zero there, DiracSystem.cpp:301-303),
+// level L > 0 the midpoints a + m H/(n_kappa 2^L), m odd.  Row: k_z, kappa,
+// |k|, weight = end factor x k_z kappa / |k| (integration_weight,
+// DiracSystem.cpp:281), the initial state, 0.
+long long kappa_nodes(const KappaSplit &sp, int n_kappa) {
+    if (sp.level == 0) return n_kappa + 1;
+    return (long long)n_kappa << (sp.level - 1);
+}
+
+void kappa_rows(const hhg_system_desc &sys, double k_z, const KappaSplit &sp, int n_kappa,
+                std::vector<double> &rows) {
+    const long long panels = (long long)n_kappa << sp.level;
+    const double h = sp.H / (double)panels;
+    const long long first = sp.level == 0 ? 0 : 1, stride = sp.level == 0 ? 1 : 2;
+    for (long long m = first; m <= panels; m += stride) {
+        const double kappa = sp.a + (double)m * h;
+        if (ref_is_zero(kappa)) continue;
+        const double mk = sqrt(k_z * k_z + kappa * kappa);
+        const double end = (sp.level == 0 && (m == 0 || m == panels)) ? 0.5 : 1.0;
+        double o[8];
+        o[0] = k_z;
+        o[1] = kappa;
+        o[2] = mk;
+        o[3] = end * (k_z * kappa / mk);
+        initial_state(sys, k_z, kappa, 0.0, o + 4);
+        o[7] = 0.0;
+        rows.insert(rows.end(), o, o + 8);
+    }
+}
+
+// Device memory owned by one call.
+struct DevBuf {
+    void *p = nullptr;
+    ~DevBuf() { if (p) cudaFree(p); }
+    template <typename T> T *as() const { return static_cast<T *>(p); }
+};
+struct PlanGuard {
+    hhg_plan *p = nullptr;
+    ~PlanGuard() { if (p) hhg_plan_destroy(p); }
+};
+
+hhg_status dirac_quadrature(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_pulse_desc *pulse,
+                            const hhg_kappa_quad *q, const hhg_solver_opts *opts, double *j_out,
+                            hhg_kappa_stats *qs, hhg_stats *stats) {
+    if (!sys || !pulse || !q) return set_err(ctx, HHG_BAD_CONFIG, "null descriptor");
+    if (sys->kind != HHG_SYS_DIRAC3D)
+        return set_err(ctx, HHG_UNSUPPORTED, "the kappa quadrature is the Dirac-3D system's");
+    if (q->n_z < 3 || q->n_z > (1 << 16))
+        return set_err(ctx, HHG_BAD_CONFIG, "n_z out of range (3 .. 65536)");
+    if (q->n_kappa < 1 || q->n_kappa > (1 << 20) || q->n_splits < 1 || q->n_splits > (1 << 20))
+        return set_err(ctx, HHG_BAD_CONFIG, "n_kappa and n_splits must be in 1 .. 2^20");
+    const int max_h = q->max_halvings > 0 ? q->max_halvings : kDefaultHalvings;
+    if (q->max_halvings < 0 || max_h > 30 || ((long long)q->n_kappa << max_h) > (1LL << 26))
+        return set_err(ctx, HHG_BAD_CONFIG, "max_halvings out of range (n_kappa 2^max_halvings <= 2^26)");
+    if (!(q->threshold > 0.0) || !std::isfinite(q->threshold) || !(q->max_k > 0.0) ||
+        !std::isfinite(q->max_k))
+        return set_err(ctx, HHG_BAD_CONFIG, "threshold and max_k must be finite and > 0");
+    hhg_solver_opts o;
+    hhg_default_solver_opts(&o);
+    if (opts) o = *opts;
+    if ((o.stepper != HHG_STEPPER_DIRAC_MAGNUS && o.stepper != HHG_STEPPER_RKF78) ||
+        o.precision != HHG_PREC_FP64 || o.proposer != HHG_PROPOSER_NONE)
+        return set_err(ctx, HHG_UNSUPPORTED,
+                       "the Dirac quadrature runs the closed-form Magnus step or FP64 RKF78 with "
+                       "the reference schedule (proposer NONE)");
+    const int n_samples = pulse->n_measurements + 1;
+
+    // k_z slices (DiracSystem.cpp:283, 296-299) and their splits
+    const int n_z = q->n_z;
+    const double dz = 2 * q->max_k / n_z;
+    std::vector<double> kz;
+    for (int z = 1; z < n_z; ++z)
+        if (z != n_z / 2) kz.push_back((z - n_z / 2) * dz);
+    const int n_slices = (int)kz.size();
+    const long long n_total = (long long)n_slices * q->n_splits;
+    if (n_total > (1LL << 28)) return set_err(ctx, HHG_BAD_CONFIG, "too many splits");
+    std::vector<KappaSplit> sp((size_t)n_total);
+    for (int z = 0; z < n_slices; ++z) {
+        // kappa_integration_upper_limit (DiracSystem.cpp:257-261)
+        const double kmax = sqrt(q->max_k * q->max_k - kz[z] * kz[z]);
+        const double H = kmax / q->n_splits;
+        for (int s = 0; s < q->n_splits; ++s) sp[(size_t)z * q->n_splits + s] = {z, s * H, H, 0, false};
+    }
+
+    // rows per launch: every split's nodes fit; otherwise bounded by the
+    // per-trajectory sample buffer
+    long long biggest = 0, first_round = 0;
+    for (const KappaSplit &x : sp) first_round += kappa_nodes(x, q->n_kappa);
+    biggest = std::max<long long>(q->n_kappa + 1, (long long)q->n_kappa << (max_h - 1));
+    const long long budget = (long long)(kKappaChunkBytes / (8.0 * n_samples));
+    const long long cap = std::max(biggest, std::min(first_round, std::max(budget, 32LL)));
+
+    // the plan: pulse staging and launch state, built on one row; the k table
+    // and the per-trajectory buffer are replaced by capacity-sized ones
+    std::vector<double> row0;
+    {
+        KappaSplit x = sp[0];
+        x.level = 1;
+        kappa_rows(*sys, kz[0], x, 1, row0);
+    }
+    hhg_grid_desc g{};
+    g.kind = HHG_GRID_EXPLICIT;
+    g.rows = row0.data();
+    g.n_rows = 1;
+    PlanGuard pg;
+    hhg_status st = hhg_plan_create(ctx, sys, pulse, 1, &g, &o, &pg.p);
+    if (st != HHG_OK) return st;
+    hhg_plan *pl = pg.p;
+    cudaStream_t s = ctx->stream;
+    HHG_CUDA(ctx, cudaFree(pl->d_ktab));
+    pl->d_ktab = nullptr;
+    HHG_CUDA(ctx, cudaMalloc(&pl->d_ktab, (size_t)cap * 8 * sizeof(double)));
+    HHG_CUDA(ctx, cudaMalloc(&pl->d_kout, (size_t)cap * n_samples * sizeof(double)));
+    pl->kout_len = cap * n_samples;
+    pl->out_mode = 4;
+    int occ = 0;
+    {
+        hhg::LaunchReq lr{};
+        lr.degree = pl->degree;
+        lr.precision = o.precision;
+        lr.stepper = o.stepper;
+        lr.proposer = 0;
+        lr.out_mode = 4;
+        lr.grid = 0;
+        lr.occupancy_out = &occ;
+        if ((st = launch_variant(pl, lr)) != HHG_OK) return st;
+    }
+    DevBuf dT, dsplit, dbeg, dend, dscale, dh, dchange, dj;
+    HHG_CUDA(ctx, cudaMalloc(&dT.p, (size_t)n_total * n_samples * sizeof(double)));
+    HHG_CUDA(ctx, cudaMemsetAsync(dT.p, 0, (size_t)n_total * n_samples * sizeof(double), s));
+    const size_t meta = (size_t)std::min<long long>(n_total, cap);  // splits per launch <= rows
+    HHG_CUDA(ctx, cudaMalloc(&dsplit.p, meta * sizeof(int)));
+    HHG_CUDA(ctx, cudaMalloc(&dbeg.p, meta * sizeof(long long)));
+    HHG_CUDA(ctx, cudaMalloc(&dend.p, meta * sizeof(long long)));
+    HHG_CUDA(ctx, cudaMalloc(&dscale.p, meta * sizeof(double)));
+    HHG_CUDA(ctx, cudaMalloc(&dh.p, meta * sizeof(double)));
+    HHG_CUDA(ctx, cudaMalloc(&dchange.p, meta * sizeof(double)));
+    HHG_CUDA(ctx, cudaMalloc(&dj.p, (size_t)n_samples * sizeof(double)));
+
+    hhg_kappa_stats qsum{};
+    qsum.splits = (int32_t)n_total;
+    hhg_stats ssum{};
+    hhg_status worst = HHG_OK;
+    std::vector<long long> active((size_t)n_total);
+    for (long long i = 0; i < n_total; ++i) active[(size_t)i] = i;
+    std::vector<double> rows, scale, hh, change;
+    std::vector<int> ids;
+    std::vector<long long> beg, end;
+    while (!active.empty()) {
+        ++qsum.rounds;
+        size_t next = 0;
+        while (next < active.size()) {
+            // one launch: as many active splits as fit in `cap` rows
+            rows.clear();
+            ids.clear();
+            beg.clear();
+            end.clear();
+            scale.clear();
+            hh.clear();
+            const size_t first = next;
+            long long used = 0;
+            while (next < active.size()) {
+                const KappaSplit &x = sp[(size_t)active[next]];
+                const long long nn = kappa_nodes(x, q->n_kappa);
+                if (next > first && used + nn > cap) break;
+                const long long r0 = (long long)rows.size() / 8;
+                kappa_rows(*sys, kz[x.slice], x, q->n_kappa, rows);
+                const long long r1 = (long long)rows.size() / 8;
+                used += nn;
+                ids.push_back((int)active[next]);
+                beg.push_back(r0);
+                end.push_back(r1);
+                scale.push_back(x.level == 0 ? 0.0 : 0.5);
+                hh.push_back(x.H / (double)((long long)q->n_kappa << x.level));
+                ++next;
+            }
+            const long long n_rows = (long long)rows.size() / 8;
+            const int nb = (int)ids.size();
+            if (n_rows > 0) {
+                HHG_CUDA(ctx, cudaMemcpyAsync(pl->d_ktab, rows.data(), rows.size() * sizeof(double),
+                                              cudaMemcpyHostToDevice, s));
+                pl->n_k = n_rows;
+                pl->tiles_per_item = 1;
+                pl->items_per_pulse = (int)((n_rows + 31) / 32);
+                pl->n_items = pl->items_per_pulse;
+                const long long need = (pl->n_items + hhg::kWarpsPerBlock - 1) / hhg::kWarpsPerBlock;
+                pl->grid = (int)std::max(1LL, std::min((long long)std::max(occ, 1) * ctx->sm_count, need));
+                if ((st = enqueue_integration(pl, s, true)) != HHG_OK) return st;
+            }
+            HHG_CUDA(ctx, cudaMemcpyAsync(dsplit.p, ids.data(), nb * sizeof(int), cudaMemcpyHostToDevice, s));
+            HHG_CUDA(ctx, cudaMemcpyAsync(dbeg.p, beg.data(), nb * sizeof(long long), cudaMemcpyHostToDevice, s));
+            HHG_CUDA(ctx, cudaMemcpyAsync(dend.p, end.data(), nb * sizeof(long long), cudaMemcpyHostToDevice, s));
+            HHG_CUDA(ctx, cudaMemcpyAsync(dscale.p, scale.data(), nb * sizeof(double), cudaMemcpyHostToDevice, s));
+            HHG_CUDA(ctx, cudaMemcpyAsync(dh.p, hh.data(), nb * sizeof(double), cudaMemcpyHostToDevice, s));
+            hhg::kappa_round_kernel<<<nb, hhg::kKappaThreads, 0, s>>>(
+                pl->d_kout, std::max(n_rows, 1LL), n_samples, dsplit.as<int>(), dbeg.as<long long>(),
+                dend.as<long long>(), dscale.as<double>(), dh.as<double>(), dT.as<double>(),
+                dchange.as<double>());
+            HHG_CUDA(ctx, cudaGetLastError());
+            if (n_rows > 0) {
+                hhg_stats sc{};
+                st = hhg_plan_fetch(pl, nullptr, &sc);
+                if (st == HHG_CUDA_ERROR || st == HHG_BAD_CONFIG) return st;
+                if (st != HHG_OK && worst == HHG_OK) worst = st;
+                ssum.k_points += sc.k_points;
+                ssum.trajectories += sc.trajectories;
+                ssum.attempted_steps += sc.attempted_steps;
+                ssum.rejected_steps += sc.rejected_steps;
+                ssum.failed_trajectories += sc.failed_trajectories;
+                ssum.poly_degree = sc.poly_degree;
+                ssum.items += sc.items;
+                ssum.kernel_ms += sc.kernel_ms;
+                ssum.total_ms += sc.total_ms;
+                qsum.trajectories += n_rows;
+            }
+            // the context stream does not synchronise with the legacy stream:
+            // copies are ordered on it
+            change.resize(nb);
+            HHG_CUDA(ctx, cudaMemcpyAsync(change.data(), dchange.p, nb * sizeof(double),
+                                          cudaMemcpyDeviceToHost, s));
+            HHG_CUDA(ctx, cudaStreamSynchronize(s));
+            // convergence: the change of a halving below the threshold
+            for (int b = 0; b < nb; ++b) {
+                KappaSplit &x = sp[(size_t)ids[b]];
+                qsum.max_level = std::max(qsum.max_level, x.level);
+                if (x.level > 0 && change[b] < q->threshold) {
+                    x.done = true;
+                } else if (x.level >= max_h || std::isnan(change[b])) {
+                    x.done = true;
+                    ++qsum.unconverged;
+                } else {
+                    ++x.level;
+                }
+            }
+        }
+        std::vector<long long> still;
+        for (long long i : active)
+            if (!sp[(size_t)i].done) still.push_back(i);
+        active.swap(still);
+    }
+    const int threads = 256;
+    hhg::kappa_sum_kernel<<<(n_samples + threads - 1) / threads, threads, 0, s>>>(
+        dT.as<double>(), n_slices, q->n_splits, n_samples, dz, dj.as<double>());
+    HHG_CUDA(ctx, cudaGetLastError());
+    HHG_CUDA(ctx, cudaMemcpyAsync(j_out, dj.p, (size_t)n_samples * sizeof(double),
+                                  cudaMemcpyDeviceToHost, s));
+    HHG_CUDA(ctx, cudaStreamSynchronize(s));
+    if (qs) *qs = qsum;
+    if (stats) *stats = ssum;
+    return worst;
+}
+}  // namespace
+
+extern "C" {
+
+hhg_status hhg_gpu_dirac_current_density(hhg_ctx *ctx, const hhg_system_desc *sys,
+                                         const hhg_pulse_desc *pulse, const hhg_kappa_quad *quad,
+                                         const hhg_solver_opts *opts, double *j_out,
+                                         hhg_kappa_stats *qstats, hhg_stats *stats) {
+    if (!ctx || !j_out) return set_err(ctx, HHG_BAD_CONFIG, "null context or output");
+    HHG_CUDA(ctx, cudaSetDevice(ctx->device));
+    return dirac_quadrature(ctx, sys, pulse, quad, opts, j_out, qstats, stats);
+}
+
+}  // extern "C"
+
 extern "C" {
 
 hhg_status hhg_gpu_spectrum_welch(hhg_ctx *ctx, const double *j, int n_measurements, double t_begin,

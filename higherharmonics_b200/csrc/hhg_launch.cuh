@@ -17,7 +17,8 @@ struct LaunchReq {
     int grid;       // CTAs; 0 = query occupancy only
     cudaStream_t stream;
     int *occupancy_out;  // blocks per SM for the selected variant (if non-null)
-    int out_mode = 0;    // bz_integrate_kernel's OUT (1-3: PiFlux models, FP64, proposer 0/1)
+    int out_mode = 0;    // bz_integrate_kernel's OUT (1-3: PiFlux models, FP64, proposer 0/1;
+                         // 4: Dirac-3D models, FP64, proposer 0)
 };
 
 struct StageReq {
@@ -48,10 +49,19 @@ cudaError_t launch_one(const LaunchReq &r) {
 }
 
 // k-resolved and split-current outputs (OUT 1-3): PiFlux models, FP64 RKF78,
-// the reference schedule or the carried step
+// the reference schedule or the carried step.  Per-trajectory current (OUT
+// 4): the Dirac-3D models, FP64, the reference schedule or (coherent) the
+// closed-form Magnus step.
 template <int M, int D>
 cudaError_t launch_out(const LaunchReq &r) {
-    if constexpr (base_model(M) == PIFLUX3D) {
+    if constexpr (base_model(M) == DIRAC3D) {
+        if (r.out_mode != 4 || r.precision != 0 || r.proposer != 0) return cudaErrorNotSupported;
+        if (r.stepper == 0) return launch_one<M, D, double, 0, 0, 4>(r);
+        if constexpr (M == DIRAC3D) {
+            if (r.stepper == 2) return launch_one<M, D, double, 2, 0, 4>(r);
+        }
+        return cudaErrorNotSupported;
+    } else if constexpr (base_model(M) == PIFLUX3D) {
         if (r.stepper != 0 || r.precision != 0 || (r.proposer != 0 && r.proposer != 1))
             return cudaErrorNotSupported;
         const bool carry = r.proposer == 1;

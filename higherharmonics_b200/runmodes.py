@@ -60,11 +60,15 @@ def _header(cfg: dict, run: config.Run, N: int, laser_type: str) -> dict:
 
 def current_density(eng: api.Engine, cfg: dict, grid: api.GridDesc | None = None,
                     n_measurements: int | None = None) -> dict:
-    """The main mode: j(t) on the system's grid and its spectrum (trapezoidal
-    FFT with 8x zero padding, or the Welch FFT for the continuous laser)."""
+    """The main mode: j(t) on the system's grid (the Dirac system: its k_z
+    slices and adaptive kappa rule) and its spectrum (trapezoidal FFT with 8x
+    zero padding, or the Welch FFT for the continuous laser)."""
     run = config.from_config(cfg, grid=grid, n_measurements=n_measurements)
     p = run.pulse
-    j, _ = eng.current_density(run.system, p, run.grid, run.opts)
+    if run.quad is not None:  # the Dirac system's k_z x kappa quadrature
+        j, _, _ = eng.dirac_current_density(run.system, p, run.quad, run.opts)
+    else:
+        j, _ = eng.current_density(run.system, p, run.grid, run.opts)
     lt = cfg["laser_type"]
     if lt == "continuous":
         fr, re, im = eng.spectrum_welch(j, p.n_measurements, p.window_begin, p.window_end)

@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define HHG_ABI_VERSION 3
+#define HHG_ABI_VERSION 4
 
 /* Errors: the reference throws std::invalid_argument / std::runtime_error
  * (sources/hhg.cpp:232, Dispatch/PiFluxDispatcher.cpp:104) and Boost.Odeint
@@ -260,6 +260,38 @@ typedef enum hhg_kresolved {
                                  sqrt((|S| -+ S.d_hat)/2), 2 doubles (PiFlux.cpp:227-235) */
 } hhg_kresolved;
 
+/* The Dirac system's momentum quadrature (DiracSystem::compute_current_density
+ * and compute_current_density_diagonal_relaxation, DiracSystem.cpp:271-331,
+ * 365-425, called by DiracDispatcher::compute, DiracDispatcher.cpp:66-79):
+ *   k_z = (z - n_z/2) dz, dz = 2 max_k / n_z, z = 1 .. n_z - 1 without n_z/2
+ *   (integer division; that slice has weight 0);
+ *   kappa over [0, sqrt(max_k^2 - k_z^2)] with the integrand
+ *   S_z(k_z, kappa, t_i) k_z kappa / |k| (0 at kappa = 0);
+ *   j(t_i) = dz * sum_z (kappa integral).
+ * The kappa integral is the adaptive trapezoidal rule the reference calls as
+ * split_integrate<100>(f, 0, kappa_max, n_kappa, threshold, elementwise
+ * error) from its author's library (not available; restated from the call):
+ * [0, kappa_max] is cut into n_splits equal splits; each split starts as the
+ * trapezoid of n_kappa panels and is halved (T <- T/2 + h sum f(midpoints))
+ * until max_i |T_new(t_i) - T_old(t_i)| < threshold or max_halvings halvings
+ * are done; the integral is the sum of the splits' last estimates. */
+typedef struct hhg_kappa_quad {
+    double max_k;          /* DiracSystem::max_k = band_width (DiracSystem.cpp:48, 62) */
+    double threshold;      /* absolute elementwise change (DiracDispatcher.cpp:13: 1e-3) */
+    int32_t n_z;           /* k_z slices + 1 (the config's n_z) */
+    int32_t n_kappa;       /* panels of a split's first trapezoid (DiracDispatcher.cpp:14: 10) */
+    int32_t n_splits;      /* equal splits of the kappa range (split_integrate<100>) */
+    int32_t max_halvings;  /* refinement cap per split; 0 = 12 */
+} hhg_kappa_quad;
+
+typedef struct hhg_kappa_stats {
+    int64_t trajectories;  /* (k_z, kappa) nodes integrated over all rounds */
+    int32_t rounds;        /* integration rounds, the first trapezoids included */
+    int32_t splits;        /* k_z slices x n_splits */
+    int32_t unconverged;   /* splits still at or above the threshold after max_halvings */
+    int32_t max_level;     /* most halvings any split took */
+} hhg_kappa_stats;
+
 /* Library / context management. */
 int hhg_abi_version(void);
 hhg_status hhg_gpu_create(hhg_ctx **ctx, int device);
@@ -446,6 +478,20 @@ hhg_status hhg_gpu_split_current(hhg_ctx *ctx, const hhg_system_desc *sys,
                                  const hhg_pulse_desc *pulse, const hhg_grid_desc *grid,
                                  const hhg_solver_opts *opts, double energy_cut, double *j_low,
                                  double *j_high, hhg_stats *stats);
+
+/* Drop-in for DiracSystem::compute_current_density (DiracSystem.cpp:271-331;
+ * with sys->inv_diag_relax > 0 compute_current_density_diagonal_relaxation,
+ * DiracSystem.cpp:365-425): j_out receives n_measurements + 1 doubles (host).
+ * HHG_SYS_DIRAC3D only; opts->stepper HHG_STEPPER_DIRAC_MAGNUS (the
+ * reference's coherent path, time_evolution_magnus) or HHG_STEPPER_RKF78 (the
+ * sigma equation, time_evolution_sigma, and the relaxation path), FP64,
+ * proposer NONE.  Every refinement round integrates its new nodes in one
+ * launch; the splits' estimates stay on the device.  qstats and stats may be
+ * NULL; stats sums the rounds' launches. */
+hhg_status hhg_gpu_dirac_current_density(hhg_ctx *ctx, const hhg_system_desc *sys,
+                                         const hhg_pulse_desc *pulse, const hhg_kappa_quad *quad,
+                                         const hhg_solver_opts *opts, double *j_out,
+                                         hhg_kappa_stats *qstats, hhg_stats *stats);
 
 /* The continuous laser's spectrum (hhg.cpp:264-275): the first n_measurements
  * samples of j times the Welch window 1 - (i - N/2)^2 / (N^2/4)

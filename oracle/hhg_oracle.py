@@ -284,6 +284,104 @@ def split_current(m, p, tc, s, ktab: np.ndarray, cut: float, threads=0):
     return lo, hi, rc
 
 
+def kappa_rows(m: OrcModel, k_z: float, a: float, H: float, level: int, n_kappa: int) -> np.ndarray:
+    """The Dirac-3D rows one split [a, a + H] integrates at `level`: level 0
+    the n_kappa + 1 trapezoid nodes a + i H/n_kappa (ends weighted 1/2),
+    level L > 0 the midpoints a + i H/(n_kappa 2^L), i odd; kappa = 0 is left
+    out (the reference's integrand is zero there, DiracSystem.cpp:301-303).
+    Row: k_z, kappa, |k|, weight x k_z kappa/|k| (DiracSystem.cpp:281), S0, 0."""
+    panels = n_kappa << level
+    h = H / panels
+    idx = range(0, panels + 1) if level == 0 else range(1, panels, 2)
+    rows = []
+    for i in idx:
+        kappa = a + i * h
+        if _is_zero(kappa):
+            continue
+        mk = float(np.sqrt(k_z * k_z + kappa * kappa))
+        end = 0.5 if level == 0 and i in (0, panels) else 1.0
+        rows.append([k_z, kappa, mk, end * (k_z * kappa / mk), *initial_state(m, k_z, kappa, 0.0), 0.0])
+    return np.array(rows, dtype=np.float64).reshape(-1, KROW)
+
+
+def adaptive_kappa(contrib, slices_kz, kappa_max, n_kappa: int, threshold: float, n_splits: int,
+                   max_halvings: int, dz: float, n_samples: int, rows_fn):
+    """The adaptive trapezoidal rule of the Dirac-3D kappa integral, restated
+    from the reference's call split_integrate<100>(f, 0, kappa_max, n_kappa,
+    threshold, elementwise error) (DiracSystem.cpp:307-310; the integrator's
+    library is not available): each of n_splits equal splits starts as the
+    n_kappa-panel trapezoid and is halved, T <- T/2 + h sum f(midpoints),
+    until max_t |T_new - T_old| < threshold or max_halvings halvings; the
+    slice's integral is the sum of its splits in order, and j = dz times the
+    sum of the slices in order (DiracSystem.cpp:313-321).  `rows_fn(z, a, H,
+    level)` gives a split's rows, `contrib(rows)` the weighted samples
+    (n_samples, n_rows).  Every round evaluates all active splits' rows in one
+    batch.  Returns j and {rounds, unconverged, max_level, trajectories}."""
+    n_slices = len(slices_kz)
+    T = np.zeros((n_slices, n_splits, n_samples))
+    level = np.zeros((n_slices, n_splits), dtype=int)
+    active = [(z, sp) for z in range(n_slices) for sp in range(n_splits)]
+    info = {"rounds": 0, "unconverged": 0, "max_level": 0, "trajectories": 0}
+    while active:
+        info["rounds"] += 1
+        H = [kappa_max[z] / n_splits for z in range(n_slices)]
+        parts = [rows_fn(z, sp * H[z], H[z], level[z, sp]) for z, sp in active]
+        batch = np.concatenate(parts) if parts else np.zeros((0, KROW))
+        info["trajectories"] += batch.shape[0]
+        c = contrib(batch) if batch.shape[0] else np.zeros((n_samples, 0))
+        off = 0
+        still = []
+        for (z, sp), rows in zip(active, parts):
+            L = level[z, sp]
+            h = H[z] / (n_kappa << L)
+            acc = c[:, off:off + rows.shape[0]].sum(axis=1)
+            off += rows.shape[0]
+            old = T[z, sp].copy()
+            T[z, sp] = (0.0 if L == 0 else 0.5) * old + h * acc
+            change = float(np.max(np.abs(T[z, sp] - old)))
+            info["max_level"] = max(info["max_level"], int(L))
+            if L > 0 and change < threshold:
+                continue
+            if L >= max_halvings or np.isnan(change):
+                info["unconverged"] += 1
+                continue
+            level[z, sp] = L + 1
+            still.append((z, sp))
+        active = still
+    j = np.zeros(n_samples)
+    for z in range(n_slices):
+        sl = np.zeros(n_samples)
+        for sp in range(n_splits):
+            sl = sl + T[z, sp]
+        j = j + sl
+    return j * dz, info
+
+
+def dirac_kappa_current(m: OrcModel, p, tc, s, max_k: float, n_z: int, n_kappa: int = 10,
+                        threshold: float = 1e-3, n_splits: int = 100, max_halvings: int = 12):
+    """DiracSystem::compute_current_density (DiracSystem.cpp:271-331; with
+    relaxation compute_current_density_diagonal_relaxation, :365-425) on the
+    oracle: k_z = (z - n_z/2) 2 max_k / n_z for z = 1 .. n_z - 1 without
+    n_z/2, kappa in [0, sqrt(max_k^2 - k_z^2)] by ``adaptive_kappa``, the
+    integrand S_z k_z kappa / |k| from orc_evolve_k with the model's stepper
+    (s.stepper 2: the closed-form Magnus step).  Returns (j, info, status)."""
+    dz = 2 * max_k / n_z
+    kz = [(z - n_z // 2) * dz for z in range(1, n_z) if z != n_z // 2]
+    kmax = [float(np.sqrt(max_k * max_k - k * k)) for k in kz]
+    status = [0]
+
+    def contrib(rows):
+        out, rc = k_resolved(m, p, tc, s, rows, 0)
+        if rc != 0:
+            status[0] = rc
+        return out[:, :, 2] * rows[:, 3][None, :]
+
+    j, info = adaptive_kappa(contrib, kz, kmax, n_kappa, threshold, n_splits, max_halvings, dz,
+                             tc.n_measurements + 1,
+                             lambda z, a, H, L: kappa_rows(m, kz[z], a, H, L, n_kappa))
+    return j, info, status[0]
+
+
 def magnus_coefficients(p: Pulse, delta_t, t0) -> np.ndarray:
     out = np.zeros(4)
     pc = p.c()

@@ -52,7 +52,10 @@ def _c_layout():
                "hhg_tune_report": ["n_candidates", "best", "tile_k", "grid", "kernel_ms"],
                "hhg_stats": ["k_points", "trajectories", "attempted_steps", "rejected_steps",
                              "failed_trajectories", "poly_degree", "items", "kernel_ms",
-                             "total_ms"]}
+                             "total_ms"],
+               "hhg_kappa_quad": ["max_k", "threshold", "n_z", "n_kappa", "n_splits",
+                                  "max_halvings"],
+               "hhg_kappa_stats": ["trajectories", "rounds", "splits", "unconverged", "max_level"]}
     src = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(){"]
     for s, fields in structs.items():
         src.append(f'printf("{s} size %zu\\n", sizeof({s}));')
@@ -77,7 +80,8 @@ def test_ctypes_layout_matches_c():
     for cname, py in [("hhg_system_desc", api.SystemDesc), ("hhg_pulse_desc", api.PulseDesc),
                       ("hhg_grid_desc", api.GridDesc), ("hhg_solver_opts", api.SolverOpts),
                       ("hhg_stats", api.Stats), ("hhg_mlp", api.Mlp),
-                      ("hhg_train_opts", api.TrainOpts), ("hhg_tune_report", api.TuneReport)]:
+                      ("hhg_train_opts", api.TrainOpts), ("hhg_tune_report", api.TuneReport),
+                      ("hhg_kappa_quad", api.KappaQuad), ("hhg_kappa_stats", api.KappaStats)]:
         assert lay[(cname, "size")] == ctypes.sizeof(py), cname
         for fname, _ in py._fields_:
             if (cname, fname) in lay:

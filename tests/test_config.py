@@ -91,12 +91,16 @@ def test_descriptors_pass_the_abi_checks():
 
 @pytest.mark.parametrize("edit,exc", [
     (("laser_type cosine", "laser_type expA"), config.UnsupportedConfig),
-    (("system_type PiFlux", "system_type Dirac"), config.UnsupportedConfig),
+    (("system_type PiFlux", "system_type ModifiedPiFlux"), config.UnsupportedConfig),
+    (("system_type PiFlux", "system_type Dirac\n"), None),
     (("debug_data no", "debug_data yes"), config.UnsupportedConfig),
     (("system_type PiFlux", "system_type Graphene"), ValueError),
     (("E_F 118\n", ""), ValueError),
 ])
 def test_refused_configurations(edit, exc):
+    if exc is None:
+        config.from_config(PIFLUX.replace(*edit))
+        return
     with pytest.raises(exc):
         config.from_config(PIFLUX.replace(*edit))
 
@@ -168,3 +172,32 @@ def test_run_modes_shorten_the_double_laser_window():
     cos_full = config.from_config(PIFLUX).pulse
     cos_red = config.from_config(PIFLUX.replace("split_current no", "split_current yes")).pulse
     assert cos_red.window_end == cos_full.window_end
+
+
+def test_dirac_mapping():
+    # DiracDispatcher (DiracDispatcher.cpp:16-79) and DiracSystem (DiracSystem.cpp:52-63)
+    cfg = PIFLUX.replace("system_type PiFlux", "system_type Dirac")
+    run = config.from_config(cfg)
+    s, p, q = run.system, run.pulse, run.quad
+    pe = 5.25
+    assert s.kind == api.SYS_DIRAC3D and run.grid is None
+    assert s.beta == pytest.approx(pe / (K_B * 300), rel=1e-15)
+    assert s.fermi_energy == pytest.approx(118 / pe, rel=1e-15)
+    assert s.inv_diag_relax == pytest.approx(1e15 * HBAR / (15 * pe), rel=1e-15)
+    assert s.inv_offdiag_relax == 0.0
+    ratio = HBAR * 1.5e6 / pe
+    assert p.amplitude == pytest.approx(ratio * 1e11 * 1.6 / pe, rel=1e-15)
+    # the cosine window ends with the laser (no extra cycle)
+    assert (p.window_begin, p.window_end) == pytest.approx((2 * math.pi, 2 * math.pi + 8 * math.pi))
+    assert p.n_measurements == 4 * 1024
+    assert (q.max_k, q.n_z, q.n_kappa, q.threshold, q.n_splits) == (300.0, 51, 10, 1e-3, 100)
+    # relaxation: FP64 RKF78; coherent: the closed-form Magnus step
+    assert run.opts.stepper == api.STEPPER_RKF78 and (run.opts.abs_tol, run.opts.rel_tol) == (1e-12, 1e-8)
+    coh = config.from_config(cfg.replace("diagonal_relaxation_time 15", "diagonal_relaxation_time -1"))
+    assert coh.system.inv_diag_relax == 0.0 and coh.opts.stepper == api.STEPPER_DIRAC_MAGNUS
+    # the Dirac dispatcher knows no Gaussian or double lasers
+    for lt in ("gauss", "dcos", "dgaussA"):
+        with pytest.raises(ValueError):
+            config.from_config(cfg.replace("laser_type cosine", f"laser_type {lt}"))
+    with pytest.raises(ValueError):
+        config.from_config(cfg.replace("n_z 51\n", ""))

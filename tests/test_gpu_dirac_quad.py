@@ -1,0 +1,135 @@
+"""The Dirac-3D momentum quadrature on the GPU (hhg_gpu_dirac_current_density,
+through the C ABI) against the oracle's restatement.
+
+Reference: DiracSystem::compute_current_density (DiracSystem.cpp:271-331) and
+compute_current_density_diagonal_relaxation (:365-425), called by
+DiracDispatcher::compute (DiracDispatcher.cpp:65-80): k_z slices times the
+adaptive trapezoidal kappa rule (restated from the reference's call, its
+library being unavailable; see tests/test_oracle_kappa.py).  Bar: the same
+refinement (rounds, levels, nodes) as the oracle, and j(t) relative L2
+<= 1e-12 for the closed-form Magnus path (no step control), 1e-9 for RKF78.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from higherharmonics_b200 import api, config, runmodes
+from oracle import hhg_oracle as O
+from tests.helpers import oracle_args, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def _system(beta=0.0, fermi=0.0, relax=0.0):
+    return api.system(api.SYS_DIRAC3D, beta=beta, fermi_energy=fermi, inv_diag_relax=relax)
+
+
+def _oracle(sys, pulse, quad, stepper):
+    m, p, tc, s = oracle_args(sys, pulse, 1e-12, 1e-8, stepper=stepper)
+    return O.dirac_kappa_current(m, p, tc, s, max_k=quad.max_k, n_z=quad.n_z,
+                                 n_kappa=quad.n_kappa, threshold=quad.threshold,
+                                 n_splits=quad.n_splits, max_halvings=quad.max_halvings or 12)
+
+
+def _same_refinement(qs, info):
+    assert (qs.rounds, qs.unconverged, qs.max_level, qs.trajectories) == \
+        (info["rounds"], info["unconverged"], info["max_level"], info["trajectories"])
+
+
+def test_magnus_parity(engine):
+    sys, pulse = _system(), api.cosine_pulse(0.6, 1, 256)
+    quad = api.kappa_quad(2.5, 8, n_kappa=4, threshold=1e-5, n_splits=5, max_halvings=8)
+    j, qs, st = engine.dirac_current_density(sys, pulse, quad)
+    jr, info, rc = _oracle(sys, pulse, quad, api.STEPPER_DIRAC_MAGNUS)
+    assert rc == 0 and st.failed_trajectories == 0
+    assert qs.splits == 6 * 5  # n_z = 8: z = 1 .. 7 without 4
+    _same_refinement(qs, info)
+    # splits stop at different levels
+    uniform = qs.splits * (5 + 4 * ((1 << qs.max_level) - 1))
+    assert qs.max_level >= 3 and qs.trajectories < uniform
+    assert rel_l2(j, jr) <= 1e-12, rel_l2(j, jr)
+
+
+def test_thermal_magnus_parity(engine):
+    sys, pulse = _system(beta=3.0, fermi=0.4), api.gauss_pulse(0.5, 1, 256)
+    quad = api.kappa_quad(2.0, 7, n_kappa=3, threshold=1e-5, n_splits=4, max_halvings=8)
+    j, qs, _ = engine.dirac_current_density(sys, pulse, quad)
+    jr, info, rc = _oracle(sys, pulse, quad, api.STEPPER_DIRAC_MAGNUS)
+    assert rc == 0 and qs.splits == 5 * 4  # odd n_z: z = 1 .. 6 without 3
+    _same_refinement(qs, info)
+    assert rel_l2(j, jr) <= 1e-12, rel_l2(j, jr)
+
+
+@pytest.mark.parametrize("relax", [0.0, 0.2])
+def test_rkf78_parity(engine, relax):
+    # the sigma equation (time_evolution_sigma) and the diagonal relaxation
+    # path (time_evolution_diagonal_relaxation), both FP64 RKF78
+    sys, pulse = _system(beta=2.0, fermi=0.2, relax=relax), api.cosine_pulse(0.5, 1, 128)
+    quad = api.kappa_quad(1.5, 6, n_kappa=3, threshold=1e-4, n_splits=3, max_halvings=6)
+    j, qs, st = engine.dirac_current_density(sys, pulse, quad, api.solver(1e-12, 1e-8))
+    jr, info, rc = _oracle(sys, pulse, quad, api.STEPPER_RKF78)
+    assert rc == 0 and st.failed_trajectories == 0 and st.attempted_steps > 0
+    _same_refinement(qs, info)
+    assert rel_l2(j, jr) <= 1e-9, rel_l2(j, jr)
+
+
+def test_odd_in_the_field_at_size(engine):
+    # even n_z and a T = 0 start: (k_z, A) -> (-k_z, -A) maps the trajectories
+    # onto each other with the weight's sign flipped, so j(-A) = -j(A) with
+    # the same refinement; at the reference's n_kappa, threshold and splits
+    quad = api.kappa_quad(2.5, 40, n_kappa=10, threshold=1e-6, n_splits=100)
+    jp, qp, _ = engine.dirac_current_density(_system(), api.cosine_pulse(0.6, 2, 2048), quad)
+    jm, qm, _ = engine.dirac_current_density(_system(), api.cosine_pulse(-0.6, 2, 2048), quad)
+    assert qp.as_dict() == qm.as_dict() and qp.unconverged == 0 and qp.rounds >= 2
+    assert np.max(np.abs(jp + jm)) <= 1e-12 * np.max(np.abs(jp))
+    # no field: the equilibrium is stationary and the k_z-odd weights cancel
+    j0, q0, _ = engine.dirac_current_density(_system(), api.cosine_pulse(0.0, 2, 2048), quad)
+    assert np.max(np.abs(j0)) <= 1e-12 * np.max(np.abs(jp))
+
+
+DIRAC_CFG = """
+T 0
+E_F 0
+v_F 1e5
+band_width 3
+field_amplitude 0.5
+photon_energy 5
+diagonal_relaxation_time -1
+laser_type cosine
+n_laser_cycles 1
+t0_offset 0
+n_z 6
+occupations no
+split_current no
+debug_data no
+system_type Dirac
+"""
+
+
+def test_dirac_config_end_to_end(engine):
+    doc = runmodes.current_density(engine, config.read_config(DIRAC_CFG), n_measurements=128)
+    run = config.from_config(DIRAC_CFG, n_measurements=128)
+    jr, info, rc = _oracle(run.system, run.pulse, run.quad, api.STEPPER_DIRAC_MAGNUS)
+    assert rc == 0
+    j = np.array(doc["current_density_time"])
+    assert rel_l2(j, jr) <= 1e-12 and np.max(np.abs(jr)) > 0
+    assert len(doc["frequencies"]) == len(doc["current_density_frequency_real"])
+
+
+def test_refusals(engine):
+    pulse = api.cosine_pulse(0.5, 1, 64)
+    quad = api.kappa_quad(2.0, 6, n_kappa=2, n_splits=2)
+    cases = [
+        (api.system(api.SYS_DIRAC2D, velocity=1.0), quad, None, api.UNSUPPORTED),
+        (_system(), quad, api.solver(proposer=api.PROPOSER_CARRY), api.UNSUPPORTED),
+        (_system(), quad, api.solver(1e-8, 1e-6, precision=api.PREC_MIXED), api.UNSUPPORTED),
+        (_system(relax=0.1), quad, api.solver(stepper=api.STEPPER_DIRAC_MAGNUS), api.UNSUPPORTED),
+        (_system(), api.kappa_quad(2.0, 2), None, api.BAD_CONFIG),
+        (_system(), api.kappa_quad(2.0, 6, threshold=0.0), None, api.BAD_CONFIG),
+        (_system(), api.kappa_quad(2.0, 6, n_kappa=1 << 20, max_halvings=12), None, api.BAD_CONFIG),
+    ]
+    for sys, q, opts, status in cases:
+        with pytest.raises(api.HHGError) as ei:
+            engine.dirac_current_density(sys, pulse, q, opts)
+        assert ei.value.status == status, (ei.value, status)
