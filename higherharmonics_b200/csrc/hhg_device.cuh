@@ -1354,19 +1354,24 @@ __global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integ
             for (int i = 0; i <= N; ++i) {
                 const double *rec = pd.s0rec;
                 if (i > 0) {
-                    // stage interval i-1 into this warp's shared slot
-                    __syncwarp();
+                    // stage interval i-1 into this warp's shared slot (the
+                    // closed-form Magnus step reads its four moments and the
+                    // record straight from the staging table: warp broadcasts)
                     const double *gslot = coef + (size_t)(i - 1) * SLOT;
-                    const double2 *src = reinterpret_cast<const double2 *>(gslot);
-                    double2 *dst = reinterpret_cast<double2 *>(slot);
-                    for (int c = lane; c < COPY / 2; c += 32) dst[c] = __ldg(src + c);
+                    if constexpr (STEPPER != 2) {
+                        __syncwarp();
+                        const double2 *src = reinterpret_cast<const double2 *>(gslot);
+                        double2 *dst = reinterpret_cast<double2 *>(slot);
+                        for (int c = lane; c < COPY / 2; c += 32) dst[c] = __ldg(src + c);
+                    }
                     if constexpr (kNarrow && PROPOSER == 0) {
                         __syncwarp();
                         for (int c = lane; c < NTAB; c += 32) stage_tab[wib][c] = Num<R>::mk(slot[TAB + c]);
                     }
                     __syncwarp();
-                    rec = slot + 4;
-                    const double t0 = slot[0], t1 = slot[1];
+                    const double *cur = STEPPER == 2 ? gslot : slot;
+                    rec = cur + 4;
+                    const double t0 = cur[0], t1 = cur[1];
                     const PolyEval<NF, D, R> poly{slot, tb, te};
                     if constexpr (STEPPER == 1) {
                         if (!dead) {
@@ -1394,7 +1399,10 @@ __global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integ
                         // the interval's Legendre moments sit where the standard
                         // schedule's table would (staging layout 3)
                         if (!dead) {
-                            dirac_magnus_step(row[0], row[1], row[2], pd.measure_every, slot + TAB, S);
+                            double mom[4];
+#pragma unroll
+                            for (int c = 0; c < 4; ++c) mom[c] = __ldg(gslot + TAB + c);
+                            dirac_magnus_step(row[0], row[1], row[2], pd.measure_every, mom, S);
                             ++my_attempts;
                         }
                     } else if constexpr (!kDyadic) {
@@ -1763,29 +1771,71 @@ reduce_partials_kernel(const PulseDev *__restrict__ pulses, int n_pulses,
 }
 
 // ---------------------------------------------------------------------------
-// The adaptive kappa rule of the Dirac-3D current density.  One refinement
-// round over a batch of splits: split b of the batch owns the contribution
-// rows [row_begin[b], row_end[b]) of contrib[i][row] (w_k S_z(k, t_i) of its
-// new nodes) and updates its trapezoid estimate
-//   T[split[b]][i] <- scale[b] T + h[b] sum_rows contrib[i][row]
-// (scale 0 on the first round, 1/2 after a halving), writing change[b] =
+// The adaptive kappa rule of the Dirac-3D current density.  A refinement
+// round works on a batch of splits; KappaItem b (host-built) holds split b's
+// slice momentum k_z, start a and this round's panel width h, its nodes
+// m = first + stride idx (idx < n) at kappa = a + m h, and the rows
+// [row0, row0 + n) of the round's k table and contributions.
+// ---------------------------------------------------------------------------
+struct KappaItem {
+    double k_z, a, h;
+    long long row0, panels;  // panels = n_kappa 2^level
+    int n, first, stride, level;
+    int split, pad;
+};
+
+// The round's k table: k_z, kappa, |k|, the weight end x k_z kappa / |k|
+// (integration_weight, DiracSystem.cpp:281; ends of a first trapezoid 1/2,
+// zero kappa weighted 0 as the reference's integrand, DiracSystem.cpp:301-303)
+// and the Fermi-occupied start (2 a0 b0, 0, a0^2 - b0^2), a0 = f(E_F + |k|),
+// b0 = f(E_F - |k|) (DiracSystem.cpp:155-158).  Products and sums are rounded
+// one by one (no contraction), as the host and the oracle form them.
+static __global__ void kappa_rows_kernel(const KappaItem *__restrict__ items, int nb,
+                                         long long n_rows, double beta, double fermi,
+                                         double *__restrict__ ktab) {
+    for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < n_rows;
+         r += (long long)gridDim.x * blockDim.x) {
+        int lo = 0, hi = nb;
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (items[mid].row0 <= r) lo = mid; else hi = mid;
+        }
+        const KappaItem &it = items[lo];
+        const long long m = it.first + (long long)it.stride * (r - it.row0);
+        const double kz = it.k_z;
+        const double kappa = __dadd_rn(it.a, __dmul_rn((double)m, it.h));
+        const double mk = sqrt(__dadd_rn(__dmul_rn(kz, kz), __dmul_rn(kappa, kappa)));
+        const double end = (it.level == 0 && (m == 0 || m == it.panels)) ? 0.5 : 1.0;
+        const double a0 = fermi_occ(fermi + mk, beta), b0 = fermi_occ(fermi - mk, beta);
+        double *o = ktab + (size_t)r * 8;
+        o[0] = kz;
+        o[1] = kappa;
+        o[2] = mk;
+        o[3] = ref_is_zero_dev(kappa) ? 0.0 : end * (kz * kappa / mk);
+        o[4] = __dmul_rn(__dmul_rn(2.0, a0), b0);
+        o[5] = 0.0;
+        o[6] = __dsub_rn(__dmul_rn(a0, a0), __dmul_rn(b0, b0));
+        o[7] = 0.0;
+    }
+}
+
+// One refinement round: split items[b] updates its trapezoid estimate
+//   T[split][i] <- scale T + h sum_rows contrib[i][row]
+// (scale 0 on the first round, 1/2 after a halving) and writes change[b] =
 // max_i |T_new - T_old| (NaN if any sample is NaN).  Rows are summed
 // lane-strided, then by the warp butterfly: a fixed order.
-// ---------------------------------------------------------------------------
 constexpr int kKappaThreads = 256;
 static __global__ void __launch_bounds__(kKappaThreads)
 kappa_round_kernel(const double *__restrict__ contrib, long long n_rows, int n_samples,
-                   const int *__restrict__ split, const long long *__restrict__ row_begin,
-                   const long long *__restrict__ row_end, const double *__restrict__ scale,
-                   const double *__restrict__ h, double *__restrict__ T,
+                   const KappaItem *__restrict__ items, double *__restrict__ T,
                    double *__restrict__ change) {
     constexpr int kWarps = kKappaThreads / 32;
     __shared__ double wmax[kWarps];
-    const int b = blockIdx.x;
+    const KappaItem &it = items[blockIdx.x];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    double *Ts = T + (size_t)split[b] * n_samples;
-    const long long r0 = row_begin[b], r1 = row_end[b];
-    const double sc = scale[b], hb = h[b];
+    double *Ts = T + (size_t)it.split * n_samples;
+    const long long r0 = it.row0, r1 = it.row0 + it.n;
+    const double sc = it.level == 0 ? 0.0 : 0.5, hb = it.h;
     double dmax = 0.0;
     for (int i = warp; i < n_samples; i += kWarps) {
         const double *c = contrib + (size_t)i * n_rows;
@@ -1807,7 +1857,7 @@ kappa_round_kernel(const double *__restrict__ contrib, long long n_rows, int n_s
         double m = 0.0;
         for (int w = 0; w < kWarps; ++w)
             if (wmax[w] > m || wmax[w] != wmax[w]) m = wmax[w];
-        change[b] = m;
+        change[blockIdx.x] = m;
     }
 }
 

@@ -2007,35 +2007,11 @@ struct KappaSplit {
 };
 
 // Nodes a split integrates at its current level: level 0 the n_kappa + 1
-// trapezoid nodes a + m H/n_kappa (the two ends weighted 1/2; kappa = 0 is
-// left out, the reference's integrand is zero there, DiracSystem.cpp:301-303),
-// level L > 0 the midpoints a + m H/(n_kappa 2^L), m odd.  Row: k_z, kappa,
-// |k|, weight = end factor x k_z kappa / |k| (integration_weight,
-// DiracSystem.cpp:281), the initial state, 0.
+// trapezoid nodes a + m H/n_kappa, level L > 0 the midpoints a + m
+// H/(n_kappa 2^L), m odd (hhg::kappa_rows_kernel builds their rows).
 long long kappa_nodes(const KappaSplit &sp, int n_kappa) {
     if (sp.level == 0) return n_kappa + 1;
     return (long long)n_kappa << (sp.level - 1);
-}
-
-void kappa_rows(const hhg_system_desc &sys, double k_z, const KappaSplit &sp, int n_kappa,
-                std::vector<double> &rows) {
-    const long long panels = (long long)n_kappa << sp.level;
-    const double h = sp.H / (double)panels;
-    const long long first = sp.level == 0 ? 0 : 1, stride = sp.level == 0 ? 1 : 2;
-    for (long long m = first; m <= panels; m += stride) {
-        const double kappa = sp.a + (double)m * h;
-        if (ref_is_zero(kappa)) continue;
-        const double mk = sqrt(k_z * k_z + kappa * kappa);
-        const double end = (sp.level == 0 && (m == 0 || m == panels)) ? 0.5 : 1.0;
-        double o[8];
-        o[0] = k_z;
-        o[1] = kappa;
-        o[2] = mk;
-        o[3] = end * (k_z * kappa / mk);
-        initial_state(sys, k_z, kappa, 0.0, o + 4);
-        o[7] = 0.0;
-        rows.insert(rows.end(), o, o + 8);
-    }
 }
 
 // Device memory owned by one call.
@@ -2092,21 +2068,20 @@ hhg_status dirac_quadrature(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_
         for (int s = 0; s < q->n_splits; ++s) sp[(size_t)z * q->n_splits + s] = {z, s * H, H, 0, false};
     }
 
-    // rows per launch: every split's nodes fit; otherwise bounded by the
-    // per-trajectory sample buffer
-    long long biggest = 0, first_round = 0;
-    for (const KappaSplit &x : sp) first_round += kappa_nodes(x, q->n_kappa);
-    biggest = std::max<long long>(q->n_kappa + 1, (long long)q->n_kappa << (max_h - 1));
+    // rows per launch: a whole round when its per-trajectory samples fit in
+    // the budget, else chunks of whole splits (a split's nodes always fit)
+    const long long biggest = std::max<long long>(q->n_kappa + 1, (long long)q->n_kappa << (max_h - 1));
     const long long budget = (long long)(kKappaChunkBytes / (8.0 * n_samples));
-    const long long cap = std::max(biggest, std::min(first_round, std::max(budget, 32LL)));
+    const long long limit = std::max(biggest, std::max(budget, 32LL));
+    long long cap = 0;  // rows the k table and the sample buffer hold now
 
     // the plan: pulse staging and launch state, built on one row; the k table
     // and the per-trajectory buffer are replaced by capacity-sized ones
-    std::vector<double> row0;
+    std::vector<double> row0(8);
     {
-        KappaSplit x = sp[0];
-        x.level = 1;
-        kappa_rows(*sys, kz[0], x, 1, row0);
+        const double kappa = 0.5 * sp[0].H;
+        const double mk = sqrt(kz[0] * kz[0] + kappa * kappa);
+        push_row(*sys, kz[0], kappa, mk, kz[0] * kappa / mk, row0.data());
     }
     hhg_grid_desc g{};
     g.kind = HHG_GRID_EXPLICIT;
@@ -2117,11 +2092,6 @@ hhg_status dirac_quadrature(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_
     if (st != HHG_OK) return st;
     hhg_plan *pl = pg.p;
     cudaStream_t s = ctx->stream;
-    HHG_CUDA(ctx, cudaFree(pl->d_ktab));
-    pl->d_ktab = nullptr;
-    HHG_CUDA(ctx, cudaMalloc(&pl->d_ktab, (size_t)cap * 8 * sizeof(double)));
-    HHG_CUDA(ctx, cudaMalloc(&pl->d_kout, (size_t)cap * n_samples * sizeof(double)));
-    pl->kout_len = cap * n_samples;
     pl->out_mode = 4;
     int occ = 0;
     {
@@ -2135,15 +2105,11 @@ hhg_status dirac_quadrature(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_
         lr.occupancy_out = &occ;
         if ((st = launch_variant(pl, lr)) != HHG_OK) return st;
     }
-    DevBuf dT, dsplit, dbeg, dend, dscale, dh, dchange, dj;
+    DevBuf dT, ditems, dchange, dj;
     HHG_CUDA(ctx, cudaMalloc(&dT.p, (size_t)n_total * n_samples * sizeof(double)));
     HHG_CUDA(ctx, cudaMemsetAsync(dT.p, 0, (size_t)n_total * n_samples * sizeof(double), s));
-    const size_t meta = (size_t)std::min<long long>(n_total, cap);  // splits per launch <= rows
-    HHG_CUDA(ctx, cudaMalloc(&dsplit.p, meta * sizeof(int)));
-    HHG_CUDA(ctx, cudaMalloc(&dbeg.p, meta * sizeof(long long)));
-    HHG_CUDA(ctx, cudaMalloc(&dend.p, meta * sizeof(long long)));
-    HHG_CUDA(ctx, cudaMalloc(&dscale.p, meta * sizeof(double)));
-    HHG_CUDA(ctx, cudaMalloc(&dh.p, meta * sizeof(double)));
+    const size_t meta = (size_t)std::min<long long>(n_total, limit);  // splits per launch <= rows
+    HHG_CUDA(ctx, cudaMalloc(&ditems.p, meta * sizeof(hhg::KappaItem)));
     HHG_CUDA(ctx, cudaMalloc(&dchange.p, meta * sizeof(double)));
     HHG_CUDA(ctx, cudaMalloc(&dj.p, (size_t)n_samples * sizeof(double)));
 
@@ -2153,42 +2119,65 @@ hhg_status dirac_quadrature(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_
     hhg_status worst = HHG_OK;
     std::vector<long long> active((size_t)n_total);
     for (long long i = 0; i < n_total; ++i) active[(size_t)i] = i;
-    std::vector<double> rows, scale, hh, change;
-    std::vector<int> ids;
-    std::vector<long long> beg, end;
+    std::vector<hhg::KappaItem> items;
+    std::vector<double> change;
     while (!active.empty()) {
         ++qsum.rounds;
+        long long round_rows = 0;
+        for (long long i : active) round_rows += kappa_nodes(sp[(size_t)i], q->n_kappa);
+        const long long want = std::min(limit, round_rows);
+        if (want > cap) {
+            // grow the k table and the per-trajectory sample buffer
+            cap = std::min(limit, std::max(want, 2 * cap));
+            HHG_CUDA(ctx, cudaFree(pl->d_ktab));
+            HHG_CUDA(ctx, cudaFree(pl->d_kout));
+            pl->d_ktab = nullptr;
+            pl->d_kout = nullptr;
+            HHG_CUDA(ctx, cudaMalloc(&pl->d_ktab, (size_t)cap * 8 * sizeof(double)));
+            HHG_CUDA(ctx, cudaMalloc(&pl->d_kout, (size_t)cap * n_samples * sizeof(double)));
+            pl->kout_len = cap * n_samples;
+        }
         size_t next = 0;
         while (next < active.size()) {
-            // one launch: as many active splits as fit in `cap` rows
-            rows.clear();
-            ids.clear();
-            beg.clear();
-            end.clear();
-            scale.clear();
-            hh.clear();
+            // one launch: as many active splits as fit in `cap` rows; the rows
+            // are built on the device from the splits' items
+            items.clear();
+            long long n_rows = 0;
             const size_t first = next;
-            long long used = 0;
             while (next < active.size()) {
                 const KappaSplit &x = sp[(size_t)active[next]];
                 const long long nn = kappa_nodes(x, q->n_kappa);
-                if (next > first && used + nn > cap) break;
-                const long long r0 = (long long)rows.size() / 8;
-                kappa_rows(*sys, kz[x.slice], x, q->n_kappa, rows);
-                const long long r1 = (long long)rows.size() / 8;
-                used += nn;
-                ids.push_back((int)active[next]);
-                beg.push_back(r0);
-                end.push_back(r1);
-                scale.push_back(x.level == 0 ? 0.0 : 0.5);
-                hh.push_back(x.H / (double)((long long)q->n_kappa << x.level));
+                if (next > first && n_rows + nn > cap) break;
+                hhg::KappaItem it{};
+                it.k_z = kz[x.slice];
+                it.a = x.a;
+                it.panels = (long long)q->n_kappa << x.level;
+                it.h = x.H / (double)it.panels;
+                it.level = x.level;
+                it.split = (int)active[next];
+                it.row0 = n_rows;
+                if (x.level == 0) {
+                    // kappa = 0 (the first node of a slice) is left out
+                    it.first = ref_is_zero(x.a) ? 1 : 0;
+                    it.stride = 1;
+                    it.n = (int)(nn - it.first);
+                } else {
+                    it.first = 1;
+                    it.stride = 2;
+                    it.n = (int)nn;
+                }
+                n_rows += it.n;
+                items.push_back(it);
                 ++next;
             }
-            const long long n_rows = (long long)rows.size() / 8;
-            const int nb = (int)ids.size();
+            const int nb = (int)items.size();
+            HHG_CUDA(ctx, cudaMemcpyAsync(ditems.p, items.data(), nb * sizeof(hhg::KappaItem),
+                                          cudaMemcpyHostToDevice, s));
             if (n_rows > 0) {
-                HHG_CUDA(ctx, cudaMemcpyAsync(pl->d_ktab, rows.data(), rows.size() * sizeof(double),
-                                              cudaMemcpyHostToDevice, s));
+                const long long blocks = std::min<long long>((n_rows + 255) / 256, 65536);
+                hhg::kappa_rows_kernel<<<(unsigned)blocks, 256, 0, s>>>(
+                    ditems.as<hhg::KappaItem>(), nb, n_rows, sys->beta, sys->fermi_energy, pl->d_ktab);
+                HHG_CUDA(ctx, cudaGetLastError());
                 pl->n_k = n_rows;
                 pl->tiles_per_item = 1;
                 pl->items_per_pulse = (int)((n_rows + 31) / 32);
@@ -2197,15 +2186,9 @@ hhg_status dirac_quadrature(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_
                 pl->grid = (int)std::max(1LL, std::min((long long)std::max(occ, 1) * ctx->sm_count, need));
                 if ((st = enqueue_integration(pl, s, true)) != HHG_OK) return st;
             }
-            HHG_CUDA(ctx, cudaMemcpyAsync(dsplit.p, ids.data(), nb * sizeof(int), cudaMemcpyHostToDevice, s));
-            HHG_CUDA(ctx, cudaMemcpyAsync(dbeg.p, beg.data(), nb * sizeof(long long), cudaMemcpyHostToDevice, s));
-            HHG_CUDA(ctx, cudaMemcpyAsync(dend.p, end.data(), nb * sizeof(long long), cudaMemcpyHostToDevice, s));
-            HHG_CUDA(ctx, cudaMemcpyAsync(dscale.p, scale.data(), nb * sizeof(double), cudaMemcpyHostToDevice, s));
-            HHG_CUDA(ctx, cudaMemcpyAsync(dh.p, hh.data(), nb * sizeof(double), cudaMemcpyHostToDevice, s));
             hhg::kappa_round_kernel<<<nb, hhg::kKappaThreads, 0, s>>>(
-                pl->d_kout, std::max(n_rows, 1LL), n_samples, dsplit.as<int>(), dbeg.as<long long>(),
-                dend.as<long long>(), dscale.as<double>(), dh.as<double>(), dT.as<double>(),
-                dchange.as<double>());
+                pl->d_kout, std::max(n_rows, 1LL), n_samples, ditems.as<hhg::KappaItem>(),
+                dT.as<double>(), dchange.as<double>());
             HHG_CUDA(ctx, cudaGetLastError());
             if (n_rows > 0) {
                 hhg_stats sc{};
@@ -2231,7 +2214,7 @@ hhg_status dirac_quadrature(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_
             HHG_CUDA(ctx, cudaStreamSynchronize(s));
             // convergence: the change of a halving below the threshold
             for (int b = 0; b < nb; ++b) {
-                KappaSplit &x = sp[(size_t)ids[b]];
+                KappaSplit &x = sp[(size_t)items[b].split];
                 qsum.max_level = std::max(qsum.max_level, x.level);
                 if (x.level > 0 && change[b] < q->threshold) {
                     x.done = true;
