@@ -467,6 +467,220 @@ def our_arm(args, wl_name):
     return 0
 
 
+# The Dirac workload's unit is one k.interval of the closed-form Magnus step
+# (DiracSystem::time_evolution_magnus): 24 cross products (216 flops), the
+# 13 series terms (78), the first-order term, moments and setup (~30) and the
+# rotation S <- exp(Omega) S (~75): ~400 FP64 flops, plus sqrt, sincos and two
+# divisions (special operations).
+MAGNUS_FLOPS_PER_KINTERVAL = 400
+MAGNUS_SPECIAL_OPS = 4
+
+
+class DiracCpuBaseline:
+    """The oracle's Dirac quadrature (the same adaptive kappa rule, the
+    oracle's closed-form Magnus step, OpenMP over trajectories) on an evenly
+    spaced subset of the (k_z slice, split) pairs, each split refined to
+    convergence; spectra/s scaled by all splits / sampled splits (the splits
+    are independent)."""
+
+    def __init__(self, wl, target_s: float):
+        from oracle import hhg_oracle as O
+        from tests.helpers import oracle_args
+        self.O = O
+        self.m, self.p, self.tc, self.s = oracle_args(wl.system, wl.pulse, wl.opts.abs_tol,
+                                                      wl.opts.rel_tol, stepper=wl.opts.stepper)
+        q = wl.quad
+        self.q = q
+        self.dz = 2 * q.max_k / q.n_z
+        self.kz = [(z - q.n_z // 2) * self.dz for z in range(1, q.n_z) if z != q.n_z // 2]
+        self.cores = (len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity")
+                      else os.cpu_count())
+        self.pairs = [(z, sp) for z in range(len(self.kz)) for sp in range(q.n_splits)]
+        # calibration: the first splits of the middle slice (the widest kappa range)
+        mid = len(self.kz) // 2 * q.n_splits
+        t0 = time.perf_counter()
+        self._splits(self.pairs[mid:mid + 4])
+        per_split = (time.perf_counter() - t0) / 4
+        n = int(min(len(self.pairs), max(4, target_s / max(per_split, 1e-9))))
+        step = len(self.pairs) / n
+        self.sample = sorted({self.pairs[int(i * step)] for i in range(n)})
+
+    def _splits(self, pairs):
+        O, q = self.O, self.q
+        kz = self.kz
+        kmax = [math.sqrt(q.max_k * q.max_k - k * k) for k in kz]
+        m, p, tc, s = self.m, self.p, self.tc, self.s
+
+        def contrib(rows):
+            out, rc = O.k_resolved(m, p, tc, s, rows, 0, threads=self.cores, fast=True)
+            if rc != 0:
+                raise RuntimeError(f"oracle status {rc}")
+            return out[:, :, 2] * rows[:, 3][None, :]
+
+        _, info = O.adaptive_kappa(contrib, kz, kmax, q.n_kappa, q.threshold, q.n_splits,
+                                   q.max_halvings or 12, self.dz, tc.n_measurements + 1,
+                                   lambda z, a, H, L: O.kappa_rows(m, kz[z], a, H, L, q.n_kappa),
+                                   only=pairs)
+        return info
+
+    def run(self):
+        t0 = time.perf_counter()
+        info = self._splits(self.sample)
+        el = time.perf_counter() - t0
+        n_all = len(self.pairs)
+        v = 1.0 / (el * n_all / len(self.sample))
+        kint = info["trajectories"] * self.tc.n_measurements
+        desc = (f"{len(self.sample)} of {n_all} (k_z slice, kappa split) pairs, evenly spaced, "
+                f"each refined to convergence ({info['trajectories']} trajectories, {kint} Magnus "
+                f"k.intervals) in {el:.2f} s on {self.cores} threads (oracle port, -O3 "
+                f"-ffast-math, OpenMP); "
+                f"spectra/s scaled by {n_all}/{len(self.sample)}")
+        return v, desc, kint / el
+
+
+def dirac_config(wl, path):
+    q = wl.quad
+    return {"workload": wl.name, "n_z": q.n_z, "n_kappa": q.n_kappa, "n_splits": q.n_splits,
+            "kappa_threshold": q.threshold, "max_k": q.max_k,
+            "n_measurements": wl.pulse.n_measurements, "stepper": "closed-form Magnus (FP64)",
+            "l2": "flushed (256 MiB write) before every timed step", "path": path}
+
+
+def dirac_reference_arm(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    from higherharmonics_b200 import workloads as W
+    wl = W.dirac3d_kappa()
+    cb = DiracCpuBaseline(wl, args.cpu_seconds)
+    per = []
+    desc = None
+    for i in range(args.warmup + args.steps):
+        v, desc, _ = cb.run()
+        if i >= args.warmup:
+            per.append(1.0 / v)
+    t = float(np.mean(per))
+    line = {"impl": "reference", "metric": METRIC, "value": 1.0 / t, "unit": UNIT, "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": dirac_config(wl, "oracle port"),
+            "cpu_baseline": {"value": 1.0 / t, "unit": UNIT, "cores": cb.cores, "kind": "port",
+                             "sample": desc},
+            "e2e": {"value": 1.0 / t, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def dirac_arm(args):
+    """One step = one Dirac spectrum through the public API:
+    Engine.dirac_current_density (k_z slices x the adaptive kappa rule, every
+    refinement round one integration launch over its new nodes, convergence
+    read back to the host) and Engine.spectrum.  The call is synchronous and
+    host-driven between rounds, so `value` is the wall time of the quadrature
+    call and `e2e` adds the spectrum; the roofline uses the integration
+    kernels' CUDA-event time summed over the rounds."""
+    import torch
+    ws, rank, local = dist_env()
+    if ws > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+    from higherharmonics_b200 import api
+    from higherharmonics_b200 import workloads as W
+    wl = W.dirac3d_kappa()
+    if ws > 1:  # one pulse instance per rank: weak scaling
+        wl.pulse.phase = wl.pulse.phase + 0.1 * rank
+    eng = api.Engine(dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    p = wl.pulse
+
+    def step():
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        j, qs, st = eng.dirac_current_density(wl.system, p, wl.quad, wl.opts)
+        t1 = time.perf_counter()
+        eng.spectrum(j, p.n_measurements, p.window_begin, p.window_end)
+        t2 = time.perf_counter()
+        return t1 - t0, t2 - t0, qs, st
+
+    for _ in range(args.warmup):
+        step()
+    peak = eng.fp64_peak_tflops()
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    except Exception:
+        pass
+    sampler = ClockSampler(uuid)
+    sampler.start()
+    time.sleep(0.3)
+    if ws > 1:
+        torch.distributed.barrier()
+    quad_s, e2e_s, kern_ms, kint, launches = 0.0, 0.0, 0.0, 0, 0
+    qs = st = None
+    for _ in range(args.steps):
+        a, b, qs, st = step()
+        quad_s += a
+        e2e_s += b
+        kern_ms += st.kernel_ms
+        kint += st.attempted_steps
+        launches += 3 * qs.launches + 1 + 3  # rows, integration, round; sum; pad, FFT, correction
+    if ws > 1:
+        torch.distributed.barrier()
+    clocks = sampler.stop()
+    if ws > 1:
+        t = torch.tensor([quad_s, e2e_s], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        quad_s, e2e_s = float(t[0]), float(t[1])
+    if rank != 0:
+        if ws > 1:
+            torch.distributed.destroy_process_group()
+        return 0
+    kernel_s = kern_ms * 1e-3
+    achieved = MAGNUS_FLOPS_PER_KINTERVAL * kint / kernel_s / 1e12
+    n_s = p.n_measurements + 1
+    n_fft = 4 * n_s + 1
+    line = {
+        "metric": METRIC, "value": ws * args.steps / quad_s, "unit": UNIT, "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * quad_s / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": dirac_config(wl, "hhg_gpu_dirac_current_density (synchronous, host-driven "
+                                   "rounds), wall clock"),
+        "k_intervals_per_spectrum": st.attempted_steps, "kappa": qs.as_dict(),
+        "gpu_launches": launches,
+        "roofline": {"bound": "fp64_pipe", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "peak_source": "measured FP64 FMA throughput (hhg_measure_fp64_peak, burst)",
+                     "kernel": "bz_integrate_kernel (closed-form Magnus, per-trajectory output)",
+                     "kernel_ms": kern_ms / args.steps,
+                     "kernel_ms_source": "CUDA events around each round's integration launch on "
+                                         "the context stream, summed over the rounds",
+                     "alg_flops_per_k_interval": MAGNUS_FLOPS_PER_KINTERVAL,
+                     "special_ops_per_k_interval": MAGNUS_SPECIAL_OPS},
+        "clocks": clocks,
+        "e2e": {"value": ws * args.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": int(8 * n_s + 3 * 8 * n_fft),
+                "path": "Engine.dirac_current_density + Engine.spectrum, host buffers, wall "
+                        "clock (inputs are descriptors: rows are built on the device)"},
+    }
+    if ws == 1 and not args.no_cpu_baseline:
+        cb = DiracCpuBaseline(wl, args.cpu_seconds)
+        v, desc, kps = cb.run()
+        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": cb.cores, "kind": "port",
+                                "sample": desc, "k_intervals_per_s": kps}
+    print(json.dumps(line), flush=True)
+    eng.close()
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
 def ncu_case(args):
     """A small case of the bench workload for ncu captures (committed so the
     profile summaries name a command that runs committed files only): the
@@ -477,6 +691,13 @@ def ncu_case(args):
     from higherharmonics_b200 import api
     from higherharmonics_b200 import workloads as W
     import inspect
+    if args.workload == "dirac3d_kappa":
+        wl = W.dirac3d_kappa(n_cycles=args.ncu_cycles)
+        eng = api.Engine(0)
+        for _ in range(2):
+            _, qs, st = eng.dirac_current_density(wl.system, wl.pulse, wl.quad, wl.opts)
+        print("ok dirac3d_kappa", qs.as_dict(), st.attempted_steps, st.kernel_ms)
+        return 0
     make = W.ALL[args.workload]
     wl = (make(n_cycles=args.ncu_cycles) if "n_cycles" in inspect.signature(make).parameters
           else make())
@@ -528,6 +749,8 @@ def main():
         return ncu_case(args)
     if args.variant == "mlp_train":
         ap.error("--variant mlp_train is a profiling case (--ncu-case)")
+    if args.workload == "dirac3d_kappa":
+        return dirac_reference_arm(args) if args.impl == "reference" else dirac_arm(args)
     if args.impl == "reference":
         return reference_arm(args, args.workload)
     return our_arm(args, args.workload)

@@ -2205,6 +2205,7 @@ hhg_status dirac_quadrature(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_
                 ssum.kernel_ms += sc.kernel_ms;
                 ssum.total_ms += sc.total_ms;
                 qsum.trajectories += n_rows;
+                ++qsum.launches;
             }
             // the context stream does not synchronise with the legacy stream:
             // copies are ordered on it

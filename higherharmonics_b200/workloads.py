@@ -166,6 +166,49 @@ def piflux3d_relax(n_cycles=16) -> Workload:
                     dict(abs_tol=1e-12, rel_tol=1e-8), piflux3d_relax.__doc__)
 
 
+# experiment.config's material (v_F 1e5 m/s, band width 200 meV, n_z 60) on
+# the Dirac system with the cosine laser of params.config's photon energy at
+# 0.1 MV/cm (A0 = 24 in the system's momentum units)
+DIRAC_CONFIG = """\
+T 300
+E_F 118
+v_F 1e5
+band_width 200
+field_amplitude 0.1
+photon_energy 5.25
+diagonal_relaxation_time -1
+laser_type cosine
+n_laser_cycles {n_cycles}
+t0_offset 0
+n_z 60
+system_type Dirac
+"""
+
+
+@dataclass
+class DiracWorkload:
+    name: str
+    system: api.SystemDesc
+    pulse: api.PulseDesc
+    quad: api.KappaQuad
+    opts: api.SolverOpts
+    description: str
+
+
+def dirac3d_kappa(n_cycles=8) -> DiracWorkload:
+    """The reference's Dirac run (DiracDispatcher::compute ->
+    DiracSystem::compute_current_density, coherent: the closed-form Magnus
+    step per interval): T = 300 K, E_F = 118 meV, v_F = 1e5 m/s, band width
+    200 meV (max_k = 200), photon energy 5.25 meV, 0.1 MV/cm, cosine laser,
+    8 cycles (8192 intervals); 59 k_z slices x 100 splits of the kappa range,
+    first trapezoids of 10 panels, halved until the elementwise change is
+    below 1e-3 (DiracDispatcher.cpp:13-14)."""
+    from . import config
+    run = config.from_config(DIRAC_CONFIG.format(n_cycles=n_cycles))
+    return DiracWorkload(f"dirac3d_kappa_nz60_{n_cycles}cyc", run.system, run.pulse, run.quad,
+                         run.opts, dirac3d_kappa.__doc__)
+
+
 ALL = {
     "dirac2d_64": dirac2d_64,
     "piflux2d_256": piflux2d_256,
@@ -173,4 +216,5 @@ ALL = {
     "dirac2d_sweep": dirac2d_sweep,
     "honeycomb_1024x64": honeycomb_1024x64,
     "piflux3d_relax": piflux3d_relax,
+    "dirac3d_kappa": dirac3d_kappa,
 }

@@ -290,6 +290,8 @@ typedef struct hhg_kappa_stats {
     int32_t splits;        /* k_z slices x n_splits */
     int32_t unconverged;   /* splits still at or above the threshold after max_halvings */
     int32_t max_level;     /* most halvings any split took */
+    int32_t launches;      /* integration launches (a round's splits in budget-sized chunks) */
+    int32_t reserved;
 } hhg_kappa_stats;
 
 /* Library / context management. */

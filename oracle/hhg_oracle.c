@@ -1104,16 +1104,25 @@ int orc_split_current(const orc_model *m, const orc_pulse *p, const orc_time_con
  * (sources/HHG/Laser/gauss.hpp:14-80): negative nodes by increasing |x|,
  * then positive nodes increasing; shifted Legendre values as gauss.hpp:82-101
  * computes them, including its legendre_4 = 20x^3 - 30x^2 + 12x + 1. */
-void orc_magnus_coefficients(const orc_pulse *p, double delta_t, double t0, double *coeffs) {
-    double x[30], w[30], ab[30], wt[30];
+/* The 30-point rule on [0, 1] in the reference's order (gauss.hpp:14-80:
+ * negative nodes by increasing |x|, then the positive ones), computed once at
+ * load time as the reference's tables are compile-time constants. */
+static double gl30_ab[30], gl30_wt[30];
+
+__attribute__((constructor)) static void gl30_init(void) {
+    double x[30], w[30];
     orc_gauss_legendre(30, x, w);
     for (int i = 0; i < 15; ++i) {
         const double xi = x[15 + i]; /* i-th positive node, ascending */
-        ab[i] = 0.5 * (-xi + 1.);
-        ab[15 + i] = 0.5 * (xi + 1.);
-        wt[i] = 0.5 * w[15 + i];
-        wt[15 + i] = 0.5 * w[15 + i];
+        gl30_ab[i] = 0.5 * (-xi + 1.);
+        gl30_ab[15 + i] = 0.5 * (xi + 1.);
+        gl30_wt[i] = 0.5 * w[15 + i];
+        gl30_wt[15 + i] = 0.5 * w[15 + i];
     }
+}
+
+void orc_magnus_coefficients(const orc_pulse *p, double delta_t, double t0, double *coeffs) {
+    const double *ab = gl30_ab, *wt = gl30_wt;
     double c0 = 0, c1 = 0, c2 = 0, c3 = 0;
     for (int i = 0; i < 30; ++i) {
         const double a = ab[i];

@@ -260,13 +260,14 @@ def current_density(m, p: Pulse, tc, s, ktab: np.ndarray, threads=0, fast=False)
     return j, st, rc
 
 
-def k_resolved(m, p, tc, s, ktab: np.ndarray, kind: int, threads=0):
-    """orc_k_resolved: (n_measurements + 1, n_k, 3 | 2) samples and status."""
+def k_resolved(m, p, tc, s, ktab: np.ndarray, kind: int, threads=0, fast=False):
+    """orc_k_resolved: (n_measurements + 1, n_k, 3 | 2) samples and status
+    (fast: the -O3 -ffast-math build, for CPU timing)."""
     ktab = np.ascontiguousarray(ktab, dtype=np.float64)
     w = 3 if kind == 0 else 2
     out = np.zeros((tc.n_measurements + 1, ktab.shape[0], w))
     pc = p.c()
-    rc = lib().orc_k_resolved(ctypes.byref(m), ctypes.byref(pc), ctypes.byref(tc), ctypes.byref(s),
+    rc = lib(fast).orc_k_resolved(ctypes.byref(m), ctypes.byref(pc), ctypes.byref(tc), ctypes.byref(s),
                               ctypes.c_int(ktab.shape[0]), _p(ktab), ctypes.c_int(kind), _p(out),
                               ctypes.c_int(threads))
     return out, rc
@@ -305,7 +306,7 @@ def kappa_rows(m: OrcModel, k_z: float, a: float, H: float, level: int, n_kappa:
 
 
 def adaptive_kappa(contrib, slices_kz, kappa_max, n_kappa: int, threshold: float, n_splits: int,
-                   max_halvings: int, dz: float, n_samples: int, rows_fn):
+                   max_halvings: int, dz: float, n_samples: int, rows_fn, only=None):
     """The adaptive trapezoidal rule of the Dirac-3D kappa integral, restated
     from the reference's call split_integrate<100>(f, 0, kappa_max, n_kappa,
     threshold, elementwise error) (DiracSystem.cpp:307-310; the integrator's
@@ -316,11 +317,14 @@ def adaptive_kappa(contrib, slices_kz, kappa_max, n_kappa: int, threshold: float
     sum of the slices in order (DiracSystem.cpp:313-321).  `rows_fn(z, a, H,
     level)` gives a split's rows, `contrib(rows)` the weighted samples
     (n_samples, n_rows).  Every round evaluates all active splits' rows in one
-    batch.  Returns j and {rounds, unconverged, max_level, trajectories}."""
+    batch.  `only` restricts the work to a list of (slice, split) pairs (the
+    splits are independent; j then sums those only).  Returns j and {rounds,
+    unconverged, max_level, trajectories}."""
     n_slices = len(slices_kz)
     T = np.zeros((n_slices, n_splits, n_samples))
     level = np.zeros((n_slices, n_splits), dtype=int)
-    active = [(z, sp) for z in range(n_slices) for sp in range(n_splits)]
+    active = (list(only) if only is not None else
+              [(z, sp) for z in range(n_slices) for sp in range(n_splits)])
     info = {"rounds": 0, "unconverged": 0, "max_level": 0, "trajectories": 0}
     while active:
         info["rounds"] += 1
