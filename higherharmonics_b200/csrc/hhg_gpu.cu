@@ -31,6 +31,17 @@ struct hhg_ctx {
     double *d_x = nullptr, *d_out = nullptr;
     double2 *d_F = nullptr;
     size_t x_cap = 0, f_cap = 0;
+    // the Dirac quadrature's state, kept between calls: the plan (pulse
+    // staging, launch state) of the last (system, pulse, options), the rows
+    // its k table and sample buffer hold, and grow-only device buffers
+    hhg_plan *kappa_plan = nullptr;
+    std::string kappa_key;
+    long long kappa_cap = 0;
+    int kappa_occ = 1;
+    struct Grow {
+        void *p = nullptr;
+        size_t bytes = 0;
+    } kappa_T, kappa_items, kappa_change, kappa_j;
 };
 
 struct hhg_plan {
@@ -897,6 +908,8 @@ void hhg_gpu_destroy(hhg_ctx *c) {
     cudaSetDevice(c->device);
     for (auto &kv : c->plan_cache) hhg_plan_destroy(kv.second);
     c->plan_cache.clear();
+    if (c->kappa_plan) hhg_plan_destroy(c->kappa_plan);
+    for (hhg_ctx::Grow *g : {&c->kappa_T, &c->kappa_items, &c->kappa_change, &c->kappa_j}) cudaFree(g->p);
     for (auto &kv : c->fft_plans) cufftDestroy(kv.second);
     cudaFree(c->d_x);
     cudaFree(c->d_F);
@@ -2014,17 +2027,6 @@ long long kappa_nodes(const KappaSplit &sp, int n_kappa) {
     return (long long)n_kappa << (sp.level - 1);
 }
 
-// Device memory owned by one call.
-struct DevBuf {
-    void *p = nullptr;
-    ~DevBuf() { if (p) cudaFree(p); }
-    template <typename T> T *as() const { return static_cast<T *>(p); }
-};
-struct PlanGuard {
-    hhg_plan *p = nullptr;
-    ~PlanGuard() { if (p) hhg_plan_destroy(p); }
-};
-
 hhg_status dirac_quadrature(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_pulse_desc *pulse,
                             const hhg_kappa_quad *q, const hhg_solver_opts *opts, double *j_out,
                             hhg_kappa_stats *qs, hhg_stats *stats) {
@@ -2070,48 +2072,71 @@ hhg_status dirac_quadrature(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_
 
     // rows per launch: a whole round when its per-trajectory samples fit in
     // the budget, else chunks of whole splits (a split's nodes always fit)
-    const long long biggest = std::max<long long>(q->n_kappa + 1, (long long)q->n_kappa << (max_h - 1));
+    // (the first round holds a split's n_kappa + 1 trapezoid nodes and its
+    // n_kappa first midpoints)
+    const long long biggest = std::max<long long>(2LL * q->n_kappa + 1, (long long)q->n_kappa << (max_h - 1));
     const long long budget = (long long)(kKappaChunkBytes / (8.0 * n_samples));
     const long long limit = std::max(biggest, std::max(budget, 32LL));
-    long long cap = 0;  // rows the k table and the sample buffer hold now
 
-    // the plan: pulse staging and launch state, built on one row; the k table
-    // and the per-trajectory buffer are replaced by capacity-sized ones
-    std::vector<double> row0(8);
-    {
-        const double kappa = 0.5 * sp[0].H;
-        const double mk = sqrt(kz[0] * kz[0] + kappa * kappa);
-        push_row(*sys, kz[0], kappa, mk, kz[0] * kappa / mk, row0.data());
-    }
+    // the plan: pulse staging and launch state, built on one placeholder row
+    // (the k table and the per-trajectory buffer are replaced by
+    // capacity-sized ones); kept in the context for the next call with the
+    // same system, pulse and options
+    static const double kPlaceholderRow[8] = {1.0, 1.0, 1.4142135623730951, 0.0, 0.0, 0.0, -1.0, 0.0};
     hhg_grid_desc g{};
     g.kind = HHG_GRID_EXPLICIT;
-    g.rows = row0.data();
+    g.rows = kPlaceholderRow;
     g.n_rows = 1;
-    PlanGuard pg;
-    hhg_status st = hhg_plan_create(ctx, sys, pulse, 1, &g, &o, &pg.p);
-    if (st != HHG_OK) return st;
-    hhg_plan *pl = pg.p;
-    cudaStream_t s = ctx->stream;
-    pl->out_mode = 4;
-    int occ = 0;
-    {
+    hhg_status st = HHG_OK;
+    const std::string key = plan_key(sys, pulse, 1, &g, &o);
+    if (!ctx->kappa_plan || ctx->kappa_key != key) {
+        if (ctx->kappa_plan) hhg_plan_destroy(ctx->kappa_plan);
+        ctx->kappa_plan = nullptr;
+        ctx->kappa_key.clear();
+        ctx->kappa_cap = 0;
+        hhg_plan *np = nullptr;
+        if ((st = hhg_plan_create(ctx, sys, pulse, 1, &g, &o, &np)) != HHG_OK) return st;
+        np->out_mode = 4;
+        int occ = 0;
         hhg::LaunchReq lr{};
-        lr.degree = pl->degree;
+        lr.degree = np->degree;
         lr.precision = o.precision;
         lr.stepper = o.stepper;
         lr.proposer = 0;
         lr.out_mode = 4;
         lr.grid = 0;
         lr.occupancy_out = &occ;
-        if ((st = launch_variant(pl, lr)) != HHG_OK) return st;
+        if ((st = launch_variant(np, lr)) != HHG_OK) {
+            hhg_plan_destroy(np);
+            return st;
+        }
+        ctx->kappa_plan = np;
+        ctx->kappa_key = key;
+        ctx->kappa_occ = std::max(occ, 1);
     }
-    DevBuf dT, ditems, dchange, dj;
-    HHG_CUDA(ctx, cudaMalloc(&dT.p, (size_t)n_total * n_samples * sizeof(double)));
-    HHG_CUDA(ctx, cudaMemsetAsync(dT.p, 0, (size_t)n_total * n_samples * sizeof(double), s));
-    const size_t meta = (size_t)std::min<long long>(n_total, limit);  // splits per launch <= rows
-    HHG_CUDA(ctx, cudaMalloc(&ditems.p, meta * sizeof(hhg::KappaItem)));
-    HHG_CUDA(ctx, cudaMalloc(&dchange.p, meta * sizeof(double)));
-    HHG_CUDA(ctx, cudaMalloc(&dj.p, (size_t)n_samples * sizeof(double)));
+    hhg_plan *pl = ctx->kappa_plan;
+    const int occ = ctx->kappa_occ;
+    long long &cap = ctx->kappa_cap;  // rows the k table and the sample buffer hold
+    cudaStream_t s = ctx->stream;
+    auto grow = [&](hhg_ctx::Grow &b, size_t bytes) -> cudaError_t {
+        if (bytes <= b.bytes) return cudaSuccess;
+        cudaFree(b.p);
+        b.p = nullptr;
+        b.bytes = 0;
+        const cudaError_t e = cudaMalloc(&b.p, bytes);
+        if (e == cudaSuccess) b.bytes = bytes;
+        return e;
+    };
+    const size_t meta = (size_t)std::min<long long>(2 * n_total, limit);  // items per launch <= rows
+    HHG_CUDA(ctx, grow(ctx->kappa_T, (size_t)n_total * n_samples * sizeof(double)));
+    HHG_CUDA(ctx, grow(ctx->kappa_items, meta * sizeof(hhg::KappaItem)));
+    HHG_CUDA(ctx, grow(ctx->kappa_change, meta * sizeof(double)));
+    HHG_CUDA(ctx, grow(ctx->kappa_j, (size_t)n_samples * sizeof(double)));
+    double *dT = static_cast<double *>(ctx->kappa_T.p);
+    hhg::KappaItem *ditems = static_cast<hhg::KappaItem *>(ctx->kappa_items.p);
+    double *dchange = static_cast<double *>(ctx->kappa_change.p);
+    double *dj = static_cast<double *>(ctx->kappa_j.p);
+    HHG_CUDA(ctx, cudaMemsetAsync(dT, 0, (size_t)n_total * n_samples * sizeof(double), s));
 
     hhg_kappa_stats qsum{};
     qsum.splits = (int32_t)n_total;
@@ -2121,10 +2146,41 @@ hhg_status dirac_quadrature(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_
     for (long long i = 0; i < n_total; ++i) active[(size_t)i] = i;
     std::vector<hhg::KappaItem> items;
     std::vector<double> change;
+    // the item of split `id` at `level`: its nodes' rows start at row0
+    auto make_item = [&](long long id, int level, long long row0) {
+        const KappaSplit &x = sp[(size_t)id];
+        hhg::KappaItem it{};
+        it.k_z = kz[x.slice];
+        it.a = x.a;
+        it.panels = (long long)q->n_kappa << level;
+        it.h = x.H / (double)it.panels;
+        it.level = level;
+        it.split = (int)id;
+        it.row0 = row0;
+        if (level == 0) {
+            // kappa = 0 (the first node of a slice) is left out
+            it.first = ref_is_zero(x.a) ? 1 : 0;
+            it.stride = 1;
+            it.n = q->n_kappa + 1 - it.first;
+        } else {
+            it.first = 1;
+            it.stride = 2;
+            it.n = (int)((long long)q->n_kappa << (level - 1));
+        }
+        return it;
+    };
+    std::vector<hhg::KappaItem> lo, hi;
     while (!active.empty()) {
-        ++qsum.rounds;
+        // every split needs its first trapezoid and one halving before the
+        // convergence test, so the first round integrates both levels in one
+        // launch (twice the trajectories in flight)
+        const bool both = sp[(size_t)active[0]].level == 0 && max_h >= 1;
+        qsum.rounds += both ? 2 : 1;
+        auto nodes = [&](const KappaSplit &x) {
+            return kappa_nodes(x, q->n_kappa) + (both ? (long long)q->n_kappa : 0);
+        };
         long long round_rows = 0;
-        for (long long i : active) round_rows += kappa_nodes(sp[(size_t)i], q->n_kappa);
+        for (long long i : active) round_rows += nodes(sp[(size_t)i]);
         const long long want = std::min(limit, round_rows);
         if (want > cap) {
             // grow the k table and the per-trajectory sample buffer
@@ -2140,43 +2196,35 @@ hhg_status dirac_quadrature(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_
         size_t next = 0;
         while (next < active.size()) {
             // one launch: as many active splits as fit in `cap` rows; the rows
-            // are built on the device from the splits' items
-            items.clear();
+            // are built on the device from the splits' items (the first
+            // round: all level-0 items, then all level-1 items)
+            lo.clear();
+            hi.clear();
             long long n_rows = 0;
             const size_t first = next;
             while (next < active.size()) {
-                const KappaSplit &x = sp[(size_t)active[next]];
-                const long long nn = kappa_nodes(x, q->n_kappa);
+                const long long id = active[next];
+                const long long nn = nodes(sp[(size_t)id]);
                 if (next > first && n_rows + nn > cap) break;
-                hhg::KappaItem it{};
-                it.k_z = kz[x.slice];
-                it.a = x.a;
-                it.panels = (long long)q->n_kappa << x.level;
-                it.h = x.H / (double)it.panels;
-                it.level = x.level;
-                it.split = (int)active[next];
-                it.row0 = n_rows;
-                if (x.level == 0) {
-                    // kappa = 0 (the first node of a slice) is left out
-                    it.first = ref_is_zero(x.a) ? 1 : 0;
-                    it.stride = 1;
-                    it.n = (int)(nn - it.first);
-                } else {
-                    it.first = 1;
-                    it.stride = 2;
-                    it.n = (int)nn;
-                }
-                n_rows += it.n;
-                items.push_back(it);
+                lo.push_back(make_item(id, sp[(size_t)id].level, 0));
+                if (both) hi.push_back(make_item(id, 1, 0));
+                n_rows += nn;
                 ++next;
             }
-            const int nb = (int)items.size();
-            HHG_CUDA(ctx, cudaMemcpyAsync(ditems.p, items.data(), nb * sizeof(hhg::KappaItem),
+            items.assign(lo.begin(), lo.end());
+            items.insert(items.end(), hi.begin(), hi.end());
+            n_rows = 0;
+            for (hhg::KappaItem &it : items) {
+                it.row0 = n_rows;
+                n_rows += it.n;
+            }
+            const int nb = (int)items.size(), n_lo = (int)lo.size();
+            HHG_CUDA(ctx, cudaMemcpyAsync(ditems, items.data(), nb * sizeof(hhg::KappaItem),
                                           cudaMemcpyHostToDevice, s));
             if (n_rows > 0) {
                 const long long blocks = std::min<long long>((n_rows + 255) / 256, 65536);
                 hhg::kappa_rows_kernel<<<(unsigned)blocks, 256, 0, s>>>(
-                    ditems.as<hhg::KappaItem>(), nb, n_rows, sys->beta, sys->fermi_energy, pl->d_ktab);
+                    ditems, nb, n_rows, sys->beta, sys->fermi_energy, pl->d_ktab);
                 HHG_CUDA(ctx, cudaGetLastError());
                 pl->n_k = n_rows;
                 pl->tiles_per_item = 1;
@@ -2186,10 +2234,17 @@ hhg_status dirac_quadrature(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_
                 pl->grid = (int)std::max(1LL, std::min((long long)std::max(occ, 1) * ctx->sm_count, need));
                 if ((st = enqueue_integration(pl, s, true)) != HHG_OK) return st;
             }
-            hhg::kappa_round_kernel<<<nb, hhg::kKappaThreads, 0, s>>>(
-                pl->d_kout, std::max(n_rows, 1LL), n_samples, ditems.as<hhg::KappaItem>(),
-                dT.as<double>(), dchange.as<double>());
+            // level-0 updates first; the level-1 ones (first round) read them
+            hhg::kappa_round_kernel<<<n_lo, hhg::kKappaThreads, 0, s>>>(
+                pl->d_kout, std::max(n_rows, 1LL), n_samples, ditems,
+                dT, dchange);
             HHG_CUDA(ctx, cudaGetLastError());
+            if (nb > n_lo) {
+                hhg::kappa_round_kernel<<<nb - n_lo, hhg::kKappaThreads, 0, s>>>(
+                    pl->d_kout, std::max(n_rows, 1LL), n_samples, ditems + n_lo,
+                    dT, dchange + n_lo);
+                HHG_CUDA(ctx, cudaGetLastError());
+            }
             if (n_rows > 0) {
                 hhg_stats sc{};
                 st = hhg_plan_fetch(pl, nullptr, &sc);
@@ -2210,12 +2265,14 @@ hhg_status dirac_quadrature(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_
             // the context stream does not synchronise with the legacy stream:
             // copies are ordered on it
             change.resize(nb);
-            HHG_CUDA(ctx, cudaMemcpyAsync(change.data(), dchange.p, nb * sizeof(double),
+            HHG_CUDA(ctx, cudaMemcpyAsync(change.data(), dchange, nb * sizeof(double),
                                           cudaMemcpyDeviceToHost, s));
             HHG_CUDA(ctx, cudaStreamSynchronize(s));
-            // convergence: the change of a halving below the threshold
-            for (int b = 0; b < nb; ++b) {
+            // convergence: the change of a halving below the threshold (each
+            // split's last item of the launch)
+            for (int b = (nb > n_lo ? n_lo : 0); b < nb; ++b) {
                 KappaSplit &x = sp[(size_t)items[b].split];
+                x.level = items[b].level;
                 qsum.max_level = std::max(qsum.max_level, x.level);
                 if (x.level > 0 && change[b] < q->threshold) {
                     x.done = true;
@@ -2234,9 +2291,9 @@ hhg_status dirac_quadrature(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_
     }
     const int threads = 256;
     hhg::kappa_sum_kernel<<<(n_samples + threads - 1) / threads, threads, 0, s>>>(
-        dT.as<double>(), n_slices, q->n_splits, n_samples, dz, dj.as<double>());
+        dT, n_slices, q->n_splits, n_samples, dz, dj);
     HHG_CUDA(ctx, cudaGetLastError());
-    HHG_CUDA(ctx, cudaMemcpyAsync(j_out, dj.p, (size_t)n_samples * sizeof(double),
+    HHG_CUDA(ctx, cudaMemcpyAsync(j_out, dj, (size_t)n_samples * sizeof(double),
                                   cudaMemcpyDeviceToHost, s));
     HHG_CUDA(ctx, cudaStreamSynchronize(s));
     if (qs) *qs = qsum;

@@ -286,7 +286,8 @@ typedef struct hhg_kappa_quad {
 
 typedef struct hhg_kappa_stats {
     int64_t trajectories;  /* (k_z, kappa) nodes integrated over all rounds */
-    int32_t rounds;        /* integration rounds, the first trapezoids included */
+    int32_t rounds;        /* refinement levels evaluated, the first trapezoids included
+                              (the first two share one launch) */
     int32_t splits;        /* k_z slices x n_splits */
     int32_t unconverged;   /* splits still at or above the threshold after max_halvings */
     int32_t max_level;     /* most halvings any split took */

@@ -133,3 +133,25 @@ def test_refusals(engine):
         with pytest.raises(api.HHGError) as ei:
             engine.dirac_current_density(sys, pulse, q, opts)
         assert ei.value.status == status, (ei.value, status)
+
+
+def test_repeated_calls_reuse_state_exactly(engine):
+    # the context keeps the quadrature's plan and buffers between calls; a
+    # different quadrature, a different pulse and a return to the first
+    # give the same results as fresh calls
+    sys = _system()
+    p1, p2 = api.cosine_pulse(0.6, 1, 256), api.cosine_pulse(0.4, 1, 128)
+    q1 = api.kappa_quad(2.5, 8, n_kappa=4, threshold=1e-5, n_splits=5, max_halvings=8)
+    q2 = api.kappa_quad(2.0, 12, n_kappa=6, threshold=1e-6, n_splits=7)
+    a, qa, _ = engine.dirac_current_density(sys, p1, q1)
+    b, qb, _ = engine.dirac_current_density(sys, p1, q2)
+    c, _, _ = engine.dirac_current_density(sys, p2, q1)
+    a2, qa2, _ = engine.dirac_current_density(sys, p1, q1)
+    assert np.array_equal(a, a2) and qa.as_dict() == qa2.as_dict()
+    fresh = api.Engine(0)
+    try:
+        for (p, q, want) in ((p1, q2, b), (p2, q1, c)):
+            j, _, _ = fresh.dirac_current_density(sys, p, q)
+            assert np.array_equal(j, want)
+    finally:
+        fresh.close()
