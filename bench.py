@@ -468,12 +468,14 @@ def our_arm(args, wl_name):
 
 
 # The Dirac workload's unit is one k.interval of the closed-form Magnus step
-# (DiracSystem::time_evolution_magnus): 24 cross products (216 flops), the
-# 13 series terms (78), the first-order term, moments and setup (~30) and the
-# rotation S <- exp(Omega) S (~75): ~400 FP64 flops, plus sqrt, sincos and two
-# divisions (special operations).
-MAGNUS_FLOPS_PER_KINTERVAL = 400
-MAGNUS_SPECIAL_OPS = 4
+# (DiracSystem::time_evolution_magnus), counted on the plane/axis form the
+# kernel evaluates (only nonzero components): moments and the plane vectors
+# (~18 flops), the three first-level cross products (9), their nested
+# products and the 13 series terms (~86), the rotation S <- exp(Omega) S
+# (~75) and the weighted sample (1): ~190 FP64 flops, plus sqrt, sincos and
+# three divisions (special operations).
+MAGNUS_FLOPS_PER_KINTERVAL = 190
+MAGNUS_SPECIAL_OPS = 5
 
 
 class DiracCpuBaseline:
@@ -623,8 +625,10 @@ def dirac_arm(args):
         torch.distributed.barrier()
     quad_s, e2e_s, kern_ms, kint, launches = 0.0, 0.0, 0.0, 0, 0
     qs = st = None
+    per_step = []
     for _ in range(args.steps):
         a, b, qs, st = step()
+        per_step.append((1e3 * a, 1e3 * b, st.kernel_ms))
         quad_s += a
         e2e_s += b
         kern_ms += st.kernel_ms
@@ -664,6 +668,9 @@ def dirac_arm(args):
                      "alg_flops_per_k_interval": MAGNUS_FLOPS_PER_KINTERVAL,
                      "special_ops_per_k_interval": MAGNUS_SPECIAL_OPS},
         "clocks": clocks,
+        "timing": {"quadrature_ms": [round(a, 3) for a, _, _ in per_step],
+                   "with_spectrum_ms": [round(b, 3) for _, b, _ in per_step],
+                   "integration_kernel_ms": [round(k, 3) for _, _, k in per_step]},
         "e2e": {"value": ws * args.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": int(8 * n_s + 3 * 8 * n_fft),
                 "path": "Engine.dirac_current_density + Engine.spectrum, host buffers, wall "

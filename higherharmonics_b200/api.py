@@ -147,10 +147,10 @@ class KappaQuad(ctypes.Structure):
 
 
 class KappaStats(ctypes.Structure):
-    _fields_ = [("trajectories", ctypes.c_int64), ("rounds", ctypes.c_int32),
-                ("splits", ctypes.c_int32), ("unconverged", ctypes.c_int32),
-                ("max_level", ctypes.c_int32), ("launches", ctypes.c_int32),
-                ("reserved", ctypes.c_int32)]
+    _fields_ = [("trajectories", ctypes.c_int64), ("speculative", ctypes.c_int64),
+                ("rounds", ctypes.c_int32), ("splits", ctypes.c_int32),
+                ("unconverged", ctypes.c_int32), ("max_level", ctypes.c_int32),
+                ("launches", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
     def as_dict(self) -> dict:
         return {n: getattr(self, n) for n, _ in self._fields_}

@@ -1035,70 +1035,52 @@ __device__ __forceinline__ void rotate(const double *w, double *S) {
 // commutator is a nested cross product; (a, b, c) of the reference's Omega
 // are (-w_2, w_1, -w_0), and U = exp(Omega) in the reference's closed form
 // (MagnusMatrix.cpp:59-75).
-__device__ __forceinline__ void cross3(const double *a, const double *b, double *o) {
-    o[0] = a[1] * b[2] - a[2] * b[1];
-    o[1] = a[2] * b[0] - a[0] * b[2];
-    o[2] = a[0] * b[1] - a[1] * b[0];
-}
+//
+// Every m_q of the series lies in the x-z plane (A_k has no y component and
+// h is along z), the cross product of two plane vectors lies along y, and
+// the cross product of a plane vector with a y vector lies in the plane
+// again; the nested cross products below are therefore evaluated on (x, z)
+// pairs and y scalars, forming none of the products with structural zeros
+// (which IEEE arithmetic would otherwise have to compute).
+struct XZ {
+    double x, z;
+};
+// (u x v)_y of two plane vectors
+__device__ __forceinline__ double xz_cross(XZ u, XZ v) { return u.z * v.x - u.x * v.z; }
+// u x (0, y, 0)
+__device__ __forceinline__ XZ xz_cross_y(XZ u, double y) { return {-u.z * y, u.x * y}; }
+// (0, y, 0) x u
+__device__ __forceinline__ XZ y_cross_xz(double y, XZ u) { return {y * u.z, -y * u.x}; }
 
 __device__ __forceinline__ void dirac_magnus_step(double k_z, double kappa, double mk, double dt,
                                                   const double *mom, double *S) {
     const double inv = 1.0 / mk;
     const double cf0 = mom[0] * inv, cf1 = mom[1] * inv, cf2 = mom[2] * inv, cf3 = mom[3] * inv;
-    const double ks = 2.0 * mk * dt, kap = 2.0 * kappa * dt, kzs = 2.0 * k_z * dt;
-    const double av[3] = {kap, 0.0, -kzs};
-    double m1[3], m2[3], m3[3], m4[3];
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-        m1[i] = (i == 2 ? ks : 0.0) + cf0 * av[i];
-        m2[i] = cf1 * av[i];
-        m3[i] = cf2 * av[i];
-        m4[i] = cf3 * av[i];
-    }
-    double c12[3], c13[3], c14[3], c112[3], c113[3], t1[3], t2[3], t3[3], w[3];
-    cross3(m1, m2, c12);
-    cross3(m1, m3, c13);
-    cross3(m1, m4, c14);
-    cross3(m1, c12, c112);
-    cross3(m1, c13, c113);
-#pragma unroll
-    for (int i = 0; i < 3; ++i) w[i] = m1[i] - c12[i] / 6.0;
-#define HHG_W(coef, v)                                  \
-    _Pragma("unroll") for (int i = 0; i < 3; ++i) w[i] += (coef) * (v)[i];
-    cross3(m2, c12, t1);
-    HHG_W(-1.0 / 60.0, t1)
-    cross3(m1, c112, t1);
-    HHG_W(1.0 / 360.0, t1)
-    cross3(m2, c14, t1);
-    HHG_W(1.0 / 140.0, t1)
-    cross3(m3, c13, t1);
-    HHG_W(-1.0 / 420.0, t1)
-    cross3(m4, c12, t1);
-    HHG_W(-1.0 / 210.0, t1)
-    cross3(m1, c14, t2);
-    cross3(m1, t2, t1);
-    HHG_W(-1.0 / 840.0, t1)
-    cross3(m2, c113, t1);
-    HHG_W(1.0 / 504.0, t1)
-    cross3(m2, c12, t2);
-    cross3(m2, t2, t1);
-    HHG_W(-1.0 / 840.0, t1)
-    cross3(m3, c112, t1);
-    HHG_W(1.0 / 2520.0, t1)
-    cross3(m1, c113, t2);
-    cross3(m1, t2, t1);
-    HHG_W(-1.0 / 2520.0, t1)
-    cross3(c12, c112, t1);
-    HHG_W(-1.0 / 7560.0, t1)
-    cross3(m1, c112, t2);
-    cross3(m2, t2, t1);
-    HHG_W(1.0 / 2520.0, t1)
-    cross3(m1, c112, t3);
-    cross3(m1, t3, t2);
-    cross3(m1, t2, t1);
-    HHG_W(-1.0 / 15120.0, t1)
-#undef HHG_W
-    const double a = -w[2], b = w[1], c = -w[0];
+    const double ks = 2.0 * mk * dt, kap = 2.0 * kappa * dt, nkzs = -(2.0 * k_z * dt);
+    const XZ m1{cf0 * kap, ks + cf0 * nkzs};
+    const XZ m2{cf1 * kap, cf1 * nkzs}, m3{cf2 * kap, cf2 * nkzs}, m4{cf3 * kap, cf3 * nkzs};
+    const double c12 = xz_cross(m1, m2), c13 = xz_cross(m1, m3), c14 = xz_cross(m1, m4);
+    const XZ c112 = xz_cross_y(m1, c12), c113 = xz_cross_y(m1, c13);
+    double wx = m1.x, wy = -(c12 / 6.0), wz = m1.z;
+    auto plane = [&](double coef, XZ t) {
+        wx += coef * t.x;
+        wz += coef * t.z;
+    };
+    plane(-1.0 / 60.0, xz_cross_y(m2, c12));
+    const double y112 = xz_cross(m1, c112);
+    wy += (1.0 / 360.0) * y112;
+    plane(1.0 / 140.0, xz_cross_y(m2, c14));
+    plane(-1.0 / 420.0, xz_cross_y(m3, c13));
+    plane(-1.0 / 210.0, xz_cross_y(m4, c12));
+    wy += (-1.0 / 840.0) * xz_cross(m1, xz_cross_y(m1, c14));
+    wy += (1.0 / 504.0) * xz_cross(m2, c113);
+    wy += (-1.0 / 840.0) * xz_cross(m2, xz_cross_y(m2, c12));
+    wy += (1.0 / 2520.0) * xz_cross(m3, c112);
+    plane(-1.0 / 2520.0, xz_cross_y(m1, xz_cross(m1, c113)));
+    plane(-1.0 / 7560.0, y_cross_xz(c12, c112));
+    plane(1.0 / 2520.0, xz_cross_y(m2, y112));
+    wy += (-1.0 / 15120.0) * xz_cross(m1, xz_cross_y(m1, y112));
+    const double a = -wz, b = wy, c = -wx;
     const double n2 = a * a + b * b + c * c;
     const double ev = sqrt(n2);
     double y, x;
@@ -1279,7 +1261,8 @@ constexpr double kCoarsen = 1.0 / 600.0;
 // OUT 3: every trajectory's band occupations at every sample, kout[i][k][2]
 //   (PiFlux::evolve_occupation_numbers, PiFlux.cpp:222-318);
 // OUT 4: every trajectory's weighted current w_k vertex(S) at every sample,
-//   kout[i][k] (the kappa integrand of DiracSystem::compute_current_density,
+//   kout[i][k], sample-major (a warp's store is one 256-byte run) (the kappa
+//   integrand of DiracSystem::compute_current_density,
 //   DiracSystem.cpp:300-311; dead trajectories give 0 and are counted).
 // OUT 1-3 are built for the PiFlux models only, OUT 4 for the Dirac-3D ones.
 template <int M, int D, typename R, int STEPPER, int PROPOSER, int OUT = 0>
@@ -1822,9 +1805,12 @@ static __global__ void kappa_rows_kernel(const KappaItem *__restrict__ items, in
 // One refinement round: split items[b] updates its trapezoid estimate
 //   T[split][i] <- scale T + h sum_rows contrib[i][row]
 // (scale 0 on the first round, 1/2 after a halving) and writes change[b] =
-// max_i |T_new - T_old| (NaN if any sample is NaN).  Rows are summed
-// lane-strided, then by the warp butterfly: a fixed order.
+// max_i |T_new - T_old| (NaN if any sample is NaN).  One CTA per split, one
+// thread per sample: each thread adds the split's rows in order (its own
+// contiguous run, kept in L1 while it is read), a fixed order.
 constexpr int kKappaThreads = 256;
+__device__ __forceinline__ double nan_max(double a, double b) { return (b > a || b != b) ? b : a; }
+
 static __global__ void __launch_bounds__(kKappaThreads)
 kappa_round_kernel(const double *__restrict__ contrib, long long n_rows, int n_samples,
                    const KappaItem *__restrict__ items, double *__restrict__ T,
@@ -1834,45 +1820,53 @@ kappa_round_kernel(const double *__restrict__ contrib, long long n_rows, int n_s
     const KappaItem &it = items[blockIdx.x];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     double *Ts = T + (size_t)it.split * n_samples;
-    const long long r0 = it.row0, r1 = it.row0 + it.n;
+    const double *c0 = contrib + it.row0;
+    const int n = it.n;
     const double sc = it.level == 0 ? 0.0 : 0.5, hb = it.h;
     double dmax = 0.0;
-    for (int i = warp; i < n_samples; i += kWarps) {
-        const double *c = contrib + (size_t)i * n_rows;
+    for (int i = threadIdx.x; i < n_samples; i += kKappaThreads) {
+        const double *c = c0 + (size_t)i * n_rows;
         double acc = 0.0;
-        for (long long r = r0 + lane; r < r1; r += 32) acc += c[r];
-        acc = warp_sum(acc);
-        if (lane == 0) {
-            const double old = Ts[i];
-            // two rounded products and a rounded sum (no contraction)
-            const double v = __dadd_rn(__dmul_rn(sc, old), __dmul_rn(hb, acc));
-            Ts[i] = v;
-            const double d = fabs(v - old);
-            if (d > dmax || d != d) dmax = d;
-        }
+#pragma unroll 4
+        for (int r = 0; r < n; ++r) acc += __ldg(c + r);
+        const double old = Ts[i];
+        // two rounded products and a rounded sum (no contraction)
+        const double v = __dadd_rn(__dmul_rn(sc, old), __dmul_rn(hb, acc));
+        Ts[i] = v;
+        dmax = nan_max(dmax, fabs(v - old));
     }
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) dmax = nan_max(dmax, __shfl_xor_sync(kFull, dmax, o));
     if (lane == 0) wmax[warp] = dmax;
     __syncthreads();
     if (threadIdx.x == 0) {
         double m = 0.0;
-        for (int w = 0; w < kWarps; ++w)
-            if (wmax[w] > m || wmax[w] != wmax[w]) m = wmax[w];
+        for (int w = 0; w < kWarps; ++w) m = nan_max(m, wmax[w]);
         change[blockIdx.x] = m;
     }
 }
 
 // j[i] = dz * sum over slices (in order) of the slice's sum over its splits
-// (in order) of T[slice][split][i] (DiracSystem.cpp:313-321).
-static __global__ void kappa_sum_kernel(const double *__restrict__ T, int n_slices, int n_splits,
+// (in order) of T[slice][split][i] (DiracSystem.cpp:313-321), in two passes:
+// the slices' sums in parallel (grid y = slice), then the slices in order.
+static __global__ void kappa_slice_kernel(const double *__restrict__ T, int n_splits,
+                                          int n_samples, double *__restrict__ slice_sum) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_samples) return;
+    const size_t z = blockIdx.y;
+    const double *t = T + z * n_splits * (size_t)n_samples + i;
+    double sl = 0.0;
+#pragma unroll 4
+    for (int s = 0; s < n_splits; ++s) sl = __dadd_rn(sl, t[(size_t)s * n_samples]);
+    slice_sum[z * n_samples + i] = sl;
+}
+
+static __global__ void kappa_sum_kernel(const double *__restrict__ slice_sum, int n_slices,
                                         int n_samples, double dz, double *__restrict__ j) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n_samples) return;
     double acc = 0.0;
-    for (int z = 0; z < n_slices; ++z) {
-        double sl = 0.0;
-        for (int s = 0; s < n_splits; ++s) sl = __dadd_rn(sl, T[((size_t)z * n_splits + s) * n_samples + i]);
-        acc = __dadd_rn(acc, sl);
-    }
+    for (int z = 0; z < n_slices; ++z) acc = __dadd_rn(acc, slice_sum[(size_t)z * n_samples + i]);
     j[i] = acc * dz;
 }
 

@@ -41,7 +41,7 @@ struct hhg_ctx {
     struct Grow {
         void *p = nullptr;
         size_t bytes = 0;
-    } kappa_T, kappa_items, kappa_change, kappa_j;
+    } kappa_T, kappa_items, kappa_change, kappa_j, kappa_slice;
 };
 
 struct hhg_plan {
@@ -909,7 +909,8 @@ void hhg_gpu_destroy(hhg_ctx *c) {
     for (auto &kv : c->plan_cache) hhg_plan_destroy(kv.second);
     c->plan_cache.clear();
     if (c->kappa_plan) hhg_plan_destroy(c->kappa_plan);
-    for (hhg_ctx::Grow *g : {&c->kappa_T, &c->kappa_items, &c->kappa_change, &c->kappa_j}) cudaFree(g->p);
+    for (hhg_ctx::Grow *g : {&c->kappa_T, &c->kappa_items, &c->kappa_change, &c->kappa_j, &c->kappa_slice})
+        cudaFree(g->p);
     for (auto &kv : c->fft_plans) cufftDestroy(kv.second);
     cudaFree(c->d_x);
     cudaFree(c->d_F);
@@ -2010,7 +2011,11 @@ hhg_status hhg_gpu_split_current(hhg_ctx *ctx, const hhg_system_desc *sys,
 namespace {
 
 constexpr int kDefaultHalvings = 12;
-constexpr double kKappaChunkBytes = 4.0 * (1 << 30);  // per-trajectory samples of one launch
+constexpr int kKappaLookahead = 8;  // levels integrated ahead of the convergence test
+// per-trajectory samples of one launch: up to 16 GiB, at most half the free
+// device memory (plus what the context holds already), at least 1 GiB
+constexpr double kKappaChunkBytes = 16.0 * (1 << 30);
+constexpr double kKappaChunkMinBytes = 1.0 * (1 << 30);
 
 struct KappaSplit {
     int slice;     // index of the k_z slice
@@ -2019,13 +2024,6 @@ struct KappaSplit {
     bool done;
 };
 
-// Nodes a split integrates at its current level: level 0 the n_kappa + 1
-// trapezoid nodes a + m H/n_kappa, level L > 0 the midpoints a + m
-// H/(n_kappa 2^L), m odd (hhg::kappa_rows_kernel builds their rows).
-long long kappa_nodes(const KappaSplit &sp, int n_kappa) {
-    if (sp.level == 0) return n_kappa + 1;
-    return (long long)n_kappa << (sp.level - 1);
-}
 
 hhg_status dirac_quadrature(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_pulse_desc *pulse,
                             const hhg_kappa_quad *q, const hhg_solver_opts *opts, double *j_out,
@@ -2075,7 +2073,11 @@ hhg_status dirac_quadrature(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_
     // (the first round holds a split's n_kappa + 1 trapezoid nodes and its
     // n_kappa first midpoints)
     const long long biggest = std::max<long long>(2LL * q->n_kappa + 1, (long long)q->n_kappa << (max_h - 1));
-    const long long budget = (long long)(kKappaChunkBytes / (8.0 * n_samples));
+    size_t free_b = 0, total_b = 0;
+    HHG_CUDA(ctx, cudaMemGetInfo(&free_b, &total_b));
+    const double held = 8.0 * (double)ctx->kappa_cap * n_samples;
+    const double chunk = std::min(kKappaChunkBytes, std::max(kKappaChunkMinBytes, 0.5 * ((double)free_b + held)));
+    const long long budget = (long long)(chunk / (8.0 * n_samples));
     const long long limit = std::max(biggest, std::max(budget, 32LL));
 
     // the plan: pulse staging and launch state, built on one placeholder row
@@ -2127,15 +2129,18 @@ hhg_status dirac_quadrature(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_
         if (e == cudaSuccess) b.bytes = bytes;
         return e;
     };
-    const size_t meta = (size_t)std::min<long long>(2 * n_total, limit);  // items per launch <= rows
+    // items per launch <= rows per launch, and <= splits x levels per launch
+    const size_t meta = (size_t)std::min<long long>((kKappaLookahead + 2) * n_total, limit);
     HHG_CUDA(ctx, grow(ctx->kappa_T, (size_t)n_total * n_samples * sizeof(double)));
     HHG_CUDA(ctx, grow(ctx->kappa_items, meta * sizeof(hhg::KappaItem)));
     HHG_CUDA(ctx, grow(ctx->kappa_change, meta * sizeof(double)));
     HHG_CUDA(ctx, grow(ctx->kappa_j, (size_t)n_samples * sizeof(double)));
+    HHG_CUDA(ctx, grow(ctx->kappa_slice, (size_t)n_slices * n_samples * sizeof(double)));
     double *dT = static_cast<double *>(ctx->kappa_T.p);
     hhg::KappaItem *ditems = static_cast<hhg::KappaItem *>(ctx->kappa_items.p);
     double *dchange = static_cast<double *>(ctx->kappa_change.p);
     double *dj = static_cast<double *>(ctx->kappa_j.p);
+    double *dslice = static_cast<double *>(ctx->kappa_slice.p);
     HHG_CUDA(ctx, cudaMemsetAsync(dT, 0, (size_t)n_total * n_samples * sizeof(double), s));
 
     hhg_kappa_stats qsum{};
@@ -2169,18 +2174,32 @@ hhg_status dirac_quadrature(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_
         }
         return it;
     };
-    std::vector<hhg::KappaItem> lo, hi;
+    // lookahead: a launch of a quarter of the resident lanes or fewer is
+    // latency-bound (each trajectory is a serial chain over all intervals;
+    // measured: such a launch takes as long as one trajectory alone), so
+    // further levels of the same splits ride along while the launch stays that
+    // small; the estimates still take the levels one by one with the
+    // convergence test in between, and rows of levels a split never reaches
+    // are discarded
+    const long long resident = (long long)occ * ctx->sm_count * hhg::kBlockThreads / 4;
+    std::vector<std::vector<hhg::KappaItem>> by_level;
+    std::vector<hhg::KappaItem> todo;
     while (!active.empty()) {
-        // every split needs its first trapezoid and one halving before the
-        // convergence test, so the first round integrates both levels in one
-        // launch (twice the trajectories in flight)
-        const bool both = sp[(size_t)active[0]].level == 0 && max_h >= 1;
-        qsum.rounds += both ? 2 : 1;
-        auto nodes = [&](const KappaSplit &x) {
-            return kappa_nodes(x, q->n_kappa) + (both ? (long long)q->n_kappa : 0);
+        const int L = sp[(size_t)active[0]].level;  // every active split is at L
+        auto level_nodes = [&](int l) {
+            return l == 0 ? (long long)q->n_kappa + 1 : (long long)q->n_kappa << (l - 1);
         };
-        long long round_rows = 0;
-        for (long long i : active) round_rows += nodes(sp[(size_t)i]);
+        // the first trapezoid and the first halving always go together
+        int last = (L == 0) ? 1 : L;
+        long long per_split = 0;
+        for (int l = L; l <= last; ++l) per_split += level_nodes(l);
+        while (last < max_h && last - L < kKappaLookahead && per_split + level_nodes(last + 1) <= limit &&
+               (long long)active.size() * (per_split + level_nodes(last + 1)) <= resident) {
+            ++last;
+            per_split += level_nodes(last);
+        }
+        const int n_lv = last - L + 1;
+        const long long round_rows = (long long)active.size() * per_split;
         const long long want = std::min(limit, round_rows);
         if (want > cap) {
             // grow the k table and the per-trajectory sample buffer
@@ -2195,30 +2214,32 @@ hhg_status dirac_quadrature(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_
         }
         size_t next = 0;
         while (next < active.size()) {
-            // one launch: as many active splits as fit in `cap` rows; the rows
-            // are built on the device from the splits' items (the first
-            // round: all level-0 items, then all level-1 items)
-            lo.clear();
-            hi.clear();
+            // one launch: as many active splits as fit in `cap` rows, each with
+            // its levels L..last; items level-major, rows in item order, built
+            // on the device
+            by_level.assign((size_t)n_lv, {});
             long long n_rows = 0;
             const size_t first = next;
             while (next < active.size()) {
                 const long long id = active[next];
-                const long long nn = nodes(sp[(size_t)id]);
-                if (next > first && n_rows + nn > cap) break;
-                lo.push_back(make_item(id, sp[(size_t)id].level, 0));
-                if (both) hi.push_back(make_item(id, 1, 0));
-                n_rows += nn;
+                if (next > first && n_rows + per_split > cap) break;
+                for (int l = L; l <= last; ++l) by_level[(size_t)(l - L)].push_back(make_item(id, l, 0));
+                n_rows += per_split;
                 ++next;
             }
-            items.assign(lo.begin(), lo.end());
-            items.insert(items.end(), hi.begin(), hi.end());
+            items.clear();
+            for (auto &v : by_level) items.insert(items.end(), v.begin(), v.end());
             n_rows = 0;
             for (hhg::KappaItem &it : items) {
                 it.row0 = n_rows;
                 n_rows += it.n;
             }
-            const int nb = (int)items.size(), n_lo = (int)lo.size();
+            {
+                size_t k = 0;  // the row offsets back into the per-level lists
+                for (auto &v : by_level)
+                    for (hhg::KappaItem &it : v) it.row0 = items[k++].row0;
+            }
+            const int nb = (int)items.size();
             HHG_CUDA(ctx, cudaMemcpyAsync(ditems, items.data(), nb * sizeof(hhg::KappaItem),
                                           cudaMemcpyHostToDevice, s));
             if (n_rows > 0) {
@@ -2233,19 +2254,6 @@ hhg_status dirac_quadrature(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_
                 const long long need = (pl->n_items + hhg::kWarpsPerBlock - 1) / hhg::kWarpsPerBlock;
                 pl->grid = (int)std::max(1LL, std::min((long long)std::max(occ, 1) * ctx->sm_count, need));
                 if ((st = enqueue_integration(pl, s, true)) != HHG_OK) return st;
-            }
-            // level-0 updates first; the level-1 ones (first round) read them
-            hhg::kappa_round_kernel<<<n_lo, hhg::kKappaThreads, 0, s>>>(
-                pl->d_kout, std::max(n_rows, 1LL), n_samples, ditems,
-                dT, dchange);
-            HHG_CUDA(ctx, cudaGetLastError());
-            if (nb > n_lo) {
-                hhg::kappa_round_kernel<<<nb - n_lo, hhg::kKappaThreads, 0, s>>>(
-                    pl->d_kout, std::max(n_rows, 1LL), n_samples, ditems + n_lo,
-                    dT, dchange + n_lo);
-                HHG_CUDA(ctx, cudaGetLastError());
-            }
-            if (n_rows > 0) {
                 hhg_stats sc{};
                 st = hhg_plan_fetch(pl, nullptr, &sc);
                 if (st == HHG_CUDA_ERROR || st == HHG_BAD_CONFIG) return st;
@@ -2259,30 +2267,45 @@ hhg_status dirac_quadrature(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_
                 ssum.items += sc.items;
                 ssum.kernel_ms += sc.kernel_ms;
                 ssum.total_ms += sc.total_ms;
-                qsum.trajectories += n_rows;
                 ++qsum.launches;
             }
-            // the context stream does not synchronise with the legacy stream:
-            // copies are ordered on it
-            change.resize(nb);
-            HHG_CUDA(ctx, cudaMemcpyAsync(change.data(), dchange, nb * sizeof(double),
-                                          cudaMemcpyDeviceToHost, s));
-            HHG_CUDA(ctx, cudaStreamSynchronize(s));
-            // convergence: the change of a halving below the threshold (each
-            // split's last item of the launch)
-            for (int b = (nb > n_lo ? n_lo : 0); b < nb; ++b) {
-                KappaSplit &x = sp[(size_t)items[b].split];
-                x.level = items[b].level;
-                qsum.max_level = std::max(qsum.max_level, x.level);
-                if (x.level > 0 && change[b] < q->threshold) {
-                    x.done = true;
-                } else if (x.level >= max_h || std::isnan(change[b])) {
-                    x.done = true;
-                    ++qsum.unconverged;
-                } else {
-                    ++x.level;
+            long long used = 0;
+            for (int lv = 0; lv < n_lv; ++lv) {
+                // the level's items of the splits still refining
+                todo.clear();
+                for (const hhg::KappaItem &it : by_level[(size_t)lv])
+                    if (!sp[(size_t)it.split].done) todo.push_back(it);
+                if (todo.empty()) break;
+                const int nt = (int)todo.size();
+                HHG_CUDA(ctx, cudaMemcpyAsync(ditems, todo.data(), nt * sizeof(hhg::KappaItem),
+                                              cudaMemcpyHostToDevice, s));
+                hhg::kappa_round_kernel<<<nt, hhg::kKappaThreads, 0, s>>>(
+                    pl->d_kout, std::max(n_rows, 1LL), n_samples, ditems, dT, dchange);
+                HHG_CUDA(ctx, cudaGetLastError());
+                // the context stream does not synchronise with the legacy
+                // stream: copies are ordered on it
+                change.resize(nt);
+                HHG_CUDA(ctx, cudaMemcpyAsync(change.data(), dchange, nt * sizeof(double),
+                                              cudaMemcpyDeviceToHost, s));
+                HHG_CUDA(ctx, cudaStreamSynchronize(s));
+                // convergence: the change of a halving below the threshold
+                for (int b = 0; b < nt; ++b) {
+                    KappaSplit &x = sp[(size_t)todo[b].split];
+                    used += todo[b].n;
+                    x.level = todo[b].level;
+                    qsum.max_level = std::max(qsum.max_level, x.level);
+                    if (x.level > 0 && change[b] < q->threshold) {
+                        x.done = true;
+                    } else if (x.level >= max_h || std::isnan(change[b])) {
+                        x.done = true;
+                        ++qsum.unconverged;
+                    } else {
+                        ++x.level;
+                    }
                 }
             }
+            qsum.trajectories += used;
+            qsum.speculative += n_rows - used;
         }
         std::vector<long long> still;
         for (long long i : active)
@@ -2290,12 +2313,16 @@ hhg_status dirac_quadrature(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_
         active.swap(still);
     }
     const int threads = 256;
-    hhg::kappa_sum_kernel<<<(n_samples + threads - 1) / threads, threads, 0, s>>>(
-        dT, n_slices, q->n_splits, n_samples, dz, dj);
+    const unsigned sblocks = (unsigned)((n_samples + threads - 1) / threads);
+    hhg::kappa_slice_kernel<<<dim3(sblocks, (unsigned)n_slices), threads, 0, s>>>(
+        dT, q->n_splits, n_samples, dslice);
+    HHG_CUDA(ctx, cudaGetLastError());
+    hhg::kappa_sum_kernel<<<sblocks, threads, 0, s>>>(dslice, n_slices, n_samples, dz, dj);
     HHG_CUDA(ctx, cudaGetLastError());
     HHG_CUDA(ctx, cudaMemcpyAsync(j_out, dj, (size_t)n_samples * sizeof(double),
                                   cudaMemcpyDeviceToHost, s));
     HHG_CUDA(ctx, cudaStreamSynchronize(s));
+    qsum.rounds = qsum.max_level + 1;  // levels evaluated, the first trapezoids included
     if (qs) *qs = qsum;
     if (stats) *stats = ssum;
     return worst;

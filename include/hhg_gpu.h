@@ -285,13 +285,13 @@ typedef struct hhg_kappa_quad {
 } hhg_kappa_quad;
 
 typedef struct hhg_kappa_stats {
-    int64_t trajectories;  /* (k_z, kappa) nodes integrated over all rounds */
-    int32_t rounds;        /* refinement levels evaluated, the first trapezoids included
-                              (the first two share one launch) */
+    int64_t trajectories;  /* (k_z, kappa) nodes whose samples entered the estimates */
+    int64_t speculative;   /* nodes integrated ahead of a convergence test and discarded */
+    int32_t rounds;        /* refinement levels evaluated, the first trapezoids included */
     int32_t splits;        /* k_z slices x n_splits */
     int32_t unconverged;   /* splits still at or above the threshold after max_halvings */
     int32_t max_level;     /* most halvings any split took */
-    int32_t launches;      /* integration launches (a round's splits in budget-sized chunks) */
+    int32_t launches;      /* integration launches (several levels and chunks of splits) */
     int32_t reserved;
 } hhg_kappa_stats;
 

@@ -55,8 +55,8 @@ def _c_layout():
                              "total_ms"],
                "hhg_kappa_quad": ["max_k", "threshold", "n_z", "n_kappa", "n_splits",
                                   "max_halvings"],
-               "hhg_kappa_stats": ["trajectories", "rounds", "splits", "unconverged", "max_level",
-                                   "launches", "reserved"]}
+               "hhg_kappa_stats": ["trajectories", "speculative", "rounds", "splits", "unconverged",
+                                   "max_level", "launches", "reserved"]}
     src = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(){"]
     for s, fields in structs.items():
         src.append(f'printf("{s} size %zu\\n", sizeof({s}));')

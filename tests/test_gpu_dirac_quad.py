@@ -48,6 +48,9 @@ def test_magnus_parity(engine):
     # splits stop at different levels
     uniform = qs.splits * (5 + 4 * ((1 << qs.max_level) - 1))
     assert qs.max_level >= 3 and qs.trajectories < uniform
+    # a small problem: later levels are integrated ahead of the convergence
+    # test (fewer launches than levels, discarded rows), same result
+    assert qs.launches < qs.rounds and qs.speculative > 0
     assert rel_l2(j, jr) <= 1e-12, rel_l2(j, jr)
 
 
