@@ -488,9 +488,12 @@ hhg_status hhg_gpu_split_current(hhg_ctx *ctx, const hhg_system_desc *sys,
  * HHG_SYS_DIRAC3D only; opts->stepper HHG_STEPPER_DIRAC_MAGNUS (the
  * reference's coherent path, time_evolution_magnus) or HHG_STEPPER_RKF78 (the
  * sigma equation, time_evolution_sigma, and the relaxation path), FP64,
- * proposer NONE.  Every refinement round integrates its new nodes in one
- * launch; the splits' estimates stay on the device.  qstats and stats may be
- * NULL; stats sums the rounds' launches. */
+ * proposer NONE.  The new nodes of a level (of several levels, when they are
+ * few) are integrated in one launch; the splits' estimates stay on the device
+ * and take the levels one by one with the convergence test in between.  The
+ * context keeps the plan and grow-only buffers for the next call with the same
+ * system, pulse and options.  qstats and stats may be NULL; stats sums the
+ * launches. */
 hhg_status hhg_gpu_dirac_current_density(hhg_ctx *ctx, const hhg_system_desc *sys,
                                          const hhg_pulse_desc *pulse, const hhg_kappa_quad *quad,
                                          const hhg_solver_opts *opts, double *j_out,
