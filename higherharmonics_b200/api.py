@@ -143,7 +143,8 @@ class KappaQuad(ctypes.Structure):
     adaptive kappa rule of DiracSystem::compute_current_density)."""
     _fields_ = [("max_k", ctypes.c_double), ("threshold", ctypes.c_double),
                 ("n_z", ctypes.c_int32), ("n_kappa", ctypes.c_int32),
-                ("n_splits", ctypes.c_int32), ("max_halvings", ctypes.c_int32)]
+                ("n_splits", ctypes.c_int32), ("max_halvings", ctypes.c_int32),
+                ("z_first", ctypes.c_int32), ("z_count", ctypes.c_int32)]
 
 
 class KappaStats(ctypes.Structure):
@@ -157,10 +158,12 @@ class KappaStats(ctypes.Structure):
 
 
 def kappa_quad(max_k: float, n_z: int, n_kappa: int = 10, threshold: float = 1e-3,
-               n_splits: int = 100, max_halvings: int = 0) -> KappaQuad:
+               n_splits: int = 100, max_halvings: int = 0, z_first: int = 0,
+               z_count: int = 0) -> KappaQuad:
     """Defaults: the reference's DiracDispatcher (n_kappa 10, threshold 1e-3,
-    DiracDispatcher.cpp:13-14) and split_integrate<100>."""
-    return KappaQuad(max_k, threshold, n_z, n_kappa, n_splits, max_halvings)
+    DiracDispatcher.cpp:13-14) and split_integrate<100>; z_count > 0 takes the
+    slices z_first .. z_first + z_count - 1 only (one rank's block)."""
+    return KappaQuad(max_k, threshold, n_z, n_kappa, n_splits, max_halvings, z_first, z_count)
 
 
 class HHGError(RuntimeError):

@@ -2049,15 +2049,30 @@ hhg_status dirac_quadrature(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_
         return set_err(ctx, HHG_UNSUPPORTED,
                        "the Dirac quadrature runs the closed-form Magnus step or FP64 RKF78 with "
                        "the reference schedule (proposer NONE)");
+    if (pulse->n_measurements < 1 || pulse->n_measurements > (1 << 24))
+        return set_err(ctx, HHG_BAD_CONFIG, "n_measurements out of range");
     const int n_samples = pulse->n_measurements + 1;
 
     // k_z slices (DiracSystem.cpp:283, 296-299) and their splits
     const int n_z = q->n_z;
     const double dz = 2 * q->max_k / n_z;
     std::vector<double> kz;
-    for (int z = 1; z < n_z; ++z)
+    // one rank's block of the z loop (DiracSystem.cpp:288-295), or all of it
+    if (q->z_count < 0 || (q->z_count > 0 && (q->z_first < 1 || q->z_first > n_z - 1 ||
+                                              q->z_count > n_z - q->z_first)))
+        return set_err(ctx, HHG_BAD_CONFIG, "slice range outside z = 1 .. n_z - 1");
+    const int z_lo = q->z_count > 0 ? q->z_first : 1;
+    const int z_hi = q->z_count > 0 ? q->z_first + q->z_count : n_z;
+    for (int z = z_lo; z < z_hi; ++z)
         if (z != n_z / 2) kz.push_back((z - n_z / 2) * dz);
     const int n_slices = (int)kz.size();
+    if (n_slices == 0) {
+        // a block holding only the weight-0 slice z = n_z / 2
+        std::fill(j_out, j_out + pulse->n_measurements + 1, 0.0);
+        if (qs) *qs = hhg_kappa_stats{};
+        if (stats) *stats = hhg_stats{};
+        return HHG_OK;
+    }
     const long long n_total = (long long)n_slices * q->n_splits;
     if (n_total > (1LL << 28)) return set_err(ctx, HHG_BAD_CONFIG, "too many splits");
     std::vector<KappaSplit> sp((size_t)n_total);

@@ -69,3 +69,34 @@ def sharded_current_density(engine, sys, pulses, grid, opts, rank: int, world: i
         g, keep = api.grid_explicit(mine)
         j, _ = engine.current_density(sys, pulses, g, opts)
     return reduce_current(j, deterministic=deterministic, group=group)
+
+
+def dirac_z_block(n_z: int, rank: int, world: int) -> tuple[int, int]:
+    """(z_first, z_count) of `rank`'s block of the Dirac system's z loop
+    z = 1 .. n_z - 1, partitioned as the reference does under MPI
+    (DiracSystem.cpp:288-295): jobs_per_rank = ceil((n_z - 1) / n_ranks),
+    [rank jobs + 1, min(n_z, rank jobs + 1 + jobs))."""
+    jobs = (n_z - 1) // world
+    if jobs * world < n_z - 1:
+        jobs += 1
+    lo = rank * jobs + 1
+    hi = min(n_z, lo + jobs)
+    return lo, max(0, hi - lo)
+
+
+def sharded_dirac_current_density(engine, sys, pulse, quad, opts, rank: int, world: int,
+                                  deterministic: bool = True, group=None):
+    """The Dirac-3D current density with the k_z slices split over ranks:
+    this rank integrates its block of slices (Engine.dirac_current_density
+    with z_first / z_count; each block already carries the factor dz, as the
+    reference's per-rank current does) and j(t) is reduced over the group
+    (the reference's MPI_Reduce, hhg.cpp:240-246); every rank returns the full
+    current."""
+    zf, zc = dirac_z_block(quad.n_z, rank, world)
+    if zc == 0:
+        j = np.zeros(pulse.n_measurements + 1)
+    else:
+        q = api.kappa_quad(quad.max_k, quad.n_z, quad.n_kappa, quad.threshold, quad.n_splits,
+                           quad.max_halvings, z_first=zf, z_count=zc)
+        j, _, _ = engine.dirac_current_density(sys, pulse, q, opts)
+    return reduce_current(j, deterministic=deterministic, group=group)

@@ -282,6 +282,8 @@ typedef struct hhg_kappa_quad {
     int32_t n_kappa;       /* panels of a split's first trapezoid (DiracDispatcher.cpp:14: 10) */
     int32_t n_splits;      /* equal splits of the kappa range (split_integrate<100>) */
     int32_t max_halvings;  /* refinement cap per split; 0 = 12 */
+    int32_t z_first;       /* slices z_first .. z_first + z_count - 1 of z = 1 .. n_z - 1 only */
+    int32_t z_count;       /* (one rank's block, DiracSystem.cpp:288-295); 0 = all slices */
 } hhg_kappa_quad;
 
 typedef struct hhg_kappa_stats {

@@ -54,7 +54,7 @@ def _c_layout():
                              "failed_trajectories", "poly_degree", "items", "kernel_ms",
                              "total_ms"],
                "hhg_kappa_quad": ["max_k", "threshold", "n_z", "n_kappa", "n_splits",
-                                  "max_halvings"],
+                                  "max_halvings", "z_first", "z_count"],
                "hhg_kappa_stats": ["trajectories", "speculative", "rounds", "splits", "unconverged",
                                    "max_level", "launches", "reserved"]}
     src = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(){"]

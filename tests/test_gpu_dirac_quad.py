@@ -158,3 +158,28 @@ def test_repeated_calls_reuse_state_exactly(engine):
             assert np.array_equal(j, want)
     finally:
         fresh.close()
+
+
+def test_slice_blocks_add_up(engine):
+    # the reference's MPI partition of the z loop (DiracSystem.cpp:288-295):
+    # per-rank blocks, each with its factor dz, sum to the whole current
+    from higherharmonics_b200.distributed import dirac_z_block
+    sys, pulse = _system(beta=1.0, fermi=0.2), api.cosine_pulse(0.6, 1, 128)
+    base = dict(max_k=2.5, n_z=9, n_kappa=4, threshold=1e-5, n_splits=3, max_halvings=6)
+    full, qf, _ = engine.dirac_current_density(sys, pulse, api.kappa_quad(**base))
+    parts, traj = [], 0
+    for r in range(3):
+        zf, zc = dirac_z_block(9, r, 3)
+        j, q, _ = engine.dirac_current_density(sys, pulse,
+                                               api.kappa_quad(**base, z_first=zf, z_count=zc))
+        parts.append(j)
+        traj += q.trajectories
+    assert traj == qf.trajectories
+    assert np.max(np.abs(sum(parts) - full)) <= 1e-13 * np.max(np.abs(full))
+    # a block holding only the weight-0 slice z = n_z / 2
+    j0, q0, _ = engine.dirac_current_density(sys, pulse, api.kappa_quad(**base, z_first=4, z_count=1))
+    assert not j0.any() and q0.trajectories == 0
+    for zf, zc in ((0, 2), (8, 2), (3, -1)):
+        with pytest.raises(api.HHGError) as ei:
+            engine.dirac_current_density(sys, pulse, api.kappa_quad(**base, z_first=zf, z_count=zc))
+        assert ei.value.status == api.BAD_CONFIG
