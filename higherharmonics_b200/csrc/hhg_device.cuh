@@ -1247,6 +1247,113 @@ __device__ __forceinline__ void lane_controller(const KParams &P, const ModelSta
 // The mixed-precision variant (R = float) evaluates the growth/shrink factor's
 // power in FP32 (the error norm, the comparison and dt stay FP64).
 // ---------------------------------------------------------------------------
+// ---------------------------------------------------------------------------
+// Free-running lanes (the relaxation models on the reference schedule, BZ
+// sum): every lane integrates its own intervals with the per-lane controller
+// of lane_controller (the same attempts, acceptances and limits), up to
+// kFreeWindow intervals ahead of the warp's slowest lane, reading its
+// interval's interpolants from the staging table, and leaves its weighted
+// sample in a per-warp ring.  A sample is reduced with the same warp
+// butterfly as the interval-synchronous loop once every lane has passed it,
+// so the result is the same; lanes no longer idle at every interval end while
+// the lane with the most steps finishes.  The slowest lane is never held back
+// by the window and every interval is bounded by max_attempts, so the loop
+// ends.
+// ---------------------------------------------------------------------------
+constexpr int kFreeWindow = 8;
+
+// Sample i's warp sum: lane i mod 32 keeps it; every 32 samples (and at the
+// last) one coalesced store (or accumulation, for later k tiles of the item).
+__device__ __forceinline__ void keep_sample(int i, double sum, int N, int sub, int lane,
+                                            double &held, double *prow) {
+    if (lane == (i & 31)) held = sum;
+    if ((i & 31) == 31 || i == N) {
+        const int base = i & ~31;
+        if (base + lane <= N) {
+            if (sub == 0)
+                prow[base + lane] = held;
+            else
+                prow[base + lane] += held;
+        }
+    }
+}
+
+template <int M, int D>
+__device__ void integrate_free(const KParams &P, const ModelState<M, double> &ms,
+                               const double *coef, double dt0, double tb, double te, int N,
+                               double w, bool &dead, double *S, double &held, double *prow,
+                               int sub, int lane, double *ring,
+                               unsigned long long &attempts_out,
+                               unsigned long long &rejects_out) {
+    constexpr int NF = Traits<M>::NF;
+    constexpr int SLOT = slot_doubles(NF, D);
+    int li = 1;  // the sample this lane integrates towards (interval li - 1)
+    double t = coef[0], t1 = coef[1], dt = dt0;
+    int fails = 0, attempts = 0;
+    int base = 1;  // the next sample to reduce
+    while (base <= N) {
+        if (li <= N && li - base < kFreeWindow) {
+            const double *gs = coef + (size_t)(li - 1) * SLOT;
+            bool finished = dead;
+            if (!dead) {
+                if ((t + dt) - t1 > kDblEps) dt = t1 - t;
+                const PolyEval<NF, D, double> poly{gs, tb, te};
+                double xn[3], e[3], k0[3];
+                rkf78_attempt<M, NF, double>(ms, poly, t, dt, S, xn, e, k0);
+                ++attempts;
+                ++attempts_out;
+                const double dt_used = dt;
+                if (control<false>(P, S, e, k0, dt)) {
+                    t += dt_used;
+                    S[0] = xn[0];
+                    S[1] = xn[1];
+                    S[2] = xn[2];
+                    fails = 0;
+                    if (!(t1 - t > kDblEps)) finished = true;
+                } else {
+                    ++rejects_out;
+                    if (++fails >= P.max_failed) {
+                        dead = true;
+                        finished = true;
+                        atomicAdd(P.counters + 3, 1ull);
+                        atomicMax(P.status, 2);
+                    }
+                }
+                if (!finished && attempts >= P.max_attempts) {
+                    dead = true;
+                    finished = true;
+                    atomicAdd(P.counters + 3, 1ull);
+                    atomicMax(P.status, 2);
+                }
+                if (finished && !dead && !(isfinite(S[0]) && isfinite(S[1]) && isfinite(S[2]))) {
+                    dead = true;
+                    atomicAdd(P.counters + 4, 1ull);
+                    atomicMax(P.status, 3);
+                }
+            }
+            if (finished) {
+                // sample li at the interval's end record
+                ring[(li % kFreeWindow) * 32 + lane] = dead ? 0.0 : w * ms.vertex(gs + 4, S);
+                ++li;
+                if (li <= N) {
+                    const double *gn = coef + (size_t)(li - 1) * SLOT;
+                    t = gn[0];
+                    t1 = gn[1];
+                    dt = dt0;
+                    fails = 0;
+                    attempts = 0;
+                }
+            }
+        }
+        // reduce every sample all lanes have passed
+        const int lo = (int)__reduce_min_sync(kFull, (unsigned)li);
+        __syncwarp();
+        for (; base < lo; ++base)
+            keep_sample(base, warp_sum(ring[(base % kFreeWindow) * 32 + lane]), N, sub, lane, held, prow);
+        __syncwarp();
+    }
+}
+
 constexpr int kLevelMax = 10;
 // dynamic shared memory of the learned-proposer kernels
 __host__ __device__ constexpr int mlp_smem_bytes() {
@@ -1279,10 +1386,13 @@ __global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integ
     constexpr bool kNarrow = sizeof(R) != sizeof(double);
     // only the reference schedule reads the standard table; the dyadic table
     // is read from global memory
-    constexpr int COPY = (PROPOSER == 0) ? SLOT : SCHED;
+    // the relaxation models on the reference schedule run free lanes (above)
+    constexpr bool kFree = Traits<M>::kRelax && PROPOSER == 0 && STEPPER == 0 && OUT == 0;
+    constexpr int COPY = kFree ? 2 : (PROPOSER == 0) ? SLOT : SCHED;
     constexpr int NTAB = kMaxStd * 13 * NF;
     using V = typename Num<R>::V;
     __shared__ __align__(16) double stage_raw[kWarpsPerBlock][COPY];
+    __shared__ double free_ring[kWarpsPerBlock][kFree ? kFreeWindow * 32 : 1];
     __shared__ __align__(16) V stage_tab[kWarpsPerBlock][kNarrow && PROPOSER == 0 ? NTAB : 1];
     // learned proposer: the network and per-warp input tiles in dynamic shared
     // memory (mlp_smem_bytes(); none for the other modes)
@@ -1334,6 +1444,13 @@ __global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integ
             double kc[4];       // momentum cosines (OUT 1-3)
             if constexpr (OUT >= 1 && OUT <= 3) piflux_cosines(row, kc);
 
+            if constexpr (kFree) {
+                // sample 0 at t_begin, then free lanes through samples 1 .. N
+                keep_sample(0, warp_sum(dead ? 0.0 : w * ms.vertex(pd.s0rec, S)), N, sub, lane, held,
+                            prow);
+                integrate_free<M, D>(P, ms, coef, dt0, tb, te, N, w, dead, S, held, prow, sub, lane,
+                                     free_ring[wib], my_attempts, my_rejects);
+            } else {
             for (int i = 0; i <= N; ++i) {
                 const double *rec = pd.s0rec;
                 if (i > 0) {
@@ -1534,6 +1651,7 @@ __global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integ
                     }
                 }
             }
+            }  // interval-synchronous loop
         }
     }
 #pragma unroll
