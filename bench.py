@@ -63,7 +63,15 @@ VARIANTS = {
     "mixed_lockstep": dict(precision=1, proposer=3, abs_tol=1e-8, rel_tol=1e-6),
     "learned": dict(proposer=2),
     "mixed_learned": dict(precision=1, proposer=2, abs_tol=1e-8, rel_tol=1e-6),
+    # one two-point Gauss Magnus step per measurement interval, the rotation
+    # exp([omega]_x) applied exactly (FP64)
+    "magnus4": dict(stepper=1, magnus_substeps=1),
 }
+# Magnus-4 flops per k.interval (PiFlux-2D): two evaluations of the staged
+# interpolants (2 functions x degree 7 Horner: 56), two d vectors (~20), the
+# generator h (d1 + d2) + c h^2 (d2 x d1) (~20), the rotation (~50); plus one
+# sqrt and one sincos
+MAGNUS4_FLOPS_PER_KSTEP = 150
 LEARNED_RECORDS = 1 << 21
 LEARNED_EPOCHS = 20
 
@@ -246,8 +254,19 @@ def compare_variants(args, eng, wl, api, stream, flush, main_variant):
     path on the same workload, same timing method (CUDA events over K graph
     launches, L2 flushed before each): the learned+FP32 vs plain FP64 ratio."""
     import torch
+    from higherharmonics_b200.analysis import (default_max_order, harmonic_intensities,
+                                               harmonic_rel_err)
+    # the plain FP64 spectrum every variant's harmonic error refers to
+    ref = eng.plan(wl.system, wl.pulses, wl.grid, wl.opts())
+    ref.execute_async()
+    ref.spectrum_async()
+    ref.fetch(copy_j=False)
+    fr0, re0, im0 = ref.fetch_spectrum(0)
+    ref.close()
+    mo = default_max_order(fr0)
+    I0 = harmonic_intensities(fr0, re0, im0, mo)
     out = {}
-    for v in ("fp64", "mixed_learned", "mixed_lockstep"):
+    for v in ("fp64", "mixed_learned", "mixed_lockstep", "magnus4"):
         if v == main_variant or (v != "fp64" and args.workload in DEFAULT_VARIANT):
             continue
         okw = dict(VARIANTS[v])
@@ -269,8 +288,11 @@ def compare_variants(args, eng, wl, api, stream, flush, main_variant):
         b.record(stream)
         torch.cuda.synchronize()
         _, st = plan.fetch(copy_j=False)
+        fr, re, im = plan.fetch_spectrum(0)
         out[v] = {"value": args.steps / (a.elapsed_time(b) * 1e-3), "unit": UNIT,
-                  "k_steps_per_spectrum": st.attempted_steps}
+                  "k_steps_per_spectrum": st.attempted_steps,
+                  "harmonic_err_vs_fp64": harmonic_rel_err(harmonic_intensities(fr, re, im, mo), I0,
+                                                           floor_rel=1e-6)}
         plan.close()
     return out
 
@@ -412,6 +434,8 @@ def our_arm(args, wl_name):
     # understates the kernel's own throughput
     kernel_s = avg_launch_s
     per_kstep = ALG_FLOPS_PER_KSTEP.get(wl_name, 421)
+    if VARIANTS[args.variant].get("stepper", 0) == 1:
+        per_kstep = MAGNUS4_FLOPS_PER_KSTEP
     if mixed:
         # the bound is whichever pipe needs longer for its share of the work:
         # FP32 (13 F_rhs + 330 flops) against the measured FP32 FMA rate
@@ -432,7 +456,8 @@ def our_arm(args, wl_name):
                 "kernel_ms_source": "mean over the timed steps of CUDA events around each graph "
                                     "launch (integration + reduction + FFT) on the launching stream",
                 "alg_flops_per_kstep": per_kstep, "bound_flops_per_kstep": bflops,
-                "special_ops_per_kstep": SPECIAL_OPS_PER_KSTEP.get(wl_name, 0)}
+                "special_ops_per_kstep": (2 if VARIANTS[args.variant].get("stepper", 0) == 1
+                                          else SPECIAL_OPS_PER_KSTEP.get(wl_name, 0))}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,

@@ -1455,10 +1455,11 @@ __global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integ
                 const double *rec = pd.s0rec;
                 if (i > 0) {
                     // stage interval i-1 into this warp's shared slot (the
-                    // closed-form Magnus step reads its four moments and the
-                    // record straight from the staging table: warp broadcasts)
+                    // Magnus steppers read their interpolants or moments and
+                    // the record straight from the staging table: warp
+                    // broadcasts of a few values per interval)
                     const double *gslot = coef + (size_t)(i - 1) * SLOT;
-                    if constexpr (STEPPER != 2) {
+                    if constexpr (STEPPER == 0) {
                         __syncwarp();
                         const double2 *src = reinterpret_cast<const double2 *>(gslot);
                         double2 *dst = reinterpret_cast<double2 *>(slot);
@@ -1469,7 +1470,7 @@ __global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integ
                         for (int c = lane; c < NTAB; c += 32) stage_tab[wib][c] = Num<R>::mk(slot[TAB + c]);
                     }
                     __syncwarp();
-                    const double *cur = STEPPER == 2 ? gslot : slot;
+                    const double *cur = STEPPER != 0 ? gslot : slot;
                     rec = cur + 4;
                     const double t0 = cur[0], t1 = cur[1];
                     const PolyEval<NF, D, R> poly{slot, tb, te};
@@ -1482,7 +1483,7 @@ __global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integ
                             for (int s = 0; s < ns; ++s) {
                                 const double ts = t0 + s * hs;
                                 double f[NF], d1[3], d2[3];
-                                const PolyEval<NF, D, double> pd64{slot, tb, te};
+                                const PolyEval<NF, D, double> pd64{cur, tb, te};
                                 pd64(0, ts + g * hs, f);
                                 ms.dvec(f, d1);
                                 pd64(0, ts + (1.0 - g) * hs, f);

@@ -193,8 +193,8 @@ def _spectrum_err(engine, sys, pulse, grid, opts, opts_ref):
 
 @pytest.mark.parametrize("model", ["piflux2d", "honeycomb", "dirac2d"])
 def test_fast_variants_meet_harmonic_bar(engine, model):
-    """Mixed precision and the carried step proposal stay within the 1e-4
-    harmonic-intensity bar of the plain FP64 path."""
+    """Mixed precision, the step proposers and the Magnus-4 stepper stay
+    within the 1e-4 harmonic-intensity bar of the plain FP64 path."""
     if model == "piflux2d":
         s = 1 / math.sqrt(2)
         sys = api.system(api.SYS_PIFLUX2D, hopping=1.0, pol=(s, s))
@@ -215,7 +215,9 @@ def test_fast_variants_meet_harmonic_bar(engine, model):
                  api.solver(ref.abs_tol, ref.rel_tol, proposer=api.PROPOSER_LOCKSTEP),
                  api.solver(1e-8, 1e-6, precision=api.PREC_MIXED),
                  api.solver(1e-8, 1e-6, precision=api.PREC_MIXED, proposer=api.PROPOSER_CARRY),
-                 api.solver(1e-8, 1e-6, precision=api.PREC_MIXED, proposer=api.PROPOSER_LOCKSTEP)):
+                 api.solver(1e-8, 1e-6, precision=api.PREC_MIXED, proposer=api.PROPOSER_LOCKSTEP),
+                 # one two-point Magnus step (exact rotation) per measurement interval
+                 api.solver(stepper=api.STEPPER_MAGNUS4, magnus_substeps=1)):
         herr, jerr, st, st_ref = _spectrum_err(engine, sys, pulse, grid, opts, ref)
         assert herr <= 1e-4, (opts.precision, opts.proposer, herr)
         assert jerr <= 1e-4, (opts.precision, opts.proposer, jerr)
