@@ -1443,6 +1443,13 @@ __global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integ
             double held2 = 0.0; // ... and of its second channel (OUT 1)
             double kc[4];       // momentum cosines (OUT 1-3)
             if constexpr (OUT >= 1 && OUT <= 3) piflux_cosines(row, kc);
+            // closed-form Magnus step: the next interval's moments are loaded
+            // while the current step computes (registers, off the step's chain)
+            double mom_next[4] = {0.0, 0.0, 0.0, 0.0};
+            if constexpr (STEPPER == 2) {
+#pragma unroll
+                for (int c = 0; c < 4; ++c) mom_next[c] = __ldg(coef + TAB + c);
+            }
 
             if constexpr (kFree) {
                 // sample 0 at t_begin, then free lanes through samples 1 .. N
@@ -1499,10 +1506,14 @@ __global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integ
                     } else if constexpr (STEPPER == 2) {
                         // the interval's Legendre moments sit where the standard
                         // schedule's table would (staging layout 3)
-                        if (!dead) {
-                            double mom[4];
+                        double mom[4];
 #pragma unroll
-                            for (int c = 0; c < 4; ++c) mom[c] = __ldg(gslot + TAB + c);
+                        for (int c = 0; c < 4; ++c) mom[c] = mom_next[c];
+                        if (i < N) {
+#pragma unroll
+                            for (int c = 0; c < 4; ++c) mom_next[c] = __ldg(gslot + SLOT + TAB + c);
+                        }
+                        if (!dead) {
                             dirac_magnus_step(row[0], row[1], row[2], pd.measure_every, mom, S);
                             ++my_attempts;
                         }
