@@ -1443,6 +1443,17 @@ __global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integ
             double held2 = 0.0; // ... and of its second channel (OUT 1)
             double kc[4];       // momentum cosines (OUT 1-3)
             if constexpr (OUT >= 1 && OUT <= 3) piflux_cosines(row, kc);
+            // Magnus-4 with one step per interval: the next interval's pulse
+            // values at its two Gauss points, evaluated one interval ahead
+            // (off the rotation's dependency chain)
+            constexpr double kGa = 0.5 - 0.28867513459481288225;
+            double ga_next[STEPPER == 1 ? NF : 1], gb_next[STEPPER == 1 ? NF : 1];
+            if constexpr (STEPPER == 1) {
+                const double h0 = coef[1] - coef[0];
+                const PolyEval<NF, D, double> pe{coef, tb, te};
+                pe(0, coef[0] + kGa * h0, ga_next);
+                pe(0, coef[0] + (1.0 - kGa) * h0, gb_next);
+            }
             // closed-form Magnus step: the next interval's moments are loaded
             // while the current step computes (registers, off the step's chain)
             double mom_next[4] = {0.0, 0.0, 0.0, 0.0};
@@ -1482,7 +1493,33 @@ __global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integ
                     const double t0 = cur[0], t1 = cur[1];
                     const PolyEval<NF, D, R> poly{slot, tb, te};
                     if constexpr (STEPPER == 1) {
-                        if (!dead) {
+                        if (P.magnus_substeps == 1) {
+                            double f1[NF], f2[NF];
+#pragma unroll
+                            for (int n = 0; n < NF; ++n) {
+                                f1[n] = ga_next[n];
+                                f2[n] = gb_next[n];
+                            }
+                            if (i < N) {
+                                const double *gn = gslot + SLOT;
+                                const double hn = gn[1] - gn[0];
+                                const PolyEval<NF, D, double> pe{gn, tb, te};
+                                pe(0, gn[0] + kGa * hn, ga_next);
+                                pe(0, gn[0] + (1.0 - kGa) * hn, gb_next);
+                            }
+                            if (!dead) {
+                                const double hs = t1 - t0;
+                                const double q3 = 0.57735026918962576451 * hs * hs;
+                                double d1[3], d2[3], wv[3];
+                                ms.dvec(f1, d1);
+                                ms.dvec(f2, d2);
+                                wv[0] = hs * (d1[0] + d2[0]) + q3 * (d2[1] * d1[2] - d2[2] * d1[1]);
+                                wv[1] = hs * (d1[1] + d2[1]) + q3 * (d2[2] * d1[0] - d2[0] * d1[2]);
+                                wv[2] = hs * (d1[2] + d2[2]) + q3 * (d2[0] * d1[1] - d2[1] * d1[0]);
+                                rotate(wv, S);
+                                ++my_attempts;
+                            }
+                        } else if (!dead) {
                             const int ns = P.magnus_substeps;
                             const double hs = (t1 - t0) / ns;
                             const double g = 0.5 - 0.28867513459481288225;
