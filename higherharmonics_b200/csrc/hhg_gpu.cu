@@ -2190,8 +2190,11 @@ hhg_status dirac_quadrature(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_
         if (e == cudaSuccess) b.bytes = bytes;
         return e;
     };
-    // items per launch <= rows per launch, and <= splits x levels per launch
-    const size_t meta = (size_t)std::min<long long>((kKappaLookahead + 2) * n_total, limit);
+    // items per launch <= rows per launch (<= the row capacity, which an
+    // earlier call may have grown beyond this call's limit), and <= splits x
+    // levels per launch
+    const size_t meta =
+        (size_t)std::min<long long>((kKappaLookahead + 2) * n_total, std::max(limit, cap));
     HHG_CUDA(ctx, grow(ctx->kappa_T, (size_t)n_total * n_samples * sizeof(double)));
     HHG_CUDA(ctx, grow(ctx->kappa_items, meta * sizeof(hhg::KappaItem)));
     HHG_CUDA(ctx, grow(ctx->kappa_change, meta * sizeof(double)));
