@@ -7,7 +7,9 @@ available; ``oracle.adaptive_kappa`` restates the rule from that call (equal
 splits, trapezoid halving until the elementwise change drops below the
 threshold).  These tests pin the restatement by its defining properties:
 exactness on linear integrands, convergence to the integral, refinement only
-where the integrand needs it, and the symmetry of the Dirac current.
+where the integrand needs it, and the symmetry of the Dirac current; its
+first trapezoid is pinned to the reference's own fixed kappa rule
+(sources/debug_output.cpp:69-95).
 """
 import math
 
@@ -127,3 +129,38 @@ def test_dirac_quadrature_converges_to_gauss_legendre():
         ref += out[:, :, 2] @ np.array(rows)[:, 3]
     ref *= dz
     assert np.max(np.abs(j - ref)) <= 1e-5 * np.max(np.abs(ref)), np.max(np.abs(j - ref))
+
+
+def test_first_trapezoid_matches_the_reference_fixed_rule():
+    # the reference's fixed kappa trapezoid (sources/debug_output.cpp:69-95):
+    # kappa = r dkappa, r = 1 .. n_kappa, weight (r == n_kappa ? 1/2 : 1)
+    # dkappa dz k_z kappa / |k|, nothing at kappa = 0; one split's first
+    # trapezoid of the adaptive rule (n_splits = 1) takes the same nodes and
+    # weights
+    m, p, tc, s = _dirac_case(beta=2.0, fermi=0.1)
+    max_k, n_z, n_kappa = 2.0, 6, 7
+    dz = 2 * max_k / n_z
+    ref = np.zeros(tc.n_measurements + 1)
+    ours = np.zeros(tc.n_measurements + 1)
+    for z in range(1, n_z):
+        k_z = (z - n_z // 2) * dz
+        kmax = math.sqrt(max_k * max_k - k_z * k_z)
+        dk = kmax / n_kappa
+        rows = []
+        for r in range(1, n_kappa + 1):
+            kappa = r * dk
+            mk = math.sqrt(k_z * k_z + kappa * kappa)
+            w = (0.5 if r == n_kappa else 1.0) * dk * dz * (k_z * kappa / mk)
+            rows.append([k_z, kappa, mk, w, *O.initial_state(m, k_z, kappa, 0.0), 0.0])
+        out, rc = O.k_resolved(m, p, tc, s, np.array(rows), 0)
+        assert rc == 0
+        ref += out[:, :, 2] @ np.array(rows)[:, 3]
+        if z == n_z // 2:
+            continue  # weight 0 (k_z = 0): the adaptive rule skips the slice
+        mine = O.kappa_rows(m, k_z, 0.0, kmax, 0, n_kappa)
+        assert mine.shape[0] == n_kappa  # kappa = 0 left out
+        assert np.allclose(mine[:, 1], np.array(rows)[:, 1], rtol=1e-15, atol=0)
+        out, rc = O.k_resolved(m, p, tc, s, mine, 0)
+        ours += (kmax / n_kappa) * (out[:, :, 2] @ mine[:, 3])
+    ours *= dz
+    assert np.max(np.abs(ours - ref)) <= 1e-13 * np.max(np.abs(ref))
