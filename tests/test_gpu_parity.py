@@ -251,3 +251,28 @@ def test_dirac_magnus_refused_elsewhere(engine):
         engine.current_density(api.system(api.SYS_DIRAC2D, velocity=1.0), pulse, grid,
                                api.solver(stepper=api.STEPPER_DIRAC_MAGNUS))
     assert ei.value.status == api.UNSUPPORTED
+
+
+def test_full_size_symmetries(engine):
+    # the benchmark's own size (PiFlux-2D 256^2, 8 cycles, 8192 intervals),
+    # beyond the oracle's reach, through properties the physics fixes: the
+    # lattice is centrosymmetric (cos even), so (k, A) -> (-k, -A) leaves
+    # every trajectory unchanged and flips the current vertex: j[-A] = -j[A]
+    # up to the order of the BZ sum (this is what removes even harmonics);
+    # without a field the start state is stationary and j = 0
+    from higherharmonics_b200 import workloads as W
+    wl = W.piflux2d_256()
+    p = wl.pulses[0]
+    opts = wl.opts()
+    jp, sp = engine.current_density(wl.system, p, wl.grid, opts)
+    pm = api.cosine_pulse(-p.amplitude, p.n_cycles, p.n_measurements,
+                          window=(p.window_begin, p.window_end), energy_scale=p.energy_scale)
+    jm, sm = engine.current_density(wl.system, pm, wl.grid, opts)
+    assert sp.failed_trajectories == 0 and sm.failed_trajectories == 0
+    scale = np.max(np.abs(jp))
+    assert scale > 0 and np.max(np.abs(jp + jm)) <= 1e-10 * scale, np.max(np.abs(jp + jm)) / scale
+    assert abs(sp.attempted_steps - sm.attempted_steps) <= 1e-6 * sp.attempted_steps
+    p0 = api.cosine_pulse(0.0, p.n_cycles, p.n_measurements,
+                          window=(p.window_begin, p.window_end), energy_scale=p.energy_scale)
+    j0, _ = engine.current_density(wl.system, p0, wl.grid, opts)
+    assert np.max(np.abs(j0)) <= 1e-12 * scale
