@@ -272,6 +272,8 @@ def compare_variants(args, eng, wl, api, stream, flush, main_variant):
         okw = dict(VARIANTS[v])
         if okw.get("proposer") == api.PROPOSER_LEARNED:
             okw["mlp"], _ = train_proposer(eng, wl, api)
+            if args.mlp_every:
+                okw["mlp_every"] = args.mlp_every
         plan = eng.plan(wl.system, wl.pulses, wl.grid, wl.opts(**okw))
         plan.autotune(reps=1)
         sptr = stream.cuda_stream
@@ -322,6 +324,8 @@ def our_arm(args, wl_name):
     if okw.get("proposer") == api.PROPOSER_LEARNED:
         net, training = train_proposer(eng, wl, api)
         okw["mlp"] = net
+        if args.mlp_every:
+            okw["mlp_every"] = args.mlp_every
     plan = eng.plan(wl.system, wl.pulses, wl.grid, wl.opts(**okw))
     tune = plan.autotune(reps=2)
     # a dedicated stream: the legacy default stream has handle 0, which the
@@ -783,6 +787,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-compare", action="store_true")
+    ap.add_argument("--mlp-every", type=int, default=None,
+                    help="intervals between network proposals of the learned variants "
+                         "(default: the library's)")
     args = ap.parse_args()
     if args.variant is None:
         args.variant = DEFAULT_VARIANT.get(args.workload, "mixed_lockstep")
