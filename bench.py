@@ -44,7 +44,7 @@ UNIT = "spectra/s"
 # 3 rsqrt).
 ALG_FLOPS_PER_KSTEP = {"piflux2d_256": 13 * 12 + 421, "dirac2d_64": 13 * 16 + 421,
                        "honeycomb_512": 13 * 30 + 421, "dirac2d_sweep": 13 * 16 + 421,
-                       "piflux3d_relax": 13 * 76 + 421}
+                       "piflux3d_relax": 13 * 76 + 421, "piflux3d_field": 13 * 12 + 421}
 SPECIAL_OPS_PER_KSTEP = {"piflux2d_256": 26, "dirac2d_64": 0, "honeycomb_512": 78,
                          "dirac2d_sweep": 0, "piflux3d_relax": 13 * 5}
 # the relaxation workload runs the reference step schedule in FP64 only

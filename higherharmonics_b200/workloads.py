@@ -166,6 +166,20 @@ def piflux3d_relax(n_cycles=16) -> Workload:
                     dict(abs_tol=1e-12, rel_tol=1e-8), piflux3d_relax.__doc__)
 
 
+def piflux3d_field(n_cycles=4) -> Workload:
+    """The production PiFlux material and field without relaxation (the
+    coherent path, thermal start at 300 K): the field drives 2t|d| to ~300
+    hbar omega, so an interval takes several RKF78 steps and the step size
+    follows the pulse (the workload a step proposer is for); reference
+    continuum grid, 1024 intervals per cycle plus one relaxation cycle."""
+    from . import config
+    cfg = PIFLUX_PRODUCTION_CONFIG.format(n_cycles=n_cycles).replace(
+        "diagonal_relaxation_time 15", "diagonal_relaxation_time -1")
+    run = config.from_config(cfg)
+    return Workload(f"piflux3d_field_ref_{n_cycles}cyc", run.system, [run.pulse], run.grid,
+                    dict(abs_tol=1e-12, rel_tol=1e-8), piflux3d_field.__doc__)
+
+
 # experiment.config's material (v_F 1e5 m/s, band width 200 meV, n_z 60) on
 # the Dirac system with the cosine laser of params.config's photon energy at
 # 0.1 MV/cm (A0 = 24 in the system's momentum units)
@@ -217,4 +231,5 @@ ALL = {
     "honeycomb_1024x64": honeycomb_1024x64,
     "piflux3d_relax": piflux3d_relax,
     "dirac3d_kappa": dirac3d_kappa,
+    "piflux3d_field": piflux3d_field,
 }
