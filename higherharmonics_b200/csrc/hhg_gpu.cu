@@ -940,7 +940,7 @@ hhg_status hhg_grid_rows(const hhg_system_desc *sys, const hhg_grid_desc *grid, 
     return HHG_OK;
 }
 
-// cost_order: for the PiFlux-3D relaxation model, order the k rows by a cost
+// cost_order: for the PiFlux-3D models, order the k rows by a cost
 // proxy (below); plans whose outputs are indexed by k keep the caller's order.
 static hhg_status plan_create_impl(hhg_ctx *ctx, const hhg_system_desc *sys,
                                    const hhg_pulse_desc *pulses, int n_pulses,
@@ -1003,13 +1003,18 @@ static hhg_status plan_create_impl(hhg_ctx *ctx, const hhg_system_desc *sys,
     pl->n_k = grid_count(*grid);
     std::vector<double> ktab((size_t)pl->n_k * 8);
     build_rows(*sys, *grid, ktab.data());
-    if (cost_order && pl->model == hhg::PIFLUX3D_RELAX && pl->n_k > 32) {
-        // A warp's lanes finish together only if their k-points need similar
-        // numbers of steps (the reference schedule adapts per k-point).  The
-        // step count follows the time average of |d(k - A(t))| (correlation
-        // -0.43 measured on the oracle); a stable sort by it raised the
-        // active lanes of a warp from 0.83 to 0.90 of 32.  Only the (fixed)
-        // order of the Brillouin-zone sum changes.
+    if (cost_order && hhg::base_model(pl->model) == hhg::PIFLUX3D && pl->n_k > 32 &&
+        (o.proposer == HHG_PROPOSER_NONE || o.proposer == HHG_PROPOSER_CARRY)) {
+        // With per-lane step control a warp's lanes finish together only if
+        // their k-points need similar numbers of steps.  The step count
+        // follows the time average of |d(k - A(t))| (correlation -0.43
+        // measured on the oracle, relaxation path); a stable sort by it raised
+        // the active lanes of a warp from 0.83 to 0.90 of 32.  Only the
+        // (fixed) order of the Brillouin-zone sum changes.  Warp-synchronous
+        // (dyadic) stepping is left in the grid's order: there a warp takes
+        // its finest lane's level at every moment, and the grid's slices keep
+        // lanes whose needs peak together (same k_z) in one warp (the sort
+        // measured 7 % slower there).
         const hhg_pulse_desc &q0 = pulses[0];
         const HostPulse hp(q0);
         constexpr int kT = 256;
