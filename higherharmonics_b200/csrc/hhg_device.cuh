@@ -1921,11 +1921,11 @@ reduce_partials_kernel(const PulseDev *__restrict__ pulses, int n_pulses,
 }
 
 // ---------------------------------------------------------------------------
-// The adaptive kappa rule of the Dirac-3D current density.  A refinement
-// round works on a batch of splits; KappaItem b (host-built) holds split b's
-// slice momentum k_z, start a and this round's panel width h, its nodes
-// m = first + stride idx (idx < n) at kappa = a + m h, and the rows
-// [row0, row0 + n) of the round's k table and contributions.
+// The adaptive kappa rule of the Dirac-3D current density.  A launch works
+// on a batch of (split, refinement level) items; KappaItem b (host-built)
+// holds its slice momentum k_z, the split's start a and the level's panel
+// width h, its nodes m = first + stride idx (idx < n) at kappa = a + m h, and
+// the rows [row0, row0 + n) of the launch's k table and contributions.
 // ---------------------------------------------------------------------------
 struct KappaItem {
     double k_z, a, h;
@@ -1934,7 +1934,7 @@ struct KappaItem {
     int split, pad;
 };
 
-// The round's k table: k_z, kappa, |k|, the weight end x k_z kappa / |k|
+// The launch's k table: k_z, kappa, |k|, the weight end x k_z kappa / |k|
 // (integration_weight, DiracSystem.cpp:281; ends of a first trapezoid 1/2,
 // zero kappa weighted 0 as the reference's integrand, DiracSystem.cpp:301-303)
 // and the Fermi-occupied start (2 a0 b0, 0, a0^2 - b0^2), a0 = f(E_F + |k|),
@@ -1969,7 +1969,7 @@ static __global__ void kappa_rows_kernel(const KappaItem *__restrict__ items, in
     }
 }
 
-// One refinement round: split items[b] updates its trapezoid estimate
+// One refinement level: item b updates its split's trapezoid estimate
 //   T[split][i] <- scale T + h sum_rows contrib[i][row]
 // (scale 0 on the first round, 1/2 after a halving) and writes change[b] =
 // max_i |T_new - T_old| (NaN if any sample is NaN).  One CTA per split, one
