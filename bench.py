@@ -513,6 +513,10 @@ def our_arm(args, wl_name):
 # (~75) and the weighted sample (1): ~190 FP64 flops, plus sqrt, sincos and
 # three divisions (special operations).
 MAGNUS_FLOPS_PER_KINTERVAL = 190
+# Dirac-3D with relaxation under FP64 RKF78: one attempted step = 13
+# right-hand sides (m_x, m_z: 4 flops; the rotation part 6; the three
+# relaxation terms 6: 16) + the tableau arithmetic (421)
+DIRAC_RELAX_FLOPS_PER_KSTEP = 13 * 16 + 421
 MAGNUS_SPECIAL_OPS = 5
 
 
@@ -571,7 +575,7 @@ class DiracCpuBaseline:
         v = 1.0 / (el * n_all / len(self.sample))
         kint = info["trajectories"] * self.tc.n_measurements
         desc = (f"{len(self.sample)} of {n_all} (k_z slice, kappa split) pairs, evenly spaced, "
-                f"each refined to convergence ({info['trajectories']} trajectories, {kint} Magnus "
+                f"each refined to convergence ({info['trajectories']} trajectories, {kint} "
                 f"k.intervals) in {el:.2f} s on {self.cores} threads (oracle port, -O3 "
                 f"-ffast-math, OpenMP); "
                 f"spectra/s scaled by {n_all}/{len(self.sample)}")
@@ -582,7 +586,9 @@ def dirac_config(wl, path):
     q = wl.quad
     return {"workload": wl.name, "n_z": q.n_z, "n_kappa": q.n_kappa, "n_splits": q.n_splits,
             "kappa_threshold": q.threshold, "max_k": q.max_k,
-            "n_measurements": wl.pulse.n_measurements, "stepper": "closed-form Magnus (FP64)",
+            "n_measurements": wl.pulse.n_measurements,
+            "stepper": ("closed-form Magnus (FP64)" if wl.opts.stepper == 2 else
+                        "RKF78 with relaxation, reference schedule (FP64)"),
             "l2": "flushed (256 MiB write) before every timed step", "path": path}
 
 
@@ -591,7 +597,7 @@ def dirac_reference_arm(args):
     if rank != 0:
         return 0
     from higherharmonics_b200 import workloads as W
-    wl = W.dirac3d_kappa()
+    wl = W.ALL[args.workload]()
     cb = DiracCpuBaseline(wl, args.cpu_seconds)
     per = []
     desc = None
@@ -631,7 +637,7 @@ def dirac_arm(args):
     dev = torch.cuda.current_device()
     from higherharmonics_b200 import api
     from higherharmonics_b200 import workloads as W
-    wl = W.dirac3d_kappa()
+    wl = W.ALL[args.workload]()
     if ws > 1:  # one pulse instance per rank: weak scaling
         wl.pulse.phase = wl.pulse.phase + 0.1 * rank
     eng = api.Engine(dev)
@@ -684,7 +690,9 @@ def dirac_arm(args):
             torch.distributed.destroy_process_group()
         return 0
     kernel_s = kern_ms * 1e-3
-    achieved = MAGNUS_FLOPS_PER_KINTERVAL * kint / kernel_s / 1e12
+    magnus = wl.opts.stepper == 2
+    per_unit = MAGNUS_FLOPS_PER_KINTERVAL if magnus else DIRAC_RELAX_FLOPS_PER_KSTEP
+    achieved = per_unit * kint / kernel_s / 1e12
     n_s = p.n_measurements + 1
     n_fft = 4 * n_s + 1
     line = {
@@ -694,7 +702,8 @@ def dirac_arm(args):
         "data": "synthetic",
         "config": dirac_config(wl, "hhg_gpu_dirac_current_density (synchronous, host-driven "
                                    "rounds), wall clock"),
-        "k_intervals_per_spectrum": st.attempted_steps, "kappa": qs.as_dict(),
+        ("k_intervals_per_spectrum" if magnus else "k_steps_per_spectrum"): st.attempted_steps,
+        "kappa": qs.as_dict(),
         "gpu_launches": launches,
         "roofline": {"bound": "fp64_pipe", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak, "traffic": traffic_from_profile("dirac3d_kappa"),
@@ -705,8 +714,9 @@ def dirac_arm(args):
                      "kernel_ms": kern_ms / args.steps,
                      "kernel_ms_source": "CUDA events around each round's integration launch on "
                                          "the context stream, summed over the rounds",
-                     "alg_flops_per_k_interval": MAGNUS_FLOPS_PER_KINTERVAL,
-                     "special_ops_per_k_interval": MAGNUS_SPECIAL_OPS},
+                     "unit_of_work": "k.interval (Magnus step)" if magnus else "attempted k.step",
+                     "alg_flops_per_unit": per_unit,
+                     "special_ops_per_unit": MAGNUS_SPECIAL_OPS if magnus else 0},
         "clocks": clocks,
         "timing": {"quadrature_ms": [round(a, 3) for a, _, _ in per_step],
                    "with_spectrum_ms": [round(b, 3) for _, b, _ in per_step],
@@ -738,8 +748,8 @@ def ncu_case(args):
     from higherharmonics_b200 import api
     from higherharmonics_b200 import workloads as W
     import inspect
-    if args.workload == "dirac3d_kappa":
-        wl = W.dirac3d_kappa(n_cycles=args.ncu_cycles)
+    if args.workload.startswith("dirac3d_kappa"):
+        wl = W.ALL[args.workload](n_cycles=args.ncu_cycles)
         eng = api.Engine(0)
         for _ in range(2):
             _, qs, st = eng.dirac_current_density(wl.system, wl.pulse, wl.quad, wl.opts)
@@ -799,7 +809,7 @@ def main():
         return ncu_case(args)
     if args.variant == "mlp_train":
         ap.error("--variant mlp_train is a profiling case (--ncu-case)")
-    if args.workload == "dirac3d_kappa":
+    if args.workload.startswith("dirac3d_kappa"):
         return dirac_reference_arm(args) if args.impl == "reference" else dirac_arm(args)
     if args.impl == "reference":
         return reference_arm(args, args.workload)

@@ -209,7 +209,7 @@ class DiracWorkload:
     description: str
 
 
-def dirac3d_kappa(n_cycles=8) -> DiracWorkload:
+def dirac3d_kappa(n_cycles=8, relax=False) -> DiracWorkload:
     """The reference's Dirac run (DiracDispatcher::compute ->
     DiracSystem::compute_current_density, coherent: the closed-form Magnus
     step per interval): T = 300 K, E_F = 118 meV, v_F = 1e5 m/s, band width
@@ -218,9 +218,14 @@ def dirac3d_kappa(n_cycles=8) -> DiracWorkload:
     first trapezoids of 10 panels, halved until the elementwise change is
     below 1e-3 (DiracDispatcher.cpp:13-14)."""
     from . import config
-    run = config.from_config(DIRAC_CONFIG.format(n_cycles=n_cycles))
-    return DiracWorkload(f"dirac3d_kappa_nz60_{n_cycles}cyc", run.system, run.pulse, run.quad,
-                         run.opts, dirac3d_kappa.__doc__)
+    cfg = DIRAC_CONFIG.format(n_cycles=n_cycles)
+    if relax:
+        # the reference's configs set a relaxation time: its production path
+        # (compute_current_density_diagonal_relaxation, FP64 RKF78)
+        cfg = cfg.replace("diagonal_relaxation_time -1", "diagonal_relaxation_time 15")
+    run = config.from_config(cfg)
+    name = f"dirac3d_kappa{'_relax' if relax else ''}_nz60_{n_cycles}cyc"
+    return DiracWorkload(name, run.system, run.pulse, run.quad, run.opts, dirac3d_kappa.__doc__)
 
 
 ALL = {
@@ -231,5 +236,6 @@ ALL = {
     "honeycomb_1024x64": honeycomb_1024x64,
     "piflux3d_relax": piflux3d_relax,
     "dirac3d_kappa": dirac3d_kappa,
+    "dirac3d_kappa_relax": lambda n_cycles=8: dirac3d_kappa(n_cycles, relax=True),
     "piflux3d_field": piflux3d_field,
 }
