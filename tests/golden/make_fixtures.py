@@ -9,6 +9,12 @@ the tests only read the JSON files written here.
   as text, plus the 30-point [0,1] table of sources/HHG/Laser/gauss.hpp.
 * magnus_dirac.json -- the Magnus generator Omega of helper/magnus_dirac.py,
   evaluated with sympy at seeded sample points (k, k_z, kappa, alpha..delta).
+* piflux_ic.json -- the thermal PiFlux initial state <sigma> of
+  helper/piflux_initial_conditions.py (the state alpha|a> + beta|b> written
+  through the helper's V and normalisation), evaluated with sympy at seeded
+  (t, beta_T, E_F, k) with alpha^2, beta^2 the reference's band occupations
+  (PiFlux.cpp:420-426, GlobalDefinitions.hpp:36-41), together with the
+  helper's closed form of |<sigma(0)>|^2.
 """
 from __future__ import annotations
 
@@ -65,12 +71,53 @@ def magnus_dirac(ref: str, n_points: int = 6, seed: int = 20261203) -> dict:
     return {"points": pts}
 
 
+def piflux_ic(ref: str, n_points: int = 12, seed: int = 20261203) -> dict:
+    import contextlib
+    import io
+    import math
+
+    import sympy
+    src = open(os.path.join(ref, "helper/piflux_initial_conditions.py")).read()
+    ns: dict = {}
+    with contextlib.redirect_stdout(io.StringIO()):
+        exec(compile(src, "piflux_initial_conditions.py", "exec"), ns)
+    a, b, x, y, z = (ns[n] for n in ("alpha", "beta", "x", "y", "z"))
+    phi, V, nrm = ns["phi"], ns["V"], ns["normalization"]
+    exprs = [sympy.simplify(nrm * (phi.H * V.H * s * V * phi)[0])
+             for s in (ns["sigma_x"], ns["sigma_y"], ns["sigma_z"])]
+    norm2 = ns["norm"]
+
+    def fermi(e, beta_t):
+        return 1.0 / (1.0 + math.exp(beta_t * e))
+
+    rng = np.random.default_rng(seed)
+    pts = []
+    for _ in range(n_points):
+        t = float(rng.uniform(0.5, 1.5))
+        beta_t = float(rng.uniform(0.05, 3.0))
+        ef = float(rng.uniform(-1.0, 1.0))
+        k = [float(v) for v in rng.uniform(-math.pi, math.pi, 3)]
+        c = [math.cos(v) for v in k]
+        disp = math.sqrt(sum(v * v for v in c))
+        a2 = fermi(-ef + 2 * t * disp, beta_t)
+        b2 = fermi(-ef - 2 * t * disp, beta_t)
+        sub = {a: sympy.sqrt(sympy.Float(a2, 30)), b: sympy.sqrt(sympy.Float(b2, 30)),
+               x: sympy.Float(c[0], 30), y: sympy.Float(c[1], 30), z: sympy.Float(c[2], 30)}
+        sigma = [float(sympy.re(sympy.N(e.subs(sub), 25))) for e in exprs]
+        n2 = float(sympy.N(norm2.subs({a: sub[a], b: sub[b]}), 25))
+        pts.append({"hopping": t, "beta": beta_t, "fermi_energy": ef, "k": k,
+                    "alpha2": a2, "beta2": b2, "sigma": sigma, "norm2": n2})
+    return {"points": pts}
+
+
 def main() -> None:
     ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     with open(os.path.join(HERE, "gauss_tables.json"), "w") as f:
         json.dump(gauss_tables(ref), f)
     with open(os.path.join(HERE, "magnus_dirac.json"), "w") as f:
         json.dump(magnus_dirac(ref), f, indent=1)
+    with open(os.path.join(HERE, "piflux_ic.json"), "w") as f:
+        json.dump(piflux_ic(ref), f, indent=1)
 
 
 if __name__ == "__main__":

@@ -10,7 +10,9 @@ Fermi-occupied states (PiFlux.cpp:519-549, Honeycomb.cpp:347-361,
 DiracSystem.cpp:155-158).
 """
 import ctypes
+import json
 import math
+import os
 
 import numpy as np
 import pytest
@@ -50,6 +52,24 @@ def test_thermal_piflux_state_is_pure(beta, ef):
         a2 = fermi(-ef + 2 * t * disp, beta)
         b2 = fermi(-ef - 2 * t * disp, beta)
         assert abs(np.linalg.norm(r[4:7]) - (a2 + b2)) <= 1e-13
+
+
+def test_thermal_piflux_state_matches_reference_derivation():
+    """The oracle's PiFlux ic_sigma against tests/golden/piflux_ic.json: the
+    expectation values of helper/piflux_initial_conditions.py (the state
+    alpha|a> + beta|b> through the helper's V and normalisation), evaluated with
+    sympy at seeded (t, beta_T, E_F, k), and the helper's closed form
+    |<sigma(0)>|^2 = (alpha^2 + beta^2)^2."""
+    path = os.path.join(os.path.dirname(__file__), "golden", "piflux_ic.json")
+    pts = json.load(open(path))["points"]
+    assert len(pts) >= 10
+    for p in pts:
+        m = O.model(O.PIFLUX3D, hopping=p["hopping"], beta=p["beta"],
+                    fermi_energy=p["fermi_energy"])
+        s0 = O.initial_state(m, *p["k"])
+        assert np.max(np.abs(s0 - np.array(p["sigma"]))) <= 1e-13, p
+        assert abs(float(s0 @ s0) - p["norm2"]) <= 1e-13
+        assert abs(p["norm2"] - (p["alpha2"] + p["beta2"]) ** 2) <= 1e-13
 
 
 @pytest.mark.parametrize("beta,ef", [(1.5, 0.4), (0.2, -0.5)])
