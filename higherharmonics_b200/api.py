@@ -22,7 +22,8 @@ STATUS_NAMES = {0: "HHG_OK", 1: "HHG_BAD_CONFIG", 2: "HHG_STEP_LIMIT", 3: "HHG_N
                 4: "HHG_CUDA_ERROR", 5: "HHG_UNSUPPORTED"}
 SYS_DIRAC2D, SYS_PIFLUX2D, SYS_PIFLUX3D, SYS_HONEYCOMB, SYS_DIRAC3D = range(5)
 (GRID_TENSOR_GL, GRID_RHOMBIC_GL, GRID_PIFLUX3D_REF, GRID_HONEYCOMB_HEX_REF, GRID_EXPLICIT,
- GRID_PIFLUX3D_OCCUPATION, GRID_PIFLUX3D_CUBE) = range(7)
+ GRID_PIFLUX3D_OCCUPATION, GRID_PIFLUX3D_CUBE, GRID_PIFLUX3D_DEBUG) = range(8)
+N_DEBUG_POINTS = 25  # n_debug_points (GlobalDefinitions.hpp)
 KOUT_BLOCH, KOUT_OCCUPATIONS = 0, 1
 STEPPER_RKF78, STEPPER_MAGNUS4, STEPPER_DIRAC_MAGNUS = 0, 1, 2
 PREC_FP64, PREC_MIXED = 0, 1
@@ -39,7 +40,7 @@ EXPORTED = [
     "hhg_learned_collect", "hhg_default_train_opts", "hhg_mlp_init", "hhg_mlp_train",
     "hhg_mlp_gradients", "hhg_mlp_predict", "hhg_plan_execute_graph", "hhg_plan_autotune", "hhg_measure_fp32_peak",
     "hhg_gpu_k_resolved", "hhg_gpu_split_current", "hhg_gpu_spectrum_welch", "hhg_pulse_values",
-    "hhg_gpu_dirac_current_density",
+    "hhg_gpu_dirac_current_density", "hhg_gpu_trapezoidal_fft",
 ]
 TUNE_MAX = 16
 ABI_VERSION = 4
@@ -229,6 +230,8 @@ def load_library() -> ctypes.CDLL:
         L.hhg_gpu_spectrum_welch.argtypes = [ctypes.c_void_p, _D, ctypes.c_int, ctypes.c_double,
                                              ctypes.c_double, _D, _D, _D]
         L.hhg_pulse_values.argtypes = [ctypes.POINTER(PulseDesc), _D, ctypes.c_int64, _D]
+        L.hhg_gpu_trapezoidal_fft.argtypes = [ctypes.c_void_p, _D, ctypes.c_int64, ctypes.c_double,
+                                              ctypes.c_double, ctypes.c_double, _D, _D, _D]
         L.hhg_gpu_dirac_current_density.argtypes = [
             ctypes.c_void_p, ctypes.POINTER(SystemDesc), ctypes.POINTER(PulseDesc),
             ctypes.POINTER(KappaQuad), ctypes.POINTER(SolverOpts), _D, ctypes.POINTER(KappaStats),
@@ -353,6 +356,12 @@ def grid_piflux3d_occupation(n: int) -> GridDesc:
 def grid_piflux3d_cube(n: int) -> GridDesc:
     """PiFlux::current_per_energy's N^3 grid and its -z mirror (PiFlux.cpp:955-1035)."""
     return GridDesc(GRID_PIFLUX3D_CUBE, n, 0, 0, 0, 0, 0, 0, None, 0)
+
+
+def grid_piflux3d_debug() -> GridDesc:
+    """The 25 momenta of PiFlux::compute_current_density_debug (PiFlux.cpp:320-371):
+    k = (pi/2, pi/2 - 0.02 pi i, 0.49 pi), weight 1."""
+    return GridDesc(GRID_PIFLUX3D_DEBUG, 0, 0, 0, 0, 0, 0, 0, None, 0)
 
 
 def pulse_values(pulse: PulseDesc, t) -> np.ndarray:
@@ -532,6 +541,17 @@ class Engine:
         self._check(self.lib.hhg_gpu_spectrum_welch(self.ctx, _ptr(j), n_measurements, t_begin, t_end,
                                                     _ptr(re), _ptr(im), _ptr(fr)),
                     "hhg_gpu_spectrum_welch")
+        return fr, re, im
+
+    def trapezoidal_fft(self, x: np.ndarray, delta_t: float, t_begin: float, t_end: float):
+        """TrapezoidalFFT::compute of x as given, without padding
+        (hhg_gpu_trapezoidal_fft): (frequencies, real, imag), len(x) // 2 + 1 each."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        n_fft = x.size // 2 + 1
+        re, im, fr = np.zeros(n_fft), np.zeros(n_fft), np.zeros(n_fft)
+        self._check(self.lib.hhg_gpu_trapezoidal_fft(self.ctx, _ptr(x), x.size, delta_t, t_begin,
+                                                     t_end, _ptr(re), _ptr(im), _ptr(fr)),
+                    "hhg_gpu_trapezoidal_fft")
         return fr, re, im
 
     def plan(self, sys: SystemDesc, pulses, grid: GridDesc, opts: SolverOpts | None = None):

@@ -267,6 +267,9 @@ void push_row(const hhg_system_desc &s, double kx, double ky, double kz, double 
     o[7] = 0.0;
 }
 
+// n_debug_points (GlobalDefinitions.hpp): the momenta of the debug traces
+constexpr int kDebugPoints = 25;
+
 int64_t grid_count(const hhg_grid_desc &g) {
     switch (g.kind) {
     case HHG_GRID_TENSOR_GL:
@@ -284,6 +287,8 @@ int64_t grid_count(const hhg_grid_desc &g) {
         return (int64_t)g.n1 * g.n1;
     case HHG_GRID_PIFLUX3D_CUBE:
         return 2 * (int64_t)g.n1 * g.n1 * g.n1;
+    case HHG_GRID_PIFLUX3D_DEBUG:
+        return kDebugPoints;
     }
     return -1;
 }
@@ -445,6 +450,12 @@ void build_rows(const hhg_system_desc &s, const hhg_grid_desc &g, double *out) {
         }
         break;
     }
+    case HHG_GRID_PIFLUX3D_DEBUG:
+        // PiFlux::compute_current_density_debug (PiFlux.cpp:320-371): momentum_type
+        // (picked_x, picked[i], picked_z) as constructed, no rescue
+        for (int i = 0; i < kDebugPoints; ++i)
+            push_row(s, 0.5 * kPi, 0.5 * kPi - (i * 0.02 * kPi), 0.49 * kPi, 1.0, out + 8 * r++);
+        break;
     }
 }
 
@@ -492,6 +503,8 @@ hhg_status check_grid(hhg_ctx *ctx, const hhg_grid_desc *g) {
         break;
     case HHG_GRID_PIFLUX3D_CUBE:
         if (g->n1 < 1 || g->n1 > 1024) return set_err(ctx, HHG_BAD_CONFIG, "cube grid N out of range");
+        break;
+    case HHG_GRID_PIFLUX3D_DEBUG:
         break;
     default:
         return set_err(ctx, HHG_BAD_CONFIG, "grid type not recognized");
@@ -1453,16 +1466,15 @@ hhg_status hhg_gpu_current_density(hhg_ctx *ctx, const hhg_system_desc *sys,
     return st;
 }
 
-hhg_status hhg_gpu_spectrum(hhg_ctx *ctx, const double *j, int n_measurements, double t_begin,
-                            double t_end, double *re_out, double *im_out, double *freq_out) {
-    if (!ctx || !j || !re_out || !im_out || !freq_out || n_measurements < 1)
-        return set_err(ctx, HHG_BAD_CONFIG, "bad spectrum arguments");
-    if (!(t_end > t_begin)) return set_err(ctx, HHG_BAD_CONFIG, "empty time window");
+}  // extern "C"
+
+namespace {
+// TrapezoidalFFT::compute of the n host samples j, zero-padded to n_in >= n
+// values, through the context's buffers and cuFFT plans.
+hhg_status trapezoidal_fft(hhg_ctx *ctx, const double *j, int n, int n_in, double delta_t,
+                           double t_begin, double t_end, double *re_out, double *im_out,
+                           double *freq_out) {
     HHG_CUDA(ctx, cudaSetDevice(ctx->device));
-    const int n = n_measurements + 1;
-    const long long n_in_ll = 8LL * n;  // zero_padding (hhg.cpp:36)
-    if (n_in_ll > (1LL << 30)) return set_err(ctx, HHG_BAD_CONFIG, "spectrum too long");
-    const int n_in = (int)n_in_ll;
     const int n_fft = n_in / 2 + 1;
     cudaStream_t s = ctx->stream;
     if (ctx->x_cap < (size_t)n_in) {
@@ -1497,7 +1509,6 @@ hhg_status hhg_gpu_spectrum(hhg_ctx *ctx, const double *j, int n_measurements, d
     HHG_CUDA(ctx, cudaGetLastError());
     if (cufftExecD2Z(plan, ctx->d_x, (cufftDoubleComplex *)ctx->d_F) != CUFFT_SUCCESS)
         return set_err(ctx, HHG_CUDA_ERROR, "cufftExecD2Z failed");
-    const double delta_t = (t_end - t_begin) / n_measurements;
     hhg::trapezoid_correct_kernel<<<(n_fft + 255) / 256, 256, 0, s>>>(
         ctx->d_F, n_fft, n_in, delta_t, t_begin, t_end, ctx->d_x, ctx->d_out,
         ctx->d_out + n_fft, ctx->d_out + 2 * n_fft);
@@ -1507,6 +1518,33 @@ hhg_status hhg_gpu_spectrum(hhg_ctx *ctx, const double *j, int n_measurements, d
     HHG_CUDA(ctx, cudaMemcpyAsync(freq_out, ctx->d_out + 2 * n_fft, sizeof(double) * n_fft, cudaMemcpyDeviceToHost, s));
     HHG_CUDA(ctx, cudaStreamSynchronize(s));
     return HHG_OK;
+}
+}  // namespace
+
+extern "C" {
+
+hhg_status hhg_gpu_spectrum(hhg_ctx *ctx, const double *j, int n_measurements, double t_begin,
+                            double t_end, double *re_out, double *im_out, double *freq_out) {
+    if (!ctx || !j || !re_out || !im_out || !freq_out || n_measurements < 1)
+        return set_err(ctx, HHG_BAD_CONFIG, "bad spectrum arguments");
+    if (!(t_end > t_begin)) return set_err(ctx, HHG_BAD_CONFIG, "empty time window");
+    const int n = n_measurements + 1;
+    const long long n_in_ll = 8LL * n;  // zero_padding (hhg.cpp:36)
+    if (n_in_ll > (1LL << 30)) return set_err(ctx, HHG_BAD_CONFIG, "spectrum too long");
+    return trapezoidal_fft(ctx, j, n, (int)n_in_ll, (t_end - t_begin) / n_measurements, t_begin,
+                           t_end, re_out, im_out, freq_out);
+}
+
+hhg_status hhg_gpu_trapezoidal_fft(hhg_ctx *ctx, const double *input, int64_t n_input,
+                                   double delta_t, double t_begin, double t_end, double *re_out,
+                                   double *im_out, double *freq_out) {
+    if (!ctx || !input || !re_out || !im_out || !freq_out || n_input < 2)
+        return set_err(ctx, HHG_BAD_CONFIG, "bad spectrum arguments");
+    if (n_input > (1LL << 30)) return set_err(ctx, HHG_BAD_CONFIG, "spectrum too long");
+    if (!(delta_t > 0.0) || !std::isfinite(delta_t) || !std::isfinite(t_begin) || !std::isfinite(t_end))
+        return set_err(ctx, HHG_BAD_CONFIG, "bad time step or window");
+    return trapezoidal_fft(ctx, input, (int)n_input, (int)n_input, delta_t, t_begin, t_end, re_out,
+                           im_out, freq_out);
 }
 
 namespace {

@@ -4,9 +4,10 @@
 reference's order: the occupation tracking (occupations != "no",
 hhg.cpp:120-168), the energy-split current (split_current != "no",
 hhg.cpp:170-219) and, unless either says "only", the current density with its
-spectrum (hhg.cpp:236-337).  Each mode returns the JSON document the reference
-writes (the same keys; the metadata files are not produced), and `save`
-writes one gzip-compressed as `*.json.gz`.
+spectrum (hhg.cpp:236-337), followed by PiFlux's debug traces when debug_data
+is "yes" or "only" (hhg.cpp:235-238, 287-291, 343-352).  Each mode returns the
+JSON document the reference writes (the same keys; the metadata files are not
+produced), and `save` writes one gzip-compressed as `*.json.gz`.
 
 Integration, Brillouin-zone sums and spectra run on the GPU through the C
 ABI; the host only builds descriptors, relabels the occupation grid and
@@ -62,10 +63,14 @@ def current_density(eng: api.Engine, cfg: dict, grid: api.GridDesc | None = None
                     n_measurements: int | None = None) -> dict:
     """The main mode: j(t) on the system's grid (the Dirac system: its k_z
     slices and adaptive kappa rule) and its spectrum (trapezoidal FFT with 8x
-    zero padding, or the Welch FFT for the continuous laser)."""
+    zero padding, or the Welch FFT for the continuous laser).  With
+    debug_data "only" the reference skips the integration and transforms its
+    zero-initialised j (hhg.cpp:235-236)."""
     run = config.from_config(cfg, grid=grid, n_measurements=n_measurements)
     p = run.pulse
-    if run.quad is not None:  # the Dirac system's k_z x kappa quadrature
+    if cfg.get("debug_data", "no") == "only":
+        j = np.zeros(p.n_measurements + 1)
+    elif run.quad is not None:  # the Dirac system's k_z x kappa quadrature
         j, _, _ = eng.dirac_current_density(run.system, p, run.quad, run.opts)
     else:
         j, _ = eng.current_density(run.system, p, run.grid, run.opts)
@@ -130,9 +135,44 @@ def split_current(eng: api.Engine, cfg: dict, N: int | None = None,
     return doc
 
 
+def debug_traces(eng: api.Engine, cfg: dict, n_measurements: int | None = None,
+                 frequencies=None) -> dict:
+    """PiFlux::compute_current_density_debug (PiFlux.cpp:320-371): S_z(t_i) of
+    the 25 momenta k = (pi/2, pi/2 - 0.02 pi i, 0.49 pi) with the system's
+    dynamics (coherent or relaxation), each transformed by TrapezoidalFFT
+    without padding (hhg.cpp:287-291).  The document is time_evolution.json
+    (hhg.cpp:343-352); its "frequencies" are the main spectrum's
+    (`frequencies`, the 8x padded grid, as the reference stores them)."""
+    if cfg["system_type"] != "PiFlux":
+        raise config.UnsupportedConfig("debug traces are built for PiFlux only "
+                                       "(PiFluxDispatcher.cpp:128-136)")
+    run = config.from_config(cfg, grid=api.grid_piflux3d_debug(), n_measurements=n_measurements)
+    p = run.pulse
+    S, _ = eng.k_resolved(run.system, p, run.grid, run.opts, kind=api.KOUT_BLOCH)
+    traces = np.ascontiguousarray(S[:, :, 2].T)  # [point][sample]
+    me = (p.window_end - p.window_begin) / p.n_measurements
+    re, im = [], []
+    for tr in traces:
+        if cfg["laser_type"] == "continuous":  # no transform on the Welch branch (hhg.cpp:258-275)
+            r = i = np.zeros(p.n_measurements + 1)
+        else:
+            _, r, i = eng.trapezoidal_fft(tr, me, p.window_begin, p.window_end)
+        re.append(r.tolist())
+        im.append(i.tolist())
+    if frequencies is None:
+        zero = np.zeros(p.n_measurements + 1)
+        spec = eng.spectrum_welch if cfg["laser_type"] == "continuous" else eng.spectrum
+        frequencies, _, _ = spec(zero, p.n_measurements, p.window_begin, p.window_end)
+    return {"time": time.strftime("%Y-%m-%d %H:%M:%S"),
+            "frequencies": list(frequencies),
+            "time_evolutions": traces.tolist(),
+            "debug_fft_real": re, "debug_fft_imag": im}
+
+
 def run(eng: api.Engine, source: str) -> dict:
     """All modes a parameter file asks for: {"occupations": doc,
-    "split_current": doc, "current_density": doc} (present ones only)."""
+    "split_current": doc, "current_density": doc, "debug": doc} (present
+    ones only)."""
     cfg = config.read_config(source)
     out = {}
     if cfg.get("occupations", "no") != "no":
@@ -144,6 +184,8 @@ def run(eng: api.Engine, source: str) -> dict:
         if cfg["split_current"] == "only":
             return out
     out["current_density"] = current_density(eng, cfg)
+    if cfg.get("debug_data", "no") != "no":
+        out["debug"] = debug_traces(eng, cfg, frequencies=out["current_density"]["frequencies"])
     return out
 
 

@@ -145,9 +145,12 @@ typedef enum hhg_grid_kind {
     HHG_GRID_EXPLICIT = 4,         /* caller rows: kx, ky, kz, weight, S0x, S0y, S0z, 0 */
     HHG_GRID_PIFLUX3D_OCCUPATION = 5, /* PiFlux::compute_occupation_numbers grid (PiFlux.cpp:909-953):
                                          k = (x pi/N, pi/2, z pi/N), x, z < N = n1, row x N + z */
-    HHG_GRID_PIFLUX3D_CUBE = 6     /* PiFlux::current_per_energy grid (PiFlux.cpp:955-1035): k =
+    HHG_GRID_PIFLUX3D_CUBE = 6,    /* PiFlux::current_per_energy grid (PiFlux.cpp:955-1035): k =
                                       (x, y, +-z) pi/N, x, y, z < N = n1, weight 1/N^3, rows
                                       2 (z N^2 + y N + x) + (0: +z, 1: -z) */
+    HHG_GRID_PIFLUX3D_DEBUG = 7    /* PiFlux::compute_current_density_debug momenta (PiFlux.cpp:320-371):
+                                      k = (pi/2, pi/2 - 0.02 pi i, 0.49 pi), i < 25 (n_debug_points,
+                                      GlobalDefinitions.hpp), weight 1; no size parameters */
 } hhg_grid_kind;
 
 typedef struct hhg_grid_desc {
@@ -508,6 +511,16 @@ hhg_status hhg_gpu_dirac_current_density(hhg_ctx *ctx, const hhg_system_desc *sy
 hhg_status hhg_gpu_spectrum_welch(hhg_ctx *ctx, const double *j, int n_measurements,
                                   double t_begin, double t_end, double *re_out, double *im_out,
                                   double *freq_out);
+
+/* TrapezoidalFFT::compute (TrapezoidalFFT.cpp:11-49) of n_input samples as
+ * given, without padding: delta_t = measure_every, [t_begin, t_end] the
+ * TimeIntegrationConfig window, input[0] and input[n_input - 1] the end-point
+ * samples.  This is the call hhg.cpp:287-290 makes on each debug trace
+ * (n_input = n_measurements + 1).  re/im/freq receive n_input / 2 + 1 values
+ * each (host, caller-owned). */
+hhg_status hhg_gpu_trapezoidal_fft(hhg_ctx *ctx, const double *input, int64_t n_input,
+                                   double delta_t, double t_begin, double t_end, double *re_out,
+                                   double *im_out, double *freq_out);
 
 /* A(t) of a pulse at n times (host only; Laser::laser_function as the engine
  * stages it, e.g. for the reference's laser_function output, hhg.cpp:301-305). */

@@ -219,6 +219,42 @@ def grid_piflux3d_ref(m: OrcModel, z_range=32, n_coarse=4) -> np.ndarray:
     return out
 
 
+def grid_piflux3d_debug(m: OrcModel) -> np.ndarray:
+    """The 25 momenta of PiFlux::compute_current_density_debug
+    (PiFlux.cpp:320-371): momentum_type(pi/2, picked[i], 0.49 pi) with
+    picked[i] = 0.5 pi - i 0.02 pi, weight 1, the model's initial state."""
+    pi = 3.141592653589793
+    out = np.zeros((25, KROW))
+    for i in range(25):
+        kx, ky, kz = 0.5 * pi, 0.5 * pi - (i * 0.02 * pi), 0.49 * pi
+        out[i, :4] = (kx, ky, kz, 1.0)
+        out[i, 4:7] = initial_state(m, kx, ky, kz)
+    return out
+
+
+def trapezoidal_fft_unpadded(x: np.ndarray, delta_t: float, t_begin: float, t_end: float):
+    """TrapezoidalFFT::compute (TrapezoidalFFT.cpp:11-49) of x as given, as
+    hhg.cpp:287-290 applies it to each debug trace: (frequencies, real, imag)."""
+    x = np.asarray(x, dtype=np.float64)
+    n_in = x.size
+    F = np.fft.rfft(x)
+    n_fft = n_in // 2 + 1
+    freq = 2 * np.arange(n_fft) * np.pi / (n_in * delta_t)
+    theta = freq * delta_t
+    W = np.empty(n_fft)
+    a0 = np.empty(n_fft, dtype=np.complex128)
+    for i, th in enumerate(theta):
+        if _is_zero(th):
+            W[i] = 1.0
+            a0[i] = -0.5
+        else:
+            W[i] = 2.0 * (1.0 - np.cos(th)) / (th * th)
+            a0[i] = (-(1.0 - np.cos(th)) + 1j * (th - np.sin(th))) / (th * th)
+    corr = a0 * x[0] + np.conj(a0) * np.exp(1j * freq * (t_end - t_begin)) * x[n_in - 1]
+    out = (delta_t * W) * np.exp(1j * freq * t_begin) * F + corr
+    return freq, delta_t * out.real, delta_t * out.imag
+
+
 def grid_honeycomb_hex_ref(m: OrcModel, n_k=64) -> np.ndarray:
     n = lib().orc_grid_honeycomb_hex_ref(ctypes.byref(m), n_k, None)
     out = np.zeros((n, KROW))

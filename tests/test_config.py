@@ -93,7 +93,10 @@ def test_descriptors_pass_the_abi_checks():
     (("laser_type cosine", "laser_type expA"), config.UnsupportedConfig),
     (("system_type PiFlux", "system_type ModifiedPiFlux"), config.UnsupportedConfig),
     (("system_type PiFlux", "system_type Dirac\n"), None),
-    (("debug_data no", "debug_data yes"), config.UnsupportedConfig),
+    (("debug_data no", "debug_data yes"), None),
+    (("debug_data no\noccupations no\nsplit_current no\nsystem_type PiFlux",
+      "debug_data only\noccupations no\nsplit_current no\nsystem_type Honeycomb"),
+     config.UnsupportedConfig),
     (("system_type PiFlux", "system_type Graphene"), ValueError),
     (("E_F 118\n", ""), ValueError),
 ])

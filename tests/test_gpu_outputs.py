@@ -3,7 +3,8 @@ reference's run modes on the GPU (through the C ABI) against the CPU oracle.
 
 Reference: PiFlux::evolve_occupation_numbers / compute_occupation_numbers
 (PiFlux.cpp:222-318, 909-953), PiFlux::current_per_energy (PiFlux.cpp:955-1035),
-the continuous-laser spectrum (hhg.cpp:264-275) and the run modes of hhg.cpp.
+PiFlux::compute_current_density_debug (PiFlux.cpp:320-371), the continuous-laser
+spectrum (hhg.cpp:264-275) and the run modes of hhg.cpp.
 Bar: 1e-9 relative for the FP64 reference schedule, as the current density,
 for the Brillouin-zone sums.  Single trajectories agree to rounding except
 where an attempt sits on the controller's acceptance threshold and the GPU and
@@ -158,6 +159,49 @@ def test_run_modes_end_to_end(engine):
     assert set(main) >= {"current_density_time", "current_density_frequency_real", "frequencies",
                          "laser_function", "photon_energy", "zero_padding"}
     assert len(main["laser_function"]) == 65
+
+
+def test_trapezoidal_fft_unpadded(engine):
+    # TrapezoidalFFT::compute on the input as given (TrapezoidalFFT.cpp:11-49)
+    rng = np.random.default_rng(11)
+    for n_in in (129, 256, 1025):
+        x = rng.normal(size=n_in)
+        me, tb = 0.37, -1.3
+        te = tb + (n_in - 1) * me
+        fr, re, im = engine.trapezoidal_fft(x, me, tb, te)
+        rfr, rre, rim = O.trapezoidal_fft_unpadded(x, me, tb, te)
+        scale = np.abs(rre + 1j * rim).max()
+        assert fr.shape == (n_in // 2 + 1,)
+        assert np.allclose(fr, rfr, rtol=1e-15, atol=0)
+        assert np.max(np.abs((re - rre) + 1j * (im - rim))) <= 1e-13 * scale
+
+
+def test_debug_traces(engine):
+    # PiFlux's debug mode: S_z of the 25 momenta of PiFlux.cpp:320-371 with the
+    # relaxation dynamics, each transformed without padding (hhg.cpp:287-291)
+    cfg = config.read_config(CFG.replace("debug_data no", "debug_data yes"))
+    n = 128
+    doc = runmodes.debug_traces(engine, cfg, n_measurements=n)
+    run = config.from_config(cfg, grid=api.grid_piflux3d_debug(), n_measurements=n)
+    rows = api.grid_rows(run.system, run.grid)
+    m, p, tc, s = oracle_args(run.system, run.pulse, 1e-12, 1e-8)
+    ref, rc = O.k_resolved(m, p, tc, s, rows, 0)
+    tr = np.array(doc["time_evolutions"])
+    assert rc == 0 and tr.shape == (api.N_DEBUG_POINTS, n + 1)
+    err = np.max(np.abs(tr - ref[:, :, 2].T), axis=1)
+    assert err.max() <= 1e-7 and np.median(err) <= 1e-12, (err.max(), np.median(err))
+    assert np.ptp(tr, axis=1).min() > 1e-6  # the field moves every trace
+    pl = run.pulse
+    me = (pl.window_end - pl.window_begin) / n
+    for i in (0, 12, 24):
+        _, rre, rim = O.trapezoidal_fft_unpadded(tr[i], me, pl.window_begin, pl.window_end)
+        got = np.array(doc["debug_fft_real"][i]) + 1j * np.array(doc["debug_fft_imag"][i])
+        assert got.shape == ((n + 1) // 2 + 1,)
+        assert np.max(np.abs(got - (rre + 1j * rim))) <= 1e-13 * np.abs(rre + 1j * rim).max()
+    assert len(doc["frequencies"]) == 4 * (n + 1) + 1  # the main spectrum's padded grid
+    only = config.read_config(CFG.replace("debug_data no", "debug_data only"))
+    main = runmodes.current_density(engine, only, grid=api.grid_piflux3d_ref(1, 1), n_measurements=n)
+    assert not np.any(main["current_density_time"])  # hhg.cpp:235-236 skips the integration
 
 
 def test_outputs_refused_outside_piflux(engine):

@@ -89,6 +89,24 @@ def test_trapezoidal_fft_matches_direct_formula():
     assert np.allclose(fr, 2 * np.arange(len(fr)) * np.pi / (8 * (n + 1) * (te - tb) / n))
 
 
+def test_unpadded_transform_is_the_padded_one_on_padded_input():
+    # hhg.cpp transforms j after padding it x8 and each debug trace as given;
+    # both are TrapezoidalFFT::compute on the vector it receives
+    rng = np.random.default_rng(3)
+    n = 200
+    j = rng.normal(size=n + 1)
+    tb, te = -0.4, 9.6
+    f1, r1, i1 = O.trapezoidal_fft(j, tb, te, n)
+    x = np.zeros(O.ZERO_PADDING * (n + 1))
+    x[: n + 1] = j
+    f2, r2, i2 = O.trapezoidal_fft_unpadded(x, (te - tb) / n, tb, te)
+    assert np.array_equal(f1, f2) and np.array_equal(r1, r2) and np.array_equal(i1, i2)
+    f3, r3, i3 = O.trapezoidal_fft_unpadded(j, (te - tb) / n, tb, te)
+    assert f3.size == (n + 1) // 2 + 1
+    # the unpadded grid is every 8th frequency of the padded one
+    assert np.allclose(f3[1:], f1[8:8 * f3.size:8][: f3.size - 1], rtol=1e-14)
+
+
 def test_harmonics_of_a_pure_tone():
     # j(t) = sin(3t) env(t): the spectrum peaks at harmonic 3
     n = 4096

@@ -157,6 +157,18 @@ def test_abi_thermal_rows_match_oracle():
     assert np.allclose(rows, ref, rtol=1e-14, atol=1e-15)
 
 
+def test_abi_debug_rows_match_oracle():
+    # the debug traces' momenta (PiFlux.cpp:320-371), cold and thermal
+    for kw in ({}, {"beta": 1.3, "fermi_energy": 0.2, "inv_diag_relax": 0.4}):
+        sys = api.system(api.SYS_PIFLUX3D, hopping=0.9, **kw)
+        rows = api.grid_rows(sys, api.grid_piflux3d_debug())
+        okw = {k: v for k, v in kw.items() if k != "inv_diag_relax"}
+        ref = O.grid_piflux3d_debug(O.model(O.PIFLUX3D, hopping=0.9, **okw))
+        assert rows.shape == (api.N_DEBUG_POINTS, 8)
+        assert np.array_equal(rows[:, :4], ref[:, :4])
+        assert np.allclose(rows, ref, rtol=1e-14, atol=1e-15)
+
+
 def _grid_rows_status(sys, grid):
     lib = api.load_library()
     n = ctypes.c_int64(0)
