@@ -176,21 +176,29 @@ def test_trapezoidal_fft_unpadded(engine):
         assert np.max(np.abs((re - rre) + 1j * (im - rim))) <= 1e-13 * scale
 
 
-def test_debug_traces(engine):
-    # PiFlux's debug mode: S_z of the 25 momenta of PiFlux.cpp:320-371 with the
-    # relaxation dynamics, each transformed without padding (hhg.cpp:287-291)
-    cfg = config.read_config(CFG.replace("debug_data no", "debug_data yes"))
-    n = 128
+def _debug_case(engine, cfg_text, n):
+    cfg = config.read_config(cfg_text.replace("debug_data no", "debug_data yes"))
     doc = runmodes.debug_traces(engine, cfg, n_measurements=n)
     run = config.from_config(cfg, grid=api.grid_piflux3d_debug(), n_measurements=n)
     rows = api.grid_rows(run.system, run.grid)
-    m, p, tc, s = oracle_args(run.system, run.pulse, 1e-12, 1e-8)
-    ref, rc = O.k_resolved(m, p, tc, s, rows, 0)
+    args = oracle_args(run.system, run.pulse, 1e-12, 1e-8)
+    ref, rc = O.k_resolved(*args, rows, 0)
     tr = np.array(doc["time_evolutions"])
     assert rc == 0 and tr.shape == (api.N_DEBUG_POINTS, n + 1)
+    return doc, run, rows, args, ref, tr
+
+
+def test_debug_traces_coherent(engine):
+    # PiFlux's debug mode (PiFlux.cpp:320-371): S_z of its 25 momenta from the
+    # thermal state under the coherent dynamics, each transformed without
+    # padding (hhg.cpp:287-291).  Trace 0 has cos kx = cos ky = 0 (to rounding):
+    # d is along z, so S_z stays constant.
+    n = 128
+    coherent = CFG.replace("diagonal_relaxation_time 20", "diagonal_relaxation_time -1")
+    doc, run, rows, args, ref, tr = _debug_case(engine, coherent, n)
     err = np.max(np.abs(tr - ref[:, :, 2].T), axis=1)
-    assert err.max() <= 1e-7 and np.median(err) <= 1e-12, (err.max(), np.median(err))
-    assert np.ptp(tr, axis=1).min() > 1e-6  # the field moves every trace
+    assert err.max() <= 1e-9, err
+    assert np.ptp(tr[1:], axis=1).min() > 0.1 and np.ptp(tr[0]) < 1e-12
     pl = run.pulse
     me = (pl.window_end - pl.window_begin) / n
     for i in (0, 12, 24):
@@ -202,6 +210,35 @@ def test_debug_traces(engine):
     only = config.read_config(CFG.replace("debug_data no", "debug_data only"))
     main = runmodes.current_density(engine, only, grid=api.grid_piflux3d_ref(1, 1), n_measurements=n)
     assert not np.any(main["current_density_time"])  # hhg.cpp:235-236 skips the integration
+
+
+def test_debug_traces_relaxation(engine):
+    # With relaxation at T > 0 the right-hand side reads the step's start state,
+    # and several of the 25 trajectories amplify rounding: the oracle itself
+    # moves by up to ~1e-6 when the initial state changes by 2e-16 (relative)
+    # or kx by 1e-15 (trace 0 crosses d = 0).  The GPU is held to rounding on the
+    # well-conditioned trajectories and to the oracle's own spread elsewhere.
+    n = 128
+    doc, run, rows, args, ref, tr = _debug_case(engine, CFG, n)
+    err = np.max(np.abs(tr - ref[:, :, 2].T), axis=1)
+    perturbed = []
+    for f in (1 + 2e-16, 1 - 2e-16):  # the initial state
+        q = rows.copy()
+        q[:, 4:7] *= f
+        perturbed.append(q)
+    for dk in (1e-15, -1e-15):  # kx = pi/2, whose cosine is rounding noise
+        q = rows.copy()
+        q[:, 0] += dk
+        perturbed.append(q)
+    spread = np.zeros(api.N_DEBUG_POINTS)
+    for q in perturbed:
+        alt, rc = O.k_resolved(*args, q, 0)
+        assert rc == 0
+        spread = np.maximum(spread, np.max(np.abs(alt[:, :, 2] - ref[:, :, 2]), axis=0))
+    well = spread < 1e-12
+    assert well.sum() >= 3, spread
+    assert err[well].max() <= 1e-10, (err, spread)
+    assert err.max() <= 10 * spread.max(), (err, spread)
 
 
 def test_outputs_refused_outside_piflux(engine):
