@@ -22,9 +22,9 @@ STATUS_NAMES = {0: "HHG_OK", 1: "HHG_BAD_CONFIG", 2: "HHG_STEP_LIMIT", 3: "HHG_N
                 4: "HHG_CUDA_ERROR", 5: "HHG_UNSUPPORTED"}
 SYS_DIRAC2D, SYS_PIFLUX2D, SYS_PIFLUX3D, SYS_HONEYCOMB, SYS_DIRAC3D = range(5)
 (GRID_TENSOR_GL, GRID_RHOMBIC_GL, GRID_PIFLUX3D_REF, GRID_HONEYCOMB_HEX_REF, GRID_EXPLICIT,
- GRID_PIFLUX3D_OCCUPATION, GRID_PIFLUX3D_CUBE, GRID_PIFLUX3D_DEBUG) = range(8)
+ GRID_PIFLUX3D_OCCUPATION, GRID_PIFLUX3D_CUBE, GRID_PIFLUX3D_DEBUG, GRID_DIRAC3D_DEBUG) = range(9)
 N_DEBUG_POINTS = 25  # n_debug_points (GlobalDefinitions.hpp)
-KOUT_BLOCH, KOUT_OCCUPATIONS = 0, 1
+KOUT_BLOCH, KOUT_OCCUPATIONS, KOUT_CURRENT = 0, 1, 2
 STEPPER_RKF78, STEPPER_MAGNUS4, STEPPER_DIRAC_MAGNUS = 0, 1, 2
 PREC_FP64, PREC_MIXED = 0, 1
 PROPOSER_NONE, PROPOSER_CARRY, PROPOSER_LEARNED, PROPOSER_LOCKSTEP = 0, 1, 2, 3
@@ -364,6 +364,13 @@ def grid_piflux3d_debug() -> GridDesc:
     return GridDesc(GRID_PIFLUX3D_DEBUG, 0, 0, 0, 0, 0, 0, 0, None, 0)
 
 
+def grid_dirac3d_debug(n_z: int, max_k: float) -> GridDesc:
+    """The 25 (k_z, kappa) of DiracSystem::compute_current_density_debug
+    (DiracSystem.cpp:333-363): k_z = (n_z/10) 2 max_k / n_z, kappa_i =
+    (i + 1) kappa_max / 26, weighted by k_z kappa / |k|."""
+    return GridDesc(GRID_DIRAC3D_DEBUG, n_z, 0, 0, 0.0, max_k, 0, 0, None, 0)
+
+
 def pulse_values(pulse: PulseDesc, t) -> np.ndarray:
     """A(t) of a pulse as the engine stages it (host)."""
     t = np.ascontiguousarray(np.atleast_1d(t), dtype=np.float64)
@@ -495,16 +502,17 @@ class Engine:
     def k_resolved(self, sys: SystemDesc, pulse: PulseDesc, grid: GridDesc,
                    opts: SolverOpts | None = None, kind: int = KOUT_BLOCH):
         """Every trajectory at every sample: (n_measurements + 1, n_k, 3) Bloch
-        vectors or (.., 2) band occupations (hhg_gpu_k_resolved)."""
+        vectors, (.., 2) band occupations or (n_measurements + 1, n_k) weighted
+        currents (hhg_gpu_k_resolved)."""
         n_k = int(grid_rows(sys, grid).shape[0])
-        w = 3 if kind == KOUT_BLOCH else 2
+        w = 3 if kind == KOUT_BLOCH else (2 if kind == KOUT_OCCUPATIONS else 1)
         out = np.zeros((pulse.n_measurements + 1, n_k, w))
         st = Stats()
         self._check(self.lib.hhg_gpu_k_resolved(self.ctx, ctypes.byref(sys), ctypes.byref(pulse),
                                                 ctypes.byref(grid),
                                                 ctypes.byref(opts) if opts else None, kind,
                                                 _ptr(out), ctypes.byref(st)), "hhg_gpu_k_resolved")
-        return out, st
+        return (out[..., 0] if w == 1 else out), st
 
     def split_current(self, sys: SystemDesc, pulse: PulseDesc, grid: GridDesc,
                       opts: SolverOpts | None = None, energy_cut: float = 0.5 * math.sqrt(3.0)):

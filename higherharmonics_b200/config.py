@@ -45,9 +45,9 @@ coherent path is the closed-form Magnus step, the relaxation path FP64 RKF78
 occupation and split-current run modes are in higherharmonics_b200.runmodes;
 requesting either shortens the double / Gaussian / experimental laser windows to
 0.75 t_end for every mode, as the dispatcher's reduced_duration does
-(PiFluxDispatcher.cpp:45).  debug_data yes / only selects PiFlux's debug
-traces in higherharmonics_b200.runmodes; for Honeycomb (whose reference
-throws) and Dirac it raises UnsupportedConfig.  data_dir and n_z are read by
+(PiFluxDispatcher.cpp:45).  debug_data yes / only selects the PiFlux
+or Dirac debug traces in higherharmonics_b200.runmodes; for Honeycomb (whose
+reference throws) it raises UnsupportedConfig.  data_dir and n_z are read by
 the run modes only.
 """
 from __future__ import annotations
@@ -130,9 +130,6 @@ def from_config(cfg: dict | str, *, grid: api.GridDesc | None = None,
     if cfg.get("debug_data", "no") != "no" and system_type == "Honeycomb":
         # Honeycomb.cpp:111-115
         raise UnsupportedConfig("Honeycomb::compute_current_density_debug is not implemented yet!")
-    if cfg.get("debug_data", "no") != "no" and system_type == "Dirac":
-        raise UnsupportedConfig(f"debug_data = {cfg['debug_data']}: the Dirac debug traces "
-                                "(DiracSystem.cpp:333-363) are not built")
     reduced = cfg.get("occupations", "no") != "no" or cfg.get("split_current", "no") != "no"
     laser_type = cfg.get("laser_type", "")
     known = {"cosine", "continuous", "gauss", "quench", "exp", "expA", "expB"} | set(DOUBLE_LASERS)

@@ -288,6 +288,7 @@ int64_t grid_count(const hhg_grid_desc &g) {
     case HHG_GRID_PIFLUX3D_CUBE:
         return 2 * (int64_t)g.n1 * g.n1 * g.n1;
     case HHG_GRID_PIFLUX3D_DEBUG:
+    case HHG_GRID_DIRAC3D_DEBUG:
         return kDebugPoints;
     }
     return -1;
@@ -456,6 +457,23 @@ void build_rows(const hhg_system_desc &s, const hhg_grid_desc &g, double *out) {
         for (int i = 0; i < kDebugPoints; ++i)
             push_row(s, 0.5 * kPi, 0.5 * kPi - (i * 0.02 * kPi), 0.49 * kPi, 1.0, out + 8 * r++);
         break;
+    case HHG_GRID_DIRAC3D_DEBUG: {
+        // DiracSystem::compute_current_density_debug (DiracSystem.cpp:333-363):
+        // picked_z = n_z/2 + n_z/10, delta_z = 2 max_k / n_z, kappa_max from
+        // kappa_integration_upper_limit (DiracSystem.cpp:257-261), rows
+        // (k_z, kappa, |k|) weighted by integration_weight k_z kappa / |k|
+        const int n_z = g.n1;
+        const double max_k = g.x_hi;
+        const double delta_z = 2 * max_k / n_z;
+        const double k_z = (n_z / 2 + n_z / 10 - n_z / 2) * delta_z;
+        const double kappa_max = std::sqrt(max_k * max_k - k_z * k_z);
+        for (int i = 0; i < kDebugPoints; ++i) {
+            const double kappa = (i + 1) * kappa_max / (kDebugPoints + 1);
+            const double mk = std::sqrt(k_z * k_z + kappa * kappa);
+            push_row(s, k_z, kappa, mk, k_z * kappa / mk, out + 8 * r++);
+        }
+        break;
+    }
     }
 }
 
@@ -505,6 +523,10 @@ hhg_status check_grid(hhg_ctx *ctx, const hhg_grid_desc *g) {
         if (g->n1 < 1 || g->n1 > 1024) return set_err(ctx, HHG_BAD_CONFIG, "cube grid N out of range");
         break;
     case HHG_GRID_PIFLUX3D_DEBUG:
+        break;
+    case HHG_GRID_DIRAC3D_DEBUG:
+        if (g->n1 < 1 || g->n1 > (1 << 24) || !(g->x_hi > 0.0) || !std::isfinite(g->x_hi))
+            return set_err(ctx, HHG_BAD_CONFIG, "Dirac debug grid needs n_z >= 1 and max_k > 0");
         break;
     default:
         return set_err(ctx, HHG_BAD_CONFIG, "grid type not recognized");
@@ -1998,15 +2020,27 @@ hhg_status output_plan(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_pulse
                        hhg_plan **out) {
     *out = nullptr;
     if (!sys || !pulse || !grid) return set_err(ctx, HHG_BAD_CONFIG, "null descriptor");
-    if (sys->kind != HHG_SYS_PIFLUX3D)
-        return set_err(ctx, HHG_UNSUPPORTED, "k-resolved and split-current outputs are PiFlux-3D's");
     hhg_solver_opts o;
     hhg_default_solver_opts(&o);
     if (opts) o = *opts;
-    if (o.stepper != HHG_STEPPER_RKF78 || o.precision != HHG_PREC_FP64 ||
-        (o.proposer != HHG_PROPOSER_NONE && o.proposer != HHG_PROPOSER_CARRY))
-        return set_err(ctx, HHG_UNSUPPORTED,
-                       "k-resolved and split-current outputs run FP64 RKF78 with the NONE or CARRY proposer");
+    if (mode == 4) {
+        // per-trajectory weighted currents: the Dirac-3D kernels of its quadrature
+        if (sys->kind != HHG_SYS_DIRAC3D)
+            return set_err(ctx, HHG_UNSUPPORTED, "per-trajectory currents are Dirac-3D's");
+        const bool relax = sys->inv_diag_relax > 0.0;
+        if (o.precision != HHG_PREC_FP64 || o.proposer != HHG_PROPOSER_NONE ||
+            !(o.stepper == HHG_STEPPER_RKF78 || (!relax && o.stepper == HHG_STEPPER_DIRAC_MAGNUS)))
+            return set_err(ctx, HHG_UNSUPPORTED,
+                           "per-trajectory currents run FP64 with the NONE proposer: the closed-form "
+                           "Magnus step (coherent) or RKF78");
+    } else {
+        if (sys->kind != HHG_SYS_PIFLUX3D)
+            return set_err(ctx, HHG_UNSUPPORTED, "k-resolved and split-current outputs are PiFlux-3D's");
+        if (o.stepper != HHG_STEPPER_RKF78 || o.precision != HHG_PREC_FP64 ||
+            (o.proposer != HHG_PROPOSER_NONE && o.proposer != HHG_PROPOSER_CARRY))
+            return set_err(ctx, HHG_UNSUPPORTED,
+                           "k-resolved and split-current outputs run FP64 RKF78 with the NONE or CARRY proposer");
+    }
     hhg_plan *pl = nullptr;
     hhg_status st = plan_create_impl(ctx, sys, pulse, 1, grid, &o, &pl, false);  // k order kept
     if (st != HHG_OK) return st;
@@ -2024,7 +2058,7 @@ hhg_status output_plan(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_pulse
         if ((e = cudaMalloc(&pl->d_part, 2 * pl->part_len * sizeof(double))) != cudaSuccess) return fail("alloc partials", e);
         if ((e = cudaMalloc(&pl->d_j, 2 * pl->j_len * sizeof(double))) != cudaSuccess) return fail("alloc j", e);
     } else {
-        const int width = mode == 2 ? 3 : 2;
+        const int width = mode == 2 ? 3 : (mode == 3 ? 2 : 1);
         pl->kout_len = (long long)(pulse->n_measurements + 1) * pl->n_k * width;
         if ((e = cudaMalloc(&pl->d_kout, pl->kout_len * sizeof(double))) != cudaSuccess)
             return fail("alloc k-resolved output", e);
@@ -2055,10 +2089,11 @@ hhg_status hhg_gpu_k_resolved(hhg_ctx *ctx, const hhg_system_desc *sys, const hh
                               const hhg_grid_desc *grid, const hhg_solver_opts *opts, int kind,
                               double *out, hhg_stats *stats) {
     if (!ctx || !out) return set_err(ctx, HHG_BAD_CONFIG, "null context or output");
-    if (kind != HHG_KOUT_BLOCH && kind != HHG_KOUT_OCCUPATIONS)
+    if (kind != HHG_KOUT_BLOCH && kind != HHG_KOUT_OCCUPATIONS && kind != HHG_KOUT_CURRENT)
         return set_err(ctx, HHG_BAD_CONFIG, "unknown k-resolved observable");
     hhg_plan *pl = nullptr;
-    hhg_status st = output_plan(ctx, sys, pulse, grid, opts, kind == HHG_KOUT_BLOCH ? 2 : 3, &pl);
+    const int mode = kind == HHG_KOUT_BLOCH ? 2 : (kind == HHG_KOUT_OCCUPATIONS ? 3 : 4);
+    hhg_status st = output_plan(ctx, sys, pulse, grid, opts, mode, &pl);
     if (st != HHG_OK) return st;
     st = hhg_plan_execute_async(pl, nullptr);
     if (st == HHG_OK) st = hhg_plan_fetch(pl, nullptr, stats);

@@ -4,8 +4,8 @@
 reference's order: the occupation tracking (occupations != "no",
 hhg.cpp:120-168), the energy-split current (split_current != "no",
 hhg.cpp:170-219) and, unless either says "only", the current density with its
-spectrum (hhg.cpp:236-337), followed by PiFlux's debug traces when debug_data
-is "yes" or "only" (hhg.cpp:235-238, 287-291, 343-352).  Each mode returns the
+spectrum (hhg.cpp:236-337), followed by the PiFlux or Dirac debug traces when
+debug_data is "yes" or "only" (hhg.cpp:235-238, 287-291, 343-352).  Each mode returns the
 JSON document the reference writes (the same keys; the metadata files are not
 produced), and `save` writes one gzip-compressed as `*.json.gz`.
 
@@ -137,19 +137,29 @@ def split_current(eng: api.Engine, cfg: dict, N: int | None = None,
 
 def debug_traces(eng: api.Engine, cfg: dict, n_measurements: int | None = None,
                  frequencies=None) -> dict:
-    """PiFlux::compute_current_density_debug (PiFlux.cpp:320-371): S_z(t_i) of
-    the 25 momenta k = (pi/2, pi/2 - 0.02 pi i, 0.49 pi) with the system's
-    dynamics (coherent or relaxation), each transformed by TrapezoidalFFT
-    without padding (hhg.cpp:287-291).  The document is time_evolution.json
+    """The debug traces: PiFlux::compute_current_density_debug
+    (PiFlux.cpp:320-371), S_z(t_i) of the 25 momenta k = (pi/2, pi/2 - 0.02 pi i,
+    0.49 pi) with the system's dynamics (coherent or relaxation), or the Dirac
+    system's 25 weighted (k_z, kappa) currents, each transformed by
+    TrapezoidalFFT without padding (hhg.cpp:287-291).  The document is time_evolution.json
     (hhg.cpp:343-352); its "frequencies" are the main spectrum's
     (`frequencies`, the 8x padded grid, as the reference stores them)."""
-    if cfg["system_type"] != "PiFlux":
-        raise config.UnsupportedConfig("debug traces are built for PiFlux only "
-                                       "(PiFluxDispatcher.cpp:128-136)")
-    run = config.from_config(cfg, grid=api.grid_piflux3d_debug(), n_measurements=n_measurements)
-    p = run.pulse
-    S, _ = eng.k_resolved(run.system, p, run.grid, run.opts, kind=api.KOUT_BLOCH)
-    traces = np.ascontiguousarray(S[:, :, 2].T)  # [point][sample]
+    if cfg["system_type"] == "Dirac":
+        # DiracSystem::compute_current_density_debug and its relaxation twin
+        # (DiracSystem.cpp:333-363, 427-457): the weighted current of 25 (k_z,
+        # kappa) trajectories, by the dispatcher's stepper (DiracDispatcher.cpp:82-92)
+        run = config.from_config(cfg, n_measurements=n_measurements)
+        p = run.pulse
+        grid = api.grid_dirac3d_debug(run.quad.n_z, run.quad.max_k)
+        cur, _ = eng.k_resolved(run.system, p, grid, run.opts, kind=api.KOUT_CURRENT)
+        traces = np.ascontiguousarray(cur.T)
+    elif cfg["system_type"] == "PiFlux":
+        run = config.from_config(cfg, grid=api.grid_piflux3d_debug(), n_measurements=n_measurements)
+        p = run.pulse
+        S, _ = eng.k_resolved(run.system, p, run.grid, run.opts, kind=api.KOUT_BLOCH)
+        traces = np.ascontiguousarray(S[:, :, 2].T)  # [point][sample]
+    else:
+        raise config.UnsupportedConfig("Honeycomb::compute_current_density_debug is not implemented yet!")
     me = (p.window_end - p.window_begin) / p.n_measurements
     re, im = [], []
     for tr in traces:

@@ -148,9 +148,13 @@ typedef enum hhg_grid_kind {
     HHG_GRID_PIFLUX3D_CUBE = 6,    /* PiFlux::current_per_energy grid (PiFlux.cpp:955-1035): k =
                                       (x, y, +-z) pi/N, x, y, z < N = n1, weight 1/N^3, rows
                                       2 (z N^2 + y N + x) + (0: +z, 1: -z) */
-    HHG_GRID_PIFLUX3D_DEBUG = 7    /* PiFlux::compute_current_density_debug momenta (PiFlux.cpp:320-371):
+    HHG_GRID_PIFLUX3D_DEBUG = 7,   /* PiFlux::compute_current_density_debug momenta (PiFlux.cpp:320-371):
                                       k = (pi/2, pi/2 - 0.02 pi i, 0.49 pi), i < 25 (n_debug_points,
                                       GlobalDefinitions.hpp), weight 1; no size parameters */
+    HHG_GRID_DIRAC3D_DEBUG = 8     /* DiracSystem::compute_current_density_debug (DiracSystem.cpp:333-363,
+                                      427-457): n1 = n_z, x_hi = max_k; k_z = (n_z/10) 2 max_k / n_z,
+                                      kappa_i = (i + 1) kappa_max / 26 with kappa_max =
+                                      sqrt(max_k^2 - k_z^2), i < 25; weight k_z kappa / |k| */
 } hhg_grid_kind;
 
 typedef struct hhg_grid_desc {
@@ -259,8 +263,10 @@ typedef struct hhg_plan hhg_plan;
 /* k-resolved observables (hhg_gpu_k_resolved). */
 typedef enum hhg_kresolved {
     HHG_KOUT_BLOCH = 0,       /* the Bloch vector S: 3 doubles */
-    HHG_KOUT_OCCUPATIONS = 1  /* lower and upper band amplitudes of S at k - A(t_i):
+    HHG_KOUT_OCCUPATIONS = 1, /* lower and upper band amplitudes of S at k - A(t_i):
                                  sqrt((|S| -+ S.d_hat)/2), 2 doubles (PiFlux.cpp:227-235) */
+    HHG_KOUT_CURRENT = 2      /* the trajectory's weighted current, weight x the
+                                 system's time-evolution output: 1 double (Dirac-3D) */
 } hhg_kresolved;
 
 /* The Dirac system's momentum quadrature (DiracSystem::compute_current_density
@@ -465,7 +471,12 @@ hhg_status hhg_mlp_predict(hhg_ctx *ctx, const float *records, int64_t n_records
 
 /* k-resolved samples of one pulse: out[(i n_k + k) width + c] for every sample i
  * <= n_measurements and k-point k (host memory, (n_measurements + 1) n_k width
- * doubles), width 3 (HHG_KOUT_BLOCH) or 2 (HHG_KOUT_OCCUPATIONS).  The
+ * doubles), width 3 (HHG_KOUT_BLOCH), 2 (HHG_KOUT_OCCUPATIONS) or 1
+ * (HHG_KOUT_CURRENT).  HHG_KOUT_CURRENT is the Dirac-3D system's: its debug
+ * traces (DiracSystem::compute_current_density_debug and the relaxation twin,
+ * DiracSystem.cpp:333-363, 427-457) are HHG_KOUT_CURRENT on
+ * HHG_GRID_DIRAC3D_DEBUG, with the closed-form Magnus stepper (coherent) or FP64
+ * RKF78 (relaxation), proposer NONE; a trajectory that failed reads 0.  The
  * reference's occupation tracking (PiFlux::evolve_occupation_numbers and
  * compute_occupation_numbers, PiFlux.cpp:222-318 and 909-953; the occupations
  * mode of hhg.cpp:120-168) is HHG_KOUT_OCCUPATIONS on

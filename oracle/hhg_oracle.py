@@ -232,6 +232,25 @@ def grid_piflux3d_debug(m: OrcModel) -> np.ndarray:
     return out
 
 
+def grid_dirac3d_debug(m: OrcModel, n_z: int, max_k: float) -> np.ndarray:
+    """The 25 rows of DiracSystem::compute_current_density_debug
+    (DiracSystem.cpp:333-363): k_z = (picked_z - n_z/2) delta_z with picked_z =
+    n_z/2 + n_z/10 and delta_z = 2 max_k / n_z, kappa_i = (i + 1) kappa_max / 26
+    (kappa_max = sqrt(max_k^2 - k_z^2), DiracSystem.cpp:257-261), weight
+    integration_weight = k_z kappa / |k|, the model's initial state."""
+    import math
+    delta_z = 2 * max_k / n_z
+    k_z = (n_z // 2 + n_z // 10 - n_z // 2) * delta_z
+    kappa_max = math.sqrt(max_k * max_k - k_z * k_z)
+    out = np.zeros((25, KROW))
+    for i in range(25):
+        kappa = (i + 1) * kappa_max / 26
+        mk = math.sqrt(k_z * k_z + kappa * kappa)
+        out[i, :4] = (k_z, kappa, mk, k_z * kappa / mk)
+        out[i, 4:7] = initial_state(m, k_z, kappa, mk)
+    return out
+
+
 def trapezoidal_fft_unpadded(x: np.ndarray, delta_t: float, t_begin: float, t_end: float):
     """TrapezoidalFFT::compute (TrapezoidalFFT.cpp:11-49) of x as given, as
     hhg.cpp:287-290 applies it to each debug trace: (frequencies, real, imag)."""

@@ -8,6 +8,8 @@ adaptive trapezoidal kappa rule (restated from the reference's call, its
 library being unavailable; see tests/test_oracle_kappa.py).  Bar: the same
 refinement (rounds, levels, nodes) as the oracle, and j(t) relative L2
 <= 1e-12 for the closed-form Magnus path (no step control), 1e-9 for RKF78.
+The debug traces (DiracSystem.cpp:333-363, 427-457) are held to the same bars
+trajectory by trajectory.
 """
 import math
 
@@ -118,6 +120,34 @@ def test_dirac_config_end_to_end(engine):
     j = np.array(doc["current_density_time"])
     assert rel_l2(j, jr) <= 1e-12 and np.max(np.abs(jr)) > 0
     assert len(doc["frequencies"]) == len(doc["current_density_frequency_real"])
+
+
+@pytest.mark.parametrize("relax", [False, True])
+def test_dirac_debug_traces(engine, relax):
+    # DiracSystem::compute_current_density_debug and its relaxation twin
+    # (DiracSystem.cpp:333-363, 427-457): the weighted current of 25 (k_z, kappa)
+    # trajectories at picked_z = n_z/2 + n_z/10, each transformed without padding
+    text = DIRAC_CFG.replace("debug_data no", "debug_data yes").replace("n_z 6", "n_z 20")
+    if relax:
+        text = text.replace("diagonal_relaxation_time -1", "diagonal_relaxation_time 20")
+    cfg = config.read_config(text)
+    n = 128
+    doc = runmodes.debug_traces(engine, cfg, n_measurements=n)
+    run = config.from_config(cfg, n_measurements=n)
+    rows = api.grid_rows(run.system, api.grid_dirac3d_debug(run.quad.n_z, run.quad.max_k))
+    stepper = api.STEPPER_RKF78 if relax else api.STEPPER_DIRAC_MAGNUS
+    m, p, tc, s = oracle_args(run.system, run.pulse, 1e-12, 1e-8, stepper=stepper)
+    tr = np.array(doc["time_evolutions"])
+    assert tr.shape == (api.N_DEBUG_POINTS, n + 1)
+    for i in range(api.N_DEBUG_POINTS):
+        ref, _, rc = O.current_density(m, p, tc, s, rows[i:i + 1])
+        assert rc == 0 and np.ptp(ref) > 0
+        assert rel_l2(tr[i], ref) <= (1e-9 if relax else 1e-12), i
+    pl = run.pulse
+    me = (pl.window_end - pl.window_begin) / n
+    _, rre, rim = O.trapezoidal_fft_unpadded(tr[7], me, pl.window_begin, pl.window_end)
+    got = np.array(doc["debug_fft_real"][7]) + 1j * np.array(doc["debug_fft_imag"][7])
+    assert np.max(np.abs(got - (rre + 1j * rim))) <= 1e-13 * np.abs(rre + 1j * rim).max()
 
 
 def test_refusals(engine):

@@ -169,6 +169,16 @@ def test_abi_debug_rows_match_oracle():
         assert np.allclose(rows, ref, rtol=1e-14, atol=1e-15)
 
 
+def test_abi_dirac_debug_rows_match_oracle():
+    # DiracSystem::compute_current_density_debug's (k_z, kappa) rows
+    for n_z, max_k, kw in ((58, 15.0, {}), (20, 3.0, {"beta": 0.8, "fermi_energy": 0.3})):
+        rows = api.grid_rows(api.system(api.SYS_DIRAC3D, **kw), api.grid_dirac3d_debug(n_z, max_k))
+        ref = O.grid_dirac3d_debug(O.model(O.DIRAC3D, **kw), n_z, max_k)
+        assert rows.shape == (api.N_DEBUG_POINTS, 8) and np.array_equal(rows, ref)
+        assert rows[0, 0] == (n_z // 10) * (2 * max_k / n_z) > 0
+    assert _grid_rows_status(api.system(api.SYS_DIRAC3D), api.grid_dirac3d_debug(0, 1.0)) == api.BAD_CONFIG
+
+
 def _grid_rows_status(sys, grid):
     lib = api.load_library()
     n = ctypes.c_int64(0)
