@@ -706,9 +706,9 @@ def dirac_arm(args):
         "kappa": qs.as_dict(),
         "gpu_launches": launches,
         "roofline": {"bound": "fp64_pipe", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                     "frac": achieved / peak, "traffic": traffic_from_profile("dirac3d_kappa"),
+                     "frac": achieved / peak, "traffic": traffic_from_profile(args.workload),
                      "traffic_note": "DRAM bytes of the first integration launch (99 % of the "
-                                     "k.intervals), scaled from the committed ncu capture",
+                                     "k.steps), scaled from the committed ncu capture",
                      "peak_source": "measured FP64 FMA throughput (hhg_measure_fp64_peak, burst)",
                      "kernel": "bz_integrate_kernel (closed-form Magnus, per-trajectory output)",
                      "kernel_ms": kern_ms / args.steps,
