@@ -1,16 +1,28 @@
 #!/usr/bin/env python
-"""Benchmark: spectra/s of the per-k-point Bloch integration -> BZ current
-sum -> trapezoidal FFT path on the 256x256 PiFlux-2D workload.
+"""Benchmark: spectra/s of the per-k-point Bloch integration -> Brillouin-zone
+current sum -> trapezoidal FFT path, learned-step mixed-precision engine vs
+plain FP64 RKF78, on the learned-proposer workload: honeycomb with staggered
+mass 0.1 on a 1024 x 1024 rhombic Gauss-Legendre grid x 64 pulse instances
+(A0 ~ U[0.5, 2], carrier phase ~ U[0, 2 pi), omega = 0.08, 6 cycles, 6144
+intervals), seeded synthetic inputs.
 
-One step = one spectrum: integrate all 65 536 k-points over the 8-cycle
-pulse (8192 measurement intervals), reduce j(t), FFT it.
+One step = one batch of 8 of the 64 pulse instances: 8.4 M trajectories in
+one persistent work-stealing launch, the BZ reduction and 8 trapezoidal FFTs,
+replayed as one CUDA graph.  Consecutive steps take consecutive batches, so 8
+timed steps cover all 64 spectra once.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--variant NAME]
-  python bench.py --impl reference ...   # the oracle port on the host cores
+                  [--workload NAME] [--scaling weak|strong]
+  python bench.py --impl reference ...   # the reference's algorithm (the
+                                         # oracle port) on the host cores
 
-Under torchrun (N > 1) every rank integrates its own pulse instance (the
-carrier phase differs per rank): weak scaling with no data-path collective;
-the only collectives are the barrier and the max-over-ranks timing.
+--gpus N without torchrun re-launches itself under torch.distributed.run with
+N ranks (one GPU each).  Weak scaling (default): every rank integrates its own
+batches (rank r takes batch k N + r at step k), no data-path collective.
+Strong scaling: every rank integrates a contiguous block of each batch's k
+rows (the reference's jobs_per_rank blocks, PiFlux.cpp:811-820) and j(t) is
+summed over the ranks with one NCCL all_reduce before the FFT (the
+reference's MPI_Reduce, sources/hhg.cpp:240-246).
 """
 from __future__ import annotations
 
@@ -28,27 +40,29 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "spectra/sec at harmonic err <=1e-4 vs FP64"
+METRIC = "spectra/sec at harmonic err <=1e-4 vs FP64; learned+FP32 vs plain FP64"
 UNIT = "spectra/s"
+DEFAULT_WORKLOAD = "honeycomb_1024x64"
+SEED = 20261203
+MEASUREMENTS_PER_CYCLE = 1 << 10
 
 # Algorithmic FP64 flops per attempted RKF78 step (one k-point): 13 right-hand
 # sides plus the tableau arithmetic 2*3*55 (stages) + 2*3*7 (solution) +
-# 2*3*4 (error) + ~25 (norm and control) = 421; the right-hand side of the
-# 2D pi-flux model costs 12 flops plus two cosines (counted separately).
-# The PiFlux relaxation right-hand side (PiFlux.cpp:113-186 in the kernel's
-# form: off-diagonal equilibrium as the normalised perpendicular part of the
-# start state, Fermi pair through one reciprocal square root) costs 76 flops:
-# cos(kz - A) 3, |u|^2 5, |u| 1, occupation energies 4, Fermi pair 11,
-# g_d (a2 - b2)/|u| 2, coherent part with -g_s S + g_d r_d 24, perpendicular
-# projection, its norm and the g_o term 26; plus 5 special operations (2 exp,
-# 3 rsqrt).
+# 2*3*4 (error) + ~25 (norm and control) = 421.  Right-hand sides: 2D pi-flux
+# 12 flops + two cosines; gapped Dirac 16; honeycomb 30 (three complex bond
+# phases, the mass and the cross product) + three sincos.  The PiFlux
+# relaxation right-hand side (PiFlux.cpp:113-186 in the kernel's form) costs
+# 76 flops + 5 special operations (2 exp, 3 rsqrt).
 ALG_FLOPS_PER_KSTEP = {"piflux2d_256": 13 * 12 + 421, "dirac2d_64": 13 * 16 + 421,
                        "honeycomb_512": 13 * 30 + 421, "dirac2d_sweep": 13 * 16 + 421,
+                       "honeycomb_1024x64": 13 * 30 + 421,
                        "piflux3d_relax": 13 * 76 + 421, "piflux3d_field": 13 * 12 + 421}
 SPECIAL_OPS_PER_KSTEP = {"piflux2d_256": 26, "dirac2d_64": 0, "honeycomb_512": 78,
-                         "dirac2d_sweep": 0, "piflux3d_relax": 13 * 5}
+                         "honeycomb_1024x64": 78, "dirac2d_sweep": 0, "piflux3d_relax": 13 * 5}
 # the relaxation workload runs the reference step schedule in FP64 only
 DEFAULT_VARIANT = {"piflux3d_relax": "fp64"}
+# pulse instances per step (one graph launch); default: all of the workload's
+PULSES_PER_STEP = {"honeycomb_1024x64": 8}
 # The mixed-precision variant splits that work: solution, error estimate, error
 # norm and control stay FP64 (2*3*7 + 2*3*4 + ~25 = 91 flops); the right-hand
 # sides and the stage sums (13 F_rhs + 2*3*55) run on the FP32 pipe.
@@ -74,25 +88,159 @@ VARIANTS = {
 MAGNUS4_FLOPS_PER_KSTEP = 150
 LEARNED_RECORDS = 1 << 21
 LEARNED_EPOCHS = 20
+# the learned-proposer workload's network is trained on the three
+# single-pulse configurations (gapped Dirac 64^2, pi-flux 256^2, honeycomb
+# 512^2), never on the workload it is evaluated on
+TRAIN_SOURCES = {"honeycomb_1024x64": ("dirac2d_64", "piflux2d_256", "honeycomb_512")}
+# k rows of the oracle subsample behind harmonic_err_vs_oracle, and pulses
+ORACLE_ROWS = 384
+ORACLE_PULSES = 2
 
 
-def train_proposer(eng, wl, api):
-    """Step-size history of a carry run of the same workload at the plain
-    tolerances -> the learned proposer, trained on the GPU (outside the timed
-    region; reported under "training")."""
-    p = wl.pulses[0]
-    every = max(1, math.ceil(wl.n_k * p.n_measurements / LEARNED_RECORDS))
-    t0 = time.perf_counter()
-    recs, cst = eng.learned_collect(wl.system, wl.pulses, wl.grid, wl.opts(), hist_every=every,
-                                    cap=LEARNED_RECORDS)
-    t1 = time.perf_counter()
-    net = api.mlp_init(1, recs)
-    loss, train_ms = eng.mlp_train(recs, net, api.train_opts(epochs=LEARNED_EPOCHS))
-    t2 = time.perf_counter()
-    return net, {"records": int(recs.shape[0]), "hist_every": every,
-                 "collect_s": t1 - t0, "train_s": t2 - t1, "train_device_ms": train_ms,
-                 "epochs": LEARNED_EPOCHS, "loss_first_last": [float(loss[0]), float(loss[-1])],
-                 "network": "8-64-64-64-1 SiLU, BF16/FP32, tcgen05 training"}
+# ---------------------------------------------------------------------------
+# The workloads as the oracle sees them.  The reference arm and the CPU
+# baseline build their inputs here, from the oracle alone (no import of the
+# engine package, whose library they must not load); tests/test_bench_contract.py
+# checks these against the engine's workloads (higherharmonics_b200.workloads).
+# ---------------------------------------------------------------------------
+def splitmix64_uniforms(n: int, seed: int = SEED) -> np.ndarray:
+    """n uniforms in [0, 1) from splitmix64 (top 53 bits)."""
+    out = np.empty(n)
+    s = seed & 0xFFFFFFFFFFFFFFFF
+    for i in range(n):
+        s = (s + 0x9E3779B97F4A7C15) & 0xFFFFFFFFFFFFFFFF
+        z = s
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & 0xFFFFFFFFFFFFFFFF
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & 0xFFFFFFFFFFFFFFFF
+        z = z ^ (z >> 31)
+        out[i] = (z >> 11) * (1.0 / (1 << 53))
+    return out
+
+
+class RefWorkload:
+    """Oracle inputs of one workload: per pulse instance the model (constants
+    already multiplied by the pulse's energy scale), the pulse and the time
+    configuration; the solver; a builder of the k rows."""
+
+    def __init__(self, name, jobs, tol, rows_fn):
+        self.name = name
+        self.jobs = jobs          # [(model, pulse, time_config)]
+        self.tol = tol            # (abs, rel)
+        self._rows_fn = rows_fn
+        self._rows = None
+
+    @property
+    def rows(self) -> np.ndarray:
+        if self._rows is None:
+            self._rows = self._rows_fn()
+        return self._rows
+
+    @property
+    def n_meas(self) -> int:
+        return int(self.jobs[0][2].n_measurements)
+
+
+def ref_workload(name: str) -> RefWorkload:
+    if name in _REF_OVERRIDE:
+        return _REF_OVERRIDE[name]
+    from oracle import hhg_oracle as O
+    two_pi = 2 * math.pi
+    if name == "dirac2d_64":
+        es = 1.0 / 0.1
+        m = O.model(O.DIRAC2D, velocity=1.0 * es, mass=0.05 * es, pol=(1.0, 0.0))
+        jobs = [(m, O.Pulse(1.0, 4), O.time_config(0.0, two_pi * 4, 4 * MEASUREMENTS_PER_CYCLE))]
+        return RefWorkload("dirac2d_64x64_4cyc", jobs, (1e-10, 1e-10),
+                           lambda: O.grid_tensor(m, 64, 64, -2, 2, -2, 2))
+    if name == "piflux2d_256":
+        es = 1.0 / 0.05
+        s = 1.0 / math.sqrt(2.0)
+        m = O.model(O.PIFLUX2D, hopping=1.0 * es, pol=(s, s))
+        jobs = [(m, O.Pulse(1.0, 8), O.time_config(0.0, two_pi * 9, 8 * MEASUREMENTS_PER_CYCLE))]
+        return RefWorkload("piflux2d_256x256_8cyc", jobs, (1e-12, 1e-8),
+                           lambda: O.grid_tensor(m, 256, 256, -math.pi, math.pi, -math.pi, math.pi))
+    if name == "honeycomb_512":
+        es = 1.0 / 0.08
+        m = O.model(O.HONEYCOMB, hopping=1.0 * es, mass=0.1 * es, pol=(1.0, 0.0))
+        a0 = 0.5 + splitmix64_uniforms(1)[0]
+        jobs = [(m, O.Pulse(a0, 6), O.time_config(0.0, two_pi * 7, 6 * MEASUREMENTS_PER_CYCLE))]
+        return RefWorkload("honeycomb_rhombic_512x512_6cyc", jobs, (1e-12, 1e-8),
+                           lambda: O.grid_rhombic(m, 512, 512))
+    if name == "dirac2d_sweep":
+        u = splitmix64_uniforms(4 * 256).reshape(256, 4)
+        jobs = []
+        for i in range(256):
+            a0 = math.exp(math.log(0.1) + u[i, 0] * (math.log(2.0) - math.log(0.1)))
+            phi = two_pi * u[i, 1]
+            ncyc = 2.0 + 8.0 * u[i, 2]
+            es = 1.0 / (0.05 + 0.1 * u[i, 3])
+            n = int(round(MEASUREMENTS_PER_CYCLE * ncyc))
+            mi = O.model(O.DIRAC2D, velocity=1.0 * es, mass=0.05 * es, pol=(1.0, 0.0))
+            jobs.append((mi, O.Pulse(a0, ncyc, 0.0, phi), O.time_config(0.0, two_pi * ncyc, n)))
+        m0 = jobs[0][0]
+        return RefWorkload("dirac2d_sweep_256x128x128", jobs, (1e-10, 1e-10),
+                           lambda: O.grid_tensor(m0, 128, 128, -2, 2, -2, 2))
+    if name == "honeycomb_1024x64":
+        es = 1.0 / 0.08
+        m = O.model(O.HONEYCOMB, hopping=1.0 * es, mass=0.1 * es, pol=(1.0, 0.0))
+        u = splitmix64_uniforms(2 * 64, SEED + 5).reshape(64, 2)
+        jobs = [(m, O.Pulse(0.5 + 1.5 * u[i, 0], 6, 0.0, two_pi * u[i, 1]),
+                 O.time_config(0.0, two_pi * 7, 6 * MEASUREMENTS_PER_CYCLE)) for i in range(64)]
+        return RefWorkload("honeycomb_rhombic_1024x1024x64", jobs, (1e-12, 1e-8),
+                           lambda: O.grid_rhombic(m, 1024, 1024))
+    raise KeyError(name)
+
+
+def host_cores() -> int:
+    return len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+
+
+class CpuBaseline:
+    """The reference's plain FP64 algorithm (the oracle port with the
+    reference's Release flags: -O3 -ffast-math, OpenMP over k-points) on all
+    host cores, over a strided k-subsample of one pulse instance per run;
+    spectra/s are the sampled fraction of a spectrum per second."""
+
+    def __init__(self, rw: RefWorkload, target_s: float):
+        from oracle import hhg_oracle as O
+        self.O = O
+        self.rw = rw
+        self.cores = host_cores()
+        self.s = O.solver(*rw.tol)
+        rows = rw.rows
+        self.n_k = rows.shape[0]
+        m, p, tc = rw.jobs[0]
+        calib = rows[:: max(1, self.n_k // max(self.cores, 8))][: max(self.cores, 8)]
+        t0 = time.perf_counter()
+        O.current_density(m, p, tc, self.s, calib, threads=self.cores, fast=True)
+        per_k = (time.perf_counter() - t0) / calib.shape[0]
+        n_sample = int(min(self.n_k, max(self.cores, target_s / max(per_k, 1e-9))))
+        self.stride = max(1, self.n_k // n_sample)
+        self.sample = np.ascontiguousarray(rows[:: self.stride])
+        self.runs = 0
+
+    def run(self, job: int | None = None):
+        """One sample (pulse instance `job`, default: the next one): returns
+        (spectra/s, seconds, description, attempted k.steps/s)."""
+        if job is None:
+            job = self.runs % len(self.rw.jobs)
+        self.runs += 1
+        m, p, tc = self.rw.jobs[job]
+        t0 = time.perf_counter()
+        _, st, rc = self.O.current_density(m, p, tc, self.s, self.sample, threads=self.cores,
+                                           fast=True)
+        el = time.perf_counter() - t0
+        if rc != 0:
+            raise RuntimeError(f"oracle status {rc}")
+        frac = self.sample.shape[0] / self.n_k
+        desc = (f"every {self.stride}th k-point ({self.sample.shape[0]} of {self.n_k}) of pulse "
+                f"instance {job} over its full {tc.n_measurements}-interval pulse: {st.attempted} "
+                f"k.steps in {el:.2f} s on {self.cores} threads (oracle port, -O3 -ffast-math, "
+                f"OpenMP); spectra/s = {frac:.3e} of a spectrum / time")
+        return frac / el, el, desc, st.attempted / el
+
+    @property
+    def timed_fraction(self) -> float:
+        return self.sample.shape[0] / self.n_k
 
 
 def dist_env():
@@ -153,67 +301,40 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-class CpuBaseline:
-    """The oracle port timed on the host cores over a strided k-subsample of
-    the workload; spectra/s are extrapolated to the full grid."""
-
-    def __init__(self, wl, rows, target_s: float):
-        from oracle import hhg_oracle as O
-        from tests.helpers import oracle_args
-        self.O = O
-        p = wl.pulses[0]
-        self.args = oracle_args(wl.system, p, wl.opts_kw["abs_tol"], wl.opts_kw["rel_tol"])
-        self.cores = (len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity")
-                      else os.cpu_count())
-        self.n_k = rows.shape[0]
-        m, p, tc, s = self.args
-        calib = rows[:: max(1, self.n_k // max(self.cores, 8))][: max(self.cores, 8)]
-        t0 = time.perf_counter()
-        O.current_density(m, p, tc, s, calib, threads=self.cores, fast=True)
-        per_k = (time.perf_counter() - t0) / calib.shape[0]
-        n_sample = int(min(self.n_k, max(self.cores, target_s / max(per_k, 1e-9))))
-        self.stride = max(1, self.n_k // n_sample)
-        self.sample = np.ascontiguousarray(rows[:: self.stride])
-        self.n_meas = tc.n_measurements
-
-    def run(self):
-        m, p, tc, s = self.args
-        t0 = time.perf_counter()
-        _, st, rc = self.O.current_density(m, p, tc, s, self.sample, threads=self.cores,
-                                           fast=True)
-        el = time.perf_counter() - t0
-        if rc != 0:
-            raise RuntimeError(f"oracle status {rc}")
-        spectra_per_s = 1.0 / (el * self.n_k / self.sample.shape[0])
-        desc = (f"every {self.stride}th k-point ({self.sample.shape[0]} of {self.n_k}) over the "
-                f"full {self.n_meas}-interval pulse, {st.attempted} k.steps in {el:.2f} s on "
-                f"{self.cores} threads (oracle port, -O3 -ffast-math, OpenMP); spectra/s "
-                f"scaled by {self.n_k}/{self.sample.shape[0]}")
-        return spectra_per_s, desc, st.attempted / el
-
-
-def reference_arm(args, wl_name):
+def reference_arm(args):
+    """The reference's algorithm on the host cores (oracle port; the
+    reference itself cannot be built here), on the same workload: each step is
+    one bounded sample -- a strided k-subsample of one pulse instance over its
+    full pulse -- sized so all K + W steps take about --reference-seconds.
+    ms_per_step is the measured wall time of a step; value = the spectra the
+    sampled fractions amount to, per second."""
     ws, rank, _ = dist_env()
     if rank != 0:
         return 0
-    from higherharmonics_b200 import workloads as W
-    from higherharmonics_b200 import api
-    wl = W.ALL[wl_name]()
-    rows = api.grid_rows(wl.system, wl.grid)
-    cb = CpuBaseline(wl, rows, target_s=args.cpu_seconds)
-    per_step = []
+    rw = ref_workload(args.workload)
+    per_step_s = max(0.5, args.reference_seconds / (args.steps + args.warmup))
+    cb = CpuBaseline(rw, target_s=per_step_s)
+    secs, fracs = [], []
     desc = ksps = None
     for i in range(args.warmup + args.steps):
-        v, desc, ksps = cb.run()
+        _, el, desc, ksps = cb.run()
         if i >= args.warmup:
-            per_step.append(1.0 / v)
-    t = float(np.mean(per_step))
-    value = 1.0 / t
+            secs.append(el)
+            fracs.append(cb.timed_fraction)
+    total_s = float(np.sum(secs))
+    value = float(np.sum(fracs)) / total_s
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total_s / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "config": config_for(wl, "oracle port, plain FP64 RKF78"),
+        "data": "synthetic",
+        "config": {"workload": rw.name, "k_points": int(rw.rows.shape[0]),
+                   "n_measurements": rw.n_meas, "pulses": len(rw.jobs),
+                   "tolerances": f"{rw.tol[0]:g}/{rw.tol[1]:g}",
+                   "variant": "oracle port of the reference's plain FP64 RKF78 (restart schedule)"},
+        "timed_fraction": cb.timed_fraction,
+        "timed_fraction_note": "spectra per step actually integrated (a k-subsample of one pulse "
+                               "instance); value = timed fractions / timed seconds",
         "k_steps_per_s": ksps,
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cb.cores, "kind": "port",
                          "sample": desc},
@@ -221,16 +342,6 @@ def reference_arm(args, wl_name):
     }
     print(json.dumps(line), flush=True)
     return 0
-
-
-def config_for(wl, variant_desc, okw=None):
-    p = wl.pulses[0]
-    tol = dict(wl.opts_kw)
-    tol.update({k: v for k, v in (okw or {}).items() if k in ("abs_tol", "rel_tol")})
-    return {"workload": wl.name, "k_points": wl.n_k, "n_measurements": p.n_measurements,
-            "pulses": len(wl.pulses), "tolerances": f"{tol['abs_tol']:g}/{tol['rel_tol']:g}",
-            "variant": variant_desc,
-            "l2": "flushed (256 MiB write) before every timed step; inputs < L2"}
 
 
 def traffic_from_profile(wl_name):
@@ -249,85 +360,211 @@ def traffic_from_profile(wl_name):
     return None
 
 
-def compare_variants(args, eng, wl, api, stream, flush, main_variant):
-    """spectra/s of the plain FP64 path and of the learned mixed-precision
-    path on the same workload, same timing method (CUDA events over K graph
-    launches, L2 flushed before each): the learned+FP32 vs plain FP64 ratio."""
+# ---------------------------------------------------------------------------
+# The GPU arm
+# ---------------------------------------------------------------------------
+def train_proposer(eng, wl_name, wl, api, W):
+    """The learned proposer: accept/reject histories of the FP64 carry
+    controller at the plain tolerances (hhg_learned_collect), on the workload's
+    training sources (TRAIN_SOURCES: configurations 1-3 for the learned-proposer
+    workload; otherwise the workload itself), then Adam on the GPU (tcgen05
+    training kernels).  Outside the timed region; reported under "training"."""
+    names = TRAIN_SOURCES.get(wl_name, (wl_name,))
+    t0 = time.perf_counter()
+    parts, sources = [], []
+    cap = LEARNED_RECORDS // len(names)
+    for nm in names:
+        src = wl if nm == wl_name else W.ALL[nm]()
+        n_int = sum(p.n_measurements for p in src.pulses)
+        every = max(1, math.ceil(src.n_k * n_int / cap))
+        recs, _ = eng.learned_collect(src.system, src.pulses, src.grid, src.opts(),
+                                      hist_every=every, cap=cap)
+        parts.append(recs)
+        sources.append({"workload": src.name, "records": int(recs.shape[0]), "hist_every": every})
+    recs = np.concatenate(parts)
+    t1 = time.perf_counter()
+    net = api.mlp_init(1, recs)
+    loss, train_ms = eng.mlp_train(recs, net, api.train_opts(epochs=LEARNED_EPOCHS))
+    t2 = time.perf_counter()
+    return net, {"records": int(recs.shape[0]), "sources": sources,
+                 "collect_s": t1 - t0, "train_s": t2 - t1, "train_device_ms": train_ms,
+                 "epochs": LEARNED_EPOCHS, "loss_first_last": [float(loss[0]), float(loss[-1])],
+                 "network": "8-64-64-64-1 SiLU, BF16/FP32, tcgen05 training"}
+
+
+def variant_opts(name, net, args, api):
+    okw = dict(VARIANTS[name])
+    if okw.get("proposer") == api.PROPOSER_LEARNED:
+        okw["mlp"] = net
+        if args.mlp_every:
+            okw["mlp_every"] = args.mlp_every
+    return okw
+
+
+def spectrum_intensities(plan, pulse_index, mo=None):
+    from higherharmonics_b200.analysis import default_max_order, harmonic_intensities
+    fr, re, im = plan.fetch_spectrum(pulse_index)
+    if mo is None:
+        mo = default_max_order(fr)
+    return harmonic_intensities(fr, re, im, mo), mo
+
+
+class OracleCheck:
+    """Harmonic error of a variant against the FP64 oracle on a seeded
+    subsample: ORACLE_ROWS k rows spread evenly over the grid and the first
+    ORACLE_PULSES pulse instances of batch 0, each over its full pulse.  The
+    oracle (strict FP64, -ffp-contract=off) integrates those rows once; a
+    variant runs the same rows through an explicit-rows grid."""
+
+    def __init__(self, wl, rows, api):
+        from oracle import hhg_oracle as O
+        from tests.helpers import harmonics, oracle_args
+        stride = max(1, rows.shape[0] // ORACLE_ROWS)
+        self.rows = np.ascontiguousarray(rows[::stride][:ORACLE_ROWS])
+        self.grid, self._keep = api.grid_explicit(self.rows)
+        self.pulses = wl.pulses[:ORACLE_PULSES]
+        self.I, self.mo = [], []
+        t0 = time.perf_counter()
+        for p in self.pulses:
+            m, op, tc, s = oracle_args(wl.system, p, wl.opts_kw["abs_tol"], wl.opts_kw["rel_tol"])
+            j, _, rc = O.current_density(m, op, tc, s, self.rows, threads=host_cores())
+            if rc != 0:
+                raise RuntimeError(f"oracle status {rc}")
+            I = harmonics(j, p)
+            self.I.append(I)
+            self.mo.append(I.size)
+        self.oracle_s = time.perf_counter() - t0
+        self.stride = stride
+
+    def error(self, eng, wl, okw) -> float:
+        from higherharmonics_b200.analysis import harmonic_rel_err
+        plan = eng.plan(wl.system, self.pulses, self.grid, wl.opts(**okw))
+        plan.execute_async()
+        plan.spectrum_async()
+        plan.fetch(copy_j=False)
+        err = 0.0
+        for i, I0 in enumerate(self.I):
+            I, _ = spectrum_intensities(plan, i, self.mo[i])
+            err = max(err, harmonic_rel_err(I, I0, floor_rel=1e-6))
+        plan.close()
+        return err
+
+    def describe(self) -> str:
+        return (f"{self.rows.shape[0]} k rows (every {self.stride}th) x the first "
+                f"{len(self.pulses)} pulse instances, full pulses; FP64 oracle "
+                f"({self.oracle_s:.1f} s on {host_cores()} threads)")
+
+
+def time_plan(plan, stream, flush, steps):
+    """Mean ms of `steps` graph launches (integration + reduction + spectra),
+    CUDA events on the launching stream, L2 flushed before each."""
     import torch
-    from higherharmonics_b200.analysis import (default_max_order, harmonic_intensities,
-                                               harmonic_rel_err)
-    # the plain FP64 spectrum every variant's harmonic error refers to
-    ref = eng.plan(wl.system, wl.pulses, wl.grid, wl.opts())
-    ref.execute_async()
-    ref.spectrum_async()
-    ref.fetch(copy_j=False)
-    fr0, re0, im0 = ref.fetch_spectrum(0)
-    ref.close()
-    mo = default_max_order(fr0)
-    I0 = harmonic_intensities(fr0, re0, im0, mo)
-    out = {}
-    for v in ("fp64", "mixed_learned", "mixed_lockstep", "magnus4"):
-        if v == main_variant or (v != "fp64" and args.workload in DEFAULT_VARIANT):
-            continue
-        okw = dict(VARIANTS[v])
-        if okw.get("proposer") == api.PROPOSER_LEARNED:
-            okw["mlp"], _ = train_proposer(eng, wl, api)
-            if args.mlp_every:
-                okw["mlp_every"] = args.mlp_every
-        plan = eng.plan(wl.system, wl.pulses, wl.grid, wl.opts(**okw))
-        plan.autotune(reps=1)
-        sptr = stream.cuda_stream
-        for _ in range(3):
-            flush.zero_()
-            plan.execute_graph(sptr, with_spectrum=True)
-        torch.cuda.synchronize()
-        a = torch.cuda.Event(enable_timing=True)
-        b = torch.cuda.Event(enable_timing=True)
+    sptr = stream.cuda_stream
+    flush.zero_()
+    plan.execute_graph(sptr, with_spectrum=True)  # warm-up (captures the graph)
+    torch.cuda.synchronize()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    total = 0.0
+    for _ in range(steps):
+        flush.zero_()
         a.record(stream)
-        for _ in range(args.steps):
-            flush.zero_()
-            plan.execute_graph(sptr, with_spectrum=True)
+        plan.execute_graph(sptr, with_spectrum=True)
         b.record(stream)
         torch.cuda.synchronize()
+        total += a.elapsed_time(b)
+    return total / steps
+
+
+def compare_variants(args, eng, wl, batch0, api, stream, flush, main_variant, net, ref_I, ocheck):
+    """spectra/s of the plain FP64 path and the other variants on batch 0 of
+    the workload, same timing method as the headline (CUDA events over graph
+    launches, L2 flushed before each), each with its harmonic error against
+    the GPU FP64 engine (full grid) and against the FP64 oracle (subsample)."""
+    from higherharmonics_b200.analysis import harmonic_rel_err
+    out = {}
+    names = ["fp64", "mixed_learned", "mixed_lockstep", "magnus4"]
+    steps = max(1, min(args.steps, 2))
+    for v in names:
+        if v == main_variant or (v != "fp64" and args.workload in DEFAULT_VARIANT):
+            continue
+        okw = variant_opts(v, net, args, api)
+        plan = eng.plan(wl.system, batch0, wl.grid, wl.opts(**okw))
+        ms = time_plan(plan, stream, flush, steps)
         _, st = plan.fetch(copy_j=False)
-        fr, re, im = plan.fetch_spectrum(0)
-        out[v] = {"value": args.steps * len(wl.pulses) / (a.elapsed_time(b) * 1e-3), "unit": UNIT,
-                  "k_steps_per_spectrum": st.attempted_steps,
-                  "harmonic_err_vs_fp64": harmonic_rel_err(harmonic_intensities(fr, re, im, mo), I0,
-                                                           floor_rel=1e-6)}
+        herr = 0.0
+        for i in range(len(batch0)):
+            I, mo = spectrum_intensities(plan, i, len(ref_I[i]))
+            herr = max(herr, harmonic_rel_err(I, ref_I[i], floor_rel=1e-6))
         plan.close()
+        out[v] = {"value": len(batch0) / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
+                  "timed_launches": steps,
+                  "k_steps_per_spectrum": st.attempted_steps / len(batch0),
+                  "harmonic_err_vs_fp64": herr,
+                  "harmonic_err_vs_oracle": ocheck.error(eng, wl, okw) if ocheck else None}
     return out
 
 
-def our_arm(args, wl_name):
+class JView:
+    """A plan's device j buffer seen by torch (zero copy), for the NCCL sum."""
+
+    def __init__(self, ptr: int, n: int):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f8", "data": (ptr, False),
+                                         "version": 2}
+
+
+def our_arm(args):
     import torch
     ws, rank, local = dist_env()
+    strong = args.scaling == "strong" and ws > 1
     if ws > 1:
+        import datetime
+
         import torch.distributed as dist
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     else:
         torch.cuda.set_device(0)
     dev = torch.cuda.current_device()
     from higherharmonics_b200 import api
     from higherharmonics_b200 import workloads as W
-    from higherharmonics_b200.analysis import (default_max_order, harmonic_intensities,
-                                               harmonic_rel_err)
+    from higherharmonics_b200.distributed import shard_range
 
-    wl = W.ALL[wl_name]()
-    if ws > 1:  # one pulse instance per rank: weak scaling
-        for p in wl.pulses:
-            p.phase = p.phase + 0.1 * rank
+    name = args.workload
+    wl = W.ALL[name]()
+    pps = args.pulses_per_step or PULSES_PER_STEP.get(name, len(wl.pulses))
+    batches = [wl.pulses[i:i + pps] for i in range(0, len(wl.pulses), pps)]
+    nb = len(batches)
     eng = api.Engine(dev)
-    okw = dict(VARIANTS[args.variant])
-    training = None
-    if okw.get("proposer") == api.PROPOSER_LEARNED:
-        net, training = train_proposer(eng, wl, api)
-        okw["mlp"] = net
-        if args.mlp_every:
-            okw["mlp_every"] = args.mlp_every
-    plan = eng.plan(wl.system, wl.pulses, wl.grid, wl.opts(**okw))
-    tune = plan.autotune(reps=2)
+    rows_all = None
+    grid = wl.grid
+    shard = None
+    if strong:
+        # this rank's contiguous block of the k rows (jobs_per_rank blocks)
+        rows_all = api.grid_rows(wl.system, wl.grid)
+        lo, hi = shard_range(rows_all.shape[0], rank, ws)
+        grid, _keep_rows = api.grid_explicit(rows_all[lo:hi])
+        shard = [lo, hi]
+
+    net = training = None
+    if VARIANTS[args.variant].get("proposer") == api.PROPOSER_LEARNED or not args.no_compare:
+        net, training = train_proposer(eng, name, wl, api, W)
+    okw = variant_opts(args.variant, net, args, api)
+
+    # one plan per batch (the batch a step integrates); weak scaling: rank r
+    # takes batch (k ws + r) mod nb at step k
+    def batch_of(k):
+        return k % nb if strong else (k * ws + rank) % nb
+
+    needed = sorted({batch_of(k) for k in range(args.warmup + args.steps)})
+    plans = {}
+    t_setup = time.perf_counter()
+    for b in needed:
+        plans[b] = eng.plan(wl.system, batches[b], grid, wl.opts(**okw))
+    setup_s = time.perf_counter() - t_setup
+    tune = None
+    if args.autotune and not strong and nb == 1:
+        tune = plans[needed[0]].autotune(reps=2)
     # a dedicated stream: the legacy default stream has handle 0, which the
     # C ABI reads as "the context's own stream"
     stream = torch.cuda.Stream()
@@ -336,34 +573,22 @@ def our_arm(args, wl_name):
     assert sptr != 0
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
-    def step():
+    def step(k):
+        plan = plans[batch_of(k)]
         flush.zero_()
-        plan.execute_graph(sptr, with_spectrum=True)
+        if not strong:
+            plan.execute_graph(sptr, with_spectrum=True)
+            return
+        # integrate this rank's rows, sum j over the ranks, then the spectra
+        plan.execute_graph(sptr, with_spectrum=False)
+        jt = torch.as_tensor(JView(plan.device_j_ptr(), plan.j_len), device="cuda")
+        torch.distributed.all_reduce(jt, op=torch.distributed.ReduceOp.SUM)
+        plan.spectrum_async(sptr)
 
-    for _ in range(args.warmup):
-        step()
+    for k in range(args.warmup):
+        step(k)
     torch.cuda.synchronize()
-    j0, st0 = plan.fetch()
-    ksteps = st0.attempted_steps
 
-    # accuracy of this variant against the plain FP64 engine (itself within
-    # 1e-9 of the oracle, see tests/test_gpu_parity.py)
-    herr = 0.0
-    if args.variant != "fp64":
-        fr, re, im = plan.fetch_spectrum(0)
-        ref = eng.plan(wl.system, wl.pulses, wl.grid, wl.opts())
-        ref.execute_async()
-        ref.spectrum_async()
-        ref.fetch(copy_j=False)
-        fr0, re0, im0 = ref.fetch_spectrum(0)
-        ref.close()
-        mo = default_max_order(fr0)
-        herr = harmonic_rel_err(harmonic_intensities(fr, re, im, mo),
-                                harmonic_intensities(fr0, re0, im0, mo), floor_rel=1e-6)
-
-    peak = eng.fp64_peak_tflops()
-    mixed = VARIANTS[args.variant].get("precision", 0) == 1
-    peak32 = eng.fp32_peak_tflops() if mixed else None
     uuid = None
     try:
         uuid = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
@@ -381,9 +606,8 @@ def our_arm(args, wl_name):
     e_end = torch.cuda.Event(enable_timing=True)
     e_start.record(stream)
     for k in range(args.steps):
-        flush.zero_()
         ev[k][0].record(stream)
-        plan.execute_graph(sptr, with_spectrum=True)
+        step(args.warmup + k)
         ev[k][1].record(stream)
     e_end.record(stream)
     torch.cuda.synchronize()
@@ -392,27 +616,42 @@ def our_arm(args, wl_name):
     clocks = sampler.stop()
     elapsed_ms = e_start.elapsed_time(e_end)
     launch_ms = [a.elapsed_time(b) for a, b in ev]
-    step_sum_ms = sum(ev[k][0].elapsed_time(ev[k + 1][0]) for k in range(args.steps - 1))
+    # attempted k.steps of the timed steps (each plan's counters hold its last run)
+    ksteps = 0
+    for k in range(args.steps):
+        _, st = plans[batch_of(args.warmup + k)].fetch(copy_j=False)
+        ksteps += st.attempted_steps
     if ws > 1:
         t = torch.tensor([elapsed_ms], device="cuda", dtype=torch.float64)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         elapsed_ms = float(t.item())
-    # one step = every pulse instance's spectrum (one graph launch)
-    value = ws * args.steps * len(wl.pulses) / (elapsed_ms * 1e-3)
+        kt = torch.tensor([float(ksteps)], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(kt, op=torch.distributed.ReduceOp.SUM)
+        ksteps_all = float(kt.item())
+    else:
+        ksteps_all = float(ksteps)
+    spectra_per_step = pps * (1 if strong else ws)
+    value = args.steps * spectra_per_step / (elapsed_ms * 1e-3)
 
-    # end to end through the public API with host buffers
+    # end to end through the public one-shot API with host buffers: every
+    # step a new batch (a plan-cache miss: the host builds and uploads the k
+    # rows, pulse records and time grids, the device stages the pulses), j
+    # back, then each pulse's spectrum from its host j
     e2e = None
-    if not args.no_e2e:
+    if not args.no_e2e and not strong:
         n_e2e = max(1, min(args.steps, 3))
-        eng.current_density(wl.system, wl.pulses, wl.grid, wl.opts(**okw))
+        e_batches = [(k * ws + rank + args.warmup) % nb for k in range(n_e2e)]
+        if nb == 1:
+            eng.current_density(wl.system, batches[0], grid, wl.opts(**okw))  # cache warm-up
         if ws > 1:
             torch.distributed.barrier()
         torch.cuda.synchronize()
+        h2d = d2h = 0
         t0 = time.perf_counter()
-        for _ in range(n_e2e):
-            j, st = eng.current_density(wl.system, wl.pulses, wl.grid, wl.opts(**okw))
+        for b in e_batches:
+            j, st = eng.current_density(wl.system, batches[b], grid, wl.opts(**okw))
             off = 0
-            for p in wl.pulses:  # every pulse instance's spectrum
+            for p in batches[b]:  # every pulse instance's spectrum
                 n_s = p.n_measurements + 1
                 eng.spectrum(j[off:off + n_s], p.n_measurements, p.window_begin, p.window_end)
                 off += n_s
@@ -422,33 +661,40 @@ def our_arm(args, wl_name):
             t = torch.tensor([el], device="cuda", dtype=torch.float64)
             torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
             el = float(t.item())
-        # k table and pulse records in; per pulse: the staging time grid
-        # (2 x samples) and j back into the spectrum call; out: j and the
-        # spectrum's three arrays
-        h2d = wl.n_k * 64 + 256 * len(wl.pulses)
-        d2h = 0
-        for p in wl.pulses:
+        # bytes copied per step: in, the k rows (64 B each) unless the plan was
+        # cached, the pulse records (256 B) and time grids (8 B x samples) of
+        # the batch, and each pulse's j into its spectrum call; out, j and
+        # each spectrum's frequencies, real and imaginary parts
+        for p in batches[e_batches[0]]:
             n_s = p.n_measurements + 1
             n_fft = 4 * n_s + 1
-            h2d += 8 * n_s * 2 + 8 * n_s
+            h2d += 256 + 8 * n_s + 8 * n_s
             d2h += 8 * n_s + 3 * 8 * n_fft
-        e2e = {"value": ws * n_e2e * len(wl.pulses) / el, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+        if nb > 1:
+            h2d += wl.n_k * 64
+        e2e = {"value": ws * n_e2e * pps / el, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h),
                "path": "Engine.current_density + Engine.spectrum (hhg_gpu_current_density + "
-                       "hhg_gpu_spectrum), host buffers, wall clock"}
+                       "hhg_gpu_spectrum), host buffers, wall clock" +
+                       (", a new batch every step (plan built and k rows uploaded)" if nb > 1 else
+                        ", plan cached by the context after the first call")}
 
     if rank != 0:
+        for p in plans.values():
+            p.close()
         if ws > 1:
             torch.distributed.destroy_process_group()
         return 0
-    avg_launch_s = float(np.mean(launch_ms)) * 1e-3
-    # the graph launch = integration kernel + BZ reduction + FFT (the
-    # integration is >= 98 % of it in the launch list), so this slightly
-    # understates the kernel's own throughput
-    kernel_s = avg_launch_s
-    per_kstep = ALG_FLOPS_PER_KSTEP.get(wl_name, 421)
-    if VARIANTS[args.variant].get("stepper", 0) == 1:
+
+    per_kstep = ALG_FLOPS_PER_KSTEP.get(name, 421)
+    magnus = VARIANTS[args.variant].get("stepper", 0) == 1
+    if magnus:
         per_kstep = MAGNUS4_FLOPS_PER_KSTEP
+    mixed = VARIANTS[args.variant].get("precision", 0) == 1
+    peak = eng.fp64_peak_tflops()
+    peak32 = eng.fp32_peak_tflops() if mixed else None
+    kernel_s = float(np.mean(launch_ms)) * 1e-3
+    ksteps_per_launch = ksteps / args.steps
     if mixed:
         # the bound is whichever pipe needs longer for its share of the work:
         # FP32 (13 F_rhs + 330 flops) against the measured FP32 FMA rate
@@ -461,48 +707,93 @@ def our_arm(args, wl_name):
         bound, bpeak, bflops = "fp64_pipe", peak, per_kstep
         peak_src = ("measured FP64 FMA throughput (hhg_measure_fp64_peak, burst); "
                     "MEASURED_PEAKS.json has no FP64 figure")
-    achieved = bflops * ksteps / kernel_s / 1e12
+    achieved = bflops * ksteps_per_launch / kernel_s / 1e12
     roofline = {"bound": bound, "achieved": achieved, "peak": bpeak, "unit": "TFLOP/s",
-                "frac": achieved / bpeak, "traffic": traffic_from_profile(wl_name),
+                "frac": achieved / bpeak, "traffic": traffic_from_profile(name),
                 "peak_source": peak_src, "fp64_peak": peak, "fp32_peak": peak32,
                 "kernel": "bz_integrate_kernel", "kernel_ms": 1e3 * kernel_s,
                 "kernel_ms_source": "mean over the timed steps of CUDA events around each graph "
-                                    "launch (integration + reduction + FFT) on the launching stream",
+                                    "launch (integration + reduction + FFTs) on the launching "
+                                    "stream (rank 0)",
                 "alg_flops_per_kstep": per_kstep, "bound_flops_per_kstep": bflops,
-                "special_ops_per_kstep": (2 if VARIANTS[args.variant].get("stepper", 0) == 1
-                                          else SPECIAL_OPS_PER_KSTEP.get(wl_name, 0))}
+                "special_ops_per_kstep": 2 if magnus else SPECIAL_OPS_PER_KSTEP.get(name, 0)}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64" if VARIANTS[args.variant].get("precision", 0) == 0 else "f32 rhs / f64 state",
-        "data": "synthetic", "config": config_for(wl, args.variant, VARIANTS[args.variant]),
-        "k_steps_per_s": ws * ksteps / kernel_s if ws == 1 else None,
-        "fraction_of_fp64_peak_fp64_equivalent": per_kstep * ksteps / kernel_s / 1e12 / peak,
-        "k_steps_per_spectrum": ksteps, "harmonic_err_vs_fp64": herr,
-        "gpu_launches": 4 * args.steps, "roofline": roofline, "clocks": clocks, "e2e": e2e,
-        "training": training,
-        "autotune": {"chosen": tune.as_list()[tune.best], "candidates": tune.as_list()},
-        "path": "plan with autotuned work decomposition, one CUDA graph launch per spectrum "
-                "(integration + BZ reduction + trapezoidal FFT)",
-        "timing": {"device_ms_total": elapsed_ms, "launch_ms": launch_ms,
-                   "mean_step_ms_between_launch_starts": (step_sum_ms / (args.steps - 1)
-                                                          if args.steps > 1 else None)},
+        "scaling": "strong" if strong else "weak", "vs_baseline": None,
+        "dtype": "f64" if not mixed else "f32 rhs / f64 state",
+        "data": "synthetic (seeded pulse table, splitmix64 seed 20261203)",
+        "config": {"workload": wl.name, "k_points": wl.n_k,
+                   "n_measurements": wl.pulses[0].n_measurements, "pulses": len(wl.pulses),
+                   "pulses_per_step": pps, "batches": nb,
+                   "tolerances": "{:g}/{:g}".format(wl.opts(**okw).abs_tol, wl.opts(**okw).rel_tol),
+                   "variant": args.variant,
+                   "l2": "flushed (256 MiB write) before every timed step",
+                   **({"k_rows_of_rank0": shard} if strong else {})},
+        "k_steps_per_s": ksteps_all / (elapsed_ms * 1e-3),
+        "k_steps_per_spectrum": ksteps / (args.steps * pps),
+        "gpu_launches": (4 + 2 * pps) * args.steps if not strong else (3 + 2 * pps) * args.steps,
+        "roofline": roofline, "clocks": clocks, "e2e": e2e, "training": training,
+        "setup_s": setup_s,
+        "path": "plans per batch of pulse instances, one CUDA graph launch per step "
+                "(integration + BZ reduction + trapezoidal FFTs)" +
+                (", j summed over ranks by NCCL all_reduce between them" if strong else ""),
+        "timing": {"device_ms_total": elapsed_ms, "launch_ms": launch_ms},
     }
-    if ws == 1 and not args.no_cpu_baseline:
-        rows = api.grid_rows(wl.system, wl.grid)
-        cb = CpuBaseline(wl, rows, target_s=args.cpu_seconds)
-        v, desc, ksps = cb.run()
-        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": cb.cores, "kind": "port",
-                                "sample": desc, "k_steps_per_s": ksps}
-    if ws == 1 and not args.no_compare:
-        line["compare"] = compare_variants(args, eng, wl, api, stream, flush, args.variant)
+    if tune is not None:
+        line["autotune"] = {"chosen": tune.as_list()[tune.best], "candidates": tune.as_list()}
+    if ws == 1:
+        # accuracy: batch 0 against the plain FP64 engine (full grid), and the
+        # variant against the FP64 oracle (k-subsample)
+        ocheck = None
+        if not args.no_oracle_check:
+            ocheck = OracleCheck(wl, api.grid_rows(wl.system, wl.grid), api)
+            line["harmonic_err_vs_oracle"] = ocheck.error(eng, wl, okw)
+            line["oracle_check"] = ocheck.describe()
+        ref = eng.plan(wl.system, batches[0], wl.grid, wl.opts())
+        ref.execute_async(sptr)
+        ref.spectrum_async(sptr)
+        ref.fetch(copy_j=False)
+        ref_I = [spectrum_intensities(ref, i)[0] for i in range(len(batches[0]))]
+        ref.close()
+        from higherharmonics_b200.analysis import harmonic_rel_err
+        p0 = plans.get(0) or eng.plan(wl.system, batches[0], wl.grid, wl.opts(**okw))
+        p0.execute_async(sptr)
+        p0.spectrum_async(sptr)
+        p0.fetch(copy_j=False)
+        herr = 0.0
+        for i in range(len(batches[0])):
+            I, _ = spectrum_intensities(p0, i, len(ref_I[i]))
+            herr = max(herr, harmonic_rel_err(I, ref_I[i], floor_rel=1e-6))
+        line["harmonic_err_vs_fp64"] = herr
+        if not args.no_cpu_baseline:
+            rw = ref_workload(name) if _has_ref(name) else engine_ref_workload(wl, api)
+            if rw is not None:
+                cb = CpuBaseline(rw, target_s=args.cpu_seconds)
+                v, _, desc, ksps = cb.run(0)
+                line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": cb.cores, "kind": "port",
+                                        "sample": desc, "k_steps_per_s": ksps}
+        if not args.no_compare:
+            line["compare"] = compare_variants(args, eng, wl, batches[0], api, stream, flush,
+                                               args.variant, net, ref_I, ocheck)
+            fp = line["compare"].get("fp64")
+            if fp:
+                line["speedup_vs_plain_fp64"] = value / fp["value"]
     print(json.dumps(line), flush=True)
-    plan.close()
+    for p in plans.values():
+        p.close()
     eng.close()
     if ws > 1:
         torch.distributed.destroy_process_group()
     return 0
+
+
+def _has_ref(name):
+    try:
+        ref_workload(name)
+        return True
+    except KeyError:
+        return False
 
 
 # The Dirac workload's unit is one k.interval of the closed-form Magnus step
@@ -568,18 +859,21 @@ class DiracCpuBaseline:
         return info
 
     def run(self):
+        """One sample: (spectra/s, seconds, description, k.intervals/s)."""
         t0 = time.perf_counter()
         info = self._splits(self.sample)
         el = time.perf_counter() - t0
-        n_all = len(self.pairs)
-        v = 1.0 / (el * n_all / len(self.sample))
+        v = self.timed_fraction / el
         kint = info["trajectories"] * self.tc.n_measurements
-        desc = (f"{len(self.sample)} of {n_all} (k_z slice, kappa split) pairs, evenly spaced, "
-                f"each refined to convergence ({info['trajectories']} trajectories, {kint} "
+        desc = (f"{len(self.sample)} of {len(self.pairs)} (k_z slice, kappa split) pairs, evenly "
+                f"spaced, each refined to convergence ({info['trajectories']} trajectories, {kint} "
                 f"k.intervals) in {el:.2f} s on {self.cores} threads (oracle port, -O3 "
-                f"-ffast-math, OpenMP); "
-                f"spectra/s scaled by {n_all}/{len(self.sample)}")
-        return v, desc, kint / el
+                f"-ffast-math, OpenMP); spectra/s = {self.timed_fraction:.3e} of a spectrum / time")
+        return v, el, desc, kint / el
+
+    @property
+    def timed_fraction(self) -> float:
+        return len(self.sample) / len(self.pairs)
 
 
 def dirac_config(wl, path):
@@ -593,26 +887,30 @@ def dirac_config(wl, path):
 
 
 def dirac_reference_arm(args):
+    """The Dirac quadrature's reference arm: each step one bounded sample of
+    (slice, split) pairs; ms_per_step is its measured wall time."""
     ws, rank, _ = dist_env()
     if rank != 0:
         return 0
     from higherharmonics_b200 import workloads as W
     wl = W.ALL[args.workload]()
-    cb = DiracCpuBaseline(wl, args.cpu_seconds)
-    per = []
+    cb = DiracCpuBaseline(wl, max(0.5, args.reference_seconds / (args.steps + args.warmup)))
+    secs = []
     desc = None
     for i in range(args.warmup + args.steps):
-        v, desc, _ = cb.run()
+        _, el, desc, _ = cb.run()
         if i >= args.warmup:
-            per.append(1.0 / v)
-    t = float(np.mean(per))
-    line = {"impl": "reference", "metric": METRIC, "value": 1.0 / t, "unit": UNIT, "n_gpus": ws,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t,
+            secs.append(el)
+    total_s = float(np.sum(secs))
+    value = args.steps * cb.timed_fraction / total_s
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total_s / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "config": dirac_config(wl, "oracle port"),
-            "cpu_baseline": {"value": 1.0 / t, "unit": UNIT, "cores": cb.cores, "kind": "port",
+            "timed_fraction": cb.timed_fraction,
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cb.cores, "kind": "port",
                              "sample": desc},
-            "e2e": {"value": 1.0 / t, "unit": UNIT, "h2d_bytes_per_step": 0,
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -728,7 +1026,7 @@ def dirac_arm(args):
     }
     if ws == 1 and not args.no_cpu_baseline:
         cb = DiracCpuBaseline(wl, args.cpu_seconds)
-        v, desc, kps = cb.run()
+        v, _, desc, kps = cb.run()
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": cb.cores, "kind": "port",
                                 "sample": desc, "k_intervals_per_s": kps}
     print(json.dumps(line), flush=True)
@@ -739,12 +1037,14 @@ def dirac_arm(args):
 
 
 def ncu_case(args):
-    """A small case of the bench workload for ncu captures (committed so the
+    """A small case of a bench workload for ncu captures (committed so the
     profile summaries name a command that runs committed files only): the
     same grid and pulse shape over --ncu-cycles cycles (default 1: 1024
-    intervals), two executions
-    of the selected variant; with --variant mlp_train, history collection on
-    that case and 2 epochs of proposer training.  Prints one line, no timing."""
+    intervals) and the first --ncu-pulses pulse instances, two executions of
+    the selected variant (the learned variants train on the workload's
+    training sources, 2 epochs); with --variant mlp_train, history collection
+    on that case and 2 epochs of proposer training.  Prints one line, no
+    timing."""
     from higherharmonics_b200 import api
     from higherharmonics_b200 import workloads as W
     import inspect
@@ -758,6 +1058,8 @@ def ncu_case(args):
     make = W.ALL[args.workload]
     wl = (make(n_cycles=args.ncu_cycles) if "n_cycles" in inspect.signature(make).parameters
           else make())
+    if args.ncu_pulses:
+        wl.pulses = wl.pulses[:args.ncu_pulses]
     eng = api.Engine(0)
     if args.variant == "mlp_train":
         recs, _ = eng.learned_collect(wl.system, wl.pulses, wl.grid, wl.opts(), hist_every=32,
@@ -780,40 +1082,99 @@ def ncu_case(args):
     return 0
 
 
-def main():
+def self_launch(args) -> int:
+    """--gpus N without a torchrun environment: re-run this command under
+    torch.distributed.run with N ranks on this node (127.0.0.1)."""
+    import socket
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           f"--nproc-per-node={args.gpus}", "--master-addr=127.0.0.1", f"--master-port={port}",
+           os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.run(cmd).returncode
+
+
+def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=8)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="piflux2d_256")
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD)
     ap.add_argument("--variant", default=None, choices=sorted(VARIANTS) + ["mlp_train"],
-                    help="default: mixed_lockstep (fp64 for piflux3d_relax)")
+                    help="default: mixed_learned (fp64 for piflux3d_relax)")
+    ap.add_argument("--scaling", default="weak", choices=["weak", "strong"],
+                    help="N > 1: every rank its own batches (weak) or every batch's k rows "
+                         "split over the ranks with j summed by NCCL (strong)")
+    ap.add_argument("--pulses-per-step", type=int, default=None,
+                    help="pulse instances per step (default: 8 of the 64 for "
+                         "honeycomb_1024x64, all of them otherwise)")
+    ap.add_argument("--autotune", action="store_true",
+                    help="autotune the work decomposition of a single-batch workload first")
     ap.add_argument("--ncu-case", action="store_true",
                     help="run the small profiling case of the workload (no timing)")
     ap.add_argument("--ncu-cycles", type=int, default=1,
                     help="pulse cycles of the --ncu-case workload (the bench uses the full length)")
-    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--ncu-pulses", type=int, default=None,
+                    help="pulse instances of the --ncu-case workload (default: all)")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0,
+                    help="seconds of the GPU arm's CPU-baseline sample")
+    ap.add_argument("--reference-seconds", type=float, default=120.0,
+                    help="seconds of CPU work of the whole --impl reference run")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-compare", action="store_true")
+    ap.add_argument("--no-oracle-check", action="store_true")
     ap.add_argument("--mlp-every", type=int, default=None,
                     help="intervals between network proposals of the learned variants "
                          "(default: the library's)")
-    args = ap.parse_args()
+    args = ap.parse_args(argv)
     if args.variant is None:
-        args.variant = DEFAULT_VARIANT.get(args.workload, "mixed_lockstep")
+        args.variant = DEFAULT_VARIANT.get(args.workload, "mixed_learned")
     if args.warmup < 3:
         args.warmup = 3
     if args.ncu_case:
         return ncu_case(args)
     if args.variant == "mlp_train":
         ap.error("--variant mlp_train is a profiling case (--ncu-case)")
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        return self_launch(args)
     if args.workload.startswith("dirac3d_kappa"):
         return dirac_reference_arm(args) if args.impl == "reference" else dirac_arm(args)
     if args.impl == "reference":
-        return reference_arm(args, args.workload)
-    return our_arm(args, args.workload)
+        if not _has_ref(args.workload):
+            return reference_arm_engine_inputs(args)
+        return reference_arm(args)
+    return our_arm(args)
+
+
+def engine_ref_workload(wl, api) -> RefWorkload:
+    """Oracle inputs of a workload whose descriptors come from the engine's
+    configuration reader (the production PiFlux runs): the descriptors mapped
+    onto the oracle's structs (tests/helpers.oracle_args), the engine's k rows."""
+    from tests.helpers import oracle_args
+    m, p, tc, _ = oracle_args(wl.system, wl.pulses[0], wl.opts_kw["abs_tol"], wl.opts_kw["rel_tol"])
+    rows = api.grid_rows(wl.system, wl.grid)
+    return RefWorkload(wl.name, [(m, p, tc)], (wl.opts_kw["abs_tol"], wl.opts_kw["rel_tol"]),
+                       lambda: rows)
+
+
+def reference_arm_engine_inputs(args):
+    """Reference arm of the workloads without an oracle-side definition (the
+    production PiFlux runs, whose inputs come from the engine's configuration
+    reader)."""
+    from higherharmonics_b200 import api
+    from higherharmonics_b200 import workloads as W
+    _REF_OVERRIDE[args.workload] = engine_ref_workload(W.ALL[args.workload](), api)
+    try:
+        return reference_arm(args)
+    finally:
+        _REF_OVERRIDE.pop(args.workload, None)
+
+
+_REF_OVERRIDE = {}
 
 
 if __name__ == "__main__":

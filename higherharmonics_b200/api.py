@@ -36,7 +36,7 @@ EXPORTED = [
     "hhg_gpu_current_density", "hhg_gpu_spectrum", "hhg_plan_create", "hhg_plan_destroy",
     "hhg_plan_j_length", "hhg_plan_execute_async", "hhg_plan_device_j", "hhg_plan_fetch",
     "hhg_plan_spectrum_async", "hhg_plan_fetch_spectrum", "hhg_measure_fp64_peak",
-    "hhg_gpu_current_density_noalloc",
+    "hhg_gpu_current_density_noalloc", "hhg_noalloc_status",
     "hhg_learned_collect", "hhg_default_train_opts", "hhg_mlp_init", "hhg_mlp_train",
     "hhg_mlp_gradients", "hhg_mlp_predict", "hhg_plan_execute_graph", "hhg_plan_autotune", "hhg_measure_fp32_peak",
     "hhg_gpu_k_resolved", "hhg_gpu_split_current", "hhg_gpu_spectrum_welch", "hhg_pulse_values",
@@ -218,6 +218,8 @@ def load_library() -> ctypes.CDLL:
             ctypes.POINTER(SystemDesc), ctypes.POINTER(PulseDesc), ctypes.c_void_p, ctypes.c_int64,
             ctypes.POINTER(SolverOpts), ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(Stats),
             ctypes.c_char_p, ctypes.c_size_t]
+        L.hhg_noalloc_status.argtypes = [ctypes.c_void_p, ctypes.POINTER(Stats), ctypes.c_char_p,
+                                         ctypes.c_size_t]
         L.hhg_default_solver_opts.argtypes = [ctypes.POINTER(SolverOpts)]
         L.hhg_gpu_k_resolved.argtypes = [ctypes.c_void_p, ctypes.POINTER(SystemDesc),
                                          ctypes.POINTER(PulseDesc), ctypes.POINTER(GridDesc),

@@ -29,9 +29,13 @@ dgauss/dgaussA/dgaussB are splines in the reference and are handed to the
 device as the same spline samples (PowerLawField.cpp:19-31,
 QuenchedField.cpp:15-29, DoubleLaser.hpp:42-68).  The photon energy of the
 system is multiplied by the experimental one for the exp and double lasers
-(Dispatcher.cpp:10-19).  The experimental lasers exp/expA/expB need the
-measured field of the reference's source, which this package does not carry:
-they raise UnsupportedConfig (api.spline_pulse takes such samples).
+(Dispatcher.cpp:10-19).  The experimental lasers exp/expA/expB build A(t)
+from a measured field (ExperimentalLaser.cpp:30-108, `experimental_pulse`):
+this package does not carry the reference's measured data, so the caller
+names a file with it (`experimental_field <path>`: two columns E_A E_B in
+MV/cm at the spacing `experimental_dt`, default 0.03335555 ps; the data's
+photon energy `experimental_photon_energy`, default 6.091420442472572 meV,
+ExperimentParams.hpp:5,12); without that key they raise UnsupportedConfig.
 
 system_type Dirac follows DiracDispatcher (DiracDispatcher.cpp:16-63) and the
 DiracSystem constructor (DiracSystem.cpp:52-63): the same beta, E_F and 1/tau,
@@ -63,7 +67,12 @@ K_B = 0.08617333262145177434     # meV / K (GlobalDefinitions.hpp:29)
 SQRT3 = 1.732050807568877293527446341
 SQRT12 = 3.464101615137754587054892683
 MEASUREMENTS_PER_CYCLE = 1 << 10
-EXP_PHOTON_ENERGY = 6.091420442472572  # meV (ExperimentParams.hpp:11)
+EXP_PHOTON_ENERGY = 6.091420442472572  # meV (ExperimentParams.hpp:12)
+EXP_DT_PS = 0.03335555  # ps between the measured field samples (ExperimentParams.hpp:5)
+# samples of the quartic tail that brings A to rest, and the zero samples
+# before and after the measured record (ExperimentParams.hpp:6-9)
+EXP_N_EXTRA, EXP_BEGIN_ZERO, EXP_ZERO_BUFF = 16, 8, 8
+EXP_LASERS = {"exp": "both", "expA": "A", "expB": "B"}
 DOUBLE_LASERS = {"dcos": ("cosine", "both"), "dcosA": ("cosine", "A"), "dcosB": ("cosine", "B"),
                  "dgauss": ("gauss", "both"), "dgaussA": ("gauss", "A"), "dgaussB": ("gauss", "B")}
 PIFLUX_Z_RANGE, PIFLUX_N_COARSE = 32, 4
@@ -136,14 +145,23 @@ def from_config(cfg: dict | str, *, grid: api.GridDesc | None = None,
     if not (laser_type in known or laser_type.startswith("powerlaw")) or \
             (system_type in ("Honeycomb", "Dirac") and (laser_type in DOUBLE_LASERS or laser_type == "gauss")):
         raise ValueError(f"Laser type '{laser_type}' is not recognized!")
-    if laser_type in ("exp", "expA", "expB"):
-        raise UnsupportedConfig(f"laser_type {laser_type}: the measured pulse of the reference's "
-                                "ExperimentalLaser is not part of this package; pass its samples "
-                                "with api.spline_pulse")
+    measured = None
+    if laser_type in EXP_LASERS:
+        if "experimental_field" not in cfg:
+            raise UnsupportedConfig(f"laser_type {laser_type}: the reference's measured field is "
+                                    "not part of this package; name a file with it "
+                                    "(experimental_field <path>: columns E_A E_B in MV/cm)")
+        measured = MeasuredField.load(cfg["experimental_field"],
+                                      float(cfg.get("experimental_dt", EXP_DT_PS)),
+                                      float(cfg.get("experimental_photon_energy",
+                                                    EXP_PHOTON_ENERGY)))
 
     T, E_F, v_F = num("T"), num("E_F"), num("v_F")
     band_width, E0, pe_in = num("band_width"), num("field_amplitude"), num("photon_energy")
-    pe = pe_in * EXP_PHOTON_ENERGY if laser_type in DOUBLE_LASERS else pe_in  # get_photon_energy
+    # Dispatcher::get_photon_energy: the exp and double lasers' photon energy
+    # is in units of the experimental one
+    exp_pe = measured.photon_energy if measured is not None else EXP_PHOTON_ENERGY
+    pe = pe_in * exp_pe if (laser_type in DOUBLE_LASERS or laser_type in EXP_LASERS) else pe_in
     tau_d = num("diagonal_relaxation_time")
     tau_o = float(cfg.get("offdiagonal_relaxation_time", "-1"))
     n_cycles = int(num("n_laser_cycles"))
@@ -163,6 +181,12 @@ def from_config(cfg: dict | str, *, grid: api.GridDesc | None = None,
             t_begin = math.pi * t0_offset
             pulse = api.cosine_pulse(_amplitude(ratio, E0, pe), n_cycles, n, t_begin=t_begin,
                                      window=(t_begin, t_begin + 2 * math.pi * n_cycles))
+        elif measured is not None:
+            # the system keeps the config's photon energy; the laser's model
+            # ratio takes the experimental one (DiracDispatcher.cpp:38-52)
+            pe_l = pe_in * measured.photon_energy
+            pulse = experimental_pulse(measured, pe_l, E0, HBAR * v_F / pe_l, t0_offset,
+                                       EXP_LASERS[laser_type], n)
         else:
             pulse = make_pulse(laser_type, ratio, E0, pe_in, n_cycles, t0_offset, n)
         quad = api.kappa_quad(band_width, int(num("n_z")), DIRAC_N_KAPPA,
@@ -186,7 +210,14 @@ def from_config(cfg: dict | str, *, grid: api.GridDesc | None = None,
     sys_ = api.system(kind, hopping=hopping, pol=pol, beta=beta, fermi_energy=E_F / pe,
                       inv_diag_relax=inv_d if relax else 0.0,
                       inv_offdiag_relax=inv_o if relax else 0.0)
-    pulse = make_pulse(laser_type, lattice, E0, pe_in, n_cycles, t0_offset, n, reduced)
+    if measured is not None:
+        # PiFlux shortens the window to 0.75 t_end for the occupation and
+        # split-current runs, Honeycomb does not (PiFluxDispatcher.cpp:59-70,
+        # HoneycombDispatcher.cpp:36-47)
+        pulse = experimental_pulse(measured, pe, E0, lattice, t0_offset, EXP_LASERS[laser_type], n,
+                                   0.75 if (reduced and system_type == "PiFlux") else 1.0)
+    else:
+        pulse = make_pulse(laser_type, lattice, E0, pe_in, n_cycles, t0_offset, n, reduced)
     return Run(system_type, sys_, pulse, g, api.solver(1e-12, 1e-8), lattice)
 
 
@@ -258,3 +289,99 @@ def make_pulse(laser_type: str, ratio: float, E0: float, pe_in: float, n_cycles:
         a, b = one(aA, n_cycles, 0.0, t), one(aB, n_cycles, 0.0, t - shift + 0.0)
         y.append(a + b if active == "both" else (a if active == "A" else b))
     return api.spline_pulse(y, 0.0, dt, n, (0.0, cut * t_max), cut=t_max, deriv=(0.0, 0.0))
+
+
+@dataclass
+class MeasuredField:
+    """A measured two-pulse electric field: E_A and E_B in MV/cm at spacing
+    dt_ps (ps), and the photon energy (meV) the data define."""
+    e_a: "np.ndarray"
+    e_b: "np.ndarray"
+    dt_ps: float = EXP_DT_PS
+    photon_energy: float = EXP_PHOTON_ENERGY
+
+    @staticmethod
+    def load(path: str, dt_ps: float = EXP_DT_PS,
+             photon_energy: float = EXP_PHOTON_ENERGY) -> "MeasuredField":
+        import numpy as np
+        data = np.loadtxt(path, ndmin=2)
+        if data.shape[1] < 2 or data.shape[0] < 3:
+            raise ValueError(f"{path}: need at least 3 rows of two columns (E_A E_B, MV/cm)")
+        return MeasuredField(np.ascontiguousarray(data[:, 0]), np.ascontiguousarray(data[:, 1]),
+                             dt_ps, photon_energy)
+
+
+def measured_vector_potential(e, dt: float):
+    """A = -int E dt of a measured record (the factor c cancels in the Peierls
+    substitution), the way ExperimentalLaser's vector_potential builds it
+    (ExperimentalLaser.cpp:30-62): EXP_BEGIN_ZERO zeros, the running sum
+    -dt sum_{m <= i} E_m, then a quartic over EXP_N_EXTRA - 1 steps that
+    continues A with its last value, slope -E_last and curvature (from the
+    last two samples) and reaches zero with zero slope, then zeros (the last
+    EXP_ZERO_BUFF + 1 entries)."""
+    import numpy as np
+    e = np.asarray(e, dtype=np.float64)
+    n = e.size
+    out = np.zeros(n + EXP_N_EXTRA + EXP_ZERO_BUFF + EXP_BEGIN_ZERO)
+    acc = 0.0
+    for i in range(n):
+        acc = acc - e[i] * dt
+        out[EXP_BEGIN_ZERO + i] = acc
+    a_last = out[EXP_BEGIN_ZERO + n - 1]
+    p1 = -e[n - 1]
+    p2 = 0.5 * (e[n - 2] - e[n - 1]) / dt
+    T = (EXP_N_EXTRA - 1) * dt
+    # p(T) = 0 and p'(T) = 0 fix the cubic and quartic coefficients
+    c3 = -4 * (p2 / (2 * T) + (3 * p1) / (4 * T * T) + a_last / (T * T * T))
+    c4 = -0.25 * (3 * c3 / T + 2 * p2 / (T * T) + p1 / (T * T * T))
+    for i in range(1, EXP_N_EXTRA):
+        t = i * dt
+        out[EXP_BEGIN_ZERO + n - 1 + i] = (a_last + p1 * t + p2 * t * t + c3 * t * t * t +
+                                           c4 * t * t * t * t)
+    out[out.size - EXP_BEGIN_ZERO - 1:] = 0.0
+    return out
+
+
+def experimental_pulse(field: MeasuredField, pe_laser: float, E0: float, lattice: float,
+                       shift_ps: float, active: str, n: int, window_scale: float = 1.0
+                       ) -> api.PulseDesc:
+    """ExperimentalLaser (ExperimentalLaser.cpp:8-108) as a spline pulse.
+
+    pe_laser is the laser's photon energy in meV (the config's photon_energy
+    times the data's), lattice the system's laser model ratio, shift_ps the
+    delay of pulse B after pulse A (t0_offset, ps; negative delays A),
+    active "both" / "A" / "B".  The two vector potentials are splined on the
+    unitless sample spacing dt = pe_laser dt_ps / (1e12 hbar), each is cut
+    after the record's end laser_end = (samples - 1 + 32) dt_ps, and their
+    sum scaled by 0.1 E0 lattice / hbar is sampled at spacing dt over [0,
+    t_end], t_end = 1.5 laser_end (unified_t_max); that sampling, splined
+    with zero end slopes, is A(t) for t <= t_end.  The window is [0,
+    window_scale t_end] with n measurement intervals."""
+    import numpy as np
+    to_unitless = pe_laser / (1e12 * HBAR)  # 1/ps
+    dt = pe_laser * (field.dt_ps / (1e12 * HBAR))
+    laser_end_ps = (field.e_a.size - 1 + EXP_N_EXTRA + EXP_BEGIN_ZERO + EXP_ZERO_BUFF) * field.dt_ps
+    t_end = (1.5 * laser_end_ps) * to_unitless
+    end = pe_laser * (laser_end_ps / (1e12 * HBAR))
+    shift = shift_ps * to_unitless
+    inner = []
+    for e in (field.e_a, field.e_b):
+        a = measured_vector_potential(e, field.dt_ps)
+        inner.append(api.spline_pulse(a, 0.0, dt, 1, (0.0, (a.size - 1) * dt), cut=1e300,
+                                      deriv=(0.0, 0.0)))
+    n_temp = int(t_end / dt + 1)
+    t = 0.0 + dt * np.arange(n_temp + 1)
+    if shift >= 0:
+        ta, tb = t, t - shift
+        in_a = ta <= end
+        in_b = (tb >= 0) & (tb <= end)
+    else:
+        ta, tb = t + shift, t
+        in_a = (ta >= 0) & (ta <= end)
+        in_b = tb <= end
+    A = np.where(in_a, api.pulse_values(inner[0], ta), 0.0)
+    B = np.where(in_b, api.pulse_values(inner[1], tb), 0.0)
+    tot = A + B if active == "both" else (A if active == "A" else B)
+    samples = (0.1 / HBAR) * E0 * lattice * tot
+    return api.spline_pulse(samples, 0.0, dt, n, (0.0, window_scale * t_end), cut=t_end,
+                            deriv=(0.0, 0.0))

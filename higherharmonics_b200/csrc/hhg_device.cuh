@@ -72,11 +72,15 @@ __host__ __device__ constexpr int base_model(int m) {
 // sin) pairs of s A(t) for the lattice models.  kRelax: FP64 RKF78 only.
 // kStart: the right-hand side also reads the step's start state.
 // kMinBlocks: integration CTAs per SM the register budget is sized for.
+// kPacked: the FP32 right-hand side runs on packed (x, y) pairs (rhs2).
+// kPairs: the FP32 staged values of the two projections are interleaved
+// (below, pair_layout), so rhs2 takes them as packed operands without moves.
 template <int M> struct Traits {
     static constexpr bool kRelax = false;
     static constexpr bool kStart = false;
     static constexpr int kMinBlocks = kMinBlocksPerSM;
-    static constexpr bool kPacked = false;  // FP32 right-hand side on packed (x, y) pairs
+    static constexpr bool kPacked = false;
+    static constexpr bool kPairs = false;
 };
 template <> struct Traits<DIRAC2D> : Traits<-1> { static constexpr int NF = 1; };
 template <> struct Traits<DIRAC3D> : Traits<-1> { static constexpr int NF = 1; };
@@ -84,14 +88,20 @@ template <> struct Traits<PIFLUX3D> : Traits<-1> { static constexpr int NF = 2; 
 template <> struct Traits<PIFLUX2D> : Traits<-1> {
     static constexpr int NF = 4;
     static constexpr bool kPacked = true;
+    static constexpr bool kPairs = true;
 };
 template <> struct Traits<PIFLUX2D_SYM> : Traits<-1> {
     static constexpr int NF = 2;
     static constexpr bool kPacked = true;
 };
 template <> struct Traits<HONEYCOMB> : Traits<-1> { static constexpr int NF = 6; };
-template <> struct Traits<HONEYCOMB_X> : Traits<-1> { static constexpr int NF = 4; };
+template <> struct Traits<HONEYCOMB_X> : Traits<-1> {
+    static constexpr int NF = 4;
+    static constexpr bool kPacked = true;
+    static constexpr bool kPairs = true;
+};
 template <> struct Traits<PIFLUX3D_RELAX> {
+    static constexpr bool kPairs = false;
     static constexpr int NF = 2;
     static constexpr bool kRelax = true;
     static constexpr bool kStart = true;
@@ -100,12 +110,14 @@ template <> struct Traits<PIFLUX3D_RELAX> {
     static constexpr int kMinBlocks = 4;
 };
 template <> struct Traits<HONEYCOMB_RELAX> {
+    static constexpr bool kPairs = false;
     static constexpr int NF = 6;
     static constexpr bool kRelax = true;
     static constexpr bool kStart = false;
     static constexpr int kMinBlocks = 4;  // 255 registers: the six staged functions spill at 168
 };
 template <> struct Traits<DIRAC3D_RELAX> {
+    static constexpr bool kPairs = false;
     static constexpr int NF = 1;
     static constexpr bool kRelax = true;
     static constexpr bool kStart = false;
@@ -145,6 +157,19 @@ __host__ __device__ constexpr int slot_doubles_dyadic(int nf, int deg) {
 // Value of staged function n outside the pulse window: A -> 0, cos -> 1, sin -> 0.
 template <int NF> __host__ __device__ constexpr double outside_value(int n) {
     return (NF > 1 && (n % 2) == 0) ? 1.0 : 0.0;
+}
+
+// Paired FP32 layout of four staged functions v = (cos a, sin a, cos b, sin b)
+// of two projections a, b, each as a float pair (hi, lo):
+//   slot 0 = (hi cos a, hi cos b), slot 1 = (lo cos a, lo cos b),
+//   slot 2 = (hi sin a, hi sin b), slot 3 = (lo sin a, lo sin b).
+// Used by the models with Traits::kPairs in the mixed-precision path (the
+// staging table's float-pair layout and the interpolants' output alike).
+__host__ __device__ __forceinline__ float2 pair_slot(const double *v, int n) {
+    const int a = (n < 2) ? 0 : 1, b = a + 2;
+    const float ha = (float)v[a], hb = (float)v[b];
+    return (n & 1) ? make_float2((float)(v[a] - (double)ha), (float)(v[b] - (double)hb))
+                   : make_float2(ha, hb);
 }
 
 // Fehlberg 7(8) nodes c_s (E. Fehlberg, NASA TR R-287, 1968).
@@ -335,7 +360,7 @@ template <> struct Num<float> {
 // Pulse evaluators used inside a step: polynomial (any t) or table (stage s of
 // a standard step).  Values come back as Num<R>::V.
 // ---------------------------------------------------------------------------
-template <int NF, int D, typename R>
+template <int NF, int D, typename R, bool PAIR = false>
 struct PolyEval {
     static constexpr bool kReuse = true;  // stages sharing a node reuse the values
     const double *hd;  // interval record
@@ -344,16 +369,29 @@ struct PolyEval {
         const double u = (t - hd[2]) * hd[3];
         const bool inside = (t > tb) && (t < te);
         const double *c0 = hd + slot_poly(NF);
+        double v[NF];
 #pragma unroll
         for (int n = 0; n < NF; ++n) {
             const double *c = c0 + n * (D + 1);
-            double v = c[D];
+            double x = c[D];
 #pragma unroll
-            for (int j = D - 1; j >= 0; --j) v = fma(v, u, c[j]);
-            f[n] = Num<R>::mk(inside ? v : outside_value<NF>(n));
+            for (int j = D - 1; j >= 0; --j) x = fma(x, u, c[j]);
+            v[n] = inside ? x : outside_value<NF>(n);
+        }
+        if constexpr (PAIR) {
+            static_assert(NF == 4, "the paired layout holds two projections");
+#pragma unroll
+            for (int n = 0; n < 4; ++n) f[n] = pair_slot(v, n);
+        } else {
+#pragma unroll
+            for (int n = 0; n < NF; ++n) f[n] = Num<R>::mk(v[n]);
         }
     }
 };
+// the paired layout applies to the kPairs models' FP32 path
+template <int M, typename R> __host__ __device__ constexpr bool pair_layout() {
+    return Traits<M>::kPairs && sizeof(R) == sizeof(float);
+}
 
 template <int NF, typename R>
 struct TableEval {
@@ -472,10 +510,16 @@ template <typename R, bool SYM> struct PiFlux2DState {
     }
     // FP32 on packed pairs: (m0, m1) = Num<float>::dot2 of both projections in
     // one set of paired FMAs, then dS = (m1 Sz, -m0 Sz, m0 Sy - m1 Sx)
+    // (the non-symmetric model's staged values arrive in the paired layout)
     __device__ __forceinline__ void rhs2(const float2 *f, float2 s_xy, float s_z, float2 &d_xy,
                                          float &d_z) const {
-        const float2 bhi = make_float2(f[0].x, f[Y].x), blo = make_float2(f[0].y, f[Y].y);
-        const float2 dhi = make_float2(f[1].x, f[Y + 1].x), dlo = make_float2(f[1].y, f[Y + 1].y);
+        float2 bhi, blo, dhi, dlo;
+        if constexpr (SYM) {
+            bhi = make_float2(f[0].x, f[0].x), blo = make_float2(f[0].y, f[0].y);
+            dhi = make_float2(f[1].x, f[1].x), dlo = make_float2(f[1].y, f[1].y);
+        } else {
+            bhi = f[0], blo = f[1], dhi = f[2], dlo = f[3];
+        }
         float2 lo = __fmul2_rn(pc_hi, blo);
         lo = __ffma2_rn(pc_lo, bhi, lo);
         lo = __ffma2_rn(ps_hi, dlo, lo);
@@ -501,12 +545,16 @@ template <typename R> struct ModelState<PIFLUX2D_SYM, R> : PiFlux2DState<R, true
 // gamma' = sum_j e^{i nn_j.k} e^{-i s_j A}, s_j = nn_j . pol,
 // dS = (-pf Sz Im g - 2m Sy, -pf Sz Re g + 2m Sx, pf (Sx Im g + Sy Re g)).
 // mp: [0] 2t (pf), [1] 2 mass, [2] px, [3] py.  X: bonds 2 and 3 share one
-// projection (field along x), so the staged pairs are those of (s_0, s_1).
+// projection (field along x), so the staged pairs are those of (s_0, s_1) and
+// the two bonds' momentum phases are summed once per k-point:
+// gamma' = e^{i nn_1.k} e^{-i s_0 A} + (e^{i nn_2.k} + e^{i nn_3.k}) e^{-i s_1 A},
+// two complex products per right-hand side instead of three.
 template <typename R, bool X> struct HoneycombState {
     using N = Num<R>;
     static constexpr int Q2 = X ? 2 : 4;
     typename N::V pc0, ps0, pc1, ps1, pc2, ps2, mc0, mc1, mc2;  // pf cos/sin(nn_j . k), -pf cos
     double c0, s0, c1, s1, c2, s2;                              // cos/sin(nn_j . k)
+    float2 pc_hi, pc_lo, ps_hi, ps_lo, mc_hi, mc_lo;            // X, FP32: (bond 1, bonds 2+3) pairs
     R dm;
     double pf, px, py;
     __device__ __forceinline__ void init(const PulseDev &p, const double *row) {
@@ -516,18 +564,32 @@ template <typename R, bool X> struct HoneycombState {
         sincos(-0.5 * row[0] + nny * row[1], &s1, &c1);
         sincos(-0.5 * row[0] - nny * row[1], &s2, &c2);
         pc0 = N::mk(pf * c0), ps0 = N::mk(pf * s0), mc0 = N::mk(-pf * c0);
-        pc1 = N::mk(pf * c1), ps1 = N::mk(pf * s1), mc1 = N::mk(-pf * c1);
-        pc2 = N::mk(pf * c2), ps2 = N::mk(pf * s2), mc2 = N::mk(-pf * c2);
+        if constexpr (X) {
+            pc1 = N::mk(pf * (c1 + c2)), ps1 = N::mk(pf * (s1 + s2)), mc1 = N::mk(-pf * (c1 + c2));
+            if constexpr (sizeof(R) == sizeof(float)) {
+                pc_hi = make_float2(pc0.x, pc1.x), pc_lo = make_float2(pc0.y, pc1.y);
+                ps_hi = make_float2(ps0.x, ps1.x), ps_lo = make_float2(ps0.y, ps1.y);
+                mc_hi = make_float2(mc0.x, mc1.x), mc_lo = make_float2(mc0.y, mc1.y);
+            }
+        } else {
+            pc1 = N::mk(pf * c1), ps1 = N::mk(pf * s1), mc1 = N::mk(-pf * c1);
+            pc2 = N::mk(pf * c2), ps2 = N::mk(pf * s2), mc2 = N::mk(-pf * c2);
+        }
         dm = R(p.mp[1]);
         px = p.mp[2];
         py = p.mp[3];
     }
     // pf Re gamma', pf Im gamma' with e^{i(a - b)} = (ca cb + sa sb) + i (sa cb - ca sb)
     __device__ __forceinline__ void gamma(const typename N::V *f, R &gr, R &gi) const {
-        gr = R(N::dot2(pc0, f[0], ps0, f[1])) + R(N::dot2(pc1, f[2], ps1, f[3])) +
-             R(N::dot2(pc2, f[Q2], ps2, f[Q2 + 1]));
-        gi = R(N::dot2(ps0, f[0], mc0, f[1])) + R(N::dot2(ps1, f[2], mc1, f[3])) +
-             R(N::dot2(ps2, f[Q2], mc2, f[Q2 + 1]));
+        if constexpr (X) {
+            gr = R(N::dot2(pc0, f[0], ps0, f[1])) + R(N::dot2(pc1, f[2], ps1, f[3]));
+            gi = R(N::dot2(ps0, f[0], mc0, f[1])) + R(N::dot2(ps1, f[2], mc1, f[3]));
+        } else {
+            gr = R(N::dot2(pc0, f[0], ps0, f[1])) + R(N::dot2(pc1, f[2], ps1, f[3])) +
+                 R(N::dot2(pc2, f[Q2], ps2, f[Q2 + 1]));
+            gi = R(N::dot2(ps0, f[0], mc0, f[1])) + R(N::dot2(ps1, f[2], mc1, f[3])) +
+                 R(N::dot2(ps2, f[Q2], mc2, f[Q2 + 1]));
+        }
     }
     __device__ __forceinline__ void rhs(const typename N::V *f, const R *S, R *dS) const {
         R gr, gi;
@@ -535,6 +597,28 @@ template <typename R, bool X> struct HoneycombState {
         dS[0] = -(S[2] * gi) - dm * S[1];
         dS[1] = -(S[2] * gr) + dm * S[0];
         dS[2] = S[0] * gi + S[1] * gr;
+    }
+    // FP32, field along x, staged values in the paired layout: the two bond
+    // groups' products sit in the two halves of paired FMAs (float-pair
+    // products hi hi + (hi lo + lo hi), one rounding per group), summed at
+    // the end: pf Re g' = PC.FC + PS.FS, pf Im g' = PS.FC - PC.FS.
+    __device__ __forceinline__ void rhs2(const float2 *f, float2 s_xy, float s_z, float2 &d_xy,
+                                         float &d_z) const {
+        static_assert(X, "paired right-hand side: field along x");
+        float2 lr = __fmul2_rn(pc_hi, f[1]);
+        lr = __ffma2_rn(pc_lo, f[0], lr);
+        lr = __ffma2_rn(ps_hi, f[3], lr);
+        lr = __ffma2_rn(ps_lo, f[2], lr);
+        float2 li = __fmul2_rn(ps_hi, f[1]);
+        li = __ffma2_rn(ps_lo, f[0], li);
+        li = __ffma2_rn(mc_hi, f[3], li);
+        li = __ffma2_rn(mc_lo, f[2], li);
+        const float2 re = __ffma2_rn(pc_hi, f[0], __ffma2_rn(ps_hi, f[2], lr));
+        const float2 im = __ffma2_rn(ps_hi, f[0], __ffma2_rn(mc_hi, f[2], li));
+        const float gr = re.x + re.y, gi = im.x + im.y;
+        const float dmf = float(dm);
+        d_xy = make_float2(fmaf(-s_z, gi, -(dmf * s_xy.y)), fmaf(-s_z, gr, dmf * s_xy.x));
+        d_z = fmaf(s_xy.x, gi, s_xy.y * gr);
     }
     __device__ __forceinline__ double vertex(const double *r, const double *S) const {
         // shifted_grad_gamma and the projection (Honeycomb.cpp:49-61, 273-279, 328-330)
@@ -550,8 +634,15 @@ template <typename R, bool X> struct HoneycombState {
     }
     __device__ __forceinline__ void dvec(const double *f, double *d) const {
         // d = t (Re g', -Im g', mass) = 0.5 (pf Re g', -pf Im g', 2 mass)
-        const double gre = (c0 * f[0] + s0 * f[1]) + (c1 * f[2] + s1 * f[3]) + (c2 * f[Q2] + s2 * f[Q2 + 1]);
-        const double gim = (s0 * f[0] - c0 * f[1]) + (s1 * f[2] - c1 * f[3]) + (s2 * f[Q2] - c2 * f[Q2 + 1]);
+        double gre, gim;
+        if constexpr (X) {
+            const double c12 = c1 + c2, s12 = s1 + s2;
+            gre = (c0 * f[0] + s0 * f[1]) + (c12 * f[2] + s12 * f[3]);
+            gim = (s0 * f[0] - c0 * f[1]) + (s12 * f[2] - c12 * f[3]);
+        } else {
+            gre = (c0 * f[0] + s0 * f[1]) + (c1 * f[2] + s1 * f[3]) + (c2 * f[Q2] + s2 * f[Q2 + 1]);
+            gim = (s0 * f[0] - c0 * f[1]) + (s1 * f[2] - c1 * f[3]) + (s2 * f[Q2] - c2 * f[Q2 + 1]);
+        }
         d[0] = 0.5 * pf * gre;
         d[1] = -0.5 * pf * gim;
         d[2] = 0.5 * double(dm);
@@ -1140,7 +1231,7 @@ __device__ __forceinline__ bool control(const KParams &P, const double *S, const
 // ---------------------------------------------------------------------------
 template <int M, int NF, int D, typename R, bool USE_STD, bool CARRY, bool REC = false>
 __device__ __forceinline__ void lane_controller(const KParams &P, const ModelState<M, R> &ms,
-                                                const PolyEval<NF, D, R> &poly,
+                                                const PolyEval<NF, D, R, pair_layout<M, R>()> &poly,
                                                 const double *slot, const typename Num<R>::V *tabv,
                                                 int n_std, double t, double dt, double t1,
                                                 double *S, bool &dead, double &carry_dt,
@@ -1384,6 +1475,7 @@ __global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integ
     constexpr int TAB = slot_table(NF, D);
     constexpr int DYA = slot_dyadic(NF, D);
     constexpr bool kNarrow = sizeof(R) != sizeof(double);
+    constexpr bool kPair = pair_layout<M, R>();
     // only the reference schedule reads the standard table; the dyadic table
     // is read from global memory
     // the relaxation models on the reference schedule run free lanes (above)
@@ -1485,13 +1577,18 @@ __global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integ
                     }
                     if constexpr (kNarrow && PROPOSER == 0) {
                         __syncwarp();
-                        for (int c = lane; c < NTAB; c += 32) stage_tab[wib][c] = Num<R>::mk(slot[TAB + c]);
+                        for (int c = lane; c < NTAB; c += 32) {
+                            if constexpr (kPair)
+                                stage_tab[wib][c] = pair_slot(slot + TAB + (c & ~3), c & 3);
+                            else
+                                stage_tab[wib][c] = Num<R>::mk(slot[TAB + c]);
+                        }
                     }
                     __syncwarp();
                     const double *cur = STEPPER != 0 ? gslot : slot;
                     rec = cur + 4;
                     const double t0 = cur[0], t1 = cur[1];
-                    const PolyEval<NF, D, R> poly{slot, tb, te};
+                    const PolyEval<NF, D, R, kPair> poly{slot, tb, te};
                     if constexpr (STEPPER == 1) {
                         if (P.magnus_substeps == 1) {
                             double f1[NF], f2[NF];
@@ -1835,6 +1932,8 @@ __global__ void stage_pulses_kernel(const PulseDev *__restrict__ pulses, int n_p
                         double *dst = out + DYA + ((((1 << L) - 1 + q) * 13 + s) * NF + n);
                         if constexpr (LAYOUT == 1) {
                             *dst = v[n];
+                        } else if constexpr (Traits<M>::kPairs) {
+                            *reinterpret_cast<float2 *>(dst) = pair_slot(v, n);
                         } else {
                             const float hi = (float)v[n];
                             *reinterpret_cast<float2 *>(dst) = make_float2(hi, (float)(v[n] - (double)hi));

@@ -14,6 +14,7 @@
 
 #include "../../include/hhg_gpu.h"
 #include "hhg_launch.cuh"
+#include "hhg_pulse_prep.hpp"
 
 using hhg::PulseDev;
 
@@ -1003,7 +1004,7 @@ static hhg_status plan_create_impl(hhg_ctx *ctx, const hhg_system_desc *sys,
         return set_err(ctx, HHG_UNSUPPORTED,
                        "the closed-form Magnus step is the Dirac-3D model's, in FP64, one step per "
                        "interval (no step proposer)");
-    if (o.stepper == HHG_STEPPER_MAGNUS4 && (o.magnus_substeps < 1 || o.magnus_substeps > 4096))
+    if (o.stepper == HHG_STEPPER_MAGNUS4 && !hhg_prep::magnus_substeps_ok(o.magnus_substeps))
         return set_err(ctx, HHG_BAD_CONFIG, "magnus_substeps out of range");
     if (o.stepper == HHG_STEPPER_MAGNUS4 && o.precision != HHG_PREC_FP64)
         return set_err(ctx, HHG_UNSUPPORTED, "Magnus-4 runs in FP64 only");
@@ -1707,7 +1708,6 @@ hhg_status hhg_measure_fp32_peak(hhg_ctx *ctx, double *tflops) {
 // Same arithmetic as hhg_plan_create for one pulse; kept separate so the plan
 // path is untouched.
 // ---------------------------------------------------------------------------
-#include "hhg_pulse_prep.hpp"
 
 namespace hhg_prep {
 

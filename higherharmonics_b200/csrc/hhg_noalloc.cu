@@ -1,4 +1,5 @@
-// hhg_noalloc.cu -- the allocation-free entry point hhg_gpu_current_density_noalloc.
+// hhg_noalloc.cu -- the allocation-free entry point hhg_gpu_current_density_noalloc
+// and its status query hhg_noalloc_status.
 //
 // Some callers cannot allocate device memory while they call this library:
 // code running inside another framework's memory pool or allocator hooks,
@@ -13,11 +14,19 @@
 //
 // The array is part of this module: every GPU that loads it (its first use on
 // that device) holds kNoAllocScratchBytes until the process exits.  All calls
-// share the array and it keeps the last call's contents; the counters are
-// cleared on every call and every other byte the kernels read is rewritten
-// first.  Calls whose work overlaps on the GPU (different streams, or
+// share the array and it keeps the last call's contents; a set-up kernel
+// clears the counters and rewrites the pulse record and time grid on every
+// call, and every other byte the kernels read is written by the staging
+// kernel first.  Calls whose work overlaps on the GPU (different streams, or
 // different host threads on one device) race on the array and must be
 // serialised by the caller.
+//
+// The call enqueues kernels only (the pulse record travels as a kernel
+// argument, the time grid is accumulated on the device), so no copy reads
+// host memory after the call returns.  The scratch address is looked up once
+// per device and cached; this assumes the device's primary context for the
+// life of the process (after cudaDeviceReset the module, and the array, may
+// be reloaded at another address).
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -97,6 +106,81 @@ cudaError_t stage_model(int model, const hhg::StageReq &s) {
     return cudaErrorInvalidValue;
 }
 
+// Scratch header (first 256 bytes): the kernels' counters [0] next item,
+// [1] attempted, [2] rejected, [3] failed, [4] non-finite (unsigned long
+// long), the status word at byte 64, and the last call's k rows, degree and
+// work items for hhg_noalloc_status.
+constexpr size_t kOffStatus = 64;
+constexpr size_t kOffInfo = 128;
+struct NoAllocInfo {
+    long long n_rows;
+    long long items;
+    int degree;
+    int pad;
+};
+
+// One thread: clears the counters and the status word, records the call's
+// sizes, writes the pulse record and the interval offsets, and accumulates the
+// measurement times exactly as the host does (t_end += measure_every, a serial
+// sum of doubles, so the grid is bitwise the regular entry point's).
+__global__ void noalloc_setup_kernel(hhg::PulseDev pd, long long n_meas, NoAllocInfo info,
+                                     unsigned char *base, hhg::PulseDev *d_pulse,
+                                     long long *d_ioff, double *d_tgrid) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    unsigned long long *cnt = reinterpret_cast<unsigned long long *>(base);
+    for (int c = 0; c < 8; ++c) cnt[c] = 0ull;
+    *reinterpret_cast<int *>(base + kOffStatus) = 0;
+    *reinterpret_cast<NoAllocInfo *>(base + kOffInfo) = info;
+    *d_pulse = pd;
+    d_ioff[0] = 0;
+    d_ioff[1] = n_meas;
+    double t_begin = pd.window_begin, t_end = t_begin + pd.measure_every;
+    d_tgrid[0] = t_begin;
+    for (long long i = 1; i <= n_meas; ++i) {
+        d_tgrid[i] = t_end;
+        t_begin = t_end;
+        t_end += pd.measure_every;
+    }
+}
+
+// Counters and status word of the last call on the current device -> stats
+// and the status code (synchronises the stream).
+hhg_status read_outcome(unsigned char *base, cudaStream_t s, hhg_stats *stats, char *err,
+                        size_t err_cap) {
+    unsigned long long cnt[8];
+    int status_h = 0;
+    NoAllocInfo info{};
+    cudaError_t e;
+    if ((e = cudaMemcpyAsync(cnt, base, sizeof cnt, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(&status_h, base + kOffStatus, sizeof status_h, cudaMemcpyDeviceToHost,
+                             s)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(&info, base + kOffInfo, sizeof info, cudaMemcpyDeviceToHost, s)) !=
+            cudaSuccess ||
+        (e = cudaStreamSynchronize(s)) != cudaSuccess) {
+        set_msg(err, err_cap, cudaGetErrorString(e));
+        return HHG_CUDA_ERROR;
+    }
+    if (stats) {
+        std::memset(stats, 0, sizeof *stats);
+        stats->k_points = info.n_rows;
+        stats->trajectories = info.n_rows;
+        stats->attempted_steps = (int64_t)cnt[1];
+        stats->rejected_steps = (int64_t)cnt[2];
+        stats->failed_trajectories = (int64_t)(cnt[3] + cnt[4]);
+        stats->poly_degree = info.degree;
+        stats->items = (int32_t)info.items;
+    }
+    if (status_h == 2) {
+        set_msg(err, err_cap, "a trajectory exceeded the failed-step or step limit");
+        return HHG_STEP_LIMIT;
+    }
+    if (status_h == 3) {
+        set_msg(err, err_cap, "non-finite Bloch vector");
+        return HHG_NONFINITE;
+    }
+    return HHG_OK;
+}
+
 }  // namespace
 
 extern "C" hhg_status hhg_gpu_current_density_noalloc(const hhg_system_desc *sys,
@@ -120,7 +204,8 @@ extern "C" hhg_status hhg_gpu_current_density_noalloc(const hhg_system_desc *sys
     }
     if ((o.stepper != HHG_STEPPER_RKF78 && o.stepper != HHG_STEPPER_MAGNUS4) ||
         (o.precision != HHG_PREC_FP64 && o.precision != HHG_PREC_MIXED) ||
-        (o.stepper == HHG_STEPPER_MAGNUS4 && (o.precision != HHG_PREC_FP64 || o.magnus_substeps < 1)) ||
+        (o.stepper == HHG_STEPPER_MAGNUS4 &&
+         (o.precision != HHG_PREC_FP64 || !hhg_prep::magnus_substeps_ok(o.magnus_substeps))) ||
         !(o.abs_tol >= 0.0) || !(o.rel_tol >= 0.0) || !(o.abs_tol + o.rel_tol > 0.0)) {
         set_msg(err, err_cap, "invalid solver options");
         return HHG_BAD_CONFIG;
@@ -182,9 +267,8 @@ extern "C" hhg_status hhg_gpu_current_density_noalloc(const hhg_system_desc *sys
     pd.part_off = 0;
     pd.j_off = 0;
     pd.items = (int)items;
-    const long long ioff[2] = {0, N};
     unsigned long long *counters = reinterpret_cast<unsigned long long *>(base);
-    int *status = reinterpret_cast<int *>(base + 64);
+    int *status = reinterpret_cast<int *>(base + kOffStatus);
     hhg::PulseDev *d_pulse = reinterpret_cast<hhg::PulseDev *>(base + off_pulse);
     long long *d_ioff = reinterpret_cast<long long *>(base + off_ioff);
     double *d_tgrid = reinterpret_cast<double *>(base + off_tgrid);
@@ -196,11 +280,9 @@ extern "C" hhg_status hhg_gpu_current_density_noalloc(const hhg_system_desc *sys
         return HHG_CUDA_ERROR;
     };
     cudaError_t e;
-    // pageable sources: each copy has consumed its source when it returns
-    if ((e = cudaMemsetAsync(base, 0, 256, s)) != cudaSuccess) return fail(e);
-    if ((e = cudaMemcpyAsync(d_pulse, &pd, sizeof pd, cudaMemcpyHostToDevice, s)) != cudaSuccess) return fail(e);
-    if ((e = cudaMemcpyAsync(d_ioff, ioff, sizeof ioff, cudaMemcpyHostToDevice, s)) != cudaSuccess) return fail(e);
-    if ((e = cudaMemcpyAsync(d_tgrid, prep.tgrid.data(), sizeof(double) * (N + 1), cudaMemcpyHostToDevice, s)) != cudaSuccess) return fail(e);
+    const NoAllocInfo info{(long long)n_rows, items, prep.degree, 0};
+    noalloc_setup_kernel<<<1, 32, 0, s>>>(pd, (long long)N, info, base, d_pulse, d_ioff, d_tgrid);
+    if ((e = cudaGetLastError()) != cudaSuccess) return fail(e);
 
     const double grow_max = 9.0 / 10.0 * pow(pow(5.0, -8.0), -1.0 / 8);
     hhg::StageReq sr{d_pulse, 1, d_tgrid, d_ioff, d_coef, (long long)N, prep.degree, grow_max, s};
@@ -243,27 +325,18 @@ extern "C" hhg_status hhg_gpu_current_density_noalloc(const hhg_system_desc *sys
     if ((e = cudaGetLastError()) != cudaSuccess) return fail(e);
 
     if (!stats) return HHG_OK;
-    // counters and status word to the host (fixed-size stack copy)
-    unsigned long long cnt[8];
-    int status_h = 0;
-    if ((e = cudaMemcpyAsync(cnt, counters, sizeof cnt, cudaMemcpyDeviceToHost, s)) != cudaSuccess) return fail(e);
-    if ((e = cudaMemcpyAsync(&status_h, status, sizeof status_h, cudaMemcpyDeviceToHost, s)) != cudaSuccess) return fail(e);
-    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return fail(e);
-    std::memset(stats, 0, sizeof *stats);
-    stats->k_points = n_rows;
-    stats->trajectories = n_rows;
-    stats->attempted_steps = (int64_t)cnt[1];
-    stats->rejected_steps = (int64_t)cnt[2];
-    stats->failed_trajectories = (int64_t)(cnt[3] + cnt[4]);
-    stats->poly_degree = prep.degree;
-    stats->items = (int32_t)items;
-    if (status_h == 2) {
-        set_msg(err, err_cap, "a trajectory exceeded the failed-step or step limit");
-        return HHG_STEP_LIMIT;
+    return read_outcome(base, s, stats, err, err_cap);
+}
+
+extern "C" hhg_status hhg_noalloc_status(void *stream, hhg_stats *stats, char *err, size_t err_cap) {
+    set_msg(err, err_cap, "");
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        set_msg(err, err_cap, "no current CUDA device");
+        return HHG_CUDA_ERROR;
     }
-    if (status_h == 3) {
-        set_msg(err, err_cap, "non-finite Bloch vector");
-        return HHG_NONFINITE;
-    }
-    return HHG_OK;
+    unsigned char *base = nullptr;
+    const hhg_status st = scratch_for_device(dev, &base, err, err_cap);
+    if (st != HHG_OK) return st;
+    return read_outcome(base, static_cast<cudaStream_t>(stream), stats, err, err_cap);
 }

@@ -10,6 +10,11 @@
 
 namespace hhg_prep {
 
+// Magnus-4 substeps per measurement interval accepted by every entry point
+// (a larger count would run a persistent launch for minutes to hours).
+constexpr int kMaxMagnusSubsteps = 4096;
+inline bool magnus_substeps_ok(int n) { return n >= 1 && n <= kMaxMagnusSubsteps; }
+
 struct PulsePrep {
     int model = 0;   // hhg::Model
     int nf = 0;      // staged pulse functions

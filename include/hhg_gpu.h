@@ -416,18 +416,32 @@ hhg_status hhg_measure_fp32_peak(hhg_ctx *ctx, double *tflops);
  * on which the entry point is used holds the 64 MiB until the process exits.
  *
  * Runs asynchronously on `stream` (a cudaStream_t; NULL = the legacy default
- * stream) on the current device.  With stats != NULL it synchronises the
- * stream and reports HHG_STEP_LIMIT / HHG_NONFINITE like the other entry
- * points; with stats == NULL those conditions are not checked.  The first
- * call on a device looks up the scratch array's device address (once per
- * device); make that first call before any stream capture.  All calls share
- * the one array: calls that overlap on the GPU race and must be serialised by
- * the caller.  err (optional, err_cap bytes) receives a message on failure. */
+ * stream) on the current device; it enqueues kernels only, so nothing it
+ * enqueues reads host memory after it returns.  With stats != NULL it
+ * synchronises the stream and reports HHG_STEP_LIMIT / HHG_NONFINITE like the
+ * other entry points; with stats == NULL it returns after enqueueing, and
+ * hhg_noalloc_status reports those conditions once the caller wants them.
+ * The first call on a device looks up the scratch array's device address
+ * (once per device, cached; the cache assumes the device's primary context
+ * and no cudaDeviceReset for the life of the process); make that first call
+ * before any stream capture.  All calls share the one array, which keeps the
+ * last call's contents: calls that overlap on the GPU race and must be
+ * serialised by the caller.  Magnus-4 takes 1 to 4096 substeps, as in the
+ * other entry points.  err (optional, err_cap bytes) receives a message on
+ * failure. */
 hhg_status hhg_gpu_current_density_noalloc(const hhg_system_desc *sys,
                                            const hhg_pulse_desc *pulse, const double *d_rows,
                                            int64_t n_rows, const hhg_solver_opts *opts,
                                            double *d_j_out, void *stream, hhg_stats *stats,
                                            char *err, size_t err_cap);
+/* Outcome of the most recent hhg_gpu_current_density_noalloc call on the
+ * current device, for callers that passed stats == NULL: synchronises
+ * `stream` (the stream that call ran on), reads the counters and the status
+ * word the call left in the shared scratch array, fills stats (optional) and
+ * returns HHG_OK, HHG_STEP_LIMIT or HHG_NONFINITE as the call would have.
+ * Another call on the device after it overwrites what this reads.  Allocates
+ * nothing; no counterpart in the reference. */
+hhg_status hhg_noalloc_status(void *stream, hhg_stats *stats, char *err, size_t err_cap);
 
 /* Learned step-size proposer: collection, training and inference.  None has
  * a counterpart in the reference.

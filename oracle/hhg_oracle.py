@@ -191,6 +191,65 @@ def laser(p: Pulse, t) -> np.ndarray:
                      for v in np.atleast_1d(t)])
 
 
+def experimental_laser(e_a, e_b, dt_ps: float, pe_laser: float, e0: float, lattice: float,
+                       shift_ps: float = 0.0, active: str = "both", hbar: float = 6.582119569509065698e-13,
+                       n_extra: int = 16, begin_zero: int = 8, zero_buff: int = 8):
+    """ExperimentalLaser (sources/HHG/Laser/ExperimentalLaser.cpp:8-108)
+    restated for a caller's measured field: returns (SplinePulse of A(t),
+    t_end).
+
+    vector_potential (:30-62): begin_zero zeros, then A_i = A_(i-1) - E_i dt
+    (dt in ps), then A continued over n_extra - 1 steps by the quartic
+    p(t) = A + P t + Q t^2 + c t^3 + d t^4 with P = -E_last, Q = (E_(n-2) -
+    E_last) / (2 dt) and c, d from p(T) = p'(T) = 0 (T = (n_extra - 1) dt),
+    the last zero_buff + 1 entries zero.  compute_spline (:64-104): each
+    record's A splined (zero end slopes) on the unitless spacing h = pe dt /
+    (1e12 hbar), read where its (shifted) time lies in [0, laser_end], their
+    sum times 0.1 E0 lattice / hbar sampled at spacing h on [0, t_end] (t_end
+    = 1.5 laser_end) and splined again with zero end slopes; A(t) = 0 after
+    t_end (Laser.hpp:32-37)."""
+    def potential(e):
+        e = np.asarray(e, dtype=np.float64)
+        n = e.size
+        a = np.zeros(begin_zero + n + n_extra + zero_buff)
+        for i in range(n):
+            a[begin_zero + i] = a[begin_zero + i - 1] - e[i] * dt_ps
+        A = a[begin_zero + n - 1]
+        P = -e[n - 1]
+        Q = 0.5 * (e[n - 2] - e[n - 1]) / dt_ps
+        T = (n_extra - 1) * dt_ps
+        c = -4 * (Q / (2 * T) + (3 * P) / (4 * T * T) + A / (T * T * T))
+        d = -0.25 * (3 * c / T + 2 * Q / (T * T) + P / (T * T * T))
+        for i in range(1, n_extra):
+            t = i * dt_ps
+            a[begin_zero + n - 1 + i] = A + P * t + Q * t * t + c * t * t * t + d * t * t * t * t
+        a[a.size - begin_zero - 1:] = 0.0
+        return a
+
+    per_ps = pe_laser / (1e12 * hbar)
+    h = pe_laser * (dt_ps / (1e12 * hbar))
+    n_rec = np.asarray(e_a).size
+    laser_end_ps = (n_rec - 1) * dt_ps + (n_extra + begin_zero + zero_buff) * dt_ps
+    t_end = (1.5 * laser_end_ps) * per_ps
+    end = pe_laser * (laser_end_ps / (1e12 * hbar))
+    shift = shift_ps * per_ps
+    sa = SplinePulse(potential(e_a), 0.0, h, cut=1e300, deriv=(0.0, 0.0))
+    sb = SplinePulse(potential(e_b), 0.0, h, cut=1e300, deriv=(0.0, 0.0))
+    m = int(t_end / h + 1)
+    vals = np.zeros(m + 1)
+    for i in range(m + 1):
+        t = h * i
+        if shift >= 0:
+            va = laser(sa, t)[0] if t <= end else 0.0
+            vb = laser(sb, t - shift)[0] if 0 <= t - shift <= end else 0.0
+        else:
+            va = laser(sa, t + shift)[0] if 0 <= t + shift <= end else 0.0
+            vb = laser(sb, t)[0] if t <= end else 0.0
+        v = va + vb if active == "both" else (va if active == "A" else vb)
+        vals[i] = (0.1 / hbar) * e0 * lattice * v
+    return SplinePulse(vals, 0.0, h, cut=t_end, deriv=(0.0, 0.0)), t_end
+
+
 def initial_state(m: OrcModel, kx: float, ky: float, kz: float) -> np.ndarray:
     """orc_initial_state: the model's initial Bloch vector at (kx, ky, kz)."""
     L = lib()

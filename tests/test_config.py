@@ -3,6 +3,7 @@ parsing, the unit mapping of the reference's dispatchers and constructors,
 and the configurations the engine refuses.  CPU only."""
 import math
 
+import numpy as np
 import pytest
 
 from higherharmonics_b200 import api, config
@@ -155,7 +156,28 @@ def test_double_lasers_use_the_experimental_photon_energy():
     assert _laser("dcosA", t0="0.5").pulse._samples[500] == pytest.approx(cosl(a, t), abs=1e-12)
 
 
+def synthetic_field(n=201, seed=7):
+    """A smooth two-pulse field in MV/cm at the reference's sample spacing
+    (seeded; not measured data): Gaussian-enveloped carriers near the data's
+    photon energy, pulse B weaker and later."""
+    rng = np.random.default_rng(seed)
+    t = np.arange(n) * config.EXP_DT_PS
+    w = 2 * math.pi * config.EXP_PHOTON_ENERGY / (1e12 * HBAR) * 1e-12  # rad / ps
+    a = 0.03 * np.exp(-((t - 2.5) / 0.9) ** 2) * np.cos(w * (t - 2.5) + rng.uniform(0, 1))
+    b = 0.012 * np.exp(-((t - 4.0) / 0.8) ** 2) * np.cos(w * (t - 4.0) + rng.uniform(0, 1))
+    return a, b
+
+
+def _exp_config(tmp_path, lt, t0="0", extra=""):
+    a, b = synthetic_field()
+    path = tmp_path / "field.dat"
+    np.savetxt(path, np.c_[a, b])
+    return PIFLUX.replace("laser_type cosine", f"laser_type {lt}\nexperimental_field {path}{extra}") \
+        .replace("t0_offset 2", f"t0_offset {t0}").replace("photon_energy 5.25", "photon_energy 1")
+
+
 def test_experimental_and_unknown_lasers():
+    # without a measured field the experimental lasers are refused
     with pytest.raises(config.UnsupportedConfig):
         _laser("expB")
     with pytest.raises(ValueError):
@@ -204,3 +226,69 @@ def test_dirac_mapping():
             config.from_config(cfg.replace("laser_type cosine", f"laser_type {lt}"))
     with pytest.raises(ValueError):
         config.from_config(cfg.replace("n_z 51\n", ""))
+
+
+def test_measured_vector_potential_construction():
+    """ExperimentalLaser's vector_potential: running sum, quartic tail that
+    lands on zero with zero slope, zero padding."""
+    a, _ = synthetic_field()
+    dt = config.EXP_DT_PS
+    A = config.measured_vector_potential(a, dt)
+    n, bz, ne = a.size, config.EXP_BEGIN_ZERO, config.EXP_N_EXTRA
+    assert A.size == n + ne + config.EXP_ZERO_BUFF + bz
+    assert np.all(A[:bz] == 0) and np.all(A[A.size - bz - 1:] == 0)
+    assert A[bz + n - 1] == pytest.approx(-dt * a.sum(), rel=1e-12)
+    # the tail's polynomial reaches 0 with zero slope at T = (n_extra - 1) dt
+    tail = A[bz + n - 1: bz + n - 1 + ne]
+    assert abs(tail[-1]) <= 1e-12 * np.abs(A).max()
+    # it is one quartic: its fit through the 16 points has p'(T) = 0 and
+    # continues A with slope -E_last
+    tt = np.arange(ne) * dt
+    c = np.polynomial.polynomial.polyfit(tt, tail, 4)
+    d = np.polynomial.polynomial.polyder(c)
+    scale = np.abs(tail).max() / tt[-1]
+    assert abs(np.polynomial.polynomial.polyval(tt[-1], d)) <= 1e-8 * scale
+    assert np.polynomial.polynomial.polyval(0.0, d) == pytest.approx(-a[-1], rel=1e-6, abs=1e-8 * scale)
+
+
+@pytest.mark.parametrize("lt,t0", [("exp", "0"), ("expA", "0"), ("expB", "0.4"), ("exp", "-0.3")])
+def test_experimental_laser_matches_the_oracle(tmp_path, lt, t0):
+    """The config reader's experimental pulse (the engine's spline samples)
+    against the oracle's independent restatement of ExperimentalLaser."""
+    from oracle import hhg_oracle as O
+    run = config.from_config(_exp_config(tmp_path, lt, t0))
+    p = run.pulse
+    assert p.kind == api.PULSE_SPLINE and (p.deriv_begin, p.deriv_end) == (0.0, 0.0)
+    pe_l = 1.0 * config.EXP_PHOTON_ENERGY
+    # the system takes the experimental photon energy too (get_photon_energy)
+    assert run.system.fermi_energy == pytest.approx(118 / pe_l)
+    lattice = math.sqrt(3) * HBAR * 1.5e6 / (pe_l * 300)
+    assert run.lattice_constant == pytest.approx(lattice, rel=1e-15)
+    a, b = synthetic_field()
+    sp, t_end = O.experimental_laser(a, b, config.EXP_DT_PS, pe_l, 1.6, lattice, float(t0),
+                                     {"exp": "both", "expA": "A", "expB": "B"}[lt])
+    assert p.spline_cut == pytest.approx(t_end, rel=1e-15)
+    assert (p.window_begin, p.window_end) == (0.0, pytest.approx(t_end, rel=1e-15))
+    assert p.n_samples == sp.y.size and p.sample_dt == pytest.approx(sp.dt, rel=1e-15)
+    scale = np.abs(sp.y).max()
+    assert scale > 0
+    assert np.max(np.abs(p._samples - sp.y)) <= 1e-13 * scale
+    # and A(t) between the knots
+    t = np.linspace(0.0, 1.1 * t_end, 777)
+    assert np.max(np.abs(api.pulse_values(p, t) - O.laser(sp, t))) <= 1e-12 * scale
+
+
+def test_experimental_laser_windows(tmp_path):
+    # PiFlux shortens the window for the run modes, Honeycomb does not
+    full = config.from_config(_exp_config(tmp_path, "exp")).pulse
+    red = config.from_config(_exp_config(tmp_path, "exp").replace("occupations no",
+                                                                  "occupations yes")).pulse
+    assert red.window_end == pytest.approx(0.75 * full.window_end)
+    hc = config.from_config(_exp_config(tmp_path, "exp").replace("system_type PiFlux",
+                                                                 "system_type Honeycomb")
+                            .replace("occupations no", "occupations yes")).pulse
+    assert hc.window_end == pytest.approx(full.window_end)
+    # the data's spacing and photon energy are keys of their own
+    alt = config.from_config(_exp_config(tmp_path, "exp",
+                                         extra="\nexperimental_photon_energy 5.0")).pulse
+    assert alt.sample_dt == pytest.approx(full.sample_dt * 5.0 / config.EXP_PHOTON_ENERGY)

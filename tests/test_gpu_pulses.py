@@ -149,6 +149,47 @@ def test_reference_laser_types_from_config(engine, laser):
     assert err <= J_TOL, (laser, err)
 
 
+@pytest.mark.parametrize("lt,t0", [("exp", "0"), ("expB", "0.3")])
+def test_experimental_laser_parity(engine, tmp_path, lt, t0):
+    """laser_type exp / expB from a (synthetic, seeded) measured field: the
+    config reader's spline pulse on the GPU against the oracle integrating its
+    own restatement of ExperimentalLaser."""
+    from oracle import hhg_oracle as O
+    from tests.helpers import oracle_args
+    from tests.test_config import HBAR, synthetic_field
+    a, b = synthetic_field()
+    path = tmp_path / "field.dat"
+    np.savetxt(path, np.c_[a, b])
+    txt = f"""
+    T 0
+    E_F 0
+    v_F 2e4
+    band_width 10
+    field_amplitude 0.8
+    photon_energy 1
+    diagonal_relaxation_time -1
+    laser_type {lt}
+    experimental_field {path}
+    n_laser_cycles 8
+    t0_offset {t0}
+    system_type PiFlux
+    """
+    run = config.from_config(txt, grid=api.grid_piflux3d_ref(1, 1))
+    pulse = run.pulse
+    rows = api.grid_rows(run.system, run.grid)
+    j, st = engine.current_density(run.system, pulse, run.grid, api.solver(1e-12, 1e-8))
+    m, _, tc, s = oracle_args(run.system, pulse, 1e-12, 1e-8)
+    pe_l = config.EXP_PHOTON_ENERGY
+    sp, _ = O.experimental_laser(a, b, config.EXP_DT_PS, pe_l, 0.8, run.lattice_constant,
+                                 float(t0), {"exp": "both", "expB": "B"}[lt], hbar=HBAR)
+    jr, _, rc = O.current_density(m, sp, tc, s, rows)
+    assert rc == 0
+    assert st.failed_trajectories == 0
+    assert np.abs(jr).max() > 0
+    assert rel_l2(j, jr) <= J_TOL, rel_l2(j, jr)
+    assert harmonic_rel_err(harmonics(j, pulse), harmonics(jr, pulse)) <= H_TOL
+
+
 def test_spline_refused_by_the_allocation_free_entry_point():
     import ctypes
 

@@ -9,8 +9,11 @@ integration scratch sits in the library's fixed 64 MiB device array.
 Checked through the C ABI against the regular entry point
 (hhg_gpu_current_density) on two consecutive calls -- the second call runs on
 whatever the first left in the shared scratch array -- within the parity
-tolerance of the GPU tests (relative L2 <= 1e-9).  This file is collected last
-so a failure here does not stop the rest of the GPU suite.
+tolerance of the GPU tests (relative L2 <= 1e-9), for the restart and carry
+proposers, the mixed-precision right-hand side and Magnus-4; an asynchronous
+call (stats == NULL) whose outcome is read afterwards with hhg_noalloc_status,
+including a step-limit status.  This file is collected last so a failure here
+does not stop the rest of the GPU suite.
 """
 import ctypes
 import math
@@ -35,24 +38,49 @@ def _noalloc(lib, sys, pulse, d_rows, n_rows, opts, d_j, stats=True):
     return rc, st, err.value.decode()
 
 
-@pytest.mark.parametrize("case", ["piflux2d", "honeycomb"])
-def test_noalloc_matches_regular_entry_point_twice(case):
+def _status(lib):
+    err = ctypes.create_string_buffer(512)
+    st = api.Stats()
+    rc = lib.hhg_noalloc_status(None, ctypes.byref(st), err, len(err))
+    return rc, st, err.value.decode()
+
+
+def _case(case):
+    if case == "piflux2d":
+        s = 1 / math.sqrt(2)
+        sys = api.system(api.SYS_PIFLUX2D, hopping=1.0, pol=(s, s))
+        pulse = api.cosine_pulse(1.0, 2, 2048, window=(0.0, 6 * math.pi), energy_scale=20.0)
+        grid = api.grid_tensor(32, 32, -math.pi, math.pi, -math.pi, math.pi)
+    else:
+        sys = api.system(api.SYS_HONEYCOMB, hopping=1.0, mass=0.1)
+        pulse = api.cosine_pulse(1.2, 2, 2048, phase=0.7, window=(0.0, 6 * math.pi),
+                                 energy_scale=12.5)
+        grid = api.grid_rhombic(24, 24)
+    return sys, pulse, grid
+
+
+OPTIONS = {
+    "restart": dict(),
+    "carry": dict(proposer=api.PROPOSER_CARRY),
+    "mixed_carry": dict(precision=api.PREC_MIXED, proposer=api.PROPOSER_CARRY, abs_tol=1e-8,
+                        rel_tol=1e-6),
+    "magnus4": dict(stepper=api.STEPPER_MAGNUS4, magnus_substeps=2),
+}
+
+
+@pytest.mark.parametrize("case,option", [("piflux2d", "restart"), ("honeycomb", "restart"),
+                                         ("piflux2d", "carry"), ("honeycomb", "mixed_carry"),
+                                         ("honeycomb", "magnus4")])
+def test_noalloc_matches_regular_entry_point_twice(case, option):
     import torch
     torch.cuda.set_device(0)
     lib = api.load_library()
     eng = api.Engine(0)
     try:
-        if case == "piflux2d":
-            s = 1 / math.sqrt(2)
-            sys = api.system(api.SYS_PIFLUX2D, hopping=1.0, pol=(s, s))
-            pulse = api.cosine_pulse(1.0, 2, 2048, window=(0.0, 6 * math.pi), energy_scale=20.0)
-            grid = api.grid_tensor(32, 32, -math.pi, math.pi, -math.pi, math.pi)
-        else:
-            sys = api.system(api.SYS_HONEYCOMB, hopping=1.0, mass=0.1)
-            pulse = api.cosine_pulse(1.2, 2, 2048, phase=0.7, window=(0.0, 6 * math.pi),
-                                     energy_scale=12.5)
-            grid = api.grid_rhombic(24, 24)
-        opts = api.solver(1e-12, 1e-8)
+        sys, pulse, grid = _case(case)
+        kw = dict(abs_tol=1e-12, rel_tol=1e-8)
+        kw.update(OPTIONS[option])
+        opts = api.solver(**kw)
         j_ref, st_ref = eng.current_density(sys, pulse, grid, opts)
         rows = api.grid_rows(sys, grid)
         d_rows = torch.from_numpy(rows).cuda()
@@ -73,7 +101,45 @@ def test_noalloc_matches_regular_entry_point_twice(case):
         eng.close()
 
 
-def test_noalloc_rejects_oversized_problem():
+def test_noalloc_async_call_and_status_query():
+    """stats == NULL: the call only enqueues; hhg_noalloc_status reports the
+    outcome afterwards -- a clean run, then a step limit, then a clean run
+    again (the counters are cleared on every call)."""
+    import torch
+    torch.cuda.set_device(0)
+    lib = api.load_library()
+    sys, pulse, grid = _case("piflux2d")
+    rows = api.grid_rows(sys, grid)
+    d_rows = torch.from_numpy(rows).cuda()
+    d_j = torch.empty(pulse.n_measurements + 1, dtype=torch.float64, device="cuda")
+    opts = api.solver(1e-12, 1e-8)
+    rc, st_sync, msg = _noalloc(lib, sys, pulse, d_rows.data_ptr(), rows.shape[0], opts,
+                                d_j.data_ptr())
+    assert rc == api.OK, msg
+    j_sync = d_j.cpu().numpy()
+    for tight in (False, True, False):
+        o = api.solver(1e-12, 1e-8)
+        if tight:
+            # the restart schedule needs 4 attempts per interval: 2 cannot land
+            o.max_attempts_per_interval = 2
+        d_j.fill_(float("nan"))
+        torch.cuda.synchronize()
+        rc, _, msg = _noalloc(lib, sys, pulse, d_rows.data_ptr(), rows.shape[0], o,
+                              d_j.data_ptr(), stats=False)
+        assert rc == api.OK, msg
+        rc, st, msg = _status(lib)
+        if tight:
+            assert rc == api.STEP_LIMIT, (rc, msg)
+            assert st.failed_trajectories > 0
+        else:
+            assert rc == api.OK, msg
+            assert st.attempted_steps == st_sync.attempted_steps
+            assert st.failed_trajectories == 0
+            assert st.k_points == rows.shape[0]
+            assert np.array_equal(d_j.cpu().numpy(), j_sync)
+
+
+def test_noalloc_rejects_oversized_problem_and_bad_options():
     import torch
     torch.cuda.set_device(0)
     lib = api.load_library()
@@ -88,3 +154,9 @@ def test_noalloc_rejects_oversized_problem():
                           d_j.data_ptr())
     assert rc == api.BAD_CONFIG
     assert "scratch" in msg, msg
+    # the regular path's Magnus-4 substep bound applies here too
+    small = d_rows[:64]
+    rc, _, msg = _noalloc(lib, sys, pulse, small.data_ptr(), 64,
+                          api.solver(stepper=api.STEPPER_MAGNUS4, magnus_substeps=5000),
+                          d_j.data_ptr())
+    assert rc == api.BAD_CONFIG, msg
