@@ -37,6 +37,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 namespace hhg {
 struct MlpPacked;
 }
@@ -396,10 +398,27 @@ template <int M, typename R> __host__ __device__ constexpr bool pair_layout() {
 template <int NF, typename R>
 struct TableEval {
     static constexpr bool kReuse = false;  // a shared-memory reload is cheaper than registers
-    const typename Num<R>::V *tab;  // 13 x NF values of one standard step
+    const typename Num<R>::V *tab;  // 13 x NF values of one standard step (16-byte aligned)
     __device__ __forceinline__ void operator()(int s, double, typename Num<R>::V *f) const {
+        if constexpr (NF % 2 == 0 && sizeof(typename Num<R>::V) == 8) {
+            // two values per 16-byte load (every table row starts on 16 bytes)
+            using V2 = typename std::conditional<sizeof(R) == sizeof(float), float4, double2>::type;
+            const V2 *t2 = reinterpret_cast<const V2 *>(tab + s * NF);
 #pragma unroll
-        for (int n = 0; n < NF; ++n) f[n] = tab[s * NF + n];
+            for (int n = 0; n < NF / 2; ++n) {
+                const V2 w = t2[n];
+                if constexpr (sizeof(R) == sizeof(float)) {
+                    f[2 * n] = make_float2(w.x, w.y);
+                    f[2 * n + 1] = make_float2(w.z, w.w);
+                } else {
+                    f[2 * n] = w.x;
+                    f[2 * n + 1] = w.y;
+                }
+            }
+        } else {
+#pragma unroll
+            for (int n = 0; n < NF; ++n) f[n] = tab[s * NF + n];
+        }
     }
 };
 

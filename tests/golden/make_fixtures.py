@@ -1,8 +1,8 @@
 """Generate the golden fixtures under tests/golden/ from the reference tree.
 
-Run in a container where the HigherHarmonics sources are mounted (default
-/root/reference, or pass the path).  Nothing at test time reads the reference;
-the tests only read the JSON files written here.
+Run as `python tests/golden/make_fixtures.py <path of the HigherHarmonics
+source tree>` where the reference sources are available.  Nothing at test time
+reads the reference; the tests only read the JSON files written here.
 
 * gauss_tables.json -- every gauss::container<N> table of
   sources/HHG/thread_gauss.hpp (positive abscissae ascending, weights), parsed
@@ -111,7 +111,9 @@ def piflux_ic(ref: str, n_points: int = 12, seed: int = 20261203) -> dict:
 
 
 def main() -> None:
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2 or not os.path.isdir(os.path.join(sys.argv[1], "sources")):
+        sys.exit("usage: make_fixtures.py <HigherHarmonics source tree (holds sources/ and helper/)>")
+    ref = sys.argv[1]
     with open(os.path.join(HERE, "gauss_tables.json"), "w") as f:
         json.dump(gauss_tables(ref), f)
     with open(os.path.join(HERE, "magnus_dirac.json"), "w") as f:
