@@ -141,10 +141,24 @@ __device__ __forceinline__ void mma_bf16_16816(float *d, const uint32_t *a, uint
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
+// Four 8x8 b16 matrices from shared memory (ldmatrix): lanes 8i .. 8i+7 give
+// the row addresses of matrix i (16-byte aligned rows); lane l receives row
+// l / 4, columns 2 (l mod 4) and 2 (l mod 4) + 1 of each matrix -- the B
+// fragment layout of mma.m16n8k16 when a matrix row is one output column's
+// eight consecutive k.
+__device__ __forceinline__ void ldsm_x4(const __nv_bfloat16 *row, uint32_t &r0, uint32_t &r1,
+                                        uint32_t &r2, uint32_t &r3) {
+    const unsigned a = (unsigned)__cvta_generic_to_shared(row);
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0, %1, %2, %3}, [%4];\n"
+                 : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
+                 : "r"(a));
+}
+
 // One hidden layer for one 16-row m-tile: acc[nt][4] = A W^T + b over eight
 // n8 tiles, SiLU, repacked in place as the next layer's A fragments
 // out[kc][4] (the m16n8 accumulators of two adjacent n-tiles form the
-// m16n8k16 A operand).
+// m16n8k16 A operand).  The B fragments of two n-tiles come from one
+// ldmatrix.x4 (W rows 8 nt .. 8 nt + 15, k halves 16 kc and 16 kc + 8).
 template <int KC, int LD>
 __device__ __forceinline__ void mlp_hidden(const uint32_t (&a)[KC][4], const __nv_bfloat16 *w,
                                            const float *b, uint32_t (&out)[4][4], int g, int tig) {
@@ -154,13 +168,17 @@ __device__ __forceinline__ void mlp_hidden(const uint32_t (&a)[KC][4], const __n
         acc[nt][0] = acc[nt][2] = b[8 * nt + 2 * tig];
         acc[nt][1] = acc[nt][3] = b[8 * nt + 2 * tig + 1];
     }
+    const int lane = threadIdx.x & 31;
+    // this lane's row address: matrix lane / 8 = (n-tile offset, k half)
+    const __nv_bfloat16 *wl = w + (8 * (lane >> 4) + (lane & 7)) * LD + 8 * ((lane >> 3) & 1);
 #pragma unroll
     for (int kc = 0; kc < KC; ++kc) {
 #pragma unroll
-        for (int nt = 0; nt < 8; ++nt) {
-            const __nv_bfloat16 *wr = w + (8 * nt + g) * LD + 16 * kc + 2 * tig;
-            mma_bf16_16816(acc[nt], a[kc], *reinterpret_cast<const uint32_t *>(wr),
-                           *reinterpret_cast<const uint32_t *>(wr + 8));
+        for (int nt = 0; nt < 8; nt += 2) {
+            uint32_t b0, b1, c0, c1;
+            ldsm_x4(wl + 8 * nt * LD + 16 * kc, b0, b1, c0, c1);
+            mma_bf16_16816(acc[nt], a[kc], b0, b1);
+            mma_bf16_16816(acc[nt + 1], a[kc], c0, c1);
         }
     }
 #pragma unroll
@@ -202,11 +220,14 @@ __device__ __forceinline__ float mlp_warp_infer(const MlpSmem &W, const float *f
         mlp_hidden<4, kLdH>(h1, W.w2, W.b2, h2, g, tig);
         mlp_hidden<4, kLdH>(h2, W.w3, W.b3, h1, g, tig);
         float o[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+        // output layer: one n8 tile; an ldmatrix.x4 carries two k slices
+        const __nv_bfloat16 *w4l = W.w4 + (lane & 7) * kLdH + 16 * (lane >> 4) + 8 * ((lane >> 3) & 1);
 #pragma unroll
-        for (int kc = 0; kc < 4; ++kc) {
-            const __nv_bfloat16 *wr = W.w4 + g * kLdH + 16 * kc + 2 * tig;
-            mma_bf16_16816(o, h1[kc], *reinterpret_cast<const uint32_t *>(wr),
-                           *reinterpret_cast<const uint32_t *>(wr + 8));
+        for (int kc = 0; kc < 4; kc += 2) {
+            uint32_t b0, b1, c0, c1;
+            ldsm_x4(w4l + 16 * kc, b0, b1, c0, c1);
+            mma_bf16_16816(o, h1[kc], b0, b1);
+            mma_bf16_16816(o, h1[kc + 1], c0, c1);
         }
         // row r of this m-tile, column 0: lane 4 (r mod 8), register 0 (r < 8) or 2
         const int r = lane & 15;
