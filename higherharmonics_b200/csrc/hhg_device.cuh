@@ -1464,18 +1464,6 @@ __device__ void integrate_free(const KParams &P, const ModelState<M, double> &ms
     }
 }
 
-// Asynchronous 16-byte global -> shared copies (cp.async, L2 only), grouped
-// per thread; a wait plus __syncwarp makes a warp's copies visible to all of
-// its lanes.
-__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
-    const unsigned a = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(a), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N> __device__ __forceinline__ void cp_async_wait() {
-    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
-}
-
 constexpr int kLevelMax = 10;
 // dynamic shared memory of the learned-proposer kernels
 __host__ __device__ constexpr int mlp_smem_bytes() {
@@ -1511,21 +1499,10 @@ __global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integ
     // is read from global memory
     // the relaxation models on the reference schedule run free lanes (above)
     constexpr bool kFree = Traits<M>::kRelax && PROPOSER == 0 && STEPPER == 0 && OUT == 0;
-    // Warp-synchronous steppers: each interval's record (header) and its
-    // level-0 stage table are fetched into shared memory one interval ahead
-    // (double buffer, cp.async), so neither the sample record nor the
-    // common one-step interval waits on global memory; the interpolants
-    // (levels >= kDyaLevels) and the finer tables are read from the staging
-    // table where a warp needs them.
-    constexpr bool kPrefetch = kDyadic && STEPPER == 0 && OUT == 0;
-    constexpr int HDR = slot_header(NF);
-    constexpr int TAB0 = (13 * NF + 1) & ~1;  // level-0 table, rounded to 16 bytes
-    constexpr int PF = HDR + TAB0;
-    constexpr int COPY = kFree ? 2 : (PROPOSER == 0) ? SLOT : kPrefetch ? 2 : SCHED;
+    constexpr int COPY = kFree ? 2 : (PROPOSER == 0) ? SLOT : SCHED;
     constexpr int NTAB = kMaxStd * 13 * NF;
     using V = typename Num<R>::V;
     __shared__ __align__(16) double stage_raw[kWarpsPerBlock][COPY];
-    __shared__ __align__(16) double pf_buf[kWarpsPerBlock][kPrefetch ? 2 : 1][kPrefetch ? PF : 2];
     __shared__ double free_ring[kWarpsPerBlock][kFree ? kFreeWindow * 32 : 1];
     __shared__ __align__(16) V stage_tab[kWarpsPerBlock][kNarrow && PROPOSER == 0 ? NTAB : 1];
     // learned proposer: the network and per-warp input tiles in dynamic shared
@@ -1573,8 +1550,8 @@ __global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integ
             bool dead = !valid;
             double carry_dt = dt0;
             int level = 0;      // warp-uniform dyadic level carried across intervals
-            // the last interval ended at level 0 with every lane's error below
-            // 1/600 of its tolerance (learned proposer: nothing to propose)
+            // the last interval took one step at level 0 without a rejection
+            // (learned proposer: the warp rests on the one-step floor)
             bool easy = false;
             double held = 0.0;  // lane (i & 31) holds the warp sum of sample i
             double held2 = 0.0; // ... and of its second channel (OUT 1)
@@ -1606,19 +1583,6 @@ __global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integ
                 integrate_free<M, D>(P, ms, coef, dt0, tb, te, N, w, dead, S, held, prow, sub, lane,
                                      free_ring[wib], my_attempts, my_rejects);
             } else {
-            // header chunks, then level-0 table chunks (16 bytes each); slot
-            // offsets DYA and HDR are even, so every chunk is 16-byte aligned
-            auto prefetch = [&](const double *gs, double *dst) {
-                for (int c = lane; c < (HDR + TAB0) / 2; c += 32) {
-                    const bool h = c < HDR / 2;
-                    cp_async16(dst + (h ? 2 * c : HDR + 2 * (c - HDR / 2)),
-                               gs + (h ? 2 * c : DYA + 2 * (c - HDR / 2)));
-                }
-                cp_async_commit();
-            };
-            if constexpr (kPrefetch) {
-                if (N > 0) prefetch(coef, pf_buf[wib][0]);
-            }
             for (int i = 0; i <= N; ++i) {
                 const double *rec = pd.s0rec;
                 if (i > 0) {
@@ -1627,16 +1591,7 @@ __global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integ
                     // the record straight from the staging table: warp
                     // broadcasts of a few values per interval)
                     const double *gslot = coef + (size_t)(i - 1) * SLOT;
-                    if constexpr (kPrefetch) {
-                        // every lane is done with the buffer the next copy fills
-                        __syncwarp();
-                        if (i < N) {
-                            prefetch(gslot + SLOT, pf_buf[wib][i & 1]);
-                            cp_async_wait<1>();
-                        } else {
-                            cp_async_wait<0>();
-                        }
-                    } else if constexpr (STEPPER == 0) {
+                    if constexpr (STEPPER == 0) {
                         __syncwarp();
                         const double2 *src = reinterpret_cast<const double2 *>(gslot);
                         double2 *dst = reinterpret_cast<double2 *>(slot);
@@ -1652,10 +1607,10 @@ __global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integ
                         }
                     }
                     __syncwarp();
-                    const double *cur = kPrefetch ? pf_buf[wib][(i - 1) & 1] : STEPPER != 0 ? gslot : slot;
+                    const double *cur = STEPPER != 0 ? gslot : slot;
                     rec = cur + 4;
                     const double t0 = cur[0], t1 = cur[1];
-                    const PolyEval<NF, D, R, kPair> poly{kPrefetch ? gslot : slot, tb, te};
+                    const PolyEval<NF, D, R, kPair> poly{slot, tb, te};
                     if constexpr (STEPPER == 1) {
                         if (P.magnus_substeps == 1) {
                             double f1[NF], f2[NF];
@@ -1734,11 +1689,11 @@ __global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integ
                         const V *dtab = reinterpret_cast<const V *>(gslot + DYA);
                         const double span = t1 - t0;
                         if constexpr (kLearned) {
-                            // A warp at level 0 whose last step passed with a 600-fold
-                            // error margin (err^(1/8) margin of 2.2 in the step) is at the
-                            // floor of one step per interval and its next interval is
-                            // predictably within it: the proposal could only refine too
-                            // early, so the network is not consulted there.
+                            // A warp whose last interval took its one step at level 0
+                            // without a rejection rests on the floor of one step per
+                            // interval: a proposal can only keep it there or refine before
+                            // any lane has asked for it, so the network is consulted where
+                            // the warp is above the floor or has just been refined.
                             if (((i - 1) % P.mlp_every) == 0 && !easy) {
                                 // the network proposes each lane's level; the warp takes the
                                 // finest one (dead lanes propose level 0)
@@ -1751,7 +1706,8 @@ __global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integ
                             }
                         }
                         int L = level, qpos = 0;
-                        bool fallback = false, coarse_end = false;
+                        const bool from_floor = level == 0;
+                        bool fallback = false, coarse_end = false, refined = false;
                         for (;;) {
                             const double h = ldexp(span, -L);
                             const double tq = t0 + qpos * h;
@@ -1760,10 +1716,7 @@ __global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integ
                             if (!dead) {
                                 double e[3], k0[3];
                                 if (L < kDyaLevels) {
-                                    // level 0 from the prefetched copy in shared memory
-                                    const TableEval<NF, R> tev{
-                                        (kPrefetch && L == 0) ? reinterpret_cast<const V *>(cur + HDR)
-                                                              : dtab + ((1 << L) - 1 + qpos) * 13 * NF};
+                                    const TableEval<NF, R> tev{dtab + ((1 << L) - 1 + qpos) * 13 * NF};
                                     rkf78_attempt<M, NF, R>(ms, tev, tq, h, S, xn, e, k0);
                                 } else {
                                     rkf78_attempt<M, NF, R>(ms, poly, tq, h, S, xn, e, k0);
@@ -1798,6 +1751,7 @@ __global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integ
                                     fallback = true;
                                     break;
                                 }
+                                refined = true;
                                 ++L;
                                 qpos <<= 1;
                             }
@@ -1810,7 +1764,7 @@ __global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integ
                                 carry_dt, my_attempts, my_rejects);
                         }
                         level = (coarse_end && L > 0) ? L - 1 : (L > kLevelMax ? kLevelMax : L);
-                        easy = coarse_end && L == 0 && !fallback;
+                        easy = from_floor && !refined && !fallback;
                     }
                     if (!dead && !(isfinite(S[0]) && isfinite(S[1]) && isfinite(S[2]))) {
                         dead = true;
