@@ -1466,9 +1466,7 @@ __device__ void integrate_free(const KParams &P, const ModelState<M, double> &ms
 
 constexpr int kLevelMax = 10;
 // dynamic shared memory of the learned-proposer kernels
-__host__ __device__ constexpr int mlp_smem_bytes() {
-    return (int)sizeof(MlpSmem) + kWarpsPerBlock * 32 * kLdIn * 2;
-}
+__host__ __device__ constexpr int mlp_smem_bytes() { return mlp_stage_bytes(kWarpsPerBlock); }
 constexpr double kCoarsen = 1.0 / 600.0;
 
 // OUT 0: the Brillouin-zone sum of the current (one partial row per item);
@@ -1482,8 +1480,16 @@ constexpr double kCoarsen = 1.0 / 600.0;
 //   integrand of DiracSystem::compute_current_density,
 //   DiracSystem.cpp:300-311; dead trajectories give 0 and are counted).
 // OUT 1-3 are built for the PiFlux models only, OUT 4 for the Dirac-3D ones.
+// CTAs per SM the register budget is sized for: the model's, or 6 (168
+// registers) for the learned proposer, whose network call would otherwise
+// push the stepping loop's state into local memory at 128 registers
+// (measured on the learned-proposer workload: 8 % slower at 7 CTAs).
+template <int M, int PROPOSER> __host__ __device__ constexpr int min_blocks() {
+    return PROPOSER == 3 && Traits<M>::kMinBlocks > 6 ? 6 : Traits<M>::kMinBlocks;
+}
+
 template <int M, int D, typename R, int STEPPER, int PROPOSER, int OUT = 0>
-__global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integrate_kernel(const KParams P) {
+__global__ void __launch_bounds__(kBlockThreads, (min_blocks<M, PROPOSER>())) bz_integrate_kernel(const KParams P) {
     constexpr int NF = Traits<M>::NF;
     constexpr bool kDyadic = PROPOSER == 2 || PROPOSER == 3;
     constexpr bool kLearned = PROPOSER == 3;
@@ -1505,18 +1511,14 @@ __global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integ
     __shared__ __align__(16) double stage_raw[kWarpsPerBlock][COPY];
     __shared__ double free_ring[kWarpsPerBlock][kFree ? kFreeWindow * 32 : 1];
     __shared__ __align__(16) V stage_tab[kWarpsPerBlock][kNarrow && PROPOSER == 0 ? NTAB : 1];
-    // learned proposer: the network and per-warp input tiles in dynamic shared
-    // memory (mlp_smem_bytes(); none for the other modes)
+    // learned proposer: per-warp input tiles in dynamic shared memory
+    // (mlp_smem_bytes(); none for the other modes); the network itself is
+    // read from global memory
     extern __shared__ __align__(16) unsigned char dyn_smem[];
-    MlpSmem *mlp_s = reinterpret_cast<MlpSmem *>(dyn_smem);
-    __nv_bfloat16 *mlp_stage = reinterpret_cast<__nv_bfloat16 *>(dyn_smem + sizeof(MlpSmem));
+    __nv_bfloat16 *mlp_stage = reinterpret_cast<__nv_bfloat16 *>(dyn_smem);
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
     double *slot = stage_raw[wib];
-    if constexpr (kLearned) {
-        mlp_load_smem(P.mlp, mlp_s);
-        __syncthreads();
-    }
     const V *tabv;
     if constexpr (kNarrow && PROPOSER == 0) tabv = stage_tab[wib];
     else tabv = reinterpret_cast<const V *>(slot + (PROPOSER == 0 ? TAB : 0));
@@ -1699,8 +1701,8 @@ __global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integ
                                 // finest one (dead lanes propose level 0)
                                 float f[kMlpIn];
                                 mlp_features(row, gslot[DYA - 2], gslot[DYA - 1], S, -double(level), f);
-                                const float T = mlp_warp_infer(*mlp_s, f, mlp_stage + wib * 32 * kLdIn);
-                                int want = dead ? 0 : (int)ceilf(T + mlp_s->level_margin);
+                                const float T = mlp_warp_infer_call(P.mlp, f, mlp_stage + wib * 32 * kLdIn);
+                                int want = dead ? 0 : (int)ceilf(T + __ldg(&P.mlp->level_margin));
                                 want = want < 0 ? 0 : (want > kLevelMax ? kLevelMax : want);
                                 level = __reduce_max_sync(kFull, (unsigned)want);
                             }

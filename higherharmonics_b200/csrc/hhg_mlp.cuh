@@ -70,47 +70,14 @@ __device__ __forceinline__ void mlp_features(const double *row, double A, double
     f[7] = float(log2_hrel);
 }
 
-// Shared-memory copy of the network for warp-level inference.  Rows are
-// padded (16 -> 24, 64 -> 72 bf16) so the B-fragment loads of the eight
-// row groups of a warp hit distinct banks.
+// Warp-level inference reads the packed network from global memory (it is
+// 18 KB and shared by every warp, so it stays in L1/L2); only the per-warp
+// feature tile needs shared memory: 32 rows of kLdIn bf16 (16 features
+// padded to 24 so the A-fragment loads of the eight row groups hit distinct
+// banks).  A shared-memory copy per CTA would take ~23 KB from every
+// 2-warp CTA's share of L1 for the whole run, while the network is
+// consulted on a small fraction of the intervals.
 constexpr int kLdIn = 24;
-constexpr int kLdH = 72;
-struct MlpSmem {
-    __nv_bfloat16 w1[kMlpH * kLdIn];
-    __nv_bfloat16 w2[kMlpH * kLdH];
-    __nv_bfloat16 w3[kMlpH * kLdH];
-    __nv_bfloat16 w4[kMlpOutPad * kLdH];
-    float b1[kMlpH], b2[kMlpH], b3[kMlpH];
-    float b4, out_mu, out_sigma, level_margin;
-    float in_mu[kMlpIn], in_isig[kMlpIn];
-};
-
-// Cooperative copy of the packed network into shared memory (whole CTA).
-__device__ __forceinline__ void mlp_load_smem(const MlpPacked *g, MlpSmem *s) {
-    for (int i = threadIdx.x; i < kMlpH * kMlpInPad; i += blockDim.x)
-        s->w1[(i / kMlpInPad) * kLdIn + (i % kMlpInPad)] = (&g->w1[0][0])[i];
-    for (int i = threadIdx.x; i < kMlpH * kMlpH; i += blockDim.x) {
-        s->w2[(i / kMlpH) * kLdH + (i % kMlpH)] = (&g->w2[0][0])[i];
-        s->w3[(i / kMlpH) * kLdH + (i % kMlpH)] = (&g->w3[0][0])[i];
-    }
-    for (int i = threadIdx.x; i < kMlpOutPad * kMlpH; i += blockDim.x)
-        s->w4[(i / kMlpH) * kLdH + (i % kMlpH)] = (&g->w4[0][0])[i];
-    for (int i = threadIdx.x; i < kMlpH; i += blockDim.x) {
-        s->b1[i] = g->b1[i];
-        s->b2[i] = g->b2[i];
-        s->b3[i] = g->b3[i];
-    }
-    if (threadIdx.x < kMlpIn) {
-        s->in_mu[threadIdx.x] = g->in_mu[threadIdx.x];
-        s->in_isig[threadIdx.x] = g->in_isig[threadIdx.x];
-    }
-    if (threadIdx.x == 0) {
-        s->b4 = g->b4;
-        s->out_mu = g->out_mu;
-        s->out_sigma = g->out_sigma;
-        s->level_margin = g->level_margin;
-    }
-}
 
 __device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
     const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
@@ -141,44 +108,31 @@ __device__ __forceinline__ void mma_bf16_16816(float *d, const uint32_t *a, uint
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
-// Four 8x8 b16 matrices from shared memory (ldmatrix): lanes 8i .. 8i+7 give
-// the row addresses of matrix i (16-byte aligned rows); lane l receives row
-// l / 4, columns 2 (l mod 4) and 2 (l mod 4) + 1 of each matrix -- the B
-// fragment layout of mma.m16n8k16 when a matrix row is one output column's
-// eight consecutive k.
-__device__ __forceinline__ void ldsm_x4(const __nv_bfloat16 *row, uint32_t &r0, uint32_t &r1,
-                                        uint32_t &r2, uint32_t &r3) {
-    const unsigned a = (unsigned)__cvta_generic_to_shared(row);
-    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0, %1, %2, %3}, [%4];\n"
-                 : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
-                 : "r"(a));
+__device__ __forceinline__ uint32_t ldg_b32(const __nv_bfloat16 *p) {
+    return __ldg(reinterpret_cast<const unsigned int *>(p));
 }
 
 // One hidden layer for one 16-row m-tile: acc[nt][4] = A W^T + b over eight
 // n8 tiles, SiLU, repacked in place as the next layer's A fragments
 // out[kc][4] (the m16n8 accumulators of two adjacent n-tiles form the
-// m16n8k16 A operand).  The B fragments of two n-tiles come from one
-// ldmatrix.x4 (W rows 8 nt .. 8 nt + 15, k halves 16 kc and 16 kc + 8).
+// m16n8k16 A operand).  W is [64][LD] bf16 in global memory; lane (g, tig)
+// loads its B fragment W[8 nt + g][16 kc + 2 tig] and [... + 8] as 32-bit
+// words.
 template <int KC, int LD>
 __device__ __forceinline__ void mlp_hidden(const uint32_t (&a)[KC][4], const __nv_bfloat16 *w,
                                            const float *b, uint32_t (&out)[4][4], int g, int tig) {
     float acc[8][4];
 #pragma unroll
     for (int nt = 0; nt < 8; ++nt) {
-        acc[nt][0] = acc[nt][2] = b[8 * nt + 2 * tig];
-        acc[nt][1] = acc[nt][3] = b[8 * nt + 2 * tig + 1];
+        acc[nt][0] = acc[nt][2] = __ldg(b + 8 * nt + 2 * tig);
+        acc[nt][1] = acc[nt][3] = __ldg(b + 8 * nt + 2 * tig + 1);
     }
-    const int lane = threadIdx.x & 31;
-    // this lane's row address: matrix lane / 8 = (n-tile offset, k half)
-    const __nv_bfloat16 *wl = w + (8 * (lane >> 4) + (lane & 7)) * LD + 8 * ((lane >> 3) & 1);
 #pragma unroll
     for (int kc = 0; kc < KC; ++kc) {
 #pragma unroll
-        for (int nt = 0; nt < 8; nt += 2) {
-            uint32_t b0, b1, c0, c1;
-            ldsm_x4(wl + 8 * nt * LD + 16 * kc, b0, b1, c0, c1);
-            mma_bf16_16816(acc[nt], a[kc], b0, b1);
-            mma_bf16_16816(acc[nt + 1], a[kc], c0, c1);
+        for (int nt = 0; nt < 8; ++nt) {
+            const __nv_bfloat16 *wr = w + (8 * nt + g) * LD + 16 * kc + 2 * tig;
+            mma_bf16_16816(acc[nt], a[kc], ldg_b32(wr), ldg_b32(wr + 8));
         }
     }
 #pragma unroll
@@ -195,13 +149,14 @@ __device__ __forceinline__ void mlp_hidden(const uint32_t (&a)[KC][4], const __n
 // predicted level T for its own row.  `stage` is a 32 x kLdIn bf16 scratch
 // area of this warp in shared memory.  The two 16-row m-tiles run one after
 // the other to keep the register footprint small.
-__device__ __forceinline__ float mlp_warp_infer(const MlpSmem &W, const float *feat,
+__device__ __forceinline__ float mlp_warp_infer(const MlpPacked *__restrict__ W, const float *feat,
                                                 __nv_bfloat16 *stage) {
     const int lane = threadIdx.x & 31;
     const int g = lane >> 2, tig = lane & 3;
     __nv_bfloat16 *my = stage + lane * kLdIn;
 #pragma unroll
-    for (int c = 0; c < kMlpIn; ++c) my[c] = __float2bfloat16_rn((feat[c] - W.in_mu[c]) * W.in_isig[c]);
+    for (int c = 0; c < kMlpIn; ++c)
+        my[c] = __float2bfloat16_rn((feat[c] - __ldg(W->in_mu + c)) * __ldg(W->in_isig + c));
 #pragma unroll
     for (int c = kMlpIn; c < kMlpInPad; ++c) my[c] = __float2bfloat16_rn(0.0f);
     __syncwarp();
@@ -216,18 +171,14 @@ __device__ __forceinline__ float mlp_warp_infer(const MlpSmem &W, const float *f
         a1[0][2] = *reinterpret_cast<const uint32_t *>(r0 + 8);
         a1[0][3] = *reinterpret_cast<const uint32_t *>(r1 + 8);
         uint32_t h1[4][4], h2[4][4];
-        mlp_hidden<1, kLdIn>(a1, W.w1, W.b1, h1, g, tig);
-        mlp_hidden<4, kLdH>(h1, W.w2, W.b2, h2, g, tig);
-        mlp_hidden<4, kLdH>(h2, W.w3, W.b3, h1, g, tig);
+        mlp_hidden<1, kMlpInPad>(a1, &W->w1[0][0], W->b1, h1, g, tig);
+        mlp_hidden<4, kMlpH>(h1, &W->w2[0][0], W->b2, h2, g, tig);
+        mlp_hidden<4, kMlpH>(h2, &W->w3[0][0], W->b3, h1, g, tig);
         float o[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-        // output layer: one n8 tile; an ldmatrix.x4 carries two k slices
-        const __nv_bfloat16 *w4l = W.w4 + (lane & 7) * kLdH + 16 * (lane >> 4) + 8 * ((lane >> 3) & 1);
 #pragma unroll
-        for (int kc = 0; kc < 4; kc += 2) {
-            uint32_t b0, b1, c0, c1;
-            ldsm_x4(w4l + 16 * kc, b0, b1, c0, c1);
-            mma_bf16_16816(o, h1[kc], b0, b1);
-            mma_bf16_16816(o, h1[kc + 1], c0, c1);
+        for (int kc = 0; kc < 4; ++kc) {
+            const __nv_bfloat16 *wr = &W->w4[g][0] + 16 * kc + 2 * tig;
+            mma_bf16_16816(o, h1[kc], ldg_b32(wr), ldg_b32(wr + 8));
         }
         // row r of this m-tile, column 0: lane 4 (r mod 8), register 0 (r < 8) or 2
         const int r = lane & 15;
@@ -236,7 +187,18 @@ __device__ __forceinline__ float mlp_warp_infer(const MlpSmem &W, const float *f
         if ((lane >> 4) == mt) y_mine = r < 8 ? v0 : v2;
     }
     __syncwarp();
-    return (y_mine + W.b4) * W.out_sigma + W.out_mu;
+    return (y_mine + __ldg(&W->b4)) * __ldg(&W->out_sigma) + __ldg(&W->out_mu);
 }
+
+// The integration kernel's call: not inlined, so the inference's registers
+// are those of a function call made on a small fraction of the intervals and
+// the stepping loop keeps its own allocation.
+static __device__ __noinline__ float mlp_warp_infer_call(const MlpPacked *__restrict__ W,
+                                                         const float *feat, __nv_bfloat16 *stage) {
+    return mlp_warp_infer(W, feat, stage);
+}
+
+// Dynamic shared memory of a CTA of `warps` warps running the inference.
+__host__ __device__ constexpr int mlp_stage_bytes(int warps) { return warps * 32 * kLdIn * 2; }
 
 }  // namespace hhg

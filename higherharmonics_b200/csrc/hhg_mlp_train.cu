@@ -334,16 +334,13 @@ __global__ void __launch_bounds__(hhg::kBlockThreads) mlp_infer_kernel(const hhg
                                                                        const float *rec, int stride,
                                                                        long long n, float *out) {
     extern __shared__ __align__(16) unsigned char dyn[];
-    hhg::MlpSmem *W = reinterpret_cast<hhg::MlpSmem *>(dyn);
-    bf16 *stage = reinterpret_cast<bf16 *>(dyn + sizeof(hhg::MlpSmem));
-    hhg::mlp_load_smem(net, W);
-    __syncthreads();
+    bf16 *stage = reinterpret_cast<bf16 *>(dyn);
     const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const long long i = (blockIdx.x * (long long)hhg::kWarpsPerBlock + wib) * 32 + lane;
     float f[kIn];
 #pragma unroll
     for (int c = 0; c < kIn; ++c) f[c] = i < n ? rec[i * stride + c] : 0.0f;
-    const float T = hhg::mlp_warp_infer(*W, f, stage + wib * 32 * hhg::kLdIn);
+    const float T = hhg::mlp_warp_infer(net, f, stage + wib * 32 * hhg::kLdIn);
     if (i < n) out[i] = T;
 }
 
