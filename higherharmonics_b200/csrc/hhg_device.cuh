@@ -1480,16 +1480,8 @@ constexpr double kCoarsen = 1.0 / 600.0;
 //   integrand of DiracSystem::compute_current_density,
 //   DiracSystem.cpp:300-311; dead trajectories give 0 and are counted).
 // OUT 1-3 are built for the PiFlux models only, OUT 4 for the Dirac-3D ones.
-// CTAs per SM the register budget is sized for: the model's, or 6 (168
-// registers) for the learned proposer, whose network call would otherwise
-// push the stepping loop's state into local memory at 128 registers
-// (measured on the learned-proposer workload: 8 % slower at 7 CTAs).
-template <int M, int PROPOSER> __host__ __device__ constexpr int min_blocks() {
-    return PROPOSER == 3 && Traits<M>::kMinBlocks > 6 ? 6 : Traits<M>::kMinBlocks;
-}
-
 template <int M, int D, typename R, int STEPPER, int PROPOSER, int OUT = 0>
-__global__ void __launch_bounds__(kBlockThreads, (min_blocks<M, PROPOSER>())) bz_integrate_kernel(const KParams P) {
+__global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integrate_kernel(const KParams P) {
     constexpr int NF = Traits<M>::NF;
     constexpr bool kDyadic = PROPOSER == 2 || PROPOSER == 3;
     constexpr bool kLearned = PROPOSER == 3;
