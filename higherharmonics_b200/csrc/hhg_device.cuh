@@ -922,101 +922,6 @@ __device__ __forceinline__ float2 pmul(double c, float2 v) { return __fmul2_rn(p
 __device__ __forceinline__ float2 pfma(double c, float2 v, float2 acc) { return __ffma2_rn(pk(c), v, acc); }
 __device__ __forceinline__ float2 padd(float2 a, float2 b) { return __fadd2_rn(a, b); }
 
-// The Fehlberg 7(8) stage sums sum_j a_sj k_j of the packed FP32 attempt,
-// x and y of every stage on paired instructions and z scalar: stage S's sum
-// over k[0 .. S-1], grouped as independent pairs (shorter dependency chains).
-#define HHG_Z(c, j) (float(c) * kz[j])
-template <int S>
-__device__ __forceinline__ void rk_stage_sum(const float2 *k2, const float *kz, float2 &s2, float &sz) {
-    if constexpr (S == 1) {
-        s2 = pmul(2.0 / 27.0, k2[0]);
-        sz = HHG_Z(2.0 / 27.0, 0);
-    } else if constexpr (S == 2) {
-        s2 = pfma(1.0 / 12.0, k2[1], pmul(1.0 / 36.0, k2[0]));
-        sz = HHG_Z(1.0 / 36.0, 0) + HHG_Z(1.0 / 12.0, 1);
-    } else if constexpr (S == 3) {
-        s2 = pfma(1.0 / 8.0, k2[2], pmul(1.0 / 24.0, k2[0]));
-        sz = HHG_Z(1.0 / 24.0, 0) + HHG_Z(1.0 / 8.0, 2);
-    } else if constexpr (S == 4) {
-        s2 = padd(pmul(5.0 / 12.0, k2[0]), pfma(25.0 / 16.0, k2[3], pmul(-25.0 / 16.0, k2[2])));
-        sz = HHG_Z(5.0 / 12.0, 0) + (HHG_Z(-25.0 / 16.0, 2) + HHG_Z(25.0 / 16.0, 3));
-    } else if constexpr (S == 5) {
-        s2 = padd(pmul(1.0 / 20.0, k2[0]), pfma(1.0 / 5.0, k2[4], pmul(1.0 / 4.0, k2[3])));
-        sz = HHG_Z(1.0 / 20.0, 0) + (HHG_Z(1.0 / 4.0, 3) + HHG_Z(1.0 / 5.0, 4));
-    } else if constexpr (S == 6) {
-        s2 = padd(pfma(125.0 / 108.0, k2[3], pmul(-25.0 / 108.0, k2[0])),
-                  pfma(125.0 / 54.0, k2[5], pmul(-65.0 / 27.0, k2[4])));
-        sz = (HHG_Z(-25.0 / 108.0, 0) + HHG_Z(125.0 / 108.0, 3)) +
-             (HHG_Z(-65.0 / 27.0, 4) + HHG_Z(125.0 / 54.0, 5));
-    } else if constexpr (S == 7) {
-        s2 = padd(pfma(61.0 / 225.0, k2[4], pmul(31.0 / 300.0, k2[0])),
-                  pfma(13.0 / 900.0, k2[6], pmul(-2.0 / 9.0, k2[5])));
-        sz = (HHG_Z(31.0 / 300.0, 0) + HHG_Z(61.0 / 225.0, 4)) +
-             (HHG_Z(-2.0 / 9.0, 5) + HHG_Z(13.0 / 900.0, 6));
-    } else if constexpr (S == 8) {
-        s2 = padd(pfma(704.0 / 45.0, k2[4], pfma(-53.0 / 6.0, k2[3], pmul(2.0, k2[0]))),
-                  pfma(3.0, k2[7], pfma(67.0 / 90.0, k2[6], pmul(-107.0 / 9.0, k2[5]))));
-        sz = (HHG_Z(2.0, 0) + HHG_Z(-53.0 / 6.0, 3) + HHG_Z(704.0 / 45.0, 4)) +
-             (HHG_Z(-107.0 / 9.0, 5) + HHG_Z(67.0 / 90.0, 6) + HHG_Z(3.0, 7));
-    } else if constexpr (S == 9) {
-        s2 = padd(pfma(311.0 / 54.0, k2[5], pfma(-976.0 / 135.0, k2[4],
-                                               pfma(23.0 / 108.0, k2[3], pmul(-91.0 / 108.0, k2[0])))),
-                  pfma(-1.0 / 12.0, k2[8], pfma(17.0 / 6.0, k2[7], pmul(-19.0 / 60.0, k2[6]))));
-        sz = (HHG_Z(-91.0 / 108.0, 0) + HHG_Z(23.0 / 108.0, 3) + HHG_Z(-976.0 / 135.0, 4) +
-              HHG_Z(311.0 / 54.0, 5)) +
-             (HHG_Z(-19.0 / 60.0, 6) + HHG_Z(17.0 / 6.0, 7) + HHG_Z(-1.0 / 12.0, 8));
-    } else if constexpr (S == 10) {
-        s2 = padd(pfma(-301.0 / 82.0, k2[5], pfma(4496.0 / 1025.0, k2[4],
-                                                pfma(-341.0 / 164.0, k2[3], pmul(2383.0 / 4100.0, k2[0])))),
-                  pfma(18.0 / 41.0, k2[9], pfma(45.0 / 164.0, k2[8],
-                                              pfma(45.0 / 82.0, k2[7], pmul(2133.0 / 4100.0, k2[6])))));
-        sz = (HHG_Z(2383.0 / 4100.0, 0) + HHG_Z(-341.0 / 164.0, 3) + HHG_Z(4496.0 / 1025.0, 4) +
-              HHG_Z(-301.0 / 82.0, 5)) +
-             (HHG_Z(2133.0 / 4100.0, 6) + HHG_Z(45.0 / 82.0, 7) + HHG_Z(45.0 / 164.0, 8) +
-              HHG_Z(18.0 / 41.0, 9));
-    } else if constexpr (S == 11) {
-        s2 = padd(pfma(-3.0 / 205.0, k2[6], pfma(-6.0 / 41.0, k2[5], pmul(3.0 / 205.0, k2[0]))),
-                  pfma(6.0 / 41.0, k2[9], pfma(3.0 / 41.0, k2[8], pmul(-3.0 / 41.0, k2[7]))));
-        sz = (HHG_Z(3.0 / 205.0, 0) + HHG_Z(-6.0 / 41.0, 5) + HHG_Z(-3.0 / 205.0, 6)) +
-             (HHG_Z(-3.0 / 41.0, 7) + HHG_Z(3.0 / 41.0, 8) + HHG_Z(6.0 / 41.0, 9));
-    } else {
-        static_assert(S == 12, "stages 1 .. 12");
-        s2 = padd(pfma(-289.0 / 82.0, k2[5], pfma(4496.0 / 1025.0, k2[4],
-                                                pfma(-341.0 / 164.0, k2[3], pmul(-1777.0 / 4100.0, k2[0])))),
-                  padd(pfma(12.0 / 41.0, k2[9], pfma(33.0 / 164.0, k2[8],
-                                                   pfma(51.0 / 82.0, k2[7], pmul(2193.0 / 4100.0, k2[6])))),
-                       k2[11]));
-        sz = (HHG_Z(-1777.0 / 4100.0, 0) + HHG_Z(-341.0 / 164.0, 3) + HHG_Z(4496.0 / 1025.0, 4) +
-              HHG_Z(-289.0 / 82.0, 5)) +
-             (HHG_Z(2193.0 / 4100.0, 6) + HHG_Z(51.0 / 82.0, 7) + HHG_Z(33.0 / 164.0, 8) +
-              HHG_Z(12.0 / 41.0, 9) + kz[11]);
-    }
-}
-
-// The 8th-order solution, error estimate and first stage of a packed attempt
-// (state, increment and error in FP64).
-__device__ __forceinline__ void rk_finish_packed(const float2 *k2, const float *kz, const double *x,
-                                                 double h, double *xn, double *e, double *k0d) {
-    const float2 inc2 = pfma(41.0 / 840.0, padd(k2[11], k2[12]),
-                             pfma(9.0 / 280.0, padd(k2[8], k2[9]),
-                                  pfma(9.0 / 35.0, padd(k2[6], k2[7]), pmul(34.0 / 105.0, k2[5]))));
-    const float incz = HHG_Z(34.0 / 105.0, 5) + float(9.0 / 35.0) * (kz[6] + kz[7]) +
-                       float(9.0 / 280.0) * (kz[8] + kz[9]) + float(41.0 / 840.0) * (kz[11] + kz[12]);
-    const float2 de2 = pfma(-1.0, padd(k2[0], k2[10]), padd(k2[11], k2[12]));
-    const float dez = (kz[11] + kz[12]) - (kz[0] + kz[10]);
-    xn[0] = x[0] + h * double(inc2.x);
-    xn[1] = x[1] + h * double(inc2.y);
-    xn[2] = x[2] + h * double(incz);
-    const double eh = 41.0 / 840.0 * h;
-    e[0] = eh * double(de2.x);
-    e[1] = eh * double(de2.y);
-    e[2] = eh * double(dez);
-    k0d[0] = double(k2[0].x);
-    k0d[1] = double(k2[0].y);
-    k0d[2] = double(kz[0]);
-}
-#undef HHG_Z
-
 template <int M, int NF, class Eval>
 __device__ __forceinline__ void rkf78_attempt_packed(const ModelState<M, float> &ms, const Eval &ev,
                                                      double t, double h, const double *x,
@@ -1036,13 +941,10 @@ __device__ __forceinline__ void rkf78_attempt_packed(const ModelState<M, float> 
 #pragma unroll
         for (int n = 0; n < NF; ++n) f0[n] = f[n];
     }
-#define HHG_PSTAGE(s)                                                               \
+#define HHG_PSTAGE(s, SUM2, SUMZ)                                                   \
     {                                                                               \
-        float2 sum2;                                                                \
-        float sumz;                                                                 \
-        rk_stage_sum<s>(k2, kz, sum2, sumz);                                        \
-        const float2 xt2 = __ffma2_rn(h2, sum2, x2);                                \
-        const float xtz = xz + hr * sumz;                                           \
+        const float2 xt2 = __ffma2_rn(h2, (SUM2), x2);                              \
+        const float xtz = xz + hr * (SUMZ);                                         \
         if constexpr (Eval::kReuse && (s == 7 || s == 11 || s == 12)) {             \
             _Pragma("unroll") for (int n = 0; n < NF; ++n)                          \
                 f[n] = (s == 7) ? f3[n] : (s == 11) ? f0[n] : f10[n];               \
@@ -1056,69 +958,67 @@ __device__ __forceinline__ void rkf78_attempt_packed(const ModelState<M, float> 
         }                                                                           \
         rhs_packed(ms, f, xt2, xtz, x, k2[s], kz[s]);                               \
     }
-    HHG_PSTAGE(1) HHG_PSTAGE(2) HHG_PSTAGE(3) HHG_PSTAGE(4) HHG_PSTAGE(5) HHG_PSTAGE(6)
-    HHG_PSTAGE(7) HHG_PSTAGE(8) HHG_PSTAGE(9) HHG_PSTAGE(10) HHG_PSTAGE(11) HHG_PSTAGE(12)
+#define Z(c, j) (float(c) * kz[j])
+    HHG_PSTAGE(1, pmul(2.0 / 27.0, k2[0]), Z(2.0 / 27.0, 0))
+    HHG_PSTAGE(2, pfma(1.0 / 12.0, k2[1], pmul(1.0 / 36.0, k2[0])),
+               Z(1.0 / 36.0, 0) + Z(1.0 / 12.0, 1))
+    HHG_PSTAGE(3, pfma(1.0 / 8.0, k2[2], pmul(1.0 / 24.0, k2[0])),
+               Z(1.0 / 24.0, 0) + Z(1.0 / 8.0, 2))
+    HHG_PSTAGE(4, padd(pmul(5.0 / 12.0, k2[0]), pfma(25.0 / 16.0, k2[3], pmul(-25.0 / 16.0, k2[2]))),
+               Z(5.0 / 12.0, 0) + (Z(-25.0 / 16.0, 2) + Z(25.0 / 16.0, 3)))
+    HHG_PSTAGE(5, padd(pmul(1.0 / 20.0, k2[0]), pfma(1.0 / 5.0, k2[4], pmul(1.0 / 4.0, k2[3]))),
+               Z(1.0 / 20.0, 0) + (Z(1.0 / 4.0, 3) + Z(1.0 / 5.0, 4)))
+    HHG_PSTAGE(6, padd(pfma(125.0 / 108.0, k2[3], pmul(-25.0 / 108.0, k2[0])),
+                       pfma(125.0 / 54.0, k2[5], pmul(-65.0 / 27.0, k2[4]))),
+               (Z(-25.0 / 108.0, 0) + Z(125.0 / 108.0, 3)) + (Z(-65.0 / 27.0, 4) + Z(125.0 / 54.0, 5)))
+    HHG_PSTAGE(7, padd(pfma(61.0 / 225.0, k2[4], pmul(31.0 / 300.0, k2[0])),
+                       pfma(13.0 / 900.0, k2[6], pmul(-2.0 / 9.0, k2[5]))),
+               (Z(31.0 / 300.0, 0) + Z(61.0 / 225.0, 4)) + (Z(-2.0 / 9.0, 5) + Z(13.0 / 900.0, 6)))
+    HHG_PSTAGE(8, padd(pfma(704.0 / 45.0, k2[4], pfma(-53.0 / 6.0, k2[3], pmul(2.0, k2[0]))),
+                       pfma(3.0, k2[7], pfma(67.0 / 90.0, k2[6], pmul(-107.0 / 9.0, k2[5])))),
+               (Z(2.0, 0) + Z(-53.0 / 6.0, 3) + Z(704.0 / 45.0, 4)) +
+                   (Z(-107.0 / 9.0, 5) + Z(67.0 / 90.0, 6) + Z(3.0, 7)))
+    HHG_PSTAGE(9, padd(pfma(311.0 / 54.0, k2[5], pfma(-976.0 / 135.0, k2[4],
+                                                      pfma(23.0 / 108.0, k2[3], pmul(-91.0 / 108.0, k2[0])))),
+                       pfma(-1.0 / 12.0, k2[8], pfma(17.0 / 6.0, k2[7], pmul(-19.0 / 60.0, k2[6])))),
+               (Z(-91.0 / 108.0, 0) + Z(23.0 / 108.0, 3) + Z(-976.0 / 135.0, 4) + Z(311.0 / 54.0, 5)) +
+                   (Z(-19.0 / 60.0, 6) + Z(17.0 / 6.0, 7) + Z(-1.0 / 12.0, 8)))
+    HHG_PSTAGE(10, padd(pfma(-301.0 / 82.0, k2[5], pfma(4496.0 / 1025.0, k2[4],
+                                                        pfma(-341.0 / 164.0, k2[3], pmul(2383.0 / 4100.0, k2[0])))),
+                        pfma(18.0 / 41.0, k2[9], pfma(45.0 / 164.0, k2[8],
+                                                      pfma(45.0 / 82.0, k2[7], pmul(2133.0 / 4100.0, k2[6]))))),
+               (Z(2383.0 / 4100.0, 0) + Z(-341.0 / 164.0, 3) + Z(4496.0 / 1025.0, 4) + Z(-301.0 / 82.0, 5)) +
+                   (Z(2133.0 / 4100.0, 6) + Z(45.0 / 82.0, 7) + Z(45.0 / 164.0, 8) + Z(18.0 / 41.0, 9)))
+    HHG_PSTAGE(11, padd(pfma(-3.0 / 205.0, k2[6], pfma(-6.0 / 41.0, k2[5], pmul(3.0 / 205.0, k2[0]))),
+                        pfma(6.0 / 41.0, k2[9], pfma(3.0 / 41.0, k2[8], pmul(-3.0 / 41.0, k2[7])))),
+               (Z(3.0 / 205.0, 0) + Z(-6.0 / 41.0, 5) + Z(-3.0 / 205.0, 6)) +
+                   (Z(-3.0 / 41.0, 7) + Z(3.0 / 41.0, 8) + Z(6.0 / 41.0, 9)))
+    HHG_PSTAGE(12, padd(pfma(-289.0 / 82.0, k2[5], pfma(4496.0 / 1025.0, k2[4],
+                                                        pfma(-341.0 / 164.0, k2[3], pmul(-1777.0 / 4100.0, k2[0])))),
+                        padd(pfma(12.0 / 41.0, k2[9], pfma(33.0 / 164.0, k2[8],
+                                                           pfma(51.0 / 82.0, k2[7], pmul(2193.0 / 4100.0, k2[6])))),
+                             k2[11])),
+               (Z(-1777.0 / 4100.0, 0) + Z(-341.0 / 164.0, 3) + Z(4496.0 / 1025.0, 4) + Z(-289.0 / 82.0, 5)) +
+                   (Z(2193.0 / 4100.0, 6) + Z(51.0 / 82.0, 7) + Z(33.0 / 164.0, 8) + Z(12.0 / 41.0, 9) + kz[11]))
 #undef HHG_PSTAGE
-    rk_finish_packed(k2, kz, x, h, xn, e, k0d);
-}
-
-// Two trajectories of one warp lane (same pulse, step and staged values, two
-// k-points): one table or interpolant read per stage serves both right-hand
-// sides, and the two independent stage chains interleave in the
-// instruction stream.  The arithmetic of each is rkf78_attempt_packed's.
-template <int M, int NF, class Eval>
-__device__ __forceinline__ void rkf78_attempt_pair(const ModelState<M, float> *ms, const Eval &ev,
-                                                   double t, double h, const double (*x)[3],
-                                                   double (*xn)[3], double (*e)[3],
-                                                   double (*k0d)[3]) {
-    float2 k2[2][13];
-    float kz[2][13];
-    typename Num<float>::V f[NF];
-    float2 x2[2];
-    float xz[2];
-#pragma unroll
-    for (int j = 0; j < 2; ++j) {
-        x2[j] = make_float2(float(x[j][0]), float(x[j][1]));
-        xz[j] = float(x[j][2]);
-    }
-    const float hr = float(h);
-    const float2 h2 = make_float2(hr, hr);
-    ev(0, t, f);
-#pragma unroll
-    for (int j = 0; j < 2; ++j) rhs_packed(ms[j], f, x2[j], xz[j], x[j], k2[j][0], kz[j][0]);
-    typename Num<float>::V f0[Eval::kReuse ? NF : 1], f3[Eval::kReuse ? NF : 1],
-        f10[Eval::kReuse ? NF : 1];
-    if constexpr (Eval::kReuse) {
-#pragma unroll
-        for (int n = 0; n < NF; ++n) f0[n] = f[n];
-    }
-#define HHG_PSTAGE2(s)                                                              \
-    {                                                                               \
-        if constexpr (Eval::kReuse && (s == 7 || s == 11 || s == 12)) {             \
-            _Pragma("unroll") for (int n = 0; n < NF; ++n)                          \
-                f[n] = (s == 7) ? f3[n] : (s == 11) ? f0[n] : f10[n];               \
-        } else {                                                                    \
-            ev(s, t + rk_c(s) * h, f);                                              \
-        }                                                                           \
-        if constexpr (Eval::kReuse && (s == 3 || s == 10)) {                        \
-            _Pragma("unroll") for (int n = 0; n < NF; ++n) {                        \
-                if (s == 3) f3[n] = f[n]; else f10[n] = f[n];                       \
-            }                                                                       \
-        }                                                                           \
-        _Pragma("unroll") for (int j = 0; j < 2; ++j) {                             \
-            float2 sum2;                                                            \
-            float sumz;                                                             \
-            rk_stage_sum<s>(k2[j], kz[j], sum2, sumz);                              \
-            const float2 xt2 = __ffma2_rn(h2, sum2, x2[j]);                         \
-            const float xtz = xz[j] + hr * sumz;                                    \
-            rhs_packed(ms[j], f, xt2, xtz, x[j], k2[j][s], kz[j][s]);               \
-        }                                                                           \
-    }
-    HHG_PSTAGE2(1) HHG_PSTAGE2(2) HHG_PSTAGE2(3) HHG_PSTAGE2(4) HHG_PSTAGE2(5) HHG_PSTAGE2(6)
-    HHG_PSTAGE2(7) HHG_PSTAGE2(8) HHG_PSTAGE2(9) HHG_PSTAGE2(10) HHG_PSTAGE2(11) HHG_PSTAGE2(12)
-#undef HHG_PSTAGE2
-#pragma unroll
-    for (int j = 0; j < 2; ++j) rk_finish_packed(k2[j], kz[j], x[j], h, xn[j], e[j], k0d[j]);
+    const float2 inc2 = pfma(41.0 / 840.0, padd(k2[11], k2[12]),
+                             pfma(9.0 / 280.0, padd(k2[8], k2[9]),
+                                  pfma(9.0 / 35.0, padd(k2[6], k2[7]), pmul(34.0 / 105.0, k2[5]))));
+    const float incz = Z(34.0 / 105.0, 5) + float(9.0 / 35.0) * (kz[6] + kz[7]) +
+                       float(9.0 / 280.0) * (kz[8] + kz[9]) + float(41.0 / 840.0) * (kz[11] + kz[12]);
+#undef Z
+    const float2 de2 = pfma(-1.0, padd(k2[0], k2[10]), padd(k2[11], k2[12]));
+    const float dez = (kz[11] + kz[12]) - (kz[0] + kz[10]);
+    xn[0] = x[0] + h * double(inc2.x);
+    xn[1] = x[1] + h * double(inc2.y);
+    xn[2] = x[2] + h * double(incz);
+    const double eh = 41.0 / 840.0 * h;
+    e[0] = eh * double(de2.x);
+    e[1] = eh * double(de2.y);
+    e[2] = eh * double(dez);
+    k0d[0] = double(k2[0].x);
+    k0d[1] = double(k2[0].y);
+    k0d[2] = double(kz[0]);
 }
 
 // ---------------------------------------------------------------------------
@@ -1580,24 +1480,8 @@ constexpr double kCoarsen = 1.0 / 600.0;
 //   integrand of DiracSystem::compute_current_density,
 //   DiracSystem.cpp:300-311; dead trajectories give 0 and are counted).
 // OUT 1-3 are built for the PiFlux models only, OUT 4 for the Dirac-3D ones.
-// Kernel variants that integrate two trajectories per lane: the mixed-precision
-// warp-synchronous steppers of the models with a paired FP32 right-hand side.
-// Their work items are made of 64-row tiles (the host's tile width) and their
-// CTAs are sized for 4 per SM (255 registers: two trajectories' stage values).
-__host__ __device__ constexpr bool pair_lanes_variant(int model, int precision, int kernel_proposer,
-                                                      int stepper, int out) {
-    return precision == 1 && (kernel_proposer == 2 || kernel_proposer == 3) && stepper == 0 &&
-           out == 0 && (model == PIFLUX2D || model == HONEYCOMB_X);
-}
-__host__ __device__ constexpr int tile_rows(int model, int precision, int kernel_proposer, int stepper,
-                                            int out) {
-    return pair_lanes_variant(model, precision, kernel_proposer, stepper, out) ? 64 : 32;
-}
-constexpr int kPairMinBlocks = 4;
-
 template <int M, int D, typename R, int STEPPER, int PROPOSER, int OUT = 0>
-__global__ void __launch_bounds__(kBlockThreads, (pair_lanes_variant(M, sizeof(R) == sizeof(float) ? 1 : 0, PROPOSER, STEPPER, OUT) ? kPairMinBlocks : Traits<M>::kMinBlocks))
-bz_integrate_kernel(const KParams P) {
+__global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integrate_kernel(const KParams P) {
     constexpr int NF = Traits<M>::NF;
     constexpr bool kDyadic = PROPOSER == 2 || PROPOSER == 3;
     constexpr bool kLearned = PROPOSER == 3;
@@ -1609,8 +1493,6 @@ bz_integrate_kernel(const KParams P) {
     constexpr int DYA = slot_dyadic(NF, D);
     constexpr bool kNarrow = sizeof(R) != sizeof(double);
     constexpr bool kPair = pair_layout<M, R>();
-    // two trajectories per lane (64-row tiles): pair_lanes_variant
-    constexpr bool kPairLanes = pair_lanes_variant(M, kNarrow ? 1 : 0, PROPOSER, STEPPER, OUT);
     // only the reference schedule reads the standard table; the dyadic table
     // is read from global memory
     // the relaxation models on the reference schedule run free lanes (above)
@@ -1649,151 +1531,6 @@ bz_integrate_kernel(const KParams P) {
         const double *coef = P.coef + pd.coef_off;
 
         for (int sub = 0; sub < P.tiles_per_item; ++sub) {
-          if constexpr (kPairLanes) {
-            // two trajectories per lane: k rows q and q + 32 of a 64-row tile
-            const int qb = (tile * P.tiles_per_item + sub) * 64 + lane;
-            ModelState<M, R> ms2[2];
-            double S2[2][3], w2[2], kxy[2][2];
-            bool dead2[2];
-#pragma unroll
-            for (int j = 0; j < 2; ++j) {
-                const int q = qb + 32 * j;
-                const bool valid = q < P.n_k;
-                double row[8];
-#pragma unroll
-                for (int c = 0; c < 8; ++c) row[c] = valid ? __ldg(P.ktab + (size_t)q * 8 + c) : 0.0;
-                ms2[j].init(pd, row);
-                S2[j][0] = row[4];
-                S2[j][1] = row[5];
-                S2[j][2] = row[6];
-                w2[j] = valid ? row[3] : 0.0;
-                dead2[j] = !valid;
-                kxy[j][0] = row[0];
-                kxy[j][1] = row[1];
-            }
-            int level = 0;
-            bool easy = false;  // as in the one-trajectory loop below
-            double held = 0.0;
-            for (int i = 0; i <= N; ++i) {
-                const double *rec = pd.s0rec;
-                if (i > 0) {
-                    const double *gslot = coef + (size_t)(i - 1) * SLOT;
-                    __syncwarp();
-                    {
-                        const double2 *src = reinterpret_cast<const double2 *>(gslot);
-                        double2 *dst = reinterpret_cast<double2 *>(slot);
-                        for (int c = lane; c < COPY / 2; c += 32) dst[c] = __ldg(src + c);
-                    }
-                    __syncwarp();
-                    rec = slot + 4;
-                    const double t0 = slot[0], t1 = slot[1];
-                    const PolyEval<NF, D, R, kPair> poly{slot, tb, te};
-                    const V *dtab = reinterpret_cast<const V *>(gslot + DYA);
-                    const double span = t1 - t0;
-                    if constexpr (kLearned) {
-                        if (((i - 1) % P.mlp_every) == 0 && !easy) {
-                            int want = 0;
-#pragma unroll
-                            for (int j = 0; j < 2; ++j) {
-                                float f[kMlpIn];
-                                mlp_features(kxy[j], gslot[DYA - 2], gslot[DYA - 1], S2[j], -double(level), f);
-                                const float T = mlp_warp_infer_call(P.mlp, f, mlp_stage + wib * 32 * kLdIn);
-                                int wj = dead2[j] ? 0 : (int)ceilf(T + __ldg(&P.mlp->level_margin));
-                                wj = wj < 0 ? 0 : (wj > kLevelMax ? kLevelMax : wj);
-                                want = wj > want ? wj : want;
-                            }
-                            level = __reduce_max_sync(kFull, (unsigned)want);
-                        }
-                    }
-                    int L = level, qpos = 0;
-                    const bool from_floor = level == 0;
-                    bool fallback = false, coarse_end = false, refined = false;
-                    for (;;) {
-                        const double h = ldexp(span, -L);
-                        const double tq = t0 + qpos * h;
-                        bool ok2[2] = {true, true}, small = true;
-                        double xn[2][3];
-                        if (!(dead2[0] && dead2[1])) {
-                            double e[2][3], k0[2][3];
-                            if (L < kDyaLevels) {
-                                const TableEval<NF, R> tev{dtab + ((1 << L) - 1 + qpos) * 13 * NF};
-                                rkf78_attempt_pair<M, NF>(ms2, tev, tq, h, S2, xn, e, k0);
-                            } else {
-                                rkf78_attempt_pair<M, NF>(ms2, poly, tq, h, S2, xn, e, k0);
-                            }
-#pragma unroll
-                            for (int j = 0; j < 2; ++j) {
-                                if (dead2[j]) continue;
-                                ++my_attempts;
-#pragma unroll
-                                for (int c = 0; c < 3; ++c) {
-                                    const double den = P.abs_tol + P.rel_tol * (fabs(S2[j][c]) + h * fabs(k0[j][c]));
-                                    ok2[j] = ok2[j] && !(fabs(e[j][c]) > den);
-                                    small = small && (fabs(e[j][c]) < kCoarsen * den);
-                                }
-                            }
-                        }
-                        if (__all_sync(kFull, ok2[0] && ok2[1])) {
-#pragma unroll
-                            for (int j = 0; j < 2; ++j) {
-                                if (dead2[j]) continue;
-                                S2[j][0] = xn[j][0];
-                                S2[j][1] = xn[j][1];
-                                S2[j][2] = xn[j][2];
-                            }
-                            ++qpos;
-                            const bool coarse = __all_sync(kFull, small);
-                            if (qpos == (1 << L)) {
-                                coarse_end = coarse;
-                                break;
-                            }
-                            if (coarse && L > 0 && !(qpos & 1)) {
-                                --L;
-                                qpos >>= 1;
-                            }
-                        } else {
-#pragma unroll
-                            for (int j = 0; j < 2; ++j)
-                                if (!dead2[j] && !ok2[j]) ++my_rejects;
-                            if (L >= kLevelMax) {
-                                fallback = true;
-                                break;
-                            }
-                            refined = true;
-                            ++L;
-                            qpos <<= 1;
-                        }
-                    }
-                    if (fallback) {
-                        // the plain controller finishes the interval, one trajectory after the other
-                        const double h = ldexp(span, -L);
-                        double carry_unused = 0.0;
-#pragma unroll
-                        for (int j = 0; j < 2; ++j)
-                            lane_controller<M, NF, D, R, false, false>(
-                                P, ms2[j], poly, slot, tabv, 0, t0 + qpos * h, 0.5 * h, t1, S2[j],
-                                dead2[j], carry_unused, my_attempts, my_rejects);
-                    }
-                    level = (coarse_end && L > 0) ? L - 1 : (L > kLevelMax ? kLevelMax : L);
-                    easy = from_floor && !refined && !fallback;
-#pragma unroll
-                    for (int j = 0; j < 2; ++j) {
-                        if (!dead2[j] && !(isfinite(S2[j][0]) && isfinite(S2[j][1]) && isfinite(S2[j][2]))) {
-                            dead2[j] = true;
-                            atomicAdd(P.counters + 4, 1ull);
-                            atomicMax(P.status, 3);
-                        }
-                    }
-                }
-                // sample i: both trajectories' weighted vertices in one warp sum
-                double c = 0.0;
-#pragma unroll
-                for (int j = 0; j < 2; ++j)
-                    if (!dead2[j]) c += w2[j] * ms2[j].vertex(rec, S2[j]);
-                keep_sample(i, warp_sum(c), N, sub, lane, held, prow);
-            }
-            continue;
-          }
             const int q = (tile * P.tiles_per_item + sub) * 32 + lane;
             const bool valid = q < P.n_k;
             double row[8];

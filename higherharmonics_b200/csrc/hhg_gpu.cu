@@ -628,13 +628,6 @@ int kernel_proposer(int abi) {
     }
 }
 
-// k rows per tile of a plan's integration kernel: 64 for the variants with two
-// trajectories per lane, else 32 (one per lane).  Plans with an output mode or
-// history recording run FP64 and use 32.
-int plan_tile_rows(int model, const hhg_solver_opts &o) {
-    return hhg::tile_rows(model, o.precision, kernel_proposer(o.proposer), o.stepper, 0);
-}
-
 int model_nf(int m) {
     switch (hhg::base_model(m)) {
     case hhg::DIRAC2D: return 1;
@@ -1131,8 +1124,7 @@ static hhg_status plan_create_impl(hhg_ctx *ctx, const hhg_system_desc *sys,
     const int slot = dyadic ? hhg::slot_doubles_dyadic(nf, degree) : hhg::slot_doubles(nf, degree);
 
     // work decomposition
-    const int tr = plan_tile_rows(pl->model, o);
-    const int64_t tiles = (pl->n_k + tr - 1) / tr;
+    const int64_t tiles = (pl->n_k + 31) / 32;
     int tpi = o.tile_k > 0 ? o.tile_k : 1;
     if (o.tile_k <= 0) {
         // auto: keep at least ~8 items per resident warp when there is work
@@ -1887,8 +1879,7 @@ void drop_graph(hhg_plan *pl) {
 // device pulse table.
 hhg_status retile(hhg_plan *pl, int tpi, long long ctas) {
     hhg_ctx *ctx = pl->ctx;
-    const int tr = plan_tile_rows(pl->model, pl->opts);
-    const long long tiles = (pl->n_k + tr - 1) / tr;
+    const long long tiles = (pl->n_k + 31) / 32;
     tpi = (int)std::max(1LL, std::min<long long>(tpi, tiles));
     const int ipp = (int)((tiles + tpi - 1) / tpi);
     long long part_len = 0;
@@ -1970,8 +1961,7 @@ hhg_status hhg_plan_autotune(hhg_plan *pl, int reps, hhg_tune_report *report) {
     hhg_ctx *ctx = pl->ctx;
     HHG_CUDA(ctx, cudaSetDevice(ctx->device));
     reps = std::max(1, std::min(reps, 16));
-    const int tr = plan_tile_rows(pl->model, pl->opts);
-    const long long tiles = (pl->n_k + tr - 1) / tr;
+    const long long tiles = (pl->n_k + 31) / 32;
     const long long resident = (long long)pl->occupancy * ctx->sm_count;
     std::vector<std::pair<int, long long>> cand;
     for (int tpi : {1, 2, 4, 8, 16}) {
