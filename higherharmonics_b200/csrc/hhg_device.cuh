@@ -162,12 +162,16 @@ template <int NF> __host__ __device__ constexpr double outside_value(int n) {
 }
 
 // Paired FP32 layout of four staged functions v = (cos a, sin a, cos b, sin b)
-// of two projections a, b: (cos a, cos b, sin a, sin b), so the two cosines and
-// the two sines are adjacent and load as the operands of paired FP32
-// instructions.  Used by the models with Traits::kPairs in the
-// mixed-precision path (the staging table and the interpolants' output).
-__host__ __device__ __forceinline__ float pair_slot(const double *v, int n) {
-    return (float)v[n == 0 ? 0 : n == 1 ? 2 : n == 2 ? 1 : 3];
+// of two projections a, b, each as a float pair (hi, lo):
+//   slot 0 = (hi cos a, hi cos b), slot 1 = (lo cos a, lo cos b),
+//   slot 2 = (hi sin a, hi sin b), slot 3 = (lo sin a, lo sin b).
+// Used by the models with Traits::kPairs in the mixed-precision path (the
+// staging table's float-pair layout and the interpolants' output alike).
+__host__ __device__ __forceinline__ float2 pair_slot(const double *v, int n) {
+    const int a = (n < 2) ? 0 : 1, b = a + 2;
+    const float ha = (float)v[a], hb = (float)v[b];
+    return (n & 1) ? make_float2((float)(v[a] - (double)ha), (float)(v[b] - (double)hb))
+                   : make_float2(ha, hb);
 }
 
 // Fehlberg 7(8) nodes c_s (E. Fehlberg, NASA TR R-287, 1968).
@@ -321,15 +325,16 @@ namespace hhg {
 
 // ---------------------------------------------------------------------------
 // Number types.  The FP64 path works in double throughout.  The mixed path
-// (R = float) stages pulse values and k-dependent constants in FP32, so no
-// FP64 <-> FP32 conversion sits inside a right-hand side.  Compensated products
+// (R = float) stages pulse values and k-dependent constants as float pairs
+// (hi, lo) so that no FP64 <-> FP32 conversion sits inside a right-hand side,
+// and forms its products from the leading parts.  Compensated products
 // (hi hi + hi lo + lo hi, so that the rounding of the staged pulse values,
 // common to all k-points, never reaches a field term) were measured on the
 // honeycomb workload at 1024 x 1024 x 8 pulses: harmonic error 1.0e-6 against
 // the FP64 engine and 3.8e-5 against the FP64 oracle with them, 1.1e-6 and
 // 3.3e-5 without, at 1.32x the kernel time; the rounding of a staged value
 // varies from stage to stage, so its effect on j(t) is broadband and far
-// below the harmonic bar; the staged tables hold plain FP32 values.
+// below the harmonic bar.
 // ---------------------------------------------------------------------------
 template <typename R> struct Num;
 template <> struct Num<double> {
@@ -340,11 +345,18 @@ template <> struct Num<double> {
     static __device__ __forceinline__ double mul(V a, V f) { return a * f; }
 };
 template <> struct Num<float> {
-    using V = float;
-    static __device__ __forceinline__ V mk(double x) { return (float)x; }
-    static __device__ __forceinline__ float lin(V a, V b, V f) { return fmaf(-b, f, a); }
-    static __device__ __forceinline__ float dot2(V a, V b, V c, V d) { return fmaf(a, b, c * d); }
-    static __device__ __forceinline__ float mul(V a, V f) { return a * f; }
+    using V = float2;
+    static __device__ __forceinline__ V mk(double x) {
+        const float h = (float)x;
+        return make_float2(h, (float)(x - (double)h));
+    }
+    // FP32 products of the leading parts (the trailing parts are kept in the
+    // staged tables but not used: see the note on precision below)
+    static __device__ __forceinline__ float lin(V a, V b, V f) { return fmaf(-b.x, f.x, a.x); }
+    static __device__ __forceinline__ float dot2(V a, V b, V c, V d) {
+        return fmaf(a.x, b.x, c.x * d.x);
+    }
+    static __device__ __forceinline__ float mul(V a, V f) { return a.x * f.x; }
 };
 
 // ---------------------------------------------------------------------------
@@ -389,26 +401,20 @@ struct TableEval {
     static constexpr bool kReuse = false;  // a shared-memory reload is cheaper than registers
     const typename Num<R>::V *tab;  // 13 x NF values of one standard step (16-byte aligned)
     __device__ __forceinline__ void operator()(int s, double, typename Num<R>::V *f) const {
-        if constexpr (sizeof(R) == sizeof(float) && NF % 4 == 0) {
-            // FP32: four values per 16-byte load (rows of 16 bytes, aligned)
-            const float4 *t4 = reinterpret_cast<const float4 *>(tab + s * NF);
-#pragma unroll
-            for (int n = 0; n < NF / 4; ++n) {
-                const float4 w = t4[n];
-                f[4 * n] = w.x;
-                f[4 * n + 1] = w.y;
-                f[4 * n + 2] = w.z;
-                f[4 * n + 3] = w.w;
-            }
-        } else if constexpr (NF % 2 == 0) {
-            // two values per load (FP32 rows of 8 or 24 bytes; FP64 rows of 16 bytes)
-            using V2 = typename std::conditional<sizeof(R) == sizeof(float), float2, double2>::type;
+        if constexpr (NF % 2 == 0 && sizeof(typename Num<R>::V) == 8) {
+            // two values per 16-byte load (every table row starts on 16 bytes)
+            using V2 = typename std::conditional<sizeof(R) == sizeof(float), float4, double2>::type;
             const V2 *t2 = reinterpret_cast<const V2 *>(tab + s * NF);
 #pragma unroll
             for (int n = 0; n < NF / 2; ++n) {
                 const V2 w = t2[n];
-                f[2 * n] = w.x;
-                f[2 * n + 1] = w.y;
+                if constexpr (sizeof(R) == sizeof(float)) {
+                    f[2 * n] = make_float2(w.x, w.y);
+                    f[2 * n + 1] = make_float2(w.z, w.w);
+                } else {
+                    f[2 * n] = w.x;
+                    f[2 * n + 1] = w.y;
+                }
             }
         } else {
 #pragma unroll
@@ -507,8 +513,8 @@ template <typename R, bool SYM> struct PiFlux2DState {
         pcy = N::mk(pf * cy);
         psy = N::mk(pf * sy);
         if constexpr (sizeof(R) == sizeof(float)) {
-            pc_hi = make_float2(pcx, pcy);
-            ps_hi = make_float2(psx, psy);
+            pc_hi = make_float2(pcx.x, pcy.x);
+            ps_hi = make_float2(psx.x, psy.x);
         }
         px = p.mp[2];
         py = p.mp[3];
@@ -523,15 +529,14 @@ template <typename R, bool SYM> struct PiFlux2DState {
     // FP32 on packed pairs: (m0, m1) = Num<float>::dot2 of both projections in
     // one set of paired FMAs, then dS = (m1 Sz, -m0 Sz, m0 Sy - m1 Sx)
     // (the non-symmetric model's staged values arrive in the paired layout)
-    __device__ __forceinline__ void rhs2(const float *f, float2 s_xy, float s_z, float2 &d_xy,
+    __device__ __forceinline__ void rhs2(const float2 *f, float2 s_xy, float s_z, float2 &d_xy,
                                          float &d_z) const {
-        float2 bhi, dhi;  // the (cos, sin) values of both projections
+        float2 bhi, dhi;  // leading parts of the (cos, sin) values of both projections
         if constexpr (SYM) {
-            bhi = make_float2(f[0], f[0]);
-            dhi = make_float2(f[1], f[1]);
+            bhi = make_float2(f[0].x, f[0].x);
+            dhi = make_float2(f[1].x, f[1].x);
         } else {
-            bhi = make_float2(f[0], f[1]);
-            dhi = make_float2(f[2], f[3]);
+            bhi = f[0], dhi = f[2];
         }
         const float2 m = __ffma2_rn(pc_hi, bhi, __fmul2_rn(ps_hi, dhi));
         d_xy = __fmul2_rn(make_float2(m.y, -m.x), make_float2(s_z, s_z));
@@ -576,9 +581,9 @@ template <typename R, bool X> struct HoneycombState {
         if constexpr (X) {
             pc1 = N::mk(pf * (c1 + c2)), ps1 = N::mk(pf * (s1 + s2)), mc1 = N::mk(-pf * (c1 + c2));
             if constexpr (sizeof(R) == sizeof(float)) {
-                pc_hi = make_float2(pc0, pc1);
-                ps_hi = make_float2(ps0, ps1);
-                mc_hi = make_float2(mc0, mc1);
+                pc_hi = make_float2(pc0.x, pc1.x);
+                ps_hi = make_float2(ps0.x, ps1.x);
+                mc_hi = make_float2(mc0.x, mc1.x);
             }
         } else {
             pc1 = N::mk(pf * c1), ps1 = N::mk(pf * s1), mc1 = N::mk(-pf * c1);
@@ -610,12 +615,11 @@ template <typename R, bool X> struct HoneycombState {
     // FP32, field along x, staged values in the paired layout: the two bond
     // groups' products sit in the two halves of paired FMAs, summed at the
     // end: pf Re g' = PC.FC + PS.FS, pf Im g' = PS.FC - PC.FS.
-    __device__ __forceinline__ void rhs2(const float *f, float2 s_xy, float s_z, float2 &d_xy,
+    __device__ __forceinline__ void rhs2(const float2 *f, float2 s_xy, float s_z, float2 &d_xy,
                                          float &d_z) const {
         static_assert(X, "paired right-hand side: field along x");
-        const float2 fc = make_float2(f[0], f[1]), fs = make_float2(f[2], f[3]);
-        const float2 re = __ffma2_rn(pc_hi, fc, __fmul2_rn(ps_hi, fs));
-        const float2 im = __ffma2_rn(ps_hi, fc, __fmul2_rn(mc_hi, fs));
+        const float2 re = __ffma2_rn(pc_hi, f[0], __fmul2_rn(ps_hi, f[2]));
+        const float2 im = __ffma2_rn(ps_hi, f[0], __fmul2_rn(mc_hi, f[2]));
         const float gr = re.x + re.y, gi = im.x + im.y;
         const float dmf = float(dm);
         d_xy = make_float2(fmaf(-s_z, gi, -(dmf * s_xy.y)), fmaf(-s_z, gr, dmf * s_xy.x));
@@ -1949,11 +1953,11 @@ __global__ void stage_pulses_kernel(const PulseDev *__restrict__ pulses, int n_p
                         double *dst = out + DYA + ((((1 << L) - 1 + q) * 13 + s) * NF + n);
                         if constexpr (LAYOUT == 1) {
                             *dst = v[n];
+                        } else if constexpr (Traits<M>::kPairs) {
+                            *reinterpret_cast<float2 *>(dst) = pair_slot(v, n);
                         } else {
-                            // FP32 values, contiguous from the table's start
-                            float *dstf = reinterpret_cast<float *>(out + DYA) +
-                                          ((((1 << L) - 1 + q) * 13 + s) * NF + n);
-                            *dstf = Traits<M>::kPairs ? pair_slot(v, n) : (float)v[n];
+                            const float hi = (float)v[n];
+                            *reinterpret_cast<float2 *>(dst) = make_float2(hi, (float)(v[n] - (double)hi));
                         }
                     }
                 }
