@@ -326,15 +326,17 @@ namespace hhg {
 // ---------------------------------------------------------------------------
 // Number types.  The FP64 path works in double throughout.  The mixed path
 // (R = float) stages pulse values and k-dependent constants as float pairs
-// (hi, lo) so that no FP64 <-> FP32 conversion sits inside a right-hand side,
-// and forms its products from the leading parts.  Compensated products
-// (hi hi + hi lo + lo hi, so that the rounding of the staged pulse values,
-// common to all k-points, never reaches a field term) were measured on the
-// honeycomb workload at 1024 x 1024 x 8 pulses: harmonic error 1.0e-6 against
-// the FP64 engine and 3.8e-5 against the FP64 oracle with them, 1.1e-6 and
-// 3.3e-5 without, at 1.32x the kernel time; the rounding of a staged value
-// varies from stage to stage, so its effect on j(t) is broadband and far
-// below the harmonic bar.
+// (hi, lo), so no FP64 <-> FP32 conversion sits inside a right-hand side, and
+// by default forms compensated products (hi hi + hi lo + lo hi, one final
+// FP32 rounding per field term): the FP32 rounding of a staged pulse value is
+// common to all k-points and would act like a field error the
+// Brillouin-zone sum cannot average.  Measured with and without the
+// compensation (harmonic error against the FP64 engine, benchmark grids):
+// pi-flux 2D 256^2 5.2e-5 / 9.9e-5, gapped Dirac sweep 3.4e-7 / 1.8e-5,
+// honeycomb with the field along x 1.0e-6 / 1.1e-6 (1024^2 x 8 pulses; 3.8e-5
+// / 3.3e-5 against the FP64 oracle on a 384-row subsample).  The honeycomb
+// right-hand side with the field along x therefore uses the leading parts
+// only (1.32x faster); the others keep the compensation.
 // ---------------------------------------------------------------------------
 template <typename R> struct Num;
 template <> struct Num<double> {
@@ -350,13 +352,18 @@ template <> struct Num<float> {
         const float h = (float)x;
         return make_float2(h, (float)(x - (double)h));
     }
-    // FP32 products of the leading parts (the trailing parts are kept in the
-    // staged tables but not used: see the note on precision below)
-    static __device__ __forceinline__ float lin(V a, V b, V f) { return fmaf(-b.x, f.x, a.x); }
-    static __device__ __forceinline__ float dot2(V a, V b, V c, V d) {
-        return fmaf(a.x, b.x, c.x * d.x);
+    // compensated products: each field term gets one final FP32 rounding
+    static __device__ __forceinline__ float lin(V a, V b, V f) {
+        const float lo = a.y - b.x * f.y - b.y * f.x;
+        return fmaf(-b.x, f.x, a.x) + lo;
     }
-    static __device__ __forceinline__ float mul(V a, V f) { return a.x * f.x; }
+    static __device__ __forceinline__ float dot2(V a, V b, V c, V d) {
+        const float lo = a.x * b.y + a.y * b.x + c.x * d.y + c.y * d.x;
+        return fmaf(a.x, b.x, fmaf(c.x, d.x, lo));
+    }
+    static __device__ __forceinline__ float mul(V a, V f) {
+        return fmaf(a.x, f.x, a.x * f.y + a.y * f.x);
+    }
 };
 
 // ---------------------------------------------------------------------------
@@ -503,7 +510,7 @@ template <typename R, bool SYM> struct PiFlux2DState {
     static constexpr int Y = SYM ? 0 : 2;
     typename N::V pcx, psx, pcy, psy;
     double cx, sx, cy, sy, px, py;
-    float2 pc_hi, ps_hi;  // FP32: (x, y) pairs of the constants' leading parts
+    float2 pc_hi, pc_lo, ps_hi, ps_lo;  // FP32: (x, y) pairs of the float-pair constants
     __device__ __forceinline__ void init(const PulseDev &p, const double *row) {
         const double pf = p.mp[0];
         sincos(row[0], &sx, &cx);
@@ -514,7 +521,9 @@ template <typename R, bool SYM> struct PiFlux2DState {
         psy = N::mk(pf * sy);
         if constexpr (sizeof(R) == sizeof(float)) {
             pc_hi = make_float2(pcx.x, pcy.x);
+            pc_lo = make_float2(pcx.y, pcy.y);
             ps_hi = make_float2(psx.x, psy.x);
+            ps_lo = make_float2(psx.y, psy.y);
         }
         px = p.mp[2];
         py = p.mp[3];
@@ -531,14 +540,18 @@ template <typename R, bool SYM> struct PiFlux2DState {
     // (the non-symmetric model's staged values arrive in the paired layout)
     __device__ __forceinline__ void rhs2(const float2 *f, float2 s_xy, float s_z, float2 &d_xy,
                                          float &d_z) const {
-        float2 bhi, dhi;  // leading parts of the (cos, sin) values of both projections
+        float2 bhi, blo, dhi, dlo;
         if constexpr (SYM) {
-            bhi = make_float2(f[0].x, f[0].x);
-            dhi = make_float2(f[1].x, f[1].x);
+            bhi = make_float2(f[0].x, f[0].x), blo = make_float2(f[0].y, f[0].y);
+            dhi = make_float2(f[1].x, f[1].x), dlo = make_float2(f[1].y, f[1].y);
         } else {
-            bhi = f[0], dhi = f[2];
+            bhi = f[0], blo = f[1], dhi = f[2], dlo = f[3];
         }
-        const float2 m = __ffma2_rn(pc_hi, bhi, __fmul2_rn(ps_hi, dhi));
+        float2 lo = __fmul2_rn(pc_hi, blo);
+        lo = __ffma2_rn(pc_lo, bhi, lo);
+        lo = __ffma2_rn(ps_hi, dlo, lo);
+        lo = __ffma2_rn(ps_lo, dhi, lo);
+        const float2 m = __ffma2_rn(pc_hi, bhi, __ffma2_rn(ps_hi, dhi, lo));
         d_xy = __fmul2_rn(make_float2(m.y, -m.x), make_float2(s_z, s_z));
         d_z = fmaf(m.x, s_xy.y, -(m.y * s_xy.x));
     }
@@ -613,8 +626,9 @@ template <typename R, bool X> struct HoneycombState {
         dS[2] = S[0] * gi + S[1] * gr;
     }
     // FP32, field along x, staged values in the paired layout: the two bond
-    // groups' products sit in the two halves of paired FMAs, summed at the
-    // end: pf Re g' = PC.FC + PS.FS, pf Im g' = PS.FC - PC.FS.
+    // groups' products of the leading parts (no compensation: see Num) sit in
+    // the two halves of paired FMAs, summed at the end:
+    // pf Re g' = PC.FC + PS.FS, pf Im g' = PS.FC - PC.FS.
     __device__ __forceinline__ void rhs2(const float2 *f, float2 s_xy, float s_z, float2 &d_xy,
                                          float &d_z) const {
         static_assert(X, "paired right-hand side: field along x");
