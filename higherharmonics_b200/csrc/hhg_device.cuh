@@ -149,7 +149,7 @@ __host__ __device__ constexpr int slot_doubles(int nf, int deg) {
 // every step of size
 // (t1 - t0) / 2^L, L < kDyaLevels, level-major: for L, position q, stage s,
 // function n at index ((2^L - 1 + q) * 13 + s) * nf + n.  Mixed precision
-// stores FP32 values from the table's start.
+// stores float pairs in the same 8-byte slots.
 constexpr int kDyaLevels = 3;
 // [A(t0), E(t0)] then the table
 __host__ __device__ constexpr int slot_dyadic(int nf, int deg) { return slot_sched(nf, deg) + 2; }
@@ -1577,21 +1577,7 @@ __global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integ
                 integrate_free<M, D>(P, ms, coef, dt0, tb, te, N, w, dead, S, held, prow, sub, lane,
                                      free_ring[wib], my_attempts, my_rejects);
             } else {
-            // The learned proposer's network runs between intervals, outside the
-            // interval loop: the loop breaks (warp-uniformly) before an interval
-            // that asks for a proposal, the proposal is made here, and the loop
-            // resumes at that interval; no call sits inside the stepping loop.
-            int i = 0, proposed_at = -1;
-            for (;;) {
-            for (; i <= N; ++i) {
-                if constexpr (kLearned) {
-                    // a warp whose last interval took its one step at level 0 without
-                    // a rejection rests on the floor of one step per interval: a
-                    // proposal can only keep it there or refine before any lane has
-                    // asked for it, so the network is consulted where the warp is
-                    // above the floor or has just been refined
-                    if (i > 0 && i != proposed_at && ((i - 1) % P.mlp_every) == 0 && !easy) break;
-                }
+            for (int i = 0; i <= N; ++i) {
                 const double *rec = pd.s0rec;
                 if (i > 0) {
                     // stage interval i-1 into this warp's shared slot (the
@@ -1696,6 +1682,23 @@ __global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integ
                     } else {
                         const V *dtab = reinterpret_cast<const V *>(gslot + DYA);
                         const double span = t1 - t0;
+                        if constexpr (kLearned) {
+                            // A warp whose last interval took its one step at level 0
+                            // without a rejection rests on the floor of one step per
+                            // interval: a proposal can only keep it there or refine before
+                            // any lane has asked for it, so the network is consulted where
+                            // the warp is above the floor or has just been refined.
+                            if (((i - 1) % P.mlp_every) == 0 && !easy) {
+                                // the network proposes each lane's level; the warp takes the
+                                // finest one (dead lanes propose level 0)
+                                float f[kMlpIn];
+                                mlp_features(row, gslot[DYA - 2], gslot[DYA - 1], S, -double(level), f);
+                                const float T = mlp_warp_infer_call(P.mlp, f, mlp_stage + wib * 32 * kLdIn);
+                                int want = dead ? 0 : (int)ceilf(T + __ldg(&P.mlp->level_margin));
+                                want = want < 0 ? 0 : (want > kLevelMax ? kLevelMax : want);
+                                level = __reduce_max_sync(kFull, (unsigned)want);
+                            }
+                        }
                         int L = level, qpos = 0;
                         const bool from_floor = level == 0;
                         bool fallback = false, coarse_end = false, refined = false;
@@ -1817,20 +1820,6 @@ __global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integ
                         piflux_occupations(rec, kc[0], kc[1], kc[2], kc[3], S, o);
                     }
                 }
-            }
-            if (i > N) break;
-            if constexpr (kLearned) {
-                // the network proposes each lane's level for interval i; the warp
-                // takes the finest one (dead lanes propose level 0)
-                const double *gslot = coef + (size_t)(i - 1) * SLOT;
-                float f[kMlpIn];
-                mlp_features(row, gslot[DYA - 2], gslot[DYA - 1], S, -double(level), f);
-                const float T = mlp_warp_infer_call(P.mlp, f, mlp_stage + wib * 32 * kLdIn);
-                int want = dead ? 0 : (int)ceilf(T + __ldg(&P.mlp->level_margin));
-                want = want < 0 ? 0 : (want > kLevelMax ? kLevelMax : want);
-                level = __reduce_max_sync(kFull, (unsigned)want);
-                proposed_at = i;
-            }
             }
             }  // interval-synchronous loop
         }
