@@ -61,12 +61,19 @@ void set_msg(char *buf, size_t cap, const char *msg) {
 // Device address of the scratch array on the current device.  In host code
 // the name g_noalloc_scratch is only a host-side stand-in, so the address is
 // looked up once per device (with that device current) and cached.
-hhg_status scratch_for_device(int dev, unsigned char **out, char *err, size_t cap) {
+// Under stream capture only a cached address is used: the first lookup may
+// load the module, which a capture must not see.
+hhg_status scratch_for_device(int dev, unsigned char **out, char *err, size_t cap,
+                              bool capturing = false) {
     if (dev < 0 || dev >= kMaxDevices) {
         set_msg(err, cap, "device ordinal out of range for the scratch table");
         return HHG_BAD_CONFIG;
     }
     std::lock_guard<std::mutex> lock(g_setup_mutex);
+    if (!g_scratch_ptr[dev] && capturing) {
+        set_msg(err, cap, "the first allocation-free call on a device must come before any stream capture");
+        return HHG_UNSUPPORTED;
+    }
     if (!g_scratch_ptr[dev]) {
         void *p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
@@ -78,6 +85,17 @@ hhg_status scratch_for_device(int dev, unsigned char **out, char *err, size_t ca
     }
     *out = static_cast<unsigned char *>(g_scratch_ptr[dev]);
     return HHG_OK;
+}
+
+// Whether `s` is being captured into a graph (an error querying it counts as
+// capturing: the caller then takes the capture-safe path or refuses).
+bool stream_capturing(cudaStream_t s) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return true;
+    }
+    return cs != cudaStreamCaptureStatusNone;
 }
 
 cudaError_t launch_model(int model, const hhg::LaunchReq &r) {
@@ -258,9 +276,15 @@ extern "C" hhg_status hhg_gpu_current_density_noalloc(const hhg_system_desc *sys
         set_msg(err, err_cap, "no current CUDA device");
         return HHG_CUDA_ERROR;
     }
-    unsigned char *base = nullptr;
-    if ((st = scratch_for_device(dev, &base, err, err_cap)) != HHG_OK) return st;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const bool capturing = stream_capturing(s);
+    if (capturing && stats) {
+        set_msg(err, err_cap, "stats != NULL synchronises the stream: pass NULL under stream capture "
+                              "and read the outcome with hhg_noalloc_status after the replay");
+        return HHG_UNSUPPORTED;
+    }
+    unsigned char *base = nullptr;
+    if ((st = scratch_for_device(dev, &base, err, err_cap, capturing)) != HHG_OK) return st;
 
     hhg::PulseDev pd = prep.pulse;
     pd.coef_off = 0;
@@ -334,6 +358,10 @@ extern "C" hhg_status hhg_noalloc_status(void *stream, hhg_stats *stats, char *e
     if (cudaGetDevice(&dev) != cudaSuccess) {
         set_msg(err, err_cap, "no current CUDA device");
         return HHG_CUDA_ERROR;
+    }
+    if (stream_capturing(static_cast<cudaStream_t>(stream))) {
+        set_msg(err, err_cap, "hhg_noalloc_status synchronises the stream: not under stream capture");
+        return HHG_UNSUPPORTED;
     }
     unsigned char *base = nullptr;
     const hhg_status st = scratch_for_device(dev, &base, err, err_cap);

@@ -423,8 +423,11 @@ hhg_status hhg_measure_fp32_peak(hhg_ctx *ctx, double *tflops);
  * hhg_noalloc_status reports those conditions once the caller wants them.
  * The first call on a device looks up the scratch array's device address
  * (once per device, cached; the cache assumes the device's primary context
- * and no cudaDeviceReset for the life of the process); make that first call
- * before any stream capture.  All calls share the one array, which keeps the
+ * and no cudaDeviceReset for the life of the process); that first call must
+ * come before any stream capture (HHG_UNSUPPORTED otherwise).  Later calls
+ * may be captured into a CUDA graph with stats == NULL (they enqueue kernels
+ * whose arguments are passed by value); with stats != NULL a capturing
+ * stream is refused with HHG_UNSUPPORTED.  All calls share the one array, which keeps the
  * last call's contents: calls that overlap on the GPU race and must be
  * serialised by the caller.  Magnus-4 takes 1 to 4096 substeps, as in the
  * other entry points.  err (optional, err_cap bytes) receives a message on
@@ -439,8 +442,9 @@ hhg_status hhg_gpu_current_density_noalloc(const hhg_system_desc *sys,
  * `stream` (the stream that call ran on), reads the counters and the status
  * word the call left in the shared scratch array, fills stats (optional) and
  * returns HHG_OK, HHG_STEP_LIMIT or HHG_NONFINITE as the call would have.
- * Another call on the device after it overwrites what this reads.  Allocates
- * nothing; no counterpart in the reference. */
+ * Another call on the device after it overwrites what this reads.  Not under
+ * stream capture (HHG_UNSUPPORTED).  Allocates nothing; no counterpart in the
+ * reference. */
 hhg_status hhg_noalloc_status(void *stream, hhg_stats *stats, char *err, size_t err_cap);
 
 /* Learned step-size proposer: collection, training and inference.  None has

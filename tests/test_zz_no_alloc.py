@@ -12,7 +12,8 @@ whatever the first left in the shared scratch array -- within the parity
 tolerance of the GPU tests (relative L2 <= 1e-9), for the restart and carry
 proposers, the mixed-precision right-hand side and Magnus-4; an asynchronous
 call (stats == NULL) whose outcome is read afterwards with hhg_noalloc_status,
-including a step-limit status.  This file is collected last so a failure here
+including a step-limit status; the asynchronous call captured into a CUDA graph
+and replayed.  This file is collected last so a failure here
 does not stop the rest of the GPU suite.
 """
 import ctypes
@@ -28,20 +29,20 @@ pytestmark = pytest.mark.gpu
 J_TOL = 1e-9
 
 
-def _noalloc(lib, sys, pulse, d_rows, n_rows, opts, d_j, stats=True):
+def _noalloc(lib, sys, pulse, d_rows, n_rows, opts, d_j, stats=True, stream=None):
     err = ctypes.create_string_buffer(512)
     st = api.Stats()
     rc = lib.hhg_gpu_current_density_noalloc(ctypes.byref(sys), ctypes.byref(pulse),
                                              ctypes.c_void_p(d_rows), n_rows, ctypes.byref(opts),
-                                             ctypes.c_void_p(d_j), None,
+                                             ctypes.c_void_p(d_j), ctypes.c_void_p(stream),
                                              ctypes.byref(st) if stats else None, err, len(err))
     return rc, st, err.value.decode()
 
 
-def _status(lib):
+def _status(lib, stream=None):
     err = ctypes.create_string_buffer(512)
     st = api.Stats()
-    rc = lib.hhg_noalloc_status(None, ctypes.byref(st), err, len(err))
+    rc = lib.hhg_noalloc_status(ctypes.c_void_p(stream), ctypes.byref(st), err, len(err))
     return rc, st, err.value.decode()
 
 
@@ -137,6 +138,47 @@ def test_noalloc_async_call_and_status_query():
             assert st.failed_trajectories == 0
             assert st.k_points == rows.shape[0]
             assert np.array_equal(d_j.cpu().numpy(), j_sync)
+
+
+def test_noalloc_call_captured_into_a_cuda_graph():
+    """After a first call outside any capture, an asynchronous call (stats ==
+    NULL) can be captured into a CUDA graph: every replay reproduces the
+    direct call's j bit for bit and leaves its outcome for hhg_noalloc_status.
+    Under capture, a call with stats != NULL and the status query are refused
+    with HHG_UNSUPPORTED without breaking the capture."""
+    import torch
+    torch.cuda.set_device(0)
+    lib = api.load_library()
+    sys, pulse, grid = _case("honeycomb")
+    rows = api.grid_rows(sys, grid)
+    d_rows = torch.from_numpy(rows).cuda()
+    d_j = torch.empty(pulse.n_measurements + 1, dtype=torch.float64, device="cuda")
+    opts = api.solver(1e-12, 1e-8, proposer=api.PROPOSER_CARRY)
+    rc, st_sync, msg = _noalloc(lib, sys, pulse, d_rows.data_ptr(), rows.shape[0], opts,
+                                d_j.data_ptr())
+    assert rc == api.OK, msg
+    j_sync = d_j.cpu().numpy()
+    stream = torch.cuda.Stream()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=stream):
+        sp = stream.cuda_stream
+        rc_cap, _, msg_cap = _noalloc(lib, sys, pulse, d_rows.data_ptr(), rows.shape[0], opts,
+                                      d_j.data_ptr(), stats=False, stream=sp)
+        rc_sync, _, msg_sync = _noalloc(lib, sys, pulse, d_rows.data_ptr(), rows.shape[0], opts,
+                                        d_j.data_ptr(), stats=True, stream=sp)
+        rc_stat, _, msg_stat = _status(lib, sp)
+    assert rc_cap == api.OK, msg_cap
+    assert rc_sync == api.UNSUPPORTED and "capture" in msg_sync, (rc_sync, msg_sync)
+    assert rc_stat == api.UNSUPPORTED and "capture" in msg_stat, (rc_stat, msg_stat)
+    for _ in range(2):
+        d_j.fill_(float("nan"))
+        torch.cuda.synchronize()
+        graph.replay()
+        rc, st, msg = _status(lib, stream.cuda_stream)
+        assert rc == api.OK, msg
+        assert st.attempted_steps == st_sync.attempted_steps
+        assert np.array_equal(d_j.cpu().numpy(), j_sync)
+    del graph
 
 
 def test_noalloc_rejects_oversized_problem_and_bad_options():
