@@ -173,7 +173,8 @@ def test_noalloc_call_captured_into_a_cuda_graph():
     for _ in range(2):
         d_j.fill_(float("nan"))
         torch.cuda.synchronize()
-        graph.replay()
+        with torch.cuda.stream(stream):
+            graph.replay()
         rc, st, msg = _status(lib, stream.cuda_stream)
         assert rc == api.OK, msg
         assert st.attempted_steps == st_sync.attempted_steps
