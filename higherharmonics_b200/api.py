@@ -108,7 +108,7 @@ class SolverOpts(ctypes.Structure):
                 ("max_failed_steps", ctypes.c_int32), ("max_attempts_per_interval", ctypes.c_int32),
                 ("tile_k", ctypes.c_int32), ("block_threads", ctypes.c_int32),
                 ("mlp", ctypes.POINTER(Mlp)), ("mlp_every", ctypes.c_int32),
-                ("reserved", ctypes.c_int32)]
+                ("coarsen_div", ctypes.c_int32)]
 
 
 class TrainOpts(ctypes.Structure):
@@ -391,7 +391,7 @@ def grid_explicit(rows: np.ndarray) -> tuple[GridDesc, np.ndarray]:
 
 def solver(abs_tol=1e-12, rel_tol=1e-8, stepper=STEPPER_RKF78, precision=PREC_FP64,
            proposer=PROPOSER_NONE, magnus_substeps=1, tile_k=0, mlp: "Mlp | None" = None,
-           mlp_every=16) -> SolverOpts:
+           mlp_every=16, coarsen_div=0) -> SolverOpts:
     o = SolverOpts()
     load_library().hhg_default_solver_opts(ctypes.byref(o))
     o.abs_tol, o.rel_tol = abs_tol, rel_tol
@@ -401,6 +401,7 @@ def solver(abs_tol=1e-12, rel_tol=1e-8, stepper=STEPPER_RKF78, precision=PREC_FP
         o.mlp = ctypes.pointer(mlp)
         o._mlp_ref = mlp  # keep the network alive as long as the options
     o.mlp_every = mlp_every
+    o.coarsen_div = coarsen_div
     return o
 
 

@@ -608,6 +608,7 @@ std::string plan_key(const hhg_system_desc *sys, const hhg_pulse_desc *pulses, i
         put(&opts->abs_tol, 8 * 2);
         put(&opts->max_failed_steps, 4 * 4);
         put(&opts->mlp_every, 4);
+        put(&opts->coarsen_div, 4);
         const bool learned = opts->proposer == HHG_PROPOSER_LEARNED && opts->mlp;
         put(&learned, 1);
         if (learned) put(opts->mlp, sizeof(hhg_mlp));
@@ -918,6 +919,7 @@ void hhg_default_solver_opts(hhg_solver_opts *o) {
     o->block_threads = 128;
     o->mlp = nullptr;
     o->mlp_every = 16;
+    o->coarsen_div = 0;
 }
 
 hhg_status hhg_gpu_create(hhg_ctx **out, int device) {
@@ -1023,6 +1025,8 @@ static hhg_status plan_create_impl(hhg_ctx *ctx, const hhg_system_desc *sys,
     }
     if (!(o.abs_tol >= 0.0) || !(o.rel_tol >= 0.0) || !(o.abs_tol + o.rel_tol > 0.0))
         return set_err(ctx, HHG_BAD_CONFIG, "tolerances must be >= 0 and not both 0");
+    if (o.coarsen_div != 0 && (o.coarsen_div < 2 || o.coarsen_div > 65536))
+        return set_err(ctx, HHG_BAD_CONFIG, "coarsen_div must be 0 (default) or in 2 .. 65536");
     if (o.max_failed_steps < 1) o.max_failed_steps = 500;
     if (o.max_attempts_per_interval < 1) o.max_attempts_per_interval = 100000;
     if ((st = check_relax(ctx, *sys, pulses, n_pulses, o)) != HHG_OK) return st;
@@ -1377,6 +1381,9 @@ hhg_status enqueue_integration(hhg_plan *pl, cudaStream_t s, bool events) {
     lr.kp.grow_max = 9.0 / 10.0 * pow(pow(5.0, -8.0), -1.0 / 8);
     lr.kp.mlp = pl->d_mlp;
     lr.kp.mlp_every = std::max(pl->opts.mlp_every, 1);
+    lr.kp.coarsen = 1.0 / (pl->opts.coarsen_div > 0 ? pl->opts.coarsen_div
+                           : pl->opts.precision == HHG_PREC_MIXED ? hhg::kCoarsenDivMixed
+                                                                  : hhg::kCoarsenDivFp64);
     lr.kp.hist_every = pl->hist_every;
     lr.kp.hist = pl->d_hist;
     lr.kp.hist_count = pl->d_hist_count;

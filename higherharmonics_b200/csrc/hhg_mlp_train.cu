@@ -825,7 +825,7 @@ hhg_status hhg_mlp_init(uint64_t seed, const float *records, int64_t n, hhg_mlp 
     }
     net->out_mu = 0.0f;
     net->out_sigma = 1.0f;
-    net->level_margin = 0.25f;
+    net->level_margin = -0.5f;
     if (records && n > 1) {
         double sum[kIn + 1] = {}, sq[kIn + 1] = {};
         for (int64_t r = 0; r < n; ++r)

@@ -330,6 +330,7 @@ extern "C" hhg_status hhg_gpu_current_density_noalloc(const hhg_system_desc *sys
     lr.kp.rel_tol = o.rel_tol;
     lr.kp.err_floor = pow(5.0, -8.0);
     lr.kp.grow_max = grow_max;
+    lr.kp.coarsen = 1.0 / hhg::kCoarsenDivFp64;  // dyadic stepping only; not offered here
     lr.degree = prep.degree;
     lr.precision = o.precision;
     lr.stepper = o.stepper;

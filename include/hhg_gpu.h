@@ -204,7 +204,12 @@ typedef struct hhg_solver_opts {
     int32_t block_threads;
     const struct hhg_mlp *mlp; /* HHG_PROPOSER_LEARNED: the trained network (host memory) */
     int32_t mlp_every;         /* intervals between network proposals (>= 1, default 16) */
-    int32_t reserved;
+    int32_t coarsen_div;       /* lockstep / learned proposers: after an accepted step the warp
+                                  halves its level when every lane's error norm is below
+                                  1 / coarsen_div; 0 = the default: 600 in FP64 (the
+                                  controller's growth rule, 0.9 err^(-1/8) >= 2), 64 in mixed
+                                  precision (the FP32 right-hand side's rounding floor in the
+                                  error estimate); 2 .. 65536 */
 } hhg_solver_opts;
 
 /* The learned step-size proposer (no counterpart in the reference, whose
@@ -466,7 +471,10 @@ void hhg_default_train_opts(hhg_train_opts *opts);
 /* Deterministic initial weights (uniform +-1/sqrt(fan_in), from `seed`) and,
  * when records != NULL, the input / output standardisation fitted to them
  * (mean and 1 / standard deviation per input; mean and standard deviation of
- * T).  level_margin is set to 0.25. */
+ * T).  level_margin is set to -0.5: a warp takes the largest of 32 lanes'
+ * proposals, and the maximum of 32 noisy predictions sits above the largest
+ * true level; at -0.5 the learned proposer takes the carried-level
+ * heuristic's steps (at +0.25 it over-refined, 1.2-1.5x more steps). */
 hhg_status hhg_mlp_init(uint64_t seed, const float *records, int64_t n_records, hhg_mlp *net);
 /* Adam on the mean squared error of the standardised level, on the GPU: the
  * forward and backward GEMMs run on the tensor cores (tcgen05, BF16 inputs,

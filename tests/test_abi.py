@@ -44,7 +44,7 @@ def _c_layout():
                "hhg_solver_opts": ["stepper", "precision", "proposer", "magnus_substeps",
                                    "abs_tol", "rel_tol", "max_failed_steps",
                                    "max_attempts_per_interval", "tile_k", "block_threads",
-                                   "mlp", "mlp_every", "reserved"],
+                                   "mlp", "mlp_every", "coarsen_div"],
                "hhg_mlp": ["params", "in_mu", "in_isig", "out_mu", "out_sigma", "level_margin",
                            "reserved"],
                "hhg_train_opts": ["epochs", "batch", "lr", "beta1", "beta2", "eps", "lr_final",

@@ -79,7 +79,7 @@ def test_mlp_init_is_deterministic_and_fits_standardisation():
     assert np.allclose(np.array(a.in_isig), 1 / x.std(0), rtol=1e-4)
     assert np.isclose(a.out_mu, rec[:, 8].astype(np.float64).mean(), rtol=1e-5)
     assert np.isclose(a.out_sigma, rec[:, 8].astype(np.float64).std(), rtol=1e-4)
-    assert a.level_margin == pytest.approx(0.25)
+    assert a.level_margin == pytest.approx(-0.5)
     # a constant input keeps isig = 1
     rec2 = rec.copy()
     rec2[:, 1] = 0.5
