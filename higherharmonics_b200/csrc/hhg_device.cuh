@@ -1298,7 +1298,8 @@ __device__ __forceinline__ void lane_controller(const KParams &P, const ModelSta
                 const unsigned long long at = atomicAdd(P.hist_count, 1ull);
                 if ((long long)at < P.hist_cap) {
                     float f[kMlpIn];
-                    mlp_features(row, laser_exact(*pd, t), laser_field(*pd, t), S, log2(dt_used / span), f);
+                    mlp_features(mlp_k_features(row), laser_exact(*pd, t), laser_field(*pd, t), S,
+                                 log2(dt_used / span), f);
                     float *o = P.hist + (size_t)at * kHistFields;
 #pragma unroll
                     for (int c = 0; c < kMlpIn; ++c) o[c] = f[c];
@@ -1555,6 +1556,8 @@ __global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integ
             const double w = valid ? row[3] : 0.0;
             bool dead = !valid;
             double carry_dt = dt0;
+            // learned proposer: the k features (kx/pi, ky/pi), kept instead of the row
+            const float2 kfeat = kLearned ? mlp_k_features(row) : make_float2(0.f, 0.f);
             int level = 0;      // warp-uniform dyadic level carried across intervals
             // the last interval took one step at level 0 without a rejection
             // (learned proposer: the warp rests on the one-step floor)
@@ -1700,12 +1703,12 @@ __global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integ
                             // interval: a proposal can only keep it there or refine before
                             // any lane has asked for it, so the network is consulted where
                             // the warp is above the floor or has just been refined.
-                            if (((i - 1) % P.mlp_every) == 0 && !easy) {
+                            if (!easy && ((i - 1) % P.mlp_every) == 0) {
                                 // the network proposes each lane's level; the warp takes the
                                 // finest one (dead lanes propose level 0)
                                 float f[kMlpIn];
-                                mlp_features(row, gslot[DYA - 2], gslot[DYA - 1], S, -double(level), f);
-                                const float T = mlp_warp_infer_call(P.mlp, f, mlp_stage + wib * 32 * kLdIn);
+                                mlp_features(kfeat, gslot[DYA - 2], gslot[DYA - 1], S, -double(level), f);
+                                const float T = mlp_warp_infer(P.mlp, f, mlp_stage + wib * kMlpWarpStage);
                                 int want = dead ? 0 : (int)ceilf(T + __ldg(&P.mlp->level_margin));
                                 want = want < 0 ? 0 : (want > kLevelMax ? kLevelMax : want);
                                 level = __reduce_max_sync(kFull, (unsigned)want);

@@ -57,11 +57,15 @@ __device__ __forceinline__ double laser_field(const PulseDev &p, double t) {
     return -p.amplitude * (denv * sc + env * cc);
 }
 
-__device__ __forceinline__ void mlp_features(const double *row, double A, double E, const double *S,
-                                             double log2_hrel, float *f) {
+__device__ __forceinline__ float2 mlp_k_features(const double *row) {
     const double ipi = 0.31830988618379067154;
-    f[0] = float(row[0] * ipi);
-    f[1] = float(row[1] * ipi);
+    return make_float2(float(row[0] * ipi), float(row[1] * ipi));
+}
+
+__device__ __forceinline__ void mlp_features(float2 kf, double A, double E, const double *S,
+                                             double log2_hrel, float *f) {
+    f[0] = kf.x;
+    f[1] = kf.y;
     f[2] = float(A);
     f[3] = float(E);
     f[4] = float(S[0]);
@@ -71,13 +75,16 @@ __device__ __forceinline__ void mlp_features(const double *row, double A, double
 }
 
 // Warp-level inference reads the packed network from global memory (it is
-// 18 KB and shared by every warp, so it stays in L1/L2); only the per-warp
-// feature tile needs shared memory: 32 rows of kLdIn bf16 (16 features
-// padded to 24 so the A-fragment loads of the eight row groups hit distinct
-// banks).  A shared-memory copy per CTA would take ~23 KB from every
-// 2-warp CTA's share of L1 for the whole run, while the network is
-// consulted on a small fraction of the intervals.
-constexpr int kLdIn = 24;
+// 18 KB and shared by every warp, so it stays in L1/L2; a shared-memory copy
+// per CTA would take ~23 KB from every 2-warp CTA's share of L1 for the whole
+// run, while the network is consulted on a small fraction of the
+// intervals).  The warp's activations live in a per-warp shared-memory tile
+// of 32 rows x kLdH bf16: the features in columns 0..15 (8 inputs, zero
+// padded), each layer's output over its input.  The row stride of 72
+// elements (36 words) puts the eight row groups of an A-fragment load on
+// distinct banks.
+constexpr int kLdH = 72;
+constexpr int kMlpWarpStage = 32 * kLdH;  // bf16 elements per warp
 
 __device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
     const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
@@ -112,93 +119,102 @@ __device__ __forceinline__ uint32_t ldg_b32(const __nv_bfloat16 *p) {
     return __ldg(reinterpret_cast<const unsigned int *>(p));
 }
 
-// One hidden layer for one 16-row m-tile: acc[nt][4] = A W^T + b over eight
-// n8 tiles, SiLU, repacked in place as the next layer's A fragments
-// out[kc][4] (the m16n8 accumulators of two adjacent n-tiles form the
-// m16n8k16 A operand).  W is [64][LD] bf16 in global memory; lane (g, tig)
-// loads its B fragment W[8 nt + g][16 kc + 2 tig] and [... + 8] as 32-bit
-// words.
+// A fragment (16 x 16 bf16, row-major) of m-tile mt, k-chunk kc from the
+// warp's activation tile H: lane (g, tig) holds rows g and g + 8, columns
+// 16 kc + 2 tig (+1) and the same + 8.
+__device__ __forceinline__ void mlp_load_a(const __nv_bfloat16 *H, int mt, int kc, int g, int tig,
+                                           uint32_t (&a)[4]) {
+    const __nv_bfloat16 *r0 = H + (16 * mt + g) * kLdH + 16 * kc + 2 * tig;
+    const __nv_bfloat16 *r1 = r0 + 8 * kLdH;
+    a[0] = *reinterpret_cast<const uint32_t *>(r0);
+    a[1] = *reinterpret_cast<const uint32_t *>(r1);
+    a[2] = *reinterpret_cast<const uint32_t *>(r0 + 8);
+    a[3] = *reinterpret_cast<const uint32_t *>(r1 + 8);
+}
+
+// One hidden layer over both 16-row m-tiles, in place on H: the layer's
+// input (KC k-chunks) is read into registers first, then every n8 tile of
+// the 64 outputs is accumulated from bias + A W^T (FP32), passed through
+// SiLU and stored back as bf16 pairs (C-fragment rows g and g + 8, columns
+// 8 nt + 2 tig, +1; exactly the next layer's A-fragment positions).  The
+// n-tile loop is not unrolled, so at most 2 x 4 accumulators and one B
+// fragment are live beside the input: the inference runs inside the
+// stepping loop without displacing its registers.  W is [64][LD] bf16 in
+// global memory; lane (g, tig) loads W[8 nt + g][16 kc + 2 tig] and
+// [... + 8] as 32-bit words.
 template <int KC, int LD>
-__device__ __forceinline__ void mlp_hidden(const uint32_t (&a)[KC][4], const __nv_bfloat16 *w,
-                                           const float *b, uint32_t (&out)[4][4], int g, int tig) {
-    float acc[8][4];
+__device__ __forceinline__ void mlp_layer(__nv_bfloat16 *H, const __nv_bfloat16 *w, const float *b,
+                                          int g, int tig) {
+    uint32_t a[2][KC][4];
 #pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+        for (int kc = 0; kc < KC; ++kc) mlp_load_a(H, mt, kc, g, tig, a[mt][kc]);
+    __syncwarp();
+#pragma unroll 1
     for (int nt = 0; nt < 8; ++nt) {
-        acc[nt][0] = acc[nt][2] = __ldg(b + 8 * nt + 2 * tig);
-        acc[nt][1] = acc[nt][3] = __ldg(b + 8 * nt + 2 * tig + 1);
-    }
+        const float b0 = __ldg(b + 8 * nt + 2 * tig), b1 = __ldg(b + 8 * nt + 2 * tig + 1);
+        float acc[2][4] = {{b0, b1, b0, b1}, {b0, b1, b0, b1}};
 #pragma unroll
-    for (int kc = 0; kc < KC; ++kc) {
-#pragma unroll
-        for (int nt = 0; nt < 8; ++nt) {
+        for (int kc = 0; kc < KC; ++kc) {
             const __nv_bfloat16 *wr = w + (8 * nt + g) * LD + 16 * kc + 2 * tig;
-            mma_bf16_16816(acc[nt], a[kc], ldg_b32(wr), ldg_b32(wr + 8));
+            const uint32_t w0 = ldg_b32(wr), w1 = ldg_b32(wr + 8);
+            mma_bf16_16816(acc[0], a[0][kc], w0, w1);
+            mma_bf16_16816(acc[1], a[1][kc], w0, w1);
+        }
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt) {
+            __nv_bfloat16 *o = H + (16 * mt + g) * kLdH + 8 * nt + 2 * tig;
+            *reinterpret_cast<uint32_t *>(o) = silu_bf16x2(acc[mt][0], acc[mt][1]);
+            *reinterpret_cast<uint32_t *>(o + 8 * kLdH) = silu_bf16x2(acc[mt][2], acc[mt][3]);
         }
     }
-#pragma unroll
-    for (int kc = 0; kc < 4; ++kc) {
-        const float *c0 = acc[2 * kc], *c1 = acc[2 * kc + 1];
-        out[kc][0] = silu_bf16x2(c0[0], c0[1]);
-        out[kc][1] = silu_bf16x2(c0[2], c0[3]);
-        out[kc][2] = silu_bf16x2(c1[0], c1[1]);
-        out[kc][3] = silu_bf16x2(c1[2], c1[3]);
-    }
+    __syncwarp();
 }
 
 // Warp-level inference: every lane passes its 8 raw features and receives the
-// predicted level T for its own row.  `stage` is a 32 x kLdIn bf16 scratch
-// area of this warp in shared memory.  The two 16-row m-tiles run one after
-// the other to keep the register footprint small.
+// predicted level T for its own row.  H is this warp's kMlpWarpStage-element
+// activation tile in shared memory.
 __device__ __forceinline__ float mlp_warp_infer(const MlpPacked *__restrict__ W, const float *feat,
-                                                __nv_bfloat16 *stage) {
+                                                __nv_bfloat16 *H) {
     const int lane = threadIdx.x & 31;
     const int g = lane >> 2, tig = lane & 3;
-    __nv_bfloat16 *my = stage + lane * kLdIn;
+    __nv_bfloat16 *my = H + lane * kLdH;
 #pragma unroll
-    for (int c = 0; c < kMlpIn; ++c)
-        my[c] = __float2bfloat16_rn((feat[c] - __ldg(W->in_mu + c)) * __ldg(W->in_isig + c));
+    for (int c = 0; c < kMlpIn; c += 2)
+        *reinterpret_cast<uint32_t *>(my + c) =
+            pack_bf16x2((feat[c] - __ldg(W->in_mu + c)) * __ldg(W->in_isig + c),
+                        (feat[c + 1] - __ldg(W->in_mu + c + 1)) * __ldg(W->in_isig + c + 1));
 #pragma unroll
-    for (int c = kMlpIn; c < kMlpInPad; ++c) my[c] = __float2bfloat16_rn(0.0f);
+    for (int c = kMlpIn; c < kMlpInPad; c += 2) *reinterpret_cast<uint32_t *>(my + c) = 0u;
     __syncwarp();
-    float y_mine = 0.0f;
-#pragma unroll 1
-    for (int mt = 0; mt < 2; ++mt) {
-        uint32_t a1[1][4];
-        const __nv_bfloat16 *r0 = stage + (16 * mt + g) * kLdIn + 2 * tig;
-        const __nv_bfloat16 *r1 = stage + (16 * mt + g + 8) * kLdIn + 2 * tig;
-        a1[0][0] = *reinterpret_cast<const uint32_t *>(r0);
-        a1[0][1] = *reinterpret_cast<const uint32_t *>(r1);
-        a1[0][2] = *reinterpret_cast<const uint32_t *>(r0 + 8);
-        a1[0][3] = *reinterpret_cast<const uint32_t *>(r1 + 8);
-        uint32_t h1[4][4], h2[4][4];
-        mlp_hidden<1, kMlpInPad>(a1, &W->w1[0][0], W->b1, h1, g, tig);
-        mlp_hidden<4, kMlpH>(h1, &W->w2[0][0], W->b2, h2, g, tig);
-        mlp_hidden<4, kMlpH>(h2, &W->w3[0][0], W->b3, h1, g, tig);
-        float o[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    mlp_layer<1, kMlpInPad>(H, &W->w1[0][0], W->b1, g, tig);
+    mlp_layer<4, kMlpH>(H, &W->w2[0][0], W->b2, g, tig);
+    mlp_layer<4, kMlpH>(H, &W->w3[0][0], W->b3, g, tig);
+    // output layer: one n8 tile (row 0 of w4 real), both m-tiles
+    float o[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
 #pragma unroll
-        for (int kc = 0; kc < 4; ++kc) {
-            const __nv_bfloat16 *wr = &W->w4[g][0] + 16 * kc + 2 * tig;
-            mma_bf16_16816(o, h1[kc], ldg_b32(wr), ldg_b32(wr + 8));
+    for (int kc = 0; kc < 4; ++kc) {
+        const __nv_bfloat16 *wr = &W->w4[g][0] + 16 * kc + 2 * tig;
+        const uint32_t w0 = ldg_b32(wr), w1 = ldg_b32(wr + 8);
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt) {
+            uint32_t a[4];
+            mlp_load_a(H, mt, kc, g, tig, a);
+            mma_bf16_16816(o[mt], a, w0, w1);
         }
-        // row r of this m-tile, column 0: lane 4 (r mod 8), register 0 (r < 8) or 2
-        const int r = lane & 15;
-        const float v0 = __shfl_sync(0xffffffffu, o[0], 4 * (r & 7));
-        const float v2 = __shfl_sync(0xffffffffu, o[2], 4 * (r & 7));
-        if ((lane >> 4) == mt) y_mine = r < 8 ? v0 : v2;
     }
-    __syncwarp();
-    return (y_mine + __ldg(&W->b4)) * __ldg(&W->out_sigma) + __ldg(&W->out_mu);
-}
-
-// The integration kernel's call: not inlined, so the inference's registers
-// are those of a function call made on a small fraction of the intervals and
-// the stepping loop keeps its own allocation.
-static __device__ __noinline__ float mlp_warp_infer_call(const MlpPacked *__restrict__ W,
-                                                         const float *feat, __nv_bfloat16 *stage) {
-    return mlp_warp_infer(W, feat, stage);
+    __syncwarp();  // H may be rewritten by the next consult
+    // row r of m-tile mt, column 0: lane 4 (r mod 8), register 0 (r < 8) or 2
+    const int r = lane & 15, src = 4 * (r & 7);
+    const float v00 = __shfl_sync(0xffffffffu, o[0][0], src), v02 = __shfl_sync(0xffffffffu, o[0][2], src);
+    const float v10 = __shfl_sync(0xffffffffu, o[1][0], src), v12 = __shfl_sync(0xffffffffu, o[1][2], src);
+    const float y = (lane < 16) ? (r < 8 ? v00 : v02) : (r < 8 ? v10 : v12);
+    return (y + __ldg(&W->b4)) * __ldg(&W->out_sigma) + __ldg(&W->out_mu);
 }
 
 // Dynamic shared memory of a CTA of `warps` warps running the inference.
-__host__ __device__ constexpr int mlp_stage_bytes(int warps) { return warps * 32 * kLdIn * 2; }
+__host__ __device__ constexpr int mlp_stage_bytes(int warps) { return warps * kMlpWarpStage * 2; }
+
 
 }  // namespace hhg

@@ -340,7 +340,7 @@ __global__ void __launch_bounds__(hhg::kBlockThreads) mlp_infer_kernel(const hhg
     float f[kIn];
 #pragma unroll
     for (int c = 0; c < kIn; ++c) f[c] = i < n ? rec[i * stride + c] : 0.0f;
-    const float T = hhg::mlp_warp_infer(net, f, stage + wib * 32 * hhg::kLdIn);
+    const float T = hhg::mlp_warp_infer(net, f, stage + wib * hhg::kMlpWarpStage);
     if (i < n) out[i] = T;
 }
 
