@@ -643,6 +643,10 @@ def our_arm(args):
         e_batches = [(k * ws + rank + args.warmup) % nb for k in range(n_e2e)]
         if nb == 1:
             eng.current_density(wl.system, batches[0], grid, wl.opts(**okw))  # cache warm-up
+        # warm-up of the spectrum path (the context's FFT plans and buffers
+        # for a length are made on its first call)
+        for n_m in sorted({p.n_measurements for b in e_batches for p in batches[b]}):
+            eng.spectrum(np.zeros(n_m + 1), n_m, 0.0, 1.0)
         if ws > 1:
             torch.distributed.barrier()
         torch.cuda.synchronize()

@@ -5,11 +5,14 @@
 #include <cufft.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/hhg_gpu.h"
@@ -120,7 +123,7 @@ hhg_status set_err(hhg_ctx *ctx, hhg_status st, const std::string &msg) {
     } while (0)
 
 // Gauss-Legendre nodes by Newton iteration on P_n in long double.
-void gauss_legendre(int n, double *x, double *w) {
+void gauss_legendre_compute(int n, double *x, double *w) {
     const long double pi = 3.141592653589793238462643383279502884L;
     const int m = (n + 1) / 2;
     for (int i = 0; i < m; ++i) {
@@ -155,6 +158,28 @@ void gauss_legendre(int n, double *x, double *w) {
         w[i] = (double)wi;
     }
     if (n & 1) x[n / 2] = 0.0;
+}
+
+// The same, remembered per n for the life of the process (a 1024-point rule
+// costs ~10 ms of long-double Newton steps, and every plan on a grid needs it).
+void gauss_legendre(int n, double *x, double *w) {
+    static std::mutex mu;
+    static std::map<int, std::vector<double>> rules;  // n nodes, then n weights
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        const auto it = rules.find(n);
+        if (it != rules.end()) {
+            std::memcpy(x, it->second.data(), sizeof(double) * n);
+            std::memcpy(w, it->second.data() + n, sizeof(double) * n);
+            return;
+        }
+    }
+    std::vector<double> r(2 * (size_t)n);
+    gauss_legendre_compute(n, r.data(), r.data() + n);
+    std::memcpy(x, r.data(), sizeof(double) * n);
+    std::memcpy(w, r.data() + n, sizeof(double) * n);
+    std::lock_guard<std::mutex> lock(mu);
+    rules.emplace(n, std::move(r));
 }
 
 // Positive half, ascending: gauss::container<n> (thread_gauss.hpp).
@@ -317,6 +342,24 @@ void piflux_rescued_row(const hhg_system_desc &s, double x, double y, double z, 
     o[7] = 0.0;
 }
 
+// body(i) for i in [0, n) on up to 32 host threads (each i writes its own
+// rows, so the table is the same whatever the schedule).
+template <class F> void parallel_for(int n, F body) {
+    const unsigned hc = std::thread::hardware_concurrency();
+    const int nt = (int)std::min<unsigned>(std::max(hc, 1u), 32u);
+    if (nt <= 1 || n < 64) {
+        for (int i = 0; i < n; ++i) body(i);
+        return;
+    }
+    std::atomic<int> next{0};
+    std::vector<std::thread> pool;
+    for (int t = 0; t < nt; ++t)
+        pool.emplace_back([&] {
+            for (int i; (i = next.fetch_add(1)) < n;) body(i);
+        });
+    for (auto &th : pool) th.join();
+}
+
 // Row builders; see the oracle for the same restatements.
 void build_rows(const hhg_system_desc &s, const hhg_grid_desc &g, double *out) {
     size_t r = 0;
@@ -327,10 +370,11 @@ void build_rows(const hhg_system_desc &s, const hhg_grid_desc &g, double *out) {
         gauss_legendre(g.n2, gy.data(), wy.data());
         const double hx = 0.5 * (g.x_hi - g.x_lo), mx = 0.5 * (g.x_hi + g.x_lo);
         const double hy = 0.5 * (g.y_hi - g.y_lo), my = 0.5 * (g.y_hi + g.y_lo);
-        for (int i = 0; i < g.n1; ++i)
+        parallel_for(g.n1, [&](int i) {
             for (int j = 0; j < g.n2; ++j)
                 push_row(s, hx * gx[i] + mx, hy * gy[j] + my, 0.0, hx * hy * wx[i] * wy[j],
-                         out + 8 * r++);
+                         out + 8 * ((size_t)i * g.n2 + j));
+        });
         break;
     }
     case HHG_GRID_RHOMBIC_GL: {
@@ -341,12 +385,13 @@ void build_rows(const hhg_system_desc &s, const hhg_grid_desc &g, double *out) {
         std::vector<double> g1(g.n1), w1(g.n1), g2(g.n2), w2(g.n2);
         gauss_legendre(g.n1, g1.data(), w1.data());
         gauss_legendre(g.n2, g2.data(), w2.data());
-        for (int i = 0; i < g.n1; ++i)
+        parallel_for(g.n1, [&](int i) {
             for (int j = 0; j < g.n2; ++j) {
                 const double f1 = 0.5 * g1[i], f2 = 0.5 * g2[j];
                 push_row(s, f1 * b1x + f2 * b2x, f1 * b1y + f2 * b2y, 0.0,
-                         0.25 * area * w1[i] * w2[j], out + 8 * r++);
+                         0.25 * area * w1[i] * w2[j], out + 8 * ((size_t)i * g.n2 + j));
             }
+        });
         break;
     }
     case HHG_GRID_PIFLUX3D_REF: {
@@ -781,10 +826,23 @@ void fill_pulse_dev(const hhg_pulse_desc &q, const HostPulse &hp, PulseDev &d) {
 // spline threshold is 2^-36 and every interval is tested; knots denser than
 // the intervals, or a spline that turns within a knot or two (QuenchedField's
 // step, 4e-9), are refused.
+// Chebyshev nodes cos(pi (k + 1/2) / 16) and the DCT matrix cos(pi j (k + 1/2) / 16)
+// of the degree test, in long double, computed once.
+struct ChebTables {
+    static constexpr int NN = 16;
+    long double node[NN], dct[NN][NN];
+    ChebTables() {
+        const long double pi = 3.141592653589793238462643383279502884L;
+        for (int k = 0; k < NN; ++k) node[k] = cosl(pi * (k + 0.5L) / NN);
+        for (int j = 0; j < NN; ++j)
+            for (int k = 0; k < NN; ++k) dct[j][k] = cosl(pi * j * (k + 0.5L) / NN);
+    }
+};
+
 int choose_degree(const hhg_pulse_desc &p, const double *proj, int nf) {
+    static const ChebTables tab;
     const HostPulse hp(p);
-    const int NN = 16;
-    const long double pi = 3.141592653589793238462643383279502884L;
+    const int NN = ChebTables::NN;
     const long double me = ((long double)p.window_end - p.window_begin) / p.n_measurements;
     const int samples = p.kind == HHG_PULSE_SPLINE ? p.n_measurements : std::min(p.n_measurements, 257);
     long double tail5 = 0.0L, tail7 = 0.0L, tail11 = 0.0L, scale = 1.0L;
@@ -796,13 +854,13 @@ int choose_degree(const hhg_pulse_desc &p, const double *proj, int nf) {
             for (int part = 0; part < (nf == 1 ? 1 : 2); ++part) {
                 long double fv[NN];
                 for (int k = 0; k < NN; ++k) {
-                    const long double A = hp.continued_ld(ctr + half * cosl(pi * (k + 0.5L) / NN));
+                    const long double A = hp.continued_ld(ctr + half * tab.node[k]);
                     if (nf == 1) fv[k] = A;
                     else fv[k] = part == 0 ? cosl(proj[n] * A) : sinl(proj[n] * A);
                 }
                 for (int j = 0; j < NN; ++j) {
                     long double acc = 0.0L;
-                    for (int k = 0; k < NN; ++k) acc += fv[k] * cosl(pi * j * (k + 0.5L) / NN);
+                    for (int k = 0; k < NN; ++k) acc += fv[k] * tab.dct[j][k];
                     acc = fabsl(acc * 2.0L / NN);
                     if (j == 0) scale = std::max(scale, acc);
                     if (j > 5) tail5 = std::max(tail5, acc);
