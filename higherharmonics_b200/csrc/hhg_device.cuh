@@ -372,23 +372,43 @@ template <> struct Num<float> {
 // Pulse evaluators used inside a step: polynomial (any t) or table (stage s of
 // a standard step).  Values come back as Num<R>::V.
 // ---------------------------------------------------------------------------
+// D = 0: no interpolant; the pulse is evaluated exactly at every stage time
+// (A(t) from the pulse's own form, then the staged functions), for spline
+// pulses whose knots a per-interval polynomial cannot follow (a step between
+// two knots, QuenchedField.cpp:15-29).  FP64 only.
 template <int NF, int D, typename R, bool PAIR = false>
 struct PolyEval {
     static constexpr bool kReuse = true;  // stages sharing a node reuse the values
     const double *hd;  // interval record
     double tb, te;
+    const PulseDev *pd = nullptr;  // D = 0: the pulse
     __device__ __forceinline__ void operator()(int, double t, typename Num<R>::V *f) const {
-        const double u = (t - hd[2]) * hd[3];
         const bool inside = (t > tb) && (t < te);
-        const double *c0 = hd + slot_poly(NF);
         double v[NF];
+        if constexpr (D == 0) {
+            const double A = laser_continued(*pd, t);
+            if constexpr (NF == 1) {
+                v[0] = inside ? A : outside_value<NF>(0);
+            } else {
 #pragma unroll
-        for (int n = 0; n < NF; ++n) {
-            const double *c = c0 + n * (D + 1);
-            double x = c[D];
+                for (int n = 0; n < NF / 2; ++n) {
+                    double sn, cn;
+                    sincos(pd->s[n] * A, &sn, &cn);
+                    v[2 * n] = inside ? cn : outside_value<NF>(2 * n);
+                    v[2 * n + 1] = inside ? sn : outside_value<NF>(2 * n + 1);
+                }
+            }
+        } else {
+            const double u = (t - hd[2]) * hd[3];
+            const double *c0 = hd + slot_poly(NF);
 #pragma unroll
-            for (int j = D - 1; j >= 0; --j) x = fma(x, u, c[j]);
-            v[n] = inside ? x : outside_value<NF>(n);
+            for (int n = 0; n < NF; ++n) {
+                const double *c = c0 + n * (D + 1);
+                double x = c[D];
+#pragma unroll
+                for (int j = D - 1; j >= 0; --j) x = fma(x, u, c[j]);
+                v[n] = inside ? x : outside_value<NF>(n);
+            }
         }
         if constexpr (PAIR) {
             static_assert(NF == 4, "the paired layout holds two projections");
@@ -1392,7 +1412,7 @@ __device__ __forceinline__ void keep_sample(int i, double sum, int N, int sub, i
 }
 
 template <int M, int D>
-__device__ void integrate_free(const KParams &P, const ModelState<M, double> &ms,
+__device__ void integrate_free(const KParams &P, const PulseDev &pd, const ModelState<M, double> &ms,
                                const double *coef, double dt0, double tb, double te, int N,
                                double w, bool &dead, double *S, double &held, double *prow,
                                int sub, int lane, double *ring,
@@ -1410,7 +1430,7 @@ __device__ void integrate_free(const KParams &P, const ModelState<M, double> &ms
             bool finished = dead;
             if (!dead) {
                 if ((t + dt) - t1 > kDblEps) dt = t1 - t;
-                const PolyEval<NF, D, double> poly{gs, tb, te};
+                const PolyEval<NF, D, double> poly{gs, tb, te, &pd};
                 double xn[3], e[3], k0[3];
                 rkf78_attempt<M, NF, double>(ms, poly, t, dt, S, xn, e, k0);
                 ++attempts;
@@ -1573,7 +1593,7 @@ __global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integ
             double ga_next[STEPPER == 1 ? NF : 1], gb_next[STEPPER == 1 ? NF : 1];
             if constexpr (STEPPER == 1) {
                 const double h0 = coef[1] - coef[0];
-                const PolyEval<NF, D, double> pe{coef, tb, te};
+                const PolyEval<NF, D, double> pe{coef, tb, te, &pd};
                 pe(0, coef[0] + kGa * h0, ga_next);
                 pe(0, coef[0] + (1.0 - kGa) * h0, gb_next);
             }
@@ -1589,7 +1609,7 @@ __global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integ
                 // sample 0 at t_begin, then free lanes through samples 1 .. N
                 keep_sample(0, warp_sum(dead ? 0.0 : w * ms.vertex(pd.s0rec, S)), N, sub, lane, held,
                             prow);
-                integrate_free<M, D>(P, ms, coef, dt0, tb, te, N, w, dead, S, held, prow, sub, lane,
+                integrate_free<M, D>(P, pd, ms, coef, dt0, tb, te, N, w, dead, S, held, prow, sub, lane,
                                      free_ring[wib], my_attempts, my_rejects);
             } else {
             for (int i = 0; i <= N; ++i) {
@@ -1619,7 +1639,7 @@ __global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integ
                     const double *cur = STEPPER != 0 ? gslot : slot;
                     rec = cur + 4;
                     const double t0 = cur[0], t1 = cur[1];
-                    const PolyEval<NF, D, R, kPair> poly{slot, tb, te};
+                    const PolyEval<NF, D, R, kPair> poly{slot, tb, te, &pd};
                     if constexpr (STEPPER == 1) {
                         if (P.magnus_substeps == 1) {
                             double f1[NF], f2[NF];
@@ -1631,7 +1651,7 @@ __global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integ
                             if (i < N) {
                                 const double *gn = gslot + SLOT;
                                 const double hn = gn[1] - gn[0];
-                                const PolyEval<NF, D, double> pe{gn, tb, te};
+                                const PolyEval<NF, D, double> pe{gn, tb, te, &pd};
                                 pe(0, gn[0] + kGa * hn, ga_next);
                                 pe(0, gn[0] + (1.0 - kGa) * hn, gb_next);
                             }
@@ -1655,7 +1675,7 @@ __global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integ
                             for (int s = 0; s < ns; ++s) {
                                 const double ts = t0 + s * hs;
                                 double f[NF], d1[3], d2[3];
-                                const PolyEval<NF, D, double> pd64{cur, tb, te};
+                                const PolyEval<NF, D, double> pd64{cur, tb, te, &pd};
                                 pd64(0, ts + g * hs, f);
                                 ms.dvec(f, d1);
                                 pd64(0, ts + (1.0 - g) * hs, f);

@@ -1168,20 +1168,32 @@ static hhg_status plan_create_impl(hhg_ctx *ctx, const hhg_system_desc *sys,
         proj[0] = 1.0;
         break;
     }
+    // A spline pulse whose knots a per-interval polynomial cannot follow (a
+    // step between two knots) is evaluated exactly at every stage time
+    // (degree 0), in FP64 RKF78 with the reference schedule or the carried step.
+    const bool exact_ok = o.stepper == HHG_STEPPER_RKF78 && o.precision == HHG_PREC_FP64 &&
+                          (o.proposer == HHG_PROPOSER_NONE || o.proposer == HHG_PROPOSER_CARRY);
     int degree = 5;
+    bool exact = false;
     for (int p = 0; p < n_pulses; ++p) {
         const int d = choose_degree(pulses[p], proj, nf);
+        if (d < 0 && pulses[p].kind == HHG_PULSE_SPLINE && exact_ok) {
+            exact = true;
+            continue;
+        }
         if (d < 0) {
             delete pl;
             return set_err(ctx, HHG_UNSUPPORTED,
                            pulses[p].kind == HHG_PULSE_SPLINE
-                               ? "spline pulse: knots too dense or too steep for the measurement "
-                                 "intervals (more n_measurements, or smoother samples)"
+                               ? "spline pulse: knots too dense or too steep for the staged "
+                                 "interpolants; exact evaluation runs FP64 RKF78 with the NONE or "
+                                 "CARRY proposer"
                                : "measurement interval too coarse for the staged pulse interpolants");
         }
         degree = std::max(degree, d);
     }
-    pl->degree = degree;
+    pl->degree = exact ? 0 : degree;
+    degree = pl->degree;
     const bool dyadic = o.proposer == HHG_PROPOSER_LOCKSTEP || o.proposer == HHG_PROPOSER_LEARNED;
     const int slot = dyadic ? hhg::slot_doubles_dyadic(nf, degree) : hhg::slot_doubles(nf, degree);
 
@@ -2109,6 +2121,12 @@ hhg_status output_plan(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_pulse
     hhg_plan *pl = nullptr;
     hhg_status st = plan_create_impl(ctx, sys, pulse, 1, grid, &o, &pl, false);  // k order kept
     if (st != HHG_OK) return st;
+    if (pl->degree == 0) {
+        hhg_plan_destroy(pl);
+        return set_err(ctx, HHG_UNSUPPORTED,
+                       "spline pulse too steep for the staged interpolants: its exact evaluation "
+                       "runs the Brillouin-zone current only");
+    }
     auto fail = [&](const char *what, cudaError_t e) {
         hhg_plan_destroy(pl);
         return set_err(ctx, HHG_CUDA_ERROR, std::string(what) + ": " + cudaGetErrorString(e));
@@ -2302,6 +2320,12 @@ hhg_status dirac_quadrature(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_
         ctx->kappa_cap = 0;
         hhg_plan *np = nullptr;
         if ((st = hhg_plan_create(ctx, sys, pulse, 1, &g, &o, &np)) != HHG_OK) return st;
+        if (np->degree == 0) {
+            hhg_plan_destroy(np);
+            return set_err(ctx, HHG_UNSUPPORTED,
+                           "spline pulse too steep for the staged interpolants: its exact "
+                           "evaluation runs the Brillouin-zone current only");
+        }
         np->out_mode = 4;
         int occ = 0;
         hhg::LaunchReq lr{};

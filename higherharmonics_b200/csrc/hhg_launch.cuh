@@ -9,7 +9,7 @@ namespace hhg {
 
 struct LaunchReq {
     KParams kp;
-    int degree;     // 5, 7 or 11
+    int degree;     // 5, 7 or 11; 0 = exact pulse evaluation (FP64 RKF78, proposer 0/1)
     int precision;  // 0 FP64, 1 mixed (FP32 right-hand side)
     int stepper;    // 0 RKF78, 1 Magnus-4
     int proposer;   // 0 restart at dt0, 1 carry, 2 warp-synchronous dyadic, 3 learned dyadic,
@@ -117,8 +117,20 @@ cudaError_t launch_deg(const LaunchReq &r) {
     }
 }
 
+// Degree 0 (pulses evaluated exactly at every stage time, no interpolant):
+// FP64 RKF78 with the reference schedule or the carried step, the current
+// only.
+template <int M>
+cudaError_t launch_exact(const LaunchReq &r) {
+    if (r.out_mode != 0 || r.stepper != 0 || r.precision != 0) return cudaErrorNotSupported;
+    if (r.proposer == 0) return launch_one<M, 0, double, 0, 0>(r);
+    if (r.proposer == 1) return launch_one<M, 0, double, 0, 1>(r);
+    return cudaErrorNotSupported;
+}
+
 template <int M>
 cudaError_t launch_model(const LaunchReq &r) {
+    if (r.degree == 0) return launch_exact<M>(r);
     if (r.degree == 5) return launch_deg<M, 5>(r);
     if (r.degree == 7) return launch_deg<M, 7>(r);
     if (r.degree == 11) return launch_deg<M, 11>(r);
@@ -146,7 +158,10 @@ cudaError_t stage_model(const StageReq &s) {
     const long long blocks = (s.total_intervals + threads - 1) / threads;
     if (s.layout < 0 || s.layout > 3 || (s.layout == 3 && (M != DIRAC3D || !s.gl30)))
         return cudaErrorInvalidValue;
-    if (s.degree == 5) stage_deg<M, 5>(s, (unsigned)blocks, threads);
+    if (s.degree == 0) {
+        if (s.layout != 0) return cudaErrorNotSupported;
+        stage_one<M, 0, 0>(s, (unsigned)blocks, threads);
+    } else if (s.degree == 5) stage_deg<M, 5>(s, (unsigned)blocks, threads);
     else if (s.degree == 7) stage_deg<M, 7>(s, (unsigned)blocks, threads);
     else if (s.degree == 11) stage_deg<M, 11>(s, (unsigned)blocks, threads);
     else return cudaErrorInvalidValue;

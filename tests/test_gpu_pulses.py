@@ -1,6 +1,7 @@
 """Pulse shapes beyond the CosineLaser on the GPU (through the C ABI) against
 the CPU oracle: ContinuousLaser, GaussLaser and the spline lasers
-(Laser.hpp:32-37 with use_spline: PowerLawField, QuenchedField, DoubleLaser),
+(Laser.hpp:32-37 with use_spline: PowerLawField, QuenchedField, DoubleLaser;
+QuenchedField's step between two knots evaluated exactly at every stage time),
 same nodes, weights and pulses.  Bar: j(t) relative L2 <= 1e-9 and harmonic
 intensities within 1e-6 above the noise floor for the reference step
 schedule; the step proposers within the 1e-4 harmonic bar.
@@ -79,18 +80,44 @@ def test_spline_cut_inside_the_window(engine):
     assert err <= J_TOL, err
 
 
-def test_steep_spline_refused(engine):
+def _quench_template(n=256, a0=0.7):
     # QuenchedField's template (QuenchedField.cpp:15-29): the field turns on
-    # within two knots, which one interpolant per measurement interval cannot
-    # follow to 2^-36; the call says so instead of losing accuracy
+    # and off within two knots, which one interpolant per measurement interval
+    # cannot follow to 2^-36
+    return [0.0 if (i < n // 4 or i > 3 * n // 4) else
+            (0.5 * a0 if i in (n // 4, 3 * n // 4) else a0) for i in range(n)]
+
+
+@pytest.mark.parametrize("model", ["dirac2d", "honeycomb"])
+def test_steep_spline_exact_evaluation_parity(engine, model):
+    """A spline the staged interpolants cannot follow is evaluated exactly at
+    every stage time (degree 0): parity with the oracle at the plain path's
+    bar, the reference schedule; the carried step within the fast bar."""
     n = 256
-    y = [0.0 if (i < 64 or i > 192) else (0.35 if i in (64, 192) else 0.7) for i in range(n)]
-    pulse = api.spline_pulse(y, 0.0, 6 * math.pi / (n - 1), 2048, (0.0, 6 * math.pi),
-                             deriv=(0.0, 0.0), energy_scale=10.0)
+    pulse = api.spline_pulse(_quench_template(n), 0.0, 6 * math.pi / (n - 1), 2048,
+                             (0.0, 6 * math.pi), deriv=(0.0, 0.0), energy_scale=10.0)
+    if model == "dirac2d":
+        sys, grid = api.system(api.SYS_DIRAC2D, velocity=1.0, mass=0.05), api.grid_tensor(8, 8, -2, 2, -2, 2)
+    else:
+        sys, grid = api.system(api.SYS_HONEYCOMB, hopping=1.0, mass=0.1), api.grid_rhombic(8, 8)
+    err, herr = _parity(engine, sys, pulse, grid)
+    assert err <= J_TOL and herr <= H_TOL, (err, herr)
+    _, st = engine.current_density(sys, pulse, grid, api.solver())
+    assert st.poly_degree == 0
+    err, herr = _parity(engine, sys, pulse, grid, proposer=api.PROPOSER_CARRY)
+    assert err <= 1e-4 and herr <= 1e-4, (err, herr)
+
+
+@pytest.mark.parametrize("okw", [dict(precision=api.PREC_MIXED, abs_tol=1e-8, rel_tol=1e-6),
+                                 dict(proposer=api.PROPOSER_LOCKSTEP)])
+def test_steep_spline_refused_by_the_fast_variants(engine, okw):
+    n = 256
+    pulse = api.spline_pulse(_quench_template(n), 0.0, 6 * math.pi / (n - 1), 2048,
+                             (0.0, 6 * math.pi), deriv=(0.0, 0.0), energy_scale=10.0)
     with pytest.raises(api.HHGError) as ei:
         engine.current_density(api.system(api.SYS_DIRAC2D, velocity=1.0, mass=0.05), pulse,
-                               api.grid_tensor(4, 4, -2, 2, -2, 2), api.solver())
-    assert ei.value.status == api.UNSUPPORTED and "spline" in str(ei.value)
+                               api.grid_tensor(4, 4, -2, 2, -2, 2), api.solver(**okw))
+    assert ei.value.status == api.UNSUPPORTED and "exact evaluation" in str(ei.value)
 
 
 def test_spline_pulse_lockstep_meets_harmonic_bar(engine):
@@ -130,7 +157,7 @@ def test_dirac_magnus_with_gauss_pulse(engine):
     assert err <= 1e-12, err
 
 
-@pytest.mark.parametrize("laser", ["dcos", "dgaussA", "powerlaw1", "gauss", "continuous"])
+@pytest.mark.parametrize("laser", ["dcos", "dgaussA", "powerlaw1", "gauss", "continuous", "quench"])
 def test_reference_laser_types_from_config(engine, laser):
     # a small PiFlux run of each laser_type the config reader hands to the device
     txt = f"""
