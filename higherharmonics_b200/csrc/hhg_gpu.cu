@@ -343,11 +343,12 @@ void piflux_rescued_row(const hhg_system_desc &s, double x, double y, double z, 
 }
 
 // body(i) for i in [0, n) on up to 32 host threads (each i writes its own
-// rows, so the table is the same whatever the schedule).
-template <class F> void parallel_for(int n, F body) {
+// outputs, so the result is the same whatever the schedule); serial below
+// min_n items.
+template <class F> void parallel_for(int n, F body, int min_n = 64) {
     const unsigned hc = std::thread::hardware_concurrency();
     const int nt = (int)std::min<unsigned>(std::max(hc, 1u), 32u);
-    if (nt <= 1 || n < 64) {
+    if (nt <= 1 || n < min_n) {
         for (int i = 0; i < n; ++i) body(i);
         return;
     }
@@ -1175,8 +1176,11 @@ static hhg_status plan_create_impl(hhg_ctx *ctx, const hhg_system_desc *sys,
                           (o.proposer == HHG_PROPOSER_NONE || o.proposer == HHG_PROPOSER_CARRY);
     int degree = 5;
     bool exact = false;
+    // the degree test costs ~5 ms of long-double work per pulse: pulses in parallel
+    std::vector<int> degs((size_t)n_pulses);
+    parallel_for(n_pulses, [&](int p) { degs[(size_t)p] = choose_degree(pulses[p], proj, nf); }, 2);
     for (int p = 0; p < n_pulses; ++p) {
-        const int d = choose_degree(pulses[p], proj, nf);
+        const int d = degs[(size_t)p];
         if (d < 0 && pulses[p].kind == HHG_PULSE_SPLINE && exact_ok) {
             exact = true;
             continue;
