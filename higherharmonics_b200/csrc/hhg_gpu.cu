@@ -10,6 +10,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -39,6 +40,11 @@ struct hhg_ctx {
     // staging, launch state) of the last (system, pulse, options), the rows
     // its k table and sample buffer hold, and grow-only device buffers
     hhg_plan *kappa_plan = nullptr;
+    // the device k table of the last plan built from a generated grid (key:
+    // the system and grid descriptors), shared with the plans that use it: a
+    // new batch of pulses on the same grid skips building and uploading rows
+    std::shared_ptr<double> ktab_shared;
+    std::string ktab_key;
     std::string kappa_key;
     long long kappa_cap = 0;
     int kappa_occ = 1;
@@ -50,6 +56,7 @@ struct hhg_ctx {
 
 struct hhg_plan {
     hhg_ctx *ctx = nullptr;
+    std::shared_ptr<double> ktab_owner;  // set when d_ktab is the context's shared table
     int model = 0, degree = 7;
     hhg_solver_opts opts{};
     int n_pulses = 0;
@@ -626,6 +633,16 @@ int kernel_model(const hhg_system_desc &s) {
 
 constexpr size_t kPlanCacheSize = 4;
 
+// Byte key of the k table a generated grid gives for a system.
+std::string ktab_key(const hhg_system_desc *sys, const hhg_grid_desc *grid) {
+    std::string k;
+    auto put = [&k](const void *p, size_t n) { k.append(static_cast<const char *>(p), n); };
+    put(sys, sizeof *sys);
+    put(&grid->kind, 4 * 3);
+    put(&grid->x_lo, 8 * 4);
+    return k;
+}
+
 // Byte key of the descriptors of one one-shot call: every field that changes
 // the computation (explicit k rows and the learned network by value).
 std::string plan_key(const hhg_system_desc *sys, const hhg_pulse_desc *pulses, int n_pulses,
@@ -1006,6 +1023,7 @@ void hhg_gpu_destroy(hhg_ctx *c) {
     for (auto &kv : c->plan_cache) hhg_plan_destroy(kv.second);
     c->plan_cache.clear();
     if (c->kappa_plan) hhg_plan_destroy(c->kappa_plan);
+    c->ktab_shared.reset();
     for (hhg_ctx::Grow *g : {&c->kappa_T, &c->kappa_items, &c->kappa_change, &c->kappa_j, &c->kappa_slice})
         cudaFree(g->p);
     for (auto &kv : c->fft_plans) cufftDestroy(kv.second);
@@ -1098,12 +1116,21 @@ static hhg_status plan_create_impl(hhg_ctx *ctx, const hhg_system_desc *sys,
     pl->n_pulses = n_pulses;
     const int nf = model_nf(pl->model);
 
-    // k table
+    // k table: built here, or the context's shared table of the same system
+    // and generated grid (the cost-ordered tables depend on the pulse and
+    // explicit rows are the caller's: neither is shared)
     pl->n_k = grid_count(*grid);
-    std::vector<double> ktab((size_t)pl->n_k * 8);
-    build_rows(*sys, *grid, ktab.data());
-    if (cost_order && hhg::base_model(pl->model) == hhg::PIFLUX3D && pl->n_k > 32 &&
-        (o.proposer == HHG_PROPOSER_NONE || o.proposer == HHG_PROPOSER_CARRY)) {
+    const bool cost_sort = cost_order && hhg::base_model(pl->model) == hhg::PIFLUX3D && pl->n_k > 32 &&
+                           (o.proposer == HHG_PROPOSER_NONE || o.proposer == HHG_PROPOSER_CARRY);
+    const bool share_ktab = !cost_sort && grid->kind != HHG_GRID_EXPLICIT;
+    const std::string kkey = share_ktab ? ktab_key(sys, grid) : std::string();
+    const bool reuse_ktab = share_ktab && ctx->ktab_shared && ctx->ktab_key == kkey;
+    std::vector<double> ktab;
+    if (!reuse_ktab) {
+        ktab.resize((size_t)pl->n_k * 8);
+        build_rows(*sys, *grid, ktab.data());
+    }
+    if (cost_sort) {
         // With per-lane step control a warp's lanes finish together only if
         // their k-points need similar numbers of steps.  The step count
         // follows the time average of |d(k - A(t))| (correlation -0.43
@@ -1331,7 +1358,16 @@ static hhg_status plan_create_impl(hhg_ctx *ctx, const hhg_system_desc *sys,
     };
     cudaError_t e;
     cudaStream_t s = ctx->stream;
-    if ((e = cudaMalloc(&pl->d_ktab, ktab.size() * sizeof(double))) != cudaSuccess) return fail("alloc k table", e);
+    if (reuse_ktab) {
+        pl->ktab_owner = ctx->ktab_shared;
+        pl->d_ktab = pl->ktab_owner.get();
+    } else if ((e = cudaMalloc(&pl->d_ktab, ktab.size() * sizeof(double))) != cudaSuccess) {
+        return fail("alloc k table", e);
+    } else if (share_ktab) {
+        pl->ktab_owner = std::shared_ptr<double>(pl->d_ktab, [](double *p) { cudaFree(p); });
+        ctx->ktab_shared = pl->ktab_owner;
+        ctx->ktab_key = kkey;
+    }
     if ((e = cudaMalloc(&pl->d_pulses, n_pulses * sizeof(PulseDev))) != cudaSuccess) return fail("alloc pulses", e);
     if ((e = cudaMalloc(&pl->d_coef, coef_len * sizeof(double))) != cudaSuccess) return fail("alloc staging", e);
     if ((e = cudaMalloc(&pl->d_part, part_len * sizeof(double))) != cudaSuccess) return fail("alloc partials", e);
@@ -1351,7 +1387,9 @@ static hhg_status plan_create_impl(hhg_ctx *ctx, const hhg_system_desc *sys,
             return fail("upload network", e);
         pl->opts.mlp = nullptr;  // the plan keeps its device copy only
     }
-    if ((e = cudaMemcpyAsync(pl->d_ktab, ktab.data(), ktab.size() * sizeof(double), cudaMemcpyHostToDevice, s)) != cudaSuccess) return fail("upload k table", e);
+    if (!reuse_ktab &&
+        (e = cudaMemcpyAsync(pl->d_ktab, ktab.data(), ktab.size() * sizeof(double), cudaMemcpyHostToDevice, s)) != cudaSuccess)
+        return fail("upload k table", e);
     if ((e = cudaMemcpyAsync(pl->d_pulses, pl->pulses.data(), n_pulses * sizeof(PulseDev), cudaMemcpyHostToDevice, s)) != cudaSuccess) return fail("upload pulses", e);
     if ((e = cudaMemcpyAsync(pl->d_tgrid, tgrid.data(), tgrid.size() * sizeof(double), cudaMemcpyHostToDevice, s)) != cudaSuccess) return fail("upload tgrid", e);
     if ((e = cudaMemcpyAsync(pl->d_ioff, ioff.data(), ioff.size() * sizeof(long long), cudaMemcpyHostToDevice, s)) != cudaSuccess) return fail("upload offsets", e);
@@ -1402,7 +1440,8 @@ hhg_status hhg_plan_create(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_p
 void hhg_plan_destroy(hhg_plan *pl) {
     if (!pl) return;
     cudaSetDevice(pl->ctx->device);
-    cudaFree(pl->d_ktab);
+    if (pl->ktab_owner) pl->ktab_owner.reset();  // the context may still hold the table
+    else cudaFree(pl->d_ktab);
     cudaFree(pl->d_pulses);
     cudaFree(pl->d_coef);
     cudaFree(pl->d_part);
@@ -2439,7 +2478,8 @@ hhg_status dirac_quadrature(hhg_ctx *ctx, const hhg_system_desc *sys, const hhg_
         if (want > cap) {
             // grow the k table and the per-trajectory sample buffer
             cap = std::min(limit, std::max(want, 2 * cap));
-            HHG_CUDA(ctx, cudaFree(pl->d_ktab));
+            if (pl->ktab_owner) pl->ktab_owner.reset();
+            else HHG_CUDA(ctx, cudaFree(pl->d_ktab));
             HHG_CUDA(ctx, cudaFree(pl->d_kout));
             pl->d_ktab = nullptr;
             pl->d_kout = nullptr;

@@ -115,3 +115,37 @@ def test_one_shot_plan_cache_has_no_stale_hits(engine):
                                                                  proposer=api.PROPOSER_CARRY))
     assert not np.array_equal(a, d)
     e2.close()
+
+
+def test_plans_share_the_k_table_of_a_grid(engine):
+    """Plans built on one context from the same system and generated grid
+    share one device k table: the results equal a fresh context's, whichever
+    plan is destroyed first, and a plan on another grid (or another system)
+    gets its own table."""
+    sys, pulses, grid = _dirac_batch()
+    opts = api.solver(1e-10, 1e-10)
+    p1 = engine.plan(sys, pulses[:1], grid, opts)
+    p2 = engine.plan(sys, pulses[1:2], grid, opts)
+    p3 = engine.plan(sys, pulses[1:2], api.grid_tensor(40, 40, -2, 2, -2, 2), opts)
+    sys_m = api.system(api.SYS_DIRAC2D, velocity=1.0, mass=0.07)
+    p4 = engine.plan(sys_m, pulses[1:2], grid, opts)
+    p1.close()  # p2 keeps the shared table alive
+    fresh = api.Engine(0)
+    try:
+        for pl, (s, g) in ((p2, (sys, grid)), (p3, (sys, api.grid_tensor(40, 40, -2, 2, -2, 2))),
+                           (p4, (sys_m, grid))):
+            pl.execute_async()
+            j, _ = pl.fetch()
+            ref, _ = fresh.current_density(s, pulses[1:2], g, opts)
+            assert np.array_equal(j, ref)
+        # a plan built after the others were closed, on the first grid again
+        for pl in (p2, p3, p4):
+            pl.close()
+        p5 = engine.plan(sys, pulses[:1], grid, opts)
+        p5.execute_async()
+        j, _ = p5.fetch()
+        ref, _ = fresh.current_density(sys, pulses[:1], grid, opts)
+        assert np.array_equal(j, ref)
+        p5.close()
+    finally:
+        fresh.close()
