@@ -349,7 +349,11 @@ hhg_status hhg_gpu_spectrum(hhg_ctx *ctx, const double *j, int n_measurements, d
                             double t_end, double *re_out, double *im_out, double *freq_out);
 
 /* Plans: build the k table, pulse staging and work list once, then execute
- * on device-resident buffers. */
+ * on device-resident buffers.  Plans of one context built from the same
+ * system and generated grid (not HHG_GRID_EXPLICIT rows, not the PiFlux-3D
+ * cost-ordered tables of the NONE / CARRY proposers) share one read-only
+ * device k table; the context keeps the last such table (n_k x 64 bytes)
+ * until another system or grid replaces it or the context is destroyed. */
 hhg_status hhg_plan_create(hhg_ctx *ctx, const hhg_system_desc *sys,
                            const hhg_pulse_desc *pulses, int n_pulses,
                            const hhg_grid_desc *grid, const hhg_solver_opts *opts,
