@@ -634,9 +634,10 @@ def our_arm(args):
     value = args.steps * spectra_per_step / (elapsed_ms * 1e-3)
 
     # end to end through the public one-shot API with host buffers: every
-    # step a new batch (a plan-cache miss: the host builds and uploads the k
-    # rows, pulse records and time grids, the device stages the pulses), j
-    # back, then each pulse's spectrum from its host j
+    # step a new batch (a plan-cache miss: the host builds and uploads the
+    # pulse records and time grids, the device stages the pulses; the k table
+    # of the grid is the context's shared one), j back, then each pulse's
+    # spectrum from its host j
     e2e = None
     if not args.no_e2e and not strong:
         n_e2e = max(1, min(args.steps, 3))
@@ -665,22 +666,20 @@ def our_arm(args):
             t = torch.tensor([el], device="cuda", dtype=torch.float64)
             torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
             el = float(t.item())
-        # bytes copied per step: in, the k rows (64 B each) unless the plan was
-        # cached, the pulse records (256 B) and time grids (8 B x samples) of
-        # the batch, and each pulse's j into its spectrum call; out, j and
-        # each spectrum's frequencies, real and imaginary parts
+        # bytes copied per step: in, the pulse records (256 B) and time grids
+        # (8 B x samples) of the batch and each pulse's j into its spectrum
+        # call (the k rows were uploaded once, by the first plan on the grid);
+        # out, j and each spectrum's frequencies, real and imaginary parts
         for p in batches[e_batches[0]]:
             n_s = p.n_measurements + 1
             n_fft = 4 * n_s + 1
             h2d += 256 + 8 * n_s + 8 * n_s
             d2h += 8 * n_s + 3 * 8 * n_fft
-        if nb > 1:
-            h2d += wl.n_k * 64
         e2e = {"value": ws * n_e2e * pps / el, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h),
                "path": "Engine.current_density + Engine.spectrum (hhg_gpu_current_density + "
                        "hhg_gpu_spectrum), host buffers, wall clock" +
-                       (", a new batch every step (plan built and k rows uploaded)" if nb > 1 else
+                       (", a new batch every step (plan built on the grid's shared k table)" if nb > 1 else
                         ", plan cached by the context after the first call")}
 
     if rank != 0:
