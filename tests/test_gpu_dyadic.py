@@ -6,8 +6,9 @@ intervals) on a 32 x 32 grid, against the CPU oracle (FP64, the reference's
 restart controller at 1e-12 / 1e-8).  In FP64 the default bound is the
 controller's growth rule (1/600) and a looser one (1/128) stays within the
 tolerance-level distance of the oracle; in mixed precision the default is
-1/64, which takes fewer attempts than the growth rule and is as accurate.  Every step is still judged by the embedded error
-estimate.  Out-of-range bounds are refused.
+1/64, which takes fewer attempts than the growth rule and is as accurate.
+Every step is still judged by the embedded error estimate.  Out-of-range
+bounds are refused.
 """
 import math
 
