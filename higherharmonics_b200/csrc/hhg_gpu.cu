@@ -1919,6 +1919,12 @@ hhg_status hhg_learned_collect(hhg_ctx *ctx, const hhg_system_desc *sys,
     hhg_plan *pl = nullptr;
     hhg_status st = hhg_plan_create(ctx, sys, pulses, n_pulses, grid, &o, &pl);
     if (st != HHG_OK) return st;
+    if (pl->degree == 0) {
+        hhg_plan_destroy(pl);
+        return set_err(ctx, HHG_UNSUPPORTED,
+                       "spline pulse too steep for the staged interpolants: its exact evaluation "
+                       "runs the Brillouin-zone current only, without history recording");
+    }
     pl->record = true;
     pl->hist_every = hist_every;
     pl->hist_cap = cap;

@@ -120,6 +120,16 @@ def test_steep_spline_refused_by_the_fast_variants(engine, okw):
     assert ei.value.status == api.UNSUPPORTED and "exact evaluation" in str(ei.value)
 
 
+def test_steep_spline_refused_by_history_collection(engine):
+    n = 256
+    pulse = api.spline_pulse(_quench_template(n), 0.0, 6 * math.pi / (n - 1), 2048,
+                             (0.0, 6 * math.pi), deriv=(0.0, 0.0), energy_scale=10.0)
+    with pytest.raises(api.HHGError) as ei:
+        engine.learned_collect(api.system(api.SYS_DIRAC2D, velocity=1.0, mass=0.05), [pulse],
+                               api.grid_tensor(4, 4, -2, 2, -2, 2), api.solver(), cap=64)
+    assert ei.value.status == api.UNSUPPORTED and "exact evaluation" in str(ei.value)
+
+
 def test_spline_pulse_lockstep_meets_harmonic_bar(engine):
     from higherharmonics_b200.analysis import (default_max_order, harmonic_intensities,
                                                harmonic_rel_err as herr_fn)
