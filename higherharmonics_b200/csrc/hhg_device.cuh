@@ -602,7 +602,7 @@ template <typename R, bool X> struct HoneycombState {
     using N = Num<R>;
     static constexpr int Q2 = X ? 2 : 4;
     typename N::V pc0, ps0, pc1, ps1, pc2, ps2, mc0, mc1, mc2;  // pf cos/sin(nn_j . k), -pf cos
-    double c0, s0, c1, s1, c2, s2;                              // cos/sin(nn_j . k)
+    double c0, s0, c1, s1, c2, s2;  // cos/sin(nn_j . k); X: c1, s1 hold bonds 2 + 3 (c2 = s2 = 0)
     float2 pc_hi, ps_hi, mc_hi;                                 // X, FP32: (bond 1, bonds 2+3) pairs
     R dm;
     double pf, px, py;
@@ -620,6 +620,10 @@ template <typename R, bool X> struct HoneycombState {
                 ps_hi = make_float2(ps0.x, ps1.x);
                 mc_hi = make_float2(mc0.x, mc1.x);
             }
+            // bonds 2 and 3 see the same field projection: only their sum enters
+            c1 += c2;
+            s1 += s2;
+            c2 = s2 = 0.0;
         } else {
             pc1 = N::mk(pf * c1), ps1 = N::mk(pf * s1), mc1 = N::mk(-pf * c1);
             pc2 = N::mk(pf * c2), ps2 = N::mk(pf * s2), mc2 = N::mk(-pf * c2);
@@ -663,6 +667,13 @@ template <typename R, bool X> struct HoneycombState {
     }
     __device__ __forceinline__ double vertex(const double *r, const double *S) const {
         // shifted_grad_gamma and the projection (Honeycomb.cpp:49-61, 273-279, 328-330)
+        if constexpr (X) {
+            // field along x (pol_y = 0): only the x component of the gradient
+            // projects; bonds 2 and 3 share the staged phase, their sum is in c1, s1
+            const double e0r = c0 * r[1] + s0 * r[2], e0i = s0 * r[1] - c0 * r[2];
+            const double e1r = c1 * r[3] + s1 * r[4], e1i = s1 * r[3] - c1 * r[4];
+            return ((e0r - 0.5 * e1r) * S[0] + (e0i - 0.5 * e1i) * S[1]) * px;
+        }
         const double nny = 0.5 * 1.732050807568877293527446341;
         const double e0r = c0 * r[1] + s0 * r[2], e0i = s0 * r[1] - c0 * r[2];
         const double e1r = c1 * r[3] + s1 * r[4], e1i = s1 * r[3] - c1 * r[4];
@@ -677,9 +688,8 @@ template <typename R, bool X> struct HoneycombState {
         // d = t (Re g', -Im g', mass) = 0.5 (pf Re g', -pf Im g', 2 mass)
         double gre, gim;
         if constexpr (X) {
-            const double c12 = c1 + c2, s12 = s1 + s2;
-            gre = (c0 * f[0] + s0 * f[1]) + (c12 * f[2] + s12 * f[3]);
-            gim = (s0 * f[0] - c0 * f[1]) + (s12 * f[2] - c12 * f[3]);
+            gre = (c0 * f[0] + s0 * f[1]) + (c1 * f[2] + s1 * f[3]);
+            gim = (s0 * f[0] - c0 * f[1]) + (s1 * f[2] - c1 * f[3]);
         } else {
             gre = (c0 * f[0] + s0 * f[1]) + (c1 * f[2] + s1 * f[3]) + (c2 * f[Q2] + s2 * f[Q2 + 1]);
             gim = (s0 * f[0] - c0 * f[1]) + (s1 * f[2] - c1 * f[3]) + (s2 * f[Q2] - c2 * f[Q2 + 1]);
