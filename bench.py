@@ -1044,9 +1044,9 @@ def ncu_case(args):
     profile summaries name a command that runs committed files only): the
     same grid and pulse shape over --ncu-cycles cycles (default 1: 1024
     intervals) and the first --ncu-pulses pulse instances, two executions of
-    the selected variant (the learned variants train on the workload's
-    training sources, 2 epochs); with --variant mlp_train, history collection
-    on that case and 2 epochs of proposer training.  Prints one line, no
+    the selected variant (the learned variants first collect histories on the
+    case itself, one launch, and train 2 epochs); with --variant mlp_train,
+    history collection on that case and 2 epochs of proposer training.  Prints one line, no
     timing."""
     from higherharmonics_b200 import api
     from higherharmonics_b200 import workloads as W
