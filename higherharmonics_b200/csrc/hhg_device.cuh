@@ -83,6 +83,7 @@ template <int M> struct Traits {
     static constexpr int kMinBlocks = kMinBlocksPerSM;
     static constexpr bool kPacked = false;
     static constexpr bool kPairs = false;
+    static constexpr bool kHiFirst = false;
 };
 template <> struct Traits<DIRAC2D> : Traits<-1> { static constexpr int NF = 1; };
 template <> struct Traits<DIRAC3D> : Traits<-1> { static constexpr int NF = 1; };
@@ -101,9 +102,11 @@ template <> struct Traits<HONEYCOMB_X> : Traits<-1> {
     static constexpr int NF = 4;
     static constexpr bool kPacked = true;
     static constexpr bool kPairs = true;
+    static constexpr bool kHiFirst = true;  // FP32 products of the leading parts only
 };
 template <> struct Traits<PIFLUX3D_RELAX> {
     static constexpr bool kPairs = false;
+    static constexpr bool kHiFirst = false;
     static constexpr int NF = 2;
     static constexpr bool kRelax = true;
     static constexpr bool kStart = true;
@@ -113,6 +116,7 @@ template <> struct Traits<PIFLUX3D_RELAX> {
 };
 template <> struct Traits<HONEYCOMB_RELAX> {
     static constexpr bool kPairs = false;
+    static constexpr bool kHiFirst = false;
     static constexpr int NF = 6;
     static constexpr bool kRelax = true;
     static constexpr bool kStart = false;
@@ -120,6 +124,7 @@ template <> struct Traits<HONEYCOMB_RELAX> {
 };
 template <> struct Traits<DIRAC3D_RELAX> {
     static constexpr bool kPairs = false;
+    static constexpr bool kHiFirst = false;
     static constexpr int NF = 1;
     static constexpr bool kRelax = true;
     static constexpr bool kStart = false;
@@ -172,6 +177,14 @@ __host__ __device__ __forceinline__ float2 pair_slot(const double *v, int n) {
     const float ha = (float)v[a], hb = (float)v[b];
     return (n & 1) ? make_float2((float)(v[a] - (double)ha), (float)(v[b] - (double)hb))
                    : make_float2(ha, hb);
+}
+// Slot n of a model's paired layout: the order above or, for the models whose
+// FP32 products take the leading parts only (Traits::kHiFirst), the leading
+// pairs first -- (hi cos, hi sin, lo cos, lo sin) -- so one 16-byte load
+// brings both.
+template <bool HI_FIRST>
+__host__ __device__ __forceinline__ float2 pair_slot_ordered(const double *v, int n) {
+    return pair_slot(v, HI_FIRST ? (((n & 1) << 1) | (n >> 1)) : n);
 }
 
 // Fehlberg 7(8) nodes c_s (E. Fehlberg, NASA TR R-287, 1968).
@@ -376,7 +389,7 @@ template <> struct Num<float> {
 // (A(t) from the pulse's own form, then the staged functions), for spline
 // pulses whose knots a per-interval polynomial cannot follow (a step between
 // two knots, QuenchedField.cpp:15-29).  FP64 only.
-template <int NF, int D, typename R, bool PAIR = false>
+template <int NF, int D, typename R, int PAIR = 0>
 struct PolyEval {
     static constexpr bool kReuse = true;  // stages sharing a node reuse the values
     const double *hd;  // interval record
@@ -410,22 +423,29 @@ struct PolyEval {
                 v[n] = inside ? x : outside_value<NF>(n);
             }
         }
-        if constexpr (PAIR) {
+        if constexpr (PAIR != 0) {
             static_assert(NF == 4, "the paired layout holds two projections");
 #pragma unroll
-            for (int n = 0; n < 4; ++n) f[n] = pair_slot(v, n);
+            for (int n = 0; n < 4; ++n) f[n] = pair_slot_ordered<PAIR == 2>(v, n);
         } else {
 #pragma unroll
             for (int n = 0; n < NF; ++n) f[n] = Num<R>::mk(v[n]);
         }
     }
 };
-// the paired layout applies to the kPairs models' FP32 path
-template <int M, typename R> __host__ __device__ constexpr bool pair_layout() {
-    return Traits<M>::kPairs && sizeof(R) == sizeof(float);
+// the paired layout applies to the kPairs models' FP32 path: 0 none, 1 the
+// standard order, 2 leading pairs first
+template <int M, typename R> __host__ __device__ constexpr int pair_layout() {
+    return (Traits<M>::kPairs && sizeof(R) == sizeof(float)) ? (Traits<M>::kHiFirst ? 2 : 1) : 0;
+}
+// staged values a table read must deliver: the leading pairs only for kHiFirst
+template <int M, typename R> __host__ __device__ constexpr int table_values() {
+    return pair_layout<M, R>() == 2 ? 2 : Traits<M>::NF;
 }
 
-template <int NF, typename R>
+// NV: the leading values of a row the caller reads (NF, or 2 for the
+// leading-pairs-first layout).
+template <int NF, typename R, int NV = NF>
 struct TableEval {
     static constexpr bool kReuse = false;  // a shared-memory reload is cheaper than registers
     const typename Num<R>::V *tab;  // 13 x NF values of one standard step (16-byte aligned)
@@ -435,7 +455,7 @@ struct TableEval {
             using V2 = typename std::conditional<sizeof(R) == sizeof(float), float4, double2>::type;
             const V2 *t2 = reinterpret_cast<const V2 *>(tab + s * NF);
 #pragma unroll
-            for (int n = 0; n < NF / 2; ++n) {
+            for (int n = 0; n < (NV + 1) / 2; ++n) {
                 const V2 w = t2[n];
                 if constexpr (sizeof(R) == sizeof(float)) {
                     f[2 * n] = make_float2(w.x, w.y);
@@ -651,15 +671,16 @@ template <typename R, bool X> struct HoneycombState {
         dS[1] = -(S[2] * gr) + dm * S[0];
         dS[2] = S[0] * gi + S[1] * gr;
     }
-    // FP32, field along x, staged values in the paired layout: the two bond
+    // FP32, field along x, staged values in the leading-pairs-first layout
+    // (f[0] = hi cos of both projections, f[1] = hi sin): the two bond
     // groups' products of the leading parts (no compensation: see Num) sit in
     // the two halves of paired FMAs, summed at the end:
     // pf Re g' = PC.FC + PS.FS, pf Im g' = PS.FC - PC.FS.
     __device__ __forceinline__ void rhs2(const float2 *f, float2 s_xy, float s_z, float2 &d_xy,
                                          float &d_z) const {
         static_assert(X, "paired right-hand side: field along x");
-        const float2 re = __ffma2_rn(pc_hi, f[0], __fmul2_rn(ps_hi, f[2]));
-        const float2 im = __ffma2_rn(ps_hi, f[0], __fmul2_rn(mc_hi, f[2]));
+        const float2 re = __ffma2_rn(pc_hi, f[0], __fmul2_rn(ps_hi, f[1]));
+        const float2 im = __ffma2_rn(ps_hi, f[0], __fmul2_rn(mc_hi, f[1]));
         const float gr = re.x + re.y, gi = im.x + im.y;
         const float dmf = float(dm);
         d_xy = make_float2(fmaf(-s_z, gi, -(dmf * s_xy.y)), fmaf(-s_z, gr, dmf * s_xy.x));
@@ -1307,7 +1328,7 @@ __device__ __forceinline__ void lane_controller(const KParams &P, const ModelSta
         if (active) {
             double xn[3], e[3], k0[3];
             if (table) {
-                const TableEval<NF, R> tev{tabv + wa * 13 * NF};
+                const TableEval<NF, R, table_values<M, R>()> tev{tabv + wa * 13 * NF};
                 rkf78_attempt<M, NF, R>(ms, tev, t, dt, S, xn, e, k0);
             } else {
                 rkf78_attempt<M, NF, R>(ms, poly, t, dt, S, xn, e, k0);
@@ -1535,7 +1556,7 @@ __global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integ
     constexpr int TAB = slot_table(NF, D);
     constexpr int DYA = slot_dyadic(NF, D);
     constexpr bool kNarrow = sizeof(R) != sizeof(double);
-    constexpr bool kPair = pair_layout<M, R>();
+    constexpr int kPair = pair_layout<M, R>();
     // only the reference schedule reads the standard table; the dyadic table
     // is read from global memory
     // the relaxation models on the reference schedule run free lanes (above)
@@ -1640,7 +1661,8 @@ __global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integ
                         __syncwarp();
                         for (int c = lane; c < NTAB; c += 32) {
                             if constexpr (kPair)
-                                stage_tab[wib][c] = pair_slot(slot + TAB + (c & ~3), c & 3);
+                                stage_tab[wib][c] =
+                                    pair_slot_ordered<Traits<M>::kHiFirst>(slot + TAB + (c & ~3), c & 3);
                             else
                                 stage_tab[wib][c] = Num<R>::mk(slot[TAB + c]);
                         }
@@ -1755,7 +1777,8 @@ __global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integ
                             if (!dead) {
                                 double e[3], k0[3];
                                 if (L < kDyaLevels) {
-                                    const TableEval<NF, R> tev{dtab + ((1 << L) - 1 + qpos) * 13 * NF};
+                                    const TableEval<NF, R, table_values<M, R>()> tev{
+                                        dtab + ((1 << L) - 1 + qpos) * 13 * NF};
                                     rkf78_attempt<M, NF, R>(ms, tev, tq, h, S, xn, e, k0);
                                 } else {
                                     rkf78_attempt<M, NF, R>(ms, poly, tq, h, S, xn, e, k0);
@@ -2002,7 +2025,7 @@ __global__ void stage_pulses_kernel(const PulseDev *__restrict__ pulses, int n_p
                         if constexpr (LAYOUT == 1) {
                             *dst = v[n];
                         } else if constexpr (Traits<M>::kPairs) {
-                            *reinterpret_cast<float2 *>(dst) = pair_slot(v, n);
+                            *reinterpret_cast<float2 *>(dst) = pair_slot_ordered<Traits<M>::kHiFirst>(v, n);
                         } else {
                             const float hi = (float)v[n];
                             *reinterpret_cast<float2 *>(dst) = make_float2(hi, (float)(v[n] - (double)hi));
