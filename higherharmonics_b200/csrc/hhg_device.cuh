@@ -1519,6 +1519,11 @@ __device__ void integrate_free(const KParams &P, const PulseDev &pd, const Model
 }
 
 constexpr int kLevelMax = 10;
+// 2^-L for 0 <= L <= 1022, exactly: the dyadic step span * 2^-L equals
+// ldexp(span, -L) without its range handling
+__device__ __forceinline__ double pow2_neg(int L) {
+    return __longlong_as_double((long long)(1023 - L) << 52);
+}
 // dynamic shared memory of the learned-proposer kernels
 __host__ __device__ constexpr int mlp_smem_bytes() { return mlp_stage_bytes(kWarpsPerBlock); }
 // Default coarsening bounds of the dyadic stepping: a warp halves its level
@@ -1770,7 +1775,7 @@ __global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integ
                         const bool from_floor = level == 0;
                         bool fallback = false, coarse_end = false, refined = false;
                         for (;;) {
-                            const double h = ldexp(span, -L);
+                            const double h = span * pow2_neg(L);
                             const double tq = t0 + qpos * h;
                             bool ok = true, small = true;
                             double xn[3];
@@ -1820,7 +1825,7 @@ __global__ void __launch_bounds__(kBlockThreads, Traits<M>::kMinBlocks) bz_integ
                         }
                         if (fallback) {
                             // the plain controller takes over for the rest of the interval
-                            const double h = ldexp(span, -L);
+                            const double h = span * pow2_neg(L);
                             lane_controller<M, NF, D, R, false, false>(
                                 P, ms, poly, slot, tabv, 0, t0 + qpos * h, 0.5 * h, t1, S, dead,
                                 carry_dt, my_attempts, my_rejects);
